@@ -1,0 +1,461 @@
+#!/usr/bin/env python
+"""Benchmark of x3div's Euler-timestep hot path on B200.
+
+Workload (one "step"): the plain derivative sweep of a 512^3 periodic box --
+u, v, w = Taylor-Green field + seeded Gaussian noise (amplitude 1e-3), and
+for each field and each direction the six compact operator families (first
+derivative, second derivative, staggered derivative v->p and p->v,
+interpolation v->p and p->v), each an explicit stencil + cyclic Thomas solve
+over all 512^2 lines of the direction: 54 operator applications per step.
+
+  value    : derivative Gpts/s of the FP32-mixed path (FP32 fields and
+             sweeps, FP64 coefficients and Sherman-Morrison scalar), inputs
+             resident in HBM, CUDA events on the launching stream, max over
+             ranks.  The plain FP64 path's figure is under "fp64", and the
+             full Euler step (transeq + int_time + divergence + FP64 Poisson
+             + gradp + cor_vel) in ms under "euler_step_ms".
+  e2e      : the same sweep through x3d_apply_batch with pinned HOST buffers:
+             each field uploaded once, all 18 of its outputs downloaded.
+  roofline : the dominant line-solve kernel, algorithmic bytes (one read +
+             one write of the field per application) / its average launch
+             time, against the measured HBM copy bandwidth.
+
+--impl reference times the reference's algorithm on the host cores: the
+reference (Fortran + MPI + 2decomp&FFT) cannot be built in this image, so
+this is the FP64 C restatement in oracle/ (OpenMP, all host threads) on a
+bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "derivative Gpts/s and Euler-step ms at 512^3: FP32-mixed vs FP64, 1 B200"
+KINDS = [("der", ("derx", "dery", "derz")), ("der2", ("derxx", "deryy", "derzz")),
+         ("dervp", ("derxvp", "deryvp", "derzvp")), ("derpv", ("derxpv", "derypv", "derzpv")),
+         ("intvp", ("intxvp", "intyvp", "intzvp")), ("intpv", ("intxpv", "intypv", "intzpv"))]
+FAMILY = {0: "ls_x_bulk", 1: "ls_yz_tma(y)", 2: "ls_yz_tma(z)"}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=512)
+    ap.add_argument("--no-euler", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    return ap.parse_args()
+
+
+def tg_noise(n, seed, amp=1e-3):
+    """Taylor-Green velocity + N(0, amp^2) noise on an n^3 box of side 2 pi,
+    returned as a C-contiguous (z, y, x) float64 array (= Fortran (x, y, z))."""
+    rng = np.random.default_rng(seed)
+    x = np.arange(n) * (2 * np.pi / n)
+    s, c = np.sin(x), np.cos(x)
+    comp = seed % 3
+    if comp == 0:      # u = sin x cos y cos z
+        f = c[:, None, None] * c[None, :, None] * s[None, None, :]
+    elif comp == 1:    # v = -cos x sin y cos z
+        f = -c[:, None, None] * s[None, :, None] * c[None, None, :]
+    else:              # w = 0
+        f = np.zeros((n, n, n))
+    f = f + amp * rng.standard_normal((n, n, n))
+    return np.ascontiguousarray(f)
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        rows = [r.split(",") for r in out.strip().splitlines() if r.count(",") >= 8]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if "Active" in r[5 + k]})
+        load = [v for v in sm if mx and v > 0.5 * max(mx)] or sm
+        return {"sm_mhz": statistics.median(load) if load else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per launch of each line-solve kernel from the committed ncu
+    summary (profiles/linesolve_traffic.json), scaled to this size."""
+    p = os.path.join(ROOT, "profiles", "linesolve_traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def dist_setup(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "b200" else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    elif args.impl == "b200":
+        torch.cuda.set_device(local)
+    return world, rank, local
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# --------------------------------------------------------------------------
+def cpu_sample(n, reps=1):
+    """The oracle on a bounded sample: one operator per direction (derx,
+    interyvp, derzz) on one n^3 FP64 field, all host threads."""
+    from oracle import oracle as O
+    O.lib()
+    f = np.asfortranarray(tg_noise(n, 0).transpose(2, 1, 0))
+    d = 2 * np.pi / n
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        O.apply("der", 0, f, d)
+        O.apply("intvp", 1, f, d)
+        O.apply("der2", 2, f, d)
+        times.append(time.perf_counter() - t0)
+    pts = 3.0 * n ** 3
+    return pts, times
+
+
+def cpu_threads():
+    return int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    n = args.n
+    sample = ("oracle/ (FP64 C restatement, OpenMP) applying derx, interyvp, derzz to one "
+              f"{n}^3 field per step (3 of the 54 applications of a sweep step)")
+    pts, _ = cpu_sample(n, reps=max(1, args.warmup))
+    pts, times = cpu_sample(n, reps=args.steps)
+    t = sum(times)
+    val = pts * args.steps / t / 1e9
+    cores = cpu_threads()
+    line = {
+        "metric": METRIC, "value": round(val, 4), "unit": "Gpts/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * t / args.steps, 2),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": f"periodic compact derivative sweep, {n}^3, TG + 1e-3 noise",
+                   "sample": sample, "parallelism": f"{cores} host threads"},
+        "cpu_baseline": {"value": round(val, 4), "unit": "Gpts/s", "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": round(val, 4), "unit": "Gpts/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "note": "reference Fortran/MPI build unavailable (no gfortran, MPI or 2decomp&FFT); "
+                "timed the oracle restatement of its algorithm",
+    }
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------
+def sweep_items(ctx, fields, outs):
+    items = []
+    k = 0
+    for f in fields:
+        for kind, names in KINDS:
+            for d, name in enumerate(names):
+                items.append((d, ctx.op(name), f, outs[k % len(outs)]))
+                k += 1
+    return items
+
+
+def timed_sweep(ctx, torch, fields, outs, steps, warmup, world, per_launch=True):
+    from x3div_b200._capi import Work
+    items = sweep_items(ctx, fields, outs)
+    stream = torch.cuda.current_stream()
+    L = ctx.L
+    h = ctx.handle
+
+    def apply(op, src, dst):
+        arr = (Work * 1)()
+        arr[0].op, arr[0].in_, arr[0].out = op.handle, src.data_ptr(), dst.data_ptr()
+        rc = L.x3d_apply_batch(h, arr, 1)
+        if rc:
+            ctx._check(rc)
+
+    for _ in range(warmup):
+        for d, op, src, dst in items:
+            apply(op, src, dst)
+    ctx.sync()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(steps * len(items))] if per_launch else []
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    k = 0
+    for _ in range(steps):
+        for d, op, src, dst in items:
+            if per_launch:
+                ev[k][0].record(stream)
+            apply(op, src, dst)
+            if per_launch:
+                ev[k][1].record(stream)
+            k += 1
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ctx.sync()
+    ms = t0.elapsed_time(t1)
+    fam = {}
+    for k, (d, op, src, dst) in enumerate(items * steps):
+        if per_launch:
+            fam.setdefault(d, []).append(ev[k][0].elapsed_time(ev[k][1]))
+    barrier(world)
+    return ms, fam, len(items)
+
+
+def run_b200(args, world, rank, local):
+    import torch
+
+    from x3div_b200 import Context
+    n = args.n
+    npts = n ** 3
+    peak, peak_kind = measured_peak()
+    clocks = Clocks(local)
+    out = {}
+
+    # ---- FP32-mixed sweep (headline) ---------------------------------------
+    ctx = Context(n, n, n, lengths=(2 * np.pi,) * 3, precision="f32", device=local,
+                  stream=torch.cuda.current_stream())
+    host = [tg_noise(n, s + 3 * rank) for s in range(3)]
+    fields = [torch.from_numpy(h).to(device="cuda", dtype=torch.float32) for h in host]
+    outs = [torch.empty_like(fields[0]) for _ in range(6)]
+    clocks.start()
+    ms, fam, nitems = timed_sweep(ctx, torch, fields, outs, args.steps, args.warmup, world)
+    ms = max_over_ranks(ms, world)
+    pts_step = nitems * npts
+    value = world * pts_step * args.steps / (ms * 1e-3) / 1e9
+    es = 4
+    fam_stats = {}
+    for d, ts in fam.items():
+        avg = sum(ts) / len(ts)
+        fam_stats[FAMILY[d]] = {"launches": len(ts), "avg_ms": round(avg, 4),
+                                "gbs": round(2 * npts * es / (avg * 1e-3) / 1e9, 1),
+                                "share": round(sum(ts) / sum(sum(v) for v in fam.values()), 3)}
+    dom_d = max(fam, key=lambda d: sum(fam[d]))
+    dom = fam_stats[FAMILY[dom_d]]
+    traffic = profiled_traffic().get(FAMILY[dom_d] + ":f32")
+    traffic_bytes = None
+    if traffic:
+        traffic_bytes = traffic["bytes_per_point"] * npts
+    roofline = {"bound": "hbm", "achieved": dom["gbs"], "peak": peak, "unit": "GB/s",
+                "frac": round(dom["gbs"] / peak, 3), "traffic": traffic_bytes,
+                "kernel": FAMILY[dom_d], "algorithmic_bytes_per_launch": 2 * npts * es,
+                "peak_source": peak_kind}
+    out.update(value=value, ms=ms, fam=fam_stats, roofline=roofline, launches=args.steps * nitems)
+
+    # ---- e2e: host buffers through x3d_apply_batch ---------------------------
+    if not args.no_e2e:
+        pin_in = [torch.from_numpy(h.astype(np.float32)).pin_memory() for h in host]
+        pin_out = [torch.empty((n, n, n), dtype=torch.float32).pin_memory() for _ in range(18)]
+        e2e_steps = max(1, min(args.steps, 2))
+
+        def e2e_step():
+            for f in pin_in:
+                items = []
+                k = 0
+                for kind, names in KINDS:
+                    for name in names:
+                        items.append((ctx.op(name), f.numpy(), pin_out[k].numpy()))
+                        k += 1
+                ctx.apply_batch(items)
+
+        e2e_step()
+        torch.cuda.synchronize()
+        barrier(world)
+        t = time.perf_counter()
+        for _ in range(e2e_steps):
+            e2e_step()
+        torch.cuda.synchronize()
+        el = max_over_ranks(time.perf_counter() - t, world)
+        out["e2e"] = {"value": round(world * pts_step * e2e_steps / el / 1e9, 3), "unit": "Gpts/s",
+                      "h2d_bytes_per_step": 3 * npts * 4, "d2h_bytes_per_step": nitems * npts * 4,
+                      "api": "x3d_apply_batch with pinned host buffers"}
+        del pin_in, pin_out
+    del fields, outs
+
+    # ---- Euler step, FP32-mixed ---------------------------------------------
+    def euler_ms(c, dt_torch):
+        U = [torch.from_numpy(h).to(device="cuda", dtype=dt_torch) for h in host]
+        du = [torch.empty_like(U[0]) for _ in range(3)]
+        pg = [torch.empty_like(U[0]) for _ in range(3)]
+        pp3 = torch.empty((n, n, n), dtype=torch.float64, device="cuda")
+        for _ in range(2):
+            c.euler_step(*U, *du, pp3, *pg, 5e-4)
+        c.sync()
+        barrier(world)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 3
+        a.record()
+        for _ in range(reps):
+            c.euler_step(*U, *du, pp3, *pg, 5e-4)
+        b.record()
+        torch.cuda.synchronize()
+        c.sync()
+        c.divergence(pp3, *U)
+        mx, mean = c.div_stats(pp3)
+        return max_over_ranks(a.elapsed_time(b) / reps, world), mx
+
+    if not args.no_euler:
+        out["euler_f32"] = euler_ms(ctx, torch.float32)
+    ctx.close()
+    torch.cuda.empty_cache()
+
+    # ---- plain FP64 path -------------------------------------------------------
+    if not args.no_fp64:
+        ctx64 = Context(n, n, n, lengths=(2 * np.pi,) * 3, precision="f64", device=local,
+                        stream=torch.cuda.current_stream())
+        fields = [torch.from_numpy(h).to(device="cuda") for h in host]
+        outs = [torch.empty_like(fields[0]) for _ in range(6)]
+        ms64, fam64, _ = timed_sweep(ctx64, torch, fields, outs, args.steps, args.warmup, world,
+                                     per_launch=True)
+        ms64 = max_over_ranks(ms64, world)
+        f64 = {"value": round(world * pts_step * args.steps / (ms64 * 1e-3) / 1e9, 2),
+               "ms_per_step": round(ms64 / args.steps, 3)}
+        f64["kernels"] = {FAMILY[d]: {"avg_ms": round(sum(ts) / len(ts), 4),
+                                      "gbs": round(2 * npts * 8 / (sum(ts) / len(ts) * 1e-3) / 1e9, 1)}
+                          for d, ts in fam64.items()}
+        out["fp64"] = f64
+        del fields, outs
+        if not args.no_euler:
+            out["euler_f64"] = euler_ms(ctx64, torch.float64)
+        ctx64.close()
+    out["clocks"] = clocks.stop()
+    return out, pts_step
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    res, pts_step = run_b200(args, world, rank, local)
+    if rank == 0:
+        n = args.n
+        sample_n = min(n, 512)
+        pts, times = cpu_sample(sample_n, reps=1)
+        cpu_val = pts / times[0] / 1e9
+        line = {
+            "metric": METRIC,
+            "value": round(res["value"], 2),
+            "unit": "Gpts/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(res["ms"] / args.steps, 3),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32 (f64 coefficients and Sherman-Morrison scalar)",
+            "data": "synthetic",
+            "config": {"workload": f"periodic compact derivative sweep, {n}^3 per GPU, 3 fields x "
+                                   "6 operator families x 3 directions = 54 line-solve applications "
+                                   "per step", "grid": [n, n, n], "fields": "Taylor-Green + seeded N(0, (1e-3)^2) noise",
+                       "l2": "inputs (0.5 GB per field) larger than L2; no flush",
+                       "parallelism": f"{world} independent box(es), one per GPU"},
+            "gpu_launches": res["launches"],
+            "roofline": res["roofline"],
+            "kernels": res["fam"],
+            "cpu_baseline": {"value": round(cpu_val, 4), "unit": "Gpts/s", "cores": cpu_threads(),
+                             "kind": "port",
+                             "sample": f"oracle (FP64 C, OpenMP) derx+interyvp+derzz on one {sample_n}^3 field"},
+        }
+        if "e2e" in res:
+            line["e2e"] = res["e2e"]
+        if "fp64" in res:
+            line["fp64"] = res["fp64"]
+        em = {}
+        if "euler_f32" in res:
+            em["f32_mixed"] = round(res["euler_f32"][0], 2)
+            em["f32_mixed_div_after_max"] = res["euler_f32"][1]
+        if "euler_f64" in res:
+            em["f64"] = round(res["euler_f64"][0], 2)
+            em["f64_div_after_max"] = res["euler_f64"][1]
+        if em:
+            line["euler_step_ms"] = em
+        if res.get("clocks"):
+            line["clocks"] = res["clocks"]
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

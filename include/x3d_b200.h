@@ -1,0 +1,266 @@
+/*
+ * x3d_b200.h -- C ABI of the B200 (sm_100a) implementation of x3div's
+ * Euler-timestep hot path: compact finite-difference derivatives, staggered
+ * derivatives and interpolations (each an explicit stencil followed by a
+ * batched periodic Thomas line solve), pencil transposes, the spectral
+ * Poisson projection and the stage compositions that call them.
+ *
+ * Every entry point mirrors one reference routine (cited beside it as
+ * path:line inside the xcompact3d/x3div source tree) with the same argument
+ * order and meaning, prefixed by a context handle, so that the reference's
+ * Fortran driver can bind to it through ISO_C_BINDING.
+ *
+ * Conventions
+ *  - Fields are (nx, ny, nz) arrays with x fastest (Fortran order), exactly
+ *    the layout of every 2decomp pencil.  At the supported 1x1 decomposition
+ *    the X, Y and Z pencils of a field share this layout.
+ *  - Field pointers are device pointers whose element type is the context
+ *    precision: double for X3D_F64, float for X3D_F32.  Pressure arguments
+ *    (pp3) are always double.  A pointer to ordinary or pinned host memory
+ *    is also accepted: the call then stages it through device memory and
+ *    returns only after the results are back in host memory.
+ *  - Calls on device pointers are asynchronous on the context's stream, as
+ *    CUDA launches are; x3d_ctx_sync() waits and reports device-side errors.
+ *  - Every function returns an int status: X3D_OK (0) or a negative code.
+ *    The reference aborts through decomp_2d_abort instead; a Fortran shim
+ *    maps a non-zero status to that call.
+ *  - Only periodic boundary conditions are supported, as in the reference,
+ *    whose Poisson solver stops on any other (src/poisson.f90:104-108).
+ *    Hence nxm == nx, nym == ny, nzm == nz in the staggered signatures.
+ *  - Line lengths must be >= 8 (the 8-point interpolation stencils).
+ */
+#ifndef X3D_B200_H
+#define X3D_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define X3D_OK 0
+#define X3D_EINVAL -1       /* bad argument: null handle, shape, kind, direction */
+#define X3D_EUNSUPPORTED -2 /* non-periodic boundary condition, line shorter than 8 */
+#define X3D_ECUDA -3        /* CUDA runtime, driver or cuFFT error */
+#define X3D_ENOMEM -4       /* device allocation failed */
+#define X3D_ETIMEOUT -5     /* a bounded device-side wait gave up (error flag set) */
+
+/* field precision of a context */
+#define X3D_F64 0 /* FP64 fields and sweeps */
+#define X3D_F32 1 /* FP32 fields and sweeps; FP64 coefficients, Sherman-Morrison scalar and Poisson */
+
+/* directions */
+#define X3D_DIR_X 0
+#define X3D_DIR_Y 1
+#define X3D_DIR_Z 2
+
+/* operator kinds (x3doperator1d families, src/x3d_operator_1d.f90:32-47) */
+#define X3D_KIND_DER 0   /* 6th-order compact first derivative, derx_00 */
+#define X3D_KIND_DER2 1  /* 6th-order compact second derivative (declared, never built, in the reference) */
+#define X3D_KIND_DERVP 2 /* staggered derivative, velocity -> pressure grid */
+#define X3D_KIND_DERPV 3 /* staggered derivative, pressure -> velocity grid */
+#define X3D_KIND_INTVP 4 /* 6th-order interpolation, velocity -> pressure grid */
+#define X3D_KIND_INTPV 5 /* 6th-order interpolation, pressure -> velocity grid */
+
+/* named operator instances of x3d_operator_1d_init (src/x3d_operator_1d.f90:135-189),
+ * plus the three second-derivative operators the reference declares at
+ * src/x3d_derive.f90:54-59 but never builds */
+#define X3D_OP_DERX 0
+#define X3D_OP_DERXP 1
+#define X3D_OP_DERY 2
+#define X3D_OP_DERYP 3
+#define X3D_OP_DERZ 4
+#define X3D_OP_DERZP 5
+#define X3D_OP_DERXVP 6
+#define X3D_OP_DERYVP 7
+#define X3D_OP_DERZVP 8
+#define X3D_OP_DERXPV 9
+#define X3D_OP_DERYPV 10
+#define X3D_OP_DERZPV 11
+#define X3D_OP_INTXVP 12
+#define X3D_OP_INTYVP 13
+#define X3D_OP_INTZVP 14
+#define X3D_OP_INTXPV 15
+#define X3D_OP_INTYPV 16
+#define X3D_OP_INTZPV 17
+#define X3D_OP_DERXX 18
+#define X3D_OP_DERYY 19
+#define X3D_OP_DERZZ 20
+#define X3D_OP_COUNT 21
+
+typedef struct x3d_ctx_s *x3d_ctx;
+typedef struct x3d_op_s *x3d_op;
+
+/* ---- context ---------------------------------------------------------- */
+
+/* Replaces init_xcompact3d's set-up path (src/x3d_tools.f90:163-185):
+ * parameter() geometry (dx = xlx/nx ...), x3d_operator_{x,y,z}_data_init,
+ * x3d_operator_1d_init, x3d_derive_init and decomp_2d_poisson_init, for a
+ * fully periodic nx*ny*nz box of size xlx*yly*zlz at a 1x1 decomposition.
+ * device: CUDA ordinal.  precision: X3D_F64 or X3D_F32. */
+int x3d_ctx_create(x3d_ctx *ctx, int nx, int ny, int nz, double xlx, double yly, double zlz,
+                   int precision, int device);
+/* finalise_xcompact3d's device-side part (src/x3d_tools.f90:212-248). */
+int x3d_ctx_destroy(x3d_ctx ctx);
+/* Run the context's work on a caller-owned stream (cudaStream_t); NULL
+ * returns to the context's own stream. */
+int x3d_ctx_set_stream(x3d_ctx ctx, void *stream);
+/* Wait for the context's stream; returns X3D_ETIMEOUT if a kernel recorded a
+ * bounded-wait failure since the last call, else a CUDA error or X3D_OK. */
+int x3d_ctx_sync(x3d_ctx ctx);
+/* Text of the last error recorded on this context (never NULL). */
+const char *x3d_ctx_last_error(x3d_ctx ctx);
+/* Geometry query: dims[3], lengths[3], spacing[3] (any may be NULL). */
+int x3d_ctx_geometry(x3d_ctx ctx, int *dims, double *lengths, double *spacing, int *precision);
+
+/* ---- operators: type x3doperator1d (src/x3d_operator_1d.f90:12-30) ---- */
+
+/* One of the X3D_OP_* instances built by x3d_ctx_create. */
+int x3d_op_builtin(x3d_ctx ctx, int which, x3d_op *op);
+/* An operator from explicit x3doperator1d contents, as the reference host
+ * would hand over after its own x3d_operator_1d_init: n, npaire, alfa, the
+ * Thomas arrays f, s, w (see prepare, src/x3d_operator_1d.f90:301-323), the
+ * Sherman-Morrison vector periodic (NULL for a non-periodic operator), plus
+ * the explicit RHS scalars that the reference keeps as module globals of
+ * x3d_operator_{x,y,z}_data (rhs[4] = a, b, c, d, e.g. afix, bfix, 0, 0 for
+ * derx, aicix6..dicix6 for interpolation).  Host pointers, FP64, copied. */
+int x3d_op_create(x3d_ctx ctx, int kind, int dir, int n, int npaire, double alfa,
+                  const double *f, const double *s, const double *w, const double *periodic,
+                  const double *rhs, x3d_op *op);
+int x3d_op_destroy(x3d_ctx ctx, x3d_op op);
+/* Read back an operator's FP64 contents: any output may be NULL.
+ * meta[0..3] = n, kind, dir, npaire; scal[0..4] = alfa, a, b, c, d;
+ * f, s, w, periodic: length n. */
+int x3d_op_info(x3d_op op, int *meta, double *scal, double *f, double *s, double *w,
+                double *periodic);
+
+/* ---- collocated derivatives: x3d_derive (src/x3d_derive.f90:18-59) ---- */
+
+/* derx_00 (src/x3d_derive.f90:111-152): tx = d(ux)/dx */
+int x3d_derx(x3d_ctx ctx, void *tx, const void *ux, x3d_op op, int nx, int ny, int nz);
+/* dery_00 (src/x3d_derive.f90:279-339); ppy is the stretching metric, unused
+ * because istret = 0 (src/parameters.f90:117); may be NULL */
+int x3d_dery(x3d_ctx ctx, void *ty, const void *uy, x3d_op op, const double *ppy, int nx, int ny,
+             int nz);
+/* derz_00 (src/x3d_derive.f90:503-558) */
+int x3d_derz(x3d_ctx ctx, void *tz, const void *uz, x3d_op op, int nx, int ny, int nz);
+/* second derivatives: the DERIVATIVE_X / _YY / _Z pointers derxx, deryy,
+ * derzz (src/x3d_derive.f90:54-59), left null by the reference */
+int x3d_derxx(x3d_ctx ctx, void *tx, const void *ux, x3d_op op, int nx, int ny, int nz);
+int x3d_deryy(x3d_ctx ctx, void *ty, const void *uy, x3d_op op, int nx, int ny, int nz);
+int x3d_derzz(x3d_ctx ctx, void *tz, const void *uz, x3d_op op, int nx, int ny, int nz);
+
+/* ---- staggered operators: x3d_staggered (src/x3d_staggered.f90) -------- */
+
+int x3d_derxvp(x3d_ctx ctx, void *tx, const void *ux, x3d_op op, int nx, int nxm, int ny, int nz);   /* :23-106 */
+int x3d_interxvp(x3d_ctx ctx, void *tx, const void *ux, x3d_op op, int nx, int nxm, int ny, int nz); /* :110-217 */
+int x3d_derxpv(x3d_ctx ctx, void *tx, const void *ux, x3d_op op, int nxm, int nx, int ny, int nz);   /* :221-285 */
+int x3d_interxpv(x3d_ctx ctx, void *tx, const void *ux, x3d_op op, int nxm, int nx, int ny, int nz); /* :289-404 */
+int x3d_interyvp(x3d_ctx ctx, void *ty, const void *uy, x3d_op op, int nx, int ny, int nym, int nz); /* :408-541 */
+int x3d_deryvp(x3d_ctx ctx, void *ty, const void *uy, x3d_op op, const double *ppyi, int nx, int ny,
+               int nym, int nz);                                                                     /* :545-637 */
+int x3d_interypv(x3d_ctx ctx, void *ty, const void *uy, x3d_op op, int nx, int nym, int ny, int nz); /* :641-786 */
+int x3d_derypv(x3d_ctx ctx, void *ty, const void *uy, x3d_op op, const double *ppy, int nx, int nym,
+               int ny, int nz);                                                                      /* :790-883 */
+int x3d_derzvp(x3d_ctx ctx, void *tz, const void *uz, x3d_op op, int nx, int ny, int nz, int nzm);   /* :887-997 */
+int x3d_interzvp(x3d_ctx ctx, void *tz, const void *uz, x3d_op op, int nx, int ny, int nz, int nzm); /* :1001-1139 */
+int x3d_derzpv(x3d_ctx ctx, void *tz, const void *uz, x3d_op op, int nx, int ny, int nzm, int nz);   /* :1143-1229 */
+int x3d_interzpv(x3d_ctx ctx, void *tz, const void *uz, x3d_op op, int nx, int ny, int nzm, int nz); /* :1233-1383 */
+
+/* ---- batched operator applications -------------------------------------- */
+
+/* One operator application of a batch: out = op(in) along op's direction. */
+typedef struct {
+    x3d_op op;      /* built-in or user operator (its kind and direction decide the routine) */
+    const void *in; /* (nx,ny,nz) input field of the context grid */
+    void *out;      /* (nx,ny,nz) output field; must not alias any input of the batch */
+} x3d_work;
+
+/* Apply every item of a work-list, e.g. all the derivative and
+ * interpolation sweeps of one RHS stage.  Items are independent.  With host
+ * pointers each distinct input is uploaded once and every output is
+ * downloaded once, and the call returns when the results are in host
+ * memory.  No reference counterpart: it replaces a sequence of der* and
+ * staggered calls (src/transeq.f90, src/navier.f90) by one call. */
+int x3d_apply_batch(x3d_ctx ctx, const x3d_work *items, int count);
+
+/* ---- batched Thomas line solves: module thomas (src/thomas.f90:15-28) --- */
+
+/* In-place solve of every line of tt.  With perio != NULL this is
+ * ?thomas_0 (periodic, Sherman-Morrison with alfa, :34-58/87-111/139-163);
+ * with perio == NULL it is ?thomas_12 (:61-84/114-136/166-188) and alfa is
+ * ignored.  ff, fs, fw, perio: FP64 arrays of the line length (host or
+ * device memory). */
+int x3d_xthomas(x3d_ctx ctx, void *tt, const double *ff, const double *fs, const double *fw,
+                const double *perio, double alfa, int nx, int ny, int nz);
+int x3d_ythomas(x3d_ctx ctx, void *tt, const double *ff, const double *fs, const double *fw,
+                const double *perio, double alfa, int nx, int ny, int nz);
+int x3d_zthomas(x3d_ctx ctx, void *tt, const double *ff, const double *fs, const double *fw,
+                const double *perio, double alfa, int nx, int ny, int nz);
+
+/* ---- pencil transposes: x3d_transpose (src/x3d_transpose.f90:21-47) ----- */
+
+/* At a 1x1 decomposition the source and destination pencils have the same
+ * shape and layout, so each transpose is a device copy (nothing when
+ * in == out).  is_complex selects the complex variants (twice the bytes). */
+int x3d_transpose_x_to_y(x3d_ctx ctx, const void *in, void *out, int is_complex);
+int x3d_transpose_y_to_z(x3d_ctx ctx, const void *in, void *out, int is_complex);
+int x3d_transpose_z_to_y(x3d_ctx ctx, const void *in, void *out, int is_complex);
+int x3d_transpose_y_to_x(x3d_ctx ctx, const void *in, void *out, int is_complex);
+
+/* ---- spectral Poisson: decomp_2d_poisson (src/poisson.f90:57-65) -------- */
+
+/* poisson_000 (src/poisson.f90:276-419), in place on the FP64 pressure-grid
+ * field rhs (nx*ny*nz doubles). */
+int x3d_poisson(x3d_ctx ctx, double *rhs);
+
+/* ---- projection stage: module navier (src/navier.f90) ------------------- */
+
+/* divergence (:98-236): pp3 = div(u) on the pressure grid (FP64 output).
+ * nlock is accepted for signature parity; the test-mode print is replaced
+ * by x3d_div_stats. */
+int x3d_divergence(x3d_ctx ctx, double *pp3, const void *ux1, const void *uy1, const void *uz1,
+                   int nlock);
+/* gradp (:249-359): px1, py1, pz1 = grad(pp3) on the velocity grid */
+int x3d_gradp(x3d_ctx ctx, void *px1, void *py1, void *pz1, const double *pp3);
+/* cor_vel (:64-91): u -= grad p */
+int x3d_cor_vel(x3d_ctx ctx, void *ux, void *uy, void *uz, const void *px, const void *py,
+                const void *pz);
+/* solve_poisson (:21-56): divergence, poisson, gradp */
+int x3d_solve_poisson(x3d_ctx ctx, double *pp3, void *px1, void *py1, void *pz1, const void *ux1,
+                      const void *uy1, const void *uz1);
+/* The DIV U max/mean figures printed by divergence in test mode
+ * (src/navier.f90:213-231), computed on the device: out[0] = max|pp3|,
+ * out[1] = mean|pp3|.  Synchronous. */
+int x3d_div_stats(x3d_ctx ctx, const double *pp3, double *out);
+
+/* ---- convective RHS and time integration -------------------------------- */
+
+/* momentum_rhs_eq (src/transeq.f90:44-355): du_c = sum_d d(u_d u_c)/dx_d
+ * + u_d du_c/dx_d, with the reference's operator pairs and sign. */
+int x3d_momentum_rhs_eq(x3d_ctx ctx, void *dux1, void *duy1, void *duz1, const void *ux1,
+                        const void *uy1, const void *uz1);
+/* int_time, Euler branch (src/time_integrators.f90:20-106): u = gdt*du + u */
+int x3d_int_time(x3d_ctx ctx, void *ux1, void *uy1, void *uz1, const void *dux1, const void *duy1,
+                 const void *duz1, double gdt);
+/* One timestep of the reference loop body (src/xcompact3d.f90:80-95):
+ * calculate_transeq_rhs, int_time, solve_poisson, cor_vel.  dux..duz,
+ * pp3 and px..pz are outputs (the reference's dux1/duy1/duz1, pp3, px1..pz1). */
+int x3d_euler_step(x3d_ctx ctx, void *ux1, void *uy1, void *uz1, void *dux1, void *duy1,
+                   void *duz1, double *pp3, void *px1, void *py1, void *pz1, double dt);
+
+/* ---- initial field and analytic checks: module mom (src/mom.f90) -------- */
+
+/* vel (:26-57) on the device */
+int x3d_vel(x3d_ctx ctx, void *u, void *v, void *w);
+/* test_du / test_dv / test_dw (:59-243): RMS error of du/dx (which=0),
+ * dv/dy (1) or dw/dz (2) against the analytic derivative of vel's field.
+ * Synchronous; result in *rms. */
+int x3d_test_rms(x3d_ctx ctx, int which, const void *du, double *rms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* X3D_B200_H */

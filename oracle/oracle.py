@@ -1,0 +1,188 @@
+"""CPU FP64 oracle for x3div's Euler-timestep hot path (test infrastructure).
+
+Only tests/, ``__graft_entry__.smoke()`` and the CPU-baseline legs of
+bench.py may import this module; the product path never does.  It wraps the
+C restatement in ``oracle/x3d_oracle.c`` (see that file's header for how the
+restatement is pinned to the reference) and adds the 3-D FFTs of the spectral
+Poisson solve with numpy's pocketfft, standing in for the external
+2decomp&FFT library that the reference calls at src/poisson.f90:318,325,412.
+
+Fields are numpy float64 arrays of shape (nx, ny, nz) in Fortran order, so
+``u[i, j, k]`` is the reference's ``u(i+1, j+1, k+1)`` and x is contiguous.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+
+DER, DER2, DERVP, DERPV, INTVP, INTPV = range(6)
+X, Y, Z = range(3)
+KIND_NAMES = {"der": DER, "der2": DER2, "dervp": DERVP, "derpv": DERPV,
+              "intvp": INTVP, "intpv": INTPV}
+
+_lib = None
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+def build() -> str:
+    """Compile the C restatement (make) and return the .so path."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        i, d, p = ctypes.c_int, ctypes.c_double, _dp
+        L.orc_build_lhs.argtypes = [i, i, d, p, p, p, p, p]
+        L.orc_apply.argtypes = [i, i, p, p, i, i, i, d]
+        L.orc_thomas_periodic.argtypes = [i, p, i, i, i, p, p, p, p, d]
+        L.orc_thomas_plain.argtypes = [i, p, i, i, i, p, p, p]
+        L.orc_poisson_spectral.argtypes = [p, i, i, i, d, d, d]
+        L.orc_poisson_tables.argtypes = [i, i, i, d, d, d, p, p, p, p, p, p]
+        L.orc_divergence.argtypes = [p, p, p, p, i, i, i, d, d, d]
+        L.orc_gradp.argtypes = [p, p, p, p, i, i, i, d, d, d]
+        L.orc_cor_vel.argtypes = [p, p, p, p, p, p, ctypes.c_long]
+        L.orc_intt.argtypes = [p, p, d, ctypes.c_long]
+        L.orc_momentum_rhs.argtypes = [p, p, p, p, p, p, i, i, i, d, d, d]
+        L.orc_vel.argtypes = [p, p, p, i, i, i, d, d, d]
+        L.orc_test_rms.argtypes = [i, p, i, i, i, d, d, d]
+        L.orc_test_rms.restype = d
+        L.orc_rhs_scalars.argtypes = [i, d, p]
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.float64 and (a.flags.f_contiguous or a.ndim == 1)
+    return a.ctypes.data_as(_dp)
+
+
+def field(shape) -> np.ndarray:
+    return np.zeros(shape, dtype=np.float64, order="F")
+
+
+def _kind(k):
+    return KIND_NAMES[k] if isinstance(k, str) else int(k)
+
+
+def lhs(kind, n: int, d: float) -> dict:
+    """Periodic operator of one kind on an n-point line with spacing d:
+    the x3doperator1d contents (f, s, w, periodic, alfa) plus the explicit
+    RHS scalars (a, b, c, d) that the reference keeps in module globals."""
+    f, s, w, per = (np.zeros(n) for _ in range(4))
+    c5 = np.zeros(5)
+    rc = lib().orc_build_lhs(_kind(kind), n, float(d), _p(f), _p(s), _p(w), _p(per), _p(c5))
+    if rc != 0:
+        raise ValueError(f"oracle: bad operator request kind={kind} n={n}")
+    return dict(f=f, s=s, w=w, periodic=per, alfa=c5[0], a=c5[1], b=c5[2], c=c5[3], d=c5[4])
+
+
+def apply(kind, direction: int, u: np.ndarray, d: float) -> np.ndarray:
+    """One operator application (RHS stencil + periodic Thomas)."""
+    u = np.asfortranarray(u, dtype=np.float64)
+    out = field(u.shape)
+    nx, ny, nz = u.shape
+    rc = lib().orc_apply(_kind(kind), int(direction), _p(out), _p(u), nx, ny, nz, float(d))
+    if rc != 0:
+        raise ValueError("oracle: bad apply request")
+    return out
+
+
+def thomas_periodic(direction: int, t: np.ndarray, op: dict) -> np.ndarray:
+    t = np.array(t, dtype=np.float64, order="F", copy=True)
+    nx, ny, nz = t.shape
+    lib().orc_thomas_periodic(int(direction), _p(t), nx, ny, nz, _p(op["f"]), _p(op["s"]),
+                              _p(op["w"]), _p(op["periodic"]), float(op["alfa"]))
+    return t
+
+
+def poisson_tables(nx, ny, nz, xlx, yly, zlz):
+    arrs = [np.zeros(n) for n in (nx, nx, ny, ny, nz, nz)]
+    lib().orc_poisson_tables(nx, ny, nz, xlx, yly, zlz, *[_p(a) for a in arrs])
+    return dict(k2x=arrs[0], tx=arrs[1], k2y=arrs[2], ty=arrs[3], k2z=arrs[4], tz=arrs[5])
+
+
+def poisson(rhs: np.ndarray, xlx: float, yly: float, zlz: float) -> np.ndarray:
+    """poisson_000 (src/poisson.f90:276-419).  The transforms are the
+    unnormalised r2c (sign -1) along z then c2c along y and x, and the
+    unnormalised c2r inverse, i.e. 2decomp's PHYSICAL_IN_Z convention."""
+    rhs = np.asfortranarray(rhs, dtype=np.float64)
+    nx, ny, nz = rhs.shape
+    a = rhs.transpose(2, 1, 0)  # C-order (nz, ny, nx) view of the F-order field
+    cw = np.fft.rfftn(a, axes=(2, 1, 0))  # real transform along axis 0 (z) -> (nz/2+1, ny, nx)
+    cw = np.ascontiguousarray(cw, dtype=np.complex128)
+    lib().orc_poisson_spectral(cw.ctypes.data_as(_dp), nx, ny, nz, xlx, yly, zlz)
+    out = np.fft.irfftn(cw, s=(nx, ny, nz), axes=(2, 1, 0), norm="forward")
+    return np.asfortranarray(out.transpose(2, 1, 0))
+
+
+def divergence(ux, uy, uz, dx, dy, dz):
+    nx, ny, nz = ux.shape
+    pp3 = field(ux.shape)
+    rc = lib().orc_divergence(_p(pp3), _p(ux), _p(uy), _p(uz), nx, ny, nz, dx, dy, dz)
+    assert rc == 0
+    return pp3
+
+
+def gradp(pp3, dx, dy, dz):
+    nx, ny, nz = pp3.shape
+    px, py, pz = field(pp3.shape), field(pp3.shape), field(pp3.shape)
+    rc = lib().orc_gradp(_p(px), _p(py), _p(pz), _p(pp3), nx, ny, nz, dx, dy, dz)
+    assert rc == 0
+    return px, py, pz
+
+
+def momentum_rhs(ux, uy, uz, dx, dy, dz):
+    nx, ny, nz = ux.shape
+    du = [field(ux.shape) for _ in range(3)]
+    rc = lib().orc_momentum_rhs(*[_p(a) for a in du], _p(ux), _p(uy), _p(uz), nx, ny, nz, dx, dy, dz)
+    assert rc == 0
+    return tuple(du)
+
+
+def intt(var, dvar, gdt):
+    lib().orc_intt(_p(var), _p(dvar), float(gdt), var.size)
+
+
+def cor_vel(ux, uy, uz, px, py, pz):
+    lib().orc_cor_vel(_p(ux), _p(uy), _p(uz), _p(px), _p(py), _p(pz), ux.size)
+
+
+def vel(nx, ny, nz, xlx=1.0, yly=1.0, zlz=1.0):
+    """Reference initial field (src/mom.f90:46-53)."""
+    u, v, w = field((nx, ny, nz)), field((nx, ny, nz)), field((nx, ny, nz))
+    lib().orc_vel(_p(u), _p(v), _p(w), nx, ny, nz, xlx, yly, zlz)
+    return u, v, w
+
+
+def test_rms(which: int, du, xlx=1.0, yly=1.0, zlz=1.0) -> float:
+    nx, ny, nz = du.shape
+    return lib().orc_test_rms(int(which), _p(du), nx, ny, nz, xlx, yly, zlz)
+
+
+def euler_step(ux, uy, uz, dt, lengths=(1.0, 1.0, 1.0)):
+    """One x3div timestep (xcompact3d.f90:80-95) at a 1x1 decomposition:
+    calculate_transeq_rhs, int_time, solve_poisson, cor_vel.  Updates
+    ux, uy, uz in place and returns (du, pp3 divergence before projection,
+    pressure after the solve)."""
+    nx, ny, nz = ux.shape
+    xlx, yly, zlz = lengths
+    dx, dy, dz = xlx / nx, yly / ny, zlz / nz
+    du = momentum_rhs(ux, uy, uz, dx, dy, dz)
+    for v, dv in zip((ux, uy, uz), du):
+        intt(v, dv, dt)
+    div = divergence(ux, uy, uz, dx, dy, dz)
+    pp3 = poisson(div, xlx, yly, zlz)
+    px, py, pz = gradp(pp3, dx, dy, dz)
+    cor_vel(ux, uy, uz, px, py, pz)
+    return du, div, pp3

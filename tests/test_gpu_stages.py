@@ -1,0 +1,172 @@
+"""Parity of the stage compositions (navier.f90, transeq.f90, poisson.f90,
+time_integrators.f90, mom.f90) against the CPU oracle, plus the
+size-independent properties checked at 512^3."""
+import numpy as np
+import pytest
+
+from conftest import rel_err, seeded_field
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [(16, 16, 16), (24, 20, 12), (32, 32, 32)]
+LEN = (2 * np.pi, 1.5, 3.0)
+
+
+def fields(shape, seeds=(1, 2, 3)):
+    return [seeded_field(shape, s, lengths=LEN, noise=1e-2) for s in seeds]
+
+
+def ctx_for(shape, prec="f64"):
+    from x3div_b200 import Context
+    return Context(*shape, lengths=LEN, precision=prec)
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+def test_poisson(oracle, torch_cuda, shape):
+    from x3div_b200 import to_device, to_host
+    ctx = ctx_for(shape)
+    rhs = seeded_field(shape, 21, kind="rand", lengths=LEN, noise=0)
+    d = to_device(rhs)
+    ctx.poisson(d)
+    ctx.sync()
+    assert rel_err(to_host(d), oracle.poisson(rhs, *LEN)) < 1e-12
+    ctx.close()
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_divergence_gradp_momentum(oracle, torch_cuda, shape, prec):
+    torch = torch_cuda
+    from x3div_b200 import to_device, to_host
+    ctx = ctx_for(shape, prec)
+    dt = torch.float64 if prec == "f64" else torch.float32
+    tol = 1e-12 if prec == "f64" else 1e-5
+    u, v, w = fields(shape)
+    ud, vd, wd = (to_device(a, dt) for a in (u, v, w))
+    uh, vh, wh = (to_host(a).astype(np.float64) for a in (ud, vd, wd))
+    dx, dy, dz = ctx.dx, ctx.dy, ctx.dz
+    # divergence (pp3 is FP64 in both precisions)
+    pp3 = torch.empty(shape[::-1], dtype=torch.float64, device="cuda")
+    ctx.divergence(pp3, ud, vd, wd)
+    ctx.sync()
+    ref_div = oracle.divergence(uh, vh, wh, dx, dy, dz)
+    assert rel_err(to_host(pp3), ref_div) < tol
+    # gradp from an FP64 pressure
+    px, py, pz = (torch.empty_like(ud) for _ in range(3))
+    p_h = seeded_field(shape, 30, kind="rand", lengths=LEN, noise=0)
+    p_d = to_device(p_h)
+    ctx.gradp(px, py, pz, p_d)
+    ctx.sync()
+    rp = oracle.gradp(p_h, dx, dy, dz)
+    for got, ref in zip((px, py, pz), rp):
+        assert rel_err(to_host(got), ref) < tol
+    # momentum_rhs_eq
+    du = [torch.empty_like(ud) for _ in range(3)]
+    ctx.momentum_rhs_eq(*du, ud, vd, wd)
+    ctx.sync()
+    ref_du = oracle.momentum_rhs(uh, vh, wh, dx, dy, dz)
+    for got, ref in zip(du, ref_du):
+        assert rel_err(to_host(got), ref) < tol * 10
+    ctx.close()
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_euler_steps_match_oracle(oracle, torch_cuda, prec):
+    """Ten x3div timesteps (dt = 1e-3) against the oracle; the divergence after
+    each projection is round-off in FP64."""
+    torch = torch_cuda
+    from x3div_b200 import to_device, to_host
+    shape = (32, 24, 16)
+    ctx = ctx_for(shape, prec)
+    dt_ = torch.float64 if prec == "f64" else torch.float32
+    u, v, w = fields(shape, (5, 6, 7))
+    U = [to_device(a, dt_) for a in (u, v, w)]
+    ref = [to_host(a).astype(np.float64) for a in U]
+    du = [torch.empty_like(U[0]) for _ in range(3)]
+    pg = [torch.empty_like(U[0]) for _ in range(3)]
+    pp3 = torch.empty(shape[::-1], dtype=torch.float64, device="cuda")
+    for _ in range(10):
+        ctx.euler_step(*U, *du, pp3, *pg, 1e-3)
+        oracle.euler_step(*ref, 1e-3, lengths=LEN)
+    ctx.sync()
+    tol = 1e-11 if prec == "f64" else 2e-5
+    for got, r in zip(U, ref):
+        assert rel_err(to_host(got), r) < tol
+    if prec == "f64":
+        div = torch.empty_like(pp3)
+        ctx.divergence(div, *U)
+        mx, mean = ctx.div_stats(div)
+        assert mx < 1e-10
+    ctx.close()
+
+
+def test_reference_test_mode(oracle, torch_cuda):
+    """test_du/dv/dw on the reference vel field (src/mom.f90) match the oracle's RMS."""
+    torch = torch_cuda
+    from x3div_b200 import Context, to_host
+    n = 64
+    ctx = Context(n, n, n)  # reference box: xlx = yly = zlz = 1
+    U = [torch.empty(n, n, n, dtype=torch.float64, device="cuda") for _ in range(3)]
+    ctx.vel(*U)
+    ctx.sync()
+    ref = oracle.vel(n, n, n)
+    for got, r in zip(U, ref):
+        assert rel_err(to_host(got), r) < 1e-14
+    names = ("derx", "dery", "derz")
+    for which in range(3):
+        t = torch.empty_like(U[0])
+        fn = getattr(ctx, names[which])
+        if which == 1:
+            fn(t, U[which], ctx.op("dery"), None, n, n, n)
+        else:
+            fn(t, U[which], ctx.op(names[which]), n, n, n)
+        rms = ctx.test_rms(which, t)
+        ref_rms = oracle.test_rms(which, oracle.apply("der", which, ref[which], 1.0 / n))
+        assert abs(rms - ref_rms) < 1e-6 * ref_rms
+    ctx.close()
+
+
+def test_transposes_are_layout_copies(torch_cuda):
+    torch = torch_cuda
+    from x3div_b200 import Context
+    ctx = Context(16, 12, 8, precision="f32")
+    a = torch.randn(8, 12, 16, device="cuda")
+    b = torch.empty_like(a)
+    for name in ("x_to_y", "y_to_z", "z_to_y", "y_to_x"):
+        b.zero_()
+        getattr(ctx, "transpose_" + name)(a, b)
+        ctx.sync()
+        assert torch.equal(a, b)
+    c = torch.randn(8, 12, 32, device="cuda")  # complex: twice the bytes
+    d = torch.empty_like(c)
+    ctx.transpose_x_to_y(c, d, is_complex=True)
+    ctx.sync()
+    assert torch.equal(c, d)
+    ctx.close()
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_512_selected_ops(oracle, torch_cuda, prec):
+    """Full-size (512^3) parity for one operator per kernel family and
+    direction, against the oracle on the same input."""
+    torch = torch_cuda
+    from x3div_b200 import Context, to_device, to_host
+    n = 512
+    ctx = Context(n, n, n, lengths=(2 * np.pi,) * 3, precision=prec)
+    dt = torch.float64 if prec == "f64" else torch.float32
+    u_h = seeded_field((n, n, n), 512, noise=1e-3)
+    u = to_device(u_h, dt)
+    del u_h
+    used = to_host(u).astype(np.float64)
+    tol = 1e-12 if prec == "f64" else 1e-5
+    t = torch.empty_like(u)
+    cases = [("derx", "derx", "der", 0), ("interyvp", "intyvp", "intvp", 1), ("derzz", "derzz", "der2", 2)]
+    for routine, opn, kind, direction in cases:
+        if routine == "interyvp":
+            ctx.interyvp(t, u, ctx.op(opn), n, n, n, n)
+        else:
+            getattr(ctx, routine)(t, u, ctx.op(opn), n, n, n)
+        ctx.sync()
+        ref = oracle.apply(kind, direction, used, 2 * np.pi / n)
+        assert rel_err(to_host(t), ref) < tol, (routine, prec)
+    ctx.close()

@@ -1,0 +1,179 @@
+"""Pins of the CPU oracle against the reference's own known answers (no GPU).
+
+The reference ships no golden vectors and cannot be compiled here (Fortran +
+MPI + 2decomp&FFT; no gfortran).  Its own known-answer formulas are:
+  * the modified wavenumber of the staggered derivative and the transfer
+    function of the interpolation, src/poisson.f90:522-533 and :631-650;
+  * the analytic derivatives of the vel field, src/mom.f90:88-113 etc.
+Every periodic compact operator is circulant, so a Fourier mode must come out
+scaled by exactly those factors (to round-off).  The first derivative is
+pinned by its own transfer function (Lele's 6th-order scheme the reference
+implements), and the second derivative -- absent from the reference -- by
+its analytic transfer function only.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_err
+
+X, Y, Z = 0, 1, 2
+KINDS = ["der", "der2", "dervp", "derpv", "intvp", "intpv"]
+
+
+def transfer(kind, w, c):
+    """Fourier factor of each operator for a mode of phase w = k*d, written
+    with the reference's scalars (c = oracle.lhs output)."""
+    al, a, b, cc, dd = c["alfa"], c["a"], c["b"], c["c"], c["d"]
+    den = 1.0 + 2.0 * al * np.cos(w)
+    if kind == "der":
+        return (2 * a * np.sin(w) + 2 * b * np.sin(2 * w)) / den
+    if kind == "der2":
+        return (2 * a * (np.cos(w) - 1) + 2 * b * (np.cos(2 * w) - 1)) / den
+    if kind in ("dervp", "derpv"):
+        # waves(): wp = acix6*2*dx*sin(w/2) + bcix6*2*dx*sin(1.5w), / (1 + 2 alcaix6 cos w); xkx = wp/dx
+        return (2 * a * np.sin(w / 2) + 2 * b * np.sin(1.5 * w)) / den
+    # waves() :640-648: (2 aicix6 cos(w/2) + 2 (bicix6 cos 1.5w + cicix6 cos 2.5w + dicix6 cos 3.5w)) / (1 + 2 ailcaix6 cos w)
+    return (2 * a * np.cos(w / 2) + 2 * (b * np.cos(1.5 * w) + cc * np.cos(2.5 * w) + dd * np.cos(3.5 * w))) / den
+
+
+def mode_case(kind, n, m, L):
+    """Input and expected output along one line for mode m."""
+    d = L / n
+    k = 2 * np.pi * m / L
+    i = np.arange(n)
+    xv = i * d            # velocity grid
+    xp = (i + 0.5) * d    # pressure grid (staggered by half a cell)
+    src_x = xp if kind in ("derpv", "intpv") else xv
+    dst_x = xp if kind in ("dervp", "intvp") else xv
+    u = np.sin(k * src_x)
+    return u, dst_x, k * d, k
+
+
+@pytest.mark.parametrize("kind", KINDS)
+@pytest.mark.parametrize("direction", [X, Y, Z])
+@pytest.mark.parametrize("n", [8, 9, 16, 17, 64])
+def test_fourier_modes(oracle, kind, direction, n):
+    L = 2 * np.pi if n != 17 else 1.0
+    c = oracle.lhs(kind, n, L / n)
+    modes = sorted({1, 2, max(1, n // 4), max(1, n // 2 - 1)})
+    other = [5, 4]
+    for m in modes:
+        u1, dst_x, w, k = mode_case(kind, n, m, L)
+        T = transfer(kind, w, c)
+        if kind in ("der", "dervp", "derpv"):
+            expect1 = T * np.cos(k * dst_x)
+        else:
+            expect1 = T * np.sin(k * dst_x)
+        # embed the line in a 3-D field, varying along the other axes too
+        shape = [other[0], other[1]]
+        shape.insert(direction, n)
+        g = 1.0 + 0.25 * np.arange(other[0] * other[1]).reshape(other)
+        u = np.moveaxis(u1[:, None, None] * g[None], 0, direction)
+        exp = np.moveaxis(expect1[:, None, None] * g[None], 0, direction)
+        out = oracle.apply(kind, direction, np.asfortranarray(u), L / n)
+        assert rel_err(out, exp) < 1e-12, (kind, direction, n, m)
+
+
+def circulant(n, taps):
+    A = np.zeros((n, n))
+    for off, v in taps.items():
+        for i in range(n):
+            A[i, (i + off) % n] += v
+    return A
+
+
+STENCIL_TAPS = {
+    "der": lambda c: {1: c["a"], -1: -c["a"], 2: c["b"], -2: -c["b"]},
+    "der2": lambda c: {1: c["a"], 0: -2 * c["a"] - 2 * c["b"], -1: c["a"], 2: c["b"], -2: c["b"]},
+    "dervp": lambda c: {1: c["a"], 0: -c["a"], 2: c["b"], -1: -c["b"]},
+    "derpv": lambda c: {0: c["a"], -1: -c["a"], 1: c["b"], -2: -c["b"]},
+    "intvp": lambda c: {1: c["a"], 0: c["a"], 2: c["b"], -1: c["b"], 3: c["c"], -2: c["c"], 4: c["d"], -3: c["d"]},
+    "intpv": lambda c: {0: c["a"], -1: c["a"], 1: c["b"], -2: c["b"], 2: c["c"], -3: c["c"], 3: c["d"], -4: c["d"]},
+}
+
+
+@pytest.mark.parametrize("kind", KINDS)
+@pytest.mark.parametrize("n", [8, 13, 32])
+def test_dense_cyclic_solve(oracle, kind, n):
+    """The Thomas + Sherman-Morrison pipeline (prepare, thomas1d periodic
+    vector, ?thomas_0) solves exactly the cyclic tridiagonal system with unit
+    diagonal and alfa off-diagonals and corners."""
+    d = 0.37
+    c = oracle.lhs(kind, n, d)
+    A = circulant(n, {0: 1.0, 1: c["alfa"], -1: c["alfa"]})
+    S = circulant(n, STENCIL_TAPS[kind](c))
+    rng = np.random.default_rng(7 + n)
+    u = np.asfortranarray(rng.standard_normal((n, 3, 2)))
+    out = oracle.apply(kind, X, u, d)
+    ref = np.linalg.solve(A, S @ u.reshape(n, -1)).reshape(u.shape)
+    assert rel_err(out, ref) < 1e-12
+
+
+@pytest.mark.parametrize("which", [0, 1, 2])
+def test_reference_test_mode_rms(oracle, which):
+    """test_du/dv/dw (src/mom.f90) on the reference vel field: the RMS error
+    printed by the reference equals |k' - k| * rms(ccc) exactly."""
+    n = 32
+    u, v, w = oracle.vel(n, n, n)
+    d = 1.0 / n
+    field = (u, v, w)[which]
+    out = oracle.apply("der", which, field, d)
+    rms = oracle.test_rms(which, out)
+    c = oracle.lhs("der", n, d)
+    k = 2 * np.pi
+    kp = transfer("der", k * d, c)
+    amp = 2.0 if which == 2 else 1.0
+    predicted = amp * abs(kp - k) / np.sqrt(8.0)
+    assert rms > 0
+    assert abs(rms - predicted) / predicted < 1e-6
+
+
+def test_poisson_projection_removes_divergence(oracle):
+    """divergence -> poisson_000 -> gradp -> cor_vel leaves a field whose
+    staggered divergence is round-off (the modified wavenumbers of waves()
+    match the staggered operators exactly)."""
+    from conftest import seeded_field
+    n = (16, 12, 20)
+    L = (2 * np.pi, 1.5, 3.0)
+    u = seeded_field(n, 1, lengths=L, noise=1e-2)
+    v = seeded_field(n, 2, kind="rand", lengths=L, noise=0)
+    w = seeded_field(n, 3, kind="rand", lengths=L, noise=0)
+    dx, dy, dz = (l / m for l, m in zip(L, n))
+    div0 = oracle.divergence(u, v, w, dx, dy, dz)
+    p = oracle.poisson(div0, *L)
+    px, py, pz = oracle.gradp(p, dx, dy, dz)
+    oracle.cor_vel(u, v, w, px, py, pz)
+    div1 = oracle.divergence(u, v, w, dx, dy, dz)
+    assert np.abs(div1).max() < 1e-12 * np.abs(div0).max()
+
+
+def test_poisson_against_dense_spectral(oracle):
+    """poisson_000's per-mode algebra (phase shifts that cancel, division by
+    -K) equals -fft(rhs)/K with K from the 1-D tables."""
+    from conftest import seeded_field
+    nx, ny, nz = 12, 10, 8
+    L = (1.0, 2.0, 3.0)
+    rhs = seeded_field((nx, ny, nz), 5, kind="rand", lengths=L, noise=0)
+    out = oracle.poisson(rhs, *L)
+    t = oracle.poisson_tables(nx, ny, nz, *L)
+    K = (t["k2x"][:, None, None] * (t["ty"][None, :, None] * t["tz"][None, None, :]) ** 2
+         + t["k2y"][None, :, None] * (t["tx"][:, None, None] * t["tz"][None, None, :]) ** 2
+         + t["k2z"][None, None, :] * (t["tx"][:, None, None] * t["ty"][None, :, None]) ** 2)
+    R = np.fft.fftn(rhs)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        P = np.where(K < 1e-16, 0.0, -R / K)
+    ref = np.real(np.fft.ifftn(P))
+    assert rel_err(out, ref) < 1e-12
+
+
+def test_euler_step_runs_and_projects(oracle):
+    from conftest import seeded_field
+    n = (16, 16, 16)
+    u = seeded_field(n, 11)
+    v = seeded_field(n, 12)
+    w = seeded_field(n, 13)
+    du, div_before, p = oracle.euler_step(u, v, w, 1e-3, lengths=(2 * np.pi,) * 3)
+    d = 2 * np.pi / 16
+    div_after = oracle.divergence(u, v, w, d, d, d)
+    assert np.isfinite(u).all()
+    assert np.abs(div_after).max() < 1e-11 * max(np.abs(div_before).max(), 1e-30)

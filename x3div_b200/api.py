@@ -1,0 +1,290 @@
+"""Python mirror of the reference's operator interface over the C ABI.
+
+Method names, argument order and meaning follow the reference routines
+(``derx(tx, ux, x3dop, nx, ny, nz)`` from src/x3d_derive.f90:111,
+``derxvp(tx, ux, x3dop, nx, nxm, ny, nz)`` from src/x3d_staggered.f90:23,
+``xthomas(tt, ff, fs, fw, perio, alfa, nx, ny, nz)`` from src/thomas.f90:34,
+``poisson(rhs)`` from src/poisson.f90:276, and so on).  A non-zero status
+from the library raises :class:`X3DError`, where the reference would call
+``decomp_2d_abort``.
+
+Field arguments are device tensors (torch, any layout-compatible view whose
+memory is the Fortran-ordered (nx, ny, nz) array -- e.g. a contiguous
+``(nz, ny, nx)`` tensor) or host numpy arrays in Fortran order; the library
+stages host arrays itself.  Element type is the context precision
+(float64 for "f64", float32 for "f32"); pressure fields are float64.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _capi
+from ._capi import KIND, OP_NAMES, X3D_F32, X3D_F64
+
+
+class X3DError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"x3d status {code}: {msg}")
+        self.code = code
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return a
+    if isinstance(a, np.ndarray):
+        if not (a.flags.f_contiguous or a.flags.c_contiguous):
+            raise ValueError("host arrays must be contiguous")
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        if not a.is_contiguous():
+            raise ValueError("device tensors must be contiguous")
+        return a.data_ptr()
+    raise TypeError(f"unsupported field argument {type(a)!r}")
+
+
+class Operator:
+    """Handle on an x3doperator1d living in the library."""
+
+    def __init__(self, ctx: "Context", handle: int, name: str, owned: bool):
+        self.ctx, self.handle, self.name, self._owned = ctx, handle, name, owned
+
+    def info(self) -> dict:
+        L = _capi.lib()
+        meta = (ctypes.c_int * 4)()
+        scal = (ctypes.c_double * 5)()
+        L.x3d_op_info(self.handle, meta, scal, None, None, None, None)
+        n = meta[0]
+        arrs = [np.zeros(n) for _ in range(4)]
+        L.x3d_op_info(self.handle, meta, scal, *[a.ctypes.data for a in arrs])
+        return dict(n=n, kind=meta[1], dir=meta[2], npaire=meta[3], alfa=scal[0], a=scal[1],
+                    b=scal[2], c=scal[3], d=scal[4], f=arrs[0], s=arrs[1], w=arrs[2],
+                    periodic=arrs[3])
+
+    def close(self):
+        if self._owned and self.handle:
+            _capi.lib().x3d_op_destroy(self.ctx.handle, self.handle)
+            self.handle = None
+
+
+class Context:
+    """A fully periodic nx*ny*nz box at a 1x1 decomposition (x3d_ctx)."""
+
+    def __init__(self, nx, ny, nz, lengths=(1.0, 1.0, 1.0), precision="f64", device=0,
+                 stream=None):
+        self.L = _capi.lib()
+        self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
+        self.lengths = tuple(float(v) for v in lengths)
+        self.precision = precision
+        self.fp32 = precision == "f32"
+        h = ctypes.c_void_p()
+        rc = self.L.x3d_ctx_create(ctypes.byref(h), self.nx, self.ny, self.nz, *self.lengths,
+                                   X3D_F32 if self.fp32 else X3D_F64, int(device))
+        if rc != 0:
+            raise X3DError(rc, "x3d_ctx_create failed")
+        self.handle = h.value
+        self.dx, self.dy, self.dz = (l / n for l, n in zip(self.lengths, (nx, ny, nz)))
+        if stream is not None:
+            self.set_stream(stream)
+        self._ops = {}
+
+    # -- plumbing ---------------------------------------------------------
+    @property
+    def np_dtype(self):
+        return np.float32 if self.fp32 else np.float64
+
+    def _check(self, rc):
+        if rc != 0:
+            msg = self.L.x3d_ctx_last_error(self.handle) or b""
+            raise X3DError(rc, msg.decode(errors="replace"))
+
+    def set_stream(self, stream):
+        """Run on a caller stream: a torch.cuda.Stream or a raw cudaStream_t."""
+        raw = getattr(stream, "cuda_stream", stream)
+        self._check(self.L.x3d_ctx_set_stream(self.handle, raw))
+
+    def sync(self):
+        self._check(self.L.x3d_ctx_sync(self.handle))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            for op in self._ops.values():
+                if op._owned:
+                    op.close()
+            self.L.x3d_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- operators --------------------------------------------------------
+    def op(self, name: str) -> Operator:
+        """One of the x3d_operator_1d instances (x3d_op_derx ... x3d_op_intzpv,
+        plus derxx/deryy/derzz)."""
+        name = name.removeprefix("x3d_op_")
+        if name not in self._ops:
+            h = ctypes.c_void_p()
+            self._check(self.L.x3d_op_builtin(self.handle, OP_NAMES.index(name), ctypes.byref(h)))
+            self._ops[name] = Operator(self, h.value, name, owned=False)
+        return self._ops[name]
+
+    def op_create(self, kind, direction, n, npaire, alfa, f, s, w, periodic, rhs) -> Operator:
+        h = ctypes.c_void_p()
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (f, s, w, periodic, rhs)]
+        kind = KIND[kind] if isinstance(kind, str) else int(kind)
+        self._check(self.L.x3d_op_create(self.handle, kind, int(direction), int(n), int(npaire),
+                                         float(alfa), *[a.ctypes.data for a in arrs],
+                                         ctypes.byref(h)))
+        return Operator(self, h.value, f"user-{kind}-{direction}", owned=True)
+
+    # -- x3d_derive -------------------------------------------------------
+    def derx(self, tx, ux, op, nx, ny, nz):
+        self._check(self.L.x3d_derx(self.handle, _ptr(tx), _ptr(ux), op.handle, nx, ny, nz))
+
+    def dery(self, ty, uy, op, ppy, nx, ny, nz):
+        self._check(self.L.x3d_dery(self.handle, _ptr(ty), _ptr(uy), op.handle, _ptr(ppy), nx, ny, nz))
+
+    def derz(self, tz, uz, op, nx, ny, nz):
+        self._check(self.L.x3d_derz(self.handle, _ptr(tz), _ptr(uz), op.handle, nx, ny, nz))
+
+    def derxx(self, tx, ux, op, nx, ny, nz):
+        self._check(self.L.x3d_derxx(self.handle, _ptr(tx), _ptr(ux), op.handle, nx, ny, nz))
+
+    def deryy(self, ty, uy, op, nx, ny, nz):
+        self._check(self.L.x3d_deryy(self.handle, _ptr(ty), _ptr(uy), op.handle, nx, ny, nz))
+
+    def derzz(self, tz, uz, op, nx, ny, nz):
+        self._check(self.L.x3d_derzz(self.handle, _ptr(tz), _ptr(uz), op.handle, nx, ny, nz))
+
+    # -- x3d_staggered ----------------------------------------------------
+    def derxvp(self, tx, ux, op, nx, nxm, ny, nz):
+        self._check(self.L.x3d_derxvp(self.handle, _ptr(tx), _ptr(ux), op.handle, nx, nxm, ny, nz))
+
+    def interxvp(self, tx, ux, op, nx, nxm, ny, nz):
+        self._check(self.L.x3d_interxvp(self.handle, _ptr(tx), _ptr(ux), op.handle, nx, nxm, ny, nz))
+
+    def derxpv(self, tx, ux, op, nxm, nx, ny, nz):
+        self._check(self.L.x3d_derxpv(self.handle, _ptr(tx), _ptr(ux), op.handle, nxm, nx, ny, nz))
+
+    def interxpv(self, tx, ux, op, nxm, nx, ny, nz):
+        self._check(self.L.x3d_interxpv(self.handle, _ptr(tx), _ptr(ux), op.handle, nxm, nx, ny, nz))
+
+    def interyvp(self, ty, uy, op, nx, ny, nym, nz):
+        self._check(self.L.x3d_interyvp(self.handle, _ptr(ty), _ptr(uy), op.handle, nx, ny, nym, nz))
+
+    def deryvp(self, ty, uy, op, ppyi, nx, ny, nym, nz):
+        self._check(self.L.x3d_deryvp(self.handle, _ptr(ty), _ptr(uy), op.handle, _ptr(ppyi), nx, ny, nym, nz))
+
+    def interypv(self, ty, uy, op, nx, nym, ny, nz):
+        self._check(self.L.x3d_interypv(self.handle, _ptr(ty), _ptr(uy), op.handle, nx, nym, ny, nz))
+
+    def derypv(self, ty, uy, op, ppy, nx, nym, ny, nz):
+        self._check(self.L.x3d_derypv(self.handle, _ptr(ty), _ptr(uy), op.handle, _ptr(ppy), nx, nym, ny, nz))
+
+    def derzvp(self, tz, uz, op, nx, ny, nz, nzm):
+        self._check(self.L.x3d_derzvp(self.handle, _ptr(tz), _ptr(uz), op.handle, nx, ny, nz, nzm))
+
+    def interzvp(self, tz, uz, op, nx, ny, nz, nzm):
+        self._check(self.L.x3d_interzvp(self.handle, _ptr(tz), _ptr(uz), op.handle, nx, ny, nz, nzm))
+
+    def derzpv(self, tz, uz, op, nx, ny, nzm, nz):
+        self._check(self.L.x3d_derzpv(self.handle, _ptr(tz), _ptr(uz), op.handle, nx, ny, nzm, nz))
+
+    def interzpv(self, tz, uz, op, nx, ny, nzm, nz):
+        self._check(self.L.x3d_interzpv(self.handle, _ptr(tz), _ptr(uz), op.handle, nx, ny, nzm, nz))
+
+    # -- batch ------------------------------------------------------------
+    def apply_batch(self, items):
+        """items: iterable of (operator, in_field, out_field)."""
+        items = list(items)
+        arr = (_capi.Work * max(1, len(items)))()
+        for k, (op, src, dst) in enumerate(items):
+            arr[k].op, arr[k].in_, arr[k].out = op.handle, _ptr(src), _ptr(dst)
+        self._check(self.L.x3d_apply_batch(self.handle, arr, len(items)))
+
+    # -- thomas -----------------------------------------------------------
+    def _thomas(self, fn, tt, ff, fs, fw, perio, alfa, nx, ny, nz):
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (ff, fs, fw, perio)]
+        self._check(fn(self.handle, _ptr(tt), *[None if a is None else a.ctypes.data for a in arrs],
+                       float(alfa), nx, ny, nz))
+
+    def xthomas(self, tt, ff, fs, fw, perio, alfa, nx, ny, nz):
+        self._thomas(self.L.x3d_xthomas, tt, ff, fs, fw, perio, alfa, nx, ny, nz)
+
+    def ythomas(self, tt, ff, fs, fw, perio, alfa, nx, ny, nz):
+        self._thomas(self.L.x3d_ythomas, tt, ff, fs, fw, perio, alfa, nx, ny, nz)
+
+    def zthomas(self, tt, ff, fs, fw, perio, alfa, nx, ny, nz):
+        self._thomas(self.L.x3d_zthomas, tt, ff, fs, fw, perio, alfa, nx, ny, nz)
+
+    # -- x3d_transpose ----------------------------------------------------
+    def transpose_x_to_y(self, src, dst, is_complex=False):
+        self._check(self.L.x3d_transpose_x_to_y(self.handle, _ptr(src), _ptr(dst), int(is_complex)))
+
+    def transpose_y_to_z(self, src, dst, is_complex=False):
+        self._check(self.L.x3d_transpose_y_to_z(self.handle, _ptr(src), _ptr(dst), int(is_complex)))
+
+    def transpose_z_to_y(self, src, dst, is_complex=False):
+        self._check(self.L.x3d_transpose_z_to_y(self.handle, _ptr(src), _ptr(dst), int(is_complex)))
+
+    def transpose_y_to_x(self, src, dst, is_complex=False):
+        self._check(self.L.x3d_transpose_y_to_x(self.handle, _ptr(src), _ptr(dst), int(is_complex)))
+
+    # -- poisson / navier / transeq / time --------------------------------
+    def poisson(self, rhs):
+        self._check(self.L.x3d_poisson(self.handle, _ptr(rhs)))
+
+    def divergence(self, pp3, ux1, uy1, uz1, nlock=1):
+        self._check(self.L.x3d_divergence(self.handle, _ptr(pp3), _ptr(ux1), _ptr(uy1), _ptr(uz1), int(nlock)))
+
+    def gradp(self, px1, py1, pz1, pp3):
+        self._check(self.L.x3d_gradp(self.handle, _ptr(px1), _ptr(py1), _ptr(pz1), _ptr(pp3)))
+
+    def cor_vel(self, ux, uy, uz, px, py, pz):
+        self._check(self.L.x3d_cor_vel(self.handle, *[_ptr(a) for a in (ux, uy, uz, px, py, pz)]))
+
+    def solve_poisson(self, pp3, px1, py1, pz1, ux1, uy1, uz1):
+        self._check(self.L.x3d_solve_poisson(self.handle, *[_ptr(a) for a in (pp3, px1, py1, pz1, ux1, uy1, uz1)]))
+
+    def div_stats(self, pp3):
+        out = (ctypes.c_double * 2)()
+        self._check(self.L.x3d_div_stats(self.handle, _ptr(pp3), out))
+        return out[0], out[1]
+
+    def momentum_rhs_eq(self, dux1, duy1, duz1, ux1, uy1, uz1):
+        self._check(self.L.x3d_momentum_rhs_eq(self.handle, *[_ptr(a) for a in (dux1, duy1, duz1, ux1, uy1, uz1)]))
+
+    def int_time(self, ux1, uy1, uz1, dux1, duy1, duz1, gdt):
+        self._check(self.L.x3d_int_time(self.handle, *[_ptr(a) for a in (ux1, uy1, uz1, dux1, duy1, duz1)], float(gdt)))
+
+    def euler_step(self, ux1, uy1, uz1, dux1, duy1, duz1, pp3, px1, py1, pz1, dt):
+        self._check(self.L.x3d_euler_step(self.handle, *[_ptr(a) for a in (ux1, uy1, uz1, dux1, duy1, duz1, pp3, px1, py1, pz1)], float(dt)))
+
+    def vel(self, u, v, w):
+        self._check(self.L.x3d_vel(self.handle, _ptr(u), _ptr(v), _ptr(w)))
+
+    def test_rms(self, which, du):
+        out = ctypes.c_double()
+        self._check(self.L.x3d_test_rms(self.handle, int(which), _ptr(du), ctypes.byref(out)))
+        return out.value
+
+
+def to_device(a: np.ndarray, dtype=None, device="cuda"):
+    """Fortran-ordered (nx, ny, nz) numpy field -> contiguous (nz, ny, nx) torch tensor."""
+    import torch
+    a = np.asarray(a)
+    t = torch.from_numpy(np.ascontiguousarray(a.transpose(2, 1, 0)))
+    if dtype is not None:
+        t = t.to(dtype)
+    return t.to(device)
+
+
+def to_host(t) -> np.ndarray:
+    """Contiguous (nz, ny, nx) torch tensor -> Fortran-ordered (nx, ny, nz) numpy array."""
+    return np.asfortranarray(t.detach().cpu().numpy().transpose(2, 1, 0))

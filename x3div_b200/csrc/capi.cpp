@@ -1,0 +1,773 @@
+// The C ABI (include/x3d_b200.h): argument checks, host-pointer staging,
+// dispatch to the line-solve kernels, and the stage compositions of
+// src/navier.f90, src/transeq.f90 and src/time_integrators.f90.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "x3d_internal.h"
+
+using namespace x3d;
+
+namespace x3d {
+
+int set_error(x3d_ctx_s *ctx, int code, const std::string &msg)
+{
+    if (ctx) ctx->last_error = msg;
+    return code;
+}
+
+int cuda_check(x3d_ctx_s *ctx, cudaError_t e, const char *what)
+{
+    if (e == cudaSuccess) return X3D_OK;
+    return set_error(ctx, X3D_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void *ctx_scratch(x3d_ctx_s *ctx, int idx)
+{
+    const size_t bytes = ctx->npts() * 8;  // large enough for either precision
+    while ((int)ctx->scratch.size() <= idx) {
+        void *p = nullptr;
+        if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+        ctx->scratch.push_back(p);
+    }
+    return ctx->scratch[idx];
+}
+
+}  // namespace x3d
+
+namespace {
+
+// Which table entry (kind, dir) each named operator instance is; derx and
+// derxp are the same operator when periodic (first_deriv_imp_ only changes
+// ffp for free-slip, src/x3d_operator_1d.f90:479-486).
+struct Named {
+    int kind, dir;
+};
+const Named kNamed[X3D_OP_COUNT] = {
+    {DER, DX},   {DER, DX},   {DER, DY},   {DER, DY},   {DER, DZ},   {DER, DZ},   {DERVP, DX},
+    {DERVP, DY}, {DERVP, DZ}, {DERPV, DX}, {DERPV, DY}, {DERPV, DZ}, {INTVP, DX}, {INTVP, DY},
+    {INTVP, DZ}, {INTPV, DX}, {INTPV, DY}, {INTPV, DZ}, {DER2, DX},  {DER2, DY},  {DER2, DZ},
+};
+
+bool is_device_ptr(const void *p)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// Host-pointer staging for one call: inputs are uploaded before the work,
+// outputs downloaded after it, and the call then synchronises.
+class Stager {
+  public:
+    explicit Stager(x3d_ctx_s *c) : ctx(c) {}
+    ~Stager() { release(); }
+    void *in(const void *p, size_t bytes) { return stage(const_cast<void *>(p), bytes, true, false); }
+    void *out(void *p, size_t bytes) { return stage(p, bytes, false, true); }
+    void *inout(void *p, size_t bytes) { return stage(p, bytes, true, true); }
+    int status() const { return rc; }
+    int finish(int work_rc)
+    {
+        if (work_rc) return work_rc;
+        if (rc) return rc;
+        if (!any_host) return X3D_OK;
+        for (auto &it : items)
+            if (it.out) {
+                int r = cuda_check(ctx, cudaMemcpyAsync(it.user, it.dev, it.bytes, cudaMemcpyDeviceToHost, ctx->stream), "stage d2h");
+                if (r) return r;
+            }
+        return cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "stage sync");
+    }
+
+  private:
+    struct Item {
+        void *user, *dev;
+        size_t bytes;
+        bool out;
+    };
+    x3d_ctx_s *ctx;
+    std::vector<Item> items;
+    std::vector<void *> owned;
+    bool any_host = false;
+    int rc = X3D_OK;
+    void *stage(void *p, size_t bytes, bool upload, bool download)
+    {
+        if (!p || rc) return p;
+        if (is_device_ptr(p)) return p;
+        for (auto &it : items)  // the same host array passed twice maps to one device copy
+            if (it.user == p) {
+                it.out = it.out || download;
+                return it.dev;
+            }
+        any_host = true;
+        void *d = nullptr;
+        if (cudaMalloc(&d, bytes) != cudaSuccess) {
+            rc = set_error(ctx, X3D_ENOMEM, "staging allocation failed");
+            return nullptr;
+        }
+        owned.push_back(d);
+        if (upload) {
+            int r = cuda_check(ctx, cudaMemcpyAsync(d, p, bytes, cudaMemcpyHostToDevice, ctx->stream), "stage h2d");
+            if (r) rc = r;
+        }
+        items.push_back({p, d, bytes, download});
+        return d;
+    }
+    void release()
+    {
+        if (!owned.empty()) cudaStreamSynchronize(ctx->stream);
+        for (void *d : owned) cudaFree(d);
+        owned.clear();
+    }
+};
+
+int check_ctx(x3d_ctx_s *ctx)
+{
+    if (!ctx) return X3D_EINVAL;
+    cudaSetDevice(ctx->device);
+    return X3D_OK;
+}
+
+bool fp32(const x3d_ctx_s *ctx) { return ctx->precision == X3D_F32; }
+
+// One operator application on (nx,ny,nz) fields along dir.
+int apply_op(x3d_ctx_s *ctx, void *t, const void *u, x3d_op_s *op, int want_kind, int want_dir,
+             int nx, int ny, int nz)
+{
+    if (!op || !t || !u) return set_error(ctx, X3D_EINVAL, "null operator or field");
+    if (op->h.kind != want_kind || op->h.dir != want_dir)
+        return set_error(ctx, X3D_EINVAL, "operator kind/direction does not match the routine");
+    if (nx <= 0 || ny <= 0 || nz <= 0) return set_error(ctx, X3D_EINVAL, "bad field shape");
+    const int n = want_dir == DX ? nx : (want_dir == DY ? ny : nz);
+    if (op->h.n != n) return set_error(ctx, X3D_EINVAL, "operator length differs from the line length");
+    if (!op->h.periodic) return set_error(ctx, X3D_EUNSUPPORTED, "only periodic operators are supported");
+    if (t == u) return set_error(ctx, X3D_EINVAL, "t and u must not alias (t is intent(out))");
+    const size_t bytes = (size_t)nx * ny * nz * ctx->elem();
+    Stager sg(ctx);
+    void *du = sg.in(u, bytes);
+    void *dt = sg.out(t, bytes);
+    if (sg.status()) return sg.status();
+    return sg.finish(launch_linesolve(ctx, op, want_kind, want_dir, du, dt, nx, ny, nz, fp32(ctx)));
+}
+
+int thomas_call(x3d_ctx_s *ctx, int dir, void *tt, const double *ff, const double *fs,
+                const double *fw, const double *perio, double alfa, int nx, int ny, int nz)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!tt || !ff || !fs || !fw) return set_error(ctx, X3D_EINVAL, "null argument");
+    const int n = dir == DX ? nx : (dir == DY ? ny : nz);
+    if (n < 8) return set_error(ctx, X3D_EUNSUPPORTED, "line length must be >= 8");
+    // The coefficient arrays may live on either side; bring them to the host.
+    auto fetch = [&](const double *p, std::vector<double> &v) {
+        v.resize(n);
+        if (is_device_ptr(p))
+            return cudaMemcpy(v.data(), p, n * sizeof(double), cudaMemcpyDeviceToHost) == cudaSuccess;
+        std::memcpy(v.data(), p, n * sizeof(double));
+        return true;
+    };
+    x3d_op_s op;
+    op.h.kind = IDENT;
+    op.h.dir = dir;
+    op.h.n = n;
+    op.h.alfa = alfa;
+    op.h.periodic = perio ? 1 : 0;
+    if (!fetch(ff, op.h.f) || !fetch(fs, op.h.s) || !fetch(fw, op.h.w))
+        return set_error(ctx, X3D_ECUDA, "coefficient copy failed");
+    if (perio && !fetch(perio, op.h.per)) return set_error(ctx, X3D_ECUDA, "coefficient copy failed");
+    finish_op(op.h);
+    rc = upload_op(&op);
+    if (rc) {
+        free_op(&op);
+        return set_error(ctx, rc, "operator upload failed");
+    }
+    const size_t bytes = (size_t)nx * ny * nz * ctx->elem();
+    Stager sg(ctx);
+    void *d = sg.inout(tt, bytes);
+    if (sg.status()) {
+        free_op(&op);
+        return sg.status();
+    }
+    rc = sg.finish(launch_linesolve(ctx, &op, IDENT, dir, d, d, nx, ny, nz, fp32(ctx)));
+    cudaStreamSynchronize(ctx->stream);  // the temporary operator dies here
+    free_op(&op);
+    return rc;
+}
+
+int check_shape(x3d_ctx_s *ctx, int nx, int ny, int nz)
+{
+    if (nx != ctx->nx || ny != ctx->ny || nz != ctx->nz)
+        return set_error(ctx, X3D_EINVAL, "field shape differs from the context grid");
+    return X3D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+// ---- context ----------------------------------------------------------------
+
+int x3d_ctx_create(x3d_ctx *out, int nx, int ny, int nz, double xlx, double yly, double zlz,
+                   int precision, int device)
+{
+    if (!out) return X3D_EINVAL;
+    *out = nullptr;
+    if (nx < 8 || ny < 8 || nz < 8) return X3D_EUNSUPPORTED;
+    if (precision != X3D_F64 && precision != X3D_F32) return X3D_EINVAL;
+    if (!(xlx > 0 && yly > 0 && zlz > 0)) return X3D_EINVAL;
+    if (cudaSetDevice(device) != cudaSuccess) return X3D_ECUDA;
+    auto *ctx = new (std::nothrow) x3d_ctx_s;
+    if (!ctx) return X3D_ENOMEM;
+    ctx->nx = nx; ctx->ny = ny; ctx->nz = nz;
+    ctx->xlx = xlx; ctx->yly = yly; ctx->zlz = zlz;
+    ctx->dx = xlx / nx; ctx->dy = yly / ny; ctx->dz = zlz / nz;  // parameter(): dx = xlx/nxm, nxm = nx
+    ctx->precision = precision;
+    ctx->device = device;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+        delete ctx;
+        return X3D_ECUDA;
+    }
+    ctx->num_sms = prop.multiProcessorCount;
+    ctx->smem_optin = prop.sharedMemPerBlockOptin;
+    if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&ctx->d_err, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&ctx->d_red, 4 * sizeof(double)) != cudaSuccess) {
+        x3d_ctx_destroy(ctx);
+        return X3D_ECUDA;
+    }
+    cudaMemset(ctx->d_err, 0, sizeof(int));
+    ctx->stream = ctx->own_stream;
+    const double dd[3] = {ctx->dx, ctx->dy, ctx->dz};
+    const int nn[3] = {nx, ny, nz};
+    for (int w = 0; w < X3D_OP_COUNT; ++w) {
+        auto *op = new (std::nothrow) x3d_op_s;
+        if (!op) {
+            x3d_ctx_destroy(ctx);
+            return X3D_ENOMEM;
+        }
+        op->builtin = true;
+        ctx->builtin[w] = op;
+        const int d = kNamed[w].dir;
+        int rc = build_periodic_op(kNamed[w].kind, d, nn[d], dd[d], op->h);
+        if (!rc) rc = upload_op(op);
+        if (rc) {
+            x3d_ctx_destroy(ctx);
+            return rc;
+        }
+    }
+    *out = ctx;
+    return X3D_OK;
+}
+
+int x3d_ctx_destroy(x3d_ctx ctx)
+{
+    if (!ctx) return X3D_EINVAL;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (auto *&op : ctx->builtin) {
+        if (op) {
+            free_op(op);
+            delete op;
+        }
+        op = nullptr;
+    }
+    poisson_free(ctx);
+    for (void *p : ctx->scratch) cudaFree(p);
+    ctx->scratch.clear();
+    if (ctx->d_err) cudaFree(ctx->d_err);
+    if (ctx->d_red) cudaFree(ctx->d_red);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return X3D_OK;
+}
+
+int x3d_ctx_set_stream(x3d_ctx ctx, void *stream)
+{
+    if (!ctx) return X3D_EINVAL;
+    ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+    return X3D_OK;
+}
+
+int x3d_ctx_sync(x3d_ctx ctx)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    rc = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "stream sync");
+    if (rc) return rc;
+    int flag = 0;
+    rc = cuda_check(ctx, cudaMemcpy(&flag, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost), "error flag read");
+    if (rc) return rc;
+    if (flag) {
+        cudaMemset(ctx->d_err, 0, sizeof(int));
+        return set_error(ctx, X3D_ETIMEOUT, "a device-side bounded wait gave up (code " + std::to_string(flag) + ")");
+    }
+    return X3D_OK;
+}
+
+const char *x3d_ctx_last_error(x3d_ctx ctx)
+{
+    if (!ctx) return "null context";
+    return ctx->last_error.c_str();
+}
+
+int x3d_ctx_geometry(x3d_ctx ctx, int *dims, double *lengths, double *spacing, int *precision)
+{
+    if (!ctx) return X3D_EINVAL;
+    if (dims) { dims[0] = ctx->nx; dims[1] = ctx->ny; dims[2] = ctx->nz; }
+    if (lengths) { lengths[0] = ctx->xlx; lengths[1] = ctx->yly; lengths[2] = ctx->zlz; }
+    if (spacing) { spacing[0] = ctx->dx; spacing[1] = ctx->dy; spacing[2] = ctx->dz; }
+    if (precision) *precision = ctx->precision;
+    return X3D_OK;
+}
+
+// ---- operators ------------------------------------------------------------------
+
+int x3d_op_builtin(x3d_ctx ctx, int which, x3d_op *op)
+{
+    if (!ctx || !op) return X3D_EINVAL;
+    if (which < 0 || which >= X3D_OP_COUNT) return set_error(ctx, X3D_EINVAL, "unknown operator instance");
+    *op = ctx->builtin[which];
+    return X3D_OK;
+}
+
+int x3d_op_create(x3d_ctx ctx, int kind, int dir, int n, int npaire, double alfa, const double *f,
+                  const double *s, const double *w, const double *periodic, const double *rhs,
+                  x3d_op *out)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!out || !f || !s || !w || !rhs) return set_error(ctx, X3D_EINVAL, "null argument");
+    if (kind < DER || kind > INTPV || dir < DX || dir > DZ) return set_error(ctx, X3D_EINVAL, "bad kind or direction");
+    if (n < 8) return set_error(ctx, X3D_EUNSUPPORTED, "line length must be >= 8");
+    if (!periodic) return set_error(ctx, X3D_EUNSUPPORTED, "only periodic operators are supported");
+    auto *op = new (std::nothrow) x3d_op_s;
+    if (!op) return X3D_ENOMEM;
+    op->h.kind = kind;
+    op->h.dir = dir;
+    op->h.n = n;
+    op->h.npaire = npaire;
+    op->h.periodic = 1;
+    op->h.alfa = alfa;
+    op->h.a = rhs[0]; op->h.b = rhs[1]; op->h.c = rhs[2]; op->h.d = rhs[3];
+    op->h.f.assign(f, f + n);
+    op->h.s.assign(s, s + n);
+    op->h.w.assign(w, w + n);
+    op->h.per.assign(periodic, periodic + n);
+    finish_op(op->h);
+    rc = upload_op(op);
+    if (rc) {
+        free_op(op);
+        delete op;
+        return set_error(ctx, rc, "operator upload failed");
+    }
+    *out = op;
+    return X3D_OK;
+}
+
+int x3d_op_destroy(x3d_ctx ctx, x3d_op op)
+{
+    if (!ctx || !op) return X3D_EINVAL;
+    if (op->builtin) return set_error(ctx, X3D_EINVAL, "built-in operators belong to the context");
+    cudaStreamSynchronize(ctx->stream);
+    free_op(op);
+    delete op;
+    return X3D_OK;
+}
+
+int x3d_op_info(x3d_op op, int *meta, double *scal, double *f, double *s, double *w, double *periodic)
+{
+    if (!op) return X3D_EINVAL;
+    const OpHost &h = op->h;
+    if (meta) { meta[0] = h.n; meta[1] = h.kind; meta[2] = h.dir; meta[3] = h.npaire; }
+    if (scal) { scal[0] = h.alfa; scal[1] = h.a; scal[2] = h.b; scal[3] = h.c; scal[4] = h.d; }
+    if (f) std::memcpy(f, h.f.data(), h.n * sizeof(double));
+    if (s) std::memcpy(s, h.s.data(), h.n * sizeof(double));
+    if (w) std::memcpy(w, h.w.data(), h.n * sizeof(double));
+    if (periodic) {
+        if (h.per.empty()) std::memset(periodic, 0, h.n * sizeof(double));
+        else std::memcpy(periodic, h.per.data(), h.n * sizeof(double));
+    }
+    return X3D_OK;
+}
+
+// ---- derivatives ------------------------------------------------------------------
+
+#define X3D_APPLY(kind, dir, t, u, op, nx, ny, nz)              \
+    do {                                                        \
+        int rc_ = check_ctx(ctx);                               \
+        if (rc_) return rc_;                                    \
+        return apply_op(ctx, t, u, op, kind, dir, nx, ny, nz);  \
+    } while (0)
+
+int x3d_derx(x3d_ctx ctx, void *tx, const void *ux, x3d_op op, int nx, int ny, int nz)
+{ X3D_APPLY(DER, DX, tx, ux, op, nx, ny, nz); }
+int x3d_dery(x3d_ctx ctx, void *ty, const void *uy, x3d_op op, const double *, int nx, int ny, int nz)
+{ X3D_APPLY(DER, DY, ty, uy, op, nx, ny, nz); }
+int x3d_derz(x3d_ctx ctx, void *tz, const void *uz, x3d_op op, int nx, int ny, int nz)
+{ X3D_APPLY(DER, DZ, tz, uz, op, nx, ny, nz); }
+int x3d_derxx(x3d_ctx ctx, void *tx, const void *ux, x3d_op op, int nx, int ny, int nz)
+{ X3D_APPLY(DER2, DX, tx, ux, op, nx, ny, nz); }
+int x3d_deryy(x3d_ctx ctx, void *ty, const void *uy, x3d_op op, int nx, int ny, int nz)
+{ X3D_APPLY(DER2, DY, ty, uy, op, nx, ny, nz); }
+int x3d_derzz(x3d_ctx ctx, void *tz, const void *uz, x3d_op op, int nx, int ny, int nz)
+{ X3D_APPLY(DER2, DZ, tz, uz, op, nx, ny, nz); }
+
+// ---- staggered ----------------------------------------------------------------------
+// Periodic only: the pressure-grid length equals the velocity-grid length.
+#define X3D_STAG(kind, dir, t, u, op, n_in, n_out, nx, ny, nz)                                      \
+    do {                                                                                            \
+        int rc_ = check_ctx(ctx);                                                                   \
+        if (rc_) return rc_;                                                                        \
+        if ((n_in) != (n_out))                                                                      \
+            return set_error(ctx, X3D_EUNSUPPORTED, "non-periodic staggered grids are not supported"); \
+        return apply_op(ctx, t, u, op, kind, dir, nx, ny, nz);                                      \
+    } while (0)
+
+int x3d_derxvp(x3d_ctx ctx, void *tx, const void *ux, x3d_op op, int nx, int nxm, int ny, int nz)
+{ X3D_STAG(DERVP, DX, tx, ux, op, nx, nxm, nx, ny, nz); }
+int x3d_interxvp(x3d_ctx ctx, void *tx, const void *ux, x3d_op op, int nx, int nxm, int ny, int nz)
+{ X3D_STAG(INTVP, DX, tx, ux, op, nx, nxm, nx, ny, nz); }
+int x3d_derxpv(x3d_ctx ctx, void *tx, const void *ux, x3d_op op, int nxm, int nx, int ny, int nz)
+{ X3D_STAG(DERPV, DX, tx, ux, op, nxm, nx, nx, ny, nz); }
+int x3d_interxpv(x3d_ctx ctx, void *tx, const void *ux, x3d_op op, int nxm, int nx, int ny, int nz)
+{ X3D_STAG(INTPV, DX, tx, ux, op, nxm, nx, nx, ny, nz); }
+int x3d_interyvp(x3d_ctx ctx, void *ty, const void *uy, x3d_op op, int nx, int ny, int nym, int nz)
+{ X3D_STAG(INTVP, DY, ty, uy, op, ny, nym, nx, ny, nz); }
+int x3d_deryvp(x3d_ctx ctx, void *ty, const void *uy, x3d_op op, const double *, int nx, int ny, int nym, int nz)
+{ X3D_STAG(DERVP, DY, ty, uy, op, ny, nym, nx, ny, nz); }
+int x3d_interypv(x3d_ctx ctx, void *ty, const void *uy, x3d_op op, int nx, int nym, int ny, int nz)
+{ X3D_STAG(INTPV, DY, ty, uy, op, nym, ny, nx, ny, nz); }
+int x3d_derypv(x3d_ctx ctx, void *ty, const void *uy, x3d_op op, const double *, int nx, int nym, int ny, int nz)
+{ X3D_STAG(DERPV, DY, ty, uy, op, nym, ny, nx, ny, nz); }
+int x3d_derzvp(x3d_ctx ctx, void *tz, const void *uz, x3d_op op, int nx, int ny, int nz, int nzm)
+{ X3D_STAG(DERVP, DZ, tz, uz, op, nz, nzm, nx, ny, nz); }
+int x3d_interzvp(x3d_ctx ctx, void *tz, const void *uz, x3d_op op, int nx, int ny, int nz, int nzm)
+{ X3D_STAG(INTVP, DZ, tz, uz, op, nz, nzm, nx, ny, nz); }
+int x3d_derzpv(x3d_ctx ctx, void *tz, const void *uz, x3d_op op, int nx, int ny, int nzm, int nz)
+{ X3D_STAG(DERPV, DZ, tz, uz, op, nzm, nz, nx, ny, nz); }
+int x3d_interzpv(x3d_ctx ctx, void *tz, const void *uz, x3d_op op, int nx, int ny, int nzm, int nz)
+{ X3D_STAG(INTPV, DZ, tz, uz, op, nzm, nz, nx, ny, nz); }
+
+// ---- batch ----------------------------------------------------------------------------
+
+int x3d_apply_batch(x3d_ctx ctx, const x3d_work *items, int count)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (count < 0 || (count > 0 && !items)) return set_error(ctx, X3D_EINVAL, "bad work-list");
+    const size_t bytes = ctx->npts() * ctx->elem();
+    for (int i = 0; i < count; ++i) {
+        const x3d_op_s *op = items[i].op;
+        if (!op || !items[i].in || !items[i].out) return set_error(ctx, X3D_EINVAL, "null work item");
+        const int n = op->h.dir == DX ? ctx->nx : (op->h.dir == DY ? ctx->ny : ctx->nz);
+        if (op->h.n != n || !op->h.periodic) return set_error(ctx, X3D_EINVAL, "operator does not fit the grid");
+        for (int j = 0; j < count; ++j)
+            if (items[i].out == items[j].in) return set_error(ctx, X3D_EINVAL, "an output aliases an input");
+    }
+    Stager sg(ctx);
+    std::vector<const void *> din(count);
+    std::vector<void *> dout(count);
+    for (int i = 0; i < count; ++i) din[i] = sg.in(items[i].in, bytes);
+    for (int i = 0; i < count; ++i) dout[i] = sg.out(items[i].out, bytes);
+    if (sg.status()) return sg.status();
+    for (int i = 0; i < count && !rc; ++i) {
+        const x3d_op_s *op = items[i].op;
+        rc = launch_linesolve(ctx, op, op->h.kind, op->h.dir, din[i], dout[i], ctx->nx, ctx->ny, ctx->nz, fp32(ctx));
+    }
+    return sg.finish(rc);
+}
+
+// ---- Thomas ------------------------------------------------------------------------
+
+int x3d_xthomas(x3d_ctx ctx, void *tt, const double *ff, const double *fs, const double *fw,
+                const double *perio, double alfa, int nx, int ny, int nz)
+{ return thomas_call(ctx, DX, tt, ff, fs, fw, perio, alfa, nx, ny, nz); }
+int x3d_ythomas(x3d_ctx ctx, void *tt, const double *ff, const double *fs, const double *fw,
+                const double *perio, double alfa, int nx, int ny, int nz)
+{ return thomas_call(ctx, DY, tt, ff, fs, fw, perio, alfa, nx, ny, nz); }
+int x3d_zthomas(x3d_ctx ctx, void *tt, const double *ff, const double *fs, const double *fw,
+                const double *perio, double alfa, int nx, int ny, int nz)
+{ return thomas_call(ctx, DZ, tt, ff, fs, fw, perio, alfa, nx, ny, nz); }
+
+// ---- transposes ---------------------------------------------------------------------
+
+static int transpose_copy(x3d_ctx ctx, const void *in, void *out, int is_complex)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!in || !out) return set_error(ctx, X3D_EINVAL, "null field");
+    const size_t bytes = ctx->npts() * ctx->elem() * (is_complex ? 2 : 1);
+    Stager sg(ctx);
+    void *di = sg.in(in, bytes);
+    void *dout = sg.out(out, bytes);
+    if (sg.status()) return sg.status();
+    return sg.finish(launch_copy(ctx, dout, di, bytes));
+}
+
+int x3d_transpose_x_to_y(x3d_ctx ctx, const void *in, void *out, int c) { return transpose_copy(ctx, in, out, c); }
+int x3d_transpose_y_to_z(x3d_ctx ctx, const void *in, void *out, int c) { return transpose_copy(ctx, in, out, c); }
+int x3d_transpose_z_to_y(x3d_ctx ctx, const void *in, void *out, int c) { return transpose_copy(ctx, in, out, c); }
+int x3d_transpose_y_to_x(x3d_ctx ctx, const void *in, void *out, int c) { return transpose_copy(ctx, in, out, c); }
+
+// ---- Poisson -------------------------------------------------------------------------
+
+int x3d_poisson(x3d_ctx ctx, double *rhs)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!rhs) return set_error(ctx, X3D_EINVAL, "null field");
+    Stager sg(ctx);
+    double *d = static_cast<double *>(sg.inout(rhs, ctx->npts() * sizeof(double)));
+    if (sg.status()) return sg.status();
+    return sg.finish(poisson_solve(ctx, d));
+}
+
+// ---- navier ----------------------------------------------------------------------------
+
+// divergence (src/navier.f90:98-236) with 1x1 transposes elided.
+static int divergence_dev(x3d_ctx_s *ctx, double *pp3, const void *ux, const void *uy, const void *uz)
+{
+    const int nx = ctx->nx, ny = ctx->ny, nz = ctx->nz;
+    const bool f = fp32(ctx);
+    const size_t N = ctx->npts();
+    void *s[5];
+    for (int i = 0; i < 5; ++i)
+        if (!(s[i] = ctx_scratch(ctx, i))) return set_error(ctx, X3D_ENOMEM, "scratch allocation failed");
+    x3d_op_s **B = ctx->builtin;
+    int rc = 0;
+    rc = rc ? rc : launch_linesolve(ctx, B[X3D_OP_DERXVP], DERVP, DX, ux, s[0], nx, ny, nz, f);  // pp1
+    rc = rc ? rc : launch_linesolve(ctx, B[X3D_OP_INTXVP], INTVP, DX, uy, s[1], nx, ny, nz, f);  // pgy1
+    rc = rc ? rc : launch_linesolve(ctx, B[X3D_OP_INTXVP], INTVP, DX, uz, s[2], nx, ny, nz, f);  // pgz1
+    rc = rc ? rc : launch_linesolve(ctx, B[X3D_OP_INTYVP], INTVP, DY, s[0], s[3], nx, ny, nz, f);  // upi2
+    rc = rc ? rc : launch_linesolve(ctx, B[X3D_OP_DERYVP], DERVP, DY, s[1], s[4], nx, ny, nz, f);  // duydypi2
+    rc = rc ? rc : launch_add(ctx, f, s[4], s[4], s[3], N);
+    rc = rc ? rc : launch_linesolve(ctx, B[X3D_OP_INTYVP], INTVP, DY, s[2], s[3], nx, ny, nz, f);  // upi2
+    if (!f) {
+        rc = rc ? rc : launch_linesolve(ctx, B[X3D_OP_INTZVP], INTVP, DZ, s[4], pp3, nx, ny, nz, f);
+        rc = rc ? rc : launch_linesolve(ctx, B[X3D_OP_DERZVP], DERVP, DZ, s[3], s[0], nx, ny, nz, f);  // po3
+        rc = rc ? rc : launch_add(ctx, false, pp3, pp3, s[0], N);
+    } else {
+        rc = rc ? rc : launch_linesolve(ctx, B[X3D_OP_INTZVP], INTVP, DZ, s[4], s[0], nx, ny, nz, f);
+        rc = rc ? rc : launch_linesolve(ctx, B[X3D_OP_DERZVP], DERVP, DZ, s[3], s[1], nx, ny, nz, f);
+        rc = rc ? rc : launch_add(ctx, true, s[0], s[0], s[1], N);
+        rc = rc ? rc : launch_convert(ctx, pp3, false, s[0], true, N);
+    }
+    return rc;
+}
+
+// gradp (src/navier.f90:249-359) with 1x1 transposes elided.
+static int gradp_dev(x3d_ctx_s *ctx, void *px, void *py, void *pz, const double *pp3)
+{
+    const int nx = ctx->nx, ny = ctx->ny, nz = ctx->nz;
+    const bool f = fp32(ctx);
+    const size_t N = ctx->npts();
+    void *s[6];
+    for (int i = 0; i < 6; ++i)
+        if (!(s[i] = ctx_scratch(ctx, i))) return set_error(ctx, X3D_ENOMEM, "scratch allocation failed");
+    x3d_op_s **B = ctx->builtin;
+    int rc = 0;
+    const void *p = pp3;
+    if (f) {
+        rc = launch_convert(ctx, s[5], true, pp3, false, N);
+        p = s[5];
+    }
+    rc = rc ? rc : launch_linesolve(ctx, B[X3D_OP_INTZPV], INTPV, DZ, p, s[0], nx, ny, nz, f);     // ppi3
+    rc = rc ? rc : launch_linesolve(ctx, B[X3D_OP_DERZPV], DERPV, DZ, p, s[1], nx, ny, nz, f);     // pgz3
+    rc = rc ? rc : launch_linesolve(ctx, B[X3D_OP_INTYPV], INTPV, DY, s[0], s[2], nx, ny, nz, f);  // ppi2
+    rc = rc ? rc : launch_linesolve(ctx, B[X3D_OP_DERYPV], DERPV, DY, s[0], s[3], nx, ny, nz, f);  // pgy2
+    rc = rc ? rc : launch_linesolve(ctx, B[X3D_OP_INTYPV], INTPV, DY, s[1], s[4], nx, ny, nz, f);  // pgzi2
+    rc = rc ? rc : launch_linesolve(ctx, B[X3D_OP_DERXPV], DERPV, DX, s[2], px, nx, ny, nz, f);
+    rc = rc ? rc : launch_linesolve(ctx, B[X3D_OP_INTXPV], INTPV, DX, s[3], py, nx, ny, nz, f);
+    rc = rc ? rc : launch_linesolve(ctx, B[X3D_OP_INTXPV], INTPV, DX, s[4], pz, nx, ny, nz, f);
+    return rc;
+}
+
+// momentum_rhs_eq (src/transeq.f90:44-355) with 1x1 transposes elided.
+static int momentum_dev(x3d_ctx_s *ctx, void *du[3], const void *u[3])
+{
+    const int nx = ctx->nx, ny = ctx->ny, nz = ctx->nz;
+    const bool f = fp32(ctx);
+    const size_t N = ctx->npts();
+    void *s[4];
+    for (int i = 0; i < 4; ++i)
+        if (!(s[i] = ctx_scratch(ctx, i))) return set_error(ctx, X3D_ENOMEM, "scratch allocation failed");
+    x3d_op_s **B = ctx->builtin;
+    void *ta = s[0], *td = s[1], *tg = s[2], *t3 = s[3];
+    int rc = 0;
+    for (int c = 0; c < 3 && !rc; ++c) {
+        const void *uc = u[c];
+        rc = rc ? rc : launch_mul(ctx, f, ta, u[0], uc, N);
+        rc = rc ? rc : launch_linesolve(ctx, B[X3D_OP_DERXP], DER, DX, ta, td, nx, ny, nz, f);
+        rc = rc ? rc : launch_linesolve(ctx, B[X3D_OP_DERX], DER, DX, uc, ta, nx, ny, nz, f);
+        rc = rc ? rc : launch_fma_acc(ctx, f, du[c], td, u[0], ta, N);
+        rc = rc ? rc : launch_mul(ctx, f, td, uc, u[1], N);
+        rc = rc ? rc : launch_linesolve(ctx, B[X3D_OP_DERY], DER, DY, td, tg, nx, ny, nz, f);
+        rc = rc ? rc : launch_linesolve(ctx, B[X3D_OP_DERYP], DER, DY, uc, td, nx, ny, nz, f);
+        rc = rc ? rc : launch_fma_acc(ctx, f, tg, tg, u[1], td, N);
+        rc = rc ? rc : launch_mul(ctx, f, td, uc, u[2], N);
+        rc = rc ? rc : launch_linesolve(ctx, B[X3D_OP_DERZ], DER, DZ, td, t3, nx, ny, nz, f);
+        rc = rc ? rc : launch_linesolve(ctx, B[X3D_OP_DERZP], DER, DZ, uc, td, nx, ny, nz, f);
+        rc = rc ? rc : launch_fma_acc(ctx, f, t3, t3, u[2], td, N);
+        rc = rc ? rc : launch_add(ctx, f, tg, tg, t3, N);
+        rc = rc ? rc : launch_add(ctx, f, du[c], du[c], tg, N);
+    }
+    return rc;
+}
+
+int x3d_divergence(x3d_ctx ctx, double *pp3, const void *ux1, const void *uy1, const void *uz1, int)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!pp3 || !ux1 || !uy1 || !uz1) return set_error(ctx, X3D_EINVAL, "null field");
+    const size_t b = ctx->npts() * ctx->elem();
+    Stager sg(ctx);
+    const void *u = sg.in(ux1, b), *v = sg.in(uy1, b), *w = sg.in(uz1, b);
+    double *p = static_cast<double *>(sg.out(pp3, ctx->npts() * sizeof(double)));
+    if (sg.status()) return sg.status();
+    return sg.finish(divergence_dev(ctx, p, u, v, w));
+}
+
+int x3d_gradp(x3d_ctx ctx, void *px1, void *py1, void *pz1, const double *pp3)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!pp3 || !px1 || !py1 || !pz1) return set_error(ctx, X3D_EINVAL, "null field");
+    const size_t b = ctx->npts() * ctx->elem();
+    Stager sg(ctx);
+    const double *p = static_cast<const double *>(sg.in(pp3, ctx->npts() * sizeof(double)));
+    void *x = sg.out(px1, b), *y = sg.out(py1, b), *z = sg.out(pz1, b);
+    if (sg.status()) return sg.status();
+    return sg.finish(gradp_dev(ctx, x, y, z, p));
+}
+
+int x3d_cor_vel(x3d_ctx ctx, void *ux, void *uy, void *uz, const void *px, const void *py, const void *pz)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!ux || !uy || !uz || !px || !py || !pz) return set_error(ctx, X3D_EINVAL, "null field");
+    const size_t b = ctx->npts() * ctx->elem();
+    Stager sg(ctx);
+    void *u = sg.inout(ux, b), *v = sg.inout(uy, b), *w = sg.inout(uz, b);
+    const void *a = sg.in(px, b), *bb = sg.in(py, b), *c = sg.in(pz, b);
+    if (sg.status()) return sg.status();
+    return sg.finish(launch_sub3(ctx, fp32(ctx), u, v, w, a, bb, c, ctx->npts()));
+}
+
+int x3d_solve_poisson(x3d_ctx ctx, double *pp3, void *px1, void *py1, void *pz1, const void *ux1,
+                      const void *uy1, const void *uz1)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!pp3 || !px1 || !py1 || !pz1 || !ux1 || !uy1 || !uz1) return set_error(ctx, X3D_EINVAL, "null field");
+    const size_t b = ctx->npts() * ctx->elem();
+    Stager sg(ctx);
+    const void *u = sg.in(ux1, b), *v = sg.in(uy1, b), *w = sg.in(uz1, b);
+    double *p = static_cast<double *>(sg.out(pp3, ctx->npts() * sizeof(double)));
+    void *x = sg.out(px1, b), *y = sg.out(py1, b), *z = sg.out(pz1, b);
+    if (sg.status()) return sg.status();
+    rc = divergence_dev(ctx, p, u, v, w);
+    rc = rc ? rc : poisson_solve(ctx, p);
+    rc = rc ? rc : gradp_dev(ctx, x, y, z, p);
+    return sg.finish(rc);
+}
+
+int x3d_div_stats(x3d_ctx ctx, const double *pp3, double *out)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!pp3 || !out) return set_error(ctx, X3D_EINVAL, "null argument");
+    Stager sg(ctx);
+    const double *p = static_cast<const double *>(sg.in(pp3, ctx->npts() * sizeof(double)));
+    if (sg.status()) return sg.status();
+    return sg.finish(reduce_absmax_mean(ctx, p, ctx->npts(), out));
+}
+
+// ---- transeq / time integration --------------------------------------------------------
+
+int x3d_momentum_rhs_eq(x3d_ctx ctx, void *dux1, void *duy1, void *duz1, const void *ux1,
+                        const void *uy1, const void *uz1)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!dux1 || !duy1 || !duz1 || !ux1 || !uy1 || !uz1) return set_error(ctx, X3D_EINVAL, "null field");
+    const size_t b = ctx->npts() * ctx->elem();
+    Stager sg(ctx);
+    const void *u[3] = {sg.in(ux1, b), sg.in(uy1, b), sg.in(uz1, b)};
+    void *du[3] = {sg.out(dux1, b), sg.out(duy1, b), sg.out(duz1, b)};
+    if (sg.status()) return sg.status();
+    return sg.finish(momentum_dev(ctx, du, u));
+}
+
+int x3d_int_time(x3d_ctx ctx, void *ux1, void *uy1, void *uz1, const void *dux1, const void *duy1,
+                 const void *duz1, double gdt)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!dux1 || !duy1 || !duz1 || !ux1 || !uy1 || !uz1) return set_error(ctx, X3D_EINVAL, "null field");
+    const size_t b = ctx->npts() * ctx->elem();
+    Stager sg(ctx);
+    void *u = sg.inout(ux1, b), *v = sg.inout(uy1, b), *w = sg.inout(uz1, b);
+    const void *a = sg.in(dux1, b), *bb = sg.in(duy1, b), *c = sg.in(duz1, b);
+    if (sg.status()) return sg.status();
+    return sg.finish(launch_axpy3(ctx, fp32(ctx), u, v, w, a, bb, c, gdt, ctx->npts()));
+}
+
+int x3d_euler_step(x3d_ctx ctx, void *ux1, void *uy1, void *uz1, void *dux1, void *duy1, void *duz1,
+                   double *pp3, void *px1, void *py1, void *pz1, double dt)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!ux1 || !uy1 || !uz1 || !dux1 || !duy1 || !duz1 || !pp3 || !px1 || !py1 || !pz1)
+        return set_error(ctx, X3D_EINVAL, "null field");
+    const size_t b = ctx->npts() * ctx->elem();
+    Stager sg(ctx);
+    void *u[3] = {sg.inout(ux1, b), sg.inout(uy1, b), sg.inout(uz1, b)};
+    void *du[3] = {sg.out(dux1, b), sg.out(duy1, b), sg.out(duz1, b)};
+    double *p = static_cast<double *>(sg.out(pp3, ctx->npts() * sizeof(double)));
+    void *px = sg.out(px1, b), *py = sg.out(py1, b), *pz = sg.out(pz1, b);
+    if (sg.status()) return sg.status();
+    const void *uc[3] = {u[0], u[1], u[2]};
+    rc = momentum_dev(ctx, du, uc);
+    rc = rc ? rc : launch_axpy3(ctx, fp32(ctx), u[0], u[1], u[2], du[0], du[1], du[2], dt, ctx->npts());
+    rc = rc ? rc : divergence_dev(ctx, p, u[0], u[1], u[2]);
+    rc = rc ? rc : poisson_solve(ctx, p);
+    rc = rc ? rc : gradp_dev(ctx, px, py, pz, p);
+    rc = rc ? rc : launch_sub3(ctx, fp32(ctx), u[0], u[1], u[2], px, py, pz, ctx->npts());
+    return sg.finish(rc);
+}
+
+// ---- mom ----------------------------------------------------------------------------------
+
+int x3d_vel(x3d_ctx ctx, void *u, void *v, void *w)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!u || !v || !w) return set_error(ctx, X3D_EINVAL, "null field");
+    const size_t b = ctx->npts() * ctx->elem();
+    Stager sg(ctx);
+    void *a = sg.out(u, b), *bb = sg.out(v, b), *c = sg.out(w, b);
+    if (sg.status()) return sg.status();
+    return sg.finish(launch_vel(ctx, fp32(ctx), a, bb, c));
+}
+
+int x3d_test_rms(x3d_ctx ctx, int which, const void *du, double *rms)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!du || !rms || which < 0 || which > 2) return set_error(ctx, X3D_EINVAL, "bad argument");
+    Stager sg(ctx);
+    const void *d = sg.in(du, ctx->npts() * ctx->elem());
+    if (sg.status()) return sg.status();
+    return sg.finish(reduce_test_rms(ctx, fp32(ctx), which, d, rms));
+}
+
+}  // extern "C"

@@ -1,0 +1,194 @@
+// FP64 operator precompute, done once per context on the host: the
+// x3d_operator_1d_init path of the reference (src/x3d_operator_1d.f90:59-195)
+// for fully periodic boundaries, plus the two vectors the single-pass GPU
+// sweep needs (g = first row of M^-1 and the Sherman-Morrison denominator).
+#include <cmath>
+#include <cstring>
+
+#include "x3d_internal.h"
+
+namespace x3d {
+
+// Explicit RHS scalars (the module globals of x3d_operator_{x,y,z}_data).
+//  DER:   first_deriv_exp_ with ifirstder = 4 (src/x3d_operator_1d.f90:350-353)
+//  DERVP, DERPV: interpol_exp_ staggered derivative (:510-512)
+//  INTVP, INTPV: interpol_exp_ with ipinter = 3 (:539-544)
+//  DER2:  Lele (1992) sixth-order compact second derivative (alpha = 2/11,
+//         a = 12/11, b = 3/11 in Lele's notation, i.e. asix = (12/11)/d^2 and
+//         bsix = (3/44)/d^2 on the (u(i+2) - 2u(i) + u(i-2)) difference).
+//         The reference declares its scalars (alsaix, asix, bsix) and arrays
+//         (sfx, ssx, swx) but never fills them.
+void rhs_scalars(int kind, double d, double *alfa, double *a, double *b, double *c, double *dd)
+{
+    *alfa = *a = *b = *c = *dd = 0.0;
+    switch (kind) {
+    case DER:
+        *alfa = 1.0 / 3.0;
+        *a = (7.0 / 9.0) / d;
+        *b = (1.0 / 36.0) / d;
+        break;
+    case DERVP:
+    case DERPV:
+        *alfa = 9.0 / 62.0;
+        *a = (63.0 / 62.0) / d;
+        *b = (17.0 / 62.0) / 3.0 / d;
+        break;
+    case INTVP:
+    case INTPV: {
+        const double al = 0.49;
+        *alfa = al;
+        *a = 1.0 / 128.0 * (75.0 + 70.0 * al);
+        *b = 1.0 / 256.0 * (126.0 * al - 25.0);
+        *c = 1.0 / 256.0 * (-10.0 * al + 3.0);
+        *dd = 0.0;
+        break;
+    }
+    case DER2:
+        *alfa = 2.0 / 11.0;
+        *a = (12.0 / 11.0) / (d * d);
+        *b = (3.0 / 44.0) / (d * d);
+        break;
+    default:
+        break;
+    }
+}
+
+// Thomas LU of the tridiagonal (b, c, f): prepare (src/x3d_operator_1d.f90:301-323).
+static void lu_prepare(const std::vector<double> &b, const std::vector<double> &c,
+                       const std::vector<double> &f, std::vector<double> &s, std::vector<double> &w)
+{
+    const int n = (int)c.size();
+    s.assign(n, 0.0);
+    w = c;
+    for (int i = 1; i < n; ++i) {
+        s[i] = b[i - 1] / w[i - 1];
+        w[i] = w[i] - f[i - 1] * s[i];
+    }
+    for (int i = 0; i < n; ++i) w[i] = 1.0 / w[i];
+}
+
+// In-place Thomas solve with the prepared factors (thomas1d, src/thomas.f90:200-218).
+static void lu_solve(std::vector<double> &t, const std::vector<double> &f,
+                     const std::vector<double> &s, const std::vector<double> &w)
+{
+    const int n = (int)t.size();
+    for (int k = 1; k < n; ++k) t[k] -= t[k - 1] * s[k];
+    t[n - 1] *= w[n - 1];
+    for (int k = n - 2; k >= 0; --k) t[k] = (t[k] - f[k] * t[k + 1]) * w[k];
+}
+
+// Periodic operator: every family shares the reference's periodic matrix
+// pattern (first_deriv_imp_ :414-445,467-471; interpol_imp_ :576-599 and
+// :622-645): off-diagonals alpha, corner rows folded by Sherman-Morrison so
+// that c(1) = 2, c(n) = 1 + alpha^2, f(n) = b(n) = 0.  The "p" copies
+// (ffxp, cifxp6) equal these when periodic (:473-486, :667-676).
+int build_periodic_op(int kind, int dir, int n, double d, OpHost &op)
+{
+    if (n < 8) return X3D_EUNSUPPORTED;
+    op.kind = kind;
+    op.dir = dir;
+    op.n = n;
+    op.periodic = 1;
+    op.npaire = (kind == DER || kind == DER2 || kind == DERPV) ? 0 : 1;
+    rhs_scalars(kind, d, &op.alfa, &op.a, &op.b, &op.c, &op.d);
+    const double al = op.alfa;
+    std::vector<double> fb(n, 0.0), fc(n, 0.0), ff(n, 0.0);
+    ff[0] = al; ff[1] = al;
+    fc[0] = 2.0; fc[1] = 1.0;
+    fb[0] = al; fb[1] = al;
+    ff[n - 3] = al; ff[n - 2] = al; ff[n - 1] = 0.0;
+    fc[n - 3] = 1.0; fc[n - 2] = 1.0; fc[n - 1] = 1.0 + al * al;
+    fb[n - 3] = al; fb[n - 2] = al; fb[n - 1] = 0.0;
+    for (int i = 2; i < n - 3; ++i) {
+        ff[i] = al;
+        fc[i] = 1.0;
+        fb[i] = al;
+    }
+    op.f = ff;
+    lu_prepare(fb, fc, ff, op.s, op.w);
+    // init(): periodic = M^-1 (-1, 0, ..., 0, alfa)  (:260-264)
+    op.per.assign(n, 0.0);
+    op.per[0] = -1.0;
+    op.per[n - 1] = al;
+    lu_solve(op.per, op.f, op.s, op.w);
+    finish_op(op);
+    return X3D_OK;
+}
+
+// g = M^-T e_1 with M = L U, L unit lower bidiagonal (L(i,i-1) = s_i) and U
+// upper bidiagonal (U(i,i) = 1/w_i, U(i,i+1) = f_i).  Then y_0 = g . r for
+// y = M^-1 r, which lets the GPU sweep form the Sherman-Morrison scalar
+// after the forward pass and emit final values during the backward pass.
+void finish_op(OpHost &op)
+{
+    const int n = op.n;
+    std::vector<double> h(n), g(n);
+    h[0] = op.w[0];  // U^T h = e_1
+    for (int i = 1; i < n; ++i) h[i] = -op.f[i - 1] * h[i - 1] * op.w[i];
+    g[n - 1] = h[n - 1];  // L^T g = h
+    for (int i = n - 2; i >= 0; --i) g[i] = h[i] - op.s[i + 1] * g[i + 1];
+    op.g = g;
+    op.glen = n;
+    while (op.glen > 1 && g[op.glen - 1] == 0.0) --op.glen;
+    if (op.periodic && !op.per.empty())
+        op.den = 1.0 + op.per[0] - op.alfa * op.per[n - 1];
+    else
+        op.den = 1.0;
+}
+
+int upload_op(x3d_op_s *op)
+{
+    const OpHost &h = op->h;
+    const int n = h.n;
+    const size_t fbytes = (size_t)4 * n * sizeof(float);
+    const size_t fpad = (fbytes + 255) & ~(size_t)255;
+    const size_t dbytes = (size_t)5 * n * sizeof(double);
+    std::vector<unsigned char> host(fpad + dbytes, 0);
+    float *hf = reinterpret_cast<float *>(host.data());
+    double *hd = reinterpret_cast<double *>(host.data() + fpad);
+    for (int i = 0; i < n; ++i) {
+        const double fw = h.f[i] * h.w[i];
+        const double p = h.per.empty() ? 0.0 : h.per[i];
+        hf[0 * n + i] = (float)h.s[i];
+        hf[1 * n + i] = (float)h.w[i];
+        hf[2 * n + i] = (float)fw;
+        hf[3 * n + i] = (float)p;
+        hd[0 * n + i] = h.s[i];
+        hd[1 * n + i] = h.w[i];
+        hd[2 * n + i] = fw;
+        hd[3 * n + i] = p;
+        hd[4 * n + i] = h.g[i];
+    }
+    if (op->dmem) cudaFree(op->dmem);
+    op->dmem = nullptr;
+    if (cudaMalloc(&op->dmem, host.size()) != cudaSuccess) return X3D_ENOMEM;
+    if (cudaMemcpy(op->dmem, host.data(), host.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        return X3D_ECUDA;
+    const float *df = reinterpret_cast<const float *>(op->dmem);
+    const double *dd = reinterpret_cast<const double *>((const unsigned char *)op->dmem + fpad);
+    auto fill = [&](auto &lo, auto *base) {
+        lo.s = base + 0 * n;
+        lo.w = base + 1 * n;
+        lo.fw = base + 2 * n;
+        lo.p = base + 3 * n;
+        lo.g = dd + 4 * n;
+        lo.alfa = h.alfa;
+        lo.den = h.den;
+        lo.n = n;
+        lo.periodic = h.periodic;
+        lo.glen = h.glen;
+    };
+    fill(op->opf, df);
+    fill(op->opd, dd);
+    op->opf.a = (float)h.a; op->opf.b = (float)h.b; op->opf.c = (float)h.c; op->opf.d = (float)h.d;
+    op->opd.a = h.a; op->opd.b = h.b; op->opd.c = h.c; op->opd.d = h.d;
+    return X3D_OK;
+}
+
+void free_op(x3d_op_s *op)
+{
+    if (op && op->dmem) cudaFree(op->dmem);
+    if (op) op->dmem = nullptr;
+}
+
+}  // namespace x3d

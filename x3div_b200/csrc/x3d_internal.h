@@ -1,0 +1,128 @@
+// Internal declarations shared by the translation units of libx3d_b200.so.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/x3d_b200.h"
+
+namespace x3d {
+
+enum Kind { DER = 0, DER2 = 1, DERVP = 2, DERPV = 3, INTVP = 4, INTPV = 5, IDENT = 6 };
+enum Dir { DX = 0, DY = 1, DZ = 2 };
+
+// Device view of one operator, in the sweep precision T.  Built once per
+// operator from the FP64 precompute; the kernels read it from global memory
+// through the read-only cache (every lane of a warp reads the same element).
+template <typename T>
+struct LineOp {
+    const T *s;       // forward factors, s[0] = 0
+    const T *w;       // inverse pivots
+    const T *fw;      // f[i] * w[i]: backward step y_i = z_i w_i - fw_i y_{i+1}
+    const T *p;       // Sherman-Morrison vector (periodic operators)
+    const double *g;  // first row of M^-1, so y_0 = sum_i g_i r_i is known after the forward pass
+    T a, b, c, d;     // explicit RHS scalars
+    double alfa;      // Sherman-Morrison alpha
+    double den;       // 1 + p_0 - alfa p_{n-1}
+    int n;
+    int periodic;
+    int glen;         // g_i == 0 (in FP64) for i >= glen
+};
+
+// Host-side operator: FP64 contents of x3doperator1d plus the RHS scalars.
+struct OpHost {
+    int kind = 0, dir = 0, n = 0, npaire = 0, periodic = 1;
+    double alfa = 0, a = 0, b = 0, c = 0, d = 0;
+    std::vector<double> f, s, w, per, g;
+    double den = 1.0;
+    int glen = 0;
+};
+
+}  // namespace x3d
+
+struct x3d_op_s {
+    x3d::OpHost h;
+    // device copies: one allocation holding float s,w,fw,p | double s,w,fw,p | double g
+    void *dmem = nullptr;
+    x3d::LineOp<float> opf{};
+    x3d::LineOp<double> opd{};
+    bool builtin = false;
+};
+
+struct x3d_ctx_s {
+    int nx = 0, ny = 0, nz = 0;
+    double xlx = 1, yly = 1, zlz = 1;
+    double dx = 1, dy = 1, dz = 1;
+    int precision = X3D_F64;
+    int device = 0;
+    int num_sms = 148;
+    size_t smem_optin = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    int *d_err = nullptr;  // device error flag written by bounded waits
+    std::string last_error;
+    x3d_op_s *builtin[X3D_OP_COUNT] = {};
+    // Poisson: cuFFT plans, spectrum and the 1-D modified-wavenumber tables
+    cufftHandle plan_d2z = 0, plan_z2d = 0;
+    bool plans_ready = false;
+    void *spectrum = nullptr;  // complex double, nz * ny * (nx/2+1)
+    double *d_k2x = nullptr, *d_tx = nullptr, *d_k2y = nullptr, *d_ty = nullptr, *d_k2z = nullptr,
+           *d_tz = nullptr;
+    // scratch fields owned by the context (sized nx*ny*nz elements)
+    std::vector<void *> scratch;
+    size_t scratch_elem_bytes = 0;
+    // host-pointer staging buffers
+    std::vector<std::pair<void *, size_t>> staging;
+    double *d_red = nullptr;  // small reduction buffer
+    size_t elem() const { return precision == X3D_F32 ? 4 : 8; }
+    size_t npts() const { return (size_t)nx * ny * nz; }
+};
+
+namespace x3d {
+
+// ---- coefficient precompute (coeffs.cpp) -------------------------------
+void rhs_scalars(int kind, double d, double *alfa, double *a, double *b, double *c, double *dd);
+int build_periodic_op(int kind, int dir, int n, double d, OpHost &op);
+void finish_op(OpHost &op);  // computes g, den, glen from f, s, w, per
+int upload_op(x3d_op_s *op);
+void free_op(x3d_op_s *op);
+
+// ---- line solves (linesolve.cu) -----------------------------------------
+// Applies op (kind given by op.kind unless kind_override >= 0) along dir to
+// the (nx,ny,nz) field in -> out (may alias for kind IDENT).
+int launch_linesolve(x3d_ctx_s *ctx, const x3d_op_s *op, int kind, int dir, const void *in,
+                     void *out, int nx, int ny, int nz, bool fp32);
+
+// ---- elementwise / reductions / transposes (fields.cu) ------------------
+int launch_copy(x3d_ctx_s *ctx, void *dst, const void *src, size_t bytes);
+int launch_axpy3(x3d_ctx_s *ctx, bool fp32, void *u, void *v, void *w, const void *du,
+                 const void *dv, const void *dw, double alpha, size_t n);  // u = alpha*du + u
+int launch_sub3(x3d_ctx_s *ctx, bool fp32, void *u, void *v, void *w, const void *a,
+                const void *b, const void *c, size_t n);                   // u -= a
+int launch_mul(x3d_ctx_s *ctx, bool fp32, void *out, const void *a, const void *b, size_t n);
+int launch_fma_acc(x3d_ctx_s *ctx, bool fp32, void *out, const void *base, const void *a,
+                   const void *b, size_t n);  // out = base + a*b
+int launch_add(x3d_ctx_s *ctx, bool fp32, void *out, const void *a, const void *b, size_t n);
+int launch_convert(x3d_ctx_s *ctx, void *dst, bool dst_fp32, const void *src, bool src_fp32,
+                   size_t n);
+int launch_vel(x3d_ctx_s *ctx, bool fp32, void *u, void *v, void *w);
+int reduce_test_rms(x3d_ctx_s *ctx, bool fp32, int which, const void *du, double *rms);
+int reduce_absmax_mean(x3d_ctx_s *ctx, const double *p, size_t n, double *out);
+
+// ---- Poisson (poisson.cu) ------------------------------------------------
+int poisson_setup(x3d_ctx_s *ctx);
+int poisson_solve(x3d_ctx_s *ctx, double *rhs);
+void poisson_free(x3d_ctx_s *ctx);
+
+// ---- helpers (capi.cpp) --------------------------------------------------
+int set_error(x3d_ctx_s *ctx, int code, const std::string &msg);
+int cuda_check(x3d_ctx_s *ctx, cudaError_t e, const char *what);
+void *ctx_scratch(x3d_ctx_s *ctx, int idx);  // scratch field idx (elem = ctx precision, or 8 bytes)
+
+}  // namespace x3d
