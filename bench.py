@@ -57,6 +57,7 @@ def parse():
     ap.add_argument("--no-euler", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     return ap.parse_args()
 
 
@@ -219,61 +220,77 @@ def run_reference(args, world, rank):
 
 
 # --------------------------------------------------------------------------
-def sweep_items(ctx, fields, outs):
-    items = []
+def sweep_groups(ctx, fields, outs, fused):
+    """The 54 applications of one step, as (direction, [(op, in, out), ...])
+    groups: with fused=True the six operator families of one field and one
+    direction form one group (one multi-output launch), else one group per
+    application."""
+    groups = []
     k = 0
     for f in fields:
-        for kind, names in KINDS:
-            for d, name in enumerate(names):
-                items.append((d, ctx.op(name), f, outs[k % len(outs)]))
+        for d in range(3):
+            g = []
+            for kind, names in KINDS:
+                g.append((ctx.op(names[d]), f, outs[k % len(outs)]))
                 k += 1
-    return items
+            if fused:
+                groups.append((d, g))
+            else:
+                groups.extend((d, [it]) for it in g)
+    return groups
 
 
-def timed_sweep(ctx, torch, fields, outs, steps, warmup, world, per_launch=True):
+def timed_sweep(ctx, torch, fields, outs, steps, warmup, world, fused=True, per_launch=True):
     from x3div_b200._capi import Work
-    items = sweep_items(ctx, fields, outs)
+    groups = sweep_groups(ctx, fields, outs, fused)
     stream = torch.cuda.current_stream()
     L = ctx.L
     h = ctx.handle
+    arrs = []
+    for d, g in groups:
+        arr = (Work * len(g))()
+        for k, (op, src, dst) in enumerate(g):
+            arr[k].op, arr[k].in_, arr[k].out = op.handle, src.data_ptr(), dst.data_ptr()
+        arrs.append((d, arr, len(g)))
 
-    def apply(op, src, dst):
-        arr = (Work * 1)()
-        arr[0].op, arr[0].in_, arr[0].out = op.handle, src.data_ptr(), dst.data_ptr()
-        rc = L.x3d_apply_batch(h, arr, 1)
+    def run(arr, n):
+        rc = L.x3d_apply_batch(h, arr, n)
         if rc:
             ctx._check(rc)
 
     for _ in range(warmup):
-        for d, op, src, dst in items:
-            apply(op, src, dst)
+        for d, arr, n in arrs:
+            run(arr, n)
     ctx.sync()
     torch.cuda.synchronize()
     barrier(world)
     torch.cuda.synchronize()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(steps * len(items))] if per_launch else []
+          for _ in range(steps * len(arrs))] if per_launch else []
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c0 = ctx.launch_count()
     t0.record(stream)
     k = 0
     for _ in range(steps):
-        for d, op, src, dst in items:
+        for d, arr, n in arrs:
             if per_launch:
                 ev[k][0].record(stream)
-            apply(op, src, dst)
+            run(arr, n)
             if per_launch:
                 ev[k][1].record(stream)
             k += 1
     t1.record(stream)
     torch.cuda.synchronize()
     ctx.sync()
+    launches = ctx.launch_count() - c0
     ms = t0.elapsed_time(t1)
     fam = {}
-    for k, (d, op, src, dst) in enumerate(items * steps):
-        if per_launch:
+    if per_launch:
+        for k, (d, arr, n) in enumerate(arrs * steps):
             fam.setdefault(d, []).append(ev[k][0].elapsed_time(ev[k][1]))
     barrier(world)
-    return ms, fam, len(items)
+    group = len(groups[0][1])
+    return ms, fam, sum(len(g) for _, g in groups), launches, group
 
 
 def run_b200(args, world, rank, local):
@@ -289,32 +306,45 @@ def run_b200(args, world, rank, local):
     # ---- FP32-mixed sweep (headline) ---------------------------------------
     ctx = Context(n, n, n, lengths=(2 * np.pi,) * 3, precision="f32", device=local,
                   stream=torch.cuda.current_stream())
+    if not args.no_autotune:
+        ctx.autotune(6)
     host = [tg_noise(n, s + 3 * rank) for s in range(3)]
     fields = [torch.from_numpy(h).to(device="cuda", dtype=torch.float32) for h in host]
-    outs = [torch.empty_like(fields[0]) for _ in range(6)]
+    outs = [torch.empty_like(fields[0]) for _ in range(18)]
     clocks.start()
-    ms, fam, nitems = timed_sweep(ctx, torch, fields, outs, args.steps, args.warmup, world)
+    ms, fam, nitems, launches, group = timed_sweep(ctx, torch, fields, outs, args.steps,
+                                                   args.warmup, world, fused=True)
     ms = max_over_ranks(ms, world)
     pts_step = nitems * npts
     value = world * pts_step * args.steps / (ms * 1e-3) / 1e9
     es = 4
+    per_launch_bytes = (1 + group) * npts * es  # one read, one write per operator
     fam_stats = {}
     for d, ts in fam.items():
         avg = sum(ts) / len(ts)
         fam_stats[FAMILY[d]] = {"launches": len(ts), "avg_ms": round(avg, 4),
-                                "gbs": round(2 * npts * es / (avg * 1e-3) / 1e9, 1),
-                                "share": round(sum(ts) / sum(sum(v) for v in fam.values()), 3)}
+                                "gbs": round(per_launch_bytes / (avg * 1e-3) / 1e9, 1),
+                                "share": round(sum(ts) / sum(sum(v) for v in fam.values()), 3),
+                                "config": ctx.autotune_choice(d, group)}
     dom_d = max(fam, key=lambda d: sum(fam[d]))
     dom = fam_stats[FAMILY[dom_d]]
-    traffic = profiled_traffic().get(FAMILY[dom_d] + ":f32")
-    traffic_bytes = None
-    if traffic:
-        traffic_bytes = traffic["bytes_per_point"] * npts
+    traffic = profiled_traffic().get(f"{FAMILY[dom_d]}:f32:group{group}")
+    traffic_bytes = traffic["bytes_per_point"] * npts if traffic else None
     roofline = {"bound": "hbm", "achieved": dom["gbs"], "peak": peak, "unit": "GB/s",
                 "frac": round(dom["gbs"] / peak, 3), "traffic": traffic_bytes,
-                "kernel": FAMILY[dom_d], "algorithmic_bytes_per_launch": 2 * npts * es,
-                "peak_source": peak_kind}
-    out.update(value=value, ms=ms, fam=fam_stats, roofline=roofline, launches=args.steps * nitems)
+                "kernel": FAMILY[dom_d] + f" ({group} operators per launch)",
+                "algorithmic_bytes_per_launch": per_launch_bytes, "peak_source": peak_kind}
+    out.update(value=value, ms=ms, fam=fam_stats, roofline=roofline, launches=launches)
+    # the same 54 applications one operator per launch
+    ms1, fam1, _, launches1, _ = timed_sweep(ctx, torch, fields, outs, args.steps, args.warmup,
+                                             world, fused=False)
+    ms1 = max_over_ranks(ms1, world)
+    out["unfused"] = {"value": round(world * pts_step * args.steps / (ms1 * 1e-3) / 1e9, 2),
+                      "ms_per_step": round(ms1 / args.steps, 3), "launches": launches1,
+                      "kernels": {FAMILY[d]: {"avg_ms": round(sum(ts) / len(ts), 4),
+                                              "gbs": round(2 * npts * es / (sum(ts) / len(ts) * 1e-3) / 1e9, 1),
+                                              "config": ctx.autotune_choice(d, 1)}
+                                  for d, ts in fam1.items()}}
 
     # ---- e2e: host buffers through x3d_apply_batch ---------------------------
     if not args.no_e2e:
@@ -377,16 +407,24 @@ def run_b200(args, world, rank, local):
     if not args.no_fp64:
         ctx64 = Context(n, n, n, lengths=(2 * np.pi,) * 3, precision="f64", device=local,
                         stream=torch.cuda.current_stream())
+        if not args.no_autotune:
+            ctx64.autotune(6)
         fields = [torch.from_numpy(h).to(device="cuda") for h in host]
-        outs = [torch.empty_like(fields[0]) for _ in range(6)]
-        ms64, fam64, _ = timed_sweep(ctx64, torch, fields, outs, args.steps, args.warmup, world,
-                                     per_launch=True)
+        outs = [torch.empty_like(fields[0]) for _ in range(18)]
+        ms64, fam64, _, l64, g64 = timed_sweep(ctx64, torch, fields, outs, args.steps, args.warmup,
+                                               world, fused=True)
         ms64 = max_over_ranks(ms64, world)
         f64 = {"value": round(world * pts_step * args.steps / (ms64 * 1e-3) / 1e9, 2),
-               "ms_per_step": round(ms64 / args.steps, 3)}
+               "ms_per_step": round(ms64 / args.steps, 3), "launches": l64}
         f64["kernels"] = {FAMILY[d]: {"avg_ms": round(sum(ts) / len(ts), 4),
-                                      "gbs": round(2 * npts * 8 / (sum(ts) / len(ts) * 1e-3) / 1e9, 1)}
+                                      "gbs": round((1 + g64) * npts * 8 / (sum(ts) / len(ts) * 1e-3) / 1e9, 1),
+                                      "config": ctx64.autotune_choice(d, g64)}
                           for d, ts in fam64.items()}
+        ms64u, _, _, l64u, _ = timed_sweep(ctx64, torch, fields, outs, args.steps, args.warmup,
+                                           world, fused=False, per_launch=False)
+        ms64u = max_over_ranks(ms64u, world)
+        f64["unfused"] = {"value": round(world * pts_step * args.steps / (ms64u * 1e-3) / 1e9, 2),
+                          "ms_per_step": round(ms64u / args.steps, 3), "launches": l64u}
         out["fp64"] = f64
         del fields, outs
         if not args.no_euler:
@@ -426,12 +464,14 @@ def main():
             "data": "synthetic",
             "config": {"workload": f"periodic compact derivative sweep, {n}^3 per GPU, 3 fields x "
                                    "6 operator families x 3 directions = 54 line-solve applications "
-                                   "per step", "grid": [n, n, n], "fields": "Taylor-Green + seeded N(0, (1e-3)^2) noise",
+                                   "per step, the 6 families of one field and direction fused into "
+                                   "one launch", "grid": [n, n, n], "fields": "Taylor-Green + seeded N(0, (1e-3)^2) noise",
                        "l2": "inputs (0.5 GB per field) larger than L2; no flush",
                        "parallelism": f"{world} independent box(es), one per GPU"},
             "gpu_launches": res["launches"],
             "roofline": res["roofline"],
             "kernels": res["fam"],
+            "unfused": res["unfused"],
             "cpu_baseline": {"value": round(cpu_val, 4), "unit": "Gpts/s", "cores": cpu_threads(),
                              "kind": "port",
                              "sample": f"oracle (FP64 C, OpenMP) derx+interyvp+derzz on one {sample_n}^3 field"},

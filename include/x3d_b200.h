@@ -103,14 +103,19 @@ int x3d_ctx_create(x3d_ctx *ctx, int nx, int ny, int nz, double xlx, double yly,
                    int precision, int device);
 /* finalise_xcompact3d's device-side part (src/x3d_tools.f90:212-248). */
 int x3d_ctx_destroy(x3d_ctx ctx);
-/* Run the context's work on a caller-owned stream (cudaStream_t); NULL
- * returns to the context's own stream. */
+/* Run the context's work on a caller-owned stream (a cudaStream_t; NULL is
+ * the legacy default stream).  A new context uses its own non-blocking
+ * stream, which x3d_ctx_get_stream returns. */
 int x3d_ctx_set_stream(x3d_ctx ctx, void *stream);
+int x3d_ctx_get_stream(x3d_ctx ctx, void **stream);
 /* Wait for the context's stream; returns X3D_ETIMEOUT if a kernel recorded a
  * bounded-wait failure since the last call, else a CUDA error or X3D_OK. */
 int x3d_ctx_sync(x3d_ctx ctx);
 /* Text of the last error recorded on this context (never NULL). */
 const char *x3d_ctx_last_error(x3d_ctx ctx);
+/* Number of this library's kernels launched on the context so far (library
+ * kernels such as cuFFT's are not counted). */
+int x3d_ctx_launch_count(x3d_ctx ctx, unsigned long long *count);
 /* Geometry query: dims[3], lengths[3], spacing[3] (any may be NULL). */
 int x3d_ctx_geometry(x3d_ctx ctx, int *dims, double *lengths, double *spacing, int *precision);
 
@@ -184,6 +189,22 @@ typedef struct {
  * memory.  No reference counterpart: it replaces a sequence of der* and
  * staggered calls (src/transeq.f90, src/navier.f90) by one call. */
 int x3d_apply_batch(x3d_ctx ctx, const x3d_work *items, int count);
+
+/* Times every kernel configuration (lines per CTA, chunk length, or one
+ * thread per line) for each direction and for groups of 1, 2, 3 and 6
+ * operators sharing an input (up to max_group), on the context grid, and
+ * keeps the fastest for later calls.  Synchronous; uses context scratch
+ * fields; not callable during stream capture.  Without it a fixed default
+ * configuration is used.  No reference counterpart. */
+int x3d_autotune(x3d_ctx ctx, int max_group);
+/* Force kernel configuration cfg (0..3 chunked, 4 one thread per line) for
+ * every later call and forget tuned choices; -1 restores the default.  A
+ * configuration that cannot handle a call (alignment, shared memory) still
+ * falls back to one that can.  No reference counterpart. */
+int x3d_ctx_set_kernel(x3d_ctx ctx, int cfg);
+/* The configuration chosen for (direction, group size): *cfg = -1 when not
+ * tuned, 0..3 chunked variants, 4 one thread per line. */
+int x3d_autotune_choice(x3d_ctx ctx, int dir, int group, int *cfg);
 
 /* ---- batched Thomas line solves: module thomas (src/thomas.f90:15-28) --- */
 

@@ -178,3 +178,70 @@ def test_bad_calls_raise(torch_cuda, contexts):
     with pytest.raises(X3DError):   # length mismatch
         ctx.derx(t, u, ctx.op("derx"), 8, 32, 16)
     ctx.sync()
+
+
+@pytest.mark.parametrize("cfg", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("shape", [(8, 8, 8), (64, 48, 40), (100, 36, 12), (96, 20, 200)])
+def test_every_kernel_configuration(oracle, torch_cuda, contexts, cfg, prec, shape):
+    """Each kernel configuration (chunked variants 0-3, one thread per line 4)
+    reproduces the oracle; configurations that cannot take a shape fall back."""
+    torch = torch_cuda
+    from x3div_b200 import to_device, to_host
+    ctx = contexts(shape, prec)
+    ctx.set_kernel(cfg)
+    dt = torch.float64 if prec == "f64" else torch.float32
+    u_d = to_device(seeded_field(shape, seed=cfg + 17, noise=1e-2), dt)
+    used = to_host(u_d).astype(np.float64)
+    d = {X: ctx.dx, Y: ctx.dy, Z: ctx.dz}
+    tol = 1e-12 if prec == "f64" else 1e-5
+    try:
+        for routine, opname, kind, direction, style in ROUTINES:
+            t_d = torch.empty_like(u_d)
+            call(ctx, routine, style, t_d, u_d, ctx.op(opname), shape)
+            ctx.sync()
+            err = rel_err(to_host(t_d), oracle.apply(kind, direction, used, d[direction]))
+            assert err < tol, (routine, cfg, err)
+    finally:
+        ctx.set_kernel(-1)
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("shape", [(64, 64, 64), (40, 36, 24)])
+def test_grouped_batch_matches_single_calls(oracle, torch_cuda, contexts, prec, shape):
+    """x3d_apply_batch: the six operator families on one input along one
+    direction run as one multi-output launch and match the oracle."""
+    torch = torch_cuda
+    from x3div_b200 import to_device, to_host
+    ctx = contexts(shape, prec)
+    dt = torch.float64 if prec == "f64" else torch.float32
+    u_d = to_device(seeded_field(shape, seed=5, noise=1e-2), dt)
+    used = to_host(u_d).astype(np.float64)
+    tol = 1e-12 if prec == "f64" else 1e-5
+    kinds = ["der", "der2", "dervp", "derpv", "intvp", "intpv"]
+    names = [("derx", "derxx", "derxvp", "derxpv", "intxvp", "intxpv"),
+             ("dery", "deryy", "deryvp", "derypv", "intyvp", "intypv"),
+             ("derz", "derzz", "derzvp", "derzpv", "intzvp", "intzpv")]
+    d = (ctx.dx, ctx.dy, ctx.dz)
+    for cfg in (0, 1, 2, 3, 4):
+        ctx.set_kernel(cfg)
+        outs = [[torch.empty_like(u_d) for _ in range(6)] for _ in range(3)]
+        items = [(ctx.op(names[di][k]), u_d, outs[di][k]) for di in range(3) for k in range(6)]
+        ctx.apply_batch(items)
+        ctx.sync()
+        for di in range(3):
+            for k, kind in enumerate(kinds):
+                err = rel_err(to_host(outs[di][k]), oracle.apply(kind, di, used, d[di]))
+                assert err < tol, (cfg, di, kind, err)
+    ctx.set_kernel(-1)
+
+
+def test_autotune_records_choices(torch_cuda, contexts):
+    shape = (64, 32, 48)
+    ctx = contexts(shape, "f32")
+    ctx.autotune(max_group=3)
+    for direction in range(3):
+        for g in (1, 2, 3):
+            assert 0 <= ctx.autotune_choice(direction, g) <= 4
+    assert ctx.autotune_choice(0, 6) == -1
+    ctx.set_kernel(-1)

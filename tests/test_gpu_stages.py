@@ -40,7 +40,9 @@ def test_divergence_gradp_momentum(oracle, torch_cuda, shape, prec):
     from x3div_b200 import to_device, to_host
     ctx = ctx_for(shape, prec)
     dt = torch.float64 if prec == "f64" else torch.float32
-    tol = 1e-12 if prec == "f64" else 1e-5
+    # FP32: each interpolation alone is ~6e-6 (cond ~ 99 for alpha = 0.49,
+    # times FP32 rounding of its LU factors); a stage chains three operators.
+    tol = 1e-12 if prec == "f64" else 1e-4
     u, v, w = fields(shape)
     ud, vd, wd = (to_device(a, dt) for a in (u, v, w))
     uh, vh, wh = (to_host(a).astype(np.float64) for a in (ud, vd, wd))
@@ -66,7 +68,7 @@ def test_divergence_gradp_momentum(oracle, torch_cuda, shape, prec):
     ctx.sync()
     ref_du = oracle.momentum_rhs(uh, vh, wh, dx, dy, dz)
     for got, ref in zip(du, ref_du):
-        assert rel_err(to_host(got), ref) < tol * 10
+        assert rel_err(to_host(got), ref) < tol
     ctx.close()
 
 
@@ -89,7 +91,7 @@ def test_euler_steps_match_oracle(oracle, torch_cuda, prec):
         ctx.euler_step(*U, *du, pp3, *pg, 1e-3)
         oracle.euler_step(*ref, 1e-3, lengths=LEN)
     ctx.sync()
-    tol = 1e-11 if prec == "f64" else 2e-5
+    tol = 1e-11 if prec == "f64" else 1e-4
     for got, r in zip(U, ref):
         assert rel_err(to_host(got), r) < tol
     if prec == "f64":

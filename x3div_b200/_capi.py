@@ -32,6 +32,8 @@ SIGNATURES = {
     "x3d_ctx_create": [ctypes.POINTER(_vp), _i, _i, _i, _d, _d, _d, _i, _i],
     "x3d_ctx_destroy": [_vp],
     "x3d_ctx_set_stream": [_vp, _vp],
+    "x3d_ctx_get_stream": [_vp, ctypes.POINTER(_vp)],
+    "x3d_ctx_launch_count": [_vp, ctypes.POINTER(ctypes.c_ulonglong)],
     "x3d_ctx_sync": [_vp],
     "x3d_ctx_last_error": [_vp],
     "x3d_ctx_geometry": [_vp, _ip, _dp, _dp, _ip],
@@ -58,6 +60,9 @@ SIGNATURES = {
     "x3d_derzpv": [_vp, _vp, _vp, _vp, _i, _i, _i, _i],
     "x3d_interzpv": [_vp, _vp, _vp, _vp, _i, _i, _i, _i],
     "x3d_apply_batch": [_vp, _vp, _i],
+    "x3d_autotune": [_vp, _i],
+    "x3d_ctx_set_kernel": [_vp, _i],
+    "x3d_autotune_choice": [_vp, _i, _i, _ip],
     "x3d_xthomas": [_vp, _vp, _vp, _vp, _vp, _vp, _d, _i, _i, _i],
     "x3d_ythomas": [_vp, _vp, _vp, _vp, _vp, _vp, _d, _i, _i, _i],
     "x3d_zthomas": [_vp, _vp, _vp, _vp, _vp, _vp, _d, _i, _i, _i],

@@ -24,6 +24,19 @@ from . import _capi
 from ._capi import KIND, OP_NAMES, X3D_F32, X3D_F64
 
 
+def _torch_current_stream():
+    """torch's current CUDA stream when torch is loaded with a device, so that
+    library work orders with torch's own work on the same tensors."""
+    import sys
+    torch = sys.modules.get("torch")
+    try:
+        if torch is not None and torch.cuda.is_available():
+            return torch.cuda.current_stream()
+    except Exception:
+        return None
+    return None
+
+
 class X3DError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"x3d status {code}: {msg}")
@@ -87,6 +100,8 @@ class Context:
             raise X3DError(rc, "x3d_ctx_create failed")
         self.handle = h.value
         self.dx, self.dy, self.dz = (l / n for l, n in zip(self.lengths, (nx, ny, nz)))
+        if stream is None:
+            stream = _torch_current_stream()
         if stream is not None:
             self.set_stream(stream)
         self._ops = {}
@@ -102,9 +117,21 @@ class Context:
             raise X3DError(rc, msg.decode(errors="replace"))
 
     def set_stream(self, stream):
-        """Run on a caller stream: a torch.cuda.Stream or a raw cudaStream_t."""
+        """Run on a caller stream: a torch.cuda.Stream or a raw cudaStream_t
+        (0 is the legacy default stream)."""
         raw = getattr(stream, "cuda_stream", stream)
         self._check(self.L.x3d_ctx_set_stream(self.handle, raw))
+
+    def launch_count(self) -> int:
+        """Kernels of this library launched on the context so far."""
+        out = ctypes.c_ulonglong()
+        self._check(self.L.x3d_ctx_launch_count(self.handle, ctypes.byref(out)))
+        return out.value
+
+    def get_stream(self) -> int:
+        out = ctypes.c_void_p()
+        self._check(self.L.x3d_ctx_get_stream(self.handle, ctypes.byref(out)))
+        return out.value or 0
 
     def sync(self):
         self._check(self.L.x3d_ctx_sync(self.handle))
@@ -207,6 +234,19 @@ class Context:
         for k, (op, src, dst) in enumerate(items):
             arr[k].op, arr[k].in_, arr[k].out = op.handle, _ptr(src), _ptr(dst)
         self._check(self.L.x3d_apply_batch(self.handle, arr, len(items)))
+
+    def autotune(self, max_group=6):
+        """Time the kernel configurations on this grid and keep the fastest."""
+        self._check(self.L.x3d_autotune(self.handle, int(max_group)))
+
+    def set_kernel(self, cfg):
+        """Force a kernel configuration (0..3 chunked, 4 thread per line, -1 default)."""
+        self._check(self.L.x3d_ctx_set_kernel(self.handle, int(cfg)))
+
+    def autotune_choice(self, direction, group):
+        out = ctypes.c_int()
+        self._check(self.L.x3d_autotune_choice(self.handle, int(direction), int(group), ctypes.byref(out)))
+        return out.value
 
     # -- thomas -----------------------------------------------------------
     def _thomas(self, fn, tt, ff, fs, fw, perio, alfa, nx, ny, nz):

@@ -293,7 +293,21 @@ int x3d_ctx_destroy(x3d_ctx ctx)
 int x3d_ctx_set_stream(x3d_ctx ctx, void *stream)
 {
     if (!ctx) return X3D_EINVAL;
-    ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+    ctx->stream = static_cast<cudaStream_t>(stream);
+    return X3D_OK;
+}
+
+int x3d_ctx_launch_count(x3d_ctx ctx, unsigned long long *count)
+{
+    if (!ctx || !count) return X3D_EINVAL;
+    *count = ctx->launches;
+    return X3D_OK;
+}
+
+int x3d_ctx_get_stream(x3d_ctx ctx, void **stream)
+{
+    if (!ctx || !stream) return X3D_EINVAL;
+    *stream = ctx->stream;
     return X3D_OK;
 }
 
@@ -479,11 +493,79 @@ int x3d_apply_batch(x3d_ctx ctx, const x3d_work *items, int count)
     for (int i = 0; i < count; ++i) din[i] = sg.in(items[i].in, bytes);
     for (int i = 0; i < count; ++i) dout[i] = sg.out(items[i].out, bytes);
     if (sg.status()) return sg.status();
+    // Items that read the same input along the same direction share one
+    // staged read: up to six of them go into one multi-output launch.
+    std::vector<char> done(count, 0);
     for (int i = 0; i < count && !rc; ++i) {
-        const x3d_op_s *op = items[i].op;
-        rc = launch_linesolve(ctx, op, op->h.kind, op->h.dir, din[i], dout[i], ctx->nx, ctx->ny, ctx->nz, fp32(ctx));
+        if (done[i]) continue;
+        const x3d_op_s *gops[6];
+        int gkind[6];
+        void *gout[6];
+        int k = 0;
+        for (int j = i; j < count && k < 6; ++j) {
+            if (done[j] || din[j] != din[i] || items[j].op->h.dir != items[i].op->h.dir) continue;
+            gops[k] = items[j].op;
+            gkind[k] = items[j].op->h.kind;
+            gout[k] = dout[j];
+            ++k;
+            done[j] = 1;
+        }
+        rc = launch_group(ctx, items[i].op->h.dir, din[i], gops, gkind, gout, k, ctx->nx, ctx->ny,
+                          ctx->nz, fp32(ctx));
     }
     return sg.finish(rc);
+}
+
+int x3d_autotune(x3d_ctx ctx, int max_group)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (max_group < 1 || max_group > 6) return set_error(ctx, X3D_EINVAL, "max_group must be 1..6");
+    if (cudaStreamCaptureStatus st; cudaStreamIsCapturing(ctx->stream, &st) == cudaSuccess &&
+                                    st != cudaStreamCaptureStatusNone)
+        return set_error(ctx, X3D_EINVAL, "cannot autotune during stream capture");
+    void *buf[7];
+    for (int i = 0; i < 7; ++i)
+        if (!(buf[i] = ctx_scratch(ctx, i))) return set_error(ctx, X3D_ENOMEM, "scratch allocation failed");
+    rc = cuda_check(ctx, cudaMemsetAsync(buf[0], 0, ctx->npts() * ctx->elem(), ctx->stream), "memset");
+    const int kinds[6] = {DER, DER2, DERVP, DERPV, INTVP, INTPV};
+    const int sizes[4] = {1, 2, 3, 6};
+    for (int dir = 0; dir < 3 && !rc; ++dir)
+        for (int g : sizes) {
+            if (g > max_group || rc) continue;
+            const x3d_op_s *ops[6];
+            void *outs[6];
+            for (int k = 0; k < g; ++k) {
+                const int idx = [&] {
+                    for (int w = 0; w < X3D_OP_COUNT; ++w)
+                        if (ctx->builtin[w]->h.kind == kinds[k] && ctx->builtin[w]->h.dir == dir) return w;
+                    return 0;
+                }();
+                ops[k] = ctx->builtin[idx];
+                outs[k] = buf[1 + k];
+            }
+            rc = autotune_group(ctx, dir, buf[0], ops, kinds, outs, g, fp32(ctx), 3, nullptr);
+        }
+    return rc;
+}
+
+int x3d_ctx_set_kernel(x3d_ctx ctx, int cfg)
+{
+    if (!ctx || cfg < -1 || cfg > 4) return X3D_EINVAL;
+    ctx->tuned.clear();
+    ctx->default_cfg = cfg < 0 ? 0 : cfg;
+    return X3D_OK;
+}
+
+int x3d_autotune_choice(x3d_ctx ctx, int dir, int group, int *cfg)
+{
+    if (!ctx || !cfg) return X3D_EINVAL;
+    const std::string key = std::to_string(dir) + ":" + std::to_string(ctx->nx) + "x" +
+                            std::to_string(ctx->ny) + "x" + std::to_string(ctx->nz) + ":" +
+                            (fp32(ctx) ? "f32" : "f64") + ":" + std::to_string(group);
+    const auto it = ctx->tuned.find(key);
+    *cfg = it == ctx->tuned.end() ? -1 : it->second;
+    return X3D_OK;
 }
 
 // ---- Thomas ------------------------------------------------------------------------

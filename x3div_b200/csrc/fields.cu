@@ -148,6 +148,7 @@ __global__ void k_absmax_sum(const double *p, size_t n, double *out)
 #define X3D_LAUNCH(kern, n, ...)                                                          \
     do {                                                                                  \
         const int bs_ = 256;                                                              \
+        ++ctx->launches;                                                                  \
         kern<<<grid_for(ctx, (n), bs_), bs_, 0, ctx->stream>>>(__VA_ARGS__);              \
         return cuda_check(ctx, cudaGetLastError(), #kern);                                \
     } while (0)
@@ -224,6 +225,7 @@ int reduce_test_rms(x3d_ctx_s *ctx, bool fp32, int which, const void *du, double
     int rc = cuda_check(ctx, cudaMemsetAsync(ctx->d_red, 0, 2 * sizeof(double), ctx->stream), "memset");
     if (rc) return rc;
     const int bs = 256;
+    ++ctx->launches;
     if (fp32)
         k_test_sq<float><<<grid_for(ctx, n, bs), bs, 0, ctx->stream>>>(
             (const float *)du, which, ctx->nx, ctx->ny, ctx->nz, ctx->xlx, ctx->yly, ctx->zlz, ctx->d_red);
@@ -246,6 +248,7 @@ int reduce_absmax_mean(x3d_ctx_s *ctx, const double *p, size_t n, double *out)
     int rc = cuda_check(ctx, cudaMemsetAsync(ctx->d_red, 0, 2 * sizeof(double), ctx->stream), "memset");
     if (rc) return rc;
     const int bs = 256;
+    ++ctx->launches;
     k_absmax_sum<<<grid_for(ctx, n, bs), bs, 0, ctx->stream>>>(p, n, ctx->d_red);
     rc = cuda_check(ctx, cudaGetLastError(), "k_absmax_sum");
     if (rc) return rc;

@@ -34,6 +34,7 @@
 #include <algorithm>
 #include <cstdio>
 
+#include "linesolve_chunk.h"
 #include "ptx.cuh"
 #include "x3d_internal.h"
 
@@ -375,10 +376,11 @@ static int run_kind(x3d_ctx_s *ctx, const x3d_op_s *op, int dir, const T *in, T 
         int pitch = n + V;  // odd number of 16-byte granules per row
         while (((size_t)pitch * es / 16) % 2 == 0) pitch += V;
         const size_t smem = (size_t)W * pitch * es;
-        if (ptr_ok && n % V == 0 && smem <= ctx->smem_optin && in != out) {
+        if (ptr_ok && n % V == 0 && smem + 1024 <= ctx->smem_optin && in != out) {
             auto kern = ls_x_bulk<T, KIND, W>;
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             const long grid = (nlines + W - 1) / W;
+            ++ctx->launches;
             kern<<<(unsigned)grid, W, smem, st>>>(in, out, lo, nlines, pitch, ctx->d_err);
             return cuda_check(ctx, cudaGetLastError(), "ls_x_bulk launch");
         }
@@ -387,7 +389,7 @@ static int run_kind(x3d_ctx_s *ctx, const x3d_op_s *op, int dir, const T *in, T 
         const int box_n = (n + nb - 1) / nb;
         const size_t smem = (size_t)nb * box_n * W * es;
         auto enc = encode_fn();
-        if (enc && ptr_ok && ((size_t)nx * es) % 16 == 0 && smem <= ctx->smem_optin) {
+        if (enc && ptr_ok && ((size_t)nx * es) % 16 == 0 && smem + 1024 <= ctx->smem_optin) {
             CUtensorMap tmap;
             cuuint64_t gdim[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
             cuuint64_t gstride[2] = {(cuuint64_t)nx * es, (cuuint64_t)nx * ny * es};
@@ -403,6 +405,7 @@ static int run_kind(x3d_ctx_s *ctx, const x3d_op_s *op, int dir, const T *in, T 
                 cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
                 const long tiles_x = (nx + W - 1) / W;
                 const long grid = tiles_x * (dir == DY ? nz : ny);
+                ++ctx->launches;
                 kern<<<(unsigned)grid, W, smem, st>>>(tmap, out, lo, nx, ny, dir, box_n, nb, ctx->d_err);
                 return cuda_check(ctx, cudaGetLastError(), "ls_yz_tma launch");
             }
@@ -410,6 +413,7 @@ static int run_kind(x3d_ctx_s *ctx, const x3d_op_s *op, int dir, const T *in, T 
     }
     long nl = dir == DX ? (long)ny * nz : (dir == DY ? (long)nx * nz : (long)nx * ny);
     const int bs = 128;
+    ++ctx->launches;
     ls_generic<T, KIND><<<(unsigned)((nl + bs - 1) / bs), bs, 0, st>>>(in, out, lo, nx, ny, nz, dir);
     return cuda_check(ctx, cudaGetLastError(), "ls_generic launch");
 }
@@ -432,11 +436,109 @@ static int run_typed(x3d_ctx_s *ctx, const x3d_op_s *op, int kind, int dir, cons
     }
 }
 
+// ---------------------------------------------------------------------------
+// Dispatch.  Candidates for a group of operators sharing one input and one
+// direction: the chunked kernel in each of its configurations (one launch
+// for the whole group), then one thread-per-line launch per operator, then
+// the generic kernel.  The autotuner times the candidates once per
+// (direction, grid, precision, group size) and remembers the fastest.
+
+static int run_tpl(x3d_ctx_s *ctx, int dir, const void *in, const x3d_op_s *const *ops,
+                   const int *kinds, void *const *outs, int nops, int nx, int ny, int nz, bool fp32)
+{
+    for (int k = 0; k < nops; ++k) {
+        const int rc = fp32 ? run_typed<float>(ctx, ops[k], kinds[k], dir, in, outs[k], nx, ny, nz)
+                            : run_typed<double>(ctx, ops[k], kinds[k], dir, in, outs[k], nx, ny, nz);
+        if (rc) return rc;
+    }
+    return X3D_OK;
+}
+
+template <typename T>
+static int run_chunk(x3d_ctx_s *ctx, int dir, const void *in, const x3d_op_s *const *ops,
+                     const int *kinds, void *const *outs, int nops, int nx, int ny, int nz, int cfg)
+{
+    ChunkOps<T> co{};
+    co.nops = nops;
+    for (int k = 0; k < nops; ++k) {
+        co.op[k] = lineop<T>(ops[k]);
+        co.kind[k] = kinds[k];
+        co.out[k] = static_cast<T *>(outs[k]);
+        if (kinds[k] == IDENT || outs[k] == in) return X3D_EUNSUPPORTED;  // in-place Thomas: other paths
+    }
+    return launch_chunk<T>(ctx, co, dir, static_cast<const T *>(in), nx, ny, nz, cfg);
+}
+
+// cfg: 0..kChunkConfigs-1 chunked, kChunkConfigs thread-per-line.
+static int run_cfg(x3d_ctx_s *ctx, int cfg, int dir, const void *in, const x3d_op_s *const *ops,
+                   const int *kinds, void *const *outs, int nops, int nx, int ny, int nz, bool fp32)
+{
+    if (cfg < kChunkConfigs)
+        return fp32 ? run_chunk<float>(ctx, dir, in, ops, kinds, outs, nops, nx, ny, nz, cfg)
+                    : run_chunk<double>(ctx, dir, in, ops, kinds, outs, nops, nx, ny, nz, cfg);
+    return run_tpl(ctx, dir, in, ops, kinds, outs, nops, nx, ny, nz, fp32);
+}
+
+static std::string tune_key(int dir, int nx, int ny, int nz, bool fp32, int nops)
+{
+    return std::to_string(dir) + ":" + std::to_string(nx) + "x" + std::to_string(ny) + "x" +
+           std::to_string(nz) + ":" + (fp32 ? "f32" : "f64") + ":" + std::to_string(nops);
+}
+
+int launch_group(x3d_ctx_s *ctx, int dir, const void *in, const x3d_op_s *const *ops,
+                 const int *kinds, void *const *outs, int nops, int nx, int ny, int nz, bool fp32)
+{
+    if (nops < 1 || nops > kMaxChunkOps) return set_error(ctx, X3D_EINVAL, "bad operator group");
+    const auto it = ctx->tuned.find(tune_key(dir, nx, ny, nz, fp32, nops));
+    const int first = it != ctx->tuned.end() ? it->second : ctx->default_cfg;
+    int rc = run_cfg(ctx, first, dir, in, ops, kinds, outs, nops, nx, ny, nz, fp32);
+    if (rc != X3D_EUNSUPPORTED) return rc;
+    for (int cfg = 0; cfg <= kChunkConfigs; ++cfg) {
+        if (cfg == first) continue;
+        rc = run_cfg(ctx, cfg, dir, in, ops, kinds, outs, nops, nx, ny, nz, fp32);
+        if (rc != X3D_EUNSUPPORTED) return rc;
+    }
+    return set_error(ctx, X3D_EUNSUPPORTED, "no kernel accepts this operator group");
+}
+
 int launch_linesolve(x3d_ctx_s *ctx, const x3d_op_s *op, int kind, int dir, const void *in,
                      void *out, int nx, int ny, int nz, bool fp32)
 {
-    if (fp32) return run_typed<float>(ctx, op, kind, dir, in, out, nx, ny, nz);
-    return run_typed<double>(ctx, op, kind, dir, in, out, nx, ny, nz);
+    return launch_group(ctx, dir, in, &op, &kind, &out, 1, nx, ny, nz, fp32);
+}
+
+// Times every candidate on the given buffers (outputs are overwritten) and
+// records the fastest.  Not callable during stream capture.
+int autotune_group(x3d_ctx_s *ctx, int dir, const void *in, const x3d_op_s *const *ops,
+                   const int *kinds, void *const *outs, int nops, bool fp32, int reps, float *best_ms)
+{
+    const int nx = ctx->nx, ny = ctx->ny, nz = ctx->nz;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    int best = -1;
+    float bt = 0.f;
+    for (int cfg = 0; cfg <= kChunkConfigs; ++cfg) {
+        int rc = run_cfg(ctx, cfg, dir, in, ops, kinds, outs, nops, nx, ny, nz, fp32);  // warm-up / probe
+        if (rc == X3D_EUNSUPPORTED) continue;
+        if (rc) break;
+        cudaEventRecord(a, ctx->stream);
+        for (int r = 0; r < reps; ++r) run_cfg(ctx, cfg, dir, in, ops, kinds, outs, nops, nx, ny, nz, fp32);
+        cudaEventRecord(b, ctx->stream);
+        cudaEventSynchronize(b);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        if (best < 0 || ms < bt) {
+            best = cfg;
+            bt = ms;
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (best < 0) return set_error(ctx, X3D_EUNSUPPORTED, "no kernel accepts this operator group");
+    ctx->tuned[tune_key(dir, nx, ny, nz, fp32, nops)] = best;
+    if (best_ms) *best_ms = bt / reps;
+    return X3D_OK;
 }
 
 }  // namespace x3d

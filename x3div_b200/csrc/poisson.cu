@@ -138,6 +138,7 @@ int poisson_solve(x3d_ctx_s *ctx, double *rhs)
     const size_t cap = (size_t)ctx->num_sms * 8;
     if (g > cap) g = cap;
     const double ntot = (double)ctx->nx * (double)ctx->ny * (double)ctx->nz;
+    ++ctx->launches;
     k_spectral_divide<<<(unsigned)g, bs, 0, ctx->stream>>>((double2 *)ctx->spectrum, nxh, ctx->ny,
                                                            ctx->nz, ctx->d_k2x, ctx->d_tx, ctx->d_k2y,
                                                            ctx->d_ty, ctx->d_k2z, ctx->d_tz, ntot);

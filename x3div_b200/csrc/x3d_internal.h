@@ -80,6 +80,11 @@ struct x3d_ctx_s {
     // host-pointer staging buffers
     std::vector<std::pair<void *, size_t>> staging;
     double *d_red = nullptr;  // small reduction buffer
+    // kernel choice per (direction, grid, precision, operator-group size):
+    // filled by the autotuner, default_cfg otherwise
+    std::map<std::string, int> tuned;
+    int default_cfg = 0;
+    unsigned long long launches = 0;  // kernels of this library launched on the context
     size_t elem() const { return precision == X3D_F32 ? 4 : 8; }
     size_t npts() const { return (size_t)nx * ny * nz; }
 };
@@ -98,6 +103,11 @@ void free_op(x3d_op_s *op);
 // the (nx,ny,nz) field in -> out (may alias for kind IDENT).
 int launch_linesolve(x3d_ctx_s *ctx, const x3d_op_s *op, int kind, int dir, const void *in,
                      void *out, int nx, int ny, int nz, bool fp32);
+// Up to six operators along one direction applied to one input, one output each.
+int launch_group(x3d_ctx_s *ctx, int dir, const void *in, const x3d_op_s *const *ops,
+                 const int *kinds, void *const *outs, int nops, int nx, int ny, int nz, bool fp32);
+int autotune_group(x3d_ctx_s *ctx, int dir, const void *in, const x3d_op_s *const *ops,
+                   const int *kinds, void *const *outs, int nops, bool fp32, int reps, float *best_ms);
 
 // ---- elementwise / reductions / transposes (fields.cu) ------------------
 int launch_copy(x3d_ctx_s *ctx, void *dst, const void *src, size_t bytes);
