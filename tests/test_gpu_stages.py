@@ -8,7 +8,9 @@ from conftest import rel_err, seeded_field
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = [(16, 16, 16), (24, 20, 12), (32, 32, 32)]
+# (18, 12, 10): x not a multiple of 4, so the fused stage kernels step aside
+# for the one-launch-per-operator composition.
+SHAPES = [(16, 16, 16), (24, 20, 12), (32, 32, 32), (18, 12, 10)]
 LEN = (2 * np.pi, 1.5, 3.0)
 
 

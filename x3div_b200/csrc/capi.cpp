@@ -615,8 +615,17 @@ int x3d_poisson(x3d_ctx ctx, double *rhs)
 
 // ---- navier ----------------------------------------------------------------------------
 
-// divergence (src/navier.f90:98-236) with 1x1 transposes elided.
+// divergence (src/navier.f90:98-236) with 1x1 transposes elided: the fused
+// stage kernels, or one launch per operator when no fused kernel fits.
+static int divergence_unfused(x3d_ctx_s *ctx, double *pp3, const void *ux, const void *uy, const void *uz);
 static int divergence_dev(x3d_ctx_s *ctx, double *pp3, const void *ux, const void *uy, const void *uz)
+{
+    const void *u[3] = {ux, uy, uz};
+    const int rc = fused_divergence(ctx, pp3, u);
+    return rc == X3D_EUNSUPPORTED ? divergence_unfused(ctx, pp3, ux, uy, uz) : rc;
+}
+
+static int divergence_unfused(x3d_ctx_s *ctx, double *pp3, const void *ux, const void *uy, const void *uz)
 {
     const int nx = ctx->nx, ny = ctx->ny, nz = ctx->nz;
     const bool f = fp32(ctx);
@@ -646,8 +655,21 @@ static int divergence_dev(x3d_ctx_s *ctx, double *pp3, const void *ux, const voi
     return rc;
 }
 
-// gradp (src/navier.f90:249-359) with 1x1 transposes elided.
-static int gradp_dev(x3d_ctx_s *ctx, void *px, void *py, void *pz, const double *pp3)
+// gradp (src/navier.f90:249-359) with 1x1 transposes elided; with ucor set
+// the x stage also applies cor_vel (u -= grad p).
+static int gradp_unfused(x3d_ctx_s *ctx, void *px, void *py, void *pz, const double *pp3);
+static int gradp_dev(x3d_ctx_s *ctx, void *px, void *py, void *pz, const double *pp3,
+                     void *const *ucor = nullptr)
+{
+    void *p[3] = {px, py, pz};
+    int rc = fused_gradp(ctx, p, pp3, ucor);
+    if (rc != X3D_EUNSUPPORTED) return rc;
+    rc = gradp_unfused(ctx, px, py, pz, pp3);
+    if (!rc && ucor) rc = launch_sub3(ctx, fp32(ctx), ucor[0], ucor[1], ucor[2], px, py, pz, ctx->npts());
+    return rc;
+}
+
+static int gradp_unfused(x3d_ctx_s *ctx, void *px, void *py, void *pz, const double *pp3)
 {
     const int nx = ctx->nx, ny = ctx->ny, nz = ctx->nz;
     const bool f = fp32(ctx);
@@ -673,8 +695,21 @@ static int gradp_dev(x3d_ctx_s *ctx, void *px, void *py, void *pz, const double 
     return rc;
 }
 
-// momentum_rhs_eq (src/transeq.f90:44-355) with 1x1 transposes elided.
-static int momentum_dev(x3d_ctx_s *ctx, void *du[3], const void *u[3])
+// momentum_rhs_eq (src/transeq.f90:44-355) with 1x1 transposes elided; with
+// step set, int_time's u = dt du + u is applied too.
+static int momentum_unfused(x3d_ctx_s *ctx, void *du[3], const void *u[3]);
+static int momentum_dev(x3d_ctx_s *ctx, void *du[3], const void *u[3], bool step = false,
+                        double dt = 0.0)
+{
+    void *un[3] = {const_cast<void *>(u[0]), const_cast<void *>(u[1]), const_cast<void *>(u[2])};
+    int rc = fused_transeq(ctx, du, u, step, dt, un);
+    if (rc != X3D_EUNSUPPORTED) return rc;
+    rc = momentum_unfused(ctx, du, u);
+    if (!rc && step) rc = launch_axpy3(ctx, fp32(ctx), un[0], un[1], un[2], du[0], du[1], du[2], dt, ctx->npts());
+    return rc;
+}
+
+static int momentum_unfused(x3d_ctx_s *ctx, void *du[3], const void *u[3])
 {
     const int nx = ctx->nx, ny = ctx->ny, nz = ctx->nz;
     const bool f = fp32(ctx);
@@ -818,12 +853,10 @@ int x3d_euler_step(x3d_ctx ctx, void *ux1, void *uy1, void *uz1, void *dux1, voi
     void *px = sg.out(px1, b), *py = sg.out(py1, b), *pz = sg.out(pz1, b);
     if (sg.status()) return sg.status();
     const void *uc[3] = {u[0], u[1], u[2]};
-    rc = momentum_dev(ctx, du, uc);
-    rc = rc ? rc : launch_axpy3(ctx, fp32(ctx), u[0], u[1], u[2], du[0], du[1], du[2], dt, ctx->npts());
-    rc = rc ? rc : divergence_dev(ctx, p, u[0], u[1], u[2]);
-    rc = rc ? rc : poisson_solve(ctx, p);
-    rc = rc ? rc : gradp_dev(ctx, px, py, pz, p);
-    rc = rc ? rc : launch_sub3(ctx, fp32(ctx), u[0], u[1], u[2], px, py, pz, ctx->npts());
+    rc = momentum_dev(ctx, du, uc, true, dt);               // calculate_transeq_rhs + int_time
+    rc = rc ? rc : divergence_dev(ctx, p, u[0], u[1], u[2]);  // solve_poisson: divergence
+    rc = rc ? rc : poisson_solve(ctx, p);                     //                poisson
+    rc = rc ? rc : gradp_dev(ctx, px, py, pz, p, u);          //                gradp + cor_vel
     return sg.finish(rc);
 }
 

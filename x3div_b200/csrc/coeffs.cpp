@@ -2,6 +2,7 @@
 // x3d_operator_1d_init path of the reference (src/x3d_operator_1d.f90:59-195)
 // for fully periodic boundaries, plus the two vectors the single-pass GPU
 // sweep needs (g = first row of M^-1 and the Sherman-Morrison denominator).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -128,24 +129,67 @@ void finish_op(OpHost &op)
     g[n - 1] = h[n - 1];  // L^T g = h
     for (int i = n - 2; i >= 0; --i) g[i] = h[i] - op.s[i + 1] * g[i + 1];
     op.g = g;
+    // g decays geometrically from i = 0; terms below 1e-18 |g_0| are below
+    // FP64 resolution of y_0 and are dropped.
     op.glen = n;
-    while (op.glen > 1 && g[op.glen - 1] == 0.0) --op.glen;
+    const double gcut = 1e-18 * std::fabs(g[0]);
+    while (op.glen > 1 && std::fabs(g[op.glen - 1]) <= gcut) --op.glen;
     if (op.periodic && !op.per.empty())
         op.den = 1.0 + op.per[0] - op.alfa * op.per[n - 1];
     else
         op.den = 1.0;
 }
 
+// Chunk record table of one operator for chunk length L (see LineOp::tab).
+static std::vector<double> chunk_table(const OpHost &h, int L)
+{
+    const int n = h.n;
+    const int C = (n + L - 1) / L;
+    std::vector<double> t((size_t)C * L * 8, 0.0);
+    for (int c = 0; c < C; ++c) {
+        const int cs = c * L, ce = std::min(n, cs + L);
+        double mf = 1.0;
+        for (int i = cs; i < cs + L; ++i) {
+            double *r = t.data() + (size_t)i * 8;
+            if (i < ce) {
+                mf *= -h.s[i];
+                r[0] = h.s[i];
+                r[1] = mf;
+                r[2] = h.w[i];
+                r[3] = h.f[i] * h.w[i];
+                r[5] = h.per.empty() ? 0.0 : h.per[i];
+            } else {
+                r[0] = -1.0;  // z_i = 0 - (-1) z_{i-1}: the last value rides to the chunk end
+                r[1] = mf;
+            }
+        }
+        double mb = 1.0;
+        for (int i = ce - 1; i >= cs; --i) {
+            mb *= -(h.f[i] * h.w[i]);
+            t[(size_t)i * 8 + 4] = mb;
+        }
+    }
+    return t;
+}
+
 int upload_op(x3d_op_s *op)
 {
     const OpHost &h = op->h;
     const int n = h.n;
-    const size_t fbytes = (size_t)4 * n * sizeof(float);
-    const size_t fpad = (fbytes + 255) & ~(size_t)255;
-    const size_t dbytes = (size_t)5 * n * sizeof(double);
-    std::vector<unsigned char> host(fpad + dbytes, 0);
-    float *hf = reinterpret_cast<float *>(host.data());
-    double *hd = reinterpret_cast<double *>(host.data() + fpad);
+    // layout (bytes, each part 256-aligned): float s,w,fw,p | double s,w,fw,p,g |
+    // float tables (L = 32, 16) | double tables (L = 16, 8)
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const std::vector<double> tf0 = chunk_table(h, kChunkLong<float>), tf1 = chunk_table(h, kChunkShort<float>);
+    const std::vector<double> td0 = chunk_table(h, kChunkLong<double>), td1 = chunk_table(h, kChunkShort<double>);
+    const size_t o_f = 0, o_d = al(o_f + 4 * n * sizeof(float));
+    const size_t o_tf0 = al(o_d + 5 * n * sizeof(double));
+    const size_t o_tf1 = al(o_tf0 + tf0.size() * sizeof(float));
+    const size_t o_td0 = al(o_tf1 + tf1.size() * sizeof(float));
+    const size_t o_td1 = al(o_td0 + td0.size() * sizeof(double));
+    const size_t total = al(o_td1 + td1.size() * sizeof(double));
+    std::vector<unsigned char> host(total, 0);
+    float *hf = reinterpret_cast<float *>(host.data() + o_f);
+    double *hd = reinterpret_cast<double *>(host.data() + o_d);
     for (int i = 0; i < n; ++i) {
         const double fw = h.f[i] * h.w[i];
         const double p = h.per.empty() ? 0.0 : h.per[i];
@@ -159,18 +203,27 @@ int upload_op(x3d_op_s *op)
         hd[3 * n + i] = p;
         hd[4 * n + i] = h.g[i];
     }
+    auto put_f = [&](size_t off, const std::vector<double> &t) {
+        float *d = reinterpret_cast<float *>(host.data() + off);
+        for (size_t i = 0; i < t.size(); ++i) d[i] = (float)t[i];
+    };
+    put_f(o_tf0, tf0);
+    put_f(o_tf1, tf1);
+    std::memcpy(host.data() + o_td0, td0.data(), td0.size() * sizeof(double));
+    std::memcpy(host.data() + o_td1, td1.data(), td1.size() * sizeof(double));
     if (op->dmem) cudaFree(op->dmem);
     op->dmem = nullptr;
     if (cudaMalloc(&op->dmem, host.size()) != cudaSuccess) return X3D_ENOMEM;
     if (cudaMemcpy(op->dmem, host.data(), host.size(), cudaMemcpyHostToDevice) != cudaSuccess)
         return X3D_ECUDA;
-    const float *df = reinterpret_cast<const float *>(op->dmem);
-    const double *dd = reinterpret_cast<const double *>((const unsigned char *)op->dmem + fpad);
-    auto fill = [&](auto &lo, auto *base) {
-        lo.s = base + 0 * n;
-        lo.w = base + 1 * n;
-        lo.fw = base + 2 * n;
-        lo.p = base + 3 * n;
+    const unsigned char *base = static_cast<const unsigned char *>(op->dmem);
+    const float *df = reinterpret_cast<const float *>(base + o_f);
+    const double *dd = reinterpret_cast<const double *>(base + o_d);
+    auto fill = [&](auto &lo, auto *arr) {
+        lo.s = arr + 0 * n;
+        lo.w = arr + 1 * n;
+        lo.fw = arr + 2 * n;
+        lo.p = arr + 3 * n;
         lo.g = dd + 4 * n;
         lo.alfa = h.alfa;
         lo.den = h.den;
@@ -180,6 +233,10 @@ int upload_op(x3d_op_s *op)
     };
     fill(op->opf, df);
     fill(op->opd, dd);
+    op->opf.tab[0] = reinterpret_cast<const float *>(base + o_tf0);
+    op->opf.tab[1] = reinterpret_cast<const float *>(base + o_tf1);
+    op->opd.tab[0] = reinterpret_cast<const double *>(base + o_td0);
+    op->opd.tab[1] = reinterpret_cast<const double *>(base + o_td1);
     op->opf.a = (float)h.a; op->opf.b = (float)h.b; op->opf.c = (float)h.c; op->opf.d = (float)h.d;
     op->opd.a = h.a; op->opd.b = h.b; op->opd.c = h.c; op->opd.d = h.d;
     return X3D_OK;

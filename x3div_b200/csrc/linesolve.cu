@@ -458,15 +458,13 @@ template <typename T>
 static int run_chunk(x3d_ctx_s *ctx, int dir, const void *in, const x3d_op_s *const *ops,
                      const int *kinds, void *const *outs, int nops, int nx, int ny, int nz, int cfg)
 {
-    ChunkOps<T> co{};
-    co.nops = nops;
+    const LineOp<T> *lops[kMaxStageOps];
     for (int k = 0; k < nops; ++k) {
-        co.op[k] = lineop<T>(ops[k]);
-        co.kind[k] = kinds[k];
-        co.out[k] = static_cast<T *>(outs[k]);
+        lops[k] = &lineop<T>(ops[k]);
         if (kinds[k] == IDENT || outs[k] == in) return X3D_EUNSUPPORTED;  // in-place Thomas: other paths
     }
-    return launch_chunk<T>(ctx, co, dir, static_cast<const T *>(in), nx, ny, nz, cfg);
+    const StageProgram<T> prog = plain_program<T>(static_cast<const T *>(in), lops, kinds, outs, nops);
+    return launch_stage<T>(ctx, prog, dir, nx, ny, nz, cfg);
 }
 
 // cfg: 0..kChunkConfigs-1 chunked, kChunkConfigs thread-per-line.
@@ -488,7 +486,7 @@ static std::string tune_key(int dir, int nx, int ny, int nz, bool fp32, int nops
 int launch_group(x3d_ctx_s *ctx, int dir, const void *in, const x3d_op_s *const *ops,
                  const int *kinds, void *const *outs, int nops, int nx, int ny, int nz, bool fp32)
 {
-    if (nops < 1 || nops > kMaxChunkOps) return set_error(ctx, X3D_EINVAL, "bad operator group");
+    if (nops < 1 || nops > kMaxStageOps) return set_error(ctx, X3D_EINVAL, "bad operator group");
     const auto it = ctx->tuned.find(tune_key(dir, nx, ny, nz, fp32, nops));
     const int first = it != ctx->tuned.end() ? it->second : ctx->default_cfg;
     int rc = run_cfg(ctx, first, dir, in, ops, kinds, outs, nops, nx, ny, nz, fp32);

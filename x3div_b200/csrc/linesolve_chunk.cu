@@ -1,6 +1,6 @@
 // Chunked periodic line solves: the fast path for whole-field operator
-// applications, and the multi-operator variant that applies up to six
-// operators to one staged input (one read of the field, K writes).
+// applications, and the stage kernels that fuse several operators, their
+// pointwise products and their sums into one pass over the staged inputs.
 //
 // The reference sweeps each line serially (?thomas_12, src/thomas.f90:61-84):
 //   forward  z_i = r_i - s_i z_{i-1}          backward y_i = (z_i - f_i y_{i+1}) w_i
@@ -12,8 +12,7 @@
 // affine in its incoming value, so a chunk is swept locally from zero and
 // later shifted by  multiplier * carry, where the multiplier is the running
 // product of the reference's own factors (-s_i forward, -f_i w_i backward):
-//   1. stencil r_i for the chunk (window of L+8 input values, read once for
-//      all K operators);
+//   1. stencil r_i for the chunk from an L+8 window of the staged input;
 //   2. local forward sweep -> chunk end value and multiplier, plus the chunk's
 //      share of y_0 = sum_i g_i r_i (g = first row of M^-1, FP64);
 //   -- barrier -- every thread scans the chunk ends (C fused multiply-adds)
@@ -22,9 +21,15 @@
 //   3. fix the forward values, local backward sweep -> chunk start value and
 //      multiplier;
 //   -- barrier -- scan for the backward carry;
-//   4. fix the backward values, subtract ss p_i, store.
+//   4. fix the backward values and subtract ss p_i.
 // Two barriers per operator, no intermediate field in shared memory, and the
 // same arithmetic as the reference Thomas + Sherman-Morrison up to rounding.
+//
+// A stage (StageProgram) runs up to six such operators over up to three
+// staged inputs, combining the results in a register accumulator and
+// writing only what the program flushes, so e.g. one x-pencil pass of
+// momentum_rhs_eq (src/transeq.f90:99-116, six derx calls and their
+// products and sums for three velocity components) is one kernel.
 //
 // Staging: y/z tiles of W x-adjacent lines arrive by TMA tensor loads and
 // results go straight to global memory, coalesced across the W lines; x
@@ -33,9 +38,9 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include "linesolve_chunk.h"
 #include "ptx.cuh"
 #include "x3d_internal.h"
-#include "linesolve_chunk.h"
 
 namespace x3d {
 
@@ -79,99 +84,114 @@ __device__ __forceinline__ void chunk_stencil_kind(int kind, const T (&w)[L + 8]
     }
 }
 
-// Scratch in shared memory after the input tile: per (chunk, line) the
+// Scratch in shared memory after the input tiles: per (chunk, line) the
 // forward end value / multiplier / y_0 share and the backward start value /
-// multiplier.
+// multiplier, and per line the Sherman-Morrison scalar.
 template <typename T>
 struct ChunkScratch {
     T *fz, *fm, *bz, *bm;
-    double *fg;
+    double *fg, *ss;
+};
+
+// Loads of the per-point records of LineOp::tab: {s, mf, w, fw, mb, p, 0, 0}.
+template <typename T>
+struct Rec;
+template <>
+struct Rec<float> {
+    __device__ static float s(const float *t) { return __ldg(t); }
+    __device__ static float4 mfwfw(const float *t) { return __ldg(reinterpret_cast<const float4 *>(t)); }
+    __device__ static float2 mbp(const float *t) { return __ldg(reinterpret_cast<const float2 *>(t + 4)); }
+};
+template <>
+struct Rec<double> {
+    __device__ static double s(const double *t) { return __ldg(t); }
+    __device__ static double4 mfwfw(const double *t)
+    {
+        const double2 a = __ldg(reinterpret_cast<const double2 *>(t));
+        const double2 b = __ldg(reinterpret_cast<const double2 *>(t + 2));
+        return make_double4(a.x, a.y, b.x, b.y);
+    }
+    __device__ static double2 mbp(const double *t) { return __ldg(reinterpret_cast<const double2 *>(t + 4)); }
 };
 
 // Steps 1-4 for one operator; the solved values end in r[] (chunk-local).
-// load(w) fills the L+8 input window u[cs-4 .. cs+L+3] (indices mod n) from
-// the staged tile; the window is dead once the stencil is evaluated.
+// load(w) fills the L+8 input window u[cs-4 .. cs+L+3] (indices mod n); the
+// window is dead once the stencil is evaluated.  tab is this chunk length's
+// record table (records padded to whole chunks, so the sweeps need no
+// bounds tests: padding keeps the forward value and zeroes the backward one).
 template <typename T, int W, int L, typename Load>
-__device__ __forceinline__ void chunk_solve(const LineOp<T> &op, int kind, const Load &load,
-                                            T (&r)[L], const ChunkScratch<T> &sc, int l, int c,
-                                            int C, int cs, int nv)
+__device__ __forceinline__ void chunk_solve(const LineOp<T> &op, const T *tab, int kind,
+                                            const Load &load, T (&r)[L], const ChunkScratch<T> &sc,
+                                            int l, int c, int C, int cs, int nv)
 {
     {
         T w[L + 8];
         load(w);
         chunk_stencil_kind<T, L>(kind, w, r, op);
     }
-    // local forward sweep
-    T zh = T(0), m = T(1);
+    if (nv < L) {  // only the last chunk: padding points get r = 0
+#pragma unroll
+        for (int j = 0; j < L; ++j)
+            if (j >= nv) r[j] = T(0);
+    }
+    const T *t = tab + (size_t)cs * 8;
+    // local forward sweep, y_0 share
+    T zh = T(0);
     double gp = 0.0;
-    const bool has_g = cs < op.glen;
+    if (cs < op.glen) {
+#pragma unroll
+        for (int j = 0; j < L; ++j) gp = fma(__ldg(op.g + min(cs + j, op.n - 1)), (double)r[j], gp);
+    }
 #pragma unroll
     for (int j = 0; j < L; ++j) {
-        if (j < nv) {
-            const int i = cs + j;
-            const T s = __ldg(op.s + i);
-            if (has_g) gp = fma(__ldg(op.g + i), (double)r[j], gp);
-            zh = r[j] - s * zh;
-            m = -s * m;
-            r[j] = zh;
-        }
+        zh = r[j] - Rec<T>::s(t + 8 * j) * zh;
+        r[j] = zh;
     }
     const int q = c * W + l;
+    const T fme = __ldg(t + 8 * (L - 1) + 1);  // product of -s over the chunk
     sc.fz[q] = zh;
-    sc.fm[q] = m;
+    sc.fm[q] = fme;
     sc.fg[q] = gp;
     __syncthreads();
-    // forward carries, y_0 and z_{n-1}
-    T carry = T(0), run = T(0);
-    double y0 = 0.0;
-    const int cg = min(C, (op.glen + L - 1) / L);
-    for (int cc = 0; cc < C; ++cc) {
-        if (cc == c) carry = run;
+    // forward carry: z at the end of chunk c-1
+    T carry = T(0);
+    for (int cc = 0; cc < c; ++cc) {
         const int qq = cc * W + l;
-        run = sc.fz[qq] + sc.fm[qq] * run;
-        if (cc < cg) y0 += sc.fg[qq];
+        carry = sc.fz[qq] + sc.fm[qq] * carry;
     }
-    const T zlast = run;
-    const int n = op.n;
-    const double ss =
-        op.periodic ? (y0 - op.alfa * ((double)zlast * (double)__ldg(op.w + (n - 1)))) / op.den : 0.0;
-    // fix forward values, local backward sweep
-    m = T(1);
-#pragma unroll
-    for (int j = 0; j < L; ++j) {
-        if (j < nv) {
-            m = -__ldg(op.s + cs + j) * m;
-            r[j] = r[j] + m * carry;
-        }
+    if (c == C - 1) {
+        // last chunk: z_{n-1} (carried to the padded end), y_0, and the
+        // Sherman-Morrison scalar for the whole line
+        const T zlast = zh + fme * carry;
+        double y0 = 0.0;
+        const int cg = min(C, (op.glen + L - 1) / L);
+        for (int cc = 0; cc < cg; ++cc) y0 += sc.fg[cc * W + l];
+        sc.ss[l] = op.periodic
+                       ? (y0 - op.alfa * ((double)zlast * (double)__ldg(op.w + (op.n - 1)))) / op.den
+                       : 0.0;
     }
-    T yh = T(0), mb = T(1);
+    // fix forward values and sweep backward locally
+    T yh = T(0);
 #pragma unroll
     for (int j = L - 1; j >= 0; --j) {
-        if (j < nv) {
-            const int i = cs + j;
-            const T fw = __ldg(op.fw + i);
-            yh = r[j] * __ldg(op.w + i) - fw * yh;
-            mb = -fw * mb;
-            r[j] = yh;
-        }
+        const auto cw = Rec<T>::mfwfw(t + 8 * j);  // (s, mf, w, fw)
+        const T z = r[j] + cw.y * carry;
+        yh = z * cw.z - cw.w * yh;
+        r[j] = yh;
     }
     sc.bz[q] = yh;
-    sc.bm[q] = mb;
+    sc.bm[q] = __ldg(t + 4);  // product of -f w over the chunk
     __syncthreads();
     T bcarry = T(0);
     for (int cc = C - 1; cc > c; --cc) {
         const int qq = cc * W + l;
         bcarry = sc.bz[qq] + sc.bm[qq] * bcarry;
     }
-    const T sst = (T)ss;
-    mb = T(1);
+    const T sst = (T)sc.ss[l];
 #pragma unroll
-    for (int j = L - 1; j >= 0; --j) {
-        if (j < nv) {
-            const int i = cs + j;
-            mb = -__ldg(op.fw + i) * mb;
-            r[j] = r[j] + mb * bcarry - sst * __ldg(op.p + i);
-        }
+    for (int j = 0; j < L; ++j) {
+        const auto mp = Rec<T>::mbp(t + 8 * j);  // (mb, p)
+        r[j] = r[j] + mp.x * bcarry - sst * mp.y;
     }
 }
 
@@ -186,21 +206,62 @@ __device__ __forceinline__ ChunkScratch<T> carve_scratch(unsigned char *base, in
     sc.bz = t + 2 * q;
     sc.bm = t + 3 * q;
     sc.fg = reinterpret_cast<double *>(base + (((size_t)4 * q * sizeof(T) + 15) & ~(size_t)15));
+    sc.ss = sc.fg + q;
     return sc;
+}
+
+// acc (+)= m * r, with m = 1 or the staged tile value at the point.
+template <typename T, int L, typename TileAt>
+__device__ __forceinline__ void accumulate(const StageOp<T> &so, T (&acc)[L], const T (&r)[L],
+                                           int nv, const TileAt &tile_at)
+{
+    if (so.mul_tile < 0) {
+        if (so.accumulate) {
+#pragma unroll
+            for (int j = 0; j < L; ++j) acc[j] += r[j];
+        } else {
+#pragma unroll
+            for (int j = 0; j < L; ++j) acc[j] = r[j];
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < L; ++j) {
+            if (j < nv) {
+                const T mv = tile_at(so.mul_tile, j);
+                acc[j] = so.accumulate ? acc[j] + mv * r[j] : mv * r[j];
+            }
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
 // y- and z-lines.
-template <typename T, int W, int L>
-__global__ void __launch_bounds__(512) ls_chunk_yz(const __grid_constant__ CUtensorMap tmap,
-                                                    const __grid_constant__ ChunkOps<T> ops, int nx,
-                                                    int ny, int dir, int box_n, int nbox,
-                                                    size_t tile_bytes, int *err)
+struct StageMaps {
+    CUtensorMap m[kMaxStageTiles];
+};
+
+template <typename T, typename U>
+__device__ __forceinline__ void flush_point(const StageOp<T> &so, size_t p, T a)
+{
+    const U *base = static_cast<const U *>(so.base);
+    U v = (U)so.sign * (U)a;
+    if (base) v = base[p] + v;
+    static_cast<U *>(so.out)[p] = v;
+    if (so.out2) {
+        const U *b2 = static_cast<const U *>(so.base2);
+        static_cast<U *>(so.out2)[p] = (b2 ? b2[p] : U(0)) + (U)so.scale2 * v;
+    }
+}
+
+template <typename T, int W, int L, bool ACC>
+__global__ void __launch_bounds__(512, 1) ls_stage_yz(const __grid_constant__ StageMaps maps,
+                                                   const __grid_constant__ StageProgram<T> prog,
+                                                   int nx, int ny, int dir, int box_n, int nbox,
+                                                   size_t tile_bytes, int *err)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ uint64_t bar;
-    T *tile = reinterpret_cast<T *>(smem_raw);
-    const int n = ops.op[0].n;
+    const int n = prog.ops[0].op.n;
     const int C = blockDim.x / W;
     const int t = threadIdx.x;
     const int l = t % W, c = t / W;
@@ -213,12 +274,15 @@ __global__ void __launch_bounds__(512) ls_chunk_yz(const __grid_constant__ CUten
     }
     __syncthreads();
     if (t == 0) {
-        mbar_arrive_expect_tx(&bar, (uint32_t)((size_t)nbox * box_n * W * sizeof(T)));
-        for (int b = 0; b < nbox; ++b) {
-            if (dir == DY)
-                tma_load_3d(tile + (size_t)b * box_n * W, &tmap, &bar, x0, b * box_n, o);
-            else
-                tma_load_3d(tile + (size_t)b * box_n * W, &tmap, &bar, x0, o, b * box_n);
+        mbar_arrive_expect_tx(&bar, (uint32_t)((size_t)prog.ntiles * nbox * box_n * W * sizeof(T)));
+        for (int ti = 0; ti < prog.ntiles; ++ti) {
+            T *tile = reinterpret_cast<T *>(smem_raw + ti * tile_bytes);
+            for (int b = 0; b < nbox; ++b) {
+                if (dir == DY)
+                    tma_load_3d(tile + (size_t)b * box_n * W, &maps.m[ti], &bar, x0, b * box_n, o);
+                else
+                    tma_load_3d(tile + (size_t)b * box_n * W, &maps.m[ti], &bar, x0, o, b * box_n);
+            }
         }
     }
     const bool ok = mbar_wait_bounded(&bar, 0, kChunkWaitNs);
@@ -227,36 +291,56 @@ __global__ void __launch_bounds__(512) ls_chunk_yz(const __grid_constant__ CUten
         mbar_wait_bounded(&bar, 0, kChunkWaitNs);
         return;
     }
-    const ChunkScratch<T> sc = carve_scratch<T>(smem_raw + tile_bytes, C, W);
+    const ChunkScratch<T> sc = carve_scratch<T>(smem_raw + prog.ntiles * tile_bytes, C, W);
     const int cs = c * L;
     const int nv = min(L, n - cs);
-    const T *col = tile + l;
     const bool wraps = cs < 4 || cs + L + 4 > n;
-    auto load = [&](T(&w)[L + 8]) {
-        if (!wraps) {
-#pragma unroll
-            for (int j = 0; j < L + 8; ++j) w[j] = col[(cs - 4 + j) * W];
-        } else {
-#pragma unroll
-            for (int j = 0; j < L + 8; ++j) {
-                int idx = (cs - 4 + j) % n;
-                idx = idx < 0 ? idx + n : idx;
-                w[j] = col[idx * W];
-            }
-        }
-    };
+    auto col = [&](int ti) { return reinterpret_cast<const T *>(smem_raw + ti * tile_bytes) + l; };
+    auto tile_at = [&](int ti, int j) { return col(ti)[(cs + j) * W]; };
     const bool live = x0 + l < nx;
     const size_t ostride = dir == DY ? (size_t)nx : (size_t)nx * ny;
     const size_t obase = (size_t)(x0 + l) + (dir == DY ? (size_t)nx * ny * o : (size_t)nx * o) +
                          (size_t)cs * ostride;
     T r[L];
-    for (int k = 0; k < ops.nops; ++k) {
-        chunk_solve<T, W, L>(ops.op[k], ops.kind[k], load, r, sc, l, c, C, cs, nv);
-        if (live) {
-            T *dst = ops.out[k] + obase;
+    T acc[ACC ? L : 1];
+    for (int k = 0; k < prog.nops; ++k) {
+        const StageOp<T> &so = prog.ops[k];
+        const T *ca = col(so.src_a);
+        const T *cb = so.src_b >= 0 ? col(so.src_b) : nullptr;
+        auto load = [&](T(&w)[L + 8]) {
 #pragma unroll
-            for (int j = 0; j < L; ++j)
-                if (j < nv) dst[(size_t)j * ostride] = r[j];
+            for (int j = 0; j < L + 8; ++j) {
+                int idx = cs - 4 + j;
+                if (wraps) {
+                    idx %= n;
+                    idx = idx < 0 ? idx + n : idx;
+                }
+                w[j] = cb ? ca[idx * W] * cb[idx * W] : ca[idx * W];
+            }
+        };
+        chunk_solve<T, W, L>(so.op, so.op.tab[L == kChunkLong<T> ? 0 : 1], so.kind, load, r, sc, l, c, C, cs, nv);
+        if constexpr (ACC) accumulate<T, L>(so, acc, r, nv, tile_at);
+        const T *res;
+        if constexpr (ACC) res = acc;
+        else res = r;
+        if (so.flush && live) {
+            if (!so.base && !so.out2 && !so.out_f64 && so.sign == 1.0) {
+                T *dst = static_cast<T *>(so.out) + obase;
+#pragma unroll
+                for (int j = 0; j < L; ++j) {
+                    if (j < nv) *dst = res[j];
+                    dst += ostride;
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < L; ++j) {
+                    if (j < nv) {
+                        const size_t p = obase + (size_t)j * ostride;
+                        if (so.out_f64) flush_point<T, double>(so, p, res[j]);
+                        else flush_point<T, T>(so, p, res[j]);
+                    }
+                }
+            }
         }
     }
 }
@@ -276,17 +360,52 @@ struct Vec4<double> {
     using type = double2;
 };
 
-template <typename T, int W, int L>
-__global__ void __launch_bounds__(512) ls_chunk_x(const T *__restrict__ in,
-                                                   const __grid_constant__ ChunkOps<T> ops,
-                                                   long nlines, int pitch, size_t tile_bytes, int *err)
+// Writes V consecutive results of one thread's chunk starting at element p0
+// as 16-byte vectors of the output type U (T, or double for out_f64).
+template <typename T, typename U, int V>
+__device__ __forceinline__ void flush_vec(const StageOp<T> &so, size_t p0, const T *a)
+{
+    using UV = typename Vec4<U>::type;
+    constexpr int VU = Vec4<U>::N;
+#pragma unroll
+    for (int h = 0; h < V; h += VU) {
+        UV q;
+        U *v = reinterpret_cast<U *>(&q);
+#pragma unroll
+        for (int e = 0; e < VU; ++e) v[e] = (U)so.sign * (U)a[h + e];
+        if (so.base) {
+            const UV bq = *reinterpret_cast<const UV *>(static_cast<const U *>(so.base) + p0 + h);
+            const U *be = reinterpret_cast<const U *>(&bq);
+#pragma unroll
+            for (int e = 0; e < VU; ++e) v[e] = be[e] + v[e];
+        }
+        *reinterpret_cast<UV *>(static_cast<U *>(so.out) + p0 + h) = q;
+        if (so.out2) {
+            UV q2;
+            U *v2 = reinterpret_cast<U *>(&q2);
+            if (so.base2) {
+                const UV bq = *reinterpret_cast<const UV *>(static_cast<const U *>(so.base2) + p0 + h);
+                const U *be = reinterpret_cast<const U *>(&bq);
+#pragma unroll
+                for (int e = 0; e < VU; ++e) v2[e] = be[e] + (U)so.scale2 * v[e];
+            } else {
+#pragma unroll
+                for (int e = 0; e < VU; ++e) v2[e] = (U)so.scale2 * v[e];
+            }
+            *reinterpret_cast<UV *>(static_cast<U *>(so.out2) + p0 + h) = q2;
+        }
+    }
+}
+
+template <typename T, int W, int L, bool ACC>
+__global__ void __launch_bounds__(512, 1) ls_stage_x(const __grid_constant__ StageProgram<T> prog,
+                                                  long nlines, int pitch, size_t tile_bytes, int *err)
 {
     using VT = typename Vec4<T>::type;
     constexpr int V = Vec4<T>::N;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ uint64_t bar;
-    T *tile = reinterpret_cast<T *>(smem_raw);
-    const int n = ops.op[0].n;
+    const int n = prog.ops[0].op.n;
     const int C = blockDim.x / W;
     const int t = threadIdx.x;
     const int l = t % W, c = t / W;
@@ -299,9 +418,12 @@ __global__ void __launch_bounds__(512) ls_chunk_x(const T *__restrict__ in,
     }
     __syncthreads();
     if (t == 0) {
-        mbar_arrive_expect_tx(&bar, row_bytes * (uint32_t)rows);
-        for (int rr = 0; rr < rows; ++rr)
-            bulk_load(tile + (size_t)rr * pitch, in + (size_t)(l0 + rr) * n, row_bytes, &bar);
+        mbar_arrive_expect_tx(&bar, row_bytes * (uint32_t)rows * (uint32_t)prog.ntiles);
+        for (int ti = 0; ti < prog.ntiles; ++ti) {
+            T *tile = reinterpret_cast<T *>(smem_raw + ti * tile_bytes);
+            for (int rr = 0; rr < rows; ++rr)
+                bulk_load(tile + (size_t)rr * pitch, prog.in[ti] + (size_t)(l0 + rr) * n, row_bytes, &bar);
+        }
     }
     const bool ok = mbar_wait_bounded(&bar, 0, kChunkWaitNs);
     if (!__syncthreads_and(ok)) {
@@ -309,35 +431,50 @@ __global__ void __launch_bounds__(512) ls_chunk_x(const T *__restrict__ in,
         mbar_wait_bounded(&bar, 0, kChunkWaitNs);
         return;
     }
-    const ChunkScratch<T> sc = carve_scratch<T>(smem_raw + tile_bytes, C, W);
+    const ChunkScratch<T> sc = carve_scratch<T>(smem_raw + prog.ntiles * tile_bytes, C, W);
     const int cs = c * L;
     const int nv = min(L, n - cs);
     const int lr = l < rows ? l : 0;  // rows past the end compute on row 0 and store nothing
-    const T *row = tile + (size_t)lr * pitch;
-    auto load = [&](T(&w)[L + 8]) {
-#pragma unroll
-        for (int j = 0; j < L + 8; j += V) {
-            int idx = (cs - 4 + j) % n;
-            idx = idx < 0 ? idx + n : idx;
-            const VT q = *reinterpret_cast<const VT *>(row + idx);
-            const T *e = reinterpret_cast<const T *>(&q);
-#pragma unroll
-            for (int v = 0; v < V; ++v) w[j + v] = e[v];
-        }
+    auto row = [&](int ti) {
+        return reinterpret_cast<const T *>(smem_raw + ti * tile_bytes) + (size_t)lr * pitch;
     };
+    auto tile_at = [&](int ti, int j) { return row(ti)[cs + j]; };
     T r[L];
-    for (int k = 0; k < ops.nops; ++k) {
-        chunk_solve<T, W, L>(ops.op[k], ops.kind[k], load, r, sc, l, c, C, cs, nv);
-        if (l < rows) {
-            T *dst = ops.out[k] + (size_t)(l0 + l) * n + cs;
+    T acc[ACC ? L : 1];
+    for (int k = 0; k < prog.nops; ++k) {
+        const StageOp<T> &so = prog.ops[k];
+        const T *ra = row(so.src_a);
+        const T *rb = so.src_b >= 0 ? row(so.src_b) : nullptr;
+        auto load = [&](T(&w)[L + 8]) {
+#pragma unroll
+            for (int j = 0; j < L + 8; j += V) {
+                int idx = (cs - 4 + j) % n;
+                idx = idx < 0 ? idx + n : idx;
+                const VT qa = *reinterpret_cast<const VT *>(ra + idx);
+                const T *ea = reinterpret_cast<const T *>(&qa);
+                if (rb) {
+                    const VT qb = *reinterpret_cast<const VT *>(rb + idx);
+                    const T *eb = reinterpret_cast<const T *>(&qb);
+#pragma unroll
+                    for (int v = 0; v < V; ++v) w[j + v] = ea[v] * eb[v];
+                } else {
+#pragma unroll
+                    for (int v = 0; v < V; ++v) w[j + v] = ea[v];
+                }
+            }
+        };
+        chunk_solve<T, W, L>(so.op, so.op.tab[L == kChunkLong<T> ? 0 : 1], so.kind, load, r, sc, l, c, C, cs, nv);
+        if constexpr (ACC) accumulate<T, L>(so, acc, r, nv, tile_at);
+        const T *res;
+        if constexpr (ACC) res = acc;
+        else res = r;
+        if (so.flush && l < rows) {
+            const size_t p0 = (size_t)(l0 + l) * n + cs;
 #pragma unroll
             for (int j = 0; j < L; j += V) {
                 if (j < nv) {
-                    VT q;
-                    T *e = reinterpret_cast<T *>(&q);
-#pragma unroll
-                    for (int v = 0; v < V; ++v) e[v] = r[j + v];
-                    *reinterpret_cast<VT *>(dst + j) = q;
+                    if (so.out_f64) flush_vec<T, double, V>(so, p0 + j, res + j);
+                    else flush_vec<T, T, V>(so, p0 + j, res + j);
                 }
             }
         }
@@ -360,83 +497,137 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_tiled()
     return fn;
 }
 
+struct StageOpView {
+    short flush, accumulate, mul_tile;
+};
+
 static size_t scratch_bytes(int C, int W, size_t es)
 {
-    return (((size_t)4 * C * W * es + 15) & ~(size_t)15) + (size_t)C * W * sizeof(double);
+    return (((size_t)4 * C * W * es + 15) & ~(size_t)15) + (size_t)(C + 1) * W * sizeof(double);
 }
 
+static bool al16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+static bool plain(const StageOpView &v) { return v.flush && !v.accumulate && v.mul_tile < 0; }
+
 template <typename T, int W, int L>
-static int launch_chunk_cfg(x3d_ctx_s *ctx, const ChunkOps<T> &ops, int dir, const T *in, int nx,
-                            int ny, int nz)
+static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir, int nx, int ny,
+                            int nz)
 {
-    const int n = ops.op[0].n;
+    bool acc = false;
+    for (int k = 0; k < prog.nops; ++k)
+        acc = acc || !plain(StageOpView{prog.ops[k].flush, prog.ops[k].accumulate, prog.ops[k].mul_tile});
+    const int n = prog.ops[0].op.n;
     const size_t es = sizeof(T);
     const int C = (n + L - 1) / L;
     const int threads = C * W;
     if (threads > 512 || threads % 32) return X3D_EUNSUPPORTED;
+    for (int ti = 0; ti < prog.ntiles; ++ti)
+        if (!al16(prog.in[ti])) return X3D_EUNSUPPORTED;
     cudaStream_t st = ctx->stream;
     if (dir == DX) {
         constexpr int V = Vec4<T>::N;
-        if (n % V || (reinterpret_cast<uintptr_t>(in) & 15)) return X3D_EUNSUPPORTED;
-        for (int k = 0; k < ops.nops; ++k)
-            if (reinterpret_cast<uintptr_t>(ops.out[k]) & 15) return X3D_EUNSUPPORTED;
+        if (n % V) return X3D_EUNSUPPORTED;
+        for (int k = 0; k < prog.nops; ++k) {
+            const StageOp<T> &so = prog.ops[k];
+            if (so.flush && (!al16(so.out) || !al16(so.base) || !al16(so.out2) || !al16(so.base2)))
+                return X3D_EUNSUPPORTED;
+        }
         int pitch = n + V;
         while (((size_t)pitch * es / 16) % 2 == 0) pitch += V;
         const size_t tile = ((size_t)W * pitch * es + 127) & ~(size_t)127;
-        const size_t smem = tile + scratch_bytes(C, W, es);
+        const size_t smem = prog.ntiles * tile + scratch_bytes(C, W, es);
         if (smem + 1024 > ctx->smem_optin) return X3D_EUNSUPPORTED;
-        auto kern = ls_chunk_x<T, W, L>;
+        auto kern = acc ? ls_stage_x<T, W, L, true> : ls_stage_x<T, W, L, false>;
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         const long nlines = (long)ny * nz;
         ++ctx->launches;
-        kern<<<(unsigned)((nlines + W - 1) / W), threads, smem, st>>>(in, ops, nlines, pitch, tile, ctx->d_err);
-        return cuda_check(ctx, cudaGetLastError(), "ls_chunk_x launch");
+        kern<<<(unsigned)((nlines + W - 1) / W), threads, smem, st>>>(prog, nlines, pitch, tile, ctx->d_err);
+        return cuda_check(ctx, cudaGetLastError(), "ls_stage_x launch");
     }
     auto enc = encode_tiled();
-    if (!enc || ((size_t)nx * es) % 16 || (reinterpret_cast<uintptr_t>(in) & 15)) return X3D_EUNSUPPORTED;
+    if (!enc || ((size_t)nx * es) % 16) return X3D_EUNSUPPORTED;
     const int nb = (n + 255) / 256;
     int box_n = (n + nb - 1) / nb;
     const int align_rows = (int)(128 / (W * es) > 0 ? 128 / (W * es) : 1);
     box_n = (box_n + align_rows - 1) / align_rows * align_rows;
     if (box_n > 256) return X3D_EUNSUPPORTED;
     const size_t tile = ((size_t)nb * box_n * W * es + 127) & ~(size_t)127;
-    const size_t smem = tile + scratch_bytes(C, W, es);
+    const size_t smem = prog.ntiles * tile + scratch_bytes(C, W, es);
     if (smem + 1024 > ctx->smem_optin) return X3D_EUNSUPPORTED;
-    CUtensorMap tmap;
-    cuuint64_t gdim[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
-    cuuint64_t gstride[2] = {(cuuint64_t)nx * es, (cuuint64_t)nx * ny * es};
-    cuuint32_t box[3] = {(cuuint32_t)W, 1, 1};
-    box[dir == DY ? 1 : 2] = (cuuint32_t)box_n;
-    cuuint32_t estr[3] = {1, 1, 1};
-    CUresult r = enc(&tmap, sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
-                     const_cast<T *>(in), gdim, gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return X3D_EUNSUPPORTED;
-    auto kern = ls_chunk_yz<T, W, L>;
+    StageMaps maps;
+    for (int ti = 0; ti < prog.ntiles; ++ti) {
+        cuuint64_t gdim[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
+        cuuint64_t gstride[2] = {(cuuint64_t)nx * es, (cuuint64_t)nx * ny * es};
+        cuuint32_t box[3] = {(cuuint32_t)W, 1, 1};
+        box[dir == DY ? 1 : 2] = (cuuint32_t)box_n;
+        cuuint32_t estr[3] = {1, 1, 1};
+        CUresult r = enc(&maps.m[ti],
+                         sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+                         const_cast<T *>(prog.in[ti]), gdim, gstride, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return X3D_EUNSUPPORTED;
+    }
+    auto kern = acc ? ls_stage_yz<T, W, L, true> : ls_stage_yz<T, W, L, false>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const long tiles_x = (nx + W - 1) / W;
     const long grid = tiles_x * (dir == DY ? nz : ny);
     ++ctx->launches;
-    kern<<<(unsigned)grid, threads, smem, st>>>(tmap, ops, nx, ny, dir, box_n, nb, tile, ctx->d_err);
-    return cuda_check(ctx, cudaGetLastError(), "ls_chunk_yz launch");
+    kern<<<(unsigned)grid, threads, smem, st>>>(maps, prog, nx, ny, dir, box_n, nb, tile, ctx->d_err);
+    return cuda_check(ctx, cudaGetLastError(), "ls_stage_yz launch");
 }
 
 template <typename T>
-int launch_chunk(x3d_ctx_s *ctx, const ChunkOps<T> &ops, int dir, const T *in, int nx, int ny, int nz,
-                 int cfg)
+int launch_stage(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir, int nx, int ny, int nz, int cfg)
 {
-    // cfg selects (lines per CTA, chunk length); see chunk_configs().
+    if (prog.nops < 1 || prog.nops > kMaxStageOps || prog.ntiles < 1 || prog.ntiles > kMaxStageTiles)
+        return X3D_EINVAL;
+    // cfg selects (lines per CTA, chunk length).
+    constexpr int Lbig = sizeof(T) == 4 ? 32 : 16;
+    constexpr int Lsmall = sizeof(T) == 4 ? 16 : 8;
     switch (cfg) {
-    case 0: return launch_chunk_cfg<T, 16, (sizeof(T) == 4 ? 32 : 16)>(ctx, ops, dir, in, nx, ny, nz);
-    case 1: return launch_chunk_cfg<T, 32, (sizeof(T) == 4 ? 32 : 16)>(ctx, ops, dir, in, nx, ny, nz);
-    case 2: return launch_chunk_cfg<T, 16, (sizeof(T) == 4 ? 16 : 8)>(ctx, ops, dir, in, nx, ny, nz);
-    case 3: return launch_chunk_cfg<T, 8, (sizeof(T) == 4 ? 32 : 16)>(ctx, ops, dir, in, nx, ny, nz);
+    case 0: return launch_stage_cfg<T, 16, Lbig>(ctx, prog, dir, nx, ny, nz);
+    case 1: return launch_stage_cfg<T, 32, Lbig>(ctx, prog, dir, nx, ny, nz);
+    case 2: return launch_stage_cfg<T, 16, Lsmall>(ctx, prog, dir, nx, ny, nz);
+    case 3: return launch_stage_cfg<T, 8, Lbig>(ctx, prog, dir, nx, ny, nz);
     default: return X3D_EUNSUPPORTED;
     }
 }
 
-template int launch_chunk<float>(x3d_ctx_s *, const ChunkOps<float> &, int, const float *, int, int, int, int);
-template int launch_chunk<double>(x3d_ctx_s *, const ChunkOps<double> &, int, const double *, int, int, int, int);
+template <typename T>
+StageProgram<T> plain_program(const T *in, const LineOp<T> *const *ops, const int *kinds,
+                              void *const *outs, int nops)
+{
+    StageProgram<T> p{};
+    p.nops = nops;
+    p.ntiles = 1;
+    p.in[0] = in;
+    for (int k = 0; k < nops; ++k) {
+        StageOp<T> &so = p.ops[k];
+        so.op = *ops[k];
+        so.kind = kinds[k];
+        so.src_a = 0;
+        so.src_b = -1;
+        so.mul_tile = -1;
+        so.accumulate = 0;
+        so.flush = 1;
+        so.out = outs[k];
+        so.base = nullptr;
+        so.out2 = nullptr;
+        so.base2 = nullptr;
+        so.sign = 1.0;
+        so.scale2 = 0.0;
+        so.out_f64 = 0;
+    }
+    return p;
+}
+
+template int launch_stage<float>(x3d_ctx_s *, const StageProgram<float> &, int, int, int, int, int);
+template int launch_stage<double>(x3d_ctx_s *, const StageProgram<double> &, int, int, int, int, int);
+template StageProgram<float> plain_program<float>(const float *, const LineOp<float> *const *,
+                                                  const int *, void *const *, int);
+template StageProgram<double> plain_program<double>(const double *, const LineOp<double> *const *,
+                                                    const int *, void *const *, int);
 
 }  // namespace x3d

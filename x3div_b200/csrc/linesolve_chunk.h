@@ -1,30 +1,57 @@
-// Chunked line-solve launch interface (linesolve_chunk.cu).
+// Chunked line-solve stage kernels (linesolve_chunk.cu).
 #pragma once
 
 #include "x3d_internal.h"
 
 namespace x3d {
 
-constexpr int kMaxChunkOps = 6;
+constexpr int kMaxStageOps = 6;
+constexpr int kMaxStageTiles = 3;
 
-// Up to six operators applied to the same input field along one direction:
-// one staged read of the field, one write per operator.
+// One operator application inside a stage.  Its input is staged tile src_a,
+// or the pointwise product of tiles src_a and src_b.  The solved values x
+// update a register accumulator: acc = m x (accumulate = 0) or acc += m x,
+// with m = 1 or m = tile[mul_tile] at the same point.  With flush set the
+// accumulator is written out:  out = base + sign * acc  (base may be null,
+// and may alias out), then optionally  out2 = base2 + scale2 * out.
 template <typename T>
-struct ChunkOps {
-    LineOp<T> op[kMaxChunkOps];
-    T *out[kMaxChunkOps];
-    int kind[kMaxChunkOps];
-    int nops;
+struct StageOp {
+    LineOp<T> op;
+    void *out;
+    const void *base;
+    void *out2;
+    const void *base2;
+    double sign, scale2;
+    int kind;
+    short src_a, src_b;
+    short mul_tile;
+    short accumulate;
+    short flush;
+    short out_f64;  // out, base, out2, base2 hold double rather than T
 };
 
-// Number of (lines per CTA, chunk length) configurations launch_chunk knows.
+// Up to six operators along one direction over up to three staged inputs of
+// one (nx, ny, nz) grid: one read of each input, the writes the flushes ask for.
+template <typename T>
+struct StageProgram {
+    StageOp<T> ops[kMaxStageOps];
+    const T *in[kMaxStageTiles];
+    int nops, ntiles;
+};
+
+// Number of (lines per CTA, chunk length) configurations launch_stage knows.
 constexpr int kChunkConfigs = 4;
 
-// Launches the chunked kernel with configuration cfg in [0, kChunkConfigs).
-// Returns X3D_EUNSUPPORTED (nothing launched) when the shape, alignment or
-// shared-memory budget rules that configuration out.
+// Launches the chunked stage kernel with configuration cfg in
+// [0, kChunkConfigs).  Returns X3D_EUNSUPPORTED, launching nothing, when the
+// shape, alignment or shared-memory budget rules that configuration out.
 template <typename T>
-int launch_chunk(x3d_ctx_s *ctx, const ChunkOps<T> &ops, int dir, const T *in, int nx, int ny,
-                 int nz, int cfg);
+int launch_stage(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir, int nx, int ny, int nz,
+                 int cfg);
+
+// A plain program: operator k reads input 0 and writes out[k].
+template <typename T>
+StageProgram<T> plain_program(const T *in, const LineOp<T> *const *ops, const int *kinds,
+                              void *const *outs, int nops);
 
 }  // namespace x3d

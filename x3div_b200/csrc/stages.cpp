@@ -1,0 +1,227 @@
+// Fused stage compositions of the Euler step, built from StageProgram
+// launches (linesolve_chunk.cu).  At the supported 1x1 decomposition every
+// transpose of the reference is a same-layout copy and is elided.
+//
+//   momentum_rhs_eq (src/transeq.f90:44-355): one launch per direction, each
+//     solving d(u_d u_c)/dx_d and d(u_c)/dx_d for the three components and
+//     accumulating  du_c += d(u_d u_c)/dx_d + u_d du_c/dx_d;  with a time step
+//     the z launch also applies int_time (src/time_integrators.f90:41-43),
+//     u_c = dt du_c + u_c, in place.
+//   divergence (src/navier.f90:166-202): x launch derxvp/interxvp/interxvp,
+//     y launch interyvp + deryvp and interyvp, z launch interzvp + derzvp into
+//     the FP64 pressure field.
+//   gradp + cor_vel (src/navier.f90:273-304, :83-87): z launch interzpv and
+//     derzpv, y launch interypv/derypv/interypv, x launch derxpv/interxpv/
+//     interxpv writing px, py, pz and, for cor_vel, u_c -= p_c in place.
+#include <cstring>
+
+#include "linesolve_chunk.h"
+#include "x3d_internal.h"
+
+namespace x3d {
+
+template <typename T>
+static const LineOp<T> &lop(const x3d_op_s *op);
+template <>
+const LineOp<float> &lop<float>(const x3d_op_s *op)
+{
+    return op->opf;
+}
+template <>
+const LineOp<double> &lop<double>(const x3d_op_s *op)
+{
+    return op->opd;
+}
+
+template <typename T>
+static StageOp<T> sop(const x3d_op_s *op, int src_a, int src_b = -1)
+{
+    StageOp<T> s;
+    std::memset(&s, 0, sizeof(s));
+    s.op = lop<T>(op);
+    s.kind = op->h.kind;
+    s.src_a = (short)src_a;
+    s.src_b = (short)src_b;
+    s.mul_tile = -1;
+    s.sign = 1.0;
+    return s;
+}
+
+template <typename T>
+static void set_flush(StageOp<T> &s, void *out, const void *base = nullptr, bool f64 = false)
+{
+    s.flush = 1;
+    s.out = out;
+    s.base = base;
+    s.out_f64 = f64 ? 1 : 0;
+}
+
+// Runs a stage with the tuned (or default) configuration, then the others.
+template <typename T>
+static int run_stage(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir)
+{
+    const int first = ctx->default_cfg < kChunkConfigs ? ctx->default_cfg : 0;
+    int rc = launch_stage<T>(ctx, prog, dir, ctx->nx, ctx->ny, ctx->nz, first);
+    for (int cfg = 0; rc == X3D_EUNSUPPORTED && cfg < kChunkConfigs; ++cfg)
+        if (cfg != first) rc = launch_stage<T>(ctx, prog, dir, ctx->nx, ctx->ny, ctx->nz, cfg);
+    return rc;
+}
+
+static x3d_op_s *B(x3d_ctx_s *ctx, int which) { return ctx->builtin[which]; }
+
+template <typename T>
+static int transeq_t(x3d_ctx_s *ctx, void *const du[3], const void *const u[3], bool step, double dt,
+                     void *const unew[3])
+{
+    const int der_op[3] = {X3D_OP_DERX, X3D_OP_DERY, X3D_OP_DERZ};
+    for (int d = 0; d < 3; ++d) {
+        StageProgram<T> p;
+        std::memset(&p, 0, sizeof(p));
+        p.ntiles = 3;
+        for (int c = 0; c < 3; ++c) p.in[c] = static_cast<const T *>(u[c]);
+        p.nops = 6;
+        for (int c = 0; c < 3; ++c) {
+            // u_d * d(u_c)/dx_d  (e.g. ux1 * derx(ux1), transeq.f90:107,114)
+            StageOp<T> a = sop<T>(B(ctx, der_op[d]), c);
+            a.mul_tile = (short)d;
+            a.accumulate = 0;
+            // + d(u_d u_c)/dx_d   (e.g. derx(ux1*ux1), transeq.f90:101,106)
+            StageOp<T> b = sop<T>(B(ctx, der_op[d]), d, c);
+            b.accumulate = 1;
+            set_flush(b, du[c], d == 0 ? nullptr : du[c]);
+            if (step && d == 2) {
+                b.out2 = unew[c];
+                b.base2 = u[c];
+                b.scale2 = dt;
+            }
+            p.ops[2 * c] = a;
+            p.ops[2 * c + 1] = b;
+        }
+        const int rc = run_stage<T>(ctx, p, d);
+        if (rc) return rc;
+    }
+    return X3D_OK;
+}
+
+template <typename T>
+static int divergence_t(x3d_ctx_s *ctx, double *pp3, const void *const u[3], void *const s[5])
+{
+    StageProgram<T> p;
+    // x pencil: pp1 = derxvp(ux), pgy1 = interxvp(uy), pgz1 = interxvp(uz)
+    std::memset(&p, 0, sizeof(p));
+    p.ntiles = 3;
+    p.nops = 3;
+    for (int c = 0; c < 3; ++c) p.in[c] = static_cast<const T *>(u[c]);
+    p.ops[0] = sop<T>(B(ctx, X3D_OP_DERXVP), 0);
+    set_flush(p.ops[0], s[0]);
+    p.ops[1] = sop<T>(B(ctx, X3D_OP_INTXVP), 1);
+    set_flush(p.ops[1], s[1]);
+    p.ops[2] = sop<T>(B(ctx, X3D_OP_INTXVP), 2);
+    set_flush(p.ops[2], s[2]);
+    int rc = run_stage<T>(ctx, p, DX);
+    if (rc) return rc;
+    // y pencil: duydypi2 = deryvp(pgy1) + interyvp(pp1) ; upi2 = interyvp(pgz1)
+    std::memset(&p, 0, sizeof(p));
+    p.ntiles = 3;
+    p.nops = 3;
+    for (int c = 0; c < 3; ++c) p.in[c] = static_cast<const T *>(s[c]);
+    p.ops[0] = sop<T>(B(ctx, X3D_OP_INTYVP), 0);
+    p.ops[1] = sop<T>(B(ctx, X3D_OP_DERYVP), 1);
+    p.ops[1].accumulate = 1;
+    set_flush(p.ops[1], s[3]);
+    p.ops[2] = sop<T>(B(ctx, X3D_OP_INTYVP), 2);
+    set_flush(p.ops[2], s[4]);
+    rc = run_stage<T>(ctx, p, DY);
+    if (rc) return rc;
+    // z pencil: pp3 = interzvp(duxydxyp3) + derzvp(uzp3), written in FP64
+    std::memset(&p, 0, sizeof(p));
+    p.ntiles = 2;
+    p.nops = 2;
+    p.in[0] = static_cast<const T *>(s[3]);
+    p.in[1] = static_cast<const T *>(s[4]);
+    p.ops[0] = sop<T>(B(ctx, X3D_OP_INTZVP), 0);
+    p.ops[1] = sop<T>(B(ctx, X3D_OP_DERZVP), 1);
+    p.ops[1].accumulate = 1;
+    set_flush(p.ops[1], pp3, nullptr, true);
+    return run_stage<T>(ctx, p, DZ);
+}
+
+template <typename T>
+static int gradp_t(x3d_ctx_s *ctx, void *const px[3], const double *pp3, void *const ucor[3],
+                   void *const s[6])
+{
+    const T *p0 = reinterpret_cast<const T *>(pp3);
+    if (sizeof(T) == 4) {
+        int rc = launch_convert(ctx, s[5], true, pp3, false, ctx->npts());
+        if (rc) return rc;
+        p0 = static_cast<const T *>(s[5]);
+    }
+    StageProgram<T> p;
+    // z pencil: ppi3 = interzpv(pp3), pgz3 = derzpv(pp3)
+    std::memset(&p, 0, sizeof(p));
+    p.ntiles = 1;
+    p.nops = 2;
+    p.in[0] = p0;
+    p.ops[0] = sop<T>(B(ctx, X3D_OP_INTZPV), 0);
+    set_flush(p.ops[0], s[0]);
+    p.ops[1] = sop<T>(B(ctx, X3D_OP_DERZPV), 0);
+    set_flush(p.ops[1], s[1]);
+    int rc = run_stage<T>(ctx, p, DZ);
+    if (rc) return rc;
+    // y pencil: ppi2 = interypv(pp2), pgy2 = derypv(pp2), pgzi2 = interypv(pgz2)
+    std::memset(&p, 0, sizeof(p));
+    p.ntiles = 2;
+    p.nops = 3;
+    p.in[0] = static_cast<const T *>(s[0]);
+    p.in[1] = static_cast<const T *>(s[1]);
+    p.ops[0] = sop<T>(B(ctx, X3D_OP_INTYPV), 0);
+    set_flush(p.ops[0], s[2]);
+    p.ops[1] = sop<T>(B(ctx, X3D_OP_DERYPV), 0);
+    set_flush(p.ops[1], s[3]);
+    p.ops[2] = sop<T>(B(ctx, X3D_OP_INTYPV), 1);
+    set_flush(p.ops[2], s[4]);
+    rc = run_stage<T>(ctx, p, DY);
+    if (rc) return rc;
+    // x pencil: px1 = derxpv(pp1), py1 = interxpv(pgy1), pz1 = interxpv(pgz1);
+    // cor_vel: u_c = u_c - p_c
+    std::memset(&p, 0, sizeof(p));
+    p.ntiles = 3;
+    p.nops = 3;
+    for (int c = 0; c < 3; ++c) p.in[c] = static_cast<const T *>(s[2 + c]);
+    const int xop[3] = {X3D_OP_DERXPV, X3D_OP_INTXPV, X3D_OP_INTXPV};
+    for (int c = 0; c < 3; ++c) {
+        p.ops[c] = sop<T>(B(ctx, xop[c]), c);
+        set_flush(p.ops[c], px[c]);
+        if (ucor) {
+            p.ops[c].out2 = ucor[c];
+            p.ops[c].base2 = ucor[c];
+            p.ops[c].scale2 = -1.0;
+        }
+    }
+    return run_stage<T>(ctx, p, DX);
+}
+
+int fused_transeq(x3d_ctx_s *ctx, void *const du[3], const void *const u[3], bool step, double dt,
+                  void *const unew[3])
+{
+    return ctx->precision == X3D_F32 ? transeq_t<float>(ctx, du, u, step, dt, unew)
+                                     : transeq_t<double>(ctx, du, u, step, dt, unew);
+}
+
+int fused_divergence(x3d_ctx_s *ctx, double *pp3, const void *const u[3])
+{
+    void *s[5];
+    for (int i = 0; i < 5; ++i)
+        if (!(s[i] = ctx_scratch(ctx, i))) return set_error(ctx, X3D_ENOMEM, "scratch allocation failed");
+    return ctx->precision == X3D_F32 ? divergence_t<float>(ctx, pp3, u, s) : divergence_t<double>(ctx, pp3, u, s);
+}
+
+int fused_gradp(x3d_ctx_s *ctx, void *const px[3], const double *pp3, void *const ucor[3])
+{
+    void *s[6];
+    for (int i = 0; i < 6; ++i)
+        if (!(s[i] = ctx_scratch(ctx, i))) return set_error(ctx, X3D_ENOMEM, "scratch allocation failed");
+    return ctx->precision == X3D_F32 ? gradp_t<float>(ctx, px, pp3, ucor, s) : gradp_t<double>(ctx, px, pp3, ucor, s);
+}
+
+}  // namespace x3d

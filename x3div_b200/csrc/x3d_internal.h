@@ -33,7 +33,19 @@ struct LineOp {
     int n;
     int periodic;
     int glen;         // g_i == 0 (in FP64) for i >= glen
+    // Per-point records for the chunked kernels, one table per chunk length
+    // (tab[0] for kChunkLong<T>, tab[1] for kChunkShort<T>), each padded to
+    // whole chunks.  Record i = {s, mf, w, fw, mb, p, 0, 0}: mf is the product
+    // of -s over the chunk up to i, mb the product of -f w from i to the
+    // chunk end.  Padding records {-1, mf_end, 0, 0, 0, 0} carry the last
+    // forward value to the chunk end and keep the backward sweep at zero.
+    const T *tab[2];
 };
+
+template <typename T>
+constexpr int kChunkLong = sizeof(T) == 4 ? 32 : 16;
+template <typename T>
+constexpr int kChunkShort = sizeof(T) == 4 ? 16 : 8;
 
 // Host-side operator: FP64 contents of x3doperator1d plus the RHS scalars.
 struct OpHost {
@@ -108,6 +120,12 @@ int launch_group(x3d_ctx_s *ctx, int dir, const void *in, const x3d_op_s *const 
                  const int *kinds, void *const *outs, int nops, int nx, int ny, int nz, bool fp32);
 int autotune_group(x3d_ctx_s *ctx, int dir, const void *in, const x3d_op_s *const *ops,
                    const int *kinds, void *const *outs, int nops, bool fp32, int reps, float *best_ms);
+
+// ---- fused stages (stages.cpp); X3D_EUNSUPPORTED when no fused kernel fits --
+int fused_transeq(x3d_ctx_s *ctx, void *const du[3], const void *const u[3], bool step, double dt,
+                  void *const unew[3]);
+int fused_divergence(x3d_ctx_s *ctx, double *pp3, const void *const u[3]);
+int fused_gradp(x3d_ctx_s *ctx, void *const px[3], const double *pp3, void *const ucor[3]);
 
 // ---- elementwise / reductions / transposes (fields.cu) ------------------
 int launch_copy(x3d_ctx_s *ctx, void *dst, const void *src, size_t bytes);
