@@ -197,14 +197,46 @@ int x3d_apply_batch(x3d_ctx ctx, const x3d_work *items, int count);
  * fields; not callable during stream capture.  Without it a fixed default
  * configuration is used.  No reference counterpart. */
 int x3d_autotune(x3d_ctx ctx, int max_group);
-/* Force kernel configuration cfg (0..3 chunked, 4 one thread per line) for
+/* Force kernel configuration cfg (0..5 chunked, 6 one thread per line) for
  * every later call and forget tuned choices; -1 restores the default.  A
  * configuration that cannot handle a call (alignment, shared memory) still
  * falls back to one that can.  No reference counterpart. */
 int x3d_ctx_set_kernel(x3d_ctx ctx, int cfg);
 /* The configuration chosen for (direction, group size): *cfg = -1 when not
- * tuned, 0..3 chunked variants, 4 one thread per line. */
+ * tuned, 0..5 chunked variants, 6 one thread per line. */
 int x3d_autotune_choice(x3d_ctx ctx, int dir, int group, int *cfg);
+
+/* ---- batches of independent boxes ----------------------------------------- */
+
+/* A periodic box of a batch (no reference counterpart: the reference runs one
+ * box per job; a batch sweeps many uneven boxes in one launch). */
+typedef struct {
+    int nx, ny, nz;
+    double xlx, yly, zlz;
+} x3d_box;
+typedef struct x3d_batch_s *x3d_batch;
+
+int x3d_batch_create(x3d_batch *batch, const x3d_box *boxes, int nboxes, int precision, int device);
+int x3d_batch_destroy(x3d_batch batch);
+/* NULL is the legacy default stream; a new batch uses its own stream. */
+int x3d_batch_set_stream(x3d_batch batch, void *stream);
+const char *x3d_batch_last_error(x3d_batch batch);
+/* Binds the derivative sweep: for box i and field f < nfields, input
+ * fields[i*nfields + f] (device, the box's grid) and, for direction d and
+ * operator family k < nops (X3D_KIND order: der, der2, dervp, derpv, intvp,
+ * intpv), output outs[((i*nfields + f)*3 + d)*6 + k].  Plans the persistent
+ * work-list (tiles, tensor maps) once; outputs must not alias inputs. */
+int x3d_batch_bind_sweep(x3d_batch batch, int nfields, void *const *fields, void *const *outs, int nops);
+/* One persistent launch over every tile of every bound job (boxes the
+ * persistent kernel cannot take run as grouped launches after it). */
+int x3d_batch_run(x3d_batch batch);
+/* Captures x3d_batch_run into a CUDA graph; x3d_batch_replay launches it. */
+int x3d_batch_capture(x3d_batch batch);
+int x3d_batch_replay(x3d_batch batch);
+int x3d_batch_sync(x3d_batch batch);
+/* points = operator-application points per run; tiles, jobs in the
+ * persistent launch; fallback_jobs run as grouped launches. */
+int x3d_batch_info(x3d_batch batch, long long *points, long long *tiles, int *jobs, int *fallback_jobs);
 
 /* ---- batched Thomas line solves: module thomas (src/thomas.f90:15-28) --- */
 

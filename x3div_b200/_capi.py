@@ -63,6 +63,16 @@ SIGNATURES = {
     "x3d_autotune": [_vp, _i],
     "x3d_ctx_set_kernel": [_vp, _i],
     "x3d_autotune_choice": [_vp, _i, _i, _ip],
+    "x3d_batch_create": [ctypes.POINTER(_vp), _vp, _i, _i, _i],
+    "x3d_batch_destroy": [_vp],
+    "x3d_batch_set_stream": [_vp, _vp],
+    "x3d_batch_last_error": [_vp],
+    "x3d_batch_bind_sweep": [_vp, _i, _vp, _vp, _i],
+    "x3d_batch_run": [_vp],
+    "x3d_batch_capture": [_vp],
+    "x3d_batch_replay": [_vp],
+    "x3d_batch_sync": [_vp],
+    "x3d_batch_info": [_vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong), _ip, _ip],
     "x3d_xthomas": [_vp, _vp, _vp, _vp, _vp, _vp, _d, _i, _i, _i],
     "x3d_ythomas": [_vp, _vp, _vp, _vp, _vp, _vp, _d, _i, _i, _i],
     "x3d_zthomas": [_vp, _vp, _vp, _vp, _vp, _vp, _d, _i, _i, _i],
@@ -82,6 +92,11 @@ SIGNATURES = {
     "x3d_vel": [_vp, _vp, _vp, _vp],
     "x3d_test_rms": [_vp, _i, _vp, _dp],
 }
+
+class Box(ctypes.Structure):
+    """x3d_box: one periodic box of a batch."""
+    _fields_ = [("nx", _i), ("ny", _i), ("nz", _i), ("xlx", _d), ("yly", _d), ("zlz", _d)]
+
 
 class Work(ctypes.Structure):
     """x3d_work: one item of an x3d_apply_batch work-list."""
@@ -108,6 +123,6 @@ def lib() -> ctypes.CDLL:
         for name, args in SIGNATURES.items():
             fn = getattr(L, name)
             fn.argtypes = args
-            fn.restype = ctypes.c_char_p if name == "x3d_ctx_last_error" else ctypes.c_int
+            fn.restype = ctypes.c_char_p if name.endswith("_last_error") else ctypes.c_int
         _lib = L
     return _lib

@@ -240,7 +240,7 @@ class Context:
         self._check(self.L.x3d_autotune(self.handle, int(max_group)))
 
     def set_kernel(self, cfg):
-        """Force a kernel configuration (0..3 chunked, 4 thread per line, -1 default)."""
+        """Force a kernel configuration (0..5 chunked, 6 thread per line, -1 default)."""
         self._check(self.L.x3d_ctx_set_kernel(self.handle, int(cfg)))
 
     def autotune_choice(self, direction, group):
@@ -328,3 +328,76 @@ def to_device(a: np.ndarray, dtype=None, device="cuda"):
 def to_host(t) -> np.ndarray:
     """Contiguous (nz, ny, nx) torch tensor -> Fortran-ordered (nx, ny, nz) numpy array."""
     return np.asfortranarray(t.detach().cpu().numpy().transpose(2, 1, 0))
+
+
+class Batch:
+    """Independent periodic boxes swept in one persistent launch (x3d_batch).
+
+    boxes: iterable of (nx, ny, nz) or (nx, ny, nz, xlx, yly, zlz)."""
+
+    def __init__(self, boxes, precision="f32", device=0, stream=None):
+        self.L = _capi.lib()
+        self.boxes = [tuple(b) + (2 * np.pi,) * (6 - len(b)) for b in boxes]
+        arr = (_capi.Box * len(self.boxes))()
+        for k, b in enumerate(self.boxes):
+            arr[k].nx, arr[k].ny, arr[k].nz = (int(v) for v in b[:3])
+            arr[k].xlx, arr[k].yly, arr[k].zlz = (float(v) for v in b[3:])
+        h = ctypes.c_void_p()
+        rc = self.L.x3d_batch_create(ctypes.byref(h), arr, len(self.boxes),
+                                     X3D_F32 if precision == "f32" else X3D_F64, int(device))
+        if rc != 0:
+            raise X3DError(rc, "x3d_batch_create failed")
+        self.handle = h.value
+        if stream is None:
+            stream = _torch_current_stream()
+        if stream is not None:
+            self._check(self.L.x3d_batch_set_stream(self.handle, getattr(stream, "cuda_stream", stream)))
+
+    def _check(self, rc):
+        if rc != 0:
+            msg = self.L.x3d_batch_last_error(self.handle) or b""
+            raise X3DError(rc, msg.decode(errors="replace"))
+
+    def bind_sweep(self, fields, outs, nops=6):
+        """fields[i][f]: field f of box i; outs[i][f][d][k]: operator family k along d."""
+        nf = len(fields[0])
+        fin = (ctypes.c_void_p * (len(fields) * nf))()
+        fout = (ctypes.c_void_p * (len(fields) * nf * 18))()
+        for i, fs in enumerate(fields):
+            for f, a in enumerate(fs):
+                fin[i * nf + f] = _ptr(a)
+                for d in range(3):
+                    for k in range(nops):
+                        fout[((i * nf + f) * 3 + d) * 6 + k] = _ptr(outs[i][f][d][k])
+        self._keep = (fin, fout)
+        self._check(self.L.x3d_batch_bind_sweep(self.handle, nf, fin, fout, int(nops)))
+
+    def run(self):
+        self._check(self.L.x3d_batch_run(self.handle))
+
+    def capture(self):
+        self._check(self.L.x3d_batch_capture(self.handle))
+
+    def replay(self):
+        self._check(self.L.x3d_batch_replay(self.handle))
+
+    def sync(self):
+        self._check(self.L.x3d_batch_sync(self.handle))
+
+    def info(self):
+        p, t = ctypes.c_longlong(), ctypes.c_longlong()
+        j, fb = ctypes.c_int(), ctypes.c_int()
+        self._check(self.L.x3d_batch_info(self.handle, ctypes.byref(p), ctypes.byref(t), ctypes.byref(j),
+                                          ctypes.byref(fb)))
+        return dict(points=p.value, tiles=t.value, jobs=j.value, fallback_jobs=fb.value)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.L.x3d_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,329 @@
+// Batches of independent periodic boxes of uneven sizes: the derivative
+// sweep of every box in one persistent launch (BatchJob work-list, see
+// linesolve_chunk.cu), capturable as a CUDA graph.  Boxes of one shape share
+// a context, hence its FP64 operator precompute.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <new>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "linesolve_chunk.h"
+#include "x3d_internal.h"
+
+using namespace x3d;
+
+struct x3d_batch_s {
+    int precision = X3D_F32;
+    int device = 0;
+    int num_sms = 148;
+    size_t smem_optin = 0;
+    std::vector<x3d_box> boxes;
+    std::vector<x3d_ctx> shape_ctx;  // owned, one per distinct (dims, lengths)
+    std::vector<int> box_shape;      // box -> shape_ctx index
+    cudaStream_t own_stream = nullptr, stream = nullptr;
+    unsigned long long *d_counter = nullptr;
+    int *d_err = nullptr;
+    void *d_jobs = nullptr;
+    size_t jobs_cap = 0;
+    int njobs = 0;
+    long total_tiles = 0;
+    size_t tile_cap = 0;
+    int grid = 0;
+    // jobs the persistent kernel cannot take run as per-box grouped launches
+    struct Fallback {
+        int box, dir;
+        const void *in;
+        const x3d_op_s *ops[6];
+        int kinds[6];
+        void *outs[6];
+        int nops;
+    };
+    std::vector<Fallback> fallback;
+    long long points = 0;  // operator-application points per run
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    std::string last_error;
+};
+
+namespace {
+
+int bfail(x3d_batch_s *b, int code, const std::string &msg)
+{
+    if (b) b->last_error = msg;
+    return code;
+}
+
+template <typename T>
+const LineOp<T> &lop(const x3d_op_s *op);
+template <>
+const LineOp<float> &lop<float>(const x3d_op_s *op)
+{
+    return op->opf;
+}
+template <>
+const LineOp<double> &lop<double>(const x3d_op_s *op)
+{
+    return op->opd;
+}
+
+template <typename T>
+int bind_typed(x3d_batch_s *b, int nfields, void *const *fields, void *const *outs, int nops_per_dir)
+{
+    std::vector<BatchJob<T>> jobs;
+    b->fallback.clear();
+    b->points = 0;
+    size_t tile_cap = 0;
+    long tiles = 0;
+    const int kinds[6] = {DER, DER2, DERVP, DERPV, INTVP, INTPV};
+    for (size_t i = 0; i < b->boxes.size(); ++i) {
+        x3d_ctx_s *ctx = b->shape_ctx[b->box_shape[i]];
+        const int dims[3] = {ctx->nx, ctx->ny, ctx->nz};
+        for (int f = 0; f < nfields; ++f) {
+            const void *in = fields[i * nfields + f];
+            for (int d = 0; d < 3; ++d) {
+                BatchJob<T> J;
+                std::memset(&J, 0, sizeof(J));
+                J.in = static_cast<const T *>(in);
+                J.nops = nops_per_dir;
+                J.dir = d;
+                J.n = dims[d];
+                J.nx = dims[0];
+                J.ny = dims[1];
+                J.nz = dims[2];
+                typename x3d_batch_s::Fallback fb{};
+                fb.box = (int)i;
+                fb.dir = d;
+                fb.in = in;
+                fb.nops = nops_per_dir;
+                for (int k = 0; k < nops_per_dir; ++k) {
+                    const x3d_op_s *op = nullptr;
+                    for (int w = 0; w < X3D_OP_COUNT; ++w)
+                        if (ctx->builtin[w]->h.kind == kinds[k] && ctx->builtin[w]->h.dir == d) {
+                            op = ctx->builtin[w];
+                            break;
+                        }
+                    J.op[k] = lop<T>(op);
+                    J.kind[k] = kinds[k];
+                    J.out[k] = static_cast<T *>(outs[((i * nfields + f) * 3 + d) * 6 + k]);
+                    fb.ops[k] = op;
+                    fb.kinds[k] = kinds[k];
+                    fb.outs[k] = J.out[k];
+                }
+                b->points += (long long)nops_per_dir * dims[0] * dims[1] * dims[2];
+                size_t tb = 0;
+                if (plan_batch_job<T>(J, kChunkLong<T>, &tb)) {
+                    J.tile0 = tiles;
+                    tiles += J.ntiles;
+                    tile_cap = std::max(tile_cap, tb);
+                    jobs.push_back(J);
+                } else {
+                    b->fallback.push_back(fb);
+                }
+            }
+        }
+    }
+    b->njobs = (int)jobs.size();
+    b->total_tiles = tiles;
+    b->tile_cap = tile_cap;
+    if (!jobs.empty()) {
+        const size_t bytes = jobs.size() * sizeof(BatchJob<T>);
+        if (bytes > b->jobs_cap) {
+            if (b->d_jobs) cudaFree(b->d_jobs);
+            b->d_jobs = nullptr;
+            b->jobs_cap = 0;
+            if (cudaMalloc(&b->d_jobs, bytes) != cudaSuccess) return bfail(b, X3D_ENOMEM, "job list allocation failed");
+            b->jobs_cap = bytes;
+        }
+        if (cudaMemcpy(b->d_jobs, jobs.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+            return bfail(b, X3D_ECUDA, "job list upload failed");
+        const int rc = prepare_batch<T>(tile_cap, b->smem_optin, b->num_sms, &b->grid);
+        if (rc) {
+            b->njobs = 0;
+            b->total_tiles = 0;
+            return bfail(b, rc, "batch kernel cannot fit its tiles in shared memory");
+        }
+    }
+    return X3D_OK;
+}
+
+template <typename T>
+int run_typed(x3d_batch_s *b)
+{
+    if (b->njobs > 0) {
+        const int rc = launch_batch<T>(b->stream, b->grid, static_cast<const BatchJob<T> *>(b->d_jobs), b->njobs,
+                                       b->total_tiles, b->d_counter, b->tile_cap, b->d_err);
+        if (rc) return bfail(b, rc, std::string("batch launch failed: ") + cudaGetErrorString(cudaGetLastError()));
+    }
+    for (auto &fb : b->fallback) {
+        x3d_ctx_s *ctx = b->shape_ctx[b->box_shape[fb.box]];
+        cudaStream_t keep = ctx->stream;
+        ctx->stream = b->stream;
+        const int rc = launch_group(ctx, fb.dir, fb.in, fb.ops, fb.kinds, fb.outs, fb.nops, ctx->nx, ctx->ny,
+                                    ctx->nz, b->precision == X3D_F32);
+        ctx->stream = keep;
+        if (rc) return bfail(b, rc, ctx->last_error);
+    }
+    return X3D_OK;
+}
+
+void drop_graph(x3d_batch_s *b)
+{
+    if (b->gexec) cudaGraphExecDestroy(b->gexec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->gexec = nullptr;
+    b->graph = nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+int x3d_batch_create(x3d_batch *out, const x3d_box *boxes, int nboxes, int precision, int device)
+{
+    if (!out || !boxes || nboxes < 1) return X3D_EINVAL;
+    *out = nullptr;
+    if (precision != X3D_F32 && precision != X3D_F64) return X3D_EINVAL;
+    if (cudaSetDevice(device) != cudaSuccess) return X3D_ECUDA;
+    auto *b = new (std::nothrow) x3d_batch_s;
+    if (!b) return X3D_ENOMEM;
+    b->precision = precision;
+    b->device = device;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+        delete b;
+        return X3D_ECUDA;
+    }
+    b->num_sms = prop.multiProcessorCount;
+    b->smem_optin = prop.sharedMemPerBlockOptin;
+    std::map<std::tuple<int, int, int, double, double, double>, int> shapes;
+    for (int i = 0; i < nboxes; ++i) {
+        const x3d_box &bx = boxes[i];
+        const auto key = std::make_tuple(bx.nx, bx.ny, bx.nz, bx.xlx, bx.yly, bx.zlz);
+        auto it = shapes.find(key);
+        if (it == shapes.end()) {
+            x3d_ctx c = nullptr;
+            const int rc = x3d_ctx_create(&c, bx.nx, bx.ny, bx.nz, bx.xlx, bx.yly, bx.zlz, precision, device);
+            if (rc) {
+                x3d_batch_destroy(b);
+                return rc;
+            }
+            it = shapes.emplace(key, (int)b->shape_ctx.size()).first;
+            b->shape_ctx.push_back(c);
+        }
+        b->boxes.push_back(bx);
+        b->box_shape.push_back(it->second);
+    }
+    if (cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&b->d_counter, sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMalloc(&b->d_err, sizeof(int)) != cudaSuccess) {
+        x3d_batch_destroy(b);
+        return X3D_ECUDA;
+    }
+    cudaMemset(b->d_err, 0, sizeof(int));
+    b->stream = b->own_stream;
+    *out = b;
+    return X3D_OK;
+}
+
+int x3d_batch_destroy(x3d_batch b)
+{
+    if (!b) return X3D_EINVAL;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    drop_graph(b);
+    for (x3d_ctx c : b->shape_ctx) x3d_ctx_destroy(c);
+    if (b->d_jobs) cudaFree(b->d_jobs);
+    if (b->d_counter) cudaFree(b->d_counter);
+    if (b->d_err) cudaFree(b->d_err);
+    if (b->own_stream) cudaStreamDestroy(b->own_stream);
+    delete b;
+    return X3D_OK;
+}
+
+int x3d_batch_set_stream(x3d_batch b, void *stream)
+{
+    if (!b) return X3D_EINVAL;
+    b->stream = static_cast<cudaStream_t>(stream);
+    drop_graph(b);
+    return X3D_OK;
+}
+
+const char *x3d_batch_last_error(x3d_batch b) { return b ? b->last_error.c_str() : "null batch"; }
+
+int x3d_batch_bind_sweep(x3d_batch b, int nfields, void *const *fields, void *const *outs, int nops)
+{
+    if (!b || nfields < 1 || !fields || !outs || nops < 1 || nops > 6) return X3D_EINVAL;
+    cudaSetDevice(b->device);
+    const size_t nin = b->boxes.size() * (size_t)nfields;
+    for (size_t i = 0; i < nin; ++i)
+        if (!fields[i]) return bfail(b, X3D_EINVAL, "null input field");
+    for (size_t i = 0; i < nin * 18; ++i)
+        if ((int)(i % 6) < nops && !outs[i]) return bfail(b, X3D_EINVAL, "null output field");
+    drop_graph(b);
+    return b->precision == X3D_F32 ? bind_typed<float>(b, nfields, fields, outs, nops)
+                                   : bind_typed<double>(b, nfields, fields, outs, nops);
+}
+
+int x3d_batch_run(x3d_batch b)
+{
+    if (!b) return X3D_EINVAL;
+    cudaSetDevice(b->device);
+    return b->precision == X3D_F32 ? run_typed<float>(b) : run_typed<double>(b);
+}
+
+int x3d_batch_capture(x3d_batch b)
+{
+    if (!b) return X3D_EINVAL;
+    cudaSetDevice(b->device);
+    drop_graph(b);
+    if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return bfail(b, X3D_ECUDA, "stream capture could not start");
+    const int rc = x3d_batch_run(b);
+    const cudaError_t e = cudaStreamEndCapture(b->stream, &b->graph);
+    if (rc) return rc;
+    if (e != cudaSuccess) return bfail(b, X3D_ECUDA, "stream capture failed");
+    if (cudaGraphInstantiate(&b->gexec, b->graph, 0) != cudaSuccess) {
+        drop_graph(b);
+        return bfail(b, X3D_ECUDA, "graph instantiation failed");
+    }
+    return X3D_OK;
+}
+
+int x3d_batch_replay(x3d_batch b)
+{
+    if (!b) return X3D_EINVAL;
+    if (!b->gexec) return bfail(b, X3D_EINVAL, "no captured graph");
+    cudaSetDevice(b->device);
+    return cudaGraphLaunch(b->gexec, b->stream) == cudaSuccess ? X3D_OK : bfail(b, X3D_ECUDA, "graph launch failed");
+}
+
+int x3d_batch_sync(x3d_batch b)
+{
+    if (!b) return X3D_EINVAL;
+    cudaSetDevice(b->device);
+    if (cudaStreamSynchronize(b->stream) != cudaSuccess) return bfail(b, X3D_ECUDA, "batch stream sync failed");
+    int flag = 0;
+    cudaMemcpy(&flag, b->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (flag) {
+        cudaMemset(b->d_err, 0, sizeof(int));
+        return bfail(b, X3D_ETIMEOUT, "a device-side bounded wait gave up");
+    }
+    return X3D_OK;
+}
+
+int x3d_batch_info(x3d_batch b, long long *points, long long *tiles, int *jobs, int *fallback_jobs)
+{
+    if (!b) return X3D_EINVAL;
+    if (points) *points = b->points;
+    if (tiles) *tiles = b->total_tiles;
+    if (jobs) *jobs = b->njobs;
+    if (fallback_jobs) *fallback_jobs = (int)b->fallback.size();
+    return X3D_OK;
+}
+
+}  // extern "C"

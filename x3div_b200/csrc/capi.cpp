@@ -9,6 +9,7 @@
 #include <string>
 #include <vector>
 
+#include "linesolve_chunk.h"
 #include "x3d_internal.h"
 
 using namespace x3d;
@@ -551,7 +552,7 @@ int x3d_autotune(x3d_ctx ctx, int max_group)
 
 int x3d_ctx_set_kernel(x3d_ctx ctx, int cfg)
 {
-    if (!ctx || cfg < -1 || cfg > 4) return X3D_EINVAL;
+    if (!ctx || cfg < -1 || cfg > kChunkConfigs) return X3D_EINVAL;
     ctx->tuned.clear();
     ctx->default_cfg = cfg < 0 ? 0 : cfg;
     return X3D_OK;

@@ -140,6 +140,34 @@ void finish_op(OpHost &op)
         op.den = 1.0;
 }
 
+// Scan depths for chunk length L: smallest k such that any k consecutive
+// chunk multipliers multiply to below 1e-20 (capped at the chunk count).
+static void scan_depths(const std::vector<double> &t, int n, int L, int *kf, int *kb)
+{
+    const int C = (n + L - 1) / L;
+    std::vector<double> fm(C), bm(C);
+    for (int c = 0; c < C; ++c) {
+        fm[c] = std::fabs(t[(size_t)(c * L + L - 1) * 8 + 1]);
+        bm[c] = std::fabs(t[(size_t)(c * L) * 8 + 4]);
+    }
+    auto depth = [&](const std::vector<double> &m) {
+        int k = 1;
+        for (int c = 0; c < C; ++c) {
+            double prod = 1.0;
+            int d = 0;
+            for (int j = c; j < C && prod >= 1e-20; ++j) {
+                prod *= m[j];
+                ++d;
+            }
+            if (prod >= 1e-20) d = C;  // reaches the end of the line
+            k = std::max(k, d);
+        }
+        return std::min(k, C);
+    };
+    *kf = depth(fm);
+    *kb = depth(bm);
+}
+
 // Chunk record table of one operator for chunk length L (see LineOp::tab).
 static std::vector<double> chunk_table(const OpHost &h, int L)
 {
@@ -233,6 +261,10 @@ int upload_op(x3d_op_s *op)
     };
     fill(op->opf, df);
     fill(op->opd, dd);
+    scan_depths(tf0, n, kChunkLong<float>, &op->opf.kf[0], &op->opf.kb[0]);
+    scan_depths(tf1, n, kChunkShort<float>, &op->opf.kf[1], &op->opf.kb[1]);
+    scan_depths(td0, n, kChunkLong<double>, &op->opd.kf[0], &op->opd.kb[0]);
+    scan_depths(td1, n, kChunkShort<double>, &op->opd.kf[1], &op->opd.kb[1]);
     op->opf.tab[0] = reinterpret_cast<const float *>(base + o_tf0);
     op->opf.tab[1] = reinterpret_cast<const float *>(base + o_tf1);
     op->opd.tab[0] = reinterpret_cast<const double *>(base + o_td0);

@@ -38,6 +38,8 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
+
 #include "linesolve_chunk.h"
 #include "ptx.cuh"
 #include "x3d_internal.h"
@@ -119,10 +121,11 @@ struct Rec<double> {
 // window is dead once the stencil is evaluated.  tab is this chunk length's
 // record table (records padded to whole chunks, so the sweeps need no
 // bounds tests: padding keeps the forward value and zeroes the backward one).
-template <typename T, int W, int L, typename Load>
+template <typename T, int L, typename Load>
 __device__ __forceinline__ void chunk_solve(const LineOp<T> &op, const T *tab, int kind,
                                             const Load &load, T (&r)[L], const ChunkScratch<T> &sc,
-                                            int l, int c, int C, int cs, int nv)
+                                            int W, int l, int c, int C, int cs, int nv, int q,
+                                            bool active)
 {
     {
         T w[L + 8];
@@ -147,19 +150,20 @@ __device__ __forceinline__ void chunk_solve(const LineOp<T> &op, const T *tab, i
         zh = r[j] - Rec<T>::s(t + 8 * j) * zh;
         r[j] = zh;
     }
-    const int q = c * W + l;
     const T fme = __ldg(t + 8 * (L - 1) + 1);  // product of -s over the chunk
     sc.fz[q] = zh;
     sc.fm[q] = fme;
     sc.fg[q] = gp;
     __syncthreads();
-    // forward carry: z at the end of chunk c-1
+    // forward carry: z at the end of chunk c-1 (earlier chunks contribute
+    // below 1e-20 beyond kf chunks)
+    const int ti = L == kChunkLong<T> ? 0 : 1;
     T carry = T(0);
-    for (int cc = 0; cc < c; ++cc) {
+    for (int cc = max(0, c - op.kf[ti]); cc < c; ++cc) {
         const int qq = cc * W + l;
         carry = sc.fz[qq] + sc.fm[qq] * carry;
     }
-    if (c == C - 1) {
+    if (active && c == C - 1) {
         // last chunk: z_{n-1} (carried to the padded end), y_0, and the
         // Sherman-Morrison scalar for the whole line
         const T zlast = zh + fme * carry;
@@ -183,7 +187,7 @@ __device__ __forceinline__ void chunk_solve(const LineOp<T> &op, const T *tab, i
     sc.bm[q] = __ldg(t + 4);  // product of -f w over the chunk
     __syncthreads();
     T bcarry = T(0);
-    for (int cc = C - 1; cc > c; --cc) {
+    for (int cc = min(C - 1, c + op.kb[ti]); cc > c; --cc) {
         const int qq = cc * W + l;
         bcarry = sc.bz[qq] + sc.bm[qq] * bcarry;
     }
@@ -254,7 +258,7 @@ __device__ __forceinline__ void flush_point(const StageOp<T> &so, size_t p, T a)
 }
 
 template <typename T, int W, int L, bool ACC>
-__global__ void __launch_bounds__(512, 1) ls_stage_yz(const __grid_constant__ StageMaps maps,
+__global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1)) ls_stage_yz(const __grid_constant__ StageMaps maps,
                                                    const __grid_constant__ StageProgram<T> prog,
                                                    int nx, int ny, int dir, int box_n, int nbox,
                                                    size_t tile_bytes, int *err)
@@ -318,7 +322,7 @@ __global__ void __launch_bounds__(512, 1) ls_stage_yz(const __grid_constant__ St
                 w[j] = cb ? ca[idx * W] * cb[idx * W] : ca[idx * W];
             }
         };
-        chunk_solve<T, W, L>(so.op, so.op.tab[L == kChunkLong<T> ? 0 : 1], so.kind, load, r, sc, l, c, C, cs, nv);
+        chunk_solve<T, L>(so.op, so.op.tab[L == kChunkLong<T> ? 0 : 1], so.kind, load, r, sc, W, l, c, C, cs, nv, c * W + l, true);
         if constexpr (ACC) accumulate<T, L>(so, acc, r, nv, tile_at);
         const T *res;
         if constexpr (ACC) res = acc;
@@ -398,7 +402,7 @@ __device__ __forceinline__ void flush_vec(const StageOp<T> &so, size_t p0, const
 }
 
 template <typename T, int W, int L, bool ACC>
-__global__ void __launch_bounds__(512, 1) ls_stage_x(const __grid_constant__ StageProgram<T> prog,
+__global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1)) ls_stage_x(const __grid_constant__ StageProgram<T> prog,
                                                   long nlines, int pitch, size_t tile_bytes, int *err)
 {
     using VT = typename Vec4<T>::type;
@@ -463,7 +467,7 @@ __global__ void __launch_bounds__(512, 1) ls_stage_x(const __grid_constant__ Sta
                 }
             }
         };
-        chunk_solve<T, W, L>(so.op, so.op.tab[L == kChunkLong<T> ? 0 : 1], so.kind, load, r, sc, l, c, C, cs, nv);
+        chunk_solve<T, L>(so.op, so.op.tab[L == kChunkLong<T> ? 0 : 1], so.kind, load, r, sc, W, l, c, C, cs, nv, c * W + l, true);
         if constexpr (ACC) accumulate<T, L>(so, acc, r, nv, tile_at);
         const T *res;
         if constexpr (ACC) res = acc;
@@ -591,6 +595,8 @@ int launch_stage(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir, int nx, i
     case 1: return launch_stage_cfg<T, 32, Lbig>(ctx, prog, dir, nx, ny, nz);
     case 2: return launch_stage_cfg<T, 16, Lsmall>(ctx, prog, dir, nx, ny, nz);
     case 3: return launch_stage_cfg<T, 8, Lbig>(ctx, prog, dir, nx, ny, nz);
+    case 4: return launch_stage_cfg<T, 32, Lsmall>(ctx, prog, dir, nx, ny, nz);
+    case 5: return launch_stage_cfg<T, 8, Lsmall>(ctx, prog, dir, nx, ny, nz);
     default: return X3D_EUNSUPPORTED;
     }
 }
@@ -622,6 +628,244 @@ StageProgram<T> plain_program(const T *in, const LineOp<T> *const *ops, const in
     }
     return p;
 }
+
+// ---------------------------------------------------------------------------
+// Batches of uneven boxes: one persistent launch applies the operator groups
+// of every (box, field, direction) job.  CTAs pull tiles from a global
+// counter, so boxes of different sizes balance across the SMs; each tile
+// uses its job's lines per tile (W), chunk count (C), tensor map or padded
+// rows.  Threads beyond W*C of a job idle through its barriers.
+template <typename T, int L>
+__global__ void __launch_bounds__(kBatchThreads, 2)
+    ls_batch(const BatchJob<T> *__restrict__ jobs, int njobs, long total,
+             unsigned long long *counter, size_t tile_cap, int *err)
+{
+    using VT = typename Vec4<T>::type;
+    constexpr int V = Vec4<T>::N;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ uint64_t bar;
+    __shared__ long s_item;
+    const int t = threadIdx.x;
+    if (t == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    uint32_t phase = 0;
+    T *tile = reinterpret_cast<T *>(smem_raw);
+    const ChunkScratch<T> scf = carve_scratch<T>(smem_raw + tile_cap, kBatchThreads / 1, 1);
+    for (;;) {
+        if (t == 0) s_item = (long)atomicAdd(counter, 1ull);
+        __syncthreads();
+        const long item = s_item;
+        if (item >= total) break;
+        int lo = 0, hi = njobs - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (jobs[mid].tile0 <= item) lo = mid;
+            else hi = mid - 1;
+        }
+        const BatchJob<T> &J = jobs[lo];
+        const long tl = item - J.tile0;
+        const int W = J.W, C = J.C, n = J.n;
+        const int dir = J.dir;
+        long l0 = 0;
+        int rows = W, x0 = 0, o = 0;
+        if (dir == DX) {
+            l0 = tl * W;
+            rows = (int)min((long)W, J.span - l0);
+        } else {
+            x0 = (int)(tl % J.span) * W;
+            o = (int)(tl / J.span);
+        }
+        if (t == 0) {
+            if (dir == DX) {
+                const uint32_t row_bytes = (uint32_t)(n * sizeof(T));
+                mbar_arrive_expect_tx(&bar, row_bytes * (uint32_t)rows);
+                for (int rr = 0; rr < rows; ++rr)
+                    bulk_load(tile + (size_t)rr * J.pitch, J.in + (size_t)(l0 + rr) * n, row_bytes, &bar);
+            } else {
+                fence_tensormap_acquire(&J.tmap);
+                mbar_arrive_expect_tx(&bar, (uint32_t)((size_t)J.nbox * J.box_n * W * sizeof(T)));
+                for (int b = 0; b < J.nbox; ++b) {
+                    if (dir == DY)
+                        tma_load_3d(tile + (size_t)b * J.box_n * W, &J.tmap, &bar, x0, b * J.box_n, o);
+                    else
+                        tma_load_3d(tile + (size_t)b * J.box_n * W, &J.tmap, &bar, x0, o, b * J.box_n);
+                }
+            }
+        }
+        const bool ok = mbar_wait_bounded(&bar, phase, kChunkWaitNs);
+        if (!__syncthreads_and(ok)) {
+            if (t == 0) atomicExch(err, 1);
+            mbar_wait_bounded(&bar, phase, kChunkWaitNs);
+            return;
+        }
+        phase ^= 1;
+        const bool active = t < W * C;
+        const int l = active ? t % W : 0, c = active ? t / W : 0;
+        const int q = t;  // scratch slot: active threads use c*W + l == t
+        ChunkScratch<T> sc = scf;
+        const int cs = c * L;
+        const int nv = min(L, n - cs);
+        T r[L];
+        if (dir == DX) {
+            const int lr = l < rows ? l : 0;
+            const T *row = tile + (size_t)lr * J.pitch;
+            auto load = [&](T(&w)[L + 8]) {
+#pragma unroll
+                for (int j = 0; j < L + 8; j += V) {
+                    int idx = (cs - 4 + j) % n;
+                    idx = idx < 0 ? idx + n : idx;
+                    const VT qa = *reinterpret_cast<const VT *>(row + idx);
+                    const T *ea = reinterpret_cast<const T *>(&qa);
+#pragma unroll
+                    for (int v = 0; v < V; ++v) w[j + v] = ea[v];
+                }
+            };
+            for (int k = 0; k < J.nops; ++k) {
+                chunk_solve<T, L>(J.op[k], J.op[k].tab[L == kChunkLong<T> ? 0 : 1], J.kind[k], load, r, sc,
+                                  W, l, c, C, cs, nv, q, active);
+                if (active && l < rows) {
+                    T *dst = J.out[k] + (size_t)(l0 + l) * n + cs;
+#pragma unroll
+                    for (int j = 0; j < L; j += V) {
+                        if (j < nv) {
+                            VT qv;
+                            T *e = reinterpret_cast<T *>(&qv);
+#pragma unroll
+                            for (int v = 0; v < V; ++v) e[v] = r[j + v];
+                            *reinterpret_cast<VT *>(dst + j) = qv;
+                        }
+                    }
+                }
+            }
+        } else {
+            const T *col = tile + l;
+            const bool wraps = cs < 4 || cs + L + 4 > n;
+            auto load = [&](T(&w)[L + 8]) {
+#pragma unroll
+                for (int j = 0; j < L + 8; ++j) {
+                    int idx = cs - 4 + j;
+                    if (wraps) {
+                        idx %= n;
+                        idx = idx < 0 ? idx + n : idx;
+                    }
+                    w[j] = col[idx * W];
+                }
+            };
+            const bool live = active && x0 + l < J.nx;
+            const size_t ostride = dir == DY ? (size_t)J.nx : (size_t)J.nx * J.ny;
+            const size_t obase = (size_t)(x0 + l) +
+                                 (dir == DY ? (size_t)J.nx * J.ny * o : (size_t)J.nx * o) +
+                                 (size_t)cs * ostride;
+            for (int k = 0; k < J.nops; ++k) {
+                chunk_solve<T, L>(J.op[k], J.op[k].tab[L == kChunkLong<T> ? 0 : 1], J.kind[k], load, r, sc,
+                                  W, l, c, C, cs, nv, q, active);
+                if (live) {
+                    T *dst = J.out[k] + obase;
+#pragma unroll
+                    for (int j = 0; j < L; ++j) {
+                        if (j < nv) *dst = r[j];
+                        dst += ostride;
+                    }
+                }
+            }
+        }
+    }
+}
+
+static int gcd_int(int a, int b) { return b ? gcd_int(b, a % b) : a; }
+
+// Fills the geometry, tiling and staging fields of a job; false when the
+// job's box cannot take the chunked batch kernel.
+template <typename T>
+bool plan_batch_job(BatchJob<T> &J, int L, size_t *tile_bytes)
+{
+    const size_t es = sizeof(T);
+    const int n = J.n;
+    constexpr int V = Vec4<T>::N;
+    J.C = (n + L - 1) / L;
+    if (J.C > kBatchThreads) return false;
+    int W = kBatchThreads / J.C;
+    const int wq = (int)(16 / es);  // TMA inner extent: multiple of 16 bytes
+    W = std::max(wq, W / wq * wq);
+    if (W * J.C > kBatchThreads || W > 256) return false;
+    J.W = W;
+    if (J.dir == DX) {
+        if (n % V || (reinterpret_cast<uintptr_t>(J.in) & 15)) return false;
+        int pitch = n + V;
+        while (((size_t)pitch * es / 16) % 2 == 0) pitch += V;
+        J.pitch = pitch;
+        J.span = (long)J.ny * J.nz;
+        J.ntiles = (J.span + W - 1) / W;
+        *tile_bytes = ((size_t)W * pitch * es + 127) & ~(size_t)127;
+        return true;
+    }
+    if (((size_t)J.nx * es) % 16) return false;
+    const int nb = (n + 255) / 256;
+    int box_n = (n + nb - 1) / nb;
+    const int align_rows = 128 / gcd_int(128, (int)(W * es));
+    box_n = (box_n + align_rows - 1) / align_rows * align_rows;
+    if (box_n > 256) return false;
+    J.box_n = box_n;
+    J.nbox = nb;
+    J.span = (J.nx + W - 1) / W;
+    J.ntiles = J.span * (J.dir == DY ? J.nz : J.ny);
+    *tile_bytes = ((size_t)nb * box_n * W * es + 127) & ~(size_t)127;
+    auto enc = encode_tiled();
+    if (!enc) return false;
+    cuuint64_t gdim[3] = {(cuuint64_t)J.nx, (cuuint64_t)J.ny, (cuuint64_t)J.nz};
+    cuuint64_t gstride[2] = {(cuuint64_t)J.nx * es, (cuuint64_t)J.nx * J.ny * es};
+    cuuint32_t box[3] = {(cuuint32_t)W, 1, 1};
+    box[J.dir == DY ? 1 : 2] = (cuuint32_t)box_n;
+    cuuint32_t estr[3] = {1, 1, 1};
+    return enc(&J.tmap, sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+               const_cast<T *>(J.in), gdim, gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <typename T>
+size_t batch_scratch_bytes()
+{
+    return (((size_t)4 * kBatchThreads * sizeof(T) + 15) & ~(size_t)15) +
+           (size_t)(kBatchThreads + kBatchThreads) * sizeof(double);
+}
+
+template <typename T>
+int prepare_batch(size_t tile_cap, size_t smem_optin, int num_sms, int *grid)
+{
+    const size_t smem = tile_cap + batch_scratch_bytes<T>();
+    if (smem + 1024 > smem_optin) return X3D_EUNSUPPORTED;
+    auto kern = ls_batch<T, kChunkLong<T>>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return X3D_ECUDA;
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBatchThreads, smem);
+    *grid = num_sms * (per_sm < 1 ? 1 : per_sm);
+    return X3D_OK;
+}
+
+template <typename T>
+int launch_batch(cudaStream_t st, int grid, const BatchJob<T> *d_jobs, int njobs, long total,
+                 unsigned long long *d_counter, size_t tile_cap, int *d_err)
+{
+    const size_t smem = tile_cap + batch_scratch_bytes<T>();
+    if (cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), st) != cudaSuccess) return X3D_ECUDA;
+    ls_batch<T, kChunkLong<T>><<<(unsigned)grid, kBatchThreads, smem, st>>>(d_jobs, njobs, total, d_counter,
+                                                                             tile_cap, d_err);
+    return cudaGetLastError() == cudaSuccess ? X3D_OK : X3D_ECUDA;
+}
+
+template bool plan_batch_job<float>(BatchJob<float> &, int, size_t *);
+template bool plan_batch_job<double>(BatchJob<double> &, int, size_t *);
+template int prepare_batch<float>(size_t, size_t, int, int *);
+template int prepare_batch<double>(size_t, size_t, int, int *);
+template int launch_batch<float>(cudaStream_t, int, const BatchJob<float> *, int, long, unsigned long long *,
+                                 size_t, int *);
+template int launch_batch<double>(cudaStream_t, int, const BatchJob<double> *, int, long, unsigned long long *,
+                                  size_t, int *);
 
 template int launch_stage<float>(x3d_ctx_s *, const StageProgram<float> &, int, int, int, int, int);
 template int launch_stage<double>(x3d_ctx_s *, const StageProgram<double> &, int, int, int, int, int);

@@ -1,6 +1,8 @@
 // Chunked line-solve stage kernels (linesolve_chunk.cu).
 #pragma once
 
+#include <cuda.h>
+
 #include "x3d_internal.h"
 
 namespace x3d {
@@ -40,7 +42,7 @@ struct StageProgram {
 };
 
 // Number of (lines per CTA, chunk length) configurations launch_stage knows.
-constexpr int kChunkConfigs = 4;
+constexpr int kChunkConfigs = 6;
 
 // Launches the chunked stage kernel with configuration cfg in
 // [0, kChunkConfigs).  Returns X3D_EUNSUPPORTED, launching nothing, when the
@@ -48,6 +50,42 @@ constexpr int kChunkConfigs = 4;
 template <typename T>
 int launch_stage(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir, int nx, int ny, int nz,
                  int cfg);
+
+// One job of a box batch: up to six operators applied along one direction to
+// one field of one box.  Filled on the host, read by the persistent batch
+// kernel from device memory (the tensor map first, for its 64-byte alignment).
+constexpr int kBatchThreads = 256;
+
+template <typename T>
+struct BatchJob {
+    CUtensorMap tmap;  // y/z input map
+    const T *in;
+    T *out[kMaxStageOps];
+    LineOp<T> op[kMaxStageOps];
+    int kind[kMaxStageOps];
+    int nops, dir, n, nx, ny, nz;
+    int W, C, box_n, nbox, pitch;
+    long span;   // x: number of lines; y/z: tiles across x
+    long tile0;  // first work item of the job
+    long ntiles;
+};
+
+// Chooses tiling for the job (chunk length L) and encodes its tensor map;
+// false when the batch kernel cannot take the job.
+template <typename T>
+bool plan_batch_job(BatchJob<T> &J, int L, size_t *tile_bytes);
+
+// Sets the batch kernel's shared-memory attribute for tiles up to tile_cap
+// bytes and returns the persistent grid (SMs x resident CTAs per SM).
+template <typename T>
+int prepare_batch(size_t tile_cap, size_t smem_optin, int num_sms, int *grid);
+
+// One persistent launch over every tile of every job (jobs and counter in
+// device memory; the counter is reset by the launch itself, so the pair of
+// operations can be captured in a CUDA graph and replayed).
+template <typename T>
+int launch_batch(cudaStream_t st, int grid, const BatchJob<T> *d_jobs, int njobs, long total,
+                 unsigned long long *d_counter, size_t tile_cap, int *d_err);
 
 // A plain program: operator k reads input 0 and writes out[k].
 template <typename T>

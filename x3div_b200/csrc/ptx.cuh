@@ -72,6 +72,13 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
         : "memory");
 }
 
+// Orders a tensor map that lives in global memory (written before the
+// launch) before the async proxy reads it.
+__device__ __forceinline__ void fence_tensormap_acquire(const void *map)
+{
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
+}
+
 // 1-D bulk copy global -> this CTA's shared memory (16-byte aligned, size % 16 == 0).
 __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
 {

@@ -40,6 +40,10 @@ struct LineOp {
     // chunk end.  Padding records {-1, mf_end, 0, 0, 0, 0} carry the last
     // forward value to the chunk end and keep the backward sweep at zero.
     const T *tab[2];
+    // Scan depths per table: the carry into a chunk only needs the previous
+    // kf (next kb) chunks, beyond which the product of chunk multipliers is
+    // below 1e-20 and the dropped terms are under FP64 resolution.
+    int kf[2], kb[2];
 };
 
 template <typename T>
