@@ -197,13 +197,14 @@ int x3d_apply_batch(x3d_ctx ctx, const x3d_work *items, int count);
  * fields; not callable during stream capture.  Without it a fixed default
  * configuration is used.  No reference counterpart. */
 int x3d_autotune(x3d_ctx ctx, int max_group);
-/* Force kernel configuration cfg (0..5 chunked, 6 one thread per line) for
+/* Force kernel configuration cfg (0..5 chunked, one CTA per tile;
+ * 6..11 the same shapes as persistent double-buffered kernels; 12 one thread per line) for
  * every later call and forget tuned choices; -1 restores the default.  A
  * configuration that cannot handle a call (alignment, shared memory) still
  * falls back to one that can.  No reference counterpart. */
 int x3d_ctx_set_kernel(x3d_ctx ctx, int cfg);
 /* The configuration chosen for (direction, group size): *cfg = -1 when not
- * tuned, 0..5 chunked variants, 6 one thread per line. */
+ * tuned, 0..11 chunked variants, 12 one thread per line. */
 int x3d_autotune_choice(x3d_ctx ctx, int dir, int group, int *cfg);
 
 /* ---- batches of independent boxes ----------------------------------------- */
@@ -230,7 +231,9 @@ int x3d_batch_bind_sweep(x3d_batch batch, int nfields, void *const *fields, void
 /* One persistent launch over every tile of every bound job (boxes the
  * persistent kernel cannot take run as grouped launches after it). */
 int x3d_batch_run(x3d_batch batch);
-/* Captures x3d_batch_run into a CUDA graph; x3d_batch_replay launches it. */
+/* Captures x3d_batch_run into a CUDA graph (on the batch's own stream, after
+ * waiting for the current one); x3d_batch_replay launches the graph on the
+ * stream set with x3d_batch_set_stream. */
 int x3d_batch_capture(x3d_batch batch);
 int x3d_batch_replay(x3d_batch batch);
 int x3d_batch_sync(x3d_batch batch);

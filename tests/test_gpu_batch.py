@@ -8,7 +8,8 @@ from conftest import rel_err, seeded_field
 pytestmark = pytest.mark.gpu
 
 KINDS = ["der", "der2", "dervp", "derpv", "intvp", "intpv"]
-# (18, 12, 10): x not a multiple of 4, so the box runs through the fallback launches
+# (18, 12, 10): in FP32 its rows are 72 bytes, not a multiple of 16, so the box
+# runs through the fallback launches; in FP64 (144-byte rows) it joins the batch
 BOXES = [(16, 16, 16), (24, 20, 12), (32, 8, 16), (64, 40, 24), (18, 12, 10), (96, 36, 20)]
 
 
@@ -28,7 +29,7 @@ def test_batch_sweep_matches_oracle(oracle, torch_cuda, prec):
     batch = Batch(BOXES, precision=prec)
     batch.bind_sweep(fields, outs)
     info = batch.info()
-    assert info["fallback_jobs"] == 3 * nf  # only the odd box
+    assert info["fallback_jobs"] == (3 * nf if prec == "f32" else 0)  # only the odd box
     assert info["points"] == 18 * nf * sum(b[0] * b[1] * b[2] for b in BOXES)
 
     def check():

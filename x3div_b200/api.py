@@ -240,7 +240,7 @@ class Context:
         self._check(self.L.x3d_autotune(self.handle, int(max_group)))
 
     def set_kernel(self, cfg):
-        """Force a kernel configuration (0..5 chunked, 6 thread per line, -1 default)."""
+        """Force a kernel configuration (0..11 chunked, 12 thread per line, -1 default)."""
         self._check(self.L.x3d_ctx_set_kernel(self.handle, int(cfg)))
 
     def autotune_choice(self, direction, group):

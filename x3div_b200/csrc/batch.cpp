@@ -281,10 +281,18 @@ int x3d_batch_capture(x3d_batch b)
     if (!b) return X3D_EINVAL;
     cudaSetDevice(b->device);
     drop_graph(b);
-    if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+    // Capture on the batch's own stream (the legacy default stream cannot be
+    // captured); x3d_batch_replay launches the graph on the batch's stream.
+    cudaStream_t user = b->stream;
+    if (cudaStreamSynchronize(user) != cudaSuccess) return bfail(b, X3D_ECUDA, "stream sync failed");
+    b->stream = b->own_stream;
+    if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        b->stream = user;
         return bfail(b, X3D_ECUDA, "stream capture could not start");
+    }
     const int rc = x3d_batch_run(b);
     const cudaError_t e = cudaStreamEndCapture(b->stream, &b->graph);
+    b->stream = user;
     if (rc) return rc;
     if (e != cudaSuccess) return bfail(b, X3D_ECUDA, "stream capture failed");
     if (cudaGraphInstantiate(&b->gexec, b->graph, 0) != cudaSuccess) {

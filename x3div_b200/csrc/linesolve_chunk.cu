@@ -257,95 +257,114 @@ __device__ __forceinline__ void flush_point(const StageOp<T> &so, size_t p, T a)
     }
 }
 
-template <typename T, int W, int L, bool ACC>
-__global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1)) ls_stage_yz(const __grid_constant__ StageMaps maps,
-                                                   const __grid_constant__ StageProgram<T> prog,
-                                                   int nx, int ny, int dir, int box_n, int nbox,
-                                                   size_t tile_bytes, int *err)
+// PERSIST: a CTA loops over tiles with two staging slots, issuing the loads
+// of tile k+1 before computing tile k; otherwise one CTA per tile.
+template <typename T, int W, int L, bool ACC, bool PERSIST>
+__global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
+    ls_stage_yz(const __grid_constant__ StageMaps maps, const __grid_constant__ StageProgram<T> prog, int nx,
+                int ny, int dir, int box_n, int nbox, size_t tile_bytes, long ntiles, int *err)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    __shared__ uint64_t bar;
+    __shared__ uint64_t bars[2];
     const int n = prog.ops[0].op.n;
     const int C = blockDim.x / W;
     const int t = threadIdx.x;
     const int l = t % W, c = t / W;
     const int tiles_x = (nx + W - 1) / W;
-    const int x0 = (blockIdx.x % tiles_x) * W;
-    const int o = blockIdx.x / tiles_x;
+    const size_t slot_bytes = (size_t)prog.ntiles * tile_bytes;
     if (t == 0) {
-        mbar_init(&bar, 1);
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
         fence_mbar_init();
     }
     __syncthreads();
-    if (t == 0) {
-        mbar_arrive_expect_tx(&bar, (uint32_t)((size_t)prog.ntiles * nbox * box_n * W * sizeof(T)));
+    auto issue = [&](long tile, int slot) {
+        const int x0 = (int)(tile % tiles_x) * W;
+        const int o = (int)(tile / tiles_x);
+        uint64_t *bar = &bars[slot];
+        mbar_arrive_expect_tx(bar, (uint32_t)((size_t)prog.ntiles * nbox * box_n * W * sizeof(T)));
         for (int ti = 0; ti < prog.ntiles; ++ti) {
-            T *tile = reinterpret_cast<T *>(smem_raw + ti * tile_bytes);
+            T *tp = reinterpret_cast<T *>(smem_raw + slot * slot_bytes + ti * tile_bytes);
             for (int b = 0; b < nbox; ++b) {
                 if (dir == DY)
-                    tma_load_3d(tile + (size_t)b * box_n * W, &maps.m[ti], &bar, x0, b * box_n, o);
+                    tma_load_3d(tp + (size_t)b * box_n * W, &maps.m[ti], bar, x0, b * box_n, o);
                 else
-                    tma_load_3d(tile + (size_t)b * box_n * W, &maps.m[ti], &bar, x0, o, b * box_n);
+                    tma_load_3d(tp + (size_t)b * box_n * W, &maps.m[ti], bar, x0, o, b * box_n);
             }
         }
-    }
-    const bool ok = mbar_wait_bounded(&bar, 0, kChunkWaitNs);
-    if (!__syncthreads_and(ok)) {
-        if (t == 0) atomicExch(err, 1);
-        mbar_wait_bounded(&bar, 0, kChunkWaitNs);
-        return;
-    }
-    const ChunkScratch<T> sc = carve_scratch<T>(smem_raw + prog.ntiles * tile_bytes, C, W);
+    };
+    const ChunkScratch<T> sc = carve_scratch<T>(smem_raw + (PERSIST ? 2 : 1) * slot_bytes, C, W);
     const int cs = c * L;
     const int nv = min(L, n - cs);
     const bool wraps = cs < 4 || cs + L + 4 > n;
-    auto col = [&](int ti) { return reinterpret_cast<const T *>(smem_raw + ti * tile_bytes) + l; };
-    auto tile_at = [&](int ti, int j) { return col(ti)[(cs + j) * W]; };
-    const bool live = x0 + l < nx;
     const size_t ostride = dir == DY ? (size_t)nx : (size_t)nx * ny;
-    const size_t obase = (size_t)(x0 + l) + (dir == DY ? (size_t)nx * ny * o : (size_t)nx * o) +
-                         (size_t)cs * ostride;
-    T r[L];
-    T acc[ACC ? L : 1];
-    for (int k = 0; k < prog.nops; ++k) {
-        const StageOp<T> &so = prog.ops[k];
-        const T *ca = col(so.src_a);
-        const T *cb = so.src_b >= 0 ? col(so.src_b) : nullptr;
-        auto load = [&](T(&w)[L + 8]) {
+    const long step = PERSIST ? (long)gridDim.x : ntiles;
+    long tile = blockIdx.x;
+    if (t == 0 && tile < ntiles) issue(tile, 0);
+    for (int it = 0; tile < ntiles; ++it, tile += step) {
+        const int slot = PERSIST ? (it & 1) : 0;
+        const bool pre = PERSIST && tile + step < ntiles;
+        if (t == 0 && pre) issue(tile + step, slot ^ 1);
+        const uint32_t parity = PERSIST ? ((it >> 1) & 1) : 0;
+        const bool ok = mbar_wait_bounded(&bars[slot], parity, kChunkWaitNs);
+        if (!__syncthreads_and(ok)) {
+            if (t == 0) atomicExch(err, 1);
+            mbar_wait_bounded(&bars[slot], parity, kChunkWaitNs);
+            if (pre) mbar_wait_bounded(&bars[slot ^ 1], ((it + 1) >> 1) & 1, kChunkWaitNs);
+            return;
+        }
+        const int x0 = (int)(tile % tiles_x) * W;
+        const int o = (int)(tile / tiles_x);
+        const unsigned char *base = smem_raw + slot * slot_bytes;
+        auto col = [&](int ti) { return reinterpret_cast<const T *>(base + ti * tile_bytes) + l; };
+        auto tile_at = [&](int ti, int j) { return col(ti)[(cs + j) * W]; };
+        const bool live = x0 + l < nx;
+        const size_t obase = (size_t)(x0 + l) + (dir == DY ? (size_t)nx * ny * o : (size_t)nx * o) +
+                             (size_t)cs * ostride;
+        T r[L];
+        T acc[ACC ? L : 1];
+        for (int k = 0; k < prog.nops; ++k) {
+            const StageOp<T> &so = prog.ops[k];
+            const T *ca = col(so.src_a);
+            const T *cb = so.src_b >= 0 ? col(so.src_b) : nullptr;
+            auto load = [&](T(&w)[L + 8]) {
 #pragma unroll
-            for (int j = 0; j < L + 8; ++j) {
-                int idx = cs - 4 + j;
-                if (wraps) {
-                    idx %= n;
-                    idx = idx < 0 ? idx + n : idx;
+                for (int j = 0; j < L + 8; ++j) {
+                    int idx = cs - 4 + j;
+                    if (wraps) {
+                        idx %= n;
+                        idx = idx < 0 ? idx + n : idx;
+                    }
+                    w[j] = cb ? ca[idx * W] * cb[idx * W] : ca[idx * W];
                 }
-                w[j] = cb ? ca[idx * W] * cb[idx * W] : ca[idx * W];
-            }
-        };
-        chunk_solve<T, L>(so.op, so.op.tab[L == kChunkLong<T> ? 0 : 1], so.kind, load, r, sc, W, l, c, C, cs, nv, c * W + l, true);
-        if constexpr (ACC) accumulate<T, L>(so, acc, r, nv, tile_at);
-        const T *res;
-        if constexpr (ACC) res = acc;
-        else res = r;
-        if (so.flush && live) {
-            if (!so.base && !so.out2 && !so.out_f64 && so.sign == 1.0) {
-                T *dst = static_cast<T *>(so.out) + obase;
+            };
+            chunk_solve<T, L>(so.op, so.op.tab[L == kChunkLong<T> ? 0 : 1], so.kind, load, r, sc, W, l, c, C, cs,
+                              nv, c * W + l, true);
+            if constexpr (ACC) accumulate<T, L>(so, acc, r, nv, tile_at);
+            const T *res;
+            if constexpr (ACC) res = acc;
+            else res = r;
+            if (so.flush && live) {
+                if (!so.base && !so.out2 && !so.out_f64 && so.sign == 1.0) {
+                    T *dst = static_cast<T *>(so.out) + obase;
 #pragma unroll
-                for (int j = 0; j < L; ++j) {
-                    if (j < nv) *dst = res[j];
-                    dst += ostride;
-                }
-            } else {
+                    for (int j = 0; j < L; ++j) {
+                        if (j < nv) *dst = res[j];
+                        dst += ostride;
+                    }
+                } else {
 #pragma unroll
-                for (int j = 0; j < L; ++j) {
-                    if (j < nv) {
-                        const size_t p = obase + (size_t)j * ostride;
-                        if (so.out_f64) flush_point<T, double>(so, p, res[j]);
-                        else flush_point<T, T>(so, p, res[j]);
+                    for (int j = 0; j < L; ++j) {
+                        if (j < nv) {
+                            const size_t p = obase + (size_t)j * ostride;
+                            if (so.out_f64) flush_point<T, double>(so, p, res[j]);
+                            else flush_point<T, T>(so, p, res[j]);
+                        }
                     }
                 }
             }
         }
+        if (PERSIST) __syncthreads();  // the slot is refilled two tiles later
     }
 }
 
@@ -401,87 +420,104 @@ __device__ __forceinline__ void flush_vec(const StageOp<T> &so, size_t p0, const
     }
 }
 
-template <typename T, int W, int L, bool ACC>
-__global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1)) ls_stage_x(const __grid_constant__ StageProgram<T> prog,
-                                                  long nlines, int pitch, size_t tile_bytes, int *err)
+template <typename T, int W, int L, bool ACC, bool PERSIST>
+__global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
+    ls_stage_x(const __grid_constant__ StageProgram<T> prog, long nlines, int pitch, size_t tile_bytes,
+               long ntiles, int *err)
 {
     using VT = typename Vec4<T>::type;
     constexpr int V = Vec4<T>::N;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    __shared__ uint64_t bar;
+    __shared__ uint64_t bars[2];
     const int n = prog.ops[0].op.n;
     const int C = blockDim.x / W;
     const int t = threadIdx.x;
     const int l = t % W, c = t / W;
-    const long l0 = (long)blockIdx.x * W;
-    const int rows = (int)min((long)W, nlines - l0);
     const uint32_t row_bytes = (uint32_t)(n * sizeof(T));
+    const size_t slot_bytes = (size_t)prog.ntiles * tile_bytes;
     if (t == 0) {
-        mbar_init(&bar, 1);
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
         fence_mbar_init();
     }
     __syncthreads();
-    if (t == 0) {
-        mbar_arrive_expect_tx(&bar, row_bytes * (uint32_t)rows * (uint32_t)prog.ntiles);
+    auto issue = [&](long tile, int slot) {
+        const long l0 = tile * W;
+        const int rows = (int)min((long)W, nlines - l0);
+        uint64_t *bar = &bars[slot];
+        mbar_arrive_expect_tx(bar, row_bytes * (uint32_t)rows * (uint32_t)prog.ntiles);
         for (int ti = 0; ti < prog.ntiles; ++ti) {
-            T *tile = reinterpret_cast<T *>(smem_raw + ti * tile_bytes);
+            T *tp = reinterpret_cast<T *>(smem_raw + slot * slot_bytes + ti * tile_bytes);
             for (int rr = 0; rr < rows; ++rr)
-                bulk_load(tile + (size_t)rr * pitch, prog.in[ti] + (size_t)(l0 + rr) * n, row_bytes, &bar);
+                bulk_load(tp + (size_t)rr * pitch, prog.in[ti] + (size_t)(l0 + rr) * n, row_bytes, bar);
         }
-    }
-    const bool ok = mbar_wait_bounded(&bar, 0, kChunkWaitNs);
-    if (!__syncthreads_and(ok)) {
-        if (t == 0) atomicExch(err, 1);
-        mbar_wait_bounded(&bar, 0, kChunkWaitNs);
-        return;
-    }
-    const ChunkScratch<T> sc = carve_scratch<T>(smem_raw + prog.ntiles * tile_bytes, C, W);
+    };
+    const ChunkScratch<T> sc = carve_scratch<T>(smem_raw + (PERSIST ? 2 : 1) * slot_bytes, C, W);
     const int cs = c * L;
     const int nv = min(L, n - cs);
-    const int lr = l < rows ? l : 0;  // rows past the end compute on row 0 and store nothing
-    auto row = [&](int ti) {
-        return reinterpret_cast<const T *>(smem_raw + ti * tile_bytes) + (size_t)lr * pitch;
-    };
-    auto tile_at = [&](int ti, int j) { return row(ti)[cs + j]; };
-    T r[L];
-    T acc[ACC ? L : 1];
-    for (int k = 0; k < prog.nops; ++k) {
-        const StageOp<T> &so = prog.ops[k];
-        const T *ra = row(so.src_a);
-        const T *rb = so.src_b >= 0 ? row(so.src_b) : nullptr;
-        auto load = [&](T(&w)[L + 8]) {
+    const long step = PERSIST ? (long)gridDim.x : ntiles;
+    long tile = blockIdx.x;
+    if (t == 0 && tile < ntiles) issue(tile, 0);
+    for (int it = 0; tile < ntiles; ++it, tile += step) {
+        const int slot = PERSIST ? (it & 1) : 0;
+        const bool pre = PERSIST && tile + step < ntiles;
+        if (t == 0 && pre) issue(tile + step, slot ^ 1);
+        const uint32_t parity = PERSIST ? ((it >> 1) & 1) : 0;
+        const bool ok = mbar_wait_bounded(&bars[slot], parity, kChunkWaitNs);
+        if (!__syncthreads_and(ok)) {
+            if (t == 0) atomicExch(err, 1);
+            mbar_wait_bounded(&bars[slot], parity, kChunkWaitNs);
+            if (pre) mbar_wait_bounded(&bars[slot ^ 1], ((it + 1) >> 1) & 1, kChunkWaitNs);
+            return;
+        }
+        const long l0 = tile * W;
+        const int rows = (int)min((long)W, nlines - l0);
+        const int lr = l < rows ? l : 0;  // rows past the end compute on row 0 and store nothing
+        const unsigned char *base = smem_raw + slot * slot_bytes;
+        auto row = [&](int ti) { return reinterpret_cast<const T *>(base + ti * tile_bytes) + (size_t)lr * pitch; };
+        auto tile_at = [&](int ti, int j) { return row(ti)[cs + j]; };
+        T r[L];
+        T acc[ACC ? L : 1];
+        for (int k = 0; k < prog.nops; ++k) {
+            const StageOp<T> &so = prog.ops[k];
+            const T *ra = row(so.src_a);
+            const T *rb = so.src_b >= 0 ? row(so.src_b) : nullptr;
+            auto load = [&](T(&w)[L + 8]) {
 #pragma unroll
-            for (int j = 0; j < L + 8; j += V) {
-                int idx = (cs - 4 + j) % n;
-                idx = idx < 0 ? idx + n : idx;
-                const VT qa = *reinterpret_cast<const VT *>(ra + idx);
-                const T *ea = reinterpret_cast<const T *>(&qa);
-                if (rb) {
-                    const VT qb = *reinterpret_cast<const VT *>(rb + idx);
-                    const T *eb = reinterpret_cast<const T *>(&qb);
+                for (int j = 0; j < L + 8; j += V) {
+                    int idx = (cs - 4 + j) % n;
+                    idx = idx < 0 ? idx + n : idx;
+                    const VT qa = *reinterpret_cast<const VT *>(ra + idx);
+                    const T *ea = reinterpret_cast<const T *>(&qa);
+                    if (rb) {
+                        const VT qb = *reinterpret_cast<const VT *>(rb + idx);
+                        const T *eb = reinterpret_cast<const T *>(&qb);
 #pragma unroll
-                    for (int v = 0; v < V; ++v) w[j + v] = ea[v] * eb[v];
-                } else {
+                        for (int v = 0; v < V; ++v) w[j + v] = ea[v] * eb[v];
+                    } else {
 #pragma unroll
-                    for (int v = 0; v < V; ++v) w[j + v] = ea[v];
+                        for (int v = 0; v < V; ++v) w[j + v] = ea[v];
+                    }
                 }
-            }
-        };
-        chunk_solve<T, L>(so.op, so.op.tab[L == kChunkLong<T> ? 0 : 1], so.kind, load, r, sc, W, l, c, C, cs, nv, c * W + l, true);
-        if constexpr (ACC) accumulate<T, L>(so, acc, r, nv, tile_at);
-        const T *res;
-        if constexpr (ACC) res = acc;
-        else res = r;
-        if (so.flush && l < rows) {
-            const size_t p0 = (size_t)(l0 + l) * n + cs;
+            };
+            chunk_solve<T, L>(so.op, so.op.tab[L == kChunkLong<T> ? 0 : 1], so.kind, load, r, sc, W, l, c, C, cs,
+                              nv, c * W + l, true);
+            if constexpr (ACC) accumulate<T, L>(so, acc, r, nv, tile_at);
+            const T *res;
+            if constexpr (ACC) res = acc;
+            else res = r;
+            if (so.flush && l < rows) {
+                const size_t p0 = (size_t)(l0 + l) * n + cs;
 #pragma unroll
-            for (int j = 0; j < L; j += V) {
-                if (j < nv) {
-                    if (so.out_f64) flush_vec<T, double, V>(so, p0 + j, res + j);
-                    else flush_vec<T, T, V>(so, p0 + j, res + j);
+                for (int j = 0; j < L; j += V) {
+                    if (j < nv) {
+                        if (so.out_f64) flush_vec<T, double, V>(so, p0 + j, res + j);
+                        else flush_vec<T, T, V>(so, p0 + j, res + j);
+                    }
                 }
             }
         }
+        if (PERSIST) __syncthreads();  // the slot is refilled two tiles later
     }
 }
 
@@ -514,7 +550,16 @@ static bool al16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) =
 
 static bool plain(const StageOpView &v) { return v.flush && !v.accumulate && v.mul_tile < 0; }
 
-template <typename T, int W, int L>
+template <typename Kern>
+static unsigned persistent_grid(x3d_ctx_s *ctx, Kern kern, int threads, size_t smem, long ntiles)
+{
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+    const long g = (long)ctx->num_sms * (per_sm < 1 ? 1 : per_sm);
+    return (unsigned)(g < ntiles ? g : ntiles);
+}
+
+template <typename T, int W, int L, bool PERSIST>
 static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir, int nx, int ny,
                             int nz)
 {
@@ -540,13 +585,15 @@ static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir
         int pitch = n + V;
         while (((size_t)pitch * es / 16) % 2 == 0) pitch += V;
         const size_t tile = ((size_t)W * pitch * es + 127) & ~(size_t)127;
-        const size_t smem = prog.ntiles * tile + scratch_bytes(C, W, es);
+        const size_t smem = (PERSIST ? 2 : 1) * prog.ntiles * tile + scratch_bytes(C, W, es);
         if (smem + 1024 > ctx->smem_optin) return X3D_EUNSUPPORTED;
-        auto kern = acc ? ls_stage_x<T, W, L, true> : ls_stage_x<T, W, L, false>;
+        auto kern = acc ? ls_stage_x<T, W, L, true, PERSIST> : ls_stage_x<T, W, L, false, PERSIST>;
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         const long nlines = (long)ny * nz;
+        const long ntiles = (nlines + W - 1) / W;
+        const unsigned grid = PERSIST ? persistent_grid(ctx, kern, threads, smem, ntiles) : (unsigned)ntiles;
         ++ctx->launches;
-        kern<<<(unsigned)((nlines + W - 1) / W), threads, smem, st>>>(prog, nlines, pitch, tile, ctx->d_err);
+        kern<<<grid, threads, smem, st>>>(prog, nlines, pitch, tile, ntiles, ctx->d_err);
         return cuda_check(ctx, cudaGetLastError(), "ls_stage_x launch");
     }
     auto enc = encode_tiled();
@@ -557,7 +604,7 @@ static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir
     box_n = (box_n + align_rows - 1) / align_rows * align_rows;
     if (box_n > 256) return X3D_EUNSUPPORTED;
     const size_t tile = ((size_t)nb * box_n * W * es + 127) & ~(size_t)127;
-    const size_t smem = prog.ntiles * tile + scratch_bytes(C, W, es);
+    const size_t smem = (PERSIST ? 2 : 1) * prog.ntiles * tile + scratch_bytes(C, W, es);
     if (smem + 1024 > ctx->smem_optin) return X3D_EUNSUPPORTED;
     StageMaps maps;
     for (int ti = 0; ti < prog.ntiles; ++ti) {
@@ -573,12 +620,13 @@ static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir
                          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
         if (r != CUDA_SUCCESS) return X3D_EUNSUPPORTED;
     }
-    auto kern = acc ? ls_stage_yz<T, W, L, true> : ls_stage_yz<T, W, L, false>;
+    auto kern = acc ? ls_stage_yz<T, W, L, true, PERSIST> : ls_stage_yz<T, W, L, false, PERSIST>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const long tiles_x = (nx + W - 1) / W;
-    const long grid = tiles_x * (dir == DY ? nz : ny);
+    const long ntiles = tiles_x * (dir == DY ? nz : ny);
+    const unsigned grid = PERSIST ? persistent_grid(ctx, kern, threads, smem, ntiles) : (unsigned)ntiles;
     ++ctx->launches;
-    kern<<<(unsigned)grid, threads, smem, st>>>(maps, prog, nx, ny, dir, box_n, nb, tile, ctx->d_err);
+    kern<<<grid, threads, smem, st>>>(maps, prog, nx, ny, dir, box_n, nb, tile, ntiles, ctx->d_err);
     return cuda_check(ctx, cudaGetLastError(), "ls_stage_yz launch");
 }
 
@@ -590,13 +638,20 @@ int launch_stage(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir, int nx, i
     // cfg selects (lines per CTA, chunk length).
     constexpr int Lbig = sizeof(T) == 4 ? 32 : 16;
     constexpr int Lsmall = sizeof(T) == 4 ? 16 : 8;
+    // 0-5: one CTA per tile; 6-11: the same shapes, persistent with two slots
     switch (cfg) {
-    case 0: return launch_stage_cfg<T, 16, Lbig>(ctx, prog, dir, nx, ny, nz);
-    case 1: return launch_stage_cfg<T, 32, Lbig>(ctx, prog, dir, nx, ny, nz);
-    case 2: return launch_stage_cfg<T, 16, Lsmall>(ctx, prog, dir, nx, ny, nz);
-    case 3: return launch_stage_cfg<T, 8, Lbig>(ctx, prog, dir, nx, ny, nz);
-    case 4: return launch_stage_cfg<T, 32, Lsmall>(ctx, prog, dir, nx, ny, nz);
-    case 5: return launch_stage_cfg<T, 8, Lsmall>(ctx, prog, dir, nx, ny, nz);
+    case 0: return launch_stage_cfg<T, 16, Lbig, false>(ctx, prog, dir, nx, ny, nz);
+    case 1: return launch_stage_cfg<T, 32, Lbig, false>(ctx, prog, dir, nx, ny, nz);
+    case 2: return launch_stage_cfg<T, 16, Lsmall, false>(ctx, prog, dir, nx, ny, nz);
+    case 3: return launch_stage_cfg<T, 8, Lbig, false>(ctx, prog, dir, nx, ny, nz);
+    case 4: return launch_stage_cfg<T, 32, Lsmall, false>(ctx, prog, dir, nx, ny, nz);
+    case 5: return launch_stage_cfg<T, 8, Lsmall, false>(ctx, prog, dir, nx, ny, nz);
+    case 6: return launch_stage_cfg<T, 16, Lbig, true>(ctx, prog, dir, nx, ny, nz);
+    case 7: return launch_stage_cfg<T, 32, Lbig, true>(ctx, prog, dir, nx, ny, nz);
+    case 8: return launch_stage_cfg<T, 16, Lsmall, true>(ctx, prog, dir, nx, ny, nz);
+    case 9: return launch_stage_cfg<T, 8, Lbig, true>(ctx, prog, dir, nx, ny, nz);
+    case 10: return launch_stage_cfg<T, 32, Lsmall, true>(ctx, prog, dir, nx, ny, nz);
+    case 11: return launch_stage_cfg<T, 8, Lsmall, true>(ctx, prog, dir, nx, ny, nz);
     default: return X3D_EUNSUPPORTED;
     }
 }

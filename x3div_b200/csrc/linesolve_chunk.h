@@ -42,7 +42,7 @@ struct StageProgram {
 };
 
 // Number of (lines per CTA, chunk length) configurations launch_stage knows.
-constexpr int kChunkConfigs = 6;
+constexpr int kChunkConfigs = 12;
 
 // Launches the chunked stage kernel with configuration cfg in
 // [0, kChunkConfigs).  Returns X3D_EUNSUPPORTED, launching nothing, when the
