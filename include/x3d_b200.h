@@ -278,6 +278,27 @@ int x3d_poisson(x3d_ctx ctx, double *rhs);
  * by x3d_div_stats. */
 int x3d_divergence(x3d_ctx ctx, double *pp3, const void *ux1, const void *uy1, const void *uz1,
                    int nlock);
+/* Largest grid (points per field) x3d_divergence_noalloc can take. */
+#define X3D_NOALLOC_MAX_POINTS 262144
+/* x3d_divergence without any device allocation.  No counterpart in the
+ * reference.  For hosts that cannot allocate device memory in their time
+ * loop -- e.g. a Fortran host that maps its whole device working set up
+ * front through OpenACC data regions and runs under a fixed memory budget,
+ * or a solver sharing the GPU that must not take memory mid-step.  The five
+ * intermediate fields live in one fixed array inside the library
+ * (5 * X3D_NOALLOC_MAX_POINTS doubles = 10 MiB, held by every GPU that loads
+ * the library until the process exits) instead of in context scratch.
+ * Inputs and output are caller-owned device pointers (host pointers are
+ * refused, since staging them would allocate); the context must already
+ * exist.  Grids above X3D_NOALLOC_MAX_POINTS points return X3D_EINVAL, grids
+ * the fused stage kernels cannot take return X3D_EUNSUPPORTED.  The first
+ * call on each device looks up the array's device address; make that first
+ * call before any stream capture.  All calls share the one array: calls that
+ * overlap on the GPU (other streams or contexts at the same time) race on
+ * it.  Every element of the array is written before it is read, so nothing
+ * has to be cleared between calls. */
+int x3d_divergence_noalloc(x3d_ctx ctx, double *pp3, const void *ux1, const void *uy1,
+                           const void *uz1);
 /* gradp (:249-359): px1, py1, pz1 = grad(pp3) on the velocity grid */
 int x3d_gradp(x3d_ctx ctx, void *px1, void *py1, void *pz1, const double *pp3);
 /* cor_vel (:64-91): u -= grad p */

@@ -82,6 +82,7 @@ SIGNATURES = {
     "x3d_transpose_y_to_x": [_vp, _vp, _vp, _i],
     "x3d_poisson": [_vp, _vp],
     "x3d_divergence": [_vp, _vp, _vp, _vp, _vp, _i],
+    "x3d_divergence_noalloc": [_vp, _vp, _vp, _vp, _vp],
     "x3d_gradp": [_vp, _vp, _vp, _vp, _vp],
     "x3d_cor_vel": [_vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "x3d_solve_poisson": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],

@@ -216,6 +216,13 @@ int fused_divergence(x3d_ctx_s *ctx, double *pp3, const void *const u[3])
     return ctx->precision == X3D_F32 ? divergence_t<float>(ctx, pp3, u, s) : divergence_t<double>(ctx, pp3, u, s);
 }
 
+// The fused divergence on caller-provided intermediate fields s[0..4] (each
+// nx*ny*nz elements of the context precision); allocates nothing.
+int fused_divergence_scratch(x3d_ctx_s *ctx, double *pp3, const void *const u[3], void *const s[5])
+{
+    return ctx->precision == X3D_F32 ? divergence_t<float>(ctx, pp3, u, s) : divergence_t<double>(ctx, pp3, u, s);
+}
+
 int fused_gradp(x3d_ctx_s *ctx, void *const px[3], const double *pp3, void *const ucor[3])
 {
     void *s[6];

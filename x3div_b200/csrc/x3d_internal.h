@@ -129,6 +129,7 @@ int autotune_group(x3d_ctx_s *ctx, int dir, const void *in, const x3d_op_s *cons
 int fused_transeq(x3d_ctx_s *ctx, void *const du[3], const void *const u[3], bool step, double dt,
                   void *const unew[3]);
 int fused_divergence(x3d_ctx_s *ctx, double *pp3, const void *const u[3]);
+int fused_divergence_scratch(x3d_ctx_s *ctx, double *pp3, const void *const u[3], void *const s[5]);
 int fused_gradp(x3d_ctx_s *ctx, void *const px[3], const double *pp3, void *const ucor[3]);
 
 // ---- elementwise / reductions / transposes (fields.cu) ------------------
