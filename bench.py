@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--kernel-config", type=int, default=None,
+                    help="force one kernel configuration (x3d_ctx_set_kernel) instead of autotuning")
     ap.add_argument("--no-b48", action="store_true")
     return ap.parse_args()
 
@@ -368,7 +370,9 @@ def run_b200(args, world, rank, local):
     # ---- FP32-mixed sweep (headline) ---------------------------------------
     ctx = Context(n, n, n, lengths=(2 * np.pi,) * 3, precision="f32", device=local,
                   stream=torch.cuda.current_stream())
-    if not args.no_autotune:
+    if args.kernel_config is not None:
+        ctx.set_kernel(args.kernel_config)
+    elif not args.no_autotune:
         ctx.autotune(6)
     host = [tg_noise(n, s + 3 * rank) for s in range(3)]
     fields = [torch.from_numpy(h).to(device="cuda", dtype=torch.float32) for h in host]
@@ -469,7 +473,9 @@ def run_b200(args, world, rank, local):
     if not args.no_fp64:
         ctx64 = Context(n, n, n, lengths=(2 * np.pi,) * 3, precision="f64", device=local,
                         stream=torch.cuda.current_stream())
-        if not args.no_autotune:
+        if args.kernel_config is not None:
+            ctx64.set_kernel(args.kernel_config)
+        elif not args.no_autotune:
             ctx64.autotune(6)
         fields = [torch.from_numpy(h).to(device="cuda") for h in host]
         outs = [torch.empty_like(fields[0]) for _ in range(18)]

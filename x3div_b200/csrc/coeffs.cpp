@@ -83,16 +83,9 @@ static void lu_solve(std::vector<double> &t, const std::vector<double> &f,
 // :622-645): off-diagonals alpha, corner rows folded by Sherman-Morrison so
 // that c(1) = 2, c(n) = 1 + alpha^2, f(n) = b(n) = 0.  The "p" copies
 // (ffxp, cifxp6) equal these when periodic (:473-486, :667-676).
-int build_periodic_op(int kind, int dir, int n, double d, OpHost &op)
+static void periodic_lu(int n, double al, std::vector<double> &f, std::vector<double> &s,
+                        std::vector<double> &w, std::vector<double> &per)
 {
-    if (n < 8) return X3D_EUNSUPPORTED;
-    op.kind = kind;
-    op.dir = dir;
-    op.n = n;
-    op.periodic = 1;
-    op.npaire = (kind == DER || kind == DER2 || kind == DERPV) ? 0 : 1;
-    rhs_scalars(kind, d, &op.alfa, &op.a, &op.b, &op.c, &op.d);
-    const double al = op.alfa;
     std::vector<double> fb(n, 0.0), fc(n, 0.0), ff(n, 0.0);
     ff[0] = al; ff[1] = al;
     fc[0] = 2.0; fc[1] = 1.0;
@@ -105,15 +98,89 @@ int build_periodic_op(int kind, int dir, int n, double d, OpHost &op)
         fc[i] = 1.0;
         fb[i] = al;
     }
-    op.f = ff;
-    lu_prepare(fb, fc, ff, op.s, op.w);
+    f = ff;
+    lu_prepare(fb, fc, ff, s, w);
     // init(): periodic = M^-1 (-1, 0, ..., 0, alfa)  (:260-264)
-    op.per.assign(n, 0.0);
-    op.per[0] = -1.0;
-    op.per[n - 1] = al;
-    lu_solve(op.per, op.f, op.s, op.w);
+    per.assign(n, 0.0);
+    per[0] = -1.0;
+    per[n - 1] = al;
+    lu_solve(per, f, s, w);
+}
+
+int build_periodic_op(int kind, int dir, int n, double d, OpHost &op)
+{
+    if (n < 8) return X3D_EUNSUPPORTED;
+    op.kind = kind;
+    op.dir = dir;
+    op.n = n;
+    op.periodic = 1;
+    op.npaire = (kind == DER || kind == DER2 || kind == DERPV) ? 0 : 1;
+    rhs_scalars(kind, d, &op.alfa, &op.a, &op.b, &op.c, &op.d);
+    periodic_lu(n, op.alfa, op.f, op.s, op.w, op.per);
     finish_op(op);
     return X3D_OK;
+}
+
+// True when an operator's factors are those of the periodic matrix for its
+// alfa (to 1e-12 relative), i.e. when it is the circulant (alfa, 1, alfa).
+static bool circulant(const OpHost &h)
+{
+    if (!h.periodic || h.per.size() != (size_t)h.n || h.n < 8) return false;
+    if (!(std::fabs(h.alfa) < 0.5)) return false;
+    std::vector<double> f, s, w, per;
+    periodic_lu(h.n, h.alfa, f, s, w, per);
+    auto same = [](const std::vector<double> &a, const std::vector<double> &b) {
+        double m = 0.0, e = 0.0;
+        for (size_t i = 0; i < a.size(); ++i) {
+            m = std::max(m, std::fabs(b[i]));
+            e = std::max(e, std::fabs(a[i] - b[i]));
+        }
+        return e <= 1e-12 * (m > 0 ? m : 1.0);
+    };
+    return same(h.f, f) && same(h.s, s) && same(h.w, w) && same(h.per, per);
+}
+
+// Chunks a carry scan must visit for chunk length L (LineOp::depth).
+static int circ_depth(double rho, int L, int n, double thr)
+{
+    const int C = (n + L - 1) / L;
+    const double ar = std::fabs(rho);
+    if (std::pow(ar, n) >= thr) return C;
+    std::vector<double> m(C, std::pow(ar, L));
+    m[C - 1] = std::pow(ar, n - (C - 1) * L);
+    int k = 1;
+    for (int c = 0; c < C; ++c) {
+        double prod = 1.0;
+        int d = 0;
+        while (prod >= thr && d < C) {
+            prod *= m[((c - d) % C + C) % C];
+            ++d;
+        }
+        k = std::max(k, d);
+    }
+    return std::min(k, C);
+}
+
+template <typename T>
+static void fill_circ(const OpHost &h, LineOp<T> &lo, double thr)
+{
+    lo.circ = circulant(h) ? 1 : 0;
+    const double al = h.alfa;
+    const double rho = al == 0.0 ? 0.0 : -2.0 * al / (1.0 + std::sqrt(1.0 - 4.0 * al * al));
+    const double sc = 1.0 + rho * rho;
+    lo.ca = (T)(h.a * sc);
+    lo.cb = (T)(h.b * sc);
+    lo.cc = (T)(h.c * sc);
+    lo.cd = (T)(h.d * sc);
+    lo.rho = (T)rho;
+    const int Ls[2] = {kChunkLong<T>, kChunkShort<T>};
+    for (int i = 0; i < 2; ++i) {
+        const int L = Ls[i], C = (h.n + L - 1) / L;
+        lo.mfull[i] = (T)std::pow(rho, L);
+        lo.mlast[i] = (T)std::pow(rho, h.n - (C - 1) * L);
+        lo.depth[i] = circ_depth(rho, L, h.n, thr);
+    }
+    lo.wrap = (T)(1.0 / (1.0 - std::pow(rho, h.n)));
 }
 
 // g = M^-T e_1 with M = L U, L unit lower bidiagonal (L(i,i-1) = s_i) and U
@@ -142,79 +209,14 @@ void finish_op(OpHost &op)
 
 // Scan depths for chunk length L: smallest k such that any k consecutive
 // chunk multipliers multiply to below 1e-20 (capped at the chunk count).
-static void scan_depths(const std::vector<double> &t, int n, int L, int *kf, int *kb)
-{
-    const int C = (n + L - 1) / L;
-    std::vector<double> fm(C), bm(C);
-    for (int c = 0; c < C; ++c) {
-        fm[c] = std::fabs(t[(size_t)(c * L + L - 1) * 8 + 1]);
-        bm[c] = std::fabs(t[(size_t)(c * L) * 8 + 4]);
-    }
-    auto depth = [&](const std::vector<double> &m) {
-        int k = 1;
-        for (int c = 0; c < C; ++c) {
-            double prod = 1.0;
-            int d = 0;
-            for (int j = c; j < C && prod >= 1e-20; ++j) {
-                prod *= m[j];
-                ++d;
-            }
-            if (prod >= 1e-20) d = C;  // reaches the end of the line
-            k = std::max(k, d);
-        }
-        return std::min(k, C);
-    };
-    *kf = depth(fm);
-    *kb = depth(bm);
-}
-
-// Chunk record table of one operator for chunk length L (see LineOp::tab).
-static std::vector<double> chunk_table(const OpHost &h, int L)
-{
-    const int n = h.n;
-    const int C = (n + L - 1) / L;
-    std::vector<double> t((size_t)C * L * 8, 0.0);
-    for (int c = 0; c < C; ++c) {
-        const int cs = c * L, ce = std::min(n, cs + L);
-        double mf = 1.0;
-        for (int i = cs; i < cs + L; ++i) {
-            double *r = t.data() + (size_t)i * 8;
-            if (i < ce) {
-                mf *= -h.s[i];
-                r[0] = h.s[i];
-                r[1] = mf;
-                r[2] = h.w[i];
-                r[3] = h.f[i] * h.w[i];
-                r[5] = h.per.empty() ? 0.0 : h.per[i];
-            } else {
-                r[0] = -1.0;  // z_i = 0 - (-1) z_{i-1}: the last value rides to the chunk end
-                r[1] = mf;
-            }
-        }
-        double mb = 1.0;
-        for (int i = ce - 1; i >= cs; --i) {
-            mb *= -(h.f[i] * h.w[i]);
-            t[(size_t)i * 8 + 4] = mb;
-        }
-    }
-    return t;
-}
-
 int upload_op(x3d_op_s *op)
 {
     const OpHost &h = op->h;
     const int n = h.n;
-    // layout (bytes, each part 256-aligned): float s,w,fw,p | double s,w,fw,p,g |
-    // float tables (L = 32, 16) | double tables (L = 16, 8)
+    // layout (bytes, each part 256-aligned): float s,w,fw,p | double s,w,fw,p,g
     auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
-    const std::vector<double> tf0 = chunk_table(h, kChunkLong<float>), tf1 = chunk_table(h, kChunkShort<float>);
-    const std::vector<double> td0 = chunk_table(h, kChunkLong<double>), td1 = chunk_table(h, kChunkShort<double>);
     const size_t o_f = 0, o_d = al(o_f + 4 * n * sizeof(float));
-    const size_t o_tf0 = al(o_d + 5 * n * sizeof(double));
-    const size_t o_tf1 = al(o_tf0 + tf0.size() * sizeof(float));
-    const size_t o_td0 = al(o_tf1 + tf1.size() * sizeof(float));
-    const size_t o_td1 = al(o_td0 + td0.size() * sizeof(double));
-    const size_t total = al(o_td1 + td1.size() * sizeof(double));
+    const size_t total = al(o_d + 5 * n * sizeof(double));
     std::vector<unsigned char> host(total, 0);
     float *hf = reinterpret_cast<float *>(host.data() + o_f);
     double *hd = reinterpret_cast<double *>(host.data() + o_d);
@@ -231,14 +233,6 @@ int upload_op(x3d_op_s *op)
         hd[3 * n + i] = p;
         hd[4 * n + i] = h.g[i];
     }
-    auto put_f = [&](size_t off, const std::vector<double> &t) {
-        float *d = reinterpret_cast<float *>(host.data() + off);
-        for (size_t i = 0; i < t.size(); ++i) d[i] = (float)t[i];
-    };
-    put_f(o_tf0, tf0);
-    put_f(o_tf1, tf1);
-    std::memcpy(host.data() + o_td0, td0.data(), td0.size() * sizeof(double));
-    std::memcpy(host.data() + o_td1, td1.data(), td1.size() * sizeof(double));
     if (op->dmem) cudaFree(op->dmem);
     op->dmem = nullptr;
     if (cudaMalloc(&op->dmem, host.size()) != cudaSuccess) return X3D_ENOMEM;
@@ -261,16 +255,10 @@ int upload_op(x3d_op_s *op)
     };
     fill(op->opf, df);
     fill(op->opd, dd);
-    scan_depths(tf0, n, kChunkLong<float>, &op->opf.kf[0], &op->opf.kb[0]);
-    scan_depths(tf1, n, kChunkShort<float>, &op->opf.kf[1], &op->opf.kb[1]);
-    scan_depths(td0, n, kChunkLong<double>, &op->opd.kf[0], &op->opd.kb[0]);
-    scan_depths(td1, n, kChunkShort<double>, &op->opd.kf[1], &op->opd.kb[1]);
-    op->opf.tab[0] = reinterpret_cast<const float *>(base + o_tf0);
-    op->opf.tab[1] = reinterpret_cast<const float *>(base + o_tf1);
-    op->opd.tab[0] = reinterpret_cast<const double *>(base + o_td0);
-    op->opd.tab[1] = reinterpret_cast<const double *>(base + o_td1);
     op->opf.a = (float)h.a; op->opf.b = (float)h.b; op->opf.c = (float)h.c; op->opf.d = (float)h.d;
     op->opd.a = h.a; op->opd.b = h.b; op->opd.c = h.c; op->opd.d = h.d;
+    fill_circ(h, op->opf, 1e-12);
+    fill_circ(h, op->opd, 1e-20);
     return X3D_OK;
 }
 

@@ -2,28 +2,28 @@
 // applications, and the stage kernels that fuse several operators, their
 // pointwise products and their sums into one pass over the staged inputs.
 //
-// The reference sweeps each line serially (?thomas_12, src/thomas.f90:61-84):
-//   forward  z_i = r_i - s_i z_{i-1}          backward y_i = (z_i - f_i y_{i+1}) w_i
-// then corrects for periodicity with the precomputed vector p
-// (xthomas_0 :49-55):  x = y - p (y_1 - alfa y_n) / (1 + p_1 - alfa p_n).
+// The reference sweeps each line serially (?thomas_12, src/thomas.f90:61-84)
+// with the LU factors of its periodic matrix, then corrects for periodicity
+// with the precomputed vector p (xthomas_0 :49-55).  The matrix that pair
+// inverts is exactly the circulant (alfa, 1, alfa), which factors as
+//   M = (1 + rho^2)^-1 (1 - rho E^-1)(1 - rho E),  alfa rho^2 + rho + alfa = 0,
+// |rho| < 1.  So y = M^-1 r is two first-order periodic recurrences with one
+// constant coefficient:
+//   forward  v_i = (1 + rho^2) r_i + rho v_{i-1}     backward  y_i = v_i + rho y_{i+1}
+// (the factor 1 + rho^2 is folded into the RHS scalars).
 //
-// Here a line of n points is cut into C chunks of L points; thread (l, c)
-// owns chunk c of line l and keeps it in registers.  Each recurrence is
-// affine in its incoming value, so a chunk is swept locally from zero and
-// later shifted by  multiplier * carry, where the multiplier is the running
-// product of the reference's own factors (-s_i forward, -f_i w_i backward):
+// A line of n points is cut into C chunks of L points; thread (l, c) owns
+// chunk c of line l and keeps it in registers.  Each recurrence is affine in
+// its incoming value, so a chunk is swept locally from zero and later
+// shifted by rho^k * carry:
 //   1. stencil r_i for the chunk from an L+8 window of the staged input;
-//   2. local forward sweep -> chunk end value and multiplier, plus the chunk's
-//      share of y_0 = sum_i g_i r_i (g = first row of M^-1, FP64);
-//   -- barrier -- every thread scans the chunk ends (C fused multiply-adds)
-//      for its carry and for z_{n-1}, so ss = (y_0 - alfa z_{n-1} w_{n-1})
-//      / (1 + p_0 - alfa p_{n-1}) is known before the backward sweep;
-//   3. fix the forward values, local backward sweep -> chunk start value and
-//      multiplier;
-//   -- barrier -- scan for the backward carry;
-//   4. fix the backward values and subtract ss p_i.
-// Two barriers per operator, no intermediate field in shared memory, and the
-// same arithmetic as the reference Thomas + Sherman-Morrison up to rounding.
+//   2. local forward sweep, chunk end value to shared memory;
+//   -- barrier -- each thread folds the end values of the chunks before it
+//      (depth chunks, or the whole line divided by 1 - rho^n) into its
+//      carry, fixes its values and sweeps backward locally;
+//   -- barrier -- the same for the backward carry from the chunks after it.
+// Every chunk does the same work: no tables, no per-line scalar, two
+// barriers per operator and one HBM read and write per application.
 //
 // A stage (StageProgram) runs up to six such operators over up to three
 // staged inputs, combining the results in a register accumulator and
@@ -48,154 +48,156 @@ namespace x3d {
 
 constexpr uint64_t kChunkWaitNs = 2000000000ull;
 
+// RHS scalars of a stencil (the operator's, times 1 + rho^2).
+template <typename T>
+struct Coef {
+    T a, b, c, d;
+};
+
 template <int KIND, typename T>
-__device__ __forceinline__ T stencil_at(const T *v, const LineOp<T> &op)
+__device__ __forceinline__ T stencil_at(const T *v, const Coef<T> &k)
 {
-    // v[k] = u_{i-4+k}
-    if constexpr (KIND == DER) return op.a * (v[5] - v[3]) + op.b * (v[6] - v[2]);
+    // v[m] = u_{i-4+m}
+    if constexpr (KIND == DER) return k.a * (v[5] - v[3]) + k.b * (v[6] - v[2]);
     if constexpr (KIND == DER2)
-        return op.a * ((v[5] - v[4]) - (v[4] - v[3])) + op.b * ((v[6] - v[4]) - (v[4] - v[2]));
-    if constexpr (KIND == DERVP) return op.a * (v[5] - v[4]) + op.b * (v[6] - v[3]);
-    if constexpr (KIND == DERPV) return op.a * (v[4] - v[3]) + op.b * (v[5] - v[2]);
+        return k.a * ((v[5] - v[4]) - (v[4] - v[3])) + k.b * ((v[6] - v[4]) - (v[4] - v[2]));
+    if constexpr (KIND == DERVP) return k.a * (v[5] - v[4]) + k.b * (v[6] - v[3]);
+    if constexpr (KIND == DERPV) return k.a * (v[4] - v[3]) + k.b * (v[5] - v[2]);
     if constexpr (KIND == INTVP)
-        return op.a * (v[5] + v[4]) + op.b * (v[6] + v[3]) + op.c * (v[7] + v[2]) + op.d * (v[8] + v[1]);
+        return k.a * (v[5] + v[4]) + k.b * (v[6] + v[3]) + k.c * (v[7] + v[2]) + k.d * (v[8] + v[1]);
     if constexpr (KIND == INTPV)
-        return op.a * (v[4] + v[3]) + op.b * (v[5] + v[2]) + op.c * (v[6] + v[1]) + op.d * (v[7] + v[0]);
+        return k.a * (v[4] + v[3]) + k.b * (v[5] + v[2]) + k.c * (v[6] + v[1]) + k.d * (v[7] + v[0]);
     return v[4];
 }
 
 template <int KIND, typename T, int L>
-__device__ __forceinline__ void chunk_stencil(const T (&w)[L + 8], T (&r)[L], const LineOp<T> &op)
+__device__ __forceinline__ void chunk_stencil(const T (&w)[L + 8], T (&r)[L], const Coef<T> &k)
 {
 #pragma unroll
-    for (int j = 0; j < L; ++j) r[j] = stencil_at<KIND>(w + j, op);
+    for (int j = 0; j < L; ++j) r[j] = stencil_at<KIND>(w + j, k);
 }
 
 template <typename T, int L>
 __device__ __forceinline__ void chunk_stencil_kind(int kind, const T (&w)[L + 8], T (&r)[L],
                                                    const LineOp<T> &op)
 {
+    const Coef<T> k{op.ca, op.cb, op.cc, op.cd};
     switch (kind) {
-    case DER: chunk_stencil<DER, T, L>(w, r, op); break;
-    case DER2: chunk_stencil<DER2, T, L>(w, r, op); break;
-    case DERVP: chunk_stencil<DERVP, T, L>(w, r, op); break;
-    case DERPV: chunk_stencil<DERPV, T, L>(w, r, op); break;
-    case INTVP: chunk_stencil<INTVP, T, L>(w, r, op); break;
-    case INTPV: chunk_stencil<INTPV, T, L>(w, r, op); break;
-    default: chunk_stencil<IDENT, T, L>(w, r, op); break;
+    case DER: chunk_stencil<DER, T, L>(w, r, k); break;
+    case DER2: chunk_stencil<DER2, T, L>(w, r, k); break;
+    case DERVP: chunk_stencil<DERVP, T, L>(w, r, k); break;
+    case DERPV: chunk_stencil<DERPV, T, L>(w, r, k); break;
+    case INTVP: chunk_stencil<INTVP, T, L>(w, r, k); break;
+    case INTPV: chunk_stencil<INTPV, T, L>(w, r, k); break;
+    default: chunk_stencil<IDENT, T, L>(w, r, k); break;
     }
 }
 
+// Window index of u_{cs-4+j} on a periodic line of n points.  Windows that
+// need it wrap at most once; indices of padding points past the end of a
+// short line are clamped into the line (their values are never used).
+__device__ __forceinline__ int wrap_index(int idx, int n, int last)
+{
+    idx = idx < 0 ? idx + n : idx;
+    idx = idx >= n ? idx - n : idx;
+    return idx > last ? last : idx;
+}
+
 // Scratch in shared memory after the input tiles: per (chunk, line) the
-// forward end value / multiplier / y_0 share and the backward start value /
-// multiplier, and per line the Sherman-Morrison scalar.
+// forward end value and the backward start value of the local sweeps.
 template <typename T>
 struct ChunkScratch {
-    T *fz, *fm, *bz, *bm;
-    double *fg, *ss;
+    T *fz, *bz;
 };
 
-// Loads of the per-point records of LineOp::tab: {s, mf, w, fw, mb, p, 0, 0}.
-template <typename T>
-struct Rec;
-template <>
-struct Rec<float> {
-    __device__ static float s(const float *t) { return __ldg(t); }
-    __device__ static float4 mfwfw(const float *t) { return __ldg(reinterpret_cast<const float4 *>(t)); }
-    __device__ static float2 mbp(const float *t) { return __ldg(reinterpret_cast<const float2 *>(t + 4)); }
-};
-template <>
-struct Rec<double> {
-    __device__ static double s(const double *t) { return __ldg(t); }
-    __device__ static double4 mfwfw(const double *t)
-    {
-        const double2 a = __ldg(reinterpret_cast<const double2 *>(t));
-        const double2 b = __ldg(reinterpret_cast<const double2 *>(t + 2));
-        return make_double4(a.x, a.y, b.x, b.y);
-    }
-    __device__ static double2 mbp(const double *t) { return __ldg(reinterpret_cast<const double2 *>(t + 4)); }
-};
-
-// Steps 1-4 for one operator; the solved values end in r[] (chunk-local).
-// load(w) fills the L+8 input window u[cs-4 .. cs+L+3] (indices mod n); the
-// window is dead once the stencil is evaluated.  tab is this chunk length's
-// record table (records padded to whole chunks, so the sweeps need no
-// bounds tests: padding keeps the forward value and zeroes the backward one).
-template <typename T, int L, typename Load>
-__device__ __forceinline__ void chunk_solve(const LineOp<T> &op, const T *tab, int kind,
-                                            const Load &load, T (&r)[L], const ChunkScratch<T> &sc,
-                                            int W, int l, int c, int C, int cs, int nv, int q,
-                                            bool active)
+// Carry into chunk c from the chunk values e (end values, scanning the
+// chunks before c, or start values scanning those after it when STEP = -1).
+template <typename T, int STEP>
+__device__ __forceinline__ T chunk_carry(const T *e, const LineOp<T> &op, int ti, int W, int l, int c, int C)
 {
+    const int K = op.depth[ti];
+    int cc = c;
+    if (K < C) {
+        cc = c - STEP * K;
+        cc = cc < 0 ? cc + C : (cc >= C ? cc - C : cc);
+    }
+    const T mf = op.mfull[ti], ml = op.mlast[ti];
+    T carry = T(0);
+    for (int k = 0; k < K; ++k) {
+        carry = fma(cc == C - 1 ? ml : mf, carry, e[cc * W + l]);
+        cc += STEP;
+        cc = cc == C ? 0 : (cc < 0 ? C - 1 : cc);
+    }
+    return K < C ? carry : carry * op.wrap;
+}
+
+// Solves one operator for one chunk; the solved values end in r[] (chunk
+// local).  load(w) fills the L+8 input window u[cs-4 .. cs+L+3] (indices mod
+// n); the window is dead once the stencil is evaluated.  nv = points of the
+// chunk inside the line (L except for the last chunk of a ragged line).
+template <typename T, int L, typename Load>
+__device__ __forceinline__ void chunk_solve(const LineOp<T> &op, int kind, const Load &load, T (&r)[L],
+                                            const ChunkScratch<T> &sc, int W, int l, int c, int C, int nv,
+                                            int q)
+{
+    constexpr int ti = L == kChunkLong<T> ? 0 : 1;
     {
         T w[L + 8];
         load(w);
         chunk_stencil_kind<T, L>(kind, w, r, op);
     }
-    if (nv < L) {  // only the last chunk: padding points get r = 0
+    const T rho = op.rho;
+    T v = T(0);
+#pragma unroll
+    for (int j = 0; j < L; ++j) {
+        v = fma(rho, v, r[j]);
+        r[j] = v;
+    }
+    if (nv < L) {  // ragged last chunk: its end is point nv - 1
+#pragma unroll
+        for (int j = 0; j < L; ++j)
+            if (j == nv - 1) v = r[j];
+    }
+    sc.fz[q] = v;
+    __syncthreads();
+    // forward carry (v just before the chunk), fix, local backward sweep
+    {
+        T pw = chunk_carry<T, 1>(sc.fz, op, ti, W, l, c, C);
+#pragma unroll
+        for (int j = 0; j < L; ++j) {
+            pw *= rho;
+            r[j] += pw;
+        }
+    }
+    if (nv < L) {
 #pragma unroll
         for (int j = 0; j < L; ++j)
             if (j >= nv) r[j] = T(0);
     }
-    const T *t = tab + (size_t)cs * 8;
-    // local forward sweep, y_0 share
-    T zh = T(0);
-    double gp = 0.0;
-    if (cs < op.glen) {
-#pragma unroll
-        for (int j = 0; j < L; ++j) gp = fma(__ldg(op.g + min(cs + j, op.n - 1)), (double)r[j], gp);
-    }
-#pragma unroll
-    for (int j = 0; j < L; ++j) {
-        zh = r[j] - Rec<T>::s(t + 8 * j) * zh;
-        r[j] = zh;
-    }
-    const T fme = __ldg(t + 8 * (L - 1) + 1);  // product of -s over the chunk
-    sc.fz[q] = zh;
-    sc.fm[q] = fme;
-    sc.fg[q] = gp;
-    __syncthreads();
-    // forward carry: z at the end of chunk c-1 (earlier chunks contribute
-    // below 1e-20 beyond kf chunks)
-    const int ti = L == kChunkLong<T> ? 0 : 1;
-    T carry = T(0);
-    for (int cc = max(0, c - op.kf[ti]); cc < c; ++cc) {
-        const int qq = cc * W + l;
-        carry = sc.fz[qq] + sc.fm[qq] * carry;
-    }
-    if (active && c == C - 1) {
-        // last chunk: z_{n-1} (carried to the padded end), y_0, and the
-        // Sherman-Morrison scalar for the whole line
-        const T zlast = zh + fme * carry;
-        double y0 = 0.0;
-        const int cg = min(C, (op.glen + L - 1) / L);
-        for (int cc = 0; cc < cg; ++cc) y0 += sc.fg[cc * W + l];
-        sc.ss[l] = op.periodic
-                       ? (y0 - op.alfa * ((double)zlast * (double)__ldg(op.w + (op.n - 1)))) / op.den
-                       : 0.0;
-    }
-    // fix forward values and sweep backward locally
-    T yh = T(0);
+    T y = T(0);
 #pragma unroll
     for (int j = L - 1; j >= 0; --j) {
-        const auto cw = Rec<T>::mfwfw(t + 8 * j);  // (s, mf, w, fw)
-        const T z = r[j] + cw.y * carry;
-        yh = z * cw.z - cw.w * yh;
-        r[j] = yh;
+        y = fma(rho, y, r[j]);
+        r[j] = y;
     }
-    sc.bz[q] = yh;
-    sc.bm[q] = __ldg(t + 4);  // product of -f w over the chunk
+    sc.bz[q] = y;
     __syncthreads();
-    T bcarry = T(0);
-    for (int cc = min(C - 1, c + op.kb[ti]); cc > c; --cc) {
-        const int qq = cc * W + l;
-        bcarry = sc.bz[qq] + sc.bm[qq] * bcarry;
-    }
-    const T sst = (T)sc.ss[l];
+    // backward carry (y just after the chunk's last point) and fix
+    T pw = chunk_carry<T, -1>(sc.bz, op, ti, W, l, c, C);
+    if (nv == L) {
 #pragma unroll
-    for (int j = 0; j < L; ++j) {
-        const auto mp = Rec<T>::mbp(t + 8 * j);  // (mb, p)
-        r[j] = r[j] + mp.x * bcarry - sst * mp.y;
+        for (int j = L - 1; j >= 0; --j) {
+            pw *= rho;
+            r[j] += pw;
+        }
+    } else {
+#pragma unroll
+        for (int j = L - 1; j >= 0; --j) {
+            if (j < nv) {
+                pw *= rho;
+                r[j] += pw;
+            }
+        }
     }
 }
 
@@ -204,13 +206,8 @@ __device__ __forceinline__ ChunkScratch<T> carve_scratch(unsigned char *base, in
 {
     ChunkScratch<T> sc;
     T *t = reinterpret_cast<T *>(base);
-    const int q = C * W;
     sc.fz = t;
-    sc.fm = t + q;
-    sc.bz = t + 2 * q;
-    sc.bm = t + 3 * q;
-    sc.fg = reinterpret_cast<double *>(base + (((size_t)4 * q * sizeof(T) + 15) & ~(size_t)15));
-    sc.ss = sc.fg + q;
+    sc.bz = t + C * W;
     return sc;
 }
 
@@ -328,18 +325,21 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
             const T *ca = col(so.src_a);
             const T *cb = so.src_b >= 0 ? col(so.src_b) : nullptr;
             auto load = [&](T(&w)[L + 8]) {
+                if (cb) {
 #pragma unroll
-                for (int j = 0; j < L + 8; ++j) {
-                    int idx = cs - 4 + j;
-                    if (wraps) {
-                        idx %= n;
-                        idx = idx < 0 ? idx + n : idx;
+                    for (int j = 0; j < L + 8; ++j) {
+                        const int idx = wraps ? wrap_index(cs - 4 + j, n, n - 1) : cs - 4 + j;
+                        w[j] = ca[idx * W] * cb[idx * W];
                     }
-                    w[j] = cb ? ca[idx * W] * cb[idx * W] : ca[idx * W];
+                } else {
+#pragma unroll
+                    for (int j = 0; j < L + 8; ++j) {
+                        const int idx = wraps ? wrap_index(cs - 4 + j, n, n - 1) : cs - 4 + j;
+                        w[j] = ca[idx * W];
+                    }
                 }
             };
-            chunk_solve<T, L>(so.op, so.op.tab[L == kChunkLong<T> ? 0 : 1], so.kind, load, r, sc, W, l, c, C, cs,
-                              nv, c * W + l, true);
+            chunk_solve<T, L>(so.op, so.kind, load, r, sc, W, l, c, C, nv, c * W + l);
             if constexpr (ACC) accumulate<T, L>(so, acc, r, nv, tile_at);
             const T *res;
             if constexpr (ACC) res = acc;
@@ -455,6 +455,7 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
     const ChunkScratch<T> sc = carve_scratch<T>(smem_raw + (PERSIST ? 2 : 1) * slot_bytes, C, W);
     const int cs = c * L;
     const int nv = min(L, n - cs);
+    const bool wraps = cs < 4 || cs + L + 4 > n;
     const long step = PERSIST ? (long)gridDim.x : ntiles;
     long tile = blockIdx.x;
     if (t == 0 && tile < ntiles) issue(tile, 0);
@@ -483,25 +484,29 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
             const T *ra = row(so.src_a);
             const T *rb = so.src_b >= 0 ? row(so.src_b) : nullptr;
             auto load = [&](T(&w)[L + 8]) {
+                if (rb) {
 #pragma unroll
-                for (int j = 0; j < L + 8; j += V) {
-                    int idx = (cs - 4 + j) % n;
-                    idx = idx < 0 ? idx + n : idx;
-                    const VT qa = *reinterpret_cast<const VT *>(ra + idx);
-                    const T *ea = reinterpret_cast<const T *>(&qa);
-                    if (rb) {
+                    for (int j = 0; j < L + 8; j += V) {
+                        const int idx = wraps ? wrap_index(cs - 4 + j, n, n - V) : cs - 4 + j;
+                        const VT qa = *reinterpret_cast<const VT *>(ra + idx);
                         const VT qb = *reinterpret_cast<const VT *>(rb + idx);
+                        const T *ea = reinterpret_cast<const T *>(&qa);
                         const T *eb = reinterpret_cast<const T *>(&qb);
 #pragma unroll
                         for (int v = 0; v < V; ++v) w[j + v] = ea[v] * eb[v];
-                    } else {
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < L + 8; j += V) {
+                        const int idx = wraps ? wrap_index(cs - 4 + j, n, n - V) : cs - 4 + j;
+                        const VT qa = *reinterpret_cast<const VT *>(ra + idx);
+                        const T *ea = reinterpret_cast<const T *>(&qa);
 #pragma unroll
                         for (int v = 0; v < V; ++v) w[j + v] = ea[v];
                     }
                 }
             };
-            chunk_solve<T, L>(so.op, so.op.tab[L == kChunkLong<T> ? 0 : 1], so.kind, load, r, sc, W, l, c, C, cs,
-                              nv, c * W + l, true);
+            chunk_solve<T, L>(so.op, so.kind, load, r, sc, W, l, c, C, nv, c * W + l);
             if constexpr (ACC) accumulate<T, L>(so, acc, r, nv, tile_at);
             const T *res;
             if constexpr (ACC) res = acc;
@@ -541,10 +546,7 @@ struct StageOpView {
     short flush, accumulate, mul_tile;
 };
 
-static size_t scratch_bytes(int C, int W, size_t es)
-{
-    return (((size_t)4 * C * W * es + 15) & ~(size_t)15) + (size_t)(C + 1) * W * sizeof(double);
-}
+static size_t scratch_bytes(int C, int W, size_t es) { return ((size_t)2 * C * W * es + 15) & ~(size_t)15; }
 
 static bool al16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
@@ -567,6 +569,8 @@ static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir
     for (int k = 0; k < prog.nops; ++k)
         acc = acc || !plain(StageOpView{prog.ops[k].flush, prog.ops[k].accumulate, prog.ops[k].mul_tile});
     const int n = prog.ops[0].op.n;
+    for (int k = 0; k < prog.nops; ++k)
+        if (!prog.ops[k].op.circ || prog.ops[k].op.n != n) return X3D_EUNSUPPORTED;
     const size_t es = sizeof(T);
     const int C = (n + L - 1) / L;
     const int threads = C * W;
@@ -767,11 +771,11 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
         if (dir == DX) {
             const int lr = l < rows ? l : 0;
             const T *row = tile + (size_t)lr * J.pitch;
+            const bool wraps = cs < 4 || cs + L + 4 > n;
             auto load = [&](T(&w)[L + 8]) {
 #pragma unroll
                 for (int j = 0; j < L + 8; j += V) {
-                    int idx = (cs - 4 + j) % n;
-                    idx = idx < 0 ? idx + n : idx;
+                    const int idx = wraps ? wrap_index(cs - 4 + j, n, n - V) : cs - 4 + j;
                     const VT qa = *reinterpret_cast<const VT *>(row + idx);
                     const T *ea = reinterpret_cast<const T *>(&qa);
 #pragma unroll
@@ -779,8 +783,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
                 }
             };
             for (int k = 0; k < J.nops; ++k) {
-                chunk_solve<T, L>(J.op[k], J.op[k].tab[L == kChunkLong<T> ? 0 : 1], J.kind[k], load, r, sc,
-                                  W, l, c, C, cs, nv, q, active);
+                chunk_solve<T, L>(J.op[k], J.kind[k], load, r, sc, W, l, c, C, nv, q);
                 if (active && l < rows) {
                     T *dst = J.out[k] + (size_t)(l0 + l) * n + cs;
 #pragma unroll
@@ -801,11 +804,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
             auto load = [&](T(&w)[L + 8]) {
 #pragma unroll
                 for (int j = 0; j < L + 8; ++j) {
-                    int idx = cs - 4 + j;
-                    if (wraps) {
-                        idx %= n;
-                        idx = idx < 0 ? idx + n : idx;
-                    }
+                    const int idx = wraps ? wrap_index(cs - 4 + j, n, n - 1) : cs - 4 + j;
                     w[j] = col[idx * W];
                 }
             };
@@ -815,8 +814,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
                                  (dir == DY ? (size_t)J.nx * J.ny * o : (size_t)J.nx * o) +
                                  (size_t)cs * ostride;
             for (int k = 0; k < J.nops; ++k) {
-                chunk_solve<T, L>(J.op[k], J.op[k].tab[L == kChunkLong<T> ? 0 : 1], J.kind[k], load, r, sc,
-                                  W, l, c, C, cs, nv, q, active);
+                chunk_solve<T, L>(J.op[k], J.kind[k], load, r, sc, W, l, c, C, nv, q);
                 if (live) {
                     T *dst = J.out[k] + obase;
 #pragma unroll
@@ -840,6 +838,8 @@ bool plan_batch_job(BatchJob<T> &J, int L, size_t *tile_bytes)
     const size_t es = sizeof(T);
     const int n = J.n;
     constexpr int V = Vec4<T>::N;
+    for (int k = 0; k < J.nops; ++k)
+        if (!J.op[k].circ || J.op[k].n != n) return false;
     J.C = (n + L - 1) / L;
     if (J.C > kBatchThreads) return false;
     int W = kBatchThreads / J.C;
@@ -884,8 +884,7 @@ bool plan_batch_job(BatchJob<T> &J, int L, size_t *tile_bytes)
 template <typename T>
 size_t batch_scratch_bytes()
 {
-    return (((size_t)4 * kBatchThreads * sizeof(T) + 15) & ~(size_t)15) +
-           (size_t)(kBatchThreads + kBatchThreads) * sizeof(double);
+    return ((size_t)2 * kBatchThreads * sizeof(T) + 15) & ~(size_t)15;
 }
 
 template <typename T>

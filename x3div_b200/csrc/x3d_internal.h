@@ -33,17 +33,23 @@ struct LineOp {
     int n;
     int periodic;
     int glen;         // g_i == 0 (in FP64) for i >= glen
-    // Per-point records for the chunked kernels, one table per chunk length
-    // (tab[0] for kChunkLong<T>, tab[1] for kChunkShort<T>), each padded to
-    // whole chunks.  Record i = {s, mf, w, fw, mb, p, 0, 0}: mf is the product
-    // of -s over the chunk up to i, mb the product of -f w from i to the
-    // chunk end.  Padding records {-1, mf_end, 0, 0, 0, 0} carry the last
-    // forward value to the chunk end and keep the backward sweep at zero.
-    const T *tab[2];
-    // Scan depths per table: the carry into a chunk only needs the previous
-    // kf (next kb) chunks, beyond which the product of chunk multipliers is
-    // below 1e-20 and the dropped terms are under FP64 resolution.
-    int kf[2], kb[2];
+    // Factorised circulant form, read by the chunked kernels.  A periodic
+    // operator of the reference is the circulant (alfa, 1, alfa) matrix once
+    // Sherman-Morrison has folded its corners back in, and that matrix is
+    //   M = (1 + rho^2)^-1 (1 - rho E^-1)(1 - rho E),   alfa rho^2 + rho + alfa = 0,
+    // with |rho| < 1 and (E y)_i = y_{i+1}.  So M y = r is two first-order
+    // periodic recurrences:  v_i = (1 + rho^2) r_i + rho v_{i-1},
+    // y_i = v_i + rho y_{i+1}.  circ = 0 for an operator whose factors are not
+    // that matrix's (the chunked kernels then decline it).
+    T ca, cb, cc, cd;      // RHS scalars times (1 + rho^2)
+    T rho;
+    T mfull[2], mlast[2];  // rho^L and rho^(last chunk's length), [0] for kChunkLong<T>, [1] kChunkShort<T>
+    T wrap;                // 1 / (1 - rho^n), the sum over turns around the line
+    // Chunks a carry scan visits: beyond depth the product of chunk
+    // multipliers is below 1e-20 (FP64) or 1e-12 (FP32); depth == C means
+    // the whole line, summed once and scaled by wrap.
+    int depth[2];
+    int circ;
 };
 
 template <typename T>
