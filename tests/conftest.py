@@ -51,3 +51,20 @@ def seeded_field(shape, seed, kind="tg", lengths=(2 * np.pi,) * 3, noise=1e-3):
         u = rng.standard_normal(shape)
     u = u + noise * rng.standard_normal(shape)
     return np.asfortranarray(u)
+
+
+def band_limited_field(n, seed, kmax_frac=0.25, slope=-5.0 / 3.0):
+    """Periodic n^3 field of Fourier modes 0 < |k| <= kmax_frac * n with
+    amplitude |k|**slope and seeded random phases, scaled to max|u| = 1
+    (Fortran-ordered, FP64)."""
+    rng = np.random.default_rng(seed)
+    k = np.fft.fftfreq(n, 1.0 / n)
+    kr = np.fft.rfftfreq(n, 1.0 / n)
+    K = np.sqrt(k[:, None, None] ** 2 + k[None, :, None] ** 2 + kr[None, None, :] ** 2)
+    amp = np.zeros_like(K)
+    band = (K > 0) & (K <= kmax_frac * n)
+    amp[band] = K[band] ** slope
+    spec = amp * np.exp(2j * np.pi * rng.random(K.shape))
+    u = np.fft.irfftn(spec, s=(n, n, n), axes=(0, 1, 2))
+    u /= np.abs(u).max()
+    return np.asfortranarray(u)

@@ -93,14 +93,28 @@ __device__ __forceinline__ void chunk_stencil_kind(int kind, const T (&w)[L + 8]
     }
 }
 
-// Window index of u_{cs-4+j} on a periodic line of n points.  Windows that
-// need it wrap at most once; indices of padding points past the end of a
-// short line are clamped into the line (their values are never used).
-__device__ __forceinline__ int wrap_index(int idx, int n, int last)
+// Staged lines carry periodic halos, so a chunk's window never wraps:
+// shared-memory row (y/z tiles) or element (x rows) kHalo + i holds point i
+// of the line for -4 <= i < n + 4, and the rows past that up to the end of
+// the last chunk's window exist but hold values that are never used.
+constexpr int kHalo = 4;
+
+// Fills the halos of ntiles staged y/z tiles of W columns whose point i sits
+// in row h0 + i: rows h0-4 .. h0-1 from points n-4 .. n-1, rows h0+n ..
+// h0+n+3 from points 0 .. 3.
+template <typename T>
+__device__ __forceinline__ void fill_halos_yz(unsigned char *base, size_t tile_bytes, int ntiles, int n, int W,
+                                              int h0)
 {
-    idx = idx < 0 ? idx + n : idx;
-    idx = idx >= n ? idx - n : idx;
-    return idx > last ? last : idx;
+    const int per = 8 * W;
+    for (int i = threadIdx.x; i < per * ntiles; i += blockDim.x) {
+        const int ti = i / per, r = i - ti * per;
+        const int h = r / W, x = r - h * W;
+        T *tp = reinterpret_cast<T *>(base + ti * tile_bytes);
+        const int dst = h < 4 ? h0 - 4 + h : h0 + n + h - 4;
+        const int src = h < 4 ? h0 + n - 4 + h : h0 + h - 4;
+        tp[dst * W + x] = tp[src * W + x];
+    }
 }
 
 // Scratch in shared memory after the input tiles: per (chunk, line) the
@@ -110,31 +124,51 @@ struct ChunkScratch {
     T *fz, *bz;
 };
 
-// Carry into chunk c from the chunk values e (end values, scanning the
-// chunks before c, or start values scanning those after it when STEP = -1).
+// Carry into chunk c: the end values e of the chunks before it (STEP = 1,
+// forward sweep) or the start values of the chunks after it (STEP = -1,
+// backward), folded from the farthest in over depth chunks, or over the
+// whole line once and scaled by 1 / (1 - rho^n).  A chunk propagates an
+// incoming carry by rho^L (rho^nv for the last, possibly short, chunk); the
+// first chunk folded multiplies zero, so only a later visit to chunk C-1
+// needs its own multiplier.  The visits run as at most two unwrapped
+// segments of e.
 template <typename T, int STEP>
 __device__ __forceinline__ T chunk_carry(const T *e, const LineOp<T> &op, int ti, int W, int l, int c, int C)
 {
     const int K = op.depth[ti];
-    int cc = c;
-    if (K < C) {
-        cc = c - STEP * K;
-        cc = cc < 0 ? cc + C : (cc >= C ? cc - C : cc);
-    }
-    const T mf = op.mfull[ti], ml = op.mlast[ti];
+    const bool full = K >= C;
+    const T mf = op.mfull[ti];
     T carry = T(0);
-    for (int k = 0; k < K; ++k) {
-        carry = fma(cc == C - 1 ? ml : mf, carry, e[cc * W + l]);
-        cc += STEP;
-        cc = cc == C ? 0 : (cc < 0 ? C - 1 : cc);
+    if (STEP == 1) {
+        int s = full ? c : c - K;
+        s = s < 0 ? s + C : s;
+        const int n1 = min(K, C - s);  // chunks s .. s+n1-1, then 0 .. K-n1-1
+        const T *p = e + s * W + l;
+        for (int k = 1; k < n1; ++k, p += W) carry = fma(mf, carry, *p);
+        carry = fma(s + n1 == C ? op.mlast[ti] : mf, carry, *p);
+        p = e + l;
+        for (int k = n1; k < K; ++k, p += W) carry = fma(mf, carry, *p);
+    } else {
+        int s = full ? c : c + K;
+        s = s >= C ? s - C : s;
+        const int n1 = min(K, s + 1);  // chunks s .. s-n1+1, then C-1 .. C-K+n1
+        const T *p = e + s * W + l;
+        for (int k = 0; k < n1; ++k, p -= W) carry = fma(mf, carry, *p);
+        if (K > n1) {
+            p = e + (C - 1) * W + l;
+            carry = fma(op.mlast[ti], carry, *p);
+            p -= W;
+            for (int k = n1 + 1; k < K; ++k, p -= W) carry = fma(mf, carry, *p);
+        }
     }
-    return K < C ? carry : carry * op.wrap;
+    return full ? carry * op.wrap : carry;
 }
 
 // Solves one operator for one chunk; the solved values end in r[] (chunk
-// local).  load(w) fills the L+8 input window u[cs-4 .. cs+L+3] (indices mod
-// n); the window is dead once the stencil is evaluated.  nv = points of the
-// chunk inside the line (L except for the last chunk of a ragged line).
+// local).  load(w) fills the L+8 input window u[cs-4 .. cs+L+3] from the
+// staged line and its periodic halos; the window is dead once the stencil is
+// evaluated.  nv = points of the chunk inside the line (L except for the last
+// chunk of a ragged line; the window values past its end are never used).
 template <typename T, int L, typename Load>
 __device__ __forceinline__ void chunk_solve(const LineOp<T> &op, int kind, const Load &load, T (&r)[L],
                                             const ChunkScratch<T> &sc, int W, int l, int c, int C, int nv,
@@ -281,7 +315,7 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
         uint64_t *bar = &bars[slot];
         mbar_arrive_expect_tx(bar, (uint32_t)((size_t)prog.ntiles * nbox * box_n * W * sizeof(T)));
         for (int ti = 0; ti < prog.ntiles; ++ti) {
-            T *tp = reinterpret_cast<T *>(smem_raw + slot * slot_bytes + ti * tile_bytes);
+            T *tp = reinterpret_cast<T *>(smem_raw + slot * slot_bytes + ti * tile_bytes) + kHalo * W;
             for (int b = 0; b < nbox; ++b) {
                 if (dir == DY)
                     tma_load_3d(tp + (size_t)b * box_n * W, &maps.m[ti], bar, x0, b * box_n, o);
@@ -293,7 +327,6 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
     const ChunkScratch<T> sc = carve_scratch<T>(smem_raw + (PERSIST ? 2 : 1) * slot_bytes, C, W);
     const int cs = c * L;
     const int nv = min(L, n - cs);
-    const bool wraps = cs < 4 || cs + L + 4 > n;
     const size_t ostride = dir == DY ? (size_t)nx : (size_t)nx * ny;
     const long step = PERSIST ? (long)gridDim.x : ntiles;
     long tile = blockIdx.x;
@@ -312,9 +345,15 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
         }
         const int x0 = (int)(tile % tiles_x) * W;
         const int o = (int)(tile / tiles_x);
-        const unsigned char *base = smem_raw + slot * slot_bytes;
-        auto col = [&](int ti) { return reinterpret_cast<const T *>(base + ti * tile_bytes) + l; };
-        auto tile_at = [&](int ti, int j) { return col(ti)[(cs + j) * W]; };
+        unsigned char *base = smem_raw + slot * slot_bytes;
+        fill_halos_yz<T>(base, tile_bytes, prog.ntiles, n, W, kHalo);
+        fence_proxy_async_smem();  // the halo rows are refilled by TMA two tiles later
+        __syncthreads();
+        // window of this chunk: rows kHalo + cs - 4 ...
+        auto col = [&](int ti) {
+            return reinterpret_cast<const T *>(base + ti * tile_bytes) + (kHalo + cs - 4) * W + l;
+        };
+        auto tile_at = [&](int ti, int j) { return col(ti)[(4 + j) * W]; };
         const bool live = x0 + l < nx;
         const size_t obase = (size_t)(x0 + l) + (dir == DY ? (size_t)nx * ny * o : (size_t)nx * o) +
                              (size_t)cs * ostride;
@@ -327,16 +366,10 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
             auto load = [&](T(&w)[L + 8]) {
                 if (cb) {
 #pragma unroll
-                    for (int j = 0; j < L + 8; ++j) {
-                        const int idx = wraps ? wrap_index(cs - 4 + j, n, n - 1) : cs - 4 + j;
-                        w[j] = ca[idx * W] * cb[idx * W];
-                    }
+                    for (int j = 0; j < L + 8; ++j) w[j] = ca[j * W] * cb[j * W];
                 } else {
 #pragma unroll
-                    for (int j = 0; j < L + 8; ++j) {
-                        const int idx = wraps ? wrap_index(cs - 4 + j, n, n - 1) : cs - 4 + j;
-                        w[j] = ca[idx * W];
-                    }
+                    for (int j = 0; j < L + 8; ++j) w[j] = ca[j * W];
                 }
             };
             chunk_solve<T, L>(so.op, so.kind, load, r, sc, W, l, c, C, nv, c * W + l);
@@ -353,13 +386,14 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
                         dst += ostride;
                     }
                 } else {
+                    size_t p = obase;
 #pragma unroll
                     for (int j = 0; j < L; ++j) {
                         if (j < nv) {
-                            const size_t p = obase + (size_t)j * ostride;
                             if (so.out_f64) flush_point<T, double>(so, p, res[j]);
                             else flush_point<T, T>(so, p, res[j]);
                         }
+                        p += ostride;
                     }
                 }
             }
@@ -420,6 +454,27 @@ __device__ __forceinline__ void flush_vec(const StageOp<T> &so, size_t p0, const
     }
 }
 
+// Fills the halos of ntiles staged x tiles of `rows` padded rows whose
+// point i sits at element kHalo + i: elements 0 .. 3 from points n-4 .. n-1,
+// elements n+4 .. n+7 from points 0 .. 3, moved as 16-byte vectors.
+template <typename T>
+__device__ __forceinline__ void fill_halos_x(unsigned char *base, size_t tile_bytes, int ntiles, int rows,
+                                             int pitch, int n)
+{
+    using VT = typename Vec4<T>::type;
+    constexpr int V = Vec4<T>::N;
+    constexpr int per_row = 8 / V;
+    const int per = rows * per_row;
+    for (int i = threadIdx.x; i < per * ntiles; i += blockDim.x) {
+        const int ti = i / per, r = i - ti * per;
+        const int rr = r / per_row, h = (r - rr * per_row) * V;
+        T *row = reinterpret_cast<T *>(base + ti * tile_bytes) + (size_t)rr * pitch;
+        const int dst = h < 4 ? h : n + h;
+        const int src = h < 4 ? n + h : h;
+        *reinterpret_cast<VT *>(row + dst) = *reinterpret_cast<const VT *>(row + src);
+    }
+}
+
 template <typename T, int W, int L, bool ACC, bool PERSIST>
 __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
     ls_stage_x(const __grid_constant__ StageProgram<T> prog, long nlines, int pitch, size_t tile_bytes,
@@ -447,7 +502,7 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
         uint64_t *bar = &bars[slot];
         mbar_arrive_expect_tx(bar, row_bytes * (uint32_t)rows * (uint32_t)prog.ntiles);
         for (int ti = 0; ti < prog.ntiles; ++ti) {
-            T *tp = reinterpret_cast<T *>(smem_raw + slot * slot_bytes + ti * tile_bytes);
+            T *tp = reinterpret_cast<T *>(smem_raw + slot * slot_bytes + ti * tile_bytes) + kHalo;
             for (int rr = 0; rr < rows; ++rr)
                 bulk_load(tp + (size_t)rr * pitch, prog.in[ti] + (size_t)(l0 + rr) * n, row_bytes, bar);
         }
@@ -455,7 +510,6 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
     const ChunkScratch<T> sc = carve_scratch<T>(smem_raw + (PERSIST ? 2 : 1) * slot_bytes, C, W);
     const int cs = c * L;
     const int nv = min(L, n - cs);
-    const bool wraps = cs < 4 || cs + L + 4 > n;
     const long step = PERSIST ? (long)gridDim.x : ntiles;
     long tile = blockIdx.x;
     if (t == 0 && tile < ntiles) issue(tile, 0);
@@ -474,9 +528,15 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
         const long l0 = tile * W;
         const int rows = (int)min((long)W, nlines - l0);
         const int lr = l < rows ? l : 0;  // rows past the end compute on row 0 and store nothing
-        const unsigned char *base = smem_raw + slot * slot_bytes;
-        auto row = [&](int ti) { return reinterpret_cast<const T *>(base + ti * tile_bytes) + (size_t)lr * pitch; };
-        auto tile_at = [&](int ti, int j) { return row(ti)[cs + j]; };
+        unsigned char *base = smem_raw + slot * slot_bytes;
+        fill_halos_x<T>(base, tile_bytes, prog.ntiles, rows, pitch, n);
+        fence_proxy_async_smem();  // halo elements are refilled by bulk copies two tiles later
+        __syncthreads();
+        // window of this chunk: elements cs .. cs+L+7 (points cs-4 .. cs+L+3)
+        auto row = [&](int ti) {
+            return reinterpret_cast<const T *>(base + ti * tile_bytes) + (size_t)lr * pitch + cs;
+        };
+        auto tile_at = [&](int ti, int j) { return row(ti)[kHalo + j]; };
         T r[L];
         T acc[ACC ? L : 1];
         for (int k = 0; k < prog.nops; ++k) {
@@ -487,9 +547,8 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
                 if (rb) {
 #pragma unroll
                     for (int j = 0; j < L + 8; j += V) {
-                        const int idx = wraps ? wrap_index(cs - 4 + j, n, n - V) : cs - 4 + j;
-                        const VT qa = *reinterpret_cast<const VT *>(ra + idx);
-                        const VT qb = *reinterpret_cast<const VT *>(rb + idx);
+                        const VT qa = *reinterpret_cast<const VT *>(ra + j);
+                        const VT qb = *reinterpret_cast<const VT *>(rb + j);
                         const T *ea = reinterpret_cast<const T *>(&qa);
                         const T *eb = reinterpret_cast<const T *>(&qb);
 #pragma unroll
@@ -498,8 +557,7 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
                 } else {
 #pragma unroll
                     for (int j = 0; j < L + 8; j += V) {
-                        const int idx = wraps ? wrap_index(cs - 4 + j, n, n - V) : cs - 4 + j;
-                        const VT qa = *reinterpret_cast<const VT *>(ra + idx);
+                        const VT qa = *reinterpret_cast<const VT *>(ra + j);
                         const T *ea = reinterpret_cast<const T *>(&qa);
 #pragma unroll
                         for (int v = 0; v < V; ++v) w[j + v] = ea[v];
@@ -586,7 +644,8 @@ static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir
             if (so.flush && (!al16(so.out) || !al16(so.base) || !al16(so.out2) || !al16(so.base2)))
                 return X3D_EUNSUPPORTED;
         }
-        int pitch = n + V;
+        // row: kHalo halo elements, the line, and room for the last chunk's window
+        int pitch = C * L + 2 * kHalo;
         while (((size_t)pitch * es / 16) % 2 == 0) pitch += V;
         const size_t tile = ((size_t)W * pitch * es + 127) & ~(size_t)127;
         const size_t smem = (PERSIST ? 2 : 1) * prog.ntiles * tile + scratch_bytes(C, W, es);
@@ -607,7 +666,10 @@ static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir
     const int align_rows = (int)(128 / (W * es) > 0 ? 128 / (W * es) : 1);
     box_n = (box_n + align_rows - 1) / align_rows * align_rows;
     if (box_n > 256) return X3D_EUNSUPPORTED;
-    const size_t tile = ((size_t)nb * box_n * W * es + 127) & ~(size_t)127;
+    // rows: kHalo halo rows (kHalo * W * es is a multiple of 128 bytes, so the
+    // boxes land 128-byte aligned), the boxes, and room for the last window
+    const int rows = kHalo + std::max(nb * box_n, C * L + kHalo);
+    const size_t tile = ((size_t)rows * W * es + 127) & ~(size_t)127;
     const size_t smem = (PERSIST ? 2 : 1) * prog.ntiles * tile + scratch_bytes(C, W, es);
     if (smem + 1024 > ctx->smem_optin) return X3D_EUNSUPPORTED;
     StageMaps maps;
@@ -742,15 +804,16 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
                 const uint32_t row_bytes = (uint32_t)(n * sizeof(T));
                 mbar_arrive_expect_tx(&bar, row_bytes * (uint32_t)rows);
                 for (int rr = 0; rr < rows; ++rr)
-                    bulk_load(tile + (size_t)rr * J.pitch, J.in + (size_t)(l0 + rr) * n, row_bytes, &bar);
+                    bulk_load(tile + (size_t)rr * J.pitch + kHalo, J.in + (size_t)(l0 + rr) * n, row_bytes, &bar);
             } else {
                 fence_tensormap_acquire(&J.tmap);
                 mbar_arrive_expect_tx(&bar, (uint32_t)((size_t)J.nbox * J.box_n * W * sizeof(T)));
+                T *dst = tile + (size_t)J.halo * W;
                 for (int b = 0; b < J.nbox; ++b) {
                     if (dir == DY)
-                        tma_load_3d(tile + (size_t)b * J.box_n * W, &J.tmap, &bar, x0, b * J.box_n, o);
+                        tma_load_3d(dst + (size_t)b * J.box_n * W, &J.tmap, &bar, x0, b * J.box_n, o);
                     else
-                        tma_load_3d(tile + (size_t)b * J.box_n * W, &J.tmap, &bar, x0, o, b * J.box_n);
+                        tma_load_3d(dst + (size_t)b * J.box_n * W, &J.tmap, &bar, x0, o, b * J.box_n);
                 }
             }
         }
@@ -761,6 +824,10 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
             return;
         }
         phase ^= 1;
+        if (dir == DX) fill_halos_x<T>(smem_raw, 0, 1, rows, J.pitch, n);
+        else fill_halos_yz<T>(smem_raw, 0, 1, n, W, J.halo);
+        fence_proxy_async_smem();  // the next item's copies overwrite the halos
+        __syncthreads();
         const bool active = t < W * C;
         const int l = active ? t % W : 0, c = active ? t / W : 0;
         const int q = t;  // scratch slot: active threads use c*W + l == t
@@ -770,13 +837,11 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
         T r[L];
         if (dir == DX) {
             const int lr = l < rows ? l : 0;
-            const T *row = tile + (size_t)lr * J.pitch;
-            const bool wraps = cs < 4 || cs + L + 4 > n;
+            const T *row = tile + (size_t)lr * J.pitch + cs;  // points cs-4 .. cs+L+3
             auto load = [&](T(&w)[L + 8]) {
 #pragma unroll
                 for (int j = 0; j < L + 8; j += V) {
-                    const int idx = wraps ? wrap_index(cs - 4 + j, n, n - V) : cs - 4 + j;
-                    const VT qa = *reinterpret_cast<const VT *>(row + idx);
+                    const VT qa = *reinterpret_cast<const VT *>(row + j);
                     const T *ea = reinterpret_cast<const T *>(&qa);
 #pragma unroll
                     for (int v = 0; v < V; ++v) w[j + v] = ea[v];
@@ -799,14 +864,10 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
                 }
             }
         } else {
-            const T *col = tile + l;
-            const bool wraps = cs < 4 || cs + L + 4 > n;
+            const T *col = tile + (size_t)(J.halo + cs - 4) * W + l;  // points cs-4 .. cs+L+3
             auto load = [&](T(&w)[L + 8]) {
 #pragma unroll
-                for (int j = 0; j < L + 8; ++j) {
-                    const int idx = wraps ? wrap_index(cs - 4 + j, n, n - 1) : cs - 4 + j;
-                    w[j] = col[idx * W];
-                }
+                for (int j = 0; j < L + 8; ++j) w[j] = col[j * W];
             };
             const bool live = active && x0 + l < J.nx;
             const size_t ostride = dir == DY ? (size_t)J.nx : (size_t)J.nx * J.ny;
@@ -849,7 +910,7 @@ bool plan_batch_job(BatchJob<T> &J, int L, size_t *tile_bytes)
     J.W = W;
     if (J.dir == DX) {
         if (n % V || (reinterpret_cast<uintptr_t>(J.in) & 15)) return false;
-        int pitch = n + V;
+        int pitch = J.C * L + 2 * kHalo;
         while (((size_t)pitch * es / 16) % 2 == 0) pitch += V;
         J.pitch = pitch;
         J.span = (long)J.ny * J.nz;
@@ -867,7 +928,12 @@ bool plan_batch_job(BatchJob<T> &J, int L, size_t *tile_bytes)
     J.nbox = nb;
     J.span = (J.nx + W - 1) / W;
     J.ntiles = J.span * (J.dir == DY ? J.nz : J.ny);
-    *tile_bytes = ((size_t)nb * box_n * W * es + 127) & ~(size_t)127;
+    // halo rows in front of the boxes: at least kHalo, keeping the boxes
+    // 128-byte aligned
+    J.halo = kHalo;
+    while (((size_t)J.halo * W * es) % 128) ++J.halo;
+    const int rows = J.halo + std::max(nb * box_n, J.C * L + kHalo);
+    *tile_bytes = ((size_t)rows * W * es + 127) & ~(size_t)127;
     auto enc = encode_tiled();
     if (!enc) return false;
     cuuint64_t gdim[3] = {(cuuint64_t)J.nx, (cuuint64_t)J.ny, (cuuint64_t)J.nz};

@@ -65,6 +65,7 @@ struct BatchJob {
     int kind[kMaxStageOps];
     int nops, dir, n, nx, ny, nz;
     int W, C, box_n, nbox, pitch;
+    int halo;    // y/z: staged rows in front of the line (periodic halo + alignment)
     long span;   // x: number of lines; y/z: tiles across x
     long tile0;  // first work item of the job
     long ntiles;
