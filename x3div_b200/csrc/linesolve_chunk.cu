@@ -39,6 +39,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <cmath>
 
 #include "linesolve_chunk.h"
 #include "ptx.cuh"
@@ -235,6 +236,63 @@ __device__ __forceinline__ void chunk_solve(const LineOp<T> &op, int kind, const
     }
 }
 
+// The same solve with the carry fixes folded into two precomputed responses.
+// Both local sweeps run before the first barrier (the backward one on the
+// local forward values), and since the solve is linear,
+//   y_j = y_j(local) + F h_j + B g_j,
+//   h_j = sum_{m=j}^{len-1} rho^(2m-j+1),   g_j = rho^(len-j),
+// with F the true v just before the chunk and B the true y just after it.
+// The chunk's start value for the backward scan is y_0(local) + F h_0, so
+// each thread publishes it after finding its own F.  h and g (resp[0..1],
+// or resp[2..3] for a short last chunk) are kernel parameters indexed by
+// compile-time constants, so each fix is one fused multiply-add per carry.
+template <typename T, int L, typename Load>
+__device__ __forceinline__ void chunk_solve_resp(const StageOp<T> &so, const Load &load, T (&r)[L],
+                                                 const ChunkScratch<T> &sc, int W, int l, int c, int C,
+                                                 int nv, int q)
+{
+    constexpr int ti = L == kChunkLong<T> ? 0 : 1;
+    const LineOp<T> &op = so.op;
+    {
+        T w[L + 8];
+        load(w);
+        chunk_stencil_kind<T, L>(so.kind, w, r, op);
+    }
+    const T rho = op.rho;
+    T v = T(0);
+#pragma unroll
+    for (int j = 0; j < L; ++j) {
+        v = fma(rho, v, r[j]);
+        r[j] = v;
+    }
+    if (nv < L) {  // short last chunk: its end is point nv - 1, nothing past it
+#pragma unroll
+        for (int j = 0; j < L; ++j) {
+            if (j == nv - 1) v = r[j];
+            if (j >= nv) r[j] = T(0);
+        }
+    }
+    T y = T(0);
+#pragma unroll
+    for (int j = L - 1; j >= 0; --j) {
+        y = fma(rho, y, r[j]);
+        r[j] = y;
+    }
+    sc.fz[q] = v;
+    __syncthreads();
+    const T F = chunk_carry<T, 1>(sc.fz, op, ti, W, l, c, C);
+    sc.bz[q] = fma(F, nv == L ? so.resp[0][0] : so.resp[2][0], y);
+    __syncthreads();
+    const T B = chunk_carry<T, -1>(sc.bz, op, ti, W, l, c, C);
+    if (nv == L) {
+#pragma unroll
+        for (int j = 0; j < L; ++j) r[j] = fma(F, so.resp[0][j], fma(B, so.resp[1][j], r[j]));
+    } else {
+#pragma unroll
+        for (int j = 0; j < L; ++j) r[j] = fma(F, so.resp[2][j], fma(B, so.resp[3][j], r[j]));
+    }
+}
+
 template <typename T>
 __device__ __forceinline__ ChunkScratch<T> carve_scratch(unsigned char *base, int C, int W)
 {
@@ -285,6 +343,32 @@ __device__ __forceinline__ void flush_point(const StageOp<T> &so, size_t p, T a)
     if (so.out2) {
         const U *b2 = static_cast<const U *>(so.base2);
         static_cast<U *>(so.out2)[p] = (b2 ? b2[p] : U(0)) + (U)so.scale2 * v;
+    }
+}
+
+// Writes one thread's solved chunk of a y/z line (points j < nv), each point
+// ostride elements after the previous one.
+template <typename T, int L>
+__device__ __forceinline__ void flush_yz(const StageOp<T> &so, const T (&res)[L], size_t obase, size_t ostride,
+                                         int nv)
+{
+    if (!so.base && !so.out2 && !so.out_f64 && so.sign == 1.0) {
+        T *dst = static_cast<T *>(so.out) + obase;
+#pragma unroll
+        for (int j = 0; j < L; ++j) {
+            if (j < nv) *dst = res[j];
+            dst += ostride;
+        }
+    } else {
+        size_t p = obase;
+#pragma unroll
+        for (int j = 0; j < L; ++j) {
+            if (j < nv) {
+                if (so.out_f64) flush_point<T, double>(so, p, res[j]);
+                else flush_point<T, T>(so, p, res[j]);
+            }
+            p += ostride;
+        }
     }
 }
 
@@ -359,7 +443,10 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
                              (size_t)cs * ostride;
         T r[L];
         T acc[ACC ? L : 1];
-        for (int k = 0; k < prog.nops; ++k) {
+        // operators unrolled: every StageOp field is a compile-time offset into the parameters
+#pragma unroll
+        for (int k = 0; k < kMaxStageOps; ++k) {
+            if (k >= prog.nops) break;
             const StageOp<T> &so = prog.ops[k];
             const T *ca = col(so.src_a);
             const T *cb = so.src_b >= 0 ? col(so.src_b) : nullptr;
@@ -372,30 +459,12 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
                     for (int j = 0; j < L + 8; ++j) w[j] = ca[j * W];
                 }
             };
-            chunk_solve<T, L>(so.op, so.kind, load, r, sc, W, l, c, C, nv, c * W + l);
-            if constexpr (ACC) accumulate<T, L>(so, acc, r, nv, tile_at);
-            const T *res;
-            if constexpr (ACC) res = acc;
-            else res = r;
-            if (so.flush && live) {
-                if (!so.base && !so.out2 && !so.out_f64 && so.sign == 1.0) {
-                    T *dst = static_cast<T *>(so.out) + obase;
-#pragma unroll
-                    for (int j = 0; j < L; ++j) {
-                        if (j < nv) *dst = res[j];
-                        dst += ostride;
-                    }
-                } else {
-                    size_t p = obase;
-#pragma unroll
-                    for (int j = 0; j < L; ++j) {
-                        if (j < nv) {
-                            if (so.out_f64) flush_point<T, double>(so, p, res[j]);
-                            else flush_point<T, T>(so, p, res[j]);
-                        }
-                        p += ostride;
-                    }
-                }
+            chunk_solve_resp<T, L>(so, load, r, sc, W, l, c, C, nv, c * W + l);
+            if constexpr (ACC) {
+                accumulate<T, L>(so, acc, r, nv, tile_at);
+                if (so.flush && live) flush_yz<T, L>(so, acc, obase, ostride, nv);
+            } else {
+                if (so.flush && live) flush_yz<T, L>(so, r, obase, ostride, nv);
             }
         }
         if (PERSIST) __syncthreads();  // the slot is refilled two tiles later
@@ -419,8 +488,8 @@ struct Vec4<double> {
 
 // Writes V consecutive results of one thread's chunk starting at element p0
 // as 16-byte vectors of the output type U (T, or double for out_f64).
-template <typename T, typename U, int V>
-__device__ __forceinline__ void flush_vec(const StageOp<T> &so, size_t p0, const T *a)
+template <typename T, typename U, int V, int L>
+__device__ __forceinline__ void flush_vec(const StageOp<T> &so, size_t p0, const T (&res)[L], int j0)
 {
     using UV = typename Vec4<U>::type;
     constexpr int VU = Vec4<U>::N;
@@ -429,7 +498,7 @@ __device__ __forceinline__ void flush_vec(const StageOp<T> &so, size_t p0, const
         UV q;
         U *v = reinterpret_cast<U *>(&q);
 #pragma unroll
-        for (int e = 0; e < VU; ++e) v[e] = (U)so.sign * (U)a[h + e];
+        for (int e = 0; e < VU; ++e) v[e] = (U)so.sign * (U)res[j0 + h + e];
         if (so.base) {
             const UV bq = *reinterpret_cast<const UV *>(static_cast<const U *>(so.base) + p0 + h);
             const U *be = reinterpret_cast<const U *>(&bq);
@@ -450,6 +519,21 @@ __device__ __forceinline__ void flush_vec(const StageOp<T> &so, size_t p0, const
                 for (int e = 0; e < VU; ++e) v2[e] = (U)so.scale2 * v[e];
             }
             *reinterpret_cast<UV *>(static_cast<U *>(so.out2) + p0 + h) = q2;
+        }
+    }
+}
+
+// Writes one thread's solved chunk of an x line (points j < nv) as 16-byte
+// vectors starting at element p0.
+template <typename T, int L>
+__device__ __forceinline__ void flush_x(const StageOp<T> &so, const T (&res)[L], size_t p0, int nv)
+{
+    constexpr int V = Vec4<T>::N;
+#pragma unroll
+    for (int j = 0; j < L; j += V) {
+        if (j < nv) {
+            if (so.out_f64) flush_vec<T, double, V, L>(so, p0 + j, res, j);
+            else flush_vec<T, T, V, L>(so, p0 + j, res, j);
         }
     }
 }
@@ -539,7 +623,10 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
         auto tile_at = [&](int ti, int j) { return row(ti)[kHalo + j]; };
         T r[L];
         T acc[ACC ? L : 1];
-        for (int k = 0; k < prog.nops; ++k) {
+        // operators unrolled: every StageOp field is a compile-time offset into the parameters
+#pragma unroll
+        for (int k = 0; k < kMaxStageOps; ++k) {
+            if (k >= prog.nops) break;
             const StageOp<T> &so = prog.ops[k];
             const T *ra = row(so.src_a);
             const T *rb = so.src_b >= 0 ? row(so.src_b) : nullptr;
@@ -564,20 +651,12 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
                     }
                 }
             };
-            chunk_solve<T, L>(so.op, so.kind, load, r, sc, W, l, c, C, nv, c * W + l);
-            if constexpr (ACC) accumulate<T, L>(so, acc, r, nv, tile_at);
-            const T *res;
-            if constexpr (ACC) res = acc;
-            else res = r;
-            if (so.flush && l < rows) {
-                const size_t p0 = (size_t)(l0 + l) * n + cs;
-#pragma unroll
-                for (int j = 0; j < L; j += V) {
-                    if (j < nv) {
-                        if (so.out_f64) flush_vec<T, double, V>(so, p0 + j, res + j);
-                        else flush_vec<T, T, V>(so, p0 + j, res + j);
-                    }
-                }
+            chunk_solve_resp<T, L>(so, load, r, sc, W, l, c, C, nv, c * W + l);
+            if constexpr (ACC) {
+                accumulate<T, L>(so, acc, r, nv, tile_at);
+                if (so.flush && l < rows) flush_x<T, L>(so, acc, (size_t)(l0 + l) * n + cs, nv);
+            } else {
+                if (so.flush && l < rows) flush_x<T, L>(so, r, (size_t)(l0 + l) * n + cs, nv);
             }
         }
         if (PERSIST) __syncthreads();  // the slot is refilled two tiles later
@@ -619,10 +698,43 @@ static unsigned persistent_grid(x3d_ctx_s *ctx, Kern kern, int threads, size_t s
     return (unsigned)(g < ntiles ? g : ntiles);
 }
 
+// Carry responses of chunk_solve_resp for chunk length L on lines of n
+// points: h_j = rho^(j+1) sum_{i < len-j} rho^(2i) and g_j = rho^(len-j),
+// len = L (resp[0..1]) and len = the last chunk's length (resp[2..3]).
+template <typename T>
+static void fill_resp(StageProgram<T> &p, int L, int n)
+{
+    const int C = (n + L - 1) / L, last = n - (C - 1) * L;
+    for (int k = 0; k < p.nops; ++k) {
+        const double al = p.ops[k].op.alfa;
+        const double rho = al == 0.0 ? 0.0 : -2.0 * al / (1.0 + std::sqrt(1.0 - 4.0 * al * al));
+        double pw[kChunkLong<T>];
+        double q = 1.0;
+        for (int j = 0; j < kChunkLong<T>; ++j) pw[j] = (q *= rho);  // rho^(j+1)
+        auto fill = [&](T *h, T *g, int len) {
+            double S = 0.0, G = 1.0;
+            for (int j = kChunkLong<T> - 1; j >= 0; --j) {
+                if (j >= len) {
+                    h[j] = g[j] = T(0);
+                    continue;
+                }
+                S = 1.0 + rho * rho * S;
+                G *= rho;
+                h[j] = (T)(pw[j] * S);
+                g[j] = (T)G;
+            }
+        };
+        fill(p.ops[k].resp[0], p.ops[k].resp[1], L);
+        fill(p.ops[k].resp[2], p.ops[k].resp[3], last);
+    }
+}
+
 template <typename T, int W, int L, bool PERSIST>
-static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir, int nx, int ny,
+static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog_in, int dir, int nx, int ny,
                             int nz)
 {
+    StageProgram<T> prog = prog_in;
+    fill_resp(prog, L, prog.ops[0].op.n);
     bool acc = false;
     for (int k = 0; k < prog.nops; ++k)
         acc = acc || !plain(StageOpView{prog.ops[k].flush, prog.ops[k].accumulate, prog.ops[k].mul_tile});

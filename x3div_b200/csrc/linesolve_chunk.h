@@ -30,6 +30,11 @@ struct StageOp {
     short accumulate;
     short flush;
     short out_f64;  // out, base, out2, base2 hold double rather than T
+    // Responses of a chunk's solved values to its carries, for the launch's
+    // chunk length L (set by launch_stage): y_j = y_j(local) + F resp[0][j]
+    // + B resp[1][j] for a full chunk, resp[2], resp[3] for a short last
+    // chunk, F and B the forward and backward carries (see chunk_solve_resp).
+    T resp[4][kChunkLong<T>];
 };
 
 // Up to six operators along one direction over up to three staged inputs of
