@@ -236,6 +236,32 @@ __device__ __forceinline__ void chunk_solve(const LineOp<T> &op, int kind, const
     }
 }
 
+// 16-byte vector of T.
+template <typename T>
+struct Vec4;
+template <>
+struct Vec4<float> {
+    static constexpr int N = 4;
+    using type = float4;
+};
+template <>
+struct Vec4<double> {
+    static constexpr int N = 2;
+    using type = double2;
+};
+
+// Shared-memory copy of the carry responses of a stage's operators, laid
+// out [operator][4][L] (see StageOp::resp), made once per CTA.
+template <typename T, int L>
+__device__ __forceinline__ void load_resp(const StageProgram<T> &prog, T *dst)
+{
+    const int total = prog.nops * 4 * L;
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+        const int k = i / (4 * L), rem = i - k * 4 * L, a = rem / L, j = rem - a * L;
+        dst[i] = prog.ops[k].resp[a][j];
+    }
+}
+
 // The same solve with the carry fixes folded into two precomputed responses.
 // Both local sweeps run before the first barrier (the backward one on the
 // local forward values), and since the solve is linear,
@@ -244,12 +270,13 @@ __device__ __forceinline__ void chunk_solve(const LineOp<T> &op, int kind, const
 // with F the true v just before the chunk and B the true y just after it.
 // The chunk's start value for the backward scan is y_0(local) + F h_0, so
 // each thread publishes it after finding its own F.  h and g (resp[0..1],
-// or resp[2..3] for a short last chunk) are kernel parameters indexed by
-// compile-time constants, so each fix is one fused multiply-add per carry.
+// or resp[2..3] for a short last chunk) come from this operator's block of
+// the shared-memory copy as 16-byte vectors, so each fix is one fused
+// multiply-add per carry and half a load per point.
 template <typename T, int L, typename Load>
-__device__ __forceinline__ void chunk_solve_resp(const StageOp<T> &so, const Load &load, T (&r)[L],
-                                                 const ChunkScratch<T> &sc, int W, int l, int c, int C,
-                                                 int nv, int q)
+__device__ __forceinline__ void chunk_solve_resp(const StageOp<T> &so, const T *resp, const Load &load,
+                                                 T (&r)[L], const ChunkScratch<T> &sc, int W, int l, int c,
+                                                 int C, int nv, int q)
 {
     constexpr int ti = L == kChunkLong<T> ? 0 : 1;
     const LineOp<T> &op = so.op;
@@ -281,15 +308,21 @@ __device__ __forceinline__ void chunk_solve_resp(const StageOp<T> &so, const Loa
     sc.fz[q] = v;
     __syncthreads();
     const T F = chunk_carry<T, 1>(sc.fz, op, ti, W, l, c, C);
-    sc.bz[q] = fma(F, nv == L ? so.resp[0][0] : so.resp[2][0], y);
+    const T *h = resp + (nv == L ? 0 : 2 * L);
+    const T *g = h + L;
+    sc.bz[q] = fma(F, h[0], y);
     __syncthreads();
     const T B = chunk_carry<T, -1>(sc.bz, op, ti, W, l, c, C);
-    if (nv == L) {
+    using VT = typename Vec4<T>::type;
+    constexpr int V = Vec4<T>::N;
 #pragma unroll
-        for (int j = 0; j < L; ++j) r[j] = fma(F, so.resp[0][j], fma(B, so.resp[1][j], r[j]));
-    } else {
+    for (int j = 0; j < L; j += V) {
+        const VT hv = *reinterpret_cast<const VT *>(h + j);
+        const VT gv = *reinterpret_cast<const VT *>(g + j);
+        const T *he = reinterpret_cast<const T *>(&hv);
+        const T *ge = reinterpret_cast<const T *>(&gv);
 #pragma unroll
-        for (int j = 0; j < L; ++j) r[j] = fma(F, so.resp[2][j], fma(B, so.resp[3][j], r[j]));
+        for (int v = 0; v < V; ++v) r[j + v] = fma(F, he[v], fma(B, ge[v], r[j + v]));
     }
 }
 
@@ -387,6 +420,9 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
     const int l = t % W, c = t / W;
     const int tiles_x = (nx + W - 1) / W;
     const size_t slot_bytes = (size_t)prog.ntiles * tile_bytes;
+    T *resp_s = reinterpret_cast<T *>(smem_raw + (PERSIST ? 2 : 1) * slot_bytes +
+                                      (((size_t)2 * C * W * sizeof(T) + 15) & ~(size_t)15));
+    load_resp<T, L>(prog, resp_s);
     if (t == 0) {
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
@@ -443,10 +479,7 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
                              (size_t)cs * ostride;
         T r[L];
         T acc[ACC ? L : 1];
-        // operators unrolled: every StageOp field is a compile-time offset into the parameters
-#pragma unroll
-        for (int k = 0; k < kMaxStageOps; ++k) {
-            if (k >= prog.nops) break;
+        for (int k = 0; k < prog.nops; ++k) {
             const StageOp<T> &so = prog.ops[k];
             const T *ca = col(so.src_a);
             const T *cb = so.src_b >= 0 ? col(so.src_b) : nullptr;
@@ -459,7 +492,7 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
                     for (int j = 0; j < L + 8; ++j) w[j] = ca[j * W];
                 }
             };
-            chunk_solve_resp<T, L>(so, load, r, sc, W, l, c, C, nv, c * W + l);
+            chunk_solve_resp<T, L>(so, resp_s + k * 4 * L, load, r, sc, W, l, c, C, nv, c * W + l);
             if constexpr (ACC) {
                 accumulate<T, L>(so, acc, r, nv, tile_at);
                 if (so.flush && live) flush_yz<T, L>(so, acc, obase, ostride, nv);
@@ -473,18 +506,6 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
 
 // ---------------------------------------------------------------------------
 // x-lines.
-template <typename T>
-struct Vec4;
-template <>
-struct Vec4<float> {
-    static constexpr int N = 4;
-    using type = float4;
-};
-template <>
-struct Vec4<double> {
-    static constexpr int N = 2;
-    using type = double2;
-};
 
 // Writes V consecutive results of one thread's chunk starting at element p0
 // as 16-byte vectors of the output type U (T, or double for out_f64).
@@ -574,6 +595,9 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
     const int l = t % W, c = t / W;
     const uint32_t row_bytes = (uint32_t)(n * sizeof(T));
     const size_t slot_bytes = (size_t)prog.ntiles * tile_bytes;
+    T *resp_s = reinterpret_cast<T *>(smem_raw + (PERSIST ? 2 : 1) * slot_bytes +
+                                      (((size_t)2 * C * W * sizeof(T) + 15) & ~(size_t)15));
+    load_resp<T, L>(prog, resp_s);
     if (t == 0) {
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
@@ -623,10 +647,7 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
         auto tile_at = [&](int ti, int j) { return row(ti)[kHalo + j]; };
         T r[L];
         T acc[ACC ? L : 1];
-        // operators unrolled: every StageOp field is a compile-time offset into the parameters
-#pragma unroll
-        for (int k = 0; k < kMaxStageOps; ++k) {
-            if (k >= prog.nops) break;
+        for (int k = 0; k < prog.nops; ++k) {
             const StageOp<T> &so = prog.ops[k];
             const T *ra = row(so.src_a);
             const T *rb = so.src_b >= 0 ? row(so.src_b) : nullptr;
@@ -651,7 +672,7 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
                     }
                 }
             };
-            chunk_solve_resp<T, L>(so, load, r, sc, W, l, c, C, nv, c * W + l);
+            chunk_solve_resp<T, L>(so, resp_s + k * 4 * L, load, r, sc, W, l, c, C, nv, c * W + l);
             if constexpr (ACC) {
                 accumulate<T, L>(so, acc, r, nv, tile_at);
                 if (so.flush && l < rows) flush_x<T, L>(so, acc, (size_t)(l0 + l) * n + cs, nv);
@@ -745,6 +766,7 @@ static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog_in, int 
     const int C = (n + L - 1) / L;
     const int threads = C * W;
     if (threads > 512 || threads % 32) return X3D_EUNSUPPORTED;
+    const size_t resp_bytes = (size_t)prog.nops * 4 * L * es;
     for (int ti = 0; ti < prog.ntiles; ++ti)
         if (!al16(prog.in[ti])) return X3D_EUNSUPPORTED;
     cudaStream_t st = ctx->stream;
@@ -760,7 +782,7 @@ static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog_in, int 
         int pitch = C * L + 2 * kHalo;
         while (((size_t)pitch * es / 16) % 2 == 0) pitch += V;
         const size_t tile = ((size_t)W * pitch * es + 127) & ~(size_t)127;
-        const size_t smem = (PERSIST ? 2 : 1) * prog.ntiles * tile + scratch_bytes(C, W, es);
+        const size_t smem = (PERSIST ? 2 : 1) * prog.ntiles * tile + scratch_bytes(C, W, es) + resp_bytes;
         if (smem + 1024 > ctx->smem_optin) return X3D_EUNSUPPORTED;
         auto kern = acc ? ls_stage_x<T, W, L, true, PERSIST> : ls_stage_x<T, W, L, false, PERSIST>;
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -782,7 +804,7 @@ static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog_in, int 
     // boxes land 128-byte aligned), the boxes, and room for the last window
     const int rows = kHalo + std::max(nb * box_n, C * L + kHalo);
     const size_t tile = ((size_t)rows * W * es + 127) & ~(size_t)127;
-    const size_t smem = (PERSIST ? 2 : 1) * prog.ntiles * tile + scratch_bytes(C, W, es);
+    const size_t smem = (PERSIST ? 2 : 1) * prog.ntiles * tile + scratch_bytes(C, W, es) + resp_bytes;
     if (smem + 1024 > ctx->smem_optin) return X3D_EUNSUPPORTED;
     StageMaps maps;
     for (int ti = 0; ti < prog.ntiles; ++ti) {
