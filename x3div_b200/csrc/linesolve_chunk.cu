@@ -134,11 +134,9 @@ struct ChunkScratch {
 // needs its own multiplier.  The visits run as at most two unwrapped
 // segments of e.
 template <typename T, int STEP>
-__device__ __forceinline__ T chunk_carry(const T *e, const LineOp<T> &op, int ti, int W, int l, int c, int C)
+__device__ __forceinline__ T chunk_carry(const T *e, int K, T mf, T ml, T wrap, int W, int l, int c, int C)
 {
-    const int K = op.depth[ti];
     const bool full = K >= C;
-    const T mf = op.mfull[ti];
     T carry = T(0);
     if (STEP == 1) {
         int s = full ? c : c - K;
@@ -146,7 +144,7 @@ __device__ __forceinline__ T chunk_carry(const T *e, const LineOp<T> &op, int ti
         const int n1 = min(K, C - s);  // chunks s .. s+n1-1, then 0 .. K-n1-1
         const T *p = e + s * W + l;
         for (int k = 1; k < n1; ++k, p += W) carry = fma(mf, carry, *p);
-        carry = fma(s + n1 == C ? op.mlast[ti] : mf, carry, *p);
+        carry = fma(s + n1 == C ? ml : mf, carry, *p);
         p = e + l;
         for (int k = n1; k < K; ++k, p += W) carry = fma(mf, carry, *p);
     } else {
@@ -157,12 +155,12 @@ __device__ __forceinline__ T chunk_carry(const T *e, const LineOp<T> &op, int ti
         for (int k = 0; k < n1; ++k, p -= W) carry = fma(mf, carry, *p);
         if (K > n1) {
             p = e + (C - 1) * W + l;
-            carry = fma(op.mlast[ti], carry, *p);
+            carry = fma(ml, carry, *p);
             p -= W;
             for (int k = n1 + 1; k < K; ++k, p -= W) carry = fma(mf, carry, *p);
         }
     }
-    return full ? carry * op.wrap : carry;
+    return full ? carry * wrap : carry;
 }
 
 // Solves one operator for one chunk; the solved values end in r[] (chunk
@@ -197,7 +195,7 @@ __device__ __forceinline__ void chunk_solve(const LineOp<T> &op, int kind, const
     __syncthreads();
     // forward carry (v just before the chunk), fix, local backward sweep
     {
-        T pw = chunk_carry<T, 1>(sc.fz, op, ti, W, l, c, C);
+        T pw = chunk_carry<T, 1>(sc.fz, op.depth[ti], op.mfull[ti], op.mlast[ti], op.wrap, W, l, c, C);
 #pragma unroll
         for (int j = 0; j < L; ++j) {
             pw *= rho;
@@ -218,7 +216,7 @@ __device__ __forceinline__ void chunk_solve(const LineOp<T> &op, int kind, const
     sc.bz[q] = y;
     __syncthreads();
     // backward carry (y just after the chunk's last point) and fix
-    T pw = chunk_carry<T, -1>(sc.bz, op, ti, W, l, c, C);
+    T pw = chunk_carry<T, -1>(sc.bz, op.depth[ti], op.mfull[ti], op.mlast[ti], op.wrap, W, l, c, C);
     if (nv == L) {
 #pragma unroll
         for (int j = L - 1; j >= 0; --j) {
@@ -279,13 +277,16 @@ __device__ __forceinline__ void chunk_solve_resp(const StageOp<T> &so, const T *
                                                  int C, int nv, int q)
 {
     constexpr int ti = L == kChunkLong<T> ? 0 : 1;
+    // operator fields into registers once (the parameters are read through
+    // a generic pointer, and would be read again after every barrier)
     const LineOp<T> &op = so.op;
+    const T rho = op.rho, mf = op.mfull[ti], ml = op.mlast[ti], wrap = op.wrap;
+    const int K = op.depth[ti];
     {
         T w[L + 8];
         load(w);
         chunk_stencil_kind<T, L>(so.kind, w, r, op);
     }
-    const T rho = op.rho;
     T v = T(0);
 #pragma unroll
     for (int j = 0; j < L; ++j) {
@@ -307,12 +308,12 @@ __device__ __forceinline__ void chunk_solve_resp(const StageOp<T> &so, const T *
     }
     sc.fz[q] = v;
     __syncthreads();
-    const T F = chunk_carry<T, 1>(sc.fz, op, ti, W, l, c, C);
+    const T F = chunk_carry<T, 1>(sc.fz, K, mf, ml, wrap, W, l, c, C);
     const T *h = resp + (nv == L ? 0 : 2 * L);
     const T *g = h + L;
     sc.bz[q] = fma(F, h[0], y);
     __syncthreads();
-    const T B = chunk_carry<T, -1>(sc.bz, op, ti, W, l, c, C);
+    const T B = chunk_carry<T, -1>(sc.bz, K, mf, ml, wrap, W, l, c, C);
     using VT = typename Vec4<T>::type;
     constexpr int V = Vec4<T>::N;
 #pragma unroll
@@ -366,27 +367,45 @@ struct StageMaps {
     CUtensorMap m[kMaxStageTiles];
 };
 
+// Flush fields of a stage operator, read from the parameters once per
+// flush rather than at every store.
+template <typename T>
+struct FlushArgs {
+    void *out;
+    const void *base;
+    void *out2;
+    const void *base2;
+    double sign, scale2;
+    bool f64, plain;
+    __device__ explicit FlushArgs(const StageOp<T> &so)
+        : out(so.out), base(so.base), out2(so.out2), base2(so.base2), sign(so.sign), scale2(so.scale2),
+          f64(so.out_f64 != 0)
+    {
+        plain = !base && !out2 && !f64 && sign == 1.0;
+    }
+};
+
 template <typename T, typename U>
-__device__ __forceinline__ void flush_point(const StageOp<T> &so, size_t p, T a)
+__device__ __forceinline__ void flush_point(const FlushArgs<T> &fa, size_t p, T a)
 {
-    const U *base = static_cast<const U *>(so.base);
-    U v = (U)so.sign * (U)a;
+    const U *base = static_cast<const U *>(fa.base);
+    U v = (U)fa.sign * (U)a;
     if (base) v = base[p] + v;
-    static_cast<U *>(so.out)[p] = v;
-    if (so.out2) {
-        const U *b2 = static_cast<const U *>(so.base2);
-        static_cast<U *>(so.out2)[p] = (b2 ? b2[p] : U(0)) + (U)so.scale2 * v;
+    static_cast<U *>(fa.out)[p] = v;
+    if (fa.out2) {
+        const U *b2 = static_cast<const U *>(fa.base2);
+        static_cast<U *>(fa.out2)[p] = (b2 ? b2[p] : U(0)) + (U)fa.scale2 * v;
     }
 }
 
 // Writes one thread's solved chunk of a y/z line (points j < nv), each point
 // ostride elements after the previous one.
 template <typename T, int L>
-__device__ __forceinline__ void flush_yz(const StageOp<T> &so, const T (&res)[L], size_t obase, size_t ostride,
-                                         int nv)
+__device__ __forceinline__ void flush_yz(const FlushArgs<T> &fa, const T (&res)[L], size_t obase,
+                                         size_t ostride, int nv)
 {
-    if (!so.base && !so.out2 && !so.out_f64 && so.sign == 1.0) {
-        T *dst = static_cast<T *>(so.out) + obase;
+    if (fa.plain) {
+        T *dst = static_cast<T *>(fa.out) + obase;
 #pragma unroll
         for (int j = 0; j < L; ++j) {
             if (j < nv) *dst = res[j];
@@ -397,8 +416,8 @@ __device__ __forceinline__ void flush_yz(const StageOp<T> &so, const T (&res)[L]
 #pragma unroll
         for (int j = 0; j < L; ++j) {
             if (j < nv) {
-                if (so.out_f64) flush_point<T, double>(so, p, res[j]);
-                else flush_point<T, T>(so, p, res[j]);
+                if (fa.f64) flush_point<T, double>(fa, p, res[j]);
+                else flush_point<T, T>(fa, p, res[j]);
             }
             p += ostride;
         }
@@ -495,9 +514,9 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
             chunk_solve_resp<T, L>(so, resp_s + k * 4 * L, load, r, sc, W, l, c, C, nv, c * W + l);
             if constexpr (ACC) {
                 accumulate<T, L>(so, acc, r, nv, tile_at);
-                if (so.flush && live) flush_yz<T, L>(so, acc, obase, ostride, nv);
+                if (so.flush && live) flush_yz<T, L>(FlushArgs<T>(so), acc, obase, ostride, nv);
             } else {
-                if (so.flush && live) flush_yz<T, L>(so, r, obase, ostride, nv);
+                if (so.flush && live) flush_yz<T, L>(FlushArgs<T>(so), r, obase, ostride, nv);
             }
         }
         if (PERSIST) __syncthreads();  // the slot is refilled two tiles later
@@ -510,7 +529,7 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
 // Writes V consecutive results of one thread's chunk starting at element p0
 // as 16-byte vectors of the output type U (T, or double for out_f64).
 template <typename T, typename U, int V, int L>
-__device__ __forceinline__ void flush_vec(const StageOp<T> &so, size_t p0, const T (&res)[L], int j0)
+__device__ __forceinline__ void flush_vec(const FlushArgs<T> &fa, size_t p0, const T (&res)[L], int j0)
 {
     using UV = typename Vec4<U>::type;
     constexpr int VU = Vec4<U>::N;
@@ -519,27 +538,27 @@ __device__ __forceinline__ void flush_vec(const StageOp<T> &so, size_t p0, const
         UV q;
         U *v = reinterpret_cast<U *>(&q);
 #pragma unroll
-        for (int e = 0; e < VU; ++e) v[e] = (U)so.sign * (U)res[j0 + h + e];
-        if (so.base) {
-            const UV bq = *reinterpret_cast<const UV *>(static_cast<const U *>(so.base) + p0 + h);
+        for (int e = 0; e < VU; ++e) v[e] = (U)fa.sign * (U)res[j0 + h + e];
+        if (fa.base) {
+            const UV bq = *reinterpret_cast<const UV *>(static_cast<const U *>(fa.base) + p0 + h);
             const U *be = reinterpret_cast<const U *>(&bq);
 #pragma unroll
             for (int e = 0; e < VU; ++e) v[e] = be[e] + v[e];
         }
-        *reinterpret_cast<UV *>(static_cast<U *>(so.out) + p0 + h) = q;
-        if (so.out2) {
+        *reinterpret_cast<UV *>(static_cast<U *>(fa.out) + p0 + h) = q;
+        if (fa.out2) {
             UV q2;
             U *v2 = reinterpret_cast<U *>(&q2);
-            if (so.base2) {
-                const UV bq = *reinterpret_cast<const UV *>(static_cast<const U *>(so.base2) + p0 + h);
+            if (fa.base2) {
+                const UV bq = *reinterpret_cast<const UV *>(static_cast<const U *>(fa.base2) + p0 + h);
                 const U *be = reinterpret_cast<const U *>(&bq);
 #pragma unroll
-                for (int e = 0; e < VU; ++e) v2[e] = be[e] + (U)so.scale2 * v[e];
+                for (int e = 0; e < VU; ++e) v2[e] = be[e] + (U)fa.scale2 * v[e];
             } else {
 #pragma unroll
-                for (int e = 0; e < VU; ++e) v2[e] = (U)so.scale2 * v[e];
+                for (int e = 0; e < VU; ++e) v2[e] = (U)fa.scale2 * v[e];
             }
-            *reinterpret_cast<UV *>(static_cast<U *>(so.out2) + p0 + h) = q2;
+            *reinterpret_cast<UV *>(static_cast<U *>(fa.out2) + p0 + h) = q2;
         }
     }
 }
@@ -547,14 +566,29 @@ __device__ __forceinline__ void flush_vec(const StageOp<T> &so, size_t p0, const
 // Writes one thread's solved chunk of an x line (points j < nv) as 16-byte
 // vectors starting at element p0.
 template <typename T, int L>
-__device__ __forceinline__ void flush_x(const StageOp<T> &so, const T (&res)[L], size_t p0, int nv)
+__device__ __forceinline__ void flush_x(const FlushArgs<T> &fa, const T (&res)[L], size_t p0, int nv)
 {
+    using VT = typename Vec4<T>::type;
     constexpr int V = Vec4<T>::N;
+    if (fa.plain) {
+        T *dst = static_cast<T *>(fa.out) + p0;
+#pragma unroll
+        for (int j = 0; j < L; j += V) {
+            if (j < nv) {
+                VT q;
+                T *e = reinterpret_cast<T *>(&q);
+#pragma unroll
+                for (int v = 0; v < V; ++v) e[v] = res[j + v];
+                *reinterpret_cast<VT *>(dst + j) = q;
+            }
+        }
+        return;
+    }
 #pragma unroll
     for (int j = 0; j < L; j += V) {
         if (j < nv) {
-            if (so.out_f64) flush_vec<T, double, V, L>(so, p0 + j, res, j);
-            else flush_vec<T, T, V, L>(so, p0 + j, res, j);
+            if (fa.f64) flush_vec<T, double, V, L>(fa, p0 + j, res, j);
+            else flush_vec<T, T, V, L>(fa, p0 + j, res, j);
         }
     }
 }
@@ -675,9 +709,9 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
             chunk_solve_resp<T, L>(so, resp_s + k * 4 * L, load, r, sc, W, l, c, C, nv, c * W + l);
             if constexpr (ACC) {
                 accumulate<T, L>(so, acc, r, nv, tile_at);
-                if (so.flush && l < rows) flush_x<T, L>(so, acc, (size_t)(l0 + l) * n + cs, nv);
+                if (so.flush && l < rows) flush_x<T, L>(FlushArgs<T>(so), acc, (size_t)(l0 + l) * n + cs, nv);
             } else {
-                if (so.flush && l < rows) flush_x<T, L>(so, r, (size_t)(l0 + l) * n + cs, nv);
+                if (so.flush && l < rows) flush_x<T, L>(FlushArgs<T>(so), r, (size_t)(l0 + l) * n + cs, nv);
             }
         }
         if (PERSIST) __syncthreads();  // the slot is refilled two tiles later
