@@ -593,6 +593,46 @@ __device__ __forceinline__ void flush_x(const FlushArgs<T> &fa, const T (&res)[L
     }
 }
 
+// Flush of one operator for a tile of x lines.  Plain outputs go through
+// shared memory: each thread writes its chunk into the tile's staging rows
+// (odd 16-byte granules per row, so the vector stores do not conflict) and
+// one thread per line sends the whole row with a bulk copy, so every line
+// leaves as one contiguous write.  Other flushes store directly.  The
+// caller waits for the copies' reads before the staging rows are reused.
+// fa.plain is the same for the whole CTA, so the barrier is uniform.
+template <typename T, int L>
+__device__ __forceinline__ void flush_x_staged(const FlushArgs<T> &fa, const T (&res)[L], T *out_s, int l,
+                                               long l0, int rows, int pitch, int n, int cs, int nv)
+{
+    using VT = typename Vec4<T>::type;
+    constexpr int V = Vec4<T>::N;
+    if (!fa.plain) {
+        if (l < rows) flush_x<T, L>(fa, res, (size_t)(l0 + l) * n + cs, nv);
+        return;
+    }
+    if (l < rows) {
+        T *dst = out_s + (size_t)l * pitch + cs;
+#pragma unroll
+        for (int j = 0; j < L; j += V) {
+            if (j < nv) {
+                VT q;
+                T *e = reinterpret_cast<T *>(&q);
+#pragma unroll
+                for (int v = 0; v < V; ++v) e[v] = res[j + v];
+                *reinterpret_cast<VT *>(dst + j) = q;
+            }
+        }
+    }
+    fence_proxy_async_smem();
+    __syncthreads();
+    const int t = threadIdx.x;
+    if (t < rows) {
+        bulk_store(static_cast<T *>(fa.out) + (size_t)(l0 + t) * n, out_s + (size_t)t * pitch,
+                   (uint32_t)(n * sizeof(T)));
+        bulk_commit();
+    }
+}
+
 // Fills the halos of ntiles staged x tiles of `rows` padded rows whose
 // point i sits at element kHalo + i: elements 0 .. 3 from points n-4 .. n-1,
 // elements n+4 .. n+7 from points 0 .. 3, moved as 16-byte vectors.
@@ -650,6 +690,9 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
         }
     };
     const ChunkScratch<T> sc = carve_scratch<T>(smem_raw + (PERSIST ? 2 : 1) * slot_bytes, C, W);
+    // staging rows for plain outputs, after the responses (128-byte aligned)
+    T *out_s = reinterpret_cast<T *>(
+        smem_raw + ((reinterpret_cast<unsigned char *>(resp_s + prog.nops * 4 * L) - smem_raw + 127) & ~(size_t)127));
     const int cs = c * L;
     const int nv = min(L, n - cs);
     const long step = PERSIST ? (long)gridDim.x : ntiles;
@@ -665,6 +708,7 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
             if (t == 0) atomicExch(err, 1);
             mbar_wait_bounded(&bars[slot], parity, kChunkWaitNs);
             if (pre) mbar_wait_bounded(&bars[slot ^ 1], ((it + 1) >> 1) & 1, kChunkWaitNs);
+            if (t < W) bulk_wait_all();
             return;
         }
         const long l0 = tile * W;
@@ -706,16 +750,20 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
                     }
                 }
             };
+            // the previous operator's row copies must have read the staging
+            // rows before anyone writes them again (after this solve's barriers)
+            if (t < W) bulk_wait_read_all();
             chunk_solve_resp<T, L>(so, resp_s + k * 4 * L, load, r, sc, W, l, c, C, nv, c * W + l);
             if constexpr (ACC) {
                 accumulate<T, L>(so, acc, r, nv, tile_at);
-                if (so.flush && l < rows) flush_x<T, L>(FlushArgs<T>(so), acc, (size_t)(l0 + l) * n + cs, nv);
+                if (so.flush) flush_x_staged<T, L>(FlushArgs<T>(so), acc, out_s, l, l0, rows, pitch, n, cs, nv);
             } else {
-                if (so.flush && l < rows) flush_x<T, L>(FlushArgs<T>(so), r, (size_t)(l0 + l) * n + cs, nv);
+                if (so.flush) flush_x_staged<T, L>(FlushArgs<T>(so), r, out_s, l, l0, rows, pitch, n, cs, nv);
             }
         }
         if (PERSIST) __syncthreads();  // the slot is refilled two tiles later
     }
+    if (t < W) bulk_wait_all();
 }
 
 // ---------------------------------------------------------------------------
@@ -816,7 +864,10 @@ static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog_in, int 
         int pitch = C * L + 2 * kHalo;
         while (((size_t)pitch * es / 16) % 2 == 0) pitch += V;
         const size_t tile = ((size_t)W * pitch * es + 127) & ~(size_t)127;
-        const size_t smem = (PERSIST ? 2 : 1) * prog.ntiles * tile + scratch_bytes(C, W, es) + resp_bytes;
+        // + staging rows for plain outputs (W rows of the same pitch, 128-byte aligned)
+        const size_t smem = (((PERSIST ? 2 : 1) * prog.ntiles * tile + scratch_bytes(C, W, es) + resp_bytes + 127) &
+                             ~(size_t)127) +
+                            (size_t)W * pitch * es;
         if (smem + 1024 > ctx->smem_optin) return X3D_EUNSUPPORTED;
         auto kern = acc ? ls_stage_x<T, W, L, true, PERSIST> : ls_stage_x<T, W, L, false, PERSIST>;
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

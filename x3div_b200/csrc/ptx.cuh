@@ -104,6 +104,9 @@ __device__ __forceinline__ void bulk_wait_read_all()
     asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }
 
+// Wait until every committed bulk group of this thread has completed.
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
 // Make generic-proxy writes to shared memory visible to the async proxy.
 __device__ __forceinline__ void fence_proxy_async_smem()
 {
