@@ -40,6 +40,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 
 #include "linesolve_chunk.h"
 #include "ptx.cuh"
@@ -71,26 +72,44 @@ __device__ __forceinline__ T stencil_at(const T *v, const Coef<T> &k)
     return v[4];
 }
 
-template <int KIND, typename T, int L>
-__device__ __forceinline__ void chunk_stencil(const T (&w)[L + 8], T (&r)[L], const Coef<T> &k)
+// r[OFF + j] for j < N from a window w of N + 8 values (w[m] = u_{OFF+j-4+m}).
+template <int KIND, typename T, int N, int L, int OFF>
+__device__ __forceinline__ void chunk_stencil(const T (&w)[N + 8], T (&r)[L], const Coef<T> &k)
 {
 #pragma unroll
-    for (int j = 0; j < L; ++j) r[j] = stencil_at<KIND>(w + j, k);
+    for (int j = 0; j < N; ++j) r[OFF + j] = stencil_at<KIND>(w + j, k);
 }
 
-template <typename T, int L>
-__device__ __forceinline__ void chunk_stencil_kind(int kind, const T (&w)[L + 8], T (&r)[L],
+template <typename T, int N, int L, int OFF>
+__device__ __forceinline__ void chunk_stencil_kind(int kind, const T (&w)[N + 8], T (&r)[L],
                                                    const LineOp<T> &op)
 {
     const Coef<T> k{op.ca, op.cb, op.cc, op.cd};
     switch (kind) {
-    case DER: chunk_stencil<DER, T, L>(w, r, k); break;
-    case DER2: chunk_stencil<DER2, T, L>(w, r, k); break;
-    case DERVP: chunk_stencil<DERVP, T, L>(w, r, k); break;
-    case DERPV: chunk_stencil<DERPV, T, L>(w, r, k); break;
-    case INTVP: chunk_stencil<INTVP, T, L>(w, r, k); break;
-    case INTPV: chunk_stencil<INTPV, T, L>(w, r, k); break;
-    default: chunk_stencil<IDENT, T, L>(w, r, k); break;
+    case DER: chunk_stencil<DER, T, N, L, OFF>(w, r, k); break;
+    case DER2: chunk_stencil<DER2, T, N, L, OFF>(w, r, k); break;
+    case DERVP: chunk_stencil<DERVP, T, N, L, OFF>(w, r, k); break;
+    case DERPV: chunk_stencil<DERPV, T, N, L, OFF>(w, r, k); break;
+    case INTVP: chunk_stencil<INTVP, T, N, L, OFF>(w, r, k); break;
+    case INTPV: chunk_stencil<INTPV, T, N, L, OFF>(w, r, k); break;
+    default: chunk_stencil<IDENT, T, N, L, OFF>(w, r, k); break;
+    }
+}
+
+// The explicit right-hand side of a whole chunk, in P parts of L/P points,
+// each from its own window of L/P + 8 staged values, so that only one part's
+// window is live next to r.  load(w, J0) fills w[m] = u_{cs+J0-4+m}.
+template <typename T, int L, int P, int I = 0, typename Load>
+__device__ __forceinline__ void chunk_rhs(int kind, const Load &load, T (&r)[L], const LineOp<T> &op)
+{
+    if constexpr (I < P) {
+        constexpr int N = L / P;
+        {
+            T w[N + 8];
+            load(w, std::integral_constant<int, I * N>{});
+            chunk_stencil_kind<T, N, L, I * N>(kind, w, r, op);
+        }
+        chunk_rhs<T, L, P, I + 1>(kind, load, r, op);
     }
 }
 
@@ -164,7 +183,7 @@ __device__ __forceinline__ T chunk_carry(const T *e, int K, T mf, T ml, T wrap, 
 }
 
 // Solves one operator for one chunk; the solved values end in r[] (chunk
-// local).  load(w) fills the L+8 input window u[cs-4 .. cs+L+3] from the
+// local).  load(w, J0) fills a window u[cs+J0-4 ...] of the size of w from the
 // staged line and its periodic halos; the window is dead once the stencil is
 // evaluated.  nv = points of the chunk inside the line (L except for the last
 // chunk of a ragged line; the window values past its end are never used).
@@ -174,11 +193,7 @@ __device__ __forceinline__ void chunk_solve(const LineOp<T> &op, int kind, const
                                             int q)
 {
     constexpr int ti = L == kChunkLong<T> ? 0 : 1;
-    {
-        T w[L + 8];
-        load(w);
-        chunk_stencil_kind<T, L>(kind, w, r, op);
-    }
+    chunk_rhs<T, L, 1>(kind, load, r, op);
     const T rho = op.rho;
     T v = T(0);
 #pragma unroll
@@ -282,11 +297,7 @@ __device__ __forceinline__ void chunk_solve_resp(const StageOp<T> &so, const T *
     const LineOp<T> &op = so.op;
     const T rho = op.rho, mf = op.mfull[ti], ml = op.mlast[ti], wrap = op.wrap;
     const int K = op.depth[ti];
-    {
-        T w[L + 8];
-        load(w);
-        chunk_stencil_kind<T, L>(so.kind, w, r, op);
-    }
+    chunk_rhs<T, L, 2>(so.kind, load, r, op);
     T v = T(0);
 #pragma unroll
     for (int j = 0; j < L; ++j) {
@@ -502,13 +513,15 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
             const StageOp<T> &so = prog.ops[k];
             const T *ca = col(so.src_a);
             const T *cb = so.src_b >= 0 ? col(so.src_b) : nullptr;
-            auto load = [&](T(&w)[L + 8]) {
+            auto load = [&](auto &w, auto j0) {
+                constexpr int J0 = decltype(j0)::value;
+                constexpr int NW = sizeof(w) / sizeof(T);
                 if (cb) {
 #pragma unroll
-                    for (int j = 0; j < L + 8; ++j) w[j] = ca[j * W] * cb[j * W];
+                    for (int j = 0; j < NW; ++j) w[j] = ca[(J0 + j) * W] * cb[(J0 + j) * W];
                 } else {
 #pragma unroll
-                    for (int j = 0; j < L + 8; ++j) w[j] = ca[j * W];
+                    for (int j = 0; j < NW; ++j) w[j] = ca[(J0 + j) * W];
                 }
             };
             chunk_solve_resp<T, L>(so, resp_s + k * 4 * L, load, r, sc, W, l, c, C, nv, c * W + l);
@@ -729,12 +742,14 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
             const StageOp<T> &so = prog.ops[k];
             const T *ra = row(so.src_a);
             const T *rb = so.src_b >= 0 ? row(so.src_b) : nullptr;
-            auto load = [&](T(&w)[L + 8]) {
+            auto load = [&](auto &w, auto j0) {
+                constexpr int J0 = decltype(j0)::value;
+                constexpr int NW = sizeof(w) / sizeof(T);
                 if (rb) {
 #pragma unroll
-                    for (int j = 0; j < L + 8; j += V) {
-                        const VT qa = *reinterpret_cast<const VT *>(ra + j);
-                        const VT qb = *reinterpret_cast<const VT *>(rb + j);
+                    for (int j = 0; j < NW; j += V) {
+                        const VT qa = *reinterpret_cast<const VT *>(ra + J0 + j);
+                        const VT qb = *reinterpret_cast<const VT *>(rb + J0 + j);
                         const T *ea = reinterpret_cast<const T *>(&qa);
                         const T *eb = reinterpret_cast<const T *>(&qb);
 #pragma unroll
@@ -742,8 +757,8 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
                     }
                 } else {
 #pragma unroll
-                    for (int j = 0; j < L + 8; j += V) {
-                        const VT qa = *reinterpret_cast<const VT *>(ra + j);
+                    for (int j = 0; j < NW; j += V) {
+                        const VT qa = *reinterpret_cast<const VT *>(ra + J0 + j);
                         const T *ea = reinterpret_cast<const T *>(&qa);
 #pragma unroll
                         for (int v = 0; v < V; ++v) w[j + v] = ea[v];
@@ -1057,10 +1072,12 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
         if (dir == DX) {
             const int lr = l < rows ? l : 0;
             const T *row = tile + (size_t)lr * J.pitch + cs;  // points cs-4 .. cs+L+3
-            auto load = [&](T(&w)[L + 8]) {
+            auto load = [&](auto &w, auto j0) {
+                constexpr int J0 = decltype(j0)::value;
+                constexpr int NW = sizeof(w) / sizeof(T);
 #pragma unroll
-                for (int j = 0; j < L + 8; j += V) {
-                    const VT qa = *reinterpret_cast<const VT *>(row + j);
+                for (int j = 0; j < NW; j += V) {
+                    const VT qa = *reinterpret_cast<const VT *>(row + J0 + j);
                     const T *ea = reinterpret_cast<const T *>(&qa);
 #pragma unroll
                     for (int v = 0; v < V; ++v) w[j + v] = ea[v];
@@ -1084,9 +1101,11 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
             }
         } else {
             const T *col = tile + (size_t)(J.halo + cs - 4) * W + l;  // points cs-4 .. cs+L+3
-            auto load = [&](T(&w)[L + 8]) {
+            auto load = [&](auto &w, auto j0) {
+                constexpr int J0 = decltype(j0)::value;
+                constexpr int NW = sizeof(w) / sizeof(T);
 #pragma unroll
-                for (int j = 0; j < L + 8; ++j) w[j] = col[j * W];
+                for (int j = 0; j < NW; ++j) w[j] = col[(J0 + j) * W];
             };
             const bool live = active && x0 + l < J.nx;
             const size_t ostride = dir == DY ? (size_t)J.nx : (size_t)J.nx * J.ny;
