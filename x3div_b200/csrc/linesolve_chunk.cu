@@ -196,17 +196,21 @@ __device__ __forceinline__ void chunk_solve(const LineOp<T> &op, int kind, const
     chunk_rhs<T, L, 1>(kind, load, r, op);
     const T rho = op.rho;
     T v = T(0);
+    if (nv == L) {
 #pragma unroll
-    for (int j = 0; j < L; ++j) {
-        v = fma(rho, v, r[j]);
-        r[j] = v;
-    }
-    if (nv < L) {  // ragged last chunk: its end is point nv - 1
+        for (int j = 0; j < L; ++j) {
+            v = fma(rho, v, r[j]);
+            r[j] = v;
+        }
+        sc.fz[q] = v;
+    } else {  // ragged last chunk: its end is point nv - 1 (captured in the sweep)
 #pragma unroll
-        for (int j = 0; j < L; ++j)
-            if (j == nv - 1) v = r[j];
+        for (int j = 0; j < L; ++j) {
+            v = fma(rho, v, r[j]);
+            if (j + 1 == nv) sc.fz[q] = v;
+            r[j] = v;
+        }
     }
-    sc.fz[q] = v;
     __syncthreads();
     // forward carry (v just before the chunk), fix, local backward sweep
     {
@@ -298,17 +302,24 @@ __device__ __forceinline__ void chunk_solve_resp(const StageOp<T> &so, const T *
     const T rho = op.rho, mf = op.mfull[ti], ml = op.mlast[ti], wrap = op.wrap;
     const int K = op.depth[ti];
     chunk_rhs<T, L, 2>(so.kind, load, r, op);
+    // local forward sweep; the chunk's end value goes straight to shared
+    // memory (for a short last chunk, the value at point nv - 1, captured in
+    // the sweep: selecting it from r afterwards would index r at run time
+    // and move the whole array to local memory)
     T v = T(0);
-#pragma unroll
-    for (int j = 0; j < L; ++j) {
-        v = fma(rho, v, r[j]);
-        r[j] = v;
-    }
-    if (nv < L) {  // short last chunk: its end is point nv - 1, nothing past it
+    if (nv == L) {
 #pragma unroll
         for (int j = 0; j < L; ++j) {
-            if (j == nv - 1) v = r[j];
-            if (j >= nv) r[j] = T(0);
+            v = fma(rho, v, r[j]);
+            r[j] = v;
+        }
+        sc.fz[q] = v;
+    } else {
+#pragma unroll
+        for (int j = 0; j < L; ++j) {
+            v = fma(rho, v, r[j]);
+            if (j + 1 == nv) sc.fz[q] = v;
+            r[j] = j < nv ? v : T(0);
         }
     }
     T y = T(0);
@@ -317,7 +328,6 @@ __device__ __forceinline__ void chunk_solve_resp(const StageOp<T> &so, const T *
         y = fma(rho, y, r[j]);
         r[j] = y;
     }
-    sc.fz[q] = v;
     __syncthreads();
     const T F = chunk_carry<T, 1>(sc.fz, K, mf, ml, wrap, W, l, c, C);
     const T *h = resp + (nv == L ? 0 : 2 * L);
