@@ -58,8 +58,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--profile-timed", action="store_true",
-                    help="bracket the timed FP32 sweep with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
+    ap.add_argument("--profile-timed", nargs="?", const="sweep", default=None, choices=["sweep", "euler"],
+                    help="bracket the timed FP32 sweep (or the FP32-mixed Euler steps) with "
+                         "cudaProfilerStart/Stop, for ncu --profile-from-start off")
     ap.add_argument("--kernel-config", type=int, default=None,
                     help="force one kernel configuration (x3d_ctx_set_kernel) instead of autotuning")
     ap.add_argument("--no-b48", action="store_true")
@@ -386,7 +387,7 @@ def run_b200(args, world, rank, local):
     clocks.start()
     ms, fam, nitems, launches, group = timed_sweep(ctx, torch, fields, outs, args.steps,
                                                    args.warmup, world, fused=True,
-                                                   profile=args.profile_timed)
+                                                   profile=args.profile_timed == "sweep")
     ms = max_over_ranks(ms, world)
     pts_step = nitems * npts
     value = world * pts_step * args.steps / (ms * 1e-3) / 1e9
@@ -450,7 +451,7 @@ def run_b200(args, world, rank, local):
     del fields, outs
 
     # ---- Euler step, FP32-mixed ---------------------------------------------
-    def euler_ms(c, dt_torch):
+    def euler_ms(c, dt_torch, profile=False):
         U = [torch.from_numpy(h).to(device="cuda", dtype=dt_torch) for h in host]
         du = [torch.empty_like(U[0]) for _ in range(3)]
         pg = [torch.empty_like(U[0]) for _ in range(3)]
@@ -461,18 +462,22 @@ def run_b200(args, world, rank, local):
         barrier(world)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         reps = 3
+        if profile:
+            torch.cuda.profiler.start()
         a.record()
         for _ in range(reps):
             c.euler_step(*U, *du, pp3, *pg, 5e-4)
         b.record()
         torch.cuda.synchronize()
+        if profile:
+            torch.cuda.profiler.stop()
         c.sync()
         c.divergence(pp3, *U)
         mx, mean = c.div_stats(pp3)
         return max_over_ranks(a.elapsed_time(b) / reps, world), mx
 
     if not args.no_euler:
-        out["euler_f32"] = euler_ms(ctx, torch.float32)
+        out["euler_f32"] = euler_ms(ctx, torch.float32, profile=args.profile_timed == "euler")
     ctx.close()
     torch.cuda.empty_cache()
 

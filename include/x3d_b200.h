@@ -193,9 +193,11 @@ int x3d_apply_batch(x3d_ctx ctx, const x3d_work *items, int count);
 /* Times every kernel configuration (lines per CTA, chunk length, or one
  * thread per line) for each direction and for groups of 1, 2, 3 and 6
  * operators sharing an input (up to max_group), on the context grid, and
- * keeps the fastest for later calls.  Synchronous; uses context scratch
- * fields; not callable during stream capture.  Without it a fixed default
- * configuration is used.  No reference counterpart. */
+ * keeps the fastest for later calls; then does the same for each fused
+ * stage of the Euler step (transeq + int_time, divergence, gradp + cor_vel,
+ * per direction).  Synchronous; uses context scratch fields (up to 14 of
+ * nx*ny*nz doubles); not callable during stream capture.  Without it a
+ * fixed default configuration is used.  No reference counterpart. */
 int x3d_autotune(x3d_ctx ctx, int max_group);
 /* Force kernel configuration cfg (0..5 chunked, one CTA per tile;
  * 6..11 the same shapes as persistent double-buffered kernels; 12 one thread per line) for

@@ -547,13 +547,37 @@ int x3d_autotune(x3d_ctx ctx, int max_group)
             }
             rc = autotune_group(ctx, dir, buf[0], ops, kinds, outs, g, fp32(ctx), 3, nullptr);
         }
-    return rc;
+    if (rc) return rc;
+    // the fused stages of the Euler step (transeq + int_time, divergence,
+    // gradp + cor_vel), run once on scratch fields 7..13 with every
+    // configuration timed; fields 0..5 are the stages' own intermediates
+    void *u[3], *du[3];
+    for (int i = 0; i < 3 && !rc; ++i) {
+        u[i] = ctx_scratch(ctx, 7 + i);
+        du[i] = ctx_scratch(ctx, 10 + i);
+        if (!u[i] || !du[i]) return set_error(ctx, X3D_ENOMEM, "scratch allocation failed");
+        rc = cuda_check(ctx, cudaMemsetAsync(u[i], 0, ctx->npts() * ctx->elem(), ctx->stream), "memset");
+        if (!rc) rc = cuda_check(ctx, cudaMemsetAsync(du[i], 0, ctx->npts() * ctx->elem(), ctx->stream), "memset");
+    }
+    double *pp3 = static_cast<double *>(ctx_scratch(ctx, 13));
+    if (!pp3) return set_error(ctx, X3D_ENOMEM, "scratch allocation failed");
+    if (rc) return rc;
+    ctx->stage_tuning = true;
+    const void *uc[3] = {u[0], u[1], u[2]};
+    rc = fused_transeq(ctx, du, uc, true, 0.0, u);
+    if (!rc || rc == X3D_EUNSUPPORTED) rc = fused_divergence(ctx, pp3, uc);
+    if (!rc || rc == X3D_EUNSUPPORTED) rc = fused_gradp(ctx, du, pp3, nullptr);
+    if (!rc || rc == X3D_EUNSUPPORTED) rc = fused_gradp(ctx, du, pp3, u);
+    ctx->stage_tuning = false;
+    // a grid no fused stage can take keeps the unfused path
+    return rc == X3D_EUNSUPPORTED ? X3D_OK : rc;
 }
 
 int x3d_ctx_set_kernel(x3d_ctx ctx, int cfg)
 {
     if (!ctx || cfg < -1 || cfg > kChunkConfigs) return X3D_EINVAL;
     ctx->tuned.clear();
+    ctx->stage_tuned.clear();
     ctx->default_cfg = cfg < 0 ? 0 : cfg;
     return X3D_OK;
 }

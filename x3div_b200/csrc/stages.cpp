@@ -56,11 +56,50 @@ static void set_flush(StageOp<T> &s, void *out, const void *base = nullptr, bool
     s.out_f64 = f64 ? 1 : 0;
 }
 
-// Runs a stage with the tuned (or default) configuration, then the others.
+// Times every configuration of a stage (one probe launch, then two timed
+// ones) and keeps the fastest for the stage's name.  Only the autotuner
+// runs stages this way, on scratch fields.
 template <typename T>
-static int run_stage(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir)
+static int tune_stage(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir, const char *name)
 {
-    const int first = ctx->default_cfg < kChunkConfigs ? ctx->default_cfg : 0;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    int best = -1, rc = X3D_OK;
+    float bt = 0.f;
+    for (int cfg = 0; cfg < kChunkConfigs; ++cfg) {
+        rc = launch_stage<T>(ctx, prog, dir, ctx->nx, ctx->ny, ctx->nz, cfg);
+        if (rc == X3D_EUNSUPPORTED) continue;
+        if (rc) break;
+        cudaEventRecord(a, ctx->stream);
+        for (int r = 0; r < 2 && !rc; ++r) rc = launch_stage<T>(ctx, prog, dir, ctx->nx, ctx->ny, ctx->nz, cfg);
+        cudaEventRecord(b, ctx->stream);
+        cudaEventSynchronize(b);
+        if (rc) break;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        if (best < 0 || ms < bt) {
+            best = cfg;
+            bt = ms;
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (rc && rc != X3D_EUNSUPPORTED) return rc;
+    if (best < 0) return X3D_EUNSUPPORTED;
+    ctx->stage_tuned[name] = best;
+    return X3D_OK;
+}
+
+// Runs a stage with its tuned (or the default) configuration, then, if that
+// one cannot take the grid, the others in order.
+template <typename T>
+static int run_stage(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir, const char *name)
+{
+    if (ctx->stage_tuning) return tune_stage<T>(ctx, prog, dir, name);
+    const auto it = ctx->stage_tuned.find(name);
+    const int first = it != ctx->stage_tuned.end() ? it->second
+                                                   : (ctx->default_cfg < kChunkConfigs ? ctx->default_cfg : 0);
     int rc = launch_stage<T>(ctx, prog, dir, ctx->nx, ctx->ny, ctx->nz, first);
     for (int cfg = 0; rc == X3D_EUNSUPPORTED && cfg < kChunkConfigs; ++cfg)
         if (cfg != first) rc = launch_stage<T>(ctx, prog, dir, ctx->nx, ctx->ny, ctx->nz, cfg);
@@ -97,7 +136,8 @@ static int transeq_t(x3d_ctx_s *ctx, void *const du[3], const void *const u[3], 
             p.ops[2 * c] = a;
             p.ops[2 * c + 1] = b;
         }
-        const int rc = run_stage<T>(ctx, p, d);
+        static const char *const names[3] = {"transeq_x", "transeq_y", "transeq_z"};
+        const int rc = run_stage<T>(ctx, p, d, names[d]);
         if (rc) return rc;
     }
     return X3D_OK;
@@ -118,7 +158,7 @@ static int divergence_t(x3d_ctx_s *ctx, double *pp3, const void *const u[3], voi
     set_flush(p.ops[1], s[1]);
     p.ops[2] = sop<T>(B(ctx, X3D_OP_INTXVP), 2);
     set_flush(p.ops[2], s[2]);
-    int rc = run_stage<T>(ctx, p, DX);
+    int rc = run_stage<T>(ctx, p, DX, "div_x");
     if (rc) return rc;
     // y pencil: duydypi2 = deryvp(pgy1) + interyvp(pp1) ; upi2 = interyvp(pgz1)
     std::memset(&p, 0, sizeof(p));
@@ -131,7 +171,7 @@ static int divergence_t(x3d_ctx_s *ctx, double *pp3, const void *const u[3], voi
     set_flush(p.ops[1], s[3]);
     p.ops[2] = sop<T>(B(ctx, X3D_OP_INTYVP), 2);
     set_flush(p.ops[2], s[4]);
-    rc = run_stage<T>(ctx, p, DY);
+    rc = run_stage<T>(ctx, p, DY, "div_y");
     if (rc) return rc;
     // z pencil: pp3 = interzvp(duxydxyp3) + derzvp(uzp3), written in FP64
     std::memset(&p, 0, sizeof(p));
@@ -143,7 +183,7 @@ static int divergence_t(x3d_ctx_s *ctx, double *pp3, const void *const u[3], voi
     p.ops[1] = sop<T>(B(ctx, X3D_OP_DERZVP), 1);
     p.ops[1].accumulate = 1;
     set_flush(p.ops[1], pp3, nullptr, true);
-    return run_stage<T>(ctx, p, DZ);
+    return run_stage<T>(ctx, p, DZ, "div_z");
 }
 
 template <typename T>
@@ -166,7 +206,7 @@ static int gradp_t(x3d_ctx_s *ctx, void *const px[3], const double *pp3, void *c
     set_flush(p.ops[0], s[0]);
     p.ops[1] = sop<T>(B(ctx, X3D_OP_DERZPV), 0);
     set_flush(p.ops[1], s[1]);
-    int rc = run_stage<T>(ctx, p, DZ);
+    int rc = run_stage<T>(ctx, p, DZ, "gradp_z");
     if (rc) return rc;
     // y pencil: ppi2 = interypv(pp2), pgy2 = derypv(pp2), pgzi2 = interypv(pgz2)
     std::memset(&p, 0, sizeof(p));
@@ -180,7 +220,7 @@ static int gradp_t(x3d_ctx_s *ctx, void *const px[3], const double *pp3, void *c
     set_flush(p.ops[1], s[3]);
     p.ops[2] = sop<T>(B(ctx, X3D_OP_INTYPV), 1);
     set_flush(p.ops[2], s[4]);
-    rc = run_stage<T>(ctx, p, DY);
+    rc = run_stage<T>(ctx, p, DY, "gradp_y");
     if (rc) return rc;
     // x pencil: px1 = derxpv(pp1), py1 = interxpv(pgy1), pz1 = interxpv(pgz1);
     // cor_vel: u_c = u_c - p_c
@@ -198,7 +238,7 @@ static int gradp_t(x3d_ctx_s *ctx, void *const px[3], const double *pp3, void *c
             p.ops[c].scale2 = -1.0;
         }
     }
-    return run_stage<T>(ctx, p, DX);
+    return run_stage<T>(ctx, p, DX, ucor ? "gradp_x_cor" : "gradp_x");
 }
 
 int fused_transeq(x3d_ctx_s *ctx, void *const du[3], const void *const u[3], bool step, double dt,

@@ -105,6 +105,11 @@ struct x3d_ctx_s {
     // kernel choice per (direction, grid, precision, operator-group size):
     // filled by the autotuner, default_cfg otherwise
     std::map<std::string, int> tuned;
+    // kernel choice per fused stage of the Euler step (transeq_x, div_y, ...),
+    // filled by the autotuner; while stage_tuning is set, each stage run
+    // times every configuration instead
+    std::map<std::string, int> stage_tuned;
+    bool stage_tuning = false;
     int default_cfg = 0;
     unsigned long long launches = 0;  // kernels of this library launched on the context
     size_t elem() const { return precision == X3D_F32 ? 4 : 8; }
