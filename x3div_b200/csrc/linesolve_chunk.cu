@@ -406,16 +406,40 @@ struct FlushArgs {
     }
 };
 
-template <typename T, typename U>
-__device__ __forceinline__ void flush_point(const FlushArgs<T> &fa, size_t p, T a)
+// General flush of a y/z chunk in blocks of up to 8 points: every load of a
+// block (base, base2) is issued before its stores.  base and base2 are often
+// the output arrays themselves (du += ..., u = u + dt du in place), so a load
+// placed after a store could not be moved ahead of it, and each point would
+// wait for memory in turn.
+template <typename T, typename U, int L>
+__device__ __forceinline__ void flush_yz_blocked(const FlushArgs<T> &fa, const T (&res)[L], size_t obase,
+                                                 size_t ostride, int nv)
 {
+    constexpr int B = L < 8 ? L : 8;
     const U *base = static_cast<const U *>(fa.base);
-    U v = (U)fa.sign * (U)a;
-    if (base) v = base[p] + v;
-    static_cast<U *>(fa.out)[p] = v;
-    if (fa.out2) {
-        const U *b2 = static_cast<const U *>(fa.base2);
-        static_cast<U *>(fa.out2)[p] = (b2 ? b2[p] : U(0)) + (U)fa.scale2 * v;
+    const U *base2 = static_cast<const U *>(fa.base2);
+    U *out = static_cast<U *>(fa.out);
+    U *out2 = static_cast<U *>(fa.out2);
+    const U sign = (U)fa.sign, scale2 = (U)fa.scale2;
+#pragma unroll
+    for (int j0 = 0; j0 < L; j0 += B) {
+        U bv[B], b2v[B];
+#pragma unroll
+        for (int i = 0; i < B; ++i) {
+            const size_t p = obase + (size_t)(j0 + i) * ostride;
+            const bool in = j0 + i < nv;
+            bv[i] = base && in ? base[p] : U(0);
+            b2v[i] = base2 && in ? base2[p] : U(0);
+        }
+#pragma unroll
+        for (int i = 0; i < B; ++i) {
+            if (j0 + i < nv) {
+                const size_t p = obase + (size_t)(j0 + i) * ostride;
+                const U v = bv[i] + sign * (U)res[j0 + i];
+                out[p] = v;
+                if (out2) out2[p] = b2v[i] + scale2 * v;
+            }
+        }
     }
 }
 
@@ -432,16 +456,10 @@ __device__ __forceinline__ void flush_yz(const FlushArgs<T> &fa, const T (&res)[
             if (j < nv) *dst = res[j];
             dst += ostride;
         }
+    } else if (fa.f64) {
+        flush_yz_blocked<T, double, L>(fa, res, obase, ostride, nv);
     } else {
-        size_t p = obase;
-#pragma unroll
-        for (int j = 0; j < L; ++j) {
-            if (j < nv) {
-                if (fa.f64) flush_point<T, double>(fa, p, res[j]);
-                else flush_point<T, T>(fa, p, res[j]);
-            }
-            p += ostride;
-        }
+        flush_yz_blocked<T, T, L>(fa, res, obase, ostride, nv);
     }
 }
 
@@ -549,39 +567,48 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
 // ---------------------------------------------------------------------------
 // x-lines.
 
-// Writes V consecutive results of one thread's chunk starting at element p0
-// as 16-byte vectors of the output type U (T, or double for out_f64).
-template <typename T, typename U, int V, int L>
-__device__ __forceinline__ void flush_vec(const FlushArgs<T> &fa, size_t p0, const T (&res)[L], int j0)
+// General flush of an x chunk (contiguous from element p0) as 16-byte
+// vectors of the output type U, in blocks of up to 8 points whose loads
+// (base, base2, often the output arrays themselves) all precede their stores.
+template <typename T, typename U, int L>
+__device__ __forceinline__ void flush_x_blocked(const FlushArgs<T> &fa, const T (&res)[L], size_t p0, int nv)
 {
     using UV = typename Vec4<U>::type;
     constexpr int VU = Vec4<U>::N;
+    constexpr int B = L < 8 ? L : 8;
+    constexpr int NQ = B / VU;
+    const U *base = static_cast<const U *>(fa.base);
+    const U *base2 = static_cast<const U *>(fa.base2);
+    U *out = static_cast<U *>(fa.out);
+    U *out2 = static_cast<U *>(fa.out2);
+    const U sign = (U)fa.sign, scale2 = (U)fa.scale2;
 #pragma unroll
-    for (int h = 0; h < V; h += VU) {
-        UV q;
-        U *v = reinterpret_cast<U *>(&q);
+    for (int j0 = 0; j0 < L; j0 += B) {
+        UV bq[NQ], b2q[NQ];
 #pragma unroll
-        for (int e = 0; e < VU; ++e) v[e] = (U)fa.sign * (U)res[j0 + h + e];
-        if (fa.base) {
-            const UV bq = *reinterpret_cast<const UV *>(static_cast<const U *>(fa.base) + p0 + h);
-            const U *be = reinterpret_cast<const U *>(&bq);
-#pragma unroll
-            for (int e = 0; e < VU; ++e) v[e] = be[e] + v[e];
+        for (int q = 0; q < NQ; ++q) {
+            const int j = j0 + q * VU;
+            const bool in = j < nv;
+            bq[q] = base && in ? *reinterpret_cast<const UV *>(base + p0 + j) : UV{};
+            b2q[q] = base2 && in ? *reinterpret_cast<const UV *>(base2 + p0 + j) : UV{};
         }
-        *reinterpret_cast<UV *>(static_cast<U *>(fa.out) + p0 + h) = q;
-        if (fa.out2) {
-            UV q2;
-            U *v2 = reinterpret_cast<U *>(&q2);
-            if (fa.base2) {
-                const UV bq = *reinterpret_cast<const UV *>(static_cast<const U *>(fa.base2) + p0 + h);
-                const U *be = reinterpret_cast<const U *>(&bq);
 #pragma unroll
-                for (int e = 0; e < VU; ++e) v2[e] = be[e] + (U)fa.scale2 * v[e];
-            } else {
+        for (int q = 0; q < NQ; ++q) {
+            const int j = j0 + q * VU;
+            if (j < nv) {
+                UV o, o2;
+                U *ov = reinterpret_cast<U *>(&o);
+                U *o2v = reinterpret_cast<U *>(&o2);
+                const U *bv = reinterpret_cast<const U *>(&bq[q]);
+                const U *b2v = reinterpret_cast<const U *>(&b2q[q]);
 #pragma unroll
-                for (int e = 0; e < VU; ++e) v2[e] = (U)fa.scale2 * v[e];
+                for (int e = 0; e < VU; ++e) {
+                    ov[e] = bv[e] + sign * (U)res[j + e];
+                    o2v[e] = b2v[e] + scale2 * ov[e];
+                }
+                *reinterpret_cast<UV *>(out + p0 + j) = o;
+                if (out2) *reinterpret_cast<UV *>(out2 + p0 + j) = o2;
             }
-            *reinterpret_cast<UV *>(static_cast<U *>(fa.out2) + p0 + h) = q2;
         }
     }
 }
@@ -607,13 +634,8 @@ __device__ __forceinline__ void flush_x(const FlushArgs<T> &fa, const T (&res)[L
         }
         return;
     }
-#pragma unroll
-    for (int j = 0; j < L; j += V) {
-        if (j < nv) {
-            if (fa.f64) flush_vec<T, double, V, L>(fa, p0 + j, res, j);
-            else flush_vec<T, T, V, L>(fa, p0 + j, res, j);
-        }
-    }
+    if (fa.f64) flush_x_blocked<T, double, L>(fa, res, p0, nv);
+    else flush_x_blocked<T, T, L>(fa, res, p0, nv);
 }
 
 // Flush of one operator for a tile of x lines.  Plain outputs go through
