@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--kernel-config", type=int, default=None,
                     help="force one kernel configuration (x3d_ctx_set_kernel) instead of autotuning")
     ap.add_argument("--no-b48", action="store_true")
+    ap.add_argument("--c5", action="store_true",
+                    help="also run 20 Euler steps at 768^3, FP32-mixed and FP64 (reported under c5)")
     return ap.parse_args()
 
 
@@ -304,6 +306,55 @@ def timed_sweep(ctx, torch, fields, outs, steps, warmup, world, fused=True, per_
     return ms, fam, sum(len(g) for _, g in groups), launches, group
 
 
+def run_c5(torch, n=768, steps=20, dt=5e-4, seed=5):
+    """Long-run check at 768^3: 20 Euler steps (dt = 5e-4) from the same
+    Taylor-Green + N(0, (1e-3)^2) field with FP32 derivatives (FP64 Poisson)
+    and with the FP64 path.  Reports ms per step, the divergence left after
+    the last step (max |div u|) and the kinetic-energy drift of each, and the
+    FP32-mixed / FP64 divergence ratio (the bar is <= 10)."""
+    from x3div_b200 import Context
+    out = {"grid": [n, n, n], "steps": steps, "dt": dt}
+    x = torch.arange(n, device="cuda", dtype=torch.float64) * (2 * np.pi / n)
+    g = torch.Generator(device="cuda")
+    res = {}
+    for prec, dtype in (("f32_mixed", torch.float32), ("f64", torch.float64)):
+        c = Context(n, n, n, lengths=(2 * np.pi,) * 3, precision="f32" if dtype == torch.float32 else "f64",
+                    stream=torch.cuda.current_stream())
+        c.autotune(1)
+        tg = [torch.cos(x)[:, None, None] * torch.cos(x)[None, :, None] * torch.sin(x)[None, None, :],
+              -torch.cos(x)[:, None, None] * torch.sin(x)[None, :, None] * torch.cos(x)[None, None, :],
+              torch.zeros(n, n, n, device="cuda", dtype=torch.float64)]
+        U = []
+        for f in range(3):
+            g.manual_seed(seed * 10 + f)
+            U.append((tg[f] + 1e-3 * torch.randn(n, n, n, device="cuda", dtype=torch.float64,
+                                                  generator=g)).to(dtype).contiguous())
+        del tg
+        du = [torch.empty_like(U[0]) for _ in range(3)]
+        pg = [torch.empty_like(U[0]) for _ in range(3)]
+        pp3 = torch.empty((n, n, n), dtype=torch.float64, device="cuda")
+        ke = lambda: 0.5 * sum(float((u.double() ** 2).mean()) for u in U)
+        ke0 = ke()
+        c.sync()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(steps):
+            c.euler_step(*U, *du, pp3, *pg, dt)
+        b.record()
+        torch.cuda.synchronize()
+        c.sync()
+        c.divergence(pp3, *U)
+        mx, _ = c.div_stats(pp3)
+        res[prec] = {"ms_per_step": round(a.elapsed_time(b) / steps, 2), "div_max_after": mx,
+                     "ke_drift": (ke() - ke0) / ke0}
+        c.close()
+        del U, du, pg, pp3
+        torch.cuda.empty_cache()
+    out.update(res)
+    out["div_ratio_f32_over_f64"] = res["f32_mixed"]["div_max_after"] / max(res["f64"]["div_max_after"], 1e-300)
+    return out
+
+
 def run_b48(args, world, rank, local, torch):
     """The batching workload: 48 seeded uneven periodic boxes (this rank's LPT
     share), 3 FP32 fields each (Taylor-Green + N(0, (1e-2)^2)), all 54 operator
@@ -513,6 +564,8 @@ def run_b200(args, world, rank, local):
     if not args.no_b48:
         out["b48"] = run_b48(args, world, rank, local, torch)
     out["clocks"] = clocks.stop()
+    if args.c5 and rank == 0:
+        out["c5"] = run_c5(torch)
     return out, pts_step
 
 
@@ -573,6 +626,8 @@ def main():
             line["euler_step_ms"] = em
         if "b48" in res:
             line["b48"] = res["b48"]
+        if "c5" in res:
+            line["c5"] = res["c5"]
         if res.get("clocks"):
             line["clocks"] = res["clocks"]
         print(json.dumps(line), flush=True)
