@@ -62,28 +62,26 @@ static void waves_tables(int n, double len, std::vector<double> &k2, std::vector
 
 // c(i,j,k) <- -c / (K ntot), K = k2x Ty^2 Tz^2 + k2y Tx^2 Tz^2 + k2z Tx^2 Ty^2
 // (waves :690-694: xk2(i) * ((Ty*Tz)**2) etc.), zero where K < 1e-16.
-__global__ void k_spectral_divide(double2 *c, int nxh, int ny, int nz, const double *k2x,
+// One division per mode (the reference divides Re and Im by ntot and then by
+// -K; the product form differs from it by a few ulp).  Indices are 32-bit:
+// the spectrum of any grid that fits one GPU has fewer than 2^32 modes.
+__global__ void k_spectral_divide(double2 *c, unsigned nxh, unsigned ny, unsigned n, const double *k2x,
                                   const double *tx, const double *k2y, const double *ty,
                                   const double *k2z, const double *tz, double ntot)
 {
-    const size_t n = (size_t)nxh * ny * nz;
-    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n;
-         p += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(p % nxh);
-        const int j = (int)((p / nxh) % ny);
-        const int k = (int)(p / ((size_t)nxh * ny));
+    for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const unsigned row = p / nxh;
+        const unsigned i = p - row * nxh;
+        const unsigned k = row / ny;
+        const unsigned j = row - k * ny;
         const double txi = __ldg(tx + i), tyj = __ldg(ty + j), tzk = __ldg(tz + k);
         const double tyz = tyj * tzk, txz = txi * tzk, txy = txi * tyj;
         const double kk = __ldg(k2x + i) * (tyz * tyz) + __ldg(k2y + j) * (txz * txz) +
                           __ldg(k2z + k) * (txy * txy);
         double2 v = c[p];
-        if (kk < 1.e-16) {
-            v.x = 0.0;
-            v.y = 0.0;
-        } else {
-            v.x = (v.x / ntot) / (-kk);
-            v.y = (v.y / ntot) / (-kk);
-        }
+        const double f = kk < 1.e-16 ? 0.0 : -1.0 / (kk * ntot);
+        v.x *= f;
+        v.y *= f;
         c[p] = v;
     }
 }
@@ -133,15 +131,17 @@ int poisson_solve(x3d_ctx_s *ctx, double *rhs)
         return set_error(ctx, X3D_ECUDA, "cufftExecD2Z failed");
     const int nxh = ctx->nx / 2 + 1;
     const size_t n = (size_t)nxh * ctx->ny * ctx->nz;
+    if (n >= (1ull << 31)) return set_error(ctx, X3D_EUNSUPPORTED, "spectrum above 2^31 modes");
     const int bs = 256;
     size_t g = (n + bs - 1) / bs;
     const size_t cap = (size_t)ctx->num_sms * 8;
     if (g > cap) g = cap;
     const double ntot = (double)ctx->nx * (double)ctx->ny * (double)ctx->nz;
     ++ctx->launches;
-    k_spectral_divide<<<(unsigned)g, bs, 0, ctx->stream>>>((double2 *)ctx->spectrum, nxh, ctx->ny,
-                                                           ctx->nz, ctx->d_k2x, ctx->d_tx, ctx->d_k2y,
-                                                           ctx->d_ty, ctx->d_k2z, ctx->d_tz, ntot);
+    k_spectral_divide<<<(unsigned)g, bs, 0, ctx->stream>>>((double2 *)ctx->spectrum, (unsigned)nxh,
+                                                           (unsigned)ctx->ny, (unsigned)n, ctx->d_k2x,
+                                                           ctx->d_tx, ctx->d_k2y, ctx->d_ty, ctx->d_k2z,
+                                                           ctx->d_tz, ntot);
     rc = cuda_check(ctx, cudaGetLastError(), "k_spectral_divide");
     if (rc) return rc;
     if (cufftExecZ2D(ctx->plan_z2d, (cufftDoubleComplex *)ctx->spectrum, rhs) != CUFFT_SUCCESS)
