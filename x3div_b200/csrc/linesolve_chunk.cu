@@ -40,6 +40,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <type_traits>
 
 #include "linesolve_chunk.h"
@@ -385,7 +386,8 @@ __device__ __forceinline__ void accumulate(const StageOp<T> &so, T (&acc)[L], co
 // ---------------------------------------------------------------------------
 // y- and z-lines.
 struct StageMaps {
-    CUtensorMap m[kMaxStageTiles];
+    CUtensorMap m[kMaxStageTiles];  // inputs
+    CUtensorMap pm[kMaxStageOps];   // base arrays prefetched into L2 (ops with prefetch_base)
 };
 
 // Flush fields of a stage operator, read from the parameters once per
@@ -398,9 +400,11 @@ struct FlushArgs {
     const void *base2;
     double sign, scale2;
     bool f64, plain;
-    __device__ explicit FlushArgs(const StageOp<T> &so)
+    const T *b2s;  // base2 from a staged tile: this thread's point cs there, or null
+    int b2step;    // elements between consecutive points of the line in that tile
+    __device__ FlushArgs(const StageOp<T> &so, const T *b2s_ = nullptr, int b2step_ = 1)
         : out(so.out), base(so.base), out2(so.out2), base2(so.base2), sign(so.sign), scale2(so.scale2),
-          f64(so.out_f64 != 0)
+          f64(so.out_f64 != 0), b2s(b2s_), b2step(b2step_)
     {
         plain = !base && !out2 && !f64 && sign == 1.0;
     }
@@ -429,7 +433,12 @@ __device__ __forceinline__ void flush_yz_blocked(const FlushArgs<T> &fa, const T
             const size_t p = obase + (size_t)(j0 + i) * ostride;
             const bool in = j0 + i < nv;
             bv[i] = base && in ? base[p] : U(0);
-            b2v[i] = base2 && in ? base2[p] : U(0);
+            if constexpr (std::is_same<T, U>::value) {
+                if (fa.b2s) b2v[i] = fa.b2s[(j0 + i) * fa.b2step];
+                else b2v[i] = base2 && in ? base2[p] : U(0);
+            } else {
+                b2v[i] = base2 && in ? base2[p] : U(0);
+            }
         }
 #pragma unroll
         for (int i = 0; i < B; ++i) {
@@ -501,6 +510,14 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
                     tma_load_3d(tp + (size_t)b * box_n * W, &maps.m[ti], bar, x0, o, b * box_n);
             }
         }
+        // the tile's base arrays (read back by the flushes) into L2
+        for (int mask = prog.prefetch_mask, k = 0; mask; mask >>= 1, ++k) {
+            if (!(mask & 1)) continue;
+            for (int b = 0; b < nbox; ++b) {
+                if (dir == DY) tma_prefetch_3d(&maps.pm[k], x0, b * box_n, o);
+                else tma_prefetch_3d(&maps.pm[k], x0, o, b * box_n);
+            }
+        }
     };
     const ChunkScratch<T> sc = carve_scratch<T>(smem_raw + (PERSIST ? 2 : 1) * slot_bytes, C, W);
     const int cs = c * L;
@@ -532,6 +549,9 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
             return reinterpret_cast<const T *>(base + ti * tile_bytes) + (kHalo + cs - 4) * W + l;
         };
         auto tile_at = [&](int ti, int j) { return col(ti)[(4 + j) * W]; };
+        auto flush_args = [&](const StageOp<T> &so) {
+            return FlushArgs<T>(so, so.base2_tile >= 0 ? col(so.base2_tile) + 4 * W : nullptr, W);
+        };
         const bool live = x0 + l < nx;
         const size_t obase = (size_t)(x0 + l) + (dir == DY ? (size_t)nx * ny * o : (size_t)nx * o) +
                              (size_t)cs * ostride;
@@ -555,9 +575,9 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
             chunk_solve_resp<T, L>(so, resp_s + k * 4 * L, load, r, sc, W, l, c, C, nv, c * W + l);
             if constexpr (ACC) {
                 accumulate<T, L>(so, acc, r, nv, tile_at);
-                if (so.flush && live) flush_yz<T, L>(FlushArgs<T>(so), acc, obase, ostride, nv);
+                if (so.flush && live) flush_yz<T, L>(flush_args(so), acc, obase, ostride, nv);
             } else {
-                if (so.flush && live) flush_yz<T, L>(FlushArgs<T>(so), r, obase, ostride, nv);
+                if (so.flush && live) flush_yz<T, L>(flush_args(so), r, obase, ostride, nv);
             }
         }
         if (PERSIST) __syncthreads();  // the slot is refilled two tiles later
@@ -590,7 +610,12 @@ __device__ __forceinline__ void flush_x_blocked(const FlushArgs<T> &fa, const T 
             const int j = j0 + q * VU;
             const bool in = j < nv;
             bq[q] = base && in ? *reinterpret_cast<const UV *>(base + p0 + j) : UV{};
-            b2q[q] = base2 && in ? *reinterpret_cast<const UV *>(base2 + p0 + j) : UV{};
+            if constexpr (std::is_same<T, U>::value) {
+                if (fa.b2s) b2q[q] = *reinterpret_cast<const UV *>(fa.b2s + j);
+                else b2q[q] = base2 && in ? *reinterpret_cast<const UV *>(base2 + p0 + j) : UV{};
+            } else {
+                b2q[q] = base2 && in ? *reinterpret_cast<const UV *>(base2 + p0 + j) : UV{};
+            }
         }
 #pragma unroll
         for (int q = 0; q < NQ; ++q) {
@@ -733,6 +758,10 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
             for (int rr = 0; rr < rows; ++rr)
                 bulk_load(tp + (size_t)rr * pitch, prog.in[ti] + (size_t)(l0 + rr) * n, row_bytes, bar);
         }
+        // the tile's base rows (read back by the flushes) into L2
+        for (int mask = prog.prefetch_mask, k = 0; mask; mask >>= 1, ++k)
+            if (mask & 1)
+                bulk_prefetch(static_cast<const T *>(prog.ops[k].base) + (size_t)l0 * n, row_bytes * (uint32_t)rows);
     };
     const ChunkScratch<T> sc = carve_scratch<T>(smem_raw + (PERSIST ? 2 : 1) * slot_bytes, C, W);
     // staging rows for plain outputs, after the responses (128-byte aligned)
@@ -768,6 +797,9 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
             return reinterpret_cast<const T *>(base + ti * tile_bytes) + (size_t)lr * pitch + cs;
         };
         auto tile_at = [&](int ti, int j) { return row(ti)[kHalo + j]; };
+        auto flush_args = [&](const StageOp<T> &so) {
+            return FlushArgs<T>(so, so.base2_tile >= 0 ? row(so.base2_tile) + kHalo : nullptr, 1);
+        };
         T r[L];
         T acc[ACC ? L : 1];
         for (int k = 0; k < prog.nops; ++k) {
@@ -803,9 +835,9 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
             chunk_solve_resp<T, L>(so, resp_s + k * 4 * L, load, r, sc, W, l, c, C, nv, c * W + l);
             if constexpr (ACC) {
                 accumulate<T, L>(so, acc, r, nv, tile_at);
-                if (so.flush) flush_x_staged<T, L>(FlushArgs<T>(so), acc, out_s, l, l0, rows, pitch, n, cs, nv);
+                if (so.flush) flush_x_staged<T, L>(flush_args(so), acc, out_s, l, l0, rows, pitch, n, cs, nv);
             } else {
-                if (so.flush) flush_x_staged<T, L>(FlushArgs<T>(so), r, out_s, l, l0, rows, pitch, n, cs, nv);
+                if (so.flush) flush_x_staged<T, L>(flush_args(so), r, out_s, l, l0, rows, pitch, n, cs, nv);
             }
         }
         if (PERSIST) __syncthreads();  // the slot is refilled two tiles later
@@ -885,6 +917,18 @@ static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog_in, int 
 {
     StageProgram<T> prog = prog_in;
     fill_resp(prog, L, prog.ops[0].op.n);
+    // base2 that is a staged input comes from shared memory; T-typed bases
+    // are prefetched into L2 with the tile's inputs
+    for (int k = 0; k < prog.nops; ++k) {
+        StageOp<T> &so = prog.ops[k];
+        so.base2_tile = -1;
+        for (int ti = 0; ti < prog.ntiles; ++ti)
+            if (!so.out_f64 && so.base2 && so.base2 == prog.in[ti]) so.base2_tile = (short)ti;
+        so.prefetch_base = (so.flush && so.base && !so.out_f64) ? 1 : 0;
+    }
+    prog.prefetch_mask = 0;
+    for (int k = 0; k < prog.nops; ++k)
+        if (prog.ops[k].prefetch_base) prog.prefetch_mask |= 1 << k;
     bool acc = false;
     for (int k = 0; k < prog.nops; ++k)
         acc = acc || !plain(StageOpView{prog.ops[k].flush, prog.ops[k].accumulate, prog.ops[k].mul_tile});
@@ -939,19 +983,25 @@ static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog_in, int 
     const size_t smem = (PERSIST ? 2 : 1) * prog.ntiles * tile + scratch_bytes(C, W, es) + resp_bytes;
     if (smem + 1024 > ctx->smem_optin) return X3D_EUNSUPPORTED;
     StageMaps maps;
-    for (int ti = 0; ti < prog.ntiles; ++ti) {
+    std::memset(&maps, 0, sizeof(maps));
+    auto encode = [&](CUtensorMap *m, const void *ptr) {
         cuuint64_t gdim[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
         cuuint64_t gstride[2] = {(cuuint64_t)nx * es, (cuuint64_t)nx * ny * es};
         cuuint32_t box[3] = {(cuuint32_t)W, 1, 1};
         box[dir == DY ? 1 : 2] = (cuuint32_t)box_n;
         cuuint32_t estr[3] = {1, 1, 1};
-        CUresult r = enc(&maps.m[ti],
-                         sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
-                         const_cast<T *>(prog.in[ti]), gdim, gstride, box, estr,
-                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-        if (r != CUDA_SUCCESS) return X3D_EUNSUPPORTED;
-    }
+        return enc(m, sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+                   const_cast<void *>(ptr), gdim, gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    };
+    for (int ti = 0; ti < prog.ntiles; ++ti)
+        if (!encode(&maps.m[ti], prog.in[ti])) return X3D_EUNSUPPORTED;
+    for (int k = 0; k < prog.nops; ++k)
+        if (prog.ops[k].prefetch_base && !encode(&maps.pm[k], prog.ops[k].base)) prog.ops[k].prefetch_base = 0;
+    prog.prefetch_mask = 0;
+    for (int k = 0; k < prog.nops; ++k)
+        if (prog.ops[k].prefetch_base) prog.prefetch_mask |= 1 << k;
     auto kern = acc ? ls_stage_yz<T, W, L, true, PERSIST> : ls_stage_yz<T, W, L, false, PERSIST>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const long tiles_x = (nx + W - 1) / W;

@@ -30,6 +30,11 @@ struct StageOp {
     short accumulate;
     short flush;
     short out_f64;  // out, base, out2, base2 hold double rather than T
+    // Set by launch_stage: base2 is staged input tile base2_tile (-1: read
+    // from global memory); prefetch_base: base is prefetched into L2 when
+    // the tile's inputs are requested.
+    short base2_tile;
+    short prefetch_base;
     // Responses of a chunk's solved values to its carries, for the launch's
     // chunk length L (set by launch_stage): y_j = y_j(local) + F resp[0][j]
     // + B resp[1][j] for a full chunk, resp[2], resp[3] for a short last
@@ -44,6 +49,7 @@ struct StageProgram {
     StageOp<T> ops[kMaxStageOps];
     const T *in[kMaxStageTiles];
     int nops, ntiles;
+    int prefetch_mask;  // bit k: operator k's base is prefetched (set by launch_stage)
 };
 
 // Number of (lines per CTA, chunk length) configurations launch_stage knows.

@@ -72,6 +72,21 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
         : "memory");
 }
 
+// Prefetch of a 3-D tensor box into L2 (no data reaches this CTA).
+__device__ __forceinline__ void tma_prefetch_3d(const CUtensorMap *map, int c0, int c1, int c2)
+{
+    asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(c0), "r"(c1), "r"(c2)
+                 : "memory");
+}
+
+// Prefetch of a contiguous global range into L2 (16-byte aligned, size % 16 == 0).
+__device__ __forceinline__ void bulk_prefetch(const void *src, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 // Orders a tensor map that lives in global memory (written before the
 // launch) before the async proxy reads it.
 __device__ __forceinline__ void fence_tensormap_acquire(const void *map)
