@@ -372,14 +372,14 @@ __device__ __forceinline__ void accumulate(const StageOp<T> &so, T (&acc)[L], co
 #pragma unroll
             for (int j = 0; j < L; ++j) acc[j] = r[j];
         }
+    } else if (so.accumulate) {
+        // points past a short chunk's end read staged halo/padding rows and
+        // are never stored
+#pragma unroll
+        for (int j = 0; j < L; ++j) acc[j] = fma(tile_at(so.mul_tile, j), r[j], acc[j]);
     } else {
 #pragma unroll
-        for (int j = 0; j < L; ++j) {
-            if (j < nv) {
-                const T mv = tile_at(so.mul_tile, j);
-                acc[j] = so.accumulate ? acc[j] + mv * r[j] : mv * r[j];
-            }
-        }
+        for (int j = 0; j < L; ++j) acc[j] = tile_at(so.mul_tile, j) * r[j];
     }
 }
 
@@ -460,10 +460,18 @@ __device__ __forceinline__ void flush_yz(const FlushArgs<T> &fa, const T (&res)[
 {
     if (fa.plain) {
         T *dst = static_cast<T *>(fa.out) + obase;
+        if (nv == L) {  // every chunk but a short last one: no per-point test
 #pragma unroll
-        for (int j = 0; j < L; ++j) {
-            if (j < nv) *dst = res[j];
-            dst += ostride;
+            for (int j = 0; j < L; ++j) {
+                *dst = res[j];
+                dst += ostride;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < L; ++j) {
+                if (j < nv) *dst = res[j];
+                dst += ostride;
+            }
         }
     } else if (fa.f64) {
         flush_yz_blocked<T, double, L>(fa, res, obase, ostride, nv);
@@ -681,16 +689,17 @@ __device__ __forceinline__ void flush_x_staged(const FlushArgs<T> &fa, const T (
         return;
     }
     if (l < rows) {
+        // the staging row is the tile's own: a short last chunk may write
+        // past the line's end there (room for the last window), and the
+        // row copy sends only the line's n points
         T *dst = out_s + (size_t)l * pitch + cs;
 #pragma unroll
         for (int j = 0; j < L; j += V) {
-            if (j < nv) {
-                VT q;
-                T *e = reinterpret_cast<T *>(&q);
+            VT q;
+            T *e = reinterpret_cast<T *>(&q);
 #pragma unroll
-                for (int v = 0; v < V; ++v) e[v] = res[j + v];
-                *reinterpret_cast<VT *>(dst + j) = q;
-            }
+            for (int v = 0; v < V; ++v) e[v] = res[j + v];
+            *reinterpret_cast<VT *>(dst + j) = q;
         }
     }
     fence_proxy_async_smem();
