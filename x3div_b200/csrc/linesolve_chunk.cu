@@ -163,20 +163,24 @@ __device__ __forceinline__ T chunk_carry(const T *e, int K, T mf, T ml, T wrap, 
         s = s < 0 ? s + C : s;
         const int n1 = min(K, C - s);  // chunks s .. s+n1-1, then 0 .. K-n1-1
         const T *p = e + s * W + l;
+#pragma unroll 4
         for (int k = 1; k < n1; ++k, p += W) carry = fma(mf, carry, *p);
         carry = fma(s + n1 == C ? ml : mf, carry, *p);
         p = e + l;
+#pragma unroll 4
         for (int k = n1; k < K; ++k, p += W) carry = fma(mf, carry, *p);
     } else {
         int s = full ? c : c + K;
         s = s >= C ? s - C : s;
         const int n1 = min(K, s + 1);  // chunks s .. s-n1+1, then C-1 .. C-K+n1
         const T *p = e + s * W + l;
+#pragma unroll 4
         for (int k = 0; k < n1; ++k, p -= W) carry = fma(mf, carry, *p);
         if (K > n1) {
             p = e + (C - 1) * W + l;
             carry = fma(ml, carry, *p);
             p -= W;
+#pragma unroll 4
             for (int k = n1 + 1; k < K; ++k, p -= W) carry = fma(mf, carry, *p);
         }
     }
