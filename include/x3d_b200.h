@@ -101,6 +101,19 @@ typedef struct x3d_op_s *x3d_op;
  * device: CUDA ordinal.  precision: X3D_F64 or X3D_F32. */
 int x3d_ctx_create(x3d_ctx *ctx, int nx, int ny, int nz, double xlx, double yly, double zlz,
                    int precision, int device);
+/* x3d_ctx_create with the boundary conditions of src/parameters.f90:
+ * ncl[6] = {nclx1, nclxn, ncly1, nclyn, nclz1, nclzn}, each 0 (periodic,
+ * both ends of a direction), 1 (free slip) or 2 (Dirichlet); NULL means all
+ * periodic.  Along a non-periodic direction nxm = nx - 1 (dx = xlx/(nx-1))
+ * and only the first-derivative operators exist: derx (npaire 0) and derxp
+ * (npaire 1) use der?_ij (src/x3d_derive.f90:156-215, 343-435, 562-665) with
+ * the closures and factors of first_deriv_exp_/first_deriv_imp_
+ * (src/x3d_operator_1d.f90:325-488).  The other operators of such a
+ * direction, and the Poisson solver and the Euler-step compositions, return
+ * X3D_EUNSUPPORTED, as the reference's Poisson solver stops on non-periodic
+ * boundaries (src/poisson.f90:104-108). */
+int x3d_ctx_create_bc(x3d_ctx *ctx, int nx, int ny, int nz, double xlx, double yly, double zlz,
+                      int precision, int device, const int *ncl);
 /* finalise_xcompact3d's device-side part (src/x3d_tools.f90:212-248). */
 int x3d_ctx_destroy(x3d_ctx ctx);
 /* Run the context's work on a caller-owned stream (a cudaStream_t; NULL is

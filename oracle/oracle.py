@@ -58,6 +58,8 @@ def lib() -> ctypes.CDLL:
         L.orc_test_rms.argtypes = [i, p, i, i, i, d, d, d]
         L.orc_test_rms.restype = d
         L.orc_rhs_scalars.argtypes = [i, d, p]
+        L.orc_build_der_np.argtypes = [i, d, i, i, i, p, p, p, p]
+        L.orc_apply_der_np.argtypes = [i, p, p, i, i, i, d, i, i, i]
         _lib = L
     return _lib
 
@@ -85,6 +87,28 @@ def lhs(kind, n: int, d: float) -> dict:
     if rc != 0:
         raise ValueError(f"oracle: bad operator request kind={kind} n={n}")
     return dict(f=f, s=s, w=w, periodic=per, alfa=c5[0], a=c5[1], b=c5[2], c=c5[3], d=c5[4])
+
+
+def lhs_np(n: int, d: float, ncl1: int, ncln: int, npaire: int) -> dict:
+    """Non-periodic first derivative on an n-point line (first_deriv_exp_ /
+    first_deriv_imp_): factors f, s, w of parity npaire and the closure
+    scalars af1, bf1, cf1, af2, afm, afn, bfn, cfn."""
+    f, s, w, cl = np.zeros(n), np.zeros(n), np.zeros(n), np.zeros(8)
+    rc = lib().orc_build_der_np(int(n), float(d), int(ncl1), int(ncln), int(npaire), _p(f), _p(s), _p(w), _p(cl))
+    if rc != 0:
+        raise ValueError(f"oracle: bad non-periodic request n={n} ncl=({ncl1},{ncln})")
+    return dict(f=f, s=s, w=w, cl=cl)
+
+
+def der_np(direction: int, u: np.ndarray, d: float, ncl1: int, ncln: int, npaire: int) -> np.ndarray:
+    """der?_ij: non-periodic first derivative of u along direction."""
+    out = field(u.shape)
+    nx, ny, nz = u.shape
+    rc = lib().orc_apply_der_np(int(direction), _p(out), _p(u), nx, ny, nz, float(d), int(ncl1), int(ncln),
+                                int(npaire))
+    if rc != 0:
+        raise ValueError("oracle: bad non-periodic request")
+    return out
 
 
 def apply(kind, direction: int, u: np.ndarray, d: float) -> np.ndarray:

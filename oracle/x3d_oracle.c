@@ -27,9 +27,12 @@
  * Arrays are Fortran-ordered: element (i,j,k) of an (nx,ny,nz) field lives at
  * i + nx*(j + ny*k), with i (x) fastest, exactly as every 2decomp pencil
  * stores data.  Indices in comments are the reference's 1-based ones.
- * Only the periodic (ncl=0) branches are restated: the reference aborts in
- * decomp_2d_poisson_init for any other boundary condition
- * (src/poisson.f90:104-108), so no other branch is reachable.
+ * The periodic (ncl=0) branches are restated for every operator; of the
+ * non-periodic ones, which the reference can only reach without its Poisson
+ * solver (it aborts in decomp_2d_poisson_init for them, src/poisson.f90:
+ * 104-108), only the first derivatives der?_ij (free slip and Dirichlet ends)
+ * are.  Those are pinned by exactness on cubics (Dirichlet closures) and by
+ * the analytic derivative of mirrored cosines and sines (free slip).
  */
 #include <math.h>
 #include <stdlib.h>
@@ -246,6 +249,103 @@ int orc_thomas_plain(int dir, double *t, int nx, int ny, int nz, const double *f
         tt[(n - 1) * st] = tt[(n - 1) * st] * w[n - 1];
         for (int i = n - 2; i >= 0; --i) tt[i * st] = (tt[i * st] - f[i] * tt[(i + 1) * st]) * w[i];
     }
+    return ORC_OK;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Non-periodic sixth-order compact first derivative (ifirstder = 4).       */
+/* first_deriv_exp_ (x3d_operator_1d.f90:325-393) closure scalars, returned */
+/* in cl[8] = {af1, bf1, cf1, af2, afm, afn, bfn, cfn}, and first_deriv_imp_ */
+/* (:395-488) factors f, s, w of the operator of parity npaire (0: ff/fs/fw,  */
+/* 1: ffp/fsp/fwp).  ncl1, ncln: 1 free slip, 2 Dirichlet.                   */
+int orc_build_der_np(int n, double d, int ncl1, int ncln, int npaire, double *f, double *s, double *w,
+                     double *cl)
+{
+    if (n < 8 || ncl1 < 1 || ncl1 > 2 || ncln < 1 || ncln > 2) return ORC_EBADARG;
+    const double alfai = 1.0 / 3.0;
+    const double alfa1 = 2.0, alfa2 = 0.25, alfan = 2.0, alfam = 0.25;
+    cl[0] = -(5.0 / 2.0) / d; cl[1] = 2.0 / d; cl[2] = 0.5 / d;  /* af1 bf1 cf1 :376-378 */
+    cl[3] = (3.0 / 4.0) / d;                                   /* af2 :382 */
+    cl[4] = (3.0 / 4.0) / d;                                   /* afm :389 */
+    cl[5] = -(5.0 / 2.0) / d; cl[6] = 2.0 / d; cl[7] = 0.5 / d;  /* afn bfn cfn :384-386 */
+    double *fb = calloc(n, sizeof(double)), *fc = calloc(n, sizeof(double)), *ff = calloc(n, sizeof(double));
+    if (ncl1 == 1) {               /* :424-430 */
+        ff[0] = alfai + alfai; ff[1] = alfai; fc[0] = 1.0; fc[1] = 1.0; fb[0] = alfai; fb[1] = alfai;
+    } else {                       /* :431-437 */
+        ff[0] = alfa1; ff[1] = alfa2; fc[0] = 1.0; fc[1] = 1.0; fb[0] = alfa2; fb[1] = alfai;
+    }
+    if (ncln == 1) {               /* :449-458 */
+        ff[n - 3] = alfai; ff[n - 2] = alfai; ff[n - 1] = 0.0;
+        fc[n - 3] = 1.0; fc[n - 2] = 1.0; fc[n - 1] = 1.0;
+        fb[n - 3] = alfai; fb[n - 2] = alfai + alfai; fb[n - 1] = 0.0;
+    } else {                       /* :459-468 */
+        ff[n - 3] = alfai; ff[n - 2] = alfam; ff[n - 1] = 0.0;
+        fc[n - 3] = 1.0; fc[n - 2] = 1.0; fc[n - 1] = 1.0;
+        fb[n - 3] = alfam; fb[n - 2] = alfan; fb[n - 1] = 0.0;
+    }
+    for (int i = 2; i < n - 3; ++i) { ff[i] = alfai; fc[i] = 1.0; fb[i] = alfai; }  /* :470-474 */
+    if (npaire == 1) {             /* :476-486 */
+        if (ncl1 == 1) ff[0] = 0.0;
+        if (ncln == 1) fb[n - 2] = 0.0;
+    }
+    for (int i = 0; i < n; ++i) f[i] = ff[i];
+    orc_prepare(fb, fc, ff, s, w, n);
+    free(fb); free(fc); free(ff);
+    return ORC_OK;
+}
+
+/* der?_ij (x3d_derive.f90:156-215 and the y/z analogues): RHS with the
+ * boundary closures, then the non-periodic Thomas solve.  1-based
+ * tx(1), tx(2), tx(nx-1), tx(nx) are rows 0, 1, n-2, n-1 here. */
+int orc_apply_der_np(int dir, double *out, const double *in, int nx, int ny, int nz, double d, int ncl1,
+                     int ncln, int npaire)
+{
+    int n; long st, nl;
+    line_geom(dir, nx, ny, nz, &n, &st, &nl);
+    double *f = malloc(sizeof(double) * n), *s = malloc(sizeof(double) * n), *w = malloc(sizeof(double) * n);
+    double cl[8];
+    int rc = orc_build_der_np(n, d, ncl1, ncln, npaire, f, s, w, cl);
+    if (rc) { free(f); free(s); free(w); return rc; }
+    const double a = (7.0 / 9.0) / d, b = (1.0 / 36.0) / d;  /* afix, bfix */
+#pragma omp parallel for schedule(static)
+    for (long l = 0; l < nl; ++l) {
+        const long b0 = line_base(dir, nx, ny, l);
+        const double *u = in + b0;
+        double *t = out + b0;
+#define U(i) u[(long)(i) * st]
+#define T(i) t[(long)(i) * st]
+        if (ncl1 == 1) {                                       /* :172-181 */
+            if (npaire == 1) {
+                T(0) = 0.0;
+                T(1) = a * (U(2) - U(0)) + b * (U(3) - U(1));
+            } else {
+                T(0) = a * (U(1) + U(1)) + b * (U(2) + U(2));
+                T(1) = a * (U(2) - U(0)) + b * (U(3) + U(1));
+            }
+        } else {                                               /* :182-185 */
+            T(0) = cl[0] * U(0) + cl[1] * U(1) + cl[2] * U(2);
+            T(1) = cl[3] * (U(2) - U(0));
+        }
+        for (int i = 2; i < n - 2; ++i) T(i) = a * (U(i + 1) - U(i - 1)) + b * (U(i + 2) - U(i - 2));
+        if (ncln == 1) {                                       /* :191-202 */
+            if (npaire == 1) {
+                T(n - 2) = a * (U(n - 1) - U(n - 3)) + b * (U(n - 2) - U(n - 4));
+                T(n - 1) = 0.0;
+            } else {
+                T(n - 2) = a * (U(n - 1) - U(n - 3)) + b * ((-U(n - 2)) - U(n - 4));
+                T(n - 1) = a * ((-U(n - 2)) - U(n - 2)) + b * ((-U(n - 3)) - U(n - 3));
+            }
+        } else {                                               /* :203-206 */
+            T(n - 2) = cl[4] * (U(n - 1) - U(n - 3));
+            T(n - 1) = -cl[5] * U(n - 1) - cl[6] * U(n - 2) - cl[7] * U(n - 3);
+        }
+        for (int i = 1; i < n; ++i) T(i) = T(i) - T(i - 1) * s[i];          /* thomas.f90:72-80 */
+        T(n - 1) = T(n - 1) * w[n - 1];
+        for (int i = n - 2; i >= 0; --i) T(i) = (T(i) - f[i] * T(i + 1)) * w[i];
+#undef U
+#undef T
+    }
+    free(f); free(s); free(w);
     return ORC_OK;
 }
 

@@ -177,3 +177,100 @@ def test_euler_step_runs_and_projects(oracle):
     div_after = oracle.divergence(u, v, w, d, d, d)
     assert np.isfinite(u).all()
     assert np.abs(div_after).max() < 1e-11 * max(np.abs(div_before).max(), 1e-30)
+
+
+# ---- non-periodic first derivatives (der?_ij) --------------------------------
+
+def _line_field(values, direction, other=(3, 2)):
+    """A Fortran-ordered field whose lines along direction all carry values."""
+    n = len(values)
+    shape = list(other)
+    shape.insert(direction, n)
+    view = [1, 1, 1]
+    view[direction] = n
+    return np.asfortranarray(np.broadcast_to(np.asarray(values).reshape(view), shape))
+
+
+def _first_line(f, direction):
+    sl = [0, 0, 0]
+    sl[direction] = slice(None)
+    return f[tuple(sl)]
+
+
+@pytest.mark.parametrize("direction", [0, 1, 2])
+@pytest.mark.parametrize("npaire", [0, 1])
+def test_der_np_dirichlet_exact_on_cubics(oracle, direction, npaire):
+    """Dirichlet ends (ncl = 2) use third-order one-sided compact closures
+    (first_deriv_exp_, src/x3d_operator_1d.f90:375-390) and the interior is
+    sixth order, so a cubic's derivative is exact to round-off everywhere."""
+    n = 40
+    h = 1.0 / (n - 1)
+    x = np.arange(n) * h
+    u = _line_field(x ** 3 - 0.5 * x ** 2 + 0.3 * x, direction)
+    d = oracle.der_np(direction, u, h, 2, 2, npaire)
+    assert np.abs(d - _line_field(3 * x ** 2 - x + 0.3, direction)).max() < 1e-12
+
+
+@pytest.mark.parametrize("npaire", [0, 1])
+def test_der_np_free_slip_mirrored_modes(oracle, npaire):
+    """Free-slip ends (ncl = 1) mirror the field: even (npaire = 1, cos) or
+    odd (npaire = 0, sin) about each wall; the derivative of such a mode
+    keeps the interior scheme's sixth-order accuracy up to the walls."""
+    errs = []
+    for n in (33, 65):
+        h = 1.0 / (n - 1)
+        x = np.arange(n) * h
+        f, df = ((np.cos(np.pi * x), -np.pi * np.sin(np.pi * x)) if npaire == 1
+                 else (np.sin(np.pi * x), np.pi * np.cos(np.pi * x)))
+        d = oracle.der_np(0, _line_field(f, 0), h, 1, 1, npaire)
+        errs.append(np.abs(_first_line(d, 0) - df).max() / np.pi)
+    assert errs[1] < 1e-10
+    assert np.log2(errs[0] / errs[1]) > 5.5  # sixth order
+
+
+@pytest.mark.parametrize("ncl", [(1, 2), (2, 1)])
+@pytest.mark.parametrize("npaire", [0, 1])
+def test_der_np_mixed_ends_converge(oracle, ncl, npaire):
+    """A free-slip end and a Dirichlet end: a quarter-wave mirrored at the
+    free-slip wall, small error at n = 64 and at least third-order
+    convergence (the one-sided closure's order)."""
+    errs = []
+    for n in (33, 64):
+        h = 1.0 / (n - 1)
+        x = np.arange(n) * h
+        y = x if ncl[0] == 1 else 1 - x  # distance from the free-slip wall
+        s = 1.0 if ncl[0] == 1 else -1.0  # d/dx of y
+        if npaire == 1:
+            f, df = np.cos(np.pi * y / 2), -s * np.pi / 2 * np.sin(np.pi * y / 2)
+        else:
+            f, df = np.sin(np.pi * y / 2), s * np.pi / 2 * np.cos(np.pi * y / 2)
+        d = oracle.der_np(0, _line_field(f, 0), h, ncl[0], ncl[1], npaire)
+        errs.append(np.abs(_first_line(d, 0) - df).max())
+    assert errs[1] < (2e-7 if npaire == 1 else 1e-5)
+    assert np.log2(errs[0] / errs[1]) / np.log2(63 / 32) > 2.8
+
+
+def test_der_np_factors_solve_the_matrix(oracle):
+    """The LU factors of first_deriv_imp_ reproduce the banded matrix of the
+    rows it assembles (checked through a dense solve of random right-hand
+    sides for each boundary pair and parity)."""
+    n = 17
+    rng = np.random.default_rng(3)
+    for ncl in [(1, 1), (1, 2), (2, 1), (2, 2)]:
+        for npaire in (0, 1):
+            op = oracle.lhs_np(n, 0.1, ncl[0], ncl[1], npaire)
+            f, s, w = op["f"], op["s"], op["w"]
+            # rebuild M from the factors: M = Lo * Up, Lo(i,i-1) = s_i, Up(i,i) = 1/w_i, Up(i,i+1) = f_i
+            Lo = np.eye(n) + np.diag(s[1:], -1)
+            Up = np.diag(1.0 / w) + np.diag(f[:-1], 1)
+            M = Lo @ Up
+            al = 1.0 / 3.0
+            assert np.allclose(np.diag(M)[2:n - 2], 1.0) and np.allclose(np.diag(M, 1)[2:n - 3], al)
+            r = rng.standard_normal(n)
+            t = r.copy()
+            for i in range(1, n):
+                t[i] -= t[i - 1] * s[i]
+            t[-1] *= w[-1]
+            for i in range(n - 2, -1, -1):
+                t[i] = (t[i] - f[i] * t[i + 1]) * w[i]
+            assert np.allclose(M @ t, r, atol=1e-12)

@@ -30,6 +30,7 @@ _ip = ctypes.POINTER(ctypes.c_int)
 # argument signatures, by exported name
 SIGNATURES = {
     "x3d_ctx_create": [ctypes.POINTER(_vp), _i, _i, _i, _d, _d, _d, _i, _i],
+    "x3d_ctx_create_bc": [ctypes.POINTER(_vp), _i, _i, _i, _d, _d, _d, _i, _i, ctypes.POINTER(_i)],
     "x3d_ctx_destroy": [_vp],
     "x3d_ctx_set_stream": [_vp, _vp],
     "x3d_ctx_get_stream": [_vp, ctypes.POINTER(_vp)],

@@ -84,22 +84,32 @@ class Operator:
 
 
 class Context:
-    """A fully periodic nx*ny*nz box at a 1x1 decomposition (x3d_ctx)."""
+    """An nx*ny*nz box at a 1x1 decomposition (x3d_ctx).  bc, if given, is the
+    reference's (nclx1, nclxn, ncly1, nclyn, nclz1, nclzn): 0 periodic, 1 free
+    slip, 2 Dirichlet (x3d_ctx_create_bc); by default every direction is
+    periodic."""
 
     def __init__(self, nx, ny, nz, lengths=(1.0, 1.0, 1.0), precision="f64", device=0,
-                 stream=None):
+                 stream=None, bc=None):
         self.L = _capi.lib()
         self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
         self.lengths = tuple(float(v) for v in lengths)
         self.precision = precision
         self.fp32 = precision == "f32"
+        self.bc = tuple(int(v) for v in bc) if bc is not None else (0,) * 6
         h = ctypes.c_void_p()
-        rc = self.L.x3d_ctx_create(ctypes.byref(h), self.nx, self.ny, self.nz, *self.lengths,
-                                   X3D_F32 if self.fp32 else X3D_F64, int(device))
+        if bc is None:
+            rc = self.L.x3d_ctx_create(ctypes.byref(h), self.nx, self.ny, self.nz, *self.lengths,
+                                       X3D_F32 if self.fp32 else X3D_F64, int(device))
+        else:
+            ncl = (ctypes.c_int * 6)(*self.bc)
+            rc = self.L.x3d_ctx_create_bc(ctypes.byref(h), self.nx, self.ny, self.nz, *self.lengths,
+                                          X3D_F32 if self.fp32 else X3D_F64, int(device), ncl)
         if rc != 0:
             raise X3DError(rc, "x3d_ctx_create failed")
         self.handle = h.value
-        self.dx, self.dy, self.dz = (l / n for l, n in zip(self.lengths, (nx, ny, nz)))
+        nm = [n - 1 if self.bc[2 * d] else n for d, n in enumerate((nx, ny, nz))]
+        self.dx, self.dy, self.dz = (l / n for l, n in zip(self.lengths, nm))
         if stream is None:
             stream = _torch_current_stream()
         if stream is not None:

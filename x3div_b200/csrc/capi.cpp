@@ -149,7 +149,9 @@ int apply_op(x3d_ctx_s *ctx, void *t, const void *u, x3d_op_s *op, int want_kind
     if (nx <= 0 || ny <= 0 || nz <= 0) return set_error(ctx, X3D_EINVAL, "bad field shape");
     const int n = want_dir == DX ? nx : (want_dir == DY ? ny : nz);
     if (op->h.n != n) return set_error(ctx, X3D_EINVAL, "operator length differs from the line length");
-    if (!op->h.periodic) return set_error(ctx, X3D_EUNSUPPORTED, "only periodic operators are supported");
+    if (!op->h.periodic && (op->h.kind != DER || !op->h.ncl1))
+        return set_error(ctx, X3D_EUNSUPPORTED,
+                         "only periodic operators and the library's non-periodic first derivatives are supported");
     if (t == u) return set_error(ctx, X3D_EINVAL, "t and u must not alias (t is intent(out))");
     const size_t bytes = (size_t)nx * ny * nz * ctx->elem();
     Stager sg(ctx);
@@ -219,8 +221,22 @@ extern "C" {
 int x3d_ctx_create(x3d_ctx *out, int nx, int ny, int nz, double xlx, double yly, double zlz,
                    int precision, int device)
 {
+    return x3d_ctx_create_bc(out, nx, ny, nz, xlx, yly, zlz, precision, device, nullptr);
+}
+
+int x3d_ctx_create_bc(x3d_ctx *out, int nx, int ny, int nz, double xlx, double yly, double zlz,
+                      int precision, int device, const int *ncl_in)
+{
     if (!out) return X3D_EINVAL;
     *out = nullptr;
+    int ncl[6] = {0, 0, 0, 0, 0, 0};
+    if (ncl_in)
+        for (int i = 0; i < 6; ++i) ncl[i] = ncl_in[i];
+    for (int d = 0; d < 3; ++d) {
+        const int a = ncl[2 * d], b = ncl[2 * d + 1];
+        if (a < 0 || a > 2 || b < 0 || b > 2) return X3D_EINVAL;
+        if ((a == 0) != (b == 0)) return X3D_EINVAL;  // periodic means both ends
+    }
     if (nx < 8 || ny < 8 || nz < 8) return X3D_EUNSUPPORTED;
     if (precision != X3D_F64 && precision != X3D_F32) return X3D_EINVAL;
     if (!(xlx > 0 && yly > 0 && zlz > 0)) return X3D_EINVAL;
@@ -229,7 +245,13 @@ int x3d_ctx_create(x3d_ctx *out, int nx, int ny, int nz, double xlx, double yly,
     if (!ctx) return X3D_ENOMEM;
     ctx->nx = nx; ctx->ny = ny; ctx->nz = nz;
     ctx->xlx = xlx; ctx->yly = yly; ctx->zlz = zlz;
-    ctx->dx = xlx / nx; ctx->dy = yly / ny; ctx->dz = zlz / nz;  // parameter(): dx = xlx/nxm, nxm = nx
+    // parameter(): dx = xlx/nxm with nxm = nx when periodic, nx - 1 otherwise
+    // (src/parameters.f90:51-71)
+    ctx->dx = xlx / (ncl[0] ? nx - 1 : nx);
+    ctx->dy = yly / (ncl[2] ? ny - 1 : ny);
+    ctx->dz = zlz / (ncl[4] ? nz - 1 : nz);
+    for (int i = 0; i < 6; ++i) ctx->ncl[i] = ncl[i];
+    ctx->periodic_all = !(ncl[0] || ncl[2] || ncl[4]);
     ctx->precision = precision;
     ctx->device = device;
     cudaDeviceProp prop;
@@ -256,9 +278,18 @@ int x3d_ctx_create(x3d_ctx *out, int nx, int ny, int nz, double xlx, double yly,
             return X3D_ENOMEM;
         }
         op->builtin = true;
-        ctx->builtin[w] = op;
         const int d = kNamed[w].dir;
-        int rc = build_periodic_op(kNamed[w].kind, d, nn[d], dd[d], op->h);
+        int rc;
+        if (!ncl[2 * d]) {
+            rc = build_periodic_op(kNamed[w].kind, d, nn[d], dd[d], op->h);
+        } else if (kNamed[w].kind == DER) {
+            // derx (npaire 0) and derxp (npaire 1), x3d_operator_1d_init :140-141
+            rc = build_nonperiodic_der(d, nn[d], dd[d], ncl[2 * d], ncl[2 * d + 1], (w & 1) ? 1 : 0, op->h);
+        } else {
+            delete op;  // defined for periodic directions only
+            continue;
+        }
+        ctx->builtin[w] = op;
         if (!rc) rc = upload_op(op);
         if (rc) {
             x3d_ctx_destroy(ctx);
@@ -350,6 +381,9 @@ int x3d_op_builtin(x3d_ctx ctx, int which, x3d_op *op)
 {
     if (!ctx || !op) return X3D_EINVAL;
     if (which < 0 || which >= X3D_OP_COUNT) return set_error(ctx, X3D_EINVAL, "unknown operator instance");
+    if (!ctx->builtin[which])
+        return set_error(ctx, X3D_EUNSUPPORTED,
+                         "operator not defined: only first derivatives exist along a non-periodic direction");
     *op = ctx->builtin[which];
     return X3D_OK;
 }
@@ -484,7 +518,10 @@ int x3d_apply_batch(x3d_ctx ctx, const x3d_work *items, int count)
         const x3d_op_s *op = items[i].op;
         if (!op || !items[i].in || !items[i].out) return set_error(ctx, X3D_EINVAL, "null work item");
         const int n = op->h.dir == DX ? ctx->nx : (op->h.dir == DY ? ctx->ny : ctx->nz);
-        if (op->h.n != n || !op->h.periodic) return set_error(ctx, X3D_EINVAL, "operator does not fit the grid");
+        if (op->h.n != n) return set_error(ctx, X3D_EINVAL, "operator does not fit the grid");
+        if (!op->h.periodic && (op->h.kind != DER || !op->h.ncl1))
+            return set_error(ctx, X3D_EUNSUPPORTED,
+                             "only periodic operators and the library's non-periodic first derivatives are supported");
         for (int j = 0; j < count; ++j)
             if (items[i].out == items[j].in) return set_error(ctx, X3D_EINVAL, "an output aliases an input");
     }
@@ -539,15 +576,20 @@ int x3d_autotune(x3d_ctx ctx, int max_group)
             for (int k = 0; k < g; ++k) {
                 const int idx = [&] {
                     for (int w = 0; w < X3D_OP_COUNT; ++w)
-                        if (ctx->builtin[w]->h.kind == kinds[k] && ctx->builtin[w]->h.dir == dir) return w;
-                    return 0;
+                        if (ctx->builtin[w] && ctx->builtin[w]->h.kind == kinds[k] && ctx->builtin[w]->h.dir == dir)
+                            return w;
+                    return -1;
                 }();
+                if (idx < 0) {  // only first derivatives along a non-periodic direction
+                    g = 0;
+                    break;
+                }
                 ops[k] = ctx->builtin[idx];
                 outs[k] = buf[1 + k];
             }
-            rc = autotune_group(ctx, dir, buf[0], ops, kinds, outs, g, fp32(ctx), 3, nullptr);
+            if (g) rc = autotune_group(ctx, dir, buf[0], ops, kinds, outs, g, fp32(ctx), 3, nullptr);
         }
-    if (rc) return rc;
+    if (rc || !ctx->periodic_all) return rc;  // the Euler stages need every direction periodic
     // the fused stages of the Euler step (transeq + int_time, divergence,
     // gradp + cor_vel), run once on scratch fields 7..13 with every
     // configuration timed; fields 0..5 are the stages' own intermediates
@@ -627,10 +669,21 @@ int x3d_transpose_y_to_x(x3d_ctx ctx, const void *in, void *out, int c) { return
 
 // ---- Poisson -------------------------------------------------------------------------
 
+// The Euler-step compositions use the staggered operators, which exist only
+// when every direction is periodic (the reference's Poisson solver likewise
+// stops on other boundary conditions, src/poisson.f90:104-108).
+static int need_periodic(x3d_ctx_s *ctx)
+{
+    return ctx->periodic_all ? X3D_OK
+                             : set_error(ctx, X3D_EUNSUPPORTED,
+                                         "this routine needs periodic boundaries in every direction");
+}
+
 int x3d_poisson(x3d_ctx ctx, double *rhs)
 {
     int rc = check_ctx(ctx);
     if (rc) return rc;
+    if ((rc = need_periodic(ctx))) return rc;
     if (!rhs) return set_error(ctx, X3D_EINVAL, "null field");
     Stager sg(ctx);
     double *d = static_cast<double *>(sg.inout(rhs, ctx->npts() * sizeof(double)));
@@ -769,6 +822,7 @@ int x3d_divergence(x3d_ctx ctx, double *pp3, const void *ux1, const void *uy1, c
 {
     int rc = check_ctx(ctx);
     if (rc) return rc;
+    if ((rc = need_periodic(ctx))) return rc;
     if (!pp3 || !ux1 || !uy1 || !uz1) return set_error(ctx, X3D_EINVAL, "null field");
     const size_t b = ctx->npts() * ctx->elem();
     Stager sg(ctx);
@@ -782,6 +836,7 @@ int x3d_gradp(x3d_ctx ctx, void *px1, void *py1, void *pz1, const double *pp3)
 {
     int rc = check_ctx(ctx);
     if (rc) return rc;
+    if ((rc = need_periodic(ctx))) return rc;
     if (!pp3 || !px1 || !py1 || !pz1) return set_error(ctx, X3D_EINVAL, "null field");
     const size_t b = ctx->npts() * ctx->elem();
     Stager sg(ctx);
@@ -809,6 +864,7 @@ int x3d_solve_poisson(x3d_ctx ctx, double *pp3, void *px1, void *py1, void *pz1,
 {
     int rc = check_ctx(ctx);
     if (rc) return rc;
+    if ((rc = need_periodic(ctx))) return rc;
     if (!pp3 || !px1 || !py1 || !pz1 || !ux1 || !uy1 || !uz1) return set_error(ctx, X3D_EINVAL, "null field");
     const size_t b = ctx->npts() * ctx->elem();
     Stager sg(ctx);
@@ -840,6 +896,7 @@ int x3d_momentum_rhs_eq(x3d_ctx ctx, void *dux1, void *duy1, void *duz1, const v
 {
     int rc = check_ctx(ctx);
     if (rc) return rc;
+    if ((rc = need_periodic(ctx))) return rc;
     if (!dux1 || !duy1 || !duz1 || !ux1 || !uy1 || !uz1) return set_error(ctx, X3D_EINVAL, "null field");
     const size_t b = ctx->npts() * ctx->elem();
     Stager sg(ctx);
@@ -868,6 +925,7 @@ int x3d_euler_step(x3d_ctx ctx, void *ux1, void *uy1, void *uz1, void *dux1, voi
 {
     int rc = check_ctx(ctx);
     if (rc) return rc;
+    if ((rc = need_periodic(ctx))) return rc;
     if (!ux1 || !uy1 || !uz1 || !dux1 || !duy1 || !duz1 || !pp3 || !px1 || !py1 || !pz1)
         return set_error(ctx, X3D_EINVAL, "null field");
     const size_t b = ctx->npts() * ctx->elem();

@@ -121,6 +121,69 @@ int build_periodic_op(int kind, int dir, int n, double d, OpHost &op)
     return X3D_OK;
 }
 
+// Non-periodic sixth-order compact first derivative, ifirstder = 4
+// (first_deriv_exp_ and first_deriv_imp_, src/x3d_operator_1d.f90:325-488):
+// interior rows (alfa, 1, alfa); free-slip ends (ncl = 1) fold the symmetric
+// ghost points into the first/last rows; Dirichlet ends (ncl = 2) use the
+// third-order one-sided rows (alfa1 = 2, alfa2 = 1/4 and their mirror).
+// The operator of parity npaire = 1 (derxp) uses the "p" factors, prepared
+// from ff with ffp(1) = 0 at a free-slip start and fb(n-1) = 0 at a free-slip
+// end (:477-486).
+int build_nonperiodic_der(int dir, int n, double d, int ncl1, int ncln, int npaire, OpHost &op)
+{
+    if (n < 8 || ncl1 < 1 || ncl1 > 2 || ncln < 1 || ncln > 2) return X3D_EUNSUPPORTED;
+    op.kind = DER;
+    op.dir = dir;
+    op.n = n;
+    op.periodic = 0;
+    op.npaire = npaire;
+    op.ncl1 = ncl1;
+    op.ncln = ncln;
+    rhs_scalars(DER, d, &op.alfa, &op.a, &op.b, &op.c, &op.d);
+    const double al = op.alfa;
+    const double alfa1 = 2.0, alfa2 = 0.25, alfan = 2.0, alfam = 0.25;
+    // af1, bf1, cf1, af2, afm, afn, bfn, cfn (:375-390)
+    const double cl[8] = {-2.5 / d, 2.0 / d, 0.5 / d, 0.75 / d, 0.75 / d, -2.5 / d, 2.0 / d, 0.5 / d};
+    for (int i = 0; i < 8; ++i) op.cl[i] = cl[i];
+    std::vector<double> fb(n, 0.0), fc(n, 0.0), ff(n, 0.0);
+    if (ncl1 == 1) {
+        ff[0] = al + al; ff[1] = al;
+        fc[0] = 1.0; fc[1] = 1.0;
+        fb[0] = al; fb[1] = al;
+    } else {
+        ff[0] = alfa1; ff[1] = alfa2;
+        fc[0] = 1.0; fc[1] = 1.0;
+        fb[0] = alfa2; fb[1] = al;
+    }
+    if (ncln == 1) {
+        ff[n - 3] = al; ff[n - 2] = al; ff[n - 1] = 0.0;
+        fc[n - 3] = 1.0; fc[n - 2] = 1.0; fc[n - 1] = 1.0;
+        fb[n - 3] = al; fb[n - 2] = al + al; fb[n - 1] = 0.0;
+    } else {
+        ff[n - 3] = al; ff[n - 2] = alfam; ff[n - 1] = 0.0;
+        fc[n - 3] = 1.0; fc[n - 2] = 1.0; fc[n - 1] = 1.0;
+        fb[n - 3] = alfam; fb[n - 2] = alfan; fb[n - 1] = 0.0;
+    }
+    for (int i = 2; i < n - 3; ++i) {
+        ff[i] = al;
+        fc[i] = 1.0;
+        fb[i] = al;
+    }
+    if (npaire == 0) {
+        op.f = ff;
+        lu_prepare(fb, fc, ff, op.s, op.w);
+    } else {
+        std::vector<double> ffp = ff;
+        if (ncl1 == 1) ffp[0] = 0.0;
+        if (ncln == 1) fb[n - 2] = 0.0;
+        op.f = ffp;
+        lu_prepare(fb, fc, ffp, op.s, op.w);
+    }
+    op.per.clear();
+    finish_op(op);
+    return X3D_OK;
+}
+
 // True when an operator's factors are those of the periodic matrix for its
 // alfa (to 1e-12 relative), i.e. when it is the circulant (alfa, 1, alfa).
 static bool circulant(const OpHost &h)
@@ -255,6 +318,13 @@ int upload_op(x3d_op_s *op)
     };
     fill(op->opf, df);
     fill(op->opd, dd);
+    op->opf.ncl1 = op->opd.ncl1 = h.ncl1;
+    op->opf.ncln = op->opd.ncln = h.ncln;
+    op->opf.npaire = op->opd.npaire = h.npaire;
+    for (int i = 0; i < 8; ++i) {
+        op->opf.cl[i] = (float)h.cl[i];
+        op->opd.cl[i] = h.cl[i];
+    }
     op->opf.a = (float)h.a; op->opf.b = (float)h.b; op->opf.c = (float)h.c; op->opf.d = (float)h.d;
     op->opd.a = h.a; op->opd.b = h.b; op->opd.c = h.c; op->opd.d = h.d;
     fill_circ(h, op->opf, 1e-12);

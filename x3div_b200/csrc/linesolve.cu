@@ -64,6 +64,37 @@ __device__ __forceinline__ T stencil(const T *v, const LineOp<T> &op)
     return T(0);
 }
 
+// Right-hand side at the first two and last two points of a non-periodic
+// first-derivative line (der?_ij, src/x3d_derive.f90:171-210): v is the same
+// 9-point window (v[k] = u_{i-4+k}; entries past the line's ends are never
+// used here).  Free slip (ncl = 1) mirrors the field (npaire = 1: even, so
+// the derivative vanishes at the wall; npaire = 0: odd); Dirichlet (ncl = 2)
+// uses the one-sided closures.  Other points keep the interior stencil r.
+template <typename T>
+__device__ __forceinline__ T der_closure(int i, int n, const T *v, const LineOp<T> &op, T r)
+{
+    const T a = op.a, b = op.b;
+    if (i == 0) {
+        if (op.ncl1 == 1) return op.npaire == 1 ? T(0) : a * (v[5] + v[5]) + b * (v[6] + v[6]);
+        return op.cl[0] * v[4] + op.cl[1] * v[5] + op.cl[2] * v[6];
+    }
+    if (i == 1) {
+        if (op.ncl1 == 1)
+            return op.npaire == 1 ? a * (v[5] - v[3]) + b * (v[6] - v[4]) : a * (v[5] - v[3]) + b * (v[6] + v[4]);
+        return op.cl[3] * (v[5] - v[3]);
+    }
+    if (i == n - 2) {
+        if (op.ncln == 1)
+            return op.npaire == 1 ? a * (v[5] - v[3]) + b * (v[4] - v[2]) : a * (v[5] - v[3]) + b * ((-v[4]) - v[2]);
+        return op.cl[4] * (v[5] - v[3]);
+    }
+    if (i == n - 1) {
+        if (op.ncln == 1) return op.npaire == 1 ? T(0) : a * ((-v[3]) - v[3]) + b * ((-v[2]) - v[2]);
+        return -op.cl[5] * v[4] - op.cl[6] * v[3] - op.cl[7] * v[2];
+    }
+    return r;
+}
+
 template <typename T>
 __device__ __forceinline__ T ldg(const T *p)
 {
@@ -102,9 +133,11 @@ __device__ __forceinline__ void solve_line(const Src &src, const ZB &zb, const D
     double acc = 0.0;
     int i = 0;
     const int nmain = n - 5;
+    const bool closed = KIND == DER && !op.periodic;
 #pragma unroll 4
     for (; i < nmain; ++i) {
-        const T r = stencil<KIND>(v, op);
+        T r = stencil<KIND>(v, op);
+        if (closed && i < 2) r = der_closure(i, n, v, op, r);
         z = r - ldg(op.s + i) * z;
         acc = fma(ldg(op.g + i), (double)r, acc);
         zb.st(i, z);
@@ -113,7 +146,8 @@ __device__ __forceinline__ void solve_line(const Src &src, const ZB &zb, const D
         v[8] = src.ld(i + 5);
     }
     for (; i < n; ++i) {
-        const T r = stencil<KIND>(v, op);
+        T r = stencil<KIND>(v, op);
+        if (closed && (i < 2 || i >= n - 2)) r = der_closure(i, n, v, op, r);
         z = r - ldg(op.s + i) * z;
         acc = fma(ldg(op.g + i), (double)r, acc);
         zb.st(i, z);
@@ -232,11 +266,13 @@ __device__ __forceinline__ void solve_row_vec(T *row, const LineOp<T> &op)
     for (int k = 0; k < 4; ++k) head[k] = wb[4 + k];
     T z = T(0);
     double acc = 0.0;
+    const bool closed = KIND == DER && !op.periodic;
     for (int i = 0; i < n; i += V) {
         T zv[V];
 #pragma unroll
         for (int q = 0; q < V; ++q) {
-            const T r = stencil<KIND>(wb + q, op);
+            T r = stencil<KIND>(wb + q, op);
+            if (closed && (i + q < 2 || i + q >= n - 2)) r = der_closure(i + q, n, wb + q, op, r);
             z = r - ldg(op.s + i + q) * z;
             acc = fma(ldg(op.g + i + q), (double)r, acc);
             zv[q] = z;

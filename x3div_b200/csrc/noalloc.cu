@@ -66,6 +66,8 @@ extern "C" int x3d_divergence_noalloc(x3d_ctx ctx, double *pp3, const void *ux1,
     if (!ctx) return X3D_EINVAL;
     if (cudaSetDevice(ctx->device) != cudaSuccess) return set_error(ctx, X3D_ECUDA, "cudaSetDevice failed");
     if (!pp3 || !ux1 || !uy1 || !uz1) return set_error(ctx, X3D_EINVAL, "null field");
+    if (!ctx->periodic_all)
+        return set_error(ctx, X3D_EUNSUPPORTED, "the divergence needs periodic boundaries in every direction");
     if (!on_device(pp3) || !on_device(ux1) || !on_device(uy1) || !on_device(uz1))
         return set_error(ctx, X3D_EINVAL,
                          "x3d_divergence_noalloc takes device pointers only (staging host arrays would allocate)");

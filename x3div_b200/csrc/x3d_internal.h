@@ -50,6 +50,12 @@ struct LineOp {
     // the whole line, summed once and scaled by wrap.
     int depth[2];
     int circ;
+    // Non-periodic first derivatives (periodic == 0): boundary conditions at
+    // the two ends (1 free slip, 2 Dirichlet), the operator's parity and the
+    // one-sided closure scalars af1, bf1, cf1, af2, afm, afn, bfn, cfn of
+    // first_deriv_exp_ (src/x3d_operator_1d.f90:375-390).
+    int ncl1, ncln, npaire;
+    T cl[8];
 };
 
 template <typename T>
@@ -60,6 +66,8 @@ constexpr int kChunkShort = sizeof(T) == 4 ? 16 : 8;
 // Host-side operator: FP64 contents of x3doperator1d plus the RHS scalars.
 struct OpHost {
     int kind = 0, dir = 0, n = 0, npaire = 0, periodic = 1;
+    int ncl1 = 0, ncln = 0;  // boundary conditions of a non-periodic operator
+    double cl[8] = {};       // its closure scalars (LineOp::cl)
     double alfa = 0, a = 0, b = 0, c = 0, d = 0;
     std::vector<double> f, s, w, per, g;
     double den = 1.0;
@@ -83,6 +91,10 @@ struct x3d_ctx_s {
     double dx = 1, dy = 1, dz = 1;
     int precision = X3D_F64;
     int device = 0;
+    // boundary conditions nclx1, nclxn, ncly1, nclyn, nclz1, nclzn (0 periodic,
+    // 1 free slip, 2 Dirichlet); the Euler-step compositions need all periodic
+    int ncl[6] = {0, 0, 0, 0, 0, 0};
+    bool periodic_all = true;
     int num_sms = 148;
     size_t smem_optin = 0;
     cudaStream_t own_stream = nullptr;
@@ -121,6 +133,8 @@ namespace x3d {
 // ---- coefficient precompute (coeffs.cpp) -------------------------------
 void rhs_scalars(int kind, double d, double *alfa, double *a, double *b, double *c, double *dd);
 int build_periodic_op(int kind, int dir, int n, double d, OpHost &op);
+// Non-periodic first derivative: ncl1, ncln in {1, 2}, npaire 0 or 1.
+int build_nonperiodic_der(int dir, int n, double d, int ncl1, int ncln, int npaire, OpHost &op);
 void finish_op(OpHost &op);  // computes g, den, glen from f, s, w, per
 int upload_op(x3d_op_s *op);
 void free_op(x3d_op_s *op);
