@@ -157,8 +157,11 @@ int x3d_op_info(x3d_op op, int *meta, double *scal, double *f, double *s, double
 
 /* derx_00 (src/x3d_derive.f90:111-152): tx = d(ux)/dx */
 int x3d_derx(x3d_ctx ctx, void *tx, const void *ux, x3d_op op, int nx, int ny, int nz);
-/* dery_00 (src/x3d_derive.f90:279-339); ppy is the stretching metric, unused
- * because istret = 0 (src/parameters.f90:117); may be NULL */
+/* dery_00 (src/x3d_derive.f90:279-339).  ppy: the stretching metric (ny
+ * values, host or device); NULL stands for istret = 0, the reference's
+ * setting (src/parameters.f90:117), otherwise ty(i,j,k) *= ppy(j) after the
+ * solve (:331-337).  deryvp takes ppyi and derypv ppy the same way
+ * (src/x3d_staggered.f90:629-635, 875-881). */
 int x3d_dery(x3d_ctx ctx, void *ty, const void *uy, x3d_op op, const double *ppy, int nx, int ny,
              int nz);
 /* derz_00 (src/x3d_derive.f90:503-558) */

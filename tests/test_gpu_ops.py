@@ -245,3 +245,42 @@ def test_autotune_records_choices(torch_cuda, contexts):
             assert 0 <= ctx.autotune_choice(direction, g) <= 12
     assert ctx.autotune_choice(0, 6) == -1
     ctx.set_kernel(-1)
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("where", ["host_metric", "device_metric", "host_fields"])
+def test_y_routines_apply_stretching_metric(oracle, torch_cuda, contexts, prec, where):
+    """dery_00 / deryvp / derypv with istret /= 0 multiply the result by
+    ppy(j) (ppyi(j) for deryvp) after the solve (src/x3d_derive.f90:331-337,
+    src/x3d_staggered.f90:629-635, 875-881)."""
+    torch = torch_cuda
+    from x3div_b200 import to_device, to_host
+    shape = (12, 20, 10)
+    nx, ny, nz = shape
+    ctx = contexts(shape, prec)
+    dt = torch.float64 if prec == "f64" else torch.float32
+    u_h = seeded_field(shape, seed=77, noise=1e-2)
+    u_d = to_device(u_h, dt)
+    u_used = to_host(u_d).astype(np.float64)
+    yj = np.arange(ny) / ny
+    metric = 1.0 + 0.3 * np.cos(2 * np.pi * yj) + 0.05 * yj  # > 0, not symmetric
+    m_arg = torch.tensor(metric, dtype=torch.float64, device="cuda") if where == "device_metric" else metric
+    tol = 1e-12 if prec == "f64" else 1e-5
+    for routine, opname, kind, style in (("dery", "dery", "der", "dy"), ("dery", "deryp", "der", "dy"),
+                                         ("deryvp", "deryvp", "dervp", "vpy"),
+                                         ("derypv", "derypv", "derpv", "pvy")):
+        op = ctx.op(opname)
+        if where == "host_fields":
+            u_arg = np.asfortranarray(u_used.astype(np.float64 if prec == "f64" else np.float32))
+            t_arg = np.zeros_like(u_arg, order="F")
+        else:
+            u_arg, t_arg = u_d, torch.empty_like(u_d)
+        if style == "dy":
+            getattr(ctx, routine)(t_arg, u_arg, op, m_arg, nx, ny, nz)
+        else:
+            getattr(ctx, routine)(t_arg, u_arg, op, m_arg, nx, ny, ny, nz)
+        ctx.sync()
+        got = t_arg if where == "host_fields" else to_host(t_arg)
+        ref = oracle.apply(kind, Y, u_used, ctx.dy) * metric[None, :, None]
+        err = rel_err(np.asarray(got, dtype=np.float64), ref)
+        assert err < tol, (routine, opname, prec, where, err)

@@ -139,9 +139,11 @@ int check_ctx(x3d_ctx_s *ctx)
 
 bool fp32(const x3d_ctx_s *ctx) { return ctx->precision == X3D_F32; }
 
-// One operator application on (nx,ny,nz) fields along dir.
+// One operator application on (nx,ny,nz) fields along dir; with ppy (a y
+// operator of dery_00/deryvp/derypv given a stretching metric, host or
+// device, ny values) the result is then multiplied by ppy(j).
 int apply_op(x3d_ctx_s *ctx, void *t, const void *u, x3d_op_s *op, int want_kind, int want_dir,
-             int nx, int ny, int nz)
+             int nx, int ny, int nz, const double *ppy = nullptr)
 {
     if (!op || !t || !u) return set_error(ctx, X3D_EINVAL, "null operator or field");
     if (op->h.kind != want_kind || op->h.dir != want_dir)
@@ -158,7 +160,27 @@ int apply_op(x3d_ctx_s *ctx, void *t, const void *u, x3d_op_s *op, int want_kind
     void *du = sg.in(u, bytes);
     void *dt = sg.out(t, bytes);
     if (sg.status()) return sg.status();
-    return sg.finish(launch_linesolve(ctx, op, want_kind, want_dir, du, dt, nx, ny, nz, fp32(ctx)));
+    int rc = launch_linesolve(ctx, op, want_kind, want_dir, du, dt, nx, ny, nz, fp32(ctx));
+    if (!rc && ppy) {
+        const double *dm = ppy;
+        if (!is_device_ptr(ppy)) {
+            if (ctx->metric_len < ny) {
+                if (ctx->d_metric) cudaFree(ctx->d_metric);
+                ctx->d_metric = nullptr;
+                ctx->metric_len = 0;
+                if (cudaMalloc(&ctx->d_metric, ny * sizeof(double)) != cudaSuccess)
+                    return sg.finish(set_error(ctx, X3D_ENOMEM, "stretching metric allocation failed"));
+                ctx->metric_len = ny;
+            }
+            rc = cuda_check(ctx, cudaMemcpyAsync(ctx->d_metric, ppy, ny * sizeof(double), cudaMemcpyHostToDevice,
+                                                 ctx->stream),
+                            "stretching metric upload");
+            if (!rc) rc = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "stretching metric upload");
+            dm = ctx->d_metric;
+        }
+        if (!rc) rc = launch_scale_y(ctx, fp32(ctx), dt, dm, nx, ny, nz);
+    }
+    return sg.finish(rc);
 }
 
 int thomas_call(x3d_ctx_s *ctx, int dir, void *tt, const double *ff, const double *fs,
@@ -317,6 +339,7 @@ int x3d_ctx_destroy(x3d_ctx ctx)
     ctx->scratch.clear();
     if (ctx->d_err) cudaFree(ctx->d_err);
     if (ctx->d_red) cudaFree(ctx->d_red);
+    if (ctx->d_metric) cudaFree(ctx->d_metric);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return X3D_OK;
@@ -459,8 +482,12 @@ int x3d_op_info(x3d_op op, int *meta, double *scal, double *f, double *s, double
 
 int x3d_derx(x3d_ctx ctx, void *tx, const void *ux, x3d_op op, int nx, int ny, int nz)
 { X3D_APPLY(DER, DX, tx, ux, op, nx, ny, nz); }
-int x3d_dery(x3d_ctx ctx, void *ty, const void *uy, x3d_op op, const double *, int nx, int ny, int nz)
-{ X3D_APPLY(DER, DY, ty, uy, op, nx, ny, nz); }
+int x3d_dery(x3d_ctx ctx, void *ty, const void *uy, x3d_op op, const double *ppy, int nx, int ny, int nz)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    return apply_op(ctx, ty, uy, op, DER, DY, nx, ny, nz, ppy);
+}
 int x3d_derz(x3d_ctx ctx, void *tz, const void *uz, x3d_op op, int nx, int ny, int nz)
 { X3D_APPLY(DER, DZ, tz, uz, op, nx, ny, nz); }
 int x3d_derxx(x3d_ctx ctx, void *tx, const void *ux, x3d_op op, int nx, int ny, int nz)
@@ -491,12 +518,22 @@ int x3d_interxpv(x3d_ctx ctx, void *tx, const void *ux, x3d_op op, int nxm, int 
 { X3D_STAG(INTPV, DX, tx, ux, op, nxm, nx, nx, ny, nz); }
 int x3d_interyvp(x3d_ctx ctx, void *ty, const void *uy, x3d_op op, int nx, int ny, int nym, int nz)
 { X3D_STAG(INTVP, DY, ty, uy, op, ny, nym, nx, ny, nz); }
-int x3d_deryvp(x3d_ctx ctx, void *ty, const void *uy, x3d_op op, const double *, int nx, int ny, int nym, int nz)
-{ X3D_STAG(DERVP, DY, ty, uy, op, ny, nym, nx, ny, nz); }
+int x3d_deryvp(x3d_ctx ctx, void *ty, const void *uy, x3d_op op, const double *ppyi, int nx, int ny, int nym, int nz)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (ny != nym) return set_error(ctx, X3D_EUNSUPPORTED, "non-periodic staggered grids are not supported");
+    return apply_op(ctx, ty, uy, op, DERVP, DY, nx, ny, nz, ppyi);
+}
 int x3d_interypv(x3d_ctx ctx, void *ty, const void *uy, x3d_op op, int nx, int nym, int ny, int nz)
 { X3D_STAG(INTPV, DY, ty, uy, op, nym, ny, nx, ny, nz); }
-int x3d_derypv(x3d_ctx ctx, void *ty, const void *uy, x3d_op op, const double *, int nx, int nym, int ny, int nz)
-{ X3D_STAG(DERPV, DY, ty, uy, op, nym, ny, nx, ny, nz); }
+int x3d_derypv(x3d_ctx ctx, void *ty, const void *uy, x3d_op op, const double *ppy, int nx, int nym, int ny, int nz)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (ny != nym) return set_error(ctx, X3D_EUNSUPPORTED, "non-periodic staggered grids are not supported");
+    return apply_op(ctx, ty, uy, op, DERPV, DY, nx, ny, nz, ppy);
+}
 int x3d_derzvp(x3d_ctx ctx, void *tz, const void *uz, x3d_op op, int nx, int ny, int nz, int nzm)
 { X3D_STAG(DERVP, DZ, tz, uz, op, nz, nzm, nx, ny, nz); }
 int x3d_interzvp(x3d_ctx ctx, void *tz, const void *uz, x3d_op op, int nx, int ny, int nz, int nzm)

@@ -145,6 +145,16 @@ __global__ void k_absmax_sum(const double *p, size_t n, double *out)
     }
 }
 
+// t(i,j,k) *= ppy(j): the stretching multiply of dery_00, deryvp and derypv
+// when istret /= 0 (src/x3d_derive.f90:331-337, src/x3d_staggered.f90:629-635,
+// 875-881).  Grid-stride over the field; j from the flat index.
+template <typename T>
+__global__ void k_scale_y(T *t, const double *ppy, int nx, int ny, size_t n)
+{
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x)
+        t[p] = (T)((double)t[p] * ppy[(p / (size_t)nx) % (size_t)ny]);
+}
+
 #define X3D_LAUNCH(kern, n, ...)                                                          \
     do {                                                                                  \
         const int bs_ = 256;                                                              \
@@ -178,6 +188,13 @@ int launch_sub3(x3d_ctx_s *ctx, bool fp32, void *u, void *v, void *w, const void
                    (const float *)b, (const float *)c, n);
     X3D_LAUNCH(k_sub3<double>, n, (double *)u, (double *)v, (double *)w, (const double *)a,
                (const double *)b, (const double *)c, n);
+}
+
+int launch_scale_y(x3d_ctx_s *ctx, bool fp32, void *t, const double *ppy, int nx, int ny, int nz)
+{
+    const size_t n = (size_t)nx * ny * nz;
+    if (fp32) X3D_LAUNCH(k_scale_y<float>, n, (float *)t, ppy, nx, ny, n);
+    X3D_LAUNCH(k_scale_y<double>, n, (double *)t, ppy, nx, ny, n);
 }
 
 int launch_mul(x3d_ctx_s *ctx, bool fp32, void *out, const void *a, const void *b, size_t n)

@@ -114,6 +114,8 @@ struct x3d_ctx_s {
     // host-pointer staging buffers
     std::vector<std::pair<void *, size_t>> staging;
     double *d_red = nullptr;  // small reduction buffer
+    double *d_metric = nullptr;  // device copy of a y stretching metric (ny doubles)
+    int metric_len = 0;
     // kernel choice per (direction, grid, precision, operator-group size):
     // filled by the autotuner, default_cfg otherwise
     std::map<std::string, int> tuned;
@@ -164,6 +166,7 @@ int launch_axpy3(x3d_ctx_s *ctx, bool fp32, void *u, void *v, void *w, const voi
 int launch_sub3(x3d_ctx_s *ctx, bool fp32, void *u, void *v, void *w, const void *a,
                 const void *b, const void *c, size_t n);                   // u -= a
 int launch_mul(x3d_ctx_s *ctx, bool fp32, void *out, const void *a, const void *b, size_t n);
+int launch_scale_y(x3d_ctx_s *ctx, bool fp32, void *t, const double *ppy, int nx, int ny, int nz);
 int launch_fma_acc(x3d_ctx_s *ctx, bool fp32, void *out, const void *base, const void *a,
                    const void *b, size_t n);  // out = base + a*b
 int launch_add(x3d_ctx_s *ctx, bool fp32, void *out, const void *a, const void *b, size_t n);
