@@ -525,7 +525,8 @@ def run_b200(args, world, rank, local):
         c.sync()
         c.divergence(pp3, *U)
         mx, mean = c.div_stats(pp3)
-        return max_over_ranks(a.elapsed_time(b) / reps, world), mx
+        stages = {s: c.autotune_stage_choice(s) for s in c.STAGES}
+        return max_over_ranks(a.elapsed_time(b) / reps, world), mx, stages
 
     if not args.no_euler:
         out["euler_f32"] = euler_ms(ctx, torch.float32, profile=args.profile_timed == "euler")
@@ -619,9 +620,11 @@ def main():
         if "euler_f32" in res:
             em["f32_mixed"] = round(res["euler_f32"][0], 2)
             em["f32_mixed_div_after_max"] = res["euler_f32"][1]
+            em["f32_stage_configs"] = res["euler_f32"][2]
         if "euler_f64" in res:
             em["f64"] = round(res["euler_f64"][0], 2)
             em["f64_div_after_max"] = res["euler_f64"][1]
+            em["f64_stage_configs"] = res["euler_f64"][2]
         if em:
             line["euler_step_ms"] = em
         if "b48" in res:

@@ -216,14 +216,20 @@ int x3d_apply_batch(x3d_ctx ctx, const x3d_work *items, int count);
  * fixed default configuration is used.  No reference counterpart. */
 int x3d_autotune(x3d_ctx ctx, int max_group);
 /* Force kernel configuration cfg (0..5 chunked, one CTA per tile;
- * 6..11 the same shapes as persistent double-buffered kernels; 12 one thread per line) for
+ * 6..11 the same shapes as persistent double-buffered kernels; 12..15 y/z
+ * kernels that carry two x-adjacent lines per thread in packed FP32
+ * registers (FP32 contexts, even nx); 16 one thread per line) for
  * every later call and forget tuned choices; -1 restores the default.  A
  * configuration that cannot handle a call (alignment, shared memory) still
  * falls back to one that can.  No reference counterpart. */
 int x3d_ctx_set_kernel(x3d_ctx ctx, int cfg);
 /* The configuration chosen for (direction, group size): *cfg = -1 when not
- * tuned, 0..11 chunked variants, 12 one thread per line. */
+ * tuned, 0..15 chunked variants, 16 one thread per line. */
 int x3d_autotune_choice(x3d_ctx ctx, int dir, int group, int *cfg);
+/* The configuration chosen for a fused stage of the Euler step (*cfg = -1
+ * when not tuned): stage is one of transeq_x, transeq_y, transeq_z, div_x,
+ * div_y, div_z, gradp_z, gradp_y, gradp_x, gradp_x_cor. */
+int x3d_autotune_stage_choice(x3d_ctx ctx, const char *stage, int *cfg);
 
 /* ---- batches of independent boxes ----------------------------------------- */
 

@@ -15,6 +15,7 @@ from conftest import rel_err, seeded_field
 pytestmark = pytest.mark.gpu
 
 X, Y, Z = 0, 1, 2
+KERNEL_CONFIGS = 17  # x3d_ctx_set_kernel: 0..15 chunked, 16 one thread per line
 
 # (routine, operator instance, oracle kind, direction, signature style)
 ROUTINES = [
@@ -180,11 +181,13 @@ def test_bad_calls_raise(torch_cuda, contexts):
     ctx.sync()
 
 
-@pytest.mark.parametrize("cfg", list(range(13)))
+@pytest.mark.parametrize("cfg", list(range(KERNEL_CONFIGS)))
 @pytest.mark.parametrize("prec", ["f64", "f32"])
-@pytest.mark.parametrize("shape", [(8, 8, 8), (64, 48, 40), (100, 36, 12), (96, 20, 200)])
+# (40, 60, 62): y and z lines of 4 chunks of 16 with a short last chunk,
+# which the paired configurations take
+@pytest.mark.parametrize("shape", [(8, 8, 8), (64, 48, 40), (100, 36, 12), (96, 20, 200), (40, 60, 62)])
 def test_every_kernel_configuration(oracle, torch_cuda, contexts, cfg, prec, shape):
-    """Each kernel configuration (chunked variants 0-11, one thread per line 12)
+    """Each kernel configuration (chunked variants 0-15, one thread per line 16)
     reproduces the oracle; configurations that cannot take a shape fall back."""
     torch = torch_cuda
     from x3div_b200 import to_device, to_host
@@ -223,7 +226,7 @@ def test_grouped_batch_matches_single_calls(oracle, torch_cuda, contexts, prec, 
              ("dery", "deryy", "deryvp", "derypv", "intyvp", "intypv"),
              ("derz", "derzz", "derzvp", "derzpv", "intzvp", "intzpv")]
     d = (ctx.dx, ctx.dy, ctx.dz)
-    for cfg in range(13):
+    for cfg in range(KERNEL_CONFIGS):
         ctx.set_kernel(cfg)
         outs = [[torch.empty_like(u_d) for _ in range(6)] for _ in range(3)]
         items = [(ctx.op(names[di][k]), u_d, outs[di][k]) for di in range(3) for k in range(6)]
@@ -242,7 +245,7 @@ def test_autotune_records_choices(torch_cuda, contexts):
     ctx.autotune(max_group=3)
     for direction in range(3):
         for g in (1, 2, 3):
-            assert 0 <= ctx.autotune_choice(direction, g) <= 12
+            assert 0 <= ctx.autotune_choice(direction, g) < KERNEL_CONFIGS
     assert ctx.autotune_choice(0, 6) == -1
     ctx.set_kernel(-1)
 

@@ -205,3 +205,30 @@ def test_512_selected_ops(oracle, torch_cuda, prec):
         ref = oracle.apply(kind, direction, used, 2 * np.pi / n)
         assert rel_err(to_host(t), ref) < tol, (routine, prec)
     ctx.close()
+
+
+@pytest.mark.parametrize("cfg", [6, 12, 13, 14, 15])
+@pytest.mark.parametrize("shape", [(64, 48, 32), (36, 60, 62)])
+def test_forced_stage_configurations_match_oracle(oracle, torch_cuda, cfg, shape):
+    """Three FP32-mixed timesteps with every fused stage forced onto one kernel
+    configuration: 6 (one line per thread), 12-15 (two x-adjacent y/z lines
+    per thread in packed FP32 registers), whose transeq, divergence and gradp
+    launches take every flush form (plain, du += ..., u = u + dt du, FP64 pp3,
+    u -= grad p).  Stages that a configuration cannot take fall back."""
+    torch = torch_cuda
+    from x3div_b200 import to_device, to_host
+    ctx = ctx_for(shape, "f32")
+    ctx.set_kernel(cfg)
+    U = [to_device(a, torch.float32) for a in fields(shape, (11, 12, 13))]
+    ref = [to_host(a).astype(np.float64) for a in U]
+    du = [torch.empty_like(U[0]) for _ in range(3)]
+    pg = [torch.empty_like(U[0]) for _ in range(3)]
+    pp3 = torch.empty(shape[::-1], dtype=torch.float64, device="cuda")
+    for _ in range(3):
+        ctx.euler_step(*U, *du, pp3, *pg, 1e-3)
+        oracle.euler_step(*ref, 1e-3, lengths=LEN)
+    ctx.sync()
+    for got, r in zip(U, ref):
+        assert rel_err(to_host(got), r) < 1e-4, cfg
+    ctx.set_kernel(-1)
+    ctx.close()

@@ -64,6 +64,7 @@ SIGNATURES = {
     "x3d_autotune": [_vp, _i],
     "x3d_ctx_set_kernel": [_vp, _i],
     "x3d_autotune_choice": [_vp, _i, _i, _ip],
+    "x3d_autotune_stage_choice": [_vp, ctypes.c_char_p, _ip],
     "x3d_batch_create": [ctypes.POINTER(_vp), _vp, _i, _i, _i],
     "x3d_batch_destroy": [_vp],
     "x3d_batch_set_stream": [_vp, _vp],

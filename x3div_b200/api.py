@@ -250,12 +250,21 @@ class Context:
         self._check(self.L.x3d_autotune(self.handle, int(max_group)))
 
     def set_kernel(self, cfg):
-        """Force a kernel configuration (0..11 chunked, 12 thread per line, -1 default)."""
+        """Force a kernel configuration (0..15 chunked, 16 thread per line, -1 default)."""
         self._check(self.L.x3d_ctx_set_kernel(self.handle, int(cfg)))
 
     def autotune_choice(self, direction, group):
         out = ctypes.c_int()
         self._check(self.L.x3d_autotune_choice(self.handle, int(direction), int(group), ctypes.byref(out)))
+        return out.value
+
+    STAGES = ("transeq_x", "transeq_y", "transeq_z", "div_x", "div_y", "div_z",
+              "gradp_z", "gradp_y", "gradp_x", "gradp_x_cor")
+
+    def autotune_stage_choice(self, stage):
+        """Configuration the autotuner chose for a fused Euler-step stage (-1: not tuned)."""
+        out = ctypes.c_int()
+        self._check(self.L.x3d_autotune_stage_choice(self.handle, stage.encode(), ctypes.byref(out)))
         return out.value
 
     # -- thomas -----------------------------------------------------------

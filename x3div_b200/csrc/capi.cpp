@@ -672,6 +672,14 @@ int x3d_autotune_choice(x3d_ctx ctx, int dir, int group, int *cfg)
     return X3D_OK;
 }
 
+int x3d_autotune_stage_choice(x3d_ctx ctx, const char *stage, int *cfg)
+{
+    if (!ctx || !stage || !cfg) return X3D_EINVAL;
+    const auto it = ctx->stage_tuned.find(stage);
+    *cfg = it == ctx->stage_tuned.end() ? -1 : it->second;
+    return X3D_OK;
+}
+
 // ---- Thomas ------------------------------------------------------------------------
 
 int x3d_xthomas(x3d_ctx ctx, void *tt, const double *ff, const double *fs, const double *fw,

@@ -51,6 +51,58 @@ namespace x3d {
 
 constexpr uint64_t kChunkWaitNs = 2000000000ull;
 
+// Two x-adjacent y/z lines' values in one 64-bit register pair, computed with
+// the packed FP32 instructions of sm_100: per lane the same IEEE operations
+// (round-to-nearest add, multiply, fused multiply-add) as the scalar code,
+// for half the instructions.
+struct F2 {
+    float2 v;
+    F2() = default;
+    __device__ __forceinline__ explicit F2(float s) : v(make_float2(s, s)) {}
+    __device__ __forceinline__ explicit F2(float2 x) : v(x) {}
+};
+__device__ __forceinline__ F2 operator+(F2 a, F2 b) { return F2(__fadd2_rn(a.v, b.v)); }
+// a - b as b * (-1) + a: one rounding of the exact difference, as a subtraction
+__device__ __forceinline__ F2 operator-(F2 a, F2 b) { return F2(__ffma2_rn(b.v, make_float2(-1.f, -1.f), a.v)); }
+__device__ __forceinline__ F2 operator*(F2 a, F2 b) { return F2(__fmul2_rn(a.v, b.v)); }
+__device__ __forceinline__ F2 &operator+=(F2 &a, F2 b) { return a = a + b; }
+// fma for the scalar types too, so that the unqualified calls below resolve
+// to the exact overload inside this namespace
+__device__ __forceinline__ F2 fma(F2 a, F2 b, F2 c) { return F2(__ffma2_rn(a.v, b.v, c.v)); }
+__device__ __forceinline__ float fma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fma(double a, double b, double c) { return ::fma(a, b, c); }
+
+// Value type of a stage kernel that carries PR lines per thread.
+template <typename T, int PR>
+struct PairOf {
+    using type = T;
+};
+template <>
+struct PairOf<float, 2> {
+    using type = F2;
+};
+
+// PR consecutive values of U (one per line of a pair), as one load or store.
+template <typename U, int PR>
+struct Lanes {
+    using type = U;
+};
+template <>
+struct Lanes<float, 2> {
+    using type = float2;
+};
+template <>
+struct Lanes<double, 2> {
+    using type = double2;
+};
+
+// Launch bounds of the stage kernels: up to 512 threads with the registers
+// of one such CTA per SM (128 per thread), so that no configuration spills
+// its chunk; a paired kernel with long chunks keeps twice the values per
+// thread and is limited to 256 threads.
+template <typename T, int L, int PR>
+constexpr int kStageThreads = PR == 2 && L == kChunkLong<T> ? 256 : 512;
+
 // RHS scalars of a stencil (the operator's, times 1 + rho^2).
 template <typename T>
 struct Coef {
@@ -60,16 +112,29 @@ struct Coef {
 template <int KIND, typename T>
 __device__ __forceinline__ T stencil_at(const T *v, const Coef<T> &k)
 {
-    // v[m] = u_{i-4+m}
-    if constexpr (KIND == DER) return k.a * (v[5] - v[3]) + k.b * (v[6] - v[2]);
+    // v[m] = u_{i-4+m}.  The packed type needs its fused multiply-adds
+    // spelled out; the scalar types leave contraction to the compiler.
+    if constexpr (!std::is_same<T, F2>::value) {
+        if constexpr (KIND == DER) return k.a * (v[5] - v[3]) + k.b * (v[6] - v[2]);
+        if constexpr (KIND == DER2)
+            return k.a * ((v[5] - v[4]) - (v[4] - v[3])) + k.b * ((v[6] - v[4]) - (v[4] - v[2]));
+        if constexpr (KIND == DERVP) return k.a * (v[5] - v[4]) + k.b * (v[6] - v[3]);
+        if constexpr (KIND == DERPV) return k.a * (v[4] - v[3]) + k.b * (v[5] - v[2]);
+        if constexpr (KIND == INTVP)
+            return k.a * (v[5] + v[4]) + k.b * (v[6] + v[3]) + k.c * (v[7] + v[2]) + k.d * (v[8] + v[1]);
+        if constexpr (KIND == INTPV)
+            return k.a * (v[4] + v[3]) + k.b * (v[5] + v[2]) + k.c * (v[6] + v[1]) + k.d * (v[7] + v[0]);
+        return v[4];
+    }
+    if constexpr (KIND == DER) return fma(k.a, v[5] - v[3], k.b * (v[6] - v[2]));
     if constexpr (KIND == DER2)
-        return k.a * ((v[5] - v[4]) - (v[4] - v[3])) + k.b * ((v[6] - v[4]) - (v[4] - v[2]));
-    if constexpr (KIND == DERVP) return k.a * (v[5] - v[4]) + k.b * (v[6] - v[3]);
-    if constexpr (KIND == DERPV) return k.a * (v[4] - v[3]) + k.b * (v[5] - v[2]);
+        return fma(k.a, (v[5] - v[4]) - (v[4] - v[3]), k.b * ((v[6] - v[4]) - (v[4] - v[2])));
+    if constexpr (KIND == DERVP) return fma(k.a, v[5] - v[4], k.b * (v[6] - v[3]));
+    if constexpr (KIND == DERPV) return fma(k.a, v[4] - v[3], k.b * (v[5] - v[2]));
     if constexpr (KIND == INTVP)
-        return k.a * (v[5] + v[4]) + k.b * (v[6] + v[3]) + k.c * (v[7] + v[2]) + k.d * (v[8] + v[1]);
+        return fma(k.a, v[5] + v[4], fma(k.b, v[6] + v[3], fma(k.c, v[7] + v[2], k.d * (v[8] + v[1]))));
     if constexpr (KIND == INTPV)
-        return k.a * (v[4] + v[3]) + k.b * (v[5] + v[2]) + k.c * (v[6] + v[1]) + k.d * (v[7] + v[0]);
+        return fma(k.a, v[4] + v[3], fma(k.b, v[5] + v[2], fma(k.c, v[6] + v[1], k.d * (v[7] + v[0]))));
     return v[4];
 }
 
@@ -81,11 +146,11 @@ __device__ __forceinline__ void chunk_stencil(const T (&w)[N + 8], T (&r)[L], co
     for (int j = 0; j < N; ++j) r[OFF + j] = stencil_at<KIND>(w + j, k);
 }
 
-template <typename T, int N, int L, int OFF>
+template <typename T, int N, int L, int OFF, typename S>
 __device__ __forceinline__ void chunk_stencil_kind(int kind, const T (&w)[N + 8], T (&r)[L],
-                                                   const LineOp<T> &op)
+                                                   const LineOp<S> &op)
 {
-    const Coef<T> k{op.ca, op.cb, op.cc, op.cd};
+    const Coef<T> k{T(op.ca), T(op.cb), T(op.cc), T(op.cd)};
     switch (kind) {
     case DER: chunk_stencil<DER, T, N, L, OFF>(w, r, k); break;
     case DER2: chunk_stencil<DER2, T, N, L, OFF>(w, r, k); break;
@@ -100,8 +165,8 @@ __device__ __forceinline__ void chunk_stencil_kind(int kind, const T (&w)[N + 8]
 // The explicit right-hand side of a whole chunk, in P parts of L/P points,
 // each from its own window of L/P + 8 staged values, so that only one part's
 // window is live next to r.  load(w, J0) fills w[m] = u_{cs+J0-4+m}.
-template <typename T, int L, int P, int I = 0, typename Load>
-__device__ __forceinline__ void chunk_rhs(int kind, const Load &load, T (&r)[L], const LineOp<T> &op)
+template <typename T, int L, int P, int I = 0, typename Load, typename S>
+__device__ __forceinline__ void chunk_rhs(int kind, const Load &load, T (&r)[L], const LineOp<S> &op)
 {
     if constexpr (I < P) {
         constexpr int N = L / P;
@@ -271,16 +336,21 @@ struct Vec4<double> {
     static constexpr int N = 2;
     using type = double2;
 };
+template <>
+struct Vec4<F2> {
+    static constexpr int N = 2;
+    using type = float4;
+};
 
 // Shared-memory copy of the carry responses of a stage's operators, laid
 // out [operator][4][L] (see StageOp::resp), made once per CTA.
-template <typename T, int L>
-__device__ __forceinline__ void load_resp(const StageProgram<T> &prog, T *dst)
+template <typename V, int L, typename S>
+__device__ __forceinline__ void load_resp(const StageProgram<S> &prog, V *dst)
 {
     const int total = prog.nops * 4 * L;
     for (int i = threadIdx.x; i < total; i += blockDim.x) {
         const int k = i / (4 * L), rem = i - k * 4 * L, a = rem / L, j = rem - a * L;
-        dst[i] = prog.ops[k].resp[a][j];
+        dst[i] = V(prog.ops[k].resp[a][j]);
     }
 }
 
@@ -295,16 +365,16 @@ __device__ __forceinline__ void load_resp(const StageProgram<T> &prog, T *dst)
 // or resp[2..3] for a short last chunk) come from this operator's block of
 // the shared-memory copy as 16-byte vectors, so each fix is one fused
 // multiply-add per carry and half a load per point.
-template <typename T, int L, typename Load>
-__device__ __forceinline__ void chunk_solve_resp(const StageOp<T> &so, const T *resp, const Load &load,
+template <typename T, int L, typename Load, typename S>
+__device__ __forceinline__ void chunk_solve_resp(const StageOp<S> &so, const T *resp, const Load &load,
                                                  T (&r)[L], const ChunkScratch<T> &sc, int W, int l, int c,
                                                  int C, int nv, int q)
 {
-    constexpr int ti = L == kChunkLong<T> ? 0 : 1;
+    constexpr int ti = L == kChunkLong<S> ? 0 : 1;
     // operator fields into registers once (the parameters are read through
     // a generic pointer, and would be read again after every barrier)
-    const LineOp<T> &op = so.op;
-    const T rho = op.rho, mf = op.mfull[ti], ml = op.mlast[ti], wrap = op.wrap;
+    const LineOp<S> &op = so.op;
+    const T rho = T(op.rho), mf = T(op.mfull[ti]), ml = T(op.mlast[ti]), wrap = T(op.wrap);
     const int K = op.depth[ti];
     chunk_rhs<T, L, 2>(so.kind, load, r, op);
     // local forward sweep; the chunk's end value goes straight to shared
@@ -364,8 +434,8 @@ __device__ __forceinline__ ChunkScratch<T> carve_scratch(unsigned char *base, in
 }
 
 // acc (+)= m * r, with m = 1 or the staged tile value at the point.
-template <typename T, int L, typename TileAt>
-__device__ __forceinline__ void accumulate(const StageOp<T> &so, T (&acc)[L], const T (&r)[L],
+template <typename T, int L, typename S, typename TileAt>
+__device__ __forceinline__ void accumulate(const StageOp<S> &so, T (&acc)[L], const T (&r)[L],
                                            int nv, const TileAt &tile_at)
 {
     if (so.mul_tile < 0) {
@@ -418,11 +488,14 @@ struct FlushArgs {
 // block (base, base2) is issued before its stores.  base and base2 are often
 // the output arrays themselves (du += ..., u = u + dt du in place), so a load
 // placed after a store could not be moved ahead of it, and each point would
-// wait for memory in turn.
-template <typename T, typename U, int L>
-__device__ __forceinline__ void flush_yz_blocked(const FlushArgs<T> &fa, const T (&res)[L], size_t obase,
+// wait for memory in turn.  V holds PR x-adjacent lines (PR = 1 or 2), moved
+// as one PR-wide load or store of U.
+template <typename T, typename V, typename U, int L>
+__device__ __forceinline__ void flush_yz_blocked(const FlushArgs<T> &fa, const V (&res)[L], size_t obase,
                                                  size_t ostride, int nv)
 {
+    constexpr int PR = sizeof(V) / sizeof(T);
+    using UP = typename Lanes<U, PR>::type;
     constexpr int B = L < 8 ? L : 8;
     const U *base = static_cast<const U *>(fa.base);
     const U *base2 = static_cast<const U *>(fa.base2);
@@ -431,77 +504,159 @@ __device__ __forceinline__ void flush_yz_blocked(const FlushArgs<T> &fa, const T
     const U sign = (U)fa.sign, scale2 = (U)fa.scale2;
 #pragma unroll
     for (int j0 = 0; j0 < L; j0 += B) {
-        U bv[B], b2v[B];
+        UP bv[B], b2v[B];
 #pragma unroll
         for (int i = 0; i < B; ++i) {
             const size_t p = obase + (size_t)(j0 + i) * ostride;
             const bool in = j0 + i < nv;
-            bv[i] = base && in ? base[p] : U(0);
+            bv[i] = base && in ? *reinterpret_cast<const UP *>(base + p) : UP{};
             if constexpr (std::is_same<T, U>::value) {
-                if (fa.b2s) b2v[i] = fa.b2s[(j0 + i) * fa.b2step];
-                else b2v[i] = base2 && in ? base2[p] : U(0);
+                if (fa.b2s) b2v[i] = *reinterpret_cast<const UP *>(fa.b2s + (j0 + i) * fa.b2step);
+                else b2v[i] = base2 && in ? *reinterpret_cast<const UP *>(base2 + p) : UP{};
             } else {
-                b2v[i] = base2 && in ? base2[p] : U(0);
+                b2v[i] = base2 && in ? *reinterpret_cast<const UP *>(base2 + p) : UP{};
             }
         }
 #pragma unroll
         for (int i = 0; i < B; ++i) {
             if (j0 + i < nv) {
                 const size_t p = obase + (size_t)(j0 + i) * ostride;
-                const U v = bv[i] + sign * (U)res[j0 + i];
-                out[p] = v;
-                if (out2) out2[p] = b2v[i] + scale2 * v;
+                const T *rv = reinterpret_cast<const T *>(&res[j0 + i]);
+                const U *bl = reinterpret_cast<const U *>(&bv[i]);
+                const U *b2l = reinterpret_cast<const U *>(&b2v[i]);
+                UP o;
+                U *ol = reinterpret_cast<U *>(&o);
+#pragma unroll
+                for (int e = 0; e < PR; ++e) ol[e] = bl[e] + sign * (U)rv[e];
+                *reinterpret_cast<UP *>(out + p) = o;
+                if (out2) {
+                    UP o2;
+                    U *o2l = reinterpret_cast<U *>(&o2);
+#pragma unroll
+                    for (int e = 0; e < PR; ++e) o2l[e] = b2l[e] + scale2 * ol[e];
+                    *reinterpret_cast<UP *>(out2 + p) = o2;
+                }
             }
         }
     }
 }
 
-// Writes one thread's solved chunk of a y/z line (points j < nv), each point
-// ostride elements after the previous one.
-template <typename T, int L>
-__device__ __forceinline__ void flush_yz(const FlushArgs<T> &fa, const T (&res)[L], size_t obase,
+// The general flush of a whole chunk (nv == L) in the forms the Euler-step
+// stages use, with every test hoisted out of the point loop and the
+// addresses stepped by pointer increments:
+//   HB:  out = base + sign * res (else out = sign * res)
+//   B2T: out2 = base2 + scale2 * out, base2 read from the staged tile b2s
+// U = double writes FP64 outputs.
+template <typename T, typename V, typename U, int L, bool HB, bool B2T>
+__device__ __forceinline__ void flush_yz_whole(const FlushArgs<T> &fa, const V (&res)[L], size_t obase,
+                                               size_t ostride)
+{
+    constexpr int PR = sizeof(V) / sizeof(T);
+    using UP = typename Lanes<U, PR>::type;
+    constexpr int B = L < 8 ? L : 8;
+    const U *bp = static_cast<const U *>(fa.base) + obase;
+    U *op = static_cast<U *>(fa.out) + obase;
+    U *op2 = static_cast<U *>(fa.out2) + obase;
+    const T *b2p = fa.b2s;
+    const int b2step = fa.b2step;
+    const U sign = (U)fa.sign, scale2 = (U)fa.scale2;
+#pragma unroll
+    for (int j0 = 0; j0 < L; j0 += B) {
+        UP bv[B];
+        if constexpr (HB) {
+#pragma unroll
+            for (int i = 0; i < B; ++i) bv[i] = *reinterpret_cast<const UP *>(bp + (size_t)i * ostride);
+            bp += (size_t)B * ostride;
+        }
+#pragma unroll
+        for (int i = 0; i < B; ++i) {
+            const T *rv = reinterpret_cast<const T *>(&res[j0 + i]);
+            UP o;
+            U *ol = reinterpret_cast<U *>(&o);
+            if constexpr (HB) {
+                const U *bl = reinterpret_cast<const U *>(&bv[i]);
+#pragma unroll
+                for (int e = 0; e < PR; ++e) ol[e] = bl[e] + sign * (U)rv[e];
+            } else {
+#pragma unroll
+                for (int e = 0; e < PR; ++e) ol[e] = sign * (U)rv[e];
+            }
+            *reinterpret_cast<UP *>(op + (size_t)i * ostride) = o;
+            if constexpr (B2T) {
+                const V b2 = *reinterpret_cast<const V *>(b2p + (j0 + i) * b2step);
+                const T *b2l = reinterpret_cast<const T *>(&b2);
+                UP o2;
+                U *o2l = reinterpret_cast<U *>(&o2);
+#pragma unroll
+                for (int e = 0; e < PR; ++e) o2l[e] = (U)b2l[e] + scale2 * ol[e];
+                *reinterpret_cast<UP *>(op2 + (size_t)i * ostride) = o2;
+            }
+        }
+        op += (size_t)B * ostride;
+        if constexpr (B2T) op2 += (size_t)B * ostride;
+    }
+}
+
+// Writes one thread's solved chunk of a y/z line, or of PR x-adjacent lines
+// (points j < nv), each point ostride elements after the previous one.
+// GENERAL = false: the program's flushes are all plain (out = res), and the
+// other forms are not compiled into the kernel.
+template <typename T, typename V, int L, bool GENERAL>
+__device__ __forceinline__ void flush_yz(const FlushArgs<T> &fa, const V (&res)[L], size_t obase,
                                          size_t ostride, int nv)
 {
-    if (fa.plain) {
+    if (GENERAL && nv == L && !fa.plain) {
+        // du += ...; du += ... with u = u + dt du; pp3 = ... in FP64
+        const bool hb = fa.base != nullptr, o2 = fa.out2 != nullptr;
+        if (!fa.f64 && hb && !o2) return flush_yz_whole<T, V, T, L, true, false>(fa, res, obase, ostride);
+        if (!fa.f64 && hb && o2 && fa.b2s)
+            return flush_yz_whole<T, V, T, L, true, true>(fa, res, obase, ostride);
+        if (fa.f64 && !hb && !o2) return flush_yz_whole<T, V, double, L, false, false>(fa, res, obase, ostride);
+    }
+    if (!GENERAL || fa.plain) {
         T *dst = static_cast<T *>(fa.out) + obase;
         if (nv == L) {  // every chunk but a short last one: no per-point test
 #pragma unroll
             for (int j = 0; j < L; ++j) {
-                *dst = res[j];
+                *reinterpret_cast<V *>(dst) = res[j];
                 dst += ostride;
             }
         } else {
 #pragma unroll
             for (int j = 0; j < L; ++j) {
-                if (j < nv) *dst = res[j];
+                if (j < nv) *reinterpret_cast<V *>(dst) = res[j];
                 dst += ostride;
             }
         }
-    } else if (fa.f64) {
-        flush_yz_blocked<T, double, L>(fa, res, obase, ostride, nv);
-    } else {
-        flush_yz_blocked<T, T, L>(fa, res, obase, ostride, nv);
+    } else if constexpr (GENERAL) {
+        if (fa.f64) flush_yz_blocked<T, V, double, L>(fa, res, obase, ostride, nv);
+        else flush_yz_blocked<T, V, T, L>(fa, res, obase, ostride, nv);
     }
 }
 
 // PERSIST: a CTA loops over tiles with two staging slots, issuing the loads
-// of tile k+1 before computing tile k; otherwise one CTA per tile.
-template <typename T, int W, int L, bool ACC, bool PERSIST>
-__global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
+// of tile k+1 before computing tile k; otherwise one CTA per tile.  PR = 2
+// (FP32 only): each thread carries the same chunk of two x-adjacent lines in
+// packed registers, so every arithmetic instruction, shared-memory load and
+// global store serves two lines (x extents must then be even).
+template <typename T, int W, int L, bool ACC, bool PERSIST, int PR = 1>
+__global__ void __launch_bounds__(kStageThreads<T, L, PR>, 1)
     ls_stage_yz(const __grid_constant__ StageMaps maps, const __grid_constant__ StageProgram<T> prog, int nx,
                 int ny, int dir, int box_n, int nbox, size_t tile_bytes, long ntiles, int *err)
 {
+    using V = typename PairOf<T, PR>::type;
+    constexpr int WP = W / PR;  // threads across the tile's lines
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ uint64_t bars[2];
     const int n = prog.ops[0].op.n;
-    const int C = blockDim.x / W;
+    const int C = blockDim.x / WP;
     const int t = threadIdx.x;
-    const int l = t % W, c = t / W;
+    const int l = t % WP, c = t / WP;
     const int tiles_x = (nx + W - 1) / W;
     const size_t slot_bytes = (size_t)prog.ntiles * tile_bytes;
-    T *resp_s = reinterpret_cast<T *>(smem_raw + (PERSIST ? 2 : 1) * slot_bytes +
+    V *resp_s = reinterpret_cast<V *>(smem_raw + (PERSIST ? 2 : 1) * slot_bytes +
                                       (((size_t)2 * C * W * sizeof(T) + 15) & ~(size_t)15));
-    load_resp<T, L>(prog, resp_s);
+    load_resp<V, L>(prog, resp_s);
     if (t == 0) {
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
@@ -531,7 +686,7 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
             }
         }
     };
-    const ChunkScratch<T> sc = carve_scratch<T>(smem_raw + (PERSIST ? 2 : 1) * slot_bytes, C, W);
+    const ChunkScratch<V> sc = carve_scratch<V>(smem_raw + (PERSIST ? 2 : 1) * slot_bytes, C, WP);
     const int cs = c * L;
     const int nv = min(L, n - cs);
     const size_t ostride = dir == DY ? (size_t)nx : (size_t)nx * ny;
@@ -558,38 +713,39 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
         __syncthreads();
         // window of this chunk: rows kHalo + cs - 4 ...
         auto col = [&](int ti) {
-            return reinterpret_cast<const T *>(base + ti * tile_bytes) + (kHalo + cs - 4) * W + l;
+            return reinterpret_cast<const T *>(base + ti * tile_bytes) + (kHalo + cs - 4) * W + PR * l;
         };
-        auto tile_at = [&](int ti, int j) { return col(ti)[(4 + j) * W]; };
+        auto at = [](const T *p) { return *reinterpret_cast<const V *>(p); };
+        auto tile_at = [&](int ti, int j) { return at(col(ti) + (4 + j) * W); };
         auto flush_args = [&](const StageOp<T> &so) {
             return FlushArgs<T>(so, so.base2_tile >= 0 ? col(so.base2_tile) + 4 * W : nullptr, W);
         };
-        const bool live = x0 + l < nx;
-        const size_t obase = (size_t)(x0 + l) + (dir == DY ? (size_t)nx * ny * o : (size_t)nx * o) +
+        const bool live = x0 + PR * l < nx;
+        const size_t obase = (size_t)(x0 + PR * l) + (dir == DY ? (size_t)nx * ny * o : (size_t)nx * o) +
                              (size_t)cs * ostride;
-        T r[L];
-        T acc[ACC ? L : 1];
+        V r[L];
+        V acc[ACC ? L : 1];
         for (int k = 0; k < prog.nops; ++k) {
             const StageOp<T> &so = prog.ops[k];
             const T *ca = col(so.src_a);
             const T *cb = so.src_b >= 0 ? col(so.src_b) : nullptr;
             auto load = [&](auto &w, auto j0) {
                 constexpr int J0 = decltype(j0)::value;
-                constexpr int NW = sizeof(w) / sizeof(T);
+                constexpr int NW = sizeof(w) / sizeof(V);
                 if (cb) {
 #pragma unroll
-                    for (int j = 0; j < NW; ++j) w[j] = ca[(J0 + j) * W] * cb[(J0 + j) * W];
+                    for (int j = 0; j < NW; ++j) w[j] = at(ca + (J0 + j) * W) * at(cb + (J0 + j) * W);
                 } else {
 #pragma unroll
-                    for (int j = 0; j < NW; ++j) w[j] = ca[(J0 + j) * W];
+                    for (int j = 0; j < NW; ++j) w[j] = at(ca + (J0 + j) * W);
                 }
             };
-            chunk_solve_resp<T, L>(so, resp_s + k * 4 * L, load, r, sc, W, l, c, C, nv, c * W + l);
+            chunk_solve_resp<V, L>(so, resp_s + k * 4 * L, load, r, sc, WP, l, c, C, nv, c * WP + l);
             if constexpr (ACC) {
-                accumulate<T, L>(so, acc, r, nv, tile_at);
-                if (so.flush && live) flush_yz<T, L>(flush_args(so), acc, obase, ostride, nv);
+                accumulate<V, L>(so, acc, r, nv, tile_at);
+                if (so.flush && live) flush_yz<T, V, L, true>(flush_args(so), acc, obase, ostride, nv);
             } else {
-                if (so.flush && live) flush_yz<T, L>(flush_args(so), r, obase, ostride, nv);
+                if (so.flush && live) flush_yz<T, V, L, false>(flush_args(so), r, obase, ostride, nv);
             }
         }
         if (PERSIST) __syncthreads();  // the slot is refilled two tiles later
@@ -675,27 +831,90 @@ __device__ __forceinline__ void flush_x(const FlushArgs<T> &fa, const T (&res)[L
     else flush_x_blocked<T, T, L>(fa, res, p0, nv);
 }
 
-// Flush of one operator for a tile of x lines.  Plain outputs go through
-// shared memory: each thread writes its chunk into the tile's staging rows
-// (odd 16-byte granules per row, so the vector stores do not conflict) and
-// one thread per line sends the whole row with a bulk copy, so every line
-// leaves as one contiguous write.  Other flushes store directly.  The
-// caller waits for the copies' reads before the staging rows are reused.
-// fa.plain is the same for the whole CTA, so the barrier is uniform.
-template <typename T, int L>
+// The general flush of a tile of x lines from its staging rows: the CTA's
+// threads sweep the rows as 16-byte vectors, consecutive threads on
+// consecutive vectors of a row, so the loads of base and base2 and the
+// stores of out and out2 are coalesced across each warp (each thread's own
+// chunk would touch a different line per vector).  U = double writes FP64
+// outputs.
+template <typename T, typename U>
+__device__ __forceinline__ void flush_x_rows(const FlushArgs<T> &fa, const T *out_s, long l0, int rows,
+                                             int pitch, int n)
+{
+    using VT = typename Vec4<T>::type;
+    constexpr int V = Vec4<T>::N;
+    using UV = typename Vec4<U>::type;
+    constexpr int NU = V / Vec4<U>::N;  // U vectors per T vector
+    const U *base = static_cast<const U *>(fa.base);
+    const U *base2 = static_cast<const U *>(fa.base2);
+    U *out = static_cast<U *>(fa.out);
+    U *out2 = static_cast<U *>(fa.out2);
+    const U sign = (U)fa.sign, scale2 = (U)fa.scale2;
+    auto one = [&](int rr, int q) {
+        const size_t g = (size_t)(l0 + rr) * n + (size_t)q * V;
+        const VT v = *reinterpret_cast<const VT *>(out_s + (size_t)rr * pitch + (size_t)q * V);
+        const T *vl = reinterpret_cast<const T *>(&v);
+        UV b[NU], b2[NU];
+#pragma unroll
+        for (int u = 0; u < NU; ++u) {
+            b[u] = base ? *reinterpret_cast<const UV *>(base + g + u * (V / NU)) : UV{};
+            b2[u] = base2 ? *reinterpret_cast<const UV *>(base2 + g + u * (V / NU)) : UV{};
+        }
+        const U *bl = reinterpret_cast<const U *>(b);
+        const U *b2l = reinterpret_cast<const U *>(b2);
+        UV o[NU], o2[NU];
+        U *ol = reinterpret_cast<U *>(o);
+        U *o2l = reinterpret_cast<U *>(o2);
+#pragma unroll
+        for (int e = 0; e < V; ++e) {
+            ol[e] = bl[e] + sign * (U)vl[e];
+            o2l[e] = b2l[e] + scale2 * ol[e];
+        }
+#pragma unroll
+        for (int u = 0; u < NU; ++u) {
+            *reinterpret_cast<UV *>(out + g + u * (V / NU)) = o[u];
+            if (out2) *reinterpret_cast<UV *>(out2 + g + u * (V / NU)) = o2[u];
+        }
+    };
+    const int per_row = n / V, nt = blockDim.x, t = threadIdx.x;
+    if (nt >= per_row) {
+        // nt / per_row rows at a time
+        const int G = nt / per_row, r0 = t / per_row, q = t - r0 * per_row;
+        if (r0 < G)
+            for (int rr = r0; rr < rows; rr += G) one(rr, q);
+    } else {
+        for (int rr = 0; rr < rows; ++rr)
+#pragma unroll 2
+            for (int q = t; q < per_row; q += nt) one(rr, q);
+    }
+}
+
+// Flush of one operator for a tile of x lines.  Every thread first writes
+// its chunk into the tile's staging rows (odd 16-byte granules per row, so
+// the vector stores do not conflict).  A plain output then leaves as one
+// bulk copy per row; any other (base, base2, FP64) is written by the whole
+// CTA row by row (flush_x_rows).  A base2 that is a staged input (read from
+// the tile, per thread) keeps the direct per-chunk flush.  The caller waits
+// for the copies' reads before the staging rows are reused.  fa.plain and
+// fa.b2s are the same for the whole CTA, so the barrier is uniform.
+// GENERAL = false: the program's flushes are all plain, and the other forms
+// are not compiled into the kernel.
+template <typename T, int L, bool GENERAL>
 __device__ __forceinline__ void flush_x_staged(const FlushArgs<T> &fa, const T (&res)[L], T *out_s, int l,
                                                long l0, int rows, int pitch, int n, int cs, int nv)
 {
     using VT = typename Vec4<T>::type;
     constexpr int V = Vec4<T>::N;
-    if (!fa.plain) {
-        if (l < rows) flush_x<T, L>(fa, res, (size_t)(l0 + l) * n + cs, nv);
-        return;
+    if constexpr (GENERAL) {
+        if (fa.b2s) {
+            if (l < rows) flush_x<T, L>(fa, res, (size_t)(l0 + l) * n + cs, nv);
+            return;
+        }
     }
     if (l < rows) {
         // the staging row is the tile's own: a short last chunk may write
         // past the line's end there (room for the last window), and the
-        // row copy sends only the line's n points
+        // row pass sends only the line's n points
         T *dst = out_s + (size_t)l * pitch + cs;
 #pragma unroll
         for (int j = 0; j < L; j += V) {
@@ -708,6 +927,13 @@ __device__ __forceinline__ void flush_x_staged(const FlushArgs<T> &fa, const T (
     }
     fence_proxy_async_smem();
     __syncthreads();
+    if constexpr (GENERAL) {
+        if (!fa.plain) {
+            if (fa.f64) flush_x_rows<T, double>(fa, out_s, l0, rows, pitch, n);
+            else flush_x_rows<T, T>(fa, out_s, l0, rows, pitch, n);
+            return;
+        }
+    }
     const int t = threadIdx.x;
     if (t < rows) {
         bulk_store(static_cast<T *>(fa.out) + (size_t)(l0 + t) * n, out_s + (size_t)t * pitch,
@@ -738,7 +964,7 @@ __device__ __forceinline__ void fill_halos_x(unsigned char *base, size_t tile_by
 }
 
 template <typename T, int W, int L, bool ACC, bool PERSIST>
-__global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
+__global__ void __launch_bounds__(512, 1)
     ls_stage_x(const __grid_constant__ StageProgram<T> prog, long nlines, int pitch, size_t tile_bytes,
                long ntiles, int *err)
 {
@@ -848,9 +1074,9 @@ __global__ void __launch_bounds__(512, (L == kChunkShort<T> ? 2 : 1))
             chunk_solve_resp<T, L>(so, resp_s + k * 4 * L, load, r, sc, W, l, c, C, nv, c * W + l);
             if constexpr (ACC) {
                 accumulate<T, L>(so, acc, r, nv, tile_at);
-                if (so.flush) flush_x_staged<T, L>(flush_args(so), acc, out_s, l, l0, rows, pitch, n, cs, nv);
+                if (so.flush) flush_x_staged<T, L, true>(flush_args(so), acc, out_s, l, l0, rows, pitch, n, cs, nv);
             } else {
-                if (so.flush) flush_x_staged<T, L>(flush_args(so), r, out_s, l, l0, rows, pitch, n, cs, nv);
+                if (so.flush) flush_x_staged<T, L, false>(flush_args(so), r, out_s, l, l0, rows, pitch, n, cs, nv);
             }
         }
         if (PERSIST) __syncthreads();  // the slot is refilled two tiles later
@@ -881,6 +1107,7 @@ struct StageOpView {
 static size_t scratch_bytes(int C, int W, size_t es) { return ((size_t)2 * C * W * es + 15) & ~(size_t)15; }
 
 static bool al16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+static bool al8(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 7) == 0; }
 
 static bool plain(const StageOpView &v) { return v.flush && !v.accumulate && v.mul_tile < 0; }
 
@@ -924,105 +1151,124 @@ static void fill_resp(StageProgram<T> &p, int L, int n)
     }
 }
 
-template <typename T, int W, int L, bool PERSIST>
+// PR = 2: the paired y/z kernel (FP32 only).
+template <typename T, int W, int L, bool PERSIST, int PR = 1>
 static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog_in, int dir, int nx, int ny,
                             int nz)
 {
-    StageProgram<T> prog = prog_in;
-    fill_resp(prog, L, prog.ops[0].op.n);
-    // base2 that is a staged input comes from shared memory; T-typed bases
-    // are prefetched into L2 with the tile's inputs
-    for (int k = 0; k < prog.nops; ++k) {
-        StageOp<T> &so = prog.ops[k];
-        so.base2_tile = -1;
-        for (int ti = 0; ti < prog.ntiles; ++ti)
-            if (!so.out_f64 && so.base2 && so.base2 == prog.in[ti]) so.base2_tile = (short)ti;
-        so.prefetch_base = (so.flush && so.base && !so.out_f64) ? 1 : 0;
-    }
-    prog.prefetch_mask = 0;
-    for (int k = 0; k < prog.nops; ++k)
-        if (prog.ops[k].prefetch_base) prog.prefetch_mask |= 1 << k;
-    bool acc = false;
-    for (int k = 0; k < prog.nops; ++k)
-        acc = acc || !plain(StageOpView{prog.ops[k].flush, prog.ops[k].accumulate, prog.ops[k].mul_tile});
-    const int n = prog.ops[0].op.n;
-    for (int k = 0; k < prog.nops; ++k)
-        if (!prog.ops[k].op.circ || prog.ops[k].op.n != n) return X3D_EUNSUPPORTED;
-    const size_t es = sizeof(T);
-    const int C = (n + L - 1) / L;
-    const int threads = C * W;
-    if (threads > 512 || threads % 32) return X3D_EUNSUPPORTED;
-    const size_t resp_bytes = (size_t)prog.nops * 4 * L * es;
-    for (int ti = 0; ti < prog.ntiles; ++ti)
-        if (!al16(prog.in[ti])) return X3D_EUNSUPPORTED;
-    cudaStream_t st = ctx->stream;
-    if (dir == DX) {
-        constexpr int V = Vec4<T>::N;
-        if (n % V) return X3D_EUNSUPPORTED;
+    if constexpr (PR == 2 && !std::is_same<T, float>::value) {
+        return X3D_EUNSUPPORTED;
+    } else {
+        StageProgram<T> prog = prog_in;
+        fill_resp(prog, L, prog.ops[0].op.n);
+        // base2 that is a staged input comes from shared memory; T-typed bases
+        // are prefetched into L2 with the tile's inputs
+        for (int k = 0; k < prog.nops; ++k) {
+            StageOp<T> &so = prog.ops[k];
+            so.base2_tile = -1;
+            for (int ti = 0; ti < prog.ntiles; ++ti)
+                if (!so.out_f64 && so.base2 && so.base2 == prog.in[ti]) so.base2_tile = (short)ti;
+            so.prefetch_base = (so.flush && so.base && !so.out_f64) ? 1 : 0;
+        }
+        prog.prefetch_mask = 0;
+        for (int k = 0; k < prog.nops; ++k)
+            if (prog.ops[k].prefetch_base) prog.prefetch_mask |= 1 << k;
+        // the ACC kernels carry the accumulator and every flush form; the
+        // others only plain operators (out = the solve)
+        bool acc = false;
         for (int k = 0; k < prog.nops; ++k) {
             const StageOp<T> &so = prog.ops[k];
-            if (so.flush && (!al16(so.out) || !al16(so.base) || !al16(so.out2) || !al16(so.base2)))
-                return X3D_EUNSUPPORTED;
+            acc = acc || !plain(StageOpView{so.flush, so.accumulate, so.mul_tile}) ||
+                  (so.flush && (so.base || so.out2 || so.out_f64 || so.sign != 1.0));
         }
-        // row: kHalo halo elements, the line, and room for the last chunk's window
-        int pitch = C * L + 2 * kHalo;
-        while (((size_t)pitch * es / 16) % 2 == 0) pitch += V;
-        const size_t tile = ((size_t)W * pitch * es + 127) & ~(size_t)127;
-        // + staging rows for plain outputs (W rows of the same pitch, 128-byte aligned)
-        const size_t smem = (((PERSIST ? 2 : 1) * prog.ntiles * tile + scratch_bytes(C, W, es) + resp_bytes + 127) &
-                             ~(size_t)127) +
-                            (size_t)W * pitch * es;
+        const int n = prog.ops[0].op.n;
+        for (int k = 0; k < prog.nops; ++k)
+            if (!prog.ops[k].op.circ || prog.ops[k].op.n != n) return X3D_EUNSUPPORTED;
+        const size_t es = sizeof(T);
+        const int C = (n + L - 1) / L;
+        const int threads = C * W / PR;
+        if (threads > kStageThreads<T, L, PR> || threads % 32) return X3D_EUNSUPPORTED;
+        const size_t resp_bytes = (size_t)prog.nops * 4 * L * es * PR;
+        for (int ti = 0; ti < prog.ntiles; ++ti)
+            if (!al16(prog.in[ti])) return X3D_EUNSUPPORTED;
+        cudaStream_t st = ctx->stream;
+        if constexpr (PR == 2) {
+            // paired y/z lines: even x extent, 8-byte aligned pair stores
+            if (dir == DX || nx % 2) return X3D_EUNSUPPORTED;
+            for (int k = 0; k < prog.nops; ++k) {
+                const StageOp<T> &so = prog.ops[k];
+                if (so.flush && (!al8(so.out) || !al8(so.base) || !al8(so.out2) || !al8(so.base2)))
+                    return X3D_EUNSUPPORTED;
+            }
+        } else if (dir == DX) {
+            constexpr int V = Vec4<T>::N;
+            if (n % V) return X3D_EUNSUPPORTED;
+            for (int k = 0; k < prog.nops; ++k) {
+                const StageOp<T> &so = prog.ops[k];
+                if (so.flush && (!al16(so.out) || !al16(so.base) || !al16(so.out2) || !al16(so.base2)))
+                    return X3D_EUNSUPPORTED;
+            }
+            // row: kHalo halo elements, the line, and room for the last chunk's window
+            int pitch = C * L + 2 * kHalo;
+            while (((size_t)pitch * es / 16) % 2 == 0) pitch += V;
+            const size_t tile = ((size_t)W * pitch * es + 127) & ~(size_t)127;
+            // + staging rows for plain outputs (W rows of the same pitch, 128-byte aligned)
+            const size_t smem = (((PERSIST ? 2 : 1) * prog.ntiles * tile + scratch_bytes(C, W, es) + resp_bytes + 127) &
+                                 ~(size_t)127) +
+                                (size_t)W * pitch * es;
+            if (smem + 1024 > ctx->smem_optin) return X3D_EUNSUPPORTED;
+            auto kern = acc ? ls_stage_x<T, W, L, true, PERSIST> : ls_stage_x<T, W, L, false, PERSIST>;
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            const long nlines = (long)ny * nz;
+            const long ntiles = (nlines + W - 1) / W;
+            const unsigned grid = PERSIST ? persistent_grid(ctx, kern, threads, smem, ntiles) : (unsigned)ntiles;
+            ++ctx->launches;
+            kern<<<grid, threads, smem, st>>>(prog, nlines, pitch, tile, ntiles, ctx->d_err);
+            return cuda_check(ctx, cudaGetLastError(), "ls_stage_x launch");
+        }
+        auto enc = encode_tiled();
+        if (!enc || ((size_t)nx * es) % 16) return X3D_EUNSUPPORTED;
+        const int nb = (n + 255) / 256;
+        int box_n = (n + nb - 1) / nb;
+        const int align_rows = (int)(128 / (W * es) > 0 ? 128 / (W * es) : 1);
+        box_n = (box_n + align_rows - 1) / align_rows * align_rows;
+        if (box_n > 256) return X3D_EUNSUPPORTED;
+        // rows: kHalo halo rows (kHalo * W * es is a multiple of 128 bytes, so the
+        // boxes land 128-byte aligned), the boxes, and room for the last window
+        const int rows = kHalo + std::max(nb * box_n, C * L + kHalo);
+        const size_t tile = ((size_t)rows * W * es + 127) & ~(size_t)127;
+        const size_t smem = (PERSIST ? 2 : 1) * prog.ntiles * tile + scratch_bytes(C, W, es) + resp_bytes;
         if (smem + 1024 > ctx->smem_optin) return X3D_EUNSUPPORTED;
-        auto kern = acc ? ls_stage_x<T, W, L, true, PERSIST> : ls_stage_x<T, W, L, false, PERSIST>;
+        StageMaps maps;
+        std::memset(&maps, 0, sizeof(maps));
+        auto encode = [&](CUtensorMap *m, const void *ptr) {
+            cuuint64_t gdim[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
+            cuuint64_t gstride[2] = {(cuuint64_t)nx * es, (cuuint64_t)nx * ny * es};
+            cuuint32_t box[3] = {(cuuint32_t)W, 1, 1};
+            box[dir == DY ? 1 : 2] = (cuuint32_t)box_n;
+            cuuint32_t estr[3] = {1, 1, 1};
+            return enc(m, sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+                       const_cast<void *>(ptr), gdim, gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                       CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+        };
+        for (int ti = 0; ti < prog.ntiles; ++ti)
+            if (!encode(&maps.m[ti], prog.in[ti])) return X3D_EUNSUPPORTED;
+        for (int k = 0; k < prog.nops; ++k)
+            if (prog.ops[k].prefetch_base && !encode(&maps.pm[k], prog.ops[k].base)) prog.ops[k].prefetch_base = 0;
+        prog.prefetch_mask = 0;
+        for (int k = 0; k < prog.nops; ++k)
+            if (prog.ops[k].prefetch_base) prog.prefetch_mask |= 1 << k;
+        auto kern = acc ? ls_stage_yz<T, W, L, true, PERSIST, PR> : ls_stage_yz<T, W, L, false, PERSIST, PR>;
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        const long nlines = (long)ny * nz;
-        const long ntiles = (nlines + W - 1) / W;
+        const long tiles_x = (nx + W - 1) / W;
+        const long ntiles = tiles_x * (dir == DY ? nz : ny);
         const unsigned grid = PERSIST ? persistent_grid(ctx, kern, threads, smem, ntiles) : (unsigned)ntiles;
         ++ctx->launches;
-        kern<<<grid, threads, smem, st>>>(prog, nlines, pitch, tile, ntiles, ctx->d_err);
-        return cuda_check(ctx, cudaGetLastError(), "ls_stage_x launch");
+        kern<<<grid, threads, smem, st>>>(maps, prog, nx, ny, dir, box_n, nb, tile, ntiles, ctx->d_err);
+        return cuda_check(ctx, cudaGetLastError(), "ls_stage_yz launch");
+
     }
-    auto enc = encode_tiled();
-    if (!enc || ((size_t)nx * es) % 16) return X3D_EUNSUPPORTED;
-    const int nb = (n + 255) / 256;
-    int box_n = (n + nb - 1) / nb;
-    const int align_rows = (int)(128 / (W * es) > 0 ? 128 / (W * es) : 1);
-    box_n = (box_n + align_rows - 1) / align_rows * align_rows;
-    if (box_n > 256) return X3D_EUNSUPPORTED;
-    // rows: kHalo halo rows (kHalo * W * es is a multiple of 128 bytes, so the
-    // boxes land 128-byte aligned), the boxes, and room for the last window
-    const int rows = kHalo + std::max(nb * box_n, C * L + kHalo);
-    const size_t tile = ((size_t)rows * W * es + 127) & ~(size_t)127;
-    const size_t smem = (PERSIST ? 2 : 1) * prog.ntiles * tile + scratch_bytes(C, W, es) + resp_bytes;
-    if (smem + 1024 > ctx->smem_optin) return X3D_EUNSUPPORTED;
-    StageMaps maps;
-    std::memset(&maps, 0, sizeof(maps));
-    auto encode = [&](CUtensorMap *m, const void *ptr) {
-        cuuint64_t gdim[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
-        cuuint64_t gstride[2] = {(cuuint64_t)nx * es, (cuuint64_t)nx * ny * es};
-        cuuint32_t box[3] = {(cuuint32_t)W, 1, 1};
-        box[dir == DY ? 1 : 2] = (cuuint32_t)box_n;
-        cuuint32_t estr[3] = {1, 1, 1};
-        return enc(m, sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
-                   const_cast<void *>(ptr), gdim, gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
-    };
-    for (int ti = 0; ti < prog.ntiles; ++ti)
-        if (!encode(&maps.m[ti], prog.in[ti])) return X3D_EUNSUPPORTED;
-    for (int k = 0; k < prog.nops; ++k)
-        if (prog.ops[k].prefetch_base && !encode(&maps.pm[k], prog.ops[k].base)) prog.ops[k].prefetch_base = 0;
-    prog.prefetch_mask = 0;
-    for (int k = 0; k < prog.nops; ++k)
-        if (prog.ops[k].prefetch_base) prog.prefetch_mask |= 1 << k;
-    auto kern = acc ? ls_stage_yz<T, W, L, true, PERSIST> : ls_stage_yz<T, W, L, false, PERSIST>;
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    const long tiles_x = (nx + W - 1) / W;
-    const long ntiles = tiles_x * (dir == DY ? nz : ny);
-    const unsigned grid = PERSIST ? persistent_grid(ctx, kern, threads, smem, ntiles) : (unsigned)ntiles;
-    ++ctx->launches;
-    kern<<<grid, threads, smem, st>>>(maps, prog, nx, ny, dir, box_n, nb, tile, ntiles, ctx->d_err);
-    return cuda_check(ctx, cudaGetLastError(), "ls_stage_yz launch");
 }
 
 template <typename T>
@@ -1047,6 +1293,11 @@ int launch_stage(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir, int nx, i
     case 9: return launch_stage_cfg<T, 8, Lbig, true>(ctx, prog, dir, nx, ny, nz);
     case 10: return launch_stage_cfg<T, 32, Lsmall, true>(ctx, prog, dir, nx, ny, nz);
     case 11: return launch_stage_cfg<T, 8, Lsmall, true>(ctx, prog, dir, nx, ny, nz);
+    // 12-15: y/z lines in packed pairs (FP32, even nx)
+    case 12: return launch_stage_cfg<T, 32, Lsmall, true, 2>(ctx, prog, dir, nx, ny, nz);
+    case 13: return launch_stage_cfg<T, 16, Lsmall, true, 2>(ctx, prog, dir, nx, ny, nz);
+    case 14: return launch_stage_cfg<T, 32, Lsmall, false, 2>(ctx, prog, dir, nx, ny, nz);
+    case 15: return launch_stage_cfg<T, 32, Lbig, true, 2>(ctx, prog, dir, nx, ny, nz);
     default: return X3D_EUNSUPPORTED;
     }
 }

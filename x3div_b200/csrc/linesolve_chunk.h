@@ -52,8 +52,9 @@ struct StageProgram {
     int prefetch_mask;  // bit k: operator k's base is prefetched (set by launch_stage)
 };
 
-// Number of (lines per CTA, chunk length) configurations launch_stage knows.
-constexpr int kChunkConfigs = 12;
+// Number of (lines per CTA, chunk length, persistence, lines per thread)
+// configurations launch_stage knows.
+constexpr int kChunkConfigs = 16;
 
 // Launches the chunked stage kernel with configuration cfg in
 // [0, kChunkConfigs).  Returns X3D_EUNSUPPORTED, launching nothing, when the
