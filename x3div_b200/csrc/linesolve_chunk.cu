@@ -461,7 +461,7 @@ __device__ __forceinline__ void accumulate(const StageOp<S> &so, T (&acc)[L], co
 // y- and z-lines.
 struct StageMaps {
     CUtensorMap m[kMaxStageTiles];  // inputs
-    CUtensorMap pm[kMaxStageOps];   // base arrays prefetched into L2 (ops with prefetch_base)
+    CUtensorMap pm[kMaxStageOps];   // base (else base2) arrays prefetched into L2 (ops with prefetch_base)
 };
 
 // Flush fields of a stage operator, read from the parameters once per
@@ -835,8 +835,11 @@ __device__ __forceinline__ void flush_x(const FlushArgs<T> &fa, const T (&res)[L
 // threads sweep the rows as 16-byte vectors, consecutive threads on
 // consecutive vectors of a row, so the loads of base and base2 and the
 // stores of out and out2 are coalesced across each warp (each thread's own
-// chunk would touch a different line per vector).  U = double writes FP64
-// outputs.
+// chunk would touch a different line per vector).  A thread's vectors go in
+// blocks of NB whose loads all precede their stores: base2 is often out2
+// itself (u = u - p in place), so a load after a store could not move ahead
+// of it and each vector would wait for memory in turn.  U = double writes
+// FP64 outputs.
 template <typename T, typename U>
 __device__ __forceinline__ void flush_x_rows(const FlushArgs<T> &fa, const T *out_s, long l0, int rows,
                                              int pitch, int n)
@@ -845,47 +848,64 @@ __device__ __forceinline__ void flush_x_rows(const FlushArgs<T> &fa, const T *ou
     constexpr int V = Vec4<T>::N;
     using UV = typename Vec4<U>::type;
     constexpr int NU = V / Vec4<U>::N;  // U vectors per T vector
+    constexpr int NB = 4;
     const U *base = static_cast<const U *>(fa.base);
     const U *base2 = static_cast<const U *>(fa.base2);
     U *out = static_cast<U *>(fa.out);
     U *out2 = static_cast<U *>(fa.out2);
     const U sign = (U)fa.sign, scale2 = (U)fa.scale2;
-    auto one = [&](int rr, int q) {
-        const size_t g = (size_t)(l0 + rr) * n + (size_t)q * V;
-        const VT v = *reinterpret_cast<const VT *>(out_s + (size_t)rr * pitch + (size_t)q * V);
-        const T *vl = reinterpret_cast<const T *>(&v);
-        UV b[NU], b2[NU];
-#pragma unroll
-        for (int u = 0; u < NU; ++u) {
-            b[u] = base ? *reinterpret_cast<const UV *>(base + g + u * (V / NU)) : UV{};
-            b2[u] = base2 ? *reinterpret_cast<const UV *>(base2 + g + u * (V / NU)) : UV{};
-        }
-        const U *bl = reinterpret_cast<const U *>(b);
-        const U *b2l = reinterpret_cast<const U *>(b2);
-        UV o[NU], o2[NU];
-        U *ol = reinterpret_cast<U *>(o);
-        U *o2l = reinterpret_cast<U *>(o2);
-#pragma unroll
-        for (int e = 0; e < V; ++e) {
-            ol[e] = bl[e] + sign * (U)vl[e];
-            o2l[e] = b2l[e] + scale2 * ol[e];
-        }
-#pragma unroll
-        for (int u = 0; u < NU; ++u) {
-            *reinterpret_cast<UV *>(out + g + u * (V / NU)) = o[u];
-            if (out2) *reinterpret_cast<UV *>(out2 + g + u * (V / NU)) = o2[u];
-        }
-    };
+    // this thread's vectors: (row r0 + i * G, vector q) for i = 0, 1, ...
     const int per_row = n / V, nt = blockDim.x, t = threadIdx.x;
+    int G, r0, q, qs;  // rows step, first row, vector, vector step
     if (nt >= per_row) {
-        // nt / per_row rows at a time
-        const int G = nt / per_row, r0 = t / per_row, q = t - r0 * per_row;
-        if (r0 < G)
-            for (int rr = r0; rr < rows; rr += G) one(rr, q);
+        G = nt / per_row;
+        r0 = t / per_row;
+        q = t - r0 * per_row;
+        qs = per_row;  // one vector per row
+        if (r0 >= G) return;
     } else {
-        for (int rr = 0; rr < rows; ++rr)
-#pragma unroll 2
-            for (int q = t; q < per_row; q += nt) one(rr, q);
+        G = 1;
+        r0 = 0;
+        q = t;
+        qs = nt;
+    }
+    for (int rr0 = r0; rr0 < rows; rr0 += NB * G) {
+        for (int q0 = q; q0 < per_row; q0 += qs) {
+            UV b[NB][NU], b2[NB][NU];
+#pragma unroll
+            for (int i = 0; i < NB; ++i) {
+                const int rr = rr0 + i * G;
+                const size_t g = (size_t)(l0 + rr) * n + (size_t)q0 * V;
+#pragma unroll
+                for (int u = 0; u < NU; ++u) {
+                    b[i][u] = base && rr < rows ? *reinterpret_cast<const UV *>(base + g + u * (V / NU)) : UV{};
+                    b2[i][u] = base2 && rr < rows ? *reinterpret_cast<const UV *>(base2 + g + u * (V / NU)) : UV{};
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < NB; ++i) {
+                const int rr = rr0 + i * G;
+                if (rr >= rows) break;
+                const size_t g = (size_t)(l0 + rr) * n + (size_t)q0 * V;
+                const VT v = *reinterpret_cast<const VT *>(out_s + (size_t)rr * pitch + (size_t)q0 * V);
+                const T *vl = reinterpret_cast<const T *>(&v);
+                const U *bl = reinterpret_cast<const U *>(b[i]);
+                const U *b2l = reinterpret_cast<const U *>(b2[i]);
+                UV o[NU], o2[NU];
+                U *ol = reinterpret_cast<U *>(o);
+                U *o2l = reinterpret_cast<U *>(o2);
+#pragma unroll
+                for (int e = 0; e < V; ++e) {
+                    ol[e] = bl[e] + sign * (U)vl[e];
+                    o2l[e] = b2l[e] + scale2 * ol[e];
+                }
+#pragma unroll
+                for (int u = 0; u < NU; ++u) {
+                    *reinterpret_cast<UV *>(out + g + u * (V / NU)) = o[u];
+                    if (out2) *reinterpret_cast<UV *>(out2 + g + u * (V / NU)) = o2[u];
+                }
+            }
+        }
     }
 }
 
@@ -1000,7 +1020,9 @@ __global__ void __launch_bounds__(512, 1)
         // the tile's base rows (read back by the flushes) into L2
         for (int mask = prog.prefetch_mask, k = 0; mask; mask >>= 1, ++k)
             if (mask & 1)
-                bulk_prefetch(static_cast<const T *>(prog.ops[k].base) + (size_t)l0 * n, row_bytes * (uint32_t)rows);
+                bulk_prefetch(static_cast<const T *>(prog.ops[k].base ? prog.ops[k].base : prog.ops[k].base2) +
+                                  (size_t)l0 * n,
+                              row_bytes * (uint32_t)rows);
     };
     const ChunkScratch<T> sc = carve_scratch<T>(smem_raw + (PERSIST ? 2 : 1) * slot_bytes, C, W);
     // staging rows for plain outputs, after the responses (128-byte aligned)
@@ -1168,7 +1190,7 @@ static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog_in, int 
             so.base2_tile = -1;
             for (int ti = 0; ti < prog.ntiles; ++ti)
                 if (!so.out_f64 && so.base2 && so.base2 == prog.in[ti]) so.base2_tile = (short)ti;
-            so.prefetch_base = (so.flush && so.base && !so.out_f64) ? 1 : 0;
+            so.prefetch_base = (so.flush && !so.out_f64 && (so.base || (so.base2 && so.base2_tile < 0))) ? 1 : 0;
         }
         prog.prefetch_mask = 0;
         for (int k = 0; k < prog.nops; ++k)
@@ -1255,7 +1277,9 @@ static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog_in, int 
         for (int ti = 0; ti < prog.ntiles; ++ti)
             if (!encode(&maps.m[ti], prog.in[ti])) return X3D_EUNSUPPORTED;
         for (int k = 0; k < prog.nops; ++k)
-            if (prog.ops[k].prefetch_base && !encode(&maps.pm[k], prog.ops[k].base)) prog.ops[k].prefetch_base = 0;
+            if (prog.ops[k].prefetch_base &&
+                !encode(&maps.pm[k], prog.ops[k].base ? prog.ops[k].base : prog.ops[k].base2))
+                prog.ops[k].prefetch_base = 0;
         prog.prefetch_mask = 0;
         for (int k = 0; k < prog.nops; ++k)
             if (prog.ops[k].prefetch_base) prog.prefetch_mask |= 1 << k;

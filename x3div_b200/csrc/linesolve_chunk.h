@@ -31,7 +31,8 @@ struct StageOp {
     short flush;
     short out_f64;  // out, base, out2, base2 hold double rather than T
     // Set by launch_stage: base2 is staged input tile base2_tile (-1: read
-    // from global memory); prefetch_base: base is prefetched into L2 when
+    // from global memory); prefetch_base: base (or, without one, a base2
+    // read from global memory) is prefetched into L2 when
     // the tile's inputs are requested.
     short base2_tile;
     short prefetch_base;
