@@ -433,8 +433,10 @@ __device__ __forceinline__ ChunkScratch<T> carve_scratch(unsigned char *base, in
     return sc;
 }
 
-// acc (+)= m * r, with m = 1 or the staged tile value at the point.
-template <typename T, int L, typename S, typename TileAt>
+// acc (+)= m * r, with m = 1 or the staged tile value at the point;
+// tile_at(ti, j) returns TV consecutive tile values from point j (a 16-byte
+// vector along an x row, one value per point down a y/z column).
+template <typename T, int L, int TV, typename S, typename TileAt>
 __device__ __forceinline__ void accumulate(const StageOp<S> &so, T (&acc)[L], const T (&r)[L],
                                            int nv, const TileAt &tile_at)
 {
@@ -450,10 +452,20 @@ __device__ __forceinline__ void accumulate(const StageOp<S> &so, T (&acc)[L], co
         // points past a short chunk's end read staged halo/padding rows and
         // are never stored
 #pragma unroll
-        for (int j = 0; j < L; ++j) acc[j] = fma(tile_at(so.mul_tile, j), r[j], acc[j]);
+        for (int j = 0; j < L; j += TV) {
+            const auto tv = tile_at(so.mul_tile, j);
+            const T *te = reinterpret_cast<const T *>(&tv);
+#pragma unroll
+            for (int v = 0; v < TV; ++v) acc[j + v] = fma(te[v], r[j + v], acc[j + v]);
+        }
     } else {
 #pragma unroll
-        for (int j = 0; j < L; ++j) acc[j] = tile_at(so.mul_tile, j) * r[j];
+        for (int j = 0; j < L; j += TV) {
+            const auto tv = tile_at(so.mul_tile, j);
+            const T *te = reinterpret_cast<const T *>(&tv);
+#pragma unroll
+            for (int v = 0; v < TV; ++v) acc[j + v] = te[v] * r[j + v];
+        }
     }
 }
 
@@ -742,7 +754,7 @@ __global__ void __launch_bounds__(kStageThreads<T, L, PR>, 1)
             };
             chunk_solve_resp<V, L>(so, resp_s + k * 4 * L, load, r, sc, WP, l, c, C, nv, c * WP + l);
             if constexpr (ACC) {
-                accumulate<V, L>(so, acc, r, nv, tile_at);
+                accumulate<V, L, 1>(so, acc, r, nv, tile_at);
                 if (so.flush && live) flush_yz<T, V, L, true>(flush_args(so), acc, obase, ostride, nv);
             } else {
                 if (so.flush && live) flush_yz<T, V, L, false>(flush_args(so), r, obase, ostride, nv);
@@ -836,7 +848,8 @@ __device__ __forceinline__ void flush_x(const FlushArgs<T> &fa, const T (&res)[L
 // consecutive vectors of a row, so the loads of base and base2 and the
 // stores of out and out2 are coalesced across each warp (each thread's own
 // chunk would touch a different line per vector).  A thread's vectors go in
-// blocks of NB whose loads all precede their stores: base2 is often out2
+// blocks of NB (2: the accumulator stays live across the flush, so more
+// would spill) whose loads all precede their stores: base2 is often out2
 // itself (u = u - p in place), so a load after a store could not move ahead
 // of it and each vector would wait for memory in turn.  U = double writes
 // FP64 outputs.
@@ -848,7 +861,7 @@ __device__ __forceinline__ void flush_x_rows(const FlushArgs<T> &fa, const T *ou
     constexpr int V = Vec4<T>::N;
     using UV = typename Vec4<U>::type;
     constexpr int NU = V / Vec4<U>::N;  // U vectors per T vector
-    constexpr int NB = 4;
+    constexpr int NB = 2;
     const U *base = static_cast<const U *>(fa.base);
     const U *base2 = static_cast<const U *>(fa.base2);
     U *out = static_cast<U *>(fa.out);
@@ -1057,7 +1070,7 @@ __global__ void __launch_bounds__(512, 1)
         auto row = [&](int ti) {
             return reinterpret_cast<const T *>(base + ti * tile_bytes) + (size_t)lr * pitch + cs;
         };
-        auto tile_at = [&](int ti, int j) { return row(ti)[kHalo + j]; };
+        auto tile_at = [&](int ti, int j) { return *reinterpret_cast<const VT *>(row(ti) + kHalo + j); };
         auto flush_args = [&](const StageOp<T> &so) {
             return FlushArgs<T>(so, so.base2_tile >= 0 ? row(so.base2_tile) + kHalo : nullptr, 1);
         };
@@ -1095,7 +1108,7 @@ __global__ void __launch_bounds__(512, 1)
             if (t < W) bulk_wait_read_all();
             chunk_solve_resp<T, L>(so, resp_s + k * 4 * L, load, r, sc, W, l, c, C, nv, c * W + l);
             if constexpr (ACC) {
-                accumulate<T, L>(so, acc, r, nv, tile_at);
+                accumulate<T, L, V>(so, acc, r, nv, tile_at);
                 if (so.flush) flush_x_staged<T, L, true>(flush_args(so), acc, out_s, l, l0, rows, pitch, n, cs, nv);
             } else {
                 if (so.flush) flush_x_staged<T, L, false>(flush_args(so), r, out_s, l, l0, rows, pitch, n, cs, nv);
