@@ -35,6 +35,22 @@ def test_poisson(oracle, torch_cuda, shape):
     ctx.close()
 
 
+# z lengths of every radix pattern of the fused z-transform kernel (8s, 4, 2,
+# 3s; one to four tiles of x modes, a last tile of one mode) and one that
+# takes the 3-D cuFFT path (nz = 40 = 8 * 5)
+@pytest.mark.parametrize("shape", [(16, 10, 8), (30, 12, 12), (34, 8, 48), (20, 8, 96), (14, 8, 192),
+                                   (8, 8, 384), (8, 8, 768), (10, 8, 1024), (12, 10, 40)])
+def test_poisson_z_lengths(oracle, torch_cuda, shape):
+    from x3div_b200 import to_device, to_host
+    ctx = ctx_for(shape)
+    rhs = seeded_field(shape, 23, kind="rand", lengths=LEN, noise=0)
+    d = to_device(rhs)
+    ctx.poisson(d)
+    ctx.sync()
+    assert rel_err(to_host(d), oracle.poisson(rhs, *LEN)) < 1e-12, shape
+    ctx.close()
+
+
 @pytest.mark.parametrize("shape", SHAPES)
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 def test_divergence_gradp_momentum(oracle, torch_cuda, shape, prec):

@@ -86,6 +86,239 @@ __global__ void k_spectral_divide(double2 *c, unsigned nxh, unsigned ny, unsigne
     }
 }
 
+// ---------------------------------------------------------------------------
+// z transforms fused with the mode division.  The 3-D transform of the
+// (nz, ny, nx) field separates into 2-D (x, y) transforms of each z plane,
+// which cuFFT does batched, and 1-D transforms along z of each (i, j) line of
+// the half spectrum.  One kernel takes a tile of W x-adjacent z lines into
+// shared memory, transforms them forward along z, divides each mode, and
+// transforms them back, so the spectrum crosses HBM once for all three steps
+// (cuFFT's z passes and a separate division kernel cross it three times).
+//
+// The z transforms are mixed-radix Stockham autosort FFTs (radix 8, 4, 2,
+// then 3), the formulation of Govindaraju et al., "High performance discrete
+// Fourier transforms on graphics processors" (SC 2008): a stage of radix R
+// over sub-transforms of size Ns reads element j + q n/R (q < R) of each
+// line, multiplies it by W_n^(q (j mod Ns) n/(Ns R)), takes the length-R DFT
+// in registers and writes the results to (j div Ns) Ns R + (j mod Ns) + q Ns.
+// Each stage reads all its inputs before a barrier and writes after it, so
+// one shared-memory buffer suffices.  Twiddles come from a table of the nz
+// roots of unity computed on the host in FP64 (copied to shared memory).
+
+constexpr int kZftThreads = 512;
+constexpr int kZftVals = 8;    // values a thread holds in one stage
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b)
+{
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+// a times -i (forward transform) or +i (inverse)
+template <bool INV>
+__device__ __forceinline__ double2 cmi(double2 a)
+{
+    return INV ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+}
+
+// Length-R DFT of v in place, exponent sign - (forward) or + (INV).
+template <int R, bool INV>
+__device__ __forceinline__ void dft(double2 (&v)[R])
+{
+    if constexpr (R == 2) {
+        const double2 a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    } else if constexpr (R == 4) {
+        const double2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+        const double2 t2 = cadd(v[1], v[3]), t3 = cmi<INV>(csub(v[1], v[3]));
+        v[0] = cadd(t0, t2);
+        v[2] = csub(t0, t2);
+        v[1] = cadd(t1, t3);
+        v[3] = csub(t1, t3);
+    } else if constexpr (R == 8) {
+        // two length-4 DFTs of the even and odd points, joined by W_8^k
+        double2 e[4] = {v[0], v[2], v[4], v[6]};
+        double2 o[4] = {v[1], v[3], v[5], v[7]};
+        dft<4, INV>(e);
+        dft<4, INV>(o);
+        const double c = 0.70710678118654752440;  // sqrt(1/2)
+        const double sg = INV ? 1.0 : -1.0;
+        const double2 w1 = make_double2(c, sg * c), w3 = make_double2(-c, sg * c);
+        const double2 o1 = cmul(o[1], w1), o2 = cmi<INV>(o[2]), o3 = cmul(o[3], w3);
+        v[0] = cadd(e[0], o[0]);
+        v[4] = csub(e[0], o[0]);
+        v[1] = cadd(e[1], o1);
+        v[5] = csub(e[1], o1);
+        v[2] = cadd(e[2], o2);
+        v[6] = csub(e[2], o2);
+        v[3] = cadd(e[3], o3);
+        v[7] = csub(e[3], o3);
+    } else {  // R == 3
+        const double s3 = 0.86602540378443864676;  // sqrt(3)/2
+        const double2 t = cadd(v[1], v[2]);
+        const double2 m = cmi<INV>(csub(v[1], v[2]));
+        const double2 h = make_double2(v[0].x - 0.5 * t.x, v[0].y - 0.5 * t.y);
+        v[0] = cadd(v[0], t);
+        v[1] = make_double2(h.x + s3 * m.x, h.y + s3 * m.y);
+        v[2] = make_double2(h.x - s3 * m.x, h.y - s3 * m.y);
+    }
+}
+
+// One Stockham stage of radix R over sub-transforms of size NS, for the W
+// lines of the tile (element e of line l at buf[e W + l]).
+template <int N, int R, int NS, int W, bool INV>
+__device__ __forceinline__ void zft_stage(double2 *buf, const double2 *tw)
+{
+    constexpr int MB = kZftVals / R;
+    constexpr int NB = W * (N / R);
+    constexpr int STRIDE = N / (NS * R);
+    static_assert(NB <= MB * kZftThreads, "tile too large for one pass of the stage");
+    double2 v[MB][R];
+    int dst[MB];
+#pragma unroll
+    for (int s = 0; s < MB; ++s) {
+        const int b = threadIdx.x + s * kZftThreads;
+        if (b < NB) {
+            const int l = b % W, j = b / W;
+            const int jm = j % NS;
+#pragma unroll
+            for (int q = 0; q < R; ++q) {
+                const double2 x = buf[(j + q * (N / R)) * W + l];
+                if (q == 0) {
+                    v[s][q] = x;
+                } else {
+                    double2 w = tw[q * jm * STRIDE];
+                    if (INV) w.y = -w.y;
+                    v[s][q] = cmul(x, w);
+                }
+            }
+            dft<R, INV>(v[s]);
+            dst[s] = ((j / NS) * NS * R + jm) * W + l;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < MB; ++s) {
+        const int b = threadIdx.x + s * kZftThreads;
+        if (b < NB) {
+#pragma unroll
+            for (int q = 0; q < R; ++q) buf[dst[s] + q * NS * W] = v[s][q];
+        }
+    }
+    __syncthreads();
+}
+
+// Radices of a length-N transform: 8s, 4, 2, then 3s.
+struct RadixSeq {
+    int count;
+    int r[10];
+};
+constexpr RadixSeq radix_seq(int n)
+{
+    RadixSeq s{0, {}};
+    int m = n;
+    while (m % 8 == 0 && m > 1) s.r[s.count++] = 8, m /= 8;
+    while (m % 4 == 0) s.r[s.count++] = 4, m /= 4;
+    while (m % 2 == 0) s.r[s.count++] = 2, m /= 2;
+    while (m % 3 == 0) s.r[s.count++] = 3, m /= 3;
+    return s;
+}
+
+template <int N, int W, bool INV, int ST = 0, int NS = 1>
+__device__ __forceinline__ void zft(double2 *buf, const double2 *tw)
+{
+    constexpr RadixSeq seq = radix_seq(N);
+    if constexpr (ST < seq.count) {
+        constexpr int R = seq.r[ST];
+        zft_stage<N, R, NS, W, INV>(buf, tw);
+        zft<N, W, INV, ST + 1, NS * R>(buf, tw);
+    }
+}
+
+// Lines per tile for a transform of length N (W N <= kZftThreads kZftVals).
+template <int N>
+constexpr int kZftW = N <= 256 ? 16 : (N <= 512 ? 8 : 4);
+
+// One CTA per (j, tile of W x-modes): z transform, c <- -c / (K ntot) with the
+// K and mask of k_spectral_divide, inverse z transform.  The tile's loads
+// and stores, and the mode scalings, run as compile-time loops of PER values
+// per thread, so each thread has all its global loads in flight at once; the
+// twiddles are copied into shared memory first.
+template <int N>
+__global__ void __launch_bounds__(kZftThreads, 2)
+    k_poisson_z(double2 *__restrict__ c, int nxh, int ny, const double2 *__restrict__ tw,
+                const double *__restrict__ k2x, const double *__restrict__ tx, const double *__restrict__ k2y,
+                const double *__restrict__ ty, const double *__restrict__ k2z, const double *__restrict__ tz,
+                double ntot)
+{
+    constexpr int W = kZftW<N>;
+    constexpr int PER = (N * W + kZftThreads - 1) / kZftThreads;
+    extern __shared__ __align__(16) double2 zbuf[];
+    double2 *const tws = zbuf + N * W;
+    const int tiles_i = (nxh + W - 1) / W;
+    const int j = blockIdx.x / tiles_i;
+    const int i0 = (blockIdx.x - j * tiles_i) * W;
+    const int lines = min(W, nxh - i0);
+    const size_t zstride = (size_t)ny * nxh;
+    double2 *const base = c + (size_t)j * nxh + i0;
+    for (int t = threadIdx.x; t < N; t += kZftThreads) tws[t] = __ldg(tw + t);
+    {
+        double2 v[PER];
+#pragma unroll
+        for (int s = 0; s < PER; ++s) {
+            const int e = threadIdx.x + s * kZftThreads;
+            const int k = e / W, l = e % W;
+            v[s] = e < N * W && l < lines ? base[(size_t)k * zstride + l] : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int s = 0; s < PER; ++s) {
+            const int e = threadIdx.x + s * kZftThreads;
+            if (e < N * W) zbuf[e] = v[s];
+        }
+    }
+    __syncthreads();
+    zft<N, W, false>(zbuf, tws);
+    const double tyj = __ldg(ty + j), k2yj = __ldg(k2y + j);
+#pragma unroll
+    for (int s = 0; s < PER; ++s) {
+        const int e = threadIdx.x + s * kZftThreads;
+        if (e < N * W) {
+            const int k = e / W, l = e % W;
+            const int i = min(i0 + l, nxh - 1);
+            const double txi = __ldg(tx + i), tzk = __ldg(tz + k);
+            const double tyz = tyj * tzk, txz = txi * tzk, txy = txi * tyj;
+            const double kk =
+                __ldg(k2x + i) * (tyz * tyz) + k2yj * (txz * txz) + __ldg(k2z + k) * (txy * txy);
+            const double f = kk < 1.e-16 ? 0.0 : -1.0 / (kk * ntot);
+            double2 v = zbuf[e];
+            v.x *= f;
+            v.y *= f;
+            zbuf[e] = v;
+        }
+    }
+    __syncthreads();
+    zft<N, W, true>(zbuf, tws);
+#pragma unroll
+    for (int s = 0; s < PER; ++s) {
+        const int e = threadIdx.x + s * kZftThreads;
+        const int k = e / W, l = e % W;
+        if (e < N * W && l < lines) base[(size_t)k * zstride + l] = zbuf[e];
+    }
+}
+
+// The z lengths with a fused kernel.
+#define X3D_ZFT_SIZES(X) X(8) X(12) X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512) X(768) X(1024)
+
+static bool zft_supported(int n)
+{
+#define X3D_ZFT_CASE(N) \
+    if (n == N) return true;
+    X3D_ZFT_SIZES(X3D_ZFT_CASE)
+#undef X3D_ZFT_CASE
+    return false;
+}
+
 int poisson_setup(x3d_ctx_s *ctx)
 {
     if (ctx->plans_ready) return X3D_OK;
@@ -114,11 +347,50 @@ int poisson_setup(x3d_ctx_s *ctx)
     ctx->d_tz = tab + 2 * nx + 2 * ny + nz;
     const size_t spec = (size_t)nz * ny * (nx / 2 + 1) * sizeof(double2);
     if (cudaMalloc(&ctx->spectrum, spec) != cudaSuccess) return set_error(ctx, X3D_ENOMEM, "poisson spectrum");
-    if (cufftPlan3d(&ctx->plan_d2z, nz, ny, nx, CUFFT_D2Z) != CUFFT_SUCCESS ||
-        cufftPlan3d(&ctx->plan_z2d, nz, ny, nx, CUFFT_Z2D) != CUFFT_SUCCESS)
+    ctx->zfused = zft_supported(nz) && ctx->zfuse_allowed;
+    if (ctx->zfused) {
+        std::vector<double> tw(2 * (size_t)nz);
+        const double twopi = 2.0 * std::acos(-1.0);
+        for (int t = 0; t < nz; ++t) {
+            tw[2 * t] = std::cos(twopi * t / nz);
+            tw[2 * t + 1] = -std::sin(twopi * t / nz);
+        }
+        if (cudaMalloc(&ctx->d_zft_tw, tw.size() * sizeof(double)) != cudaSuccess)
+            return set_error(ctx, X3D_ENOMEM, "poisson twiddles");
+        cudaMemcpy(ctx->d_zft_tw, tw.data(), tw.size() * sizeof(double), cudaMemcpyHostToDevice);
+        int dims[2] = {ny, nx};
+        if (cufftPlanMany(&ctx->plan_d2z, 2, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_D2Z, nz) != CUFFT_SUCCESS ||
+            cufftPlanMany(&ctx->plan_z2d, 2, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_Z2D, nz) != CUFFT_SUCCESS)
+            return set_error(ctx, X3D_ECUDA, "cufftPlanMany failed");
+    } else if (cufftPlan3d(&ctx->plan_d2z, nz, ny, nx, CUFFT_D2Z) != CUFFT_SUCCESS ||
+               cufftPlan3d(&ctx->plan_z2d, nz, ny, nx, CUFFT_Z2D) != CUFFT_SUCCESS) {
         return set_error(ctx, X3D_ECUDA, "cufftPlan3d failed");
+    }
     ctx->plans_ready = true;
     return X3D_OK;
+}
+
+static int launch_poisson_z(x3d_ctx_s *ctx)
+{
+    const int nxh = ctx->nx / 2 + 1;
+    const double ntot = (double)ctx->nx * (double)ctx->ny * (double)ctx->nz;
+    auto go = [&](auto kern, int W) {
+        const unsigned grid = (unsigned)(((nxh + W - 1) / W) * ctx->ny);
+        const size_t smem = ((size_t)ctx->nz * W + ctx->nz) * sizeof(double2);  // tile + twiddles
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        ++ctx->launches;
+        kern<<<grid, kZftThreads, smem, ctx->stream>>>((double2 *)ctx->spectrum, nxh, ctx->ny,
+                                                       (const double2 *)ctx->d_zft_tw, ctx->d_k2x, ctx->d_tx,
+                                                       ctx->d_k2y, ctx->d_ty, ctx->d_k2z, ctx->d_tz, ntot);
+        return cuda_check(ctx, cudaGetLastError(), "k_poisson_z");
+    };
+    switch (ctx->nz) {
+#define X3D_ZFT_LAUNCH(N) \
+    case N: return go(k_poisson_z<N>, kZftW<N>);
+        X3D_ZFT_SIZES(X3D_ZFT_LAUNCH)
+#undef X3D_ZFT_LAUNCH
+    default: return set_error(ctx, X3D_EUNSUPPORTED, "no fused z transform for this nz");
+    }
 }
 
 int poisson_solve(x3d_ctx_s *ctx, double *rhs)
@@ -129,6 +401,13 @@ int poisson_solve(x3d_ctx_s *ctx, double *rhs)
     cufftSetStream(ctx->plan_z2d, ctx->stream);
     if (cufftExecD2Z(ctx->plan_d2z, rhs, (cufftDoubleComplex *)ctx->spectrum) != CUFFT_SUCCESS)
         return set_error(ctx, X3D_ECUDA, "cufftExecD2Z failed");
+    if (ctx->zfused) {
+        rc = launch_poisson_z(ctx);
+        if (rc) return rc;
+        if (cufftExecZ2D(ctx->plan_z2d, (cufftDoubleComplex *)ctx->spectrum, rhs) != CUFFT_SUCCESS)
+            return set_error(ctx, X3D_ECUDA, "cufftExecZ2D failed");
+        return X3D_OK;
+    }
     const int nxh = ctx->nx / 2 + 1;
     const size_t n = (size_t)nxh * ctx->ny * ctx->nz;
     if (n >= (1ull << 31)) return set_error(ctx, X3D_EUNSUPPORTED, "spectrum above 2^31 modes");
@@ -160,6 +439,9 @@ void poisson_free(x3d_ctx_s *ctx)
     ctx->spectrum = nullptr;
     if (ctx->d_k2x) cudaFree(ctx->d_k2x);
     ctx->d_k2x = nullptr;
+    if (ctx->d_zft_tw) cudaFree(ctx->d_zft_tw);
+    ctx->d_zft_tw = nullptr;
+    ctx->zfused = false;
 }
 
 }  // namespace x3d

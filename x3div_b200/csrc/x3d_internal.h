@@ -102,9 +102,14 @@ struct x3d_ctx_s {
     int *d_err = nullptr;  // device error flag written by bounded waits
     std::string last_error;
     x3d_op_s *builtin[X3D_OP_COUNT] = {};
-    // Poisson: cuFFT plans, spectrum and the 1-D modified-wavenumber tables
+    // Poisson: cuFFT plans, spectrum and the 1-D modified-wavenumber tables.
+    // With zfused the plans are 2-D (x, y) transforms batched over the z
+    // planes, and one kernel does the z transforms and the mode division.
     cufftHandle plan_d2z = 0, plan_z2d = 0;
     bool plans_ready = false;
+    bool zfused = false;
+    bool zfuse_allowed = true;  // cleared to force the 3-D cuFFT path
+    double *d_zft_tw = nullptr;  // e^{-2 pi i t / nz}, t < nz (complex)
     void *spectrum = nullptr;  // complex double, nz * ny * (nx/2+1)
     double *d_k2x = nullptr, *d_tx = nullptr, *d_k2y = nullptr, *d_ty = nullptr, *d_k2z = nullptr,
            *d_tz = nullptr;
