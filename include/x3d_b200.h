@@ -18,7 +18,9 @@
  *    precision: double for X3D_F64, float for X3D_F32.  Pressure arguments
  *    (pp3) are always double.  A pointer to ordinary or pinned host memory
  *    is also accepted: the call then stages it through device memory and
- *    returns only after the results are back in host memory.
+ *    returns only after the results are back in host memory.  The staging
+ *    buffers stay with the context for later calls (freed by
+ *    x3d_ctx_destroy).
  *  - Calls on device pointers are asynchronous on the context's stream, as
  *    CUDA launches are; x3d_ctx_sync() waits and reports device-side errors.
  *  - Every function returns an int status: X3D_OK (0) or a negative code.

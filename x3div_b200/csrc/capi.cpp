@@ -96,7 +96,7 @@ class Stager {
     };
     x3d_ctx_s *ctx;
     std::vector<Item> items;
-    std::vector<void *> owned;
+    size_t used = 0;  // staging-pool buffers taken by this call
     bool any_host = false;
     int rc = X3D_OK;
     void *stage(void *p, size_t bytes, bool upload, bool download)
@@ -109,12 +109,11 @@ class Stager {
                 return it.dev;
             }
         any_host = true;
-        void *d = nullptr;
-        if (cudaMalloc(&d, bytes) != cudaSuccess) {
+        void *d = take(bytes);
+        if (!d) {
             rc = set_error(ctx, X3D_ENOMEM, "staging allocation failed");
             return nullptr;
         }
-        owned.push_back(d);
         if (upload) {
             int r = cuda_check(ctx, cudaMemcpyAsync(d, p, bytes, cudaMemcpyHostToDevice, ctx->stream), "stage h2d");
             if (r) rc = r;
@@ -122,11 +121,31 @@ class Stager {
         items.push_back({p, d, bytes, download});
         return d;
     }
+    // The next device buffer of the context's staging pool, grown to bytes.
+    // The pool outlives the call (freed by x3d_ctx_destroy), so repeated
+    // calls on host arrays allocate nothing: allocating and mapping
+    // hundreds of MB per call would cost more than the copies themselves.
+    void *take(size_t bytes)
+    {
+        auto &pool = ctx->staging;
+        if (used < pool.size() && pool[used].second >= bytes) return pool[used++].first;
+        if (used < pool.size()) {
+            cudaStreamSynchronize(ctx->stream);
+            cudaFree(pool[used].first);
+            pool[used] = {nullptr, 0};
+        }
+        void *d = nullptr;
+        if (cudaMalloc(&d, bytes) != cudaSuccess) return nullptr;
+        if (used < pool.size()) pool[used] = {d, bytes};
+        else pool.push_back({d, bytes});
+        ++used;
+        return d;
+    }
+    // The pool's buffers may be taken by the next call only after this
+    // call's copies are done.
     void release()
     {
-        if (!owned.empty()) cudaStreamSynchronize(ctx->stream);
-        for (void *d : owned) cudaFree(d);
-        owned.clear();
+        if (used) cudaStreamSynchronize(ctx->stream);
     }
 };
 
@@ -337,6 +356,8 @@ int x3d_ctx_destroy(x3d_ctx ctx)
     poisson_free(ctx);
     for (void *p : ctx->scratch) cudaFree(p);
     ctx->scratch.clear();
+    for (auto &b : ctx->staging) cudaFree(b.first);
+    ctx->staging.clear();
     if (ctx->d_err) cudaFree(ctx->d_err);
     if (ctx->d_red) cudaFree(ctx->d_red);
     if (ctx->d_metric) cudaFree(ctx->d_metric);

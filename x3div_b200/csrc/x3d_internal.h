@@ -116,7 +116,8 @@ struct x3d_ctx_s {
     // scratch fields owned by the context (sized nx*ny*nz elements)
     std::vector<void *> scratch;
     size_t scratch_elem_bytes = 0;
-    // host-pointer staging buffers
+    // device buffers for host-pointer arguments (pointer, bytes), reused by
+    // later calls and freed with the context
     std::vector<std::pair<void *, size_t>> staging;
     double *d_red = nullptr;  // small reduction buffer
     double *d_metric = nullptr;  // device copy of a y stretching metric (ny doubles)
