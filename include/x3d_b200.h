@@ -352,6 +352,33 @@ int x3d_int_time(x3d_ctx ctx, void *ux1, void *uy1, void *uz1, const void *dux1,
  * pp3 and px..pz are outputs (the reference's dux1/duy1/duz1, pp3, px1..pz1). */
 int x3d_euler_step(x3d_ctx ctx, void *ux1, void *uy1, void *uz1, void *dux1, void *duy1,
                    void *duz1, double *pp3, void *px1, void *py1, void *pz1, double dt);
+/* Records x3d_euler_step on these fields into a CUDA graph kept by the
+ * context (nothing runs), after allocating what the step would allocate on
+ * first use; x3d_step_launch replays it on the context's stream, one
+ * timestep per launch.  The fields must be device pointers or registered
+ * host arrays (x3d_buf_register), and the context must be on a created
+ * stream (not the legacy or per-thread default).  The graph keeps the
+ * kernel configurations chosen at capture time; a new capture replaces it.
+ * x3d_ctx_launch_count counts the captured launches once.  No reference
+ * counterpart: the reference calls the step's routines one by one. */
+int x3d_step_capture(x3d_ctx ctx, void *ux1, void *uy1, void *uz1, void *dux1, void *duy1,
+                     void *duz1, double *pp3, void *px1, void *py1, void *pz1, double dt);
+int x3d_step_launch(x3d_ctx ctx);
+
+/* ---- device-resident host arrays ------------------------------------------ */
+
+/* The reference keeps its fields on the device between calls with OpenACC
+ * data regions (src/xcompact3d.f90:43-72).  x3d_buf_register gives a host
+ * array of nbytes a device mirror (filled from the host once; *dev, if not
+ * NULL, receives its address): every later call passed a pointer inside the
+ * host array works on the mirror, with no copies and no host results, until
+ * x3d_sync_to_host copies the mirror back (x3d_sync_to_device the other
+ * way).  x3d_buf_unregister frees the mirror without copying.  Registered
+ * arrays must not overlap.  Synchronous.  No reference counterpart. */
+int x3d_buf_register(x3d_ctx ctx, void *host, size_t nbytes, void **dev);
+int x3d_buf_unregister(x3d_ctx ctx, void *host);
+int x3d_sync_to_device(x3d_ctx ctx, void *host);
+int x3d_sync_to_host(x3d_ctx ctx, void *host);
 
 /* ---- initial field and analytic checks: module mom (src/mom.f90) -------- */
 

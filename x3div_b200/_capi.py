@@ -65,6 +65,12 @@ SIGNATURES = {
     "x3d_ctx_set_kernel": [_vp, _i],
     "x3d_autotune_choice": [_vp, _i, _i, _ip],
     "x3d_autotune_stage_choice": [_vp, ctypes.c_char_p, _ip],
+    "x3d_step_capture": [_vp] + [_vp] * 10 + [ctypes.c_double],
+    "x3d_step_launch": [_vp],
+    "x3d_buf_register": [_vp, _vp, ctypes.c_size_t, ctypes.POINTER(_vp)],
+    "x3d_buf_unregister": [_vp, _vp],
+    "x3d_sync_to_device": [_vp, _vp],
+    "x3d_sync_to_host": [_vp, _vp],
     "x3d_batch_create": [ctypes.POINTER(_vp), _vp, _i, _i, _i],
     "x3d_batch_destroy": [_vp],
     "x3d_batch_set_stream": [_vp, _vp],

@@ -325,6 +325,33 @@ class Context:
     def euler_step(self, ux1, uy1, uz1, dux1, duy1, duz1, pp3, px1, py1, pz1, dt):
         self._check(self.L.x3d_euler_step(self.handle, *[_ptr(a) for a in (ux1, uy1, uz1, dux1, duy1, duz1, pp3, px1, py1, pz1)], float(dt)))
 
+    def step_capture(self, ux1, uy1, uz1, dux1, duy1, duz1, pp3, px1, py1, pz1, dt):
+        """x3d_step_capture: record one Euler step on these fields into a CUDA graph."""
+        self._check(self.L.x3d_step_capture(self.handle, *[_ptr(a) for a in (ux1, uy1, uz1, dux1, duy1, duz1, pp3, px1, py1, pz1)], float(dt)))
+
+    def step_launch(self):
+        """x3d_step_launch: replay the captured step once."""
+        self._check(self.L.x3d_step_launch(self.handle))
+
+    # -- device-resident host arrays ---------------------------------------
+    def buf_register(self, host):
+        """x3d_buf_register: give a contiguous host numpy array a device mirror;
+        returns the mirror's device address."""
+        if not isinstance(host, np.ndarray) or not (host.flags.f_contiguous or host.flags.c_contiguous):
+            raise ValueError("buf_register takes a contiguous numpy array")
+        dev = ctypes.c_void_p()
+        self._check(self.L.x3d_buf_register(self.handle, host.ctypes.data, host.nbytes, ctypes.byref(dev)))
+        return dev.value
+
+    def buf_unregister(self, host):
+        self._check(self.L.x3d_buf_unregister(self.handle, host.ctypes.data))
+
+    def sync_to_device(self, host):
+        self._check(self.L.x3d_sync_to_device(self.handle, host.ctypes.data))
+
+    def sync_to_host(self, host):
+        self._check(self.L.x3d_sync_to_host(self.handle, host.ctypes.data))
+
     def vel(self, u, v, w):
         self._check(self.L.x3d_vel(self.handle, _ptr(u), _ptr(v), _ptr(w)))
 

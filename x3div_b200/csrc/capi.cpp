@@ -67,6 +67,18 @@ bool is_device_ptr(const void *p)
 
 // Host-pointer staging for one call: inputs are uploaded before the work,
 // outputs downloaded after it, and the call then synchronises.
+// The device mirror of [p, p + bytes) when that range lies inside a host
+// array registered with x3d_buf_register, else null.
+void *resident_dev(const x3d_ctx_s *ctx, const void *p, size_t bytes)
+{
+    const char *c = static_cast<const char *>(p);
+    for (const auto &r : ctx->resident) {
+        const char *h = static_cast<const char *>(r.host);
+        if (c >= h && c + bytes <= h + r.bytes) return static_cast<char *>(r.dev) + (c - h);
+    }
+    return nullptr;
+}
+
 class Stager {
   public:
     explicit Stager(x3d_ctx_s *c) : ctx(c) {}
@@ -102,6 +114,7 @@ class Stager {
     void *stage(void *p, size_t bytes, bool upload, bool download)
     {
         if (!p || rc) return p;
+        if (void *d = resident_dev(ctx, p, bytes)) return d;  // registered: no copies
         if (is_device_ptr(p)) return p;
         for (auto &it : items)  // the same host array passed twice maps to one device copy
             if (it.user == p) {
@@ -182,7 +195,9 @@ int apply_op(x3d_ctx_s *ctx, void *t, const void *u, x3d_op_s *op, int want_kind
     int rc = launch_linesolve(ctx, op, want_kind, want_dir, du, dt, nx, ny, nz, fp32(ctx));
     if (!rc && ppy) {
         const double *dm = ppy;
-        if (!is_device_ptr(ppy)) {
+        if (const void *r = resident_dev(ctx, ppy, ny * sizeof(double))) {
+            dm = static_cast<const double *>(r);
+        } else if (!is_device_ptr(ppy)) {
             if (ctx->metric_len < ny) {
                 if (ctx->d_metric) cudaFree(ctx->d_metric);
                 ctx->d_metric = nullptr;
@@ -358,6 +373,10 @@ int x3d_ctx_destroy(x3d_ctx ctx)
     ctx->scratch.clear();
     for (auto &b : ctx->staging) cudaFree(b.first);
     ctx->staging.clear();
+    for (auto &r : ctx->resident) cudaFree(r.dev);
+    ctx->resident.clear();
+    if (ctx->step_exec) cudaGraphExecDestroy(ctx->step_exec);
+    if (ctx->step_graph) cudaGraphDestroy(ctx->step_graph);
     if (ctx->d_err) cudaFree(ctx->d_err);
     if (ctx->d_red) cudaFree(ctx->d_red);
     if (ctx->d_metric) cudaFree(ctx->d_metric);
@@ -986,6 +1005,17 @@ int x3d_int_time(x3d_ctx ctx, void *ux1, void *uy1, void *uz1, const void *dux1,
     return sg.finish(launch_axpy3(ctx, fp32(ctx), u, v, w, a, bb, c, gdt, ctx->npts()));
 }
 
+// One timestep on device fields (src/xcompact3d.f90:80-95).
+static int euler_dev(x3d_ctx_s *ctx, void *u[3], void *du[3], double *p, void *px, void *py, void *pz, double dt)
+{
+    const void *uc[3] = {u[0], u[1], u[2]};
+    int rc = momentum_dev(ctx, du, uc, true, dt);             // calculate_transeq_rhs + int_time
+    rc = rc ? rc : divergence_dev(ctx, p, u[0], u[1], u[2]);  // solve_poisson: divergence
+    rc = rc ? rc : poisson_solve(ctx, p);                     //                poisson
+    rc = rc ? rc : gradp_dev(ctx, px, py, pz, p, u);          //                gradp + cor_vel
+    return rc;
+}
+
 int x3d_euler_step(x3d_ctx ctx, void *ux1, void *uy1, void *uz1, void *dux1, void *duy1, void *duz1,
                    double *pp3, void *px1, void *py1, void *pz1, double dt)
 {
@@ -1001,12 +1031,130 @@ int x3d_euler_step(x3d_ctx ctx, void *ux1, void *uy1, void *uz1, void *dux1, voi
     double *p = static_cast<double *>(sg.out(pp3, ctx->npts() * sizeof(double)));
     void *px = sg.out(px1, b), *py = sg.out(py1, b), *pz = sg.out(pz1, b);
     if (sg.status()) return sg.status();
-    const void *uc[3] = {u[0], u[1], u[2]};
-    rc = momentum_dev(ctx, du, uc, true, dt);               // calculate_transeq_rhs + int_time
-    rc = rc ? rc : divergence_dev(ctx, p, u[0], u[1], u[2]);  // solve_poisson: divergence
-    rc = rc ? rc : poisson_solve(ctx, p);                     //                poisson
-    rc = rc ? rc : gradp_dev(ctx, px, py, pz, p, u);          //                gradp + cor_vel
-    return sg.finish(rc);
+    return sg.finish(euler_dev(ctx, u, du, p, px, py, pz, dt));
+}
+
+int x3d_step_capture(x3d_ctx ctx, void *ux1, void *uy1, void *uz1, void *dux1, void *duy1, void *duz1,
+                     double *pp3, void *px1, void *py1, void *pz1, double dt)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if ((rc = need_periodic(ctx))) return rc;
+    if (!ctx->stream || ctx->stream == cudaStreamLegacy || ctx->stream == cudaStreamPerThread)
+        return set_error(ctx, X3D_EUNSUPPORTED, "capture needs the context on a created stream");
+    const size_t b = ctx->npts() * ctx->elem();
+    void *const user[10] = {ux1, uy1, uz1, dux1, duy1, duz1, pp3, px1, py1, pz1};
+    void *dev[10];
+    for (int i = 0; i < 10; ++i) {
+        const size_t bytes = i == 6 ? ctx->npts() * sizeof(double) : b;
+        if (!user[i]) return set_error(ctx, X3D_EINVAL, "null field");
+        dev[i] = resident_dev(ctx, user[i], bytes);
+        if (!dev[i] && is_device_ptr(user[i])) dev[i] = user[i];
+        if (!dev[i]) return set_error(ctx, X3D_EINVAL, "capture needs device or registered fields");
+    }
+    // everything the step allocates on first use, before the capture
+    if (!ctx_scratch(ctx, 5)) return set_error(ctx, X3D_ENOMEM, "scratch allocation failed");
+    if ((rc = poisson_setup(ctx))) return rc;
+    if ((rc = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "capture"))) return rc;
+    if (ctx->step_exec) cudaGraphExecDestroy(ctx->step_exec);
+    if (ctx->step_graph) cudaGraphDestroy(ctx->step_graph);
+    ctx->step_exec = nullptr;
+    ctx->step_graph = nullptr;
+    rc = cuda_check(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    if (rc) return rc;
+    void *u[3] = {dev[0], dev[1], dev[2]}, *du[3] = {dev[3], dev[4], dev[5]};
+    const int work = euler_dev(ctx, u, du, static_cast<double *>(dev[6]), dev[7], dev[8], dev[9], dt);
+    cudaGraph_t g = nullptr;
+    rc = cuda_check(ctx, cudaStreamEndCapture(ctx->stream, &g), "end capture");
+    if (work || rc) {
+        if (g) cudaGraphDestroy(g);
+        return work ? work : rc;
+    }
+    cudaGraphExec_t e = nullptr;
+    if ((rc = cuda_check(ctx, cudaGraphInstantiate(&e, g, 0), "graph instantiate"))) {
+        cudaGraphDestroy(g);
+        return rc;
+    }
+    ctx->step_graph = g;
+    ctx->step_exec = e;
+    return X3D_OK;
+}
+
+int x3d_step_launch(x3d_ctx ctx)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!ctx->step_exec) return set_error(ctx, X3D_EINVAL, "no captured step");
+    return cuda_check(ctx, cudaGraphLaunch(ctx->step_exec, ctx->stream), "graph launch");
+}
+
+// ---- device-resident mirrors ------------------------------------------------------------
+
+int x3d_buf_register(x3d_ctx ctx, void *host, size_t nbytes, void **dev)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!host || !nbytes) return set_error(ctx, X3D_EINVAL, "null or empty host array");
+    if (is_device_ptr(host)) return set_error(ctx, X3D_EINVAL, "already a device pointer");
+    const char *h = static_cast<const char *>(host);
+    for (const auto &r : ctx->resident) {
+        const char *o = static_cast<const char *>(r.host);
+        if (h < o + r.bytes && o < h + nbytes) return set_error(ctx, X3D_EINVAL, "overlaps a registered array");
+    }
+    void *d = nullptr;
+    if (cudaMalloc(&d, nbytes) != cudaSuccess) return set_error(ctx, X3D_ENOMEM, "mirror allocation failed");
+    rc = cuda_check(ctx, cudaMemcpyAsync(d, host, nbytes, cudaMemcpyHostToDevice, ctx->stream), "mirror upload");
+    if (!rc) rc = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "mirror upload");
+    if (rc) {
+        cudaFree(d);
+        return rc;
+    }
+    ctx->resident.push_back({host, d, nbytes});
+    if (dev) *dev = d;
+    return X3D_OK;
+}
+
+static x3d_ctx_s::Resident *find_resident(x3d_ctx_s *ctx, const void *host)
+{
+    for (auto &r : ctx->resident)
+        if (r.host == host) return &r;
+    return nullptr;
+}
+
+int x3d_buf_unregister(x3d_ctx ctx, void *host)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    for (size_t i = 0; i < ctx->resident.size(); ++i)
+        if (ctx->resident[i].host == host) {
+            cudaStreamSynchronize(ctx->stream);
+            cudaFree(ctx->resident[i].dev);
+            ctx->resident.erase(ctx->resident.begin() + i);
+            return X3D_OK;
+        }
+    return set_error(ctx, X3D_EINVAL, "not a registered array");
+}
+
+int x3d_sync_to_device(x3d_ctx ctx, void *host)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    auto *r = find_resident(ctx, host);
+    if (!r) return set_error(ctx, X3D_EINVAL, "not a registered array");
+    rc = cuda_check(ctx, cudaMemcpyAsync(r->dev, r->host, r->bytes, cudaMemcpyHostToDevice, ctx->stream),
+                    "sync to device");
+    return rc ? rc : cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync to device");
+}
+
+int x3d_sync_to_host(x3d_ctx ctx, void *host)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    auto *r = find_resident(ctx, host);
+    if (!r) return set_error(ctx, X3D_EINVAL, "not a registered array");
+    rc = cuda_check(ctx, cudaMemcpyAsync(r->host, r->dev, r->bytes, cudaMemcpyDeviceToHost, ctx->stream),
+                    "sync to host");
+    return rc ? rc : cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync to host");
 }
 
 // ---- mom ----------------------------------------------------------------------------------

@@ -122,6 +122,15 @@ struct x3d_ctx_s {
     double *d_red = nullptr;  // small reduction buffer
     double *d_metric = nullptr;  // device copy of a y stretching metric (ny doubles)
     int metric_len = 0;
+    // host arrays with device-resident mirrors (x3d_buf_register)
+    struct Resident {
+        void *host, *dev;
+        size_t bytes;
+    };
+    std::vector<Resident> resident;
+    // one Euler step recorded by x3d_step_capture
+    cudaGraph_t step_graph = nullptr;
+    cudaGraphExec_t step_exec = nullptr;
     // kernel choice per (direction, grid, precision, operator-group size):
     // filled by the autotuner, default_cfg otherwise
     std::map<std::string, int> tuned;
