@@ -26,9 +26,12 @@
  *  - Every function returns an int status: X3D_OK (0) or a negative code.
  *    The reference aborts through decomp_2d_abort instead; a Fortran shim
  *    maps a non-zero status to that call.
- *  - Only periodic boundary conditions are supported, as in the reference,
- *    whose Poisson solver stops on any other (src/poisson.f90:104-108).
- *    Hence nxm == nx, nym == ny, nzm == nz in the staggered signatures.
+ *  - Boundaries are periodic unless the context is made with
+ *    x3d_ctx_create_bc; then the operators of a non-periodic direction
+ *    exist, nxm = nx - 1 in its staggered signatures, and the Poisson solver
+ *    and Euler-step compositions refuse it, as the reference's Poisson
+ *    solver stops on non-periodic boundaries (src/poisson.f90:104-108).
+ *    Periodic directions have nxm == nx, nym == ny, nzm == nz.
  *  - Line lengths must be >= 8 (the 8-point interpolation stencils).
  */
 #ifndef X3D_B200_H
@@ -106,14 +109,21 @@ int x3d_ctx_create(x3d_ctx *ctx, int nx, int ny, int nz, double xlx, double yly,
 /* x3d_ctx_create with the boundary conditions of src/parameters.f90:
  * ncl[6] = {nclx1, nclxn, ncly1, nclyn, nclz1, nclzn}, each 0 (periodic,
  * both ends of a direction), 1 (free slip) or 2 (Dirichlet); NULL means all
- * periodic.  Along a non-periodic direction nxm = nx - 1 (dx = xlx/(nx-1))
- * and only the first-derivative operators exist: derx (npaire 0) and derxp
- * (npaire 1) use der?_ij (src/x3d_derive.f90:156-215, 343-435, 562-665) with
- * the closures and factors of first_deriv_exp_/first_deriv_imp_
- * (src/x3d_operator_1d.f90:325-488).  The other operators of such a
- * direction, and the Poisson solver and the Euler-step compositions, return
- * X3D_EUNSUPPORTED, as the reference's Poisson solver stops on non-periodic
- * boundaries (src/poisson.f90:104-108). */
+ * periodic.  Along a non-periodic direction nxm = nx - 1 (dx = xlx/(nx-1)):
+ *  - derx (npaire 0) and derxp (npaire 1) use der?_ij (src/x3d_derive.f90:
+ *    156-215, 343-435, 562-665) with the closures and factors of
+ *    first_deriv_exp_/first_deriv_imp_ (src/x3d_operator_1d.f90:325-488);
+ *  - the staggered operators take the factors of interpol_imp_
+ *    (:549-706) with the parities x3d_operator_1d_init binds (:152-189:
+ *    dervp 1, derpv 0, intvp 1, intpv 1) and run the nclx = .false.
+ *    branches of src/x3d_staggered.f90 from an nx-point to an nxm-point
+ *    line or back.  Where the reference has no branch for an operator's
+ *    parity (deryvp npaire 1, :595; der?pv npaire 0, :262, :843, :1199) it
+ *    computes nothing, and the call returns X3D_EUNSUPPORTED;
+ *  - the second derivatives do not exist, and the Poisson solver and the
+ *    Euler-step compositions return X3D_EUNSUPPORTED, as the reference's
+ *    Poisson solver stops on non-periodic boundaries (src/poisson.f90:
+ *    104-108). */
 int x3d_ctx_create_bc(x3d_ctx *ctx, int nx, int ny, int nz, double xlx, double yly, double zlz,
                       int precision, int device, const int *ncl);
 /* finalise_xcompact3d's device-side part (src/x3d_tools.f90:212-248). */
@@ -141,10 +151,14 @@ int x3d_op_builtin(x3d_ctx ctx, int which, x3d_op *op);
 /* An operator from explicit x3doperator1d contents, as the reference host
  * would hand over after its own x3d_operator_1d_init: n, npaire, alfa, the
  * Thomas arrays f, s, w (see prepare, src/x3d_operator_1d.f90:301-323), the
- * Sherman-Morrison vector periodic (NULL for a non-periodic operator), plus
- * the explicit RHS scalars that the reference keeps as module globals of
- * x3d_operator_{x,y,z}_data (rhs[4] = a, b, c, d, e.g. afix, bfix, 0, 0 for
- * derx, aicix6..dicix6 for interpolation).  Host pointers, FP64, copied. */
+ * Sherman-Morrison vector periodic, plus the explicit RHS scalars that the
+ * reference keeps as module globals of x3d_operator_{x,y,z}_data (rhs[4] =
+ * a, b, c, d, e.g. afix, bfix, 0, 0 for derx, aicix6..dicix6 for
+ * interpolation).  periodic = NULL makes a non-periodic staggered operator
+ * (kinds DERVP, DERPV, INTVP, INTPV; n is its output length, nm = nx - 1
+ * for the vp kinds), applied by the staggered routines when nxm = nx - 1;
+ * non-periodic first derivatives come from x3d_ctx_create_bc, which knows
+ * their boundary closures.  Host pointers, FP64, copied. */
 int x3d_op_create(x3d_ctx ctx, int kind, int dir, int n, int npaire, double alfa,
                   const double *f, const double *s, const double *w, const double *periodic,
                   const double *rhs, x3d_op *op);

@@ -60,6 +60,9 @@ def lib() -> ctypes.CDLL:
         L.orc_rhs_scalars.argtypes = [i, d, p]
         L.orc_build_der_np.argtypes = [i, d, i, i, i, p, p, p, p]
         L.orc_apply_der_np.argtypes = [i, p, p, i, i, i, d, i, i, i]
+        L.orc_build_stag_np.argtypes = [i, i, d, i, i, p, p, p, ctypes.POINTER(ctypes.c_int)]
+        L.orc_rhs_scalars.argtypes = [i, d, p]
+        L.orc_apply_stag_np.argtypes = [i, i, p, p, i, i, i, d, i, i, i]
         _lib = L
     return _lib
 
@@ -108,6 +111,48 @@ def der_np(direction: int, u: np.ndarray, d: float, ncl1: int, ncln: int, npaire
                                 int(npaire))
     if rc != 0:
         raise ValueError("oracle: bad non-periodic request")
+    return out
+
+
+def rhs_scalars(kind, d: float) -> dict:
+    """alfa and the explicit RHS scalars a, b, c, d of an operator kind."""
+    out = np.zeros(5)
+    lib().orc_rhs_scalars(_kind(kind), float(d), _p(out))
+    return dict(alfa=out[0], rhs=out[1:5].copy())
+
+
+def lhs_stag_np(kind, n: int, d: float, ncl1: int, ncln: int) -> dict:
+    """Non-periodic staggered LHS for a direction of n velocity points
+    (interpol_imp_): factors f, s, w of its m rows (n - 1 for vp kinds)."""
+    f, s, w = np.zeros(n), np.zeros(n), np.zeros(n)
+    m = ctypes.c_int()
+    rc = lib().orc_build_stag_np(_kind(kind), int(n), float(d), int(ncl1), int(ncln), _p(f), _p(s), _p(w),
+                                 ctypes.byref(m))
+    if rc != 0:
+        raise ValueError("oracle: bad non-periodic staggered request")
+    r = m.value
+    return dict(f=f[:r].copy(), s=s[:r].copy(), w=w[:r].copy(), m=r)
+
+
+def stag_np(kind, direction: int, u: np.ndarray, d: float, ncl1: int, ncln: int, npaire: int) -> np.ndarray:
+    """A staggered routine's non-periodic branch (src/x3d_staggered.f90,
+    nclx = .false.): u on the velocity grid (vp kinds) or the pressure grid
+    (pv kinds, one point fewer along direction); returns the other grid."""
+    k = _kind(kind)
+    u = np.asfortranarray(u, dtype=np.float64)
+    vp = k in (KIND_NAMES["dervp"], KIND_NAMES["intvp"])
+    shape = list(u.shape)
+    vel = list(u.shape)
+    if vp:
+        shape[direction] -= 1
+    else:
+        shape[direction] += 1
+        vel[direction] += 1
+    out = field(tuple(shape))
+    rc = lib().orc_apply_stag_np(k, int(direction), _p(out), _p(u), vel[0], vel[1], vel[2], float(d), int(ncl1),
+                                 int(ncln), int(npaire))
+    if rc != 0:
+        raise ValueError("oracle: no non-periodic branch for this routine and parity")
     return out
 
 

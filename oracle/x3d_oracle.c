@@ -30,9 +30,10 @@
  * The periodic (ncl=0) branches are restated for every operator; of the
  * non-periodic ones, which the reference can only reach without its Poisson
  * solver (it aborts in decomp_2d_poisson_init for them, src/poisson.f90:
- * 104-108), only the first derivatives der?_ij (free slip and Dirichlet ends)
- * are.  Those are pinned by exactness on cubics (Dirichlet closures) and by
- * the analytic derivative of mirrored cosines and sines (free slip).
+ * 104-108), the first derivatives der?_ij (free slip and Dirichlet ends) and
+ * the staggered routines' nclx = .false. branches are.  Those are pinned by
+ * exactness on cubics (Dirichlet closures) and by the analytic derivatives
+ * and interpolants of mirrored cosines (free slip, staggered).
  */
 #include <math.h>
 #include <stdlib.h>
@@ -342,6 +343,147 @@ int orc_apply_der_np(int dir, double *out, const double *in, int nx, int ny, int
         for (int i = 1; i < n; ++i) T(i) = T(i) - T(i - 1) * s[i];          /* thomas.f90:72-80 */
         T(n - 1) = T(n - 1) * w[n - 1];
         for (int i = n - 2; i >= 0; --i) T(i) = (T(i) - f[i] * T(i + 1)) * w[i];
+#undef U
+#undef T
+    }
+    free(f); free(s); free(w);
+    return ORC_OK;
+}
+
+/* Non-periodic staggered LHS (interpol_imp_, x3d_operator_1d.f90:549-706),
+ * for a direction of n velocity points, nm = n - 1, with the arrays that
+ * x3d_operator_1d_init binds (:152-189).  *m receives the row count.
+ *   DERVP: cbx6 ccx6 cfx6 (:576-599), prepared at :677 (before :686-703)
+ *   INTVP: cibx6 cicx6 cifxp6 (= cifx6, :667-670), re-prepared at :697
+ *   DERPV: cbi6 cci6 cfip6 (cfip6(1) = 0, :676), cbi6(nx-1) = 0, :698
+ *   INTPV: cibi6 cici6 cifip6 (= cifi6), re-prepared at :698 */
+int orc_build_stag_np(int kind, int n, double d, int ncl1, int ncln, double *f, double *s, double *w, int *m)
+{
+    if (n < 9 || ncl1 < 1 || ncl1 > 2 || ncln < 1 || ncln > 2) return ORC_EBADARG;
+    double sc[5];
+    orc_rhs_scalars(kind, d, sc);
+    const double al = sc[0];
+    const int vp = kind == ORC_DERVP || kind == ORC_INTVP;
+    if (!vp && kind != ORC_DERPV && kind != ORC_INTPV) return ORC_EBADARG;
+    const int nm = n - 1, r = vp ? nm : n;
+    double *b = calloc(r, sizeof(double)), *c = calloc(r, sizeof(double)), *ff = calloc(r, sizeof(double));
+    if (vp) {  /* cfx6/ccx6/cbx6 (:576-599), cifx6/cicx6/cibx6 (:622-645) */
+        ff[0] = al; ff[1] = al; ff[nm - 3] = al; ff[nm - 2] = al; ff[nm - 1] = 0.0;
+        c[0] = 1.0 + al;  /* nclx1 = 1 or 2 */
+        c[1] = 1.0; c[nm - 3] = 1.0; c[nm - 2] = 1.0;
+        c[nm - 1] = 1.0 + al;  /* nclxn = 1 or 2 */
+        b[0] = al; b[1] = al; b[nm - 3] = al; b[nm - 2] = al; b[nm - 1] = 0.0;
+        for (int i = 2; i <= nm - 4; ++i) { ff[i] = al; c[i] = 1.0; b[i] = al; }
+        if (kind == ORC_INTVP) b[nm - 1] = 0.0;  /* cibx6(nxm) = 0 (:688) */
+    } else {   /* cfi6/cci6/cbi6 (:601-620), cifi6/cici6/cibi6 (:646-665) */
+        ff[0] = al + al; ff[1] = al; ff[n - 3] = al; ff[n - 2] = al; ff[n - 1] = 0.0;
+        c[0] = 1.0; c[1] = 1.0; c[n - 3] = 1.0; c[n - 2] = 1.0; c[n - 1] = 1.0;
+        b[0] = al; b[1] = al; b[n - 3] = al; b[n - 2] = al + al; b[n - 1] = 0.0;
+        for (int i = 2; i <= n - 4; ++i) { ff[i] = al; c[i] = 1.0; b[i] = al; }
+        if (kind == ORC_DERPV) {
+            ff[0] = 0.0;      /* cfip6(1) = 0 (:676) */
+            b[n - 2] = 0.0;   /* cbi6(nx-1) = 0 (:689) */
+        } else {
+            b[n - 1] = 0.0;   /* cibi6(nx) = 0 (:691) */
+        }
+    }
+    for (int i = 0; i < r; ++i) f[i] = ff[i];
+    orc_prepare(b, c, ff, s, w, r);
+    free(b); free(c); free(ff);
+    *m = r;
+    return ORC_OK;
+}
+
+/* Non-periodic branches of the 12 staggered routines, row by row as the
+ * reference writes them (1-based comments), then ?thomas_12.  (nx, ny, nz)
+ * are the velocity-grid extents; along dir the input has n (vp) or n - 1
+ * (pv) points and the output the other.  The branches that exist
+ * (x3d_staggered.f90): derxvp/derzvp npaire 1 (:64, :944) and otherwise (the
+ * odd closure, :83, :968); deryvp npaire 0 only (:595, the odd closure);
+ * the others npaire 1 only.  Returns ORC_EBADARG where there is none. */
+int orc_apply_stag_np(int kind, int dir, double *out, const double *in, int nx, int ny, int nz, double d, int ncl1,
+                      int ncln, int npaire)
+{
+    const int n = dir == ORC_X ? nx : (dir == ORC_Y ? ny : nz);
+    const int vp = kind == ORC_DERVP || kind == ORC_INTVP;
+    int odd = 0;
+    if (kind == ORC_DERVP) {
+        if (dir == ORC_Y) { if (npaire != 0) return ORC_EBADARG; odd = 1; }
+        else odd = npaire != 1;
+    } else if (npaire != 1) {
+        return ORC_EBADARG;
+    }
+    double *f = malloc(sizeof(double) * n), *s = malloc(sizeof(double) * n), *w = malloc(sizeof(double) * n);
+    int m = 0;
+    const int rc = orc_build_stag_np(kind, n, d, ncl1, ncln, f, s, w, &m);
+    if (rc) { free(f); free(s); free(w); return rc; }
+    const int ni = vp ? n : n - 1, nm = n - 1;
+    double sc[5];
+    orc_rhs_scalars(kind, d, sc);
+    const double a = sc[1], b = sc[2], c = sc[3], dd = sc[4];
+    const int o1 = dir == ORC_X ? ny : nx, o2 = dir == ORC_Z ? ny : nz;
+    long st = dir == ORC_X ? 1 : (dir == ORC_Y ? nx : (long)nx * ny);
+    const long nl = (long)o1 * o2;
+#pragma omp parallel for schedule(static)
+    for (long l = 0; l < nl; ++l) {
+        long bi, bo;
+        if (dir == ORC_X) { bi = l * ni; bo = l * m; }
+        else if (dir == ORC_Y) { const long i = l % nx, k = l / nx; bi = i + (long)nx * ni * k; bo = i + (long)nx * m * k; }
+        else { bi = bo = l; }
+        const double *u = in + bi;
+        double *t = out + bo;
+#define U(i) u[(long)((i) - 1) * st]
+#define T(i) t[(long)((i) - 1) * st]
+        if (kind == ORC_DERVP) {       /* derxvp :64-101, deryvp :595-622, derzvp :944-988 */
+            if (!odd) {
+                T(1) = a * (U(2) - U(1)) + b * (U(3) - U(2));
+                T(nm) = a * (U(n) - U(nm)) + b * (U(nm) - U(nm - 1));
+            } else {
+                T(1) = a * (U(2) - U(1)) + b * (U(3) - 2.0 * U(1) + U(2));
+                T(nm) = a * (U(n) - U(nm)) + b * (2.0 * U(n) - U(nm) - U(nm - 1));
+            }
+            T(2) = a * (U(3) - U(2)) + b * (U(4) - U(1));
+            for (int i = 3; i <= nm - 2; ++i) T(i) = a * (U(i + 1) - U(i)) + b * (U(i + 2) - U(i - 1));
+            T(nm - 1) = a * (U(nm) - U(nm - 1)) + b * (U(n) - U(nm - 2));
+        } else if (kind == ORC_INTVP) { /* interxvp :173-206 */
+            T(1) = a * (U(2) + U(1)) + b * (U(3) + U(2)) + c * (U(4) + U(3)) + dd * (U(5) + U(4));
+            T(2) = a * (U(3) + U(2)) + b * (U(4) + U(1)) + c * (U(5) + U(2)) + dd * (U(6) + U(3));
+            T(3) = a * (U(4) + U(3)) + b * (U(5) + U(2)) + c * (U(6) + U(1)) + dd * (U(7) + U(2));
+            for (int i = 4; i <= nm - 3; ++i)
+                T(i) = a * (U(i + 1) + U(i)) + b * (U(i + 2) + U(i - 1)) + c * (U(i + 3) + U(i - 2)) +
+                       dd * (U(i + 4) + U(i - 3));
+            T(nm - 2) = a * (U(nm - 1) + U(nm - 2)) + b * (U(nm) + U(nm - 3)) + c * (U(n) + U(nm - 4)) +
+                        dd * (U(nm) + U(nm - 5));
+            T(nm - 1) = a * (U(nm) + U(nm - 1)) + b * (U(n) + U(nm - 2)) + c * (U(nm) + U(nm - 3)) +
+                        dd * (U(nm - 1) + U(nm - 4));
+            T(nm) = a * (U(n) + U(nm)) + b * (U(nm) + U(nm - 1)) + c * (U(nm - 1) + U(nm - 2)) +
+                    dd * (U(nm - 2) + U(nm - 3));
+        } else if (kind == ORC_DERPV) { /* derxpv :262-277 */
+            T(1) = 0.0;
+            T(2) = a * (U(2) - U(1)) + b * (U(3) - U(1));
+            for (int i = 3; i <= n - 2; ++i) T(i) = a * (U(i) - U(i - 1)) + b * (U(i + 1) - U(i - 2));
+            T(n - 1) = a * (U(n - 1) - U(n - 2)) + b * (U(n - 1) - U(n - 3));
+            T(n) = 0.0;
+        } else {                        /* interxpv :352-397 */
+            T(1) = a * (U(1) + U(1)) + b * (U(2) + U(2)) + c * (U(3) + U(3)) + dd * (U(4) + U(4));
+            T(2) = a * (U(2) + U(1)) + b * (U(3) + U(1)) + c * (U(4) + U(2)) + dd * (U(5) + U(3));
+            T(3) = a * (U(3) + U(2)) + b * (U(4) + U(1)) + c * (U(5) + U(1)) + dd * (U(6) + U(2));
+            T(4) = a * (U(4) + U(3)) + b * (U(5) + U(2)) + c * (U(6) + U(1)) + dd * (U(7) + U(1));
+            for (int i = 5; i <= n - 4; ++i)
+                T(i) = a * (U(i) + U(i - 1)) + b * (U(i + 1) + U(i - 2)) + c * (U(i + 2) + U(i - 3)) +
+                       dd * (U(i + 3) + U(i - 4));
+            T(n - 3) = a * (U(n - 3) + U(n - 4)) + b * (U(n - 2) + U(n - 5)) + c * (U(n - 1) + U(n - 6)) +
+                       dd * (U(n - 1) + U(n - 7));
+            T(n - 2) = a * (U(n - 2) + U(n - 3)) + b * (U(n - 1) + U(n - 4)) + c * (U(n - 1) + U(n - 5)) +
+                       dd * (U(n - 2) + U(n - 6));
+            T(n - 1) = a * (U(n - 1) + U(n - 2)) + b * (U(n - 1) + U(n - 3)) + c * (U(n - 2) + U(n - 4)) +
+                       dd * (U(n - 3) + U(n - 5));
+            T(n) = a * (U(n - 1) + U(n - 1)) + b * (U(n - 2) + U(n - 2)) + c * (U(n - 3) + U(n - 3)) +
+                   dd * (U(n - 4) + U(n - 4));
+        }
+        for (int i = 2; i <= m; ++i) T(i) = T(i) - T(i - 1) * s[i - 1];   /* thomas.f90:72-80 */
+        T(m) = T(m) * w[m - 1];
+        for (int i = m - 1; i >= 1; --i) T(i) = (T(i) - f[i - 1] * T(i + 1)) * w[i - 1];
 #undef U
 #undef T
     }

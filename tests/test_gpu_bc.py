@@ -62,7 +62,7 @@ def test_nonperiodic_context_refuses_what_needs_periodicity(torch_cuda):
     shape = (16, 16, 16)
     ctx = Context(*shape, lengths=(1.0, 1.0, 1.0), bc=(2, 2, 0, 0, 0, 0))
     with pytest.raises(X3DError):
-        ctx.op("derxvp")
+        ctx.op("derxx")  # no non-periodic second derivative
     ctx.op("dery")  # periodic directions keep every operator
     ctx.op("intyvp")
     u = [torch.zeros(shape[::-1], dtype=torch.float64, device="cuda") for _ in range(3)]
@@ -81,3 +81,126 @@ def test_bad_boundary_conditions_are_rejected(torch_cuda):
     for bc in [(0, 1, 0, 0, 0, 0), (3, 3, 0, 0, 0, 0), (1, 1, 0, 0, -1, 0)]:
         with pytest.raises(X3DError):
             Context(16, 16, 16, bc=bc)
+
+
+# ---- non-periodic staggered routines (nclx = .false. branches) -------------
+
+STAG = {0: ("derxvp", "interxvp", "derxpv", "interxpv"),
+        1: ("deryvp", "interyvp", "derypv", "interypv"),
+        2: ("derzvp", "interzvp", "derzpv", "interzpv")}
+KIND_OF = {"der": "dervp", "int": "intvp"}
+
+
+def _kind(routine):
+    base = "der" if routine.startswith("der") else "int"
+    return base + routine[-2:]
+
+
+def _stag_call(ctx, direction, routine, t, u, op, shape):
+    """A staggered routine with the reference's argument order; shape is the
+    velocity grid (nx, ny, nz) and the pressure grid has one point fewer
+    along direction."""
+    nx, ny, nz = shape
+    nm = shape[direction] - 1
+    fn = getattr(ctx, routine)
+    vp = routine.endswith("vp")
+    if direction == 0:
+        fn(t, u, op, *((nx, nm) if vp else (nm, nx)), ny, nz)
+    elif direction == 1:
+        lens = (ny, nm) if vp else (nm, ny)
+        if routine.startswith("der"):
+            fn(t, u, op, None, nx, *lens, nz)
+        else:
+            fn(t, u, op, nx, *lens, nz)
+    else:
+        fn(t, u, op, nx, ny, *((nz, nm) if vp else (nm, nz)))
+
+
+def _grid(shape, direction, pressure):
+    s = list(shape)
+    if pressure:
+        s[direction] -= 1
+    return tuple(s)
+
+
+def _run_stag(oracle, torch, ctx, direction, routine, op, shape, lengths, prec, ncl, npaire):
+    from x3div_b200 import to_device, to_host
+    dt = torch.float64 if prec == "f64" else torch.float32
+    vp = routine.endswith("vp")
+    in_shape = _grid(shape, direction, not vp)
+    out_shape = _grid(shape, direction, vp)
+    u = seeded_field(in_shape, 60 + direction * 7 + len(routine), lengths=lengths, noise=1e-2)
+    d_u = to_device(u, dt)
+    used = to_host(d_u).astype(np.float64)
+    t = torch.full(out_shape[::-1], float("nan"), dtype=dt, device="cuda")
+    _stag_call(ctx, direction, routine, t, d_u, op, shape)
+    ctx.sync()
+    h = lengths[direction] / (shape[direction] - 1)
+    ref = oracle.stag_np(_kind(routine), direction, used, h, ncl[0], ncl[1], npaire)
+    return rel_err(to_host(t), ref)
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("shape", [(20, 18, 16), (12, 10, 9)])
+@pytest.mark.parametrize("ncl", [(1, 1), (2, 1), (2, 2)])
+def test_nonperiodic_staggered_builtins_match_oracle(oracle, torch_cuda, prec, shape, ncl):
+    """The built-in staggered operators of a non-periodic direction, with the
+    parities x3d_operator_1d_init binds (dervp 1, derpv 0, intvp 1, intpv 1):
+    where the reference has a branch for that parity the result matches the
+    oracle; where it has none (deryvp, der?pv) the call is refused."""
+    torch = torch_cuda
+    from x3div_b200 import Context, X3DError
+    tol = 1e-12 if prec == "f64" else 1e-5
+    lengths = (1.0, 2.0, 1.5)
+    for direction in range(3):
+        bc = [0] * 6
+        bc[2 * direction], bc[2 * direction + 1] = ncl
+        ctx = Context(*shape, lengths=lengths, precision=prec, bc=bc)
+        for routine in STAG[direction]:
+            op = ctx.op(routine.replace("inter", "int"))
+            npaire = 0 if routine.startswith("der") and routine.endswith("pv") else 1
+            no_branch = routine.endswith("pv") and routine.startswith("der") or routine == "deryvp"
+            if no_branch:
+                with pytest.raises(X3DError):
+                    _run_stag(oracle, torch, ctx, direction, routine, op, shape, lengths, prec, ncl, npaire)
+                continue
+            err = _run_stag(oracle, torch, ctx, direction, routine, op, shape, lengths, prec, ncl, npaire)
+            assert err < tol, (direction, routine, ncl, err)
+        ctx.close()
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_nonperiodic_staggered_other_parities(oracle, torch_cuda, prec):
+    """The reference's other non-periodic branches, through operators
+    created from the oracle's factors (x3d_op_create, no periodic vector):
+    derxvp/derzvp npaire 0 (the odd closure), deryvp npaire 0 (its only
+    branch) and der?pv npaire 1."""
+    torch = torch_cuda
+    from x3div_b200 import Context, X3DError
+    tol = 1e-12 if prec == "f64" else 1e-5
+    shape = (20, 18, 16)
+    lengths = (1.0, 2.0, 1.5)
+    ncl = (2, 1)
+    for direction in range(3):
+        bc = [0] * 6
+        bc[2 * direction], bc[2 * direction + 1] = ncl
+        ctx = Context(*shape, lengths=lengths, precision=prec, bc=bc)
+        h = lengths[direction] / (shape[direction] - 1)
+        cases = [(STAG[direction][0], "dervp", 0), (STAG[direction][2], "derpv", 1)]
+        for routine, kind, npaire in cases:
+            lhs = oracle.lhs_stag_np(kind, shape[direction], h, *ncl)
+            sc = oracle.rhs_scalars(kind, h)
+            op = ctx.op_create(kind, direction, lhs["m"], npaire, sc["alfa"], lhs["f"], lhs["s"], lhs["w"],
+                               None, sc["rhs"])
+            err = _run_stag(oracle, torch, ctx, direction, routine, op, shape, lengths, prec, ncl, npaire)
+            assert err < tol, (direction, routine, npaire, err)
+            op.close()
+        # the other parity of deryvp has no branch
+        if direction == 1:
+            lhs = oracle.lhs_stag_np("dervp", shape[1], h, *ncl)
+            sc = oracle.rhs_scalars("dervp", h)
+            op = ctx.op_create("dervp", 1, lhs["m"], 1, sc["alfa"], lhs["f"], lhs["s"], lhs["w"], None, sc["rhs"])
+            with pytest.raises(X3DError):
+                _run_stag(oracle, torch, ctx, 1, "deryvp", op, shape, lengths, prec, ncl, 1)
+            op.close()
+        ctx.close()

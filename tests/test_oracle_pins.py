@@ -274,3 +274,81 @@ def test_der_np_factors_solve_the_matrix(oracle):
             for i in range(n - 2, -1, -1):
                 t[i] = (t[i] - f[i] * t[i + 1]) * w[i]
             assert np.allclose(M @ t, r, atol=1e-12)
+
+
+# ---- non-periodic staggered branches (src/x3d_staggered.f90, nclx = .false.) ----
+
+def _stag_errors(oracle, kind, npaire, fun, dfun, n, L=2.0):
+    """Max error of the oracle's kind along x on an n-point velocity grid
+    (walls at 0 and L, nm = n - 1 pressure points at the cell centres)."""
+    d = L / (n - 1)
+    xv = np.arange(n) * d
+    xp = (np.arange(n - 1) + 0.5) * d
+    vp = kind in ("dervp", "intvp")
+    src = fun(xv if vp else xp)
+    exact = (dfun if kind.startswith("der") else fun)(xp if vp else xv)
+    u = np.asfortranarray(np.broadcast_to(src[:, None, None], (src.size, 9, 8)))
+    out = oracle.stag_np(kind, 0, u, d, 2, 1, npaire)
+    return np.abs(out[:, 4, 3] - exact)
+
+
+EVEN = (lambda x: np.cos(np.pi * x / 2.0) + 0.3 * np.cos(3 * np.pi * x / 2.0),
+        lambda x: -np.pi / 2.0 * np.sin(np.pi * x / 2.0) - 0.45 * np.pi * np.sin(3 * np.pi * x / 2.0))
+ODD = (lambda x: np.sin(np.pi * x / 2.0) + 0.2 * np.sin(np.pi * x) + 0.5,
+       lambda x: np.pi / 2.0 * np.cos(np.pi * x / 2.0) + 0.2 * np.pi * np.cos(np.pi * x))
+
+
+@pytest.mark.parametrize("kind,npaire,fields", [("intvp", 1, EVEN), ("intpv", 1, EVEN), ("derpv", 1, EVEN),
+                                                ("dervp", 0, ODD)])
+def test_stag_np_sixth_order_on_mirrored_fields(oracle, kind, npaire, fields):
+    """The npaire 1 branches extend the field evenly about the walls, the odd
+    closure of derxvp (:83-101) oddly about its wall values: on fields with
+    that symmetry every row, boundary rows included, is 6th-order accurate
+    (error ratio 64 per grid doubling; > 40 asserted)."""
+    e1 = _stag_errors(oracle, kind, npaire, *fields, 33).max()
+    e2 = _stag_errors(oracle, kind, npaire, *fields, 65).max()
+    assert e1 < 1e-6 and e1 / e2 > 40, (kind, e1, e2)
+
+
+def test_stag_np_dervp_even_rows(oracle):
+    """derxvp's npaire 1 matrix carries 1 + alfa at its end rows (:579-584)
+    although the derivative of an even field is odd about the wall, so its
+    boundary rows are first order; the error decays away from the walls
+    (the implicit rows damp it by rho = -0.15 per point) and the interior is
+    6th order."""
+    e1 = _stag_errors(oracle, "dervp", 1, *EVEN, 65)
+    e2 = _stag_errors(oracle, "dervp", 1, *EVEN, 129)
+    assert 1.8 < e1.max() / e2.max() < 2.2  # first order at the walls
+    assert e1[24:-24].max() / e2[48:-48].max() > 40  # the same interior points, 6th order
+
+
+def test_stag_np_missing_branches_refused(oracle):
+    u = np.asfortranarray(np.ones((20, 9, 8)))
+    p = np.asfortranarray(np.ones((19, 9, 8)))
+    for kind, field, npaire in (("intvp", u, 0), ("derpv", p, 0), ("intpv", p, 0)):
+        with pytest.raises(ValueError):
+            oracle.stag_np(kind, 0, field, 0.1, 1, 1, npaire)
+    uy = np.asfortranarray(np.ones((9, 20, 8)))
+    with pytest.raises(ValueError):  # deryvp: npaire 0 only (:595)
+        oracle.stag_np("dervp", 1, uy, 0.1, 1, 1, 1)
+    oracle.stag_np("dervp", 1, uy, 0.1, 1, 1, 0)
+
+
+def test_stag_np_factors_solve_the_matrix(oracle):
+    """lhs_stag_np's factors reproduce the interpol_imp_ matrices: solving
+    with them inverts the tridiagonal (b, c, f) assembled from the reference
+    arrays (here for intpv: cibi6, cici6, cifip6 = cifi6)."""
+    n, al = 12, 0.49
+    lhs = oracle.lhs_stag_np("intpv", n, 0.1, 1, 1)
+    m = lhs["m"]
+    f = np.full(m, al); f[0] = 2 * al; f[-1] = 0.0
+    b = np.full(m, al); b[-2] = 2 * al; b[-1] = 0.0
+    A = np.diag(np.ones(m)) + np.diag(f[:-1], 1) + np.diag(b[:-1], -1)
+    r = np.random.default_rng(1).standard_normal(m)
+    z = r.copy()
+    for i in range(1, m):
+        z[i] -= z[i - 1] * lhs["s"][i]
+    z[-1] *= lhs["w"][-1]
+    for i in range(m - 2, -1, -1):
+        z[i] = (z[i] - lhs["f"][i] * z[i + 1]) * lhs["w"][i]
+    assert np.abs(A @ z - r).max() < 1e-13

@@ -173,10 +173,11 @@ class Context:
 
     def op_create(self, kind, direction, n, npaire, alfa, f, s, w, periodic, rhs) -> Operator:
         h = ctypes.c_void_p()
-        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (f, s, w, periodic, rhs)]
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+                for a in (f, s, w, periodic, rhs)]  # periodic None: a non-periodic operator
         kind = KIND[kind] if isinstance(kind, str) else int(kind)
         self._check(self.L.x3d_op_create(self.handle, kind, int(direction), int(n), int(npaire),
-                                         float(alfa), *[a.ctypes.data for a in arrs],
+                                         float(alfa), *[None if a is None else a.ctypes.data for a in arrs],
                                          ctypes.byref(h)))
         return Operator(self, h.value, f"user-{kind}-{direction}", owned=True)
 

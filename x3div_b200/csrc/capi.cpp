@@ -65,8 +65,6 @@ bool is_device_ptr(const void *p)
     return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
-// Host-pointer staging for one call: inputs are uploaded before the work,
-// outputs downloaded after it, and the call then synchronises.
 // The device mirror of [p, p + bytes) when that range lies inside a host
 // array registered with x3d_buf_register, else null.
 void *resident_dev(const x3d_ctx_s *ctx, const void *p, size_t bytes)
@@ -79,6 +77,8 @@ void *resident_dev(const x3d_ctx_s *ctx, const void *p, size_t bytes)
     return nullptr;
 }
 
+// Host-pointer staging for one call: inputs are uploaded before the work,
+// outputs downloaded after it, and the call then synchronises.
 class Stager {
   public:
     explicit Stager(x3d_ctx_s *c) : ctx(c) {}
@@ -171,6 +171,33 @@ int check_ctx(x3d_ctx_s *ctx)
 
 bool fp32(const x3d_ctx_s *ctx) { return ctx->precision == X3D_F32; }
 
+// t(i,j,k) *= ppy(j) for a (nx, ny, nz) device field, ppy a host, device or
+// registered array of ny doubles (the istret /= 0 multiply of dery_00,
+// deryvp and derypv).
+static int scale_by_metric(x3d_ctx_s *ctx, void *dt, const double *ppy, int nx, int ny, int nz)
+{
+    const double *dm = ppy;
+    int rc = X3D_OK;
+    if (const void *r = resident_dev(ctx, ppy, ny * sizeof(double))) {
+        dm = static_cast<const double *>(r);
+    } else if (!is_device_ptr(ppy)) {
+        if (ctx->metric_len < ny) {
+            if (ctx->d_metric) cudaFree(ctx->d_metric);
+            ctx->d_metric = nullptr;
+            ctx->metric_len = 0;
+            if (cudaMalloc(&ctx->d_metric, ny * sizeof(double)) != cudaSuccess)
+                return set_error(ctx, X3D_ENOMEM, "stretching metric allocation failed");
+            ctx->metric_len = ny;
+        }
+        rc = cuda_check(ctx, cudaMemcpyAsync(ctx->d_metric, ppy, ny * sizeof(double), cudaMemcpyHostToDevice,
+                                             ctx->stream),
+                        "stretching metric upload");
+        if (!rc) rc = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "stretching metric upload");
+        dm = ctx->d_metric;
+    }
+    return rc ? rc : launch_scale_y(ctx, fp32(ctx), dt, dm, nx, ny, nz);
+}
+
 // One operator application on (nx,ny,nz) fields along dir; with ppy (a y
 // operator of dery_00/deryvp/derypv given a stretching metric, host or
 // device, ny values) the result is then multiplied by ppy(j).
@@ -193,27 +220,34 @@ int apply_op(x3d_ctx_s *ctx, void *t, const void *u, x3d_op_s *op, int want_kind
     void *dt = sg.out(t, bytes);
     if (sg.status()) return sg.status();
     int rc = launch_linesolve(ctx, op, want_kind, want_dir, du, dt, nx, ny, nz, fp32(ctx));
-    if (!rc && ppy) {
-        const double *dm = ppy;
-        if (const void *r = resident_dev(ctx, ppy, ny * sizeof(double))) {
-            dm = static_cast<const double *>(r);
-        } else if (!is_device_ptr(ppy)) {
-            if (ctx->metric_len < ny) {
-                if (ctx->d_metric) cudaFree(ctx->d_metric);
-                ctx->d_metric = nullptr;
-                ctx->metric_len = 0;
-                if (cudaMalloc(&ctx->d_metric, ny * sizeof(double)) != cudaSuccess)
-                    return sg.finish(set_error(ctx, X3D_ENOMEM, "stretching metric allocation failed"));
-                ctx->metric_len = ny;
-            }
-            rc = cuda_check(ctx, cudaMemcpyAsync(ctx->d_metric, ppy, ny * sizeof(double), cudaMemcpyHostToDevice,
-                                                 ctx->stream),
-                            "stretching metric upload");
-            if (!rc) rc = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "stretching metric upload");
-            dm = ctx->d_metric;
-        }
-        if (!rc) rc = launch_scale_y(ctx, fp32(ctx), dt, dm, nx, ny, nz);
-    }
+    if (!rc && ppy) rc = scale_by_metric(ctx, dt, ppy, nx, ny, nz);
+    return sg.finish(rc);
+}
+
+// A staggered operator along a non-periodic direction (src/x3d_staggered.f90,
+// the nclx = .false. branches): input of n_in points along dir, output of
+// n_out = n_in -/+ 1 (the pressure grid has nxm = nx - 1 points); nx, ny, nz
+// are the velocity-grid extents.  ppy: as in apply_op, for the output's ny.
+int apply_stag_np(x3d_ctx_s *ctx, void *t, const void *u, x3d_op_s *op, int kind, int dir, int n_in, int n_out,
+                  int nx, int ny, int nz, const double *ppy = nullptr)
+{
+    if (!op || !t || !u) return set_error(ctx, X3D_EINVAL, "null operator or field");
+    if (op->h.kind != kind || op->h.dir != dir)
+        return set_error(ctx, X3D_EINVAL, "operator kind/direction does not match the routine");
+    if (op->h.periodic) return set_error(ctx, X3D_EINVAL, "a periodic staggered operator needs nxm = nx");
+    const bool vp = kind == DERVP || kind == INTVP;
+    const int nv = dir == DX ? nx : (dir == DY ? ny : nz);
+    if ((vp ? (n_in != nv || n_out != nv - 1) : (n_out != nv || n_in != nv - 1)) || op->h.n != n_out || nv < 9)
+        return set_error(ctx, X3D_EINVAL, "extents do not match the non-periodic staggered grids");
+    if (t == u) return set_error(ctx, X3D_EINVAL, "t and u must not alias (t is intent(out))");
+    const int o1 = dir == DX ? ny : nx, o2 = dir == DZ ? ny : nz;
+    const size_t es = ctx->elem();
+    Stager sg(ctx);
+    void *du = sg.in(u, (size_t)n_in * o1 * o2 * es);
+    void *dt = sg.out(t, (size_t)n_out * o1 * o2 * es);
+    if (sg.status()) return sg.status();
+    int rc = launch_np_stag(ctx, op, dir, du, dt, n_in, o1, o2, fp32(ctx));
+    if (!rc && ppy) rc = scale_by_metric(ctx, dt, ppy, nx, n_out, nz);
     return sg.finish(rc);
 }
 
@@ -341,6 +375,12 @@ int x3d_ctx_create_bc(x3d_ctx *out, int nx, int ny, int nz, double xlx, double y
         } else if (kNamed[w].kind == DER) {
             // derx (npaire 0) and derxp (npaire 1), x3d_operator_1d_init :140-141
             rc = build_nonperiodic_der(d, nn[d], dd[d], ncl[2 * d], ncl[2 * d + 1], (w & 1) ? 1 : 0, op->h);
+        } else if (kNamed[w].kind != DER2) {
+            // staggered operators with the parities x3d_operator_1d_init binds
+            // (:152-189): derxvp 1, derxpv 0, intxvp 1, intxpv 1
+            const int k = kNamed[w].kind;
+            rc = build_nonperiodic_stag(k, d, nn[d], dd[d], ncl[2 * d], ncl[2 * d + 1], k == DERPV ? 0 : 1,
+                                        op->h);
         } else {
             delete op;  // defined for periodic directions only
             continue;
@@ -460,20 +500,24 @@ int x3d_op_create(x3d_ctx ctx, int kind, int dir, int n, int npaire, double alfa
     if (!out || !f || !s || !w || !rhs) return set_error(ctx, X3D_EINVAL, "null argument");
     if (kind < DER || kind > INTPV || dir < DX || dir > DZ) return set_error(ctx, X3D_EINVAL, "bad kind or direction");
     if (n < 8) return set_error(ctx, X3D_EUNSUPPORTED, "line length must be >= 8");
-    if (!periodic) return set_error(ctx, X3D_EUNSUPPORTED, "only periodic operators are supported");
+    const bool stag = kind == DERVP || kind == DERPV || kind == INTVP || kind == INTPV;
+    if (!periodic && !stag)
+        return set_error(ctx, X3D_EUNSUPPORTED,
+                         "a non-periodic first or second derivative needs its boundary closures (x3d_ctx_create_bc)");
     auto *op = new (std::nothrow) x3d_op_s;
     if (!op) return X3D_ENOMEM;
     op->h.kind = kind;
     op->h.dir = dir;
     op->h.n = n;
     op->h.npaire = npaire;
-    op->h.periodic = 1;
+    op->h.periodic = periodic ? 1 : 0;
     op->h.alfa = alfa;
     op->h.a = rhs[0]; op->h.b = rhs[1]; op->h.c = rhs[2]; op->h.d = rhs[3];
     op->h.f.assign(f, f + n);
     op->h.s.assign(s, s + n);
     op->h.w.assign(w, w + n);
-    op->h.per.assign(periodic, periodic + n);
+    if (periodic) op->h.per.assign(periodic, periodic + n);
+    else op->h.per.clear();
     finish_op(op->h);
     rc = upload_op(op);
     if (rc) {
@@ -544,7 +588,7 @@ int x3d_derzz(x3d_ctx ctx, void *tz, const void *uz, x3d_op op, int nx, int ny, 
         int rc_ = check_ctx(ctx);                                                                   \
         if (rc_) return rc_;                                                                        \
         if ((n_in) != (n_out))                                                                      \
-            return set_error(ctx, X3D_EUNSUPPORTED, "non-periodic staggered grids are not supported"); \
+            return apply_stag_np(ctx, t, u, op, kind, dir, n_in, n_out, nx, ny, nz);                \
         return apply_op(ctx, t, u, op, kind, dir, nx, ny, nz);                                      \
     } while (0)
 
@@ -562,7 +606,7 @@ int x3d_deryvp(x3d_ctx ctx, void *ty, const void *uy, x3d_op op, const double *p
 {
     int rc = check_ctx(ctx);
     if (rc) return rc;
-    if (ny != nym) return set_error(ctx, X3D_EUNSUPPORTED, "non-periodic staggered grids are not supported");
+    if (ny != nym) return apply_stag_np(ctx, ty, uy, op, DERVP, DY, ny, nym, nx, ny, nz, ppyi);
     return apply_op(ctx, ty, uy, op, DERVP, DY, nx, ny, nz, ppyi);
 }
 int x3d_interypv(x3d_ctx ctx, void *ty, const void *uy, x3d_op op, int nx, int nym, int ny, int nz)
@@ -571,7 +615,7 @@ int x3d_derypv(x3d_ctx ctx, void *ty, const void *uy, x3d_op op, const double *p
 {
     int rc = check_ctx(ctx);
     if (rc) return rc;
-    if (ny != nym) return set_error(ctx, X3D_EUNSUPPORTED, "non-periodic staggered grids are not supported");
+    if (ny != nym) return apply_stag_np(ctx, ty, uy, op, DERPV, DY, nym, ny, nx, ny, nz, ppy);
     return apply_op(ctx, ty, uy, op, DERPV, DY, nx, ny, nz, ppy);
 }
 int x3d_derzvp(x3d_ctx ctx, void *tz, const void *uz, x3d_op op, int nx, int ny, int nz, int nzm)

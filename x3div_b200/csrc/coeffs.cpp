@@ -184,6 +184,52 @@ int build_nonperiodic_der(int dir, int n, double d, int ncl1, int ncln, int npai
     return X3D_OK;
 }
 
+// Non-periodic staggered operators: the LHS of interpol_imp_
+// (src/x3d_operator_1d.f90:549-706) for a direction of n velocity points and
+// nm = n - 1 pressure points, with the bindings of x3d_operator_1d_init
+// (:152-189).  The operator's n is its output length m.
+//   DERVP (m = nm): cbx6, ccx6, cfx6 (:576-599), factored at :677, before the
+//     last-end edits;
+//   INTVP (m = nm): cibx6, cicx6 and cifxp6 (a copy of cifx6, :667-670),
+//     factored after cibx6(nxm) = 0 (:688, :697);
+//   DERPV (m = n):  cbi6, cci6 and cfip6 (cfi6 with cfip6(1) = 0, :676),
+//     factored after cbi6(nx-1) = 0 (:689, :698);
+//   INTPV (m = n):  cibi6, cici6 and cifip6 (a copy of cifi6), factored
+//     after cibi6(nx) = 0.  Only cfxp6(1) and cfip6(1) are zeroed (:675-676).
+// The first and last diagonal entries of the nm-point matrices are 1 + alfa
+// for free slip and Dirichlet ends alike (:579-584, :625-630).
+int build_nonperiodic_stag(int kind, int dir, int n, double d, int ncl1, int ncln, int npaire, OpHost &op)
+{
+    if (n < 9 || ncl1 < 1 || ncl1 > 2 || ncln < 1 || ncln > 2) return X3D_EUNSUPPORTED;
+    if (kind != DERVP && kind != INTVP && kind != DERPV && kind != INTPV) return X3D_EINVAL;
+    const bool vp = kind == DERVP || kind == INTVP;
+    const int m = vp ? n - 1 : n;
+    op.kind = kind;
+    op.dir = dir;
+    op.n = m;
+    op.periodic = 0;
+    op.npaire = npaire;
+    op.ncl1 = ncl1;
+    op.ncln = ncln;
+    rhs_scalars(kind, d, &op.alfa, &op.a, &op.b, &op.c, &op.d);
+    const double al = op.alfa;
+    std::vector<double> fb(m, al), fc(m, 1.0), ff(m, al);
+    ff[m - 1] = 0.0;
+    fb[m - 1] = 0.0;
+    if (vp) {
+        fc[0] = 1.0 + al;
+        fc[m - 1] = 1.0 + al;
+    } else {
+        ff[0] = kind == DERPV ? 0.0 : al + al;  // cfi6(1) = 2 alfa; cfip6(1) = 0
+        fb[m - 2] = kind == DERPV ? 0.0 : al + al;  // cbi6(nx-1) = 2 alfa, zeroed for derxpv
+    }
+    op.f = ff;
+    lu_prepare(fb, fc, ff, op.s, op.w);
+    op.per.clear();
+    finish_op(op);
+    return X3D_OK;
+}
+
 // True when an operator's factors are those of the periodic matrix for its
 // alfa (to 1e-12 relative), i.e. when it is the circulant (alfa, 1, alfa).
 static bool circulant(const OpHost &h)

@@ -364,6 +364,80 @@ __global__ void ls_generic(const T *in, T *out, const LineOp<T> op, int nx, int 
 }
 
 // ---------------------------------------------------------------------------
+// Non-periodic staggered operators (the nclx = .false. branches of
+// src/x3d_staggered.f90): one thread per line, from an input line of n_in
+// points to an output line of op.n = n_in -/+ 1 points.  Every boundary row
+// of the reference is the interior stencil applied to a reflected input:
+//   velocity-grid input (vp), npaire 1: u(1-k) = u(1+k), u(n+k) = u(n-k),
+//     a mirror about the end points (the walls);
+//   velocity-grid input, the odd closure of derxvp's other branch (:83-101,
+//     and deryvp's only one, :595-622): u(1-k) = 2 u(1) - u(1+k), likewise
+//     at n;
+//   pressure-grid input (pv), npaire 1: p(1-k) = p(k), p(nm+k) = p(nm+1-k),
+//     a mirror about the walls half a cell outside.
+// E.g. derxvp's tx(1) = a(u(2)-u(1)) + b(u(3)-u(2)) is the interior
+// a(u(i+1)-u(i)) + b(u(i+2)-u(i-1)) with u(0) = u(2), and derxpv's
+// tx(1) = 0 is the interior with p(0) = p(1), p(-1) = p(2).  The solve is the
+// plain Thomas of ?thomas_12 (src/thomas.f90:61-84).  Lines of the other two
+// directions are enumerated as (o1, o2), the input's and output's extents
+// there.
+enum { kReflEven = 0, kReflOdd = 1 };
+
+template <typename T, int KIND>
+__global__ void ls_np_stag(const T *__restrict__ in, T *__restrict__ out, const LineOp<T> op, int n_in, int o1,
+                           int o2, int dir, int refl)
+{
+    constexpr bool VP = KIND == DERVP || KIND == INTVP;
+    const long l = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= (long)o1 * o2) return;
+    const int m = op.n;
+    size_t bi, bo, st;
+    if (dir == DX) {
+        bi = (size_t)l * n_in;
+        bo = (size_t)l * m;
+        st = 1;
+    } else if (dir == DY) {
+        const size_t i = (size_t)(l % o1), k = (size_t)(l / o1);
+        bi = i + (size_t)o1 * n_in * k;
+        bo = i + (size_t)o1 * m * k;
+        st = (size_t)o1;
+    } else {
+        bi = bo = (size_t)l;
+        st = (size_t)o1 * o2;
+    }
+    const T *u = in + bi;
+    T *t = out + bo;
+    auto ld = [&](int k) -> T {
+        if (k >= 0 && k < n_in) return u[(size_t)k * st];
+        if (VP) {
+            const T v = u[(size_t)(k < 0 ? -k : 2 * (n_in - 1) - k) * st];
+            if (refl == kReflOdd) {
+                const T e = u[(size_t)(k < 0 ? 0 : n_in - 1) * st];
+                return (e + e) - v;
+            }
+            return v;
+        }
+        return u[(size_t)(k < 0 ? -1 - k : 2 * n_in - 1 - k) * st];
+    };
+    T v[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) v[k] = ld(k - 4);
+    T z = T(0);
+    for (int i = 0; i < m; ++i) {
+        z = stencil<KIND>(v, op) - ldg(op.s + i) * z;
+        t[(size_t)i * st] = z;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] = v[k + 1];
+        v[8] = ld(i + 5);
+    }
+    T y = T(0);
+    for (int i = m - 1; i >= 0; --i) {
+        y = t[(size_t)i * st] * ldg(op.w + i) - ldg(op.fw + i) * y;
+        t[(size_t)i * st] = y;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Host side.
 
 static PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
@@ -573,6 +647,57 @@ int autotune_group(x3d_ctx_s *ctx, int dir, const void *in, const x3d_op_s *cons
     ctx->tuned[tune_key(dir, nx, ny, nz, fp32, nops)] = best;
     if (best_ms) *best_ms = bt / reps;
     return X3D_OK;
+}
+
+// Which non-periodic branches the reference has (src/x3d_staggered.f90):
+// derxvp and derzvp one for npaire 1 and one for the rest (:64, :944),
+// deryvp only the odd one, for npaire 0 (:595); every other staggered
+// routine only npaire 1.  Without a branch the reference computes nothing;
+// here the call returns X3D_EUNSUPPORTED.
+int launch_np_stag(x3d_ctx_s *ctx, const x3d_op_s *op, int dir, const void *in, void *out, int n_in, int o1, int o2,
+                   bool fp32)
+{
+    const int kind = op->h.kind, np = op->h.npaire;
+    int refl = kReflEven;
+    if (kind == DERVP) {
+        if (dir == DY) {
+            if (np != 0)
+                return set_error(ctx, X3D_EUNSUPPORTED,
+                                 "deryvp has a non-periodic branch for npaire 0 only (src/x3d_staggered.f90:595)");
+            refl = kReflOdd;
+        } else {
+            refl = np == 1 ? kReflEven : kReflOdd;
+        }
+    } else if (np != 1) {
+        return set_error(ctx, X3D_EUNSUPPORTED,
+                         "this staggered routine has a non-periodic branch for npaire 1 only (src/x3d_staggered.f90)");
+    }
+    const long nl = (long)o1 * o2;
+    const int bs = 128;
+    const unsigned grid = (unsigned)((nl + bs - 1) / bs);
+    auto go = [&](auto kern, const auto *i, auto *o, const auto &lo) {
+        ++ctx->launches;
+        kern<<<grid, bs, 0, ctx->stream>>>(i, o, lo, n_in, o1, o2, dir, refl);
+        return cuda_check(ctx, cudaGetLastError(), "ls_np_stag launch");
+    };
+    if (fp32) {
+        const float *i = static_cast<const float *>(in);
+        float *o = static_cast<float *>(out);
+        switch (kind) {
+        case DERVP: return go(ls_np_stag<float, DERVP>, i, o, op->opf);
+        case INTVP: return go(ls_np_stag<float, INTVP>, i, o, op->opf);
+        case DERPV: return go(ls_np_stag<float, DERPV>, i, o, op->opf);
+        default: return go(ls_np_stag<float, INTPV>, i, o, op->opf);
+        }
+    }
+    const double *i = static_cast<const double *>(in);
+    double *o = static_cast<double *>(out);
+    switch (kind) {
+    case DERVP: return go(ls_np_stag<double, DERVP>, i, o, op->opd);
+    case INTVP: return go(ls_np_stag<double, INTVP>, i, o, op->opd);
+    case DERPV: return go(ls_np_stag<double, DERPV>, i, o, op->opd);
+    default: return go(ls_np_stag<double, INTPV>, i, o, op->opd);
+    }
 }
 
 }  // namespace x3d

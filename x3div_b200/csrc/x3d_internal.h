@@ -152,6 +152,9 @@ void rhs_scalars(int kind, double d, double *alfa, double *a, double *b, double 
 int build_periodic_op(int kind, int dir, int n, double d, OpHost &op);
 // Non-periodic first derivative: ncl1, ncln in {1, 2}, npaire 0 or 1.
 int build_nonperiodic_der(int dir, int n, double d, int ncl1, int ncln, int npaire, OpHost &op);
+int build_nonperiodic_stag(int kind, int dir, int n, double d, int ncl1, int ncln, int npaire, OpHost &op);
+int launch_np_stag(x3d_ctx_s *ctx, const x3d_op_s *op, int dir, const void *in, void *out, int n_in, int o1, int o2,
+                   bool fp32);
 void finish_op(OpHost &op);  // computes g, den, glen from f, s, w, per
 int upload_op(x3d_op_s *op);
 void free_op(x3d_op_s *op);
