@@ -165,17 +165,42 @@ __device__ __forceinline__ void dft(double2 (&v)[R])
     }
 }
 
+// Where a stage reads and writes: the tile in shared memory, or (first
+// forward stage) the spectrum's z lines in global memory and (last inverse
+// stage) back to them; the last forward stage also divides each mode.
+struct ZLines {
+    double2 *base;   // the tile's first line at k = 0
+    size_t zstride;  // elements between consecutive k
+    int lines;       // x modes of the tile inside the spectrum (<= W)
+    int i0, nxh;
+    double tyj, k2yj, ntot;
+    const double *__restrict__ tx, *__restrict__ k2x, *__restrict__ tz, *__restrict__ k2z;
+    // c <- -c / (K ntot), zero where K < 1e-16: the K and mask of
+    // k_spectral_divide for mode (i0 + l, j, k)
+    __device__ __forceinline__ double2 divide(double2 v, int k, int l) const
+    {
+        const int i = min(i0 + l, nxh - 1);
+        const double txi = __ldg(tx + i), tzk = __ldg(tz + k);
+        const double tyz = tyj * tzk, txz = txi * tzk, txy = txi * tyj;
+        const double kk = __ldg(k2x + i) * (tyz * tyz) + k2yj * (txz * txz) + __ldg(k2z + k) * (txy * txy);
+        const double f = kk < 1.e-16 ? 0.0 : -1.0 / (kk * ntot);
+        return make_double2(v.x * f, v.y * f);
+    }
+};
+
 // One Stockham stage of radix R over sub-transforms of size NS, for the W
-// lines of the tile (element e of line l at buf[e W + l]).
-template <int N, int R, int NS, int W, bool INV>
-__device__ __forceinline__ void zft_stage(double2 *buf, const double2 *tw)
+// lines of the tile (element e of line l at buf[e W + l]).  SRC_G: read the
+// lines from global memory; DST_G: write them to global memory; SCALE:
+// divide each mode as it is written.
+template <int N, int R, int NS, int W, bool INV, bool SRC_G, bool DST_G, bool SCALE>
+__device__ __forceinline__ void zft_stage(double2 *buf, const double2 *tw, const ZLines &zl)
 {
     constexpr int MB = kZftVals / R;
     constexpr int NB = W * (N / R);
     constexpr int STRIDE = N / (NS * R);
     static_assert(NB <= MB * kZftThreads, "tile too large for one pass of the stage");
     double2 v[MB][R];
-    int dst[MB];
+    int dk[MB], dl[MB];
 #pragma unroll
     for (int s = 0; s < MB; ++s) {
         const int b = threadIdx.x + s * kZftThreads;
@@ -184,7 +209,12 @@ __device__ __forceinline__ void zft_stage(double2 *buf, const double2 *tw)
             const int jm = j % NS;
 #pragma unroll
             for (int q = 0; q < R; ++q) {
-                const double2 x = buf[(j + q * (N / R)) * W + l];
+                const int k = j + q * (N / R);
+                double2 x;
+                if constexpr (SRC_G)
+                    x = l < zl.lines ? zl.base[(size_t)k * zl.zstride + l] : make_double2(0.0, 0.0);
+                else
+                    x = buf[k * W + l];
                 if (q == 0) {
                     v[s][q] = x;
                 } else {
@@ -194,19 +224,29 @@ __device__ __forceinline__ void zft_stage(double2 *buf, const double2 *tw)
                 }
             }
             dft<R, INV>(v[s]);
-            dst[s] = ((j / NS) * NS * R + jm) * W + l;
+            dk[s] = (j / NS) * NS * R + jm;
+            dl[s] = l;
         }
     }
-    __syncthreads();
+    if constexpr (!SRC_G && !DST_G) __syncthreads();  // in place in shared memory
 #pragma unroll
     for (int s = 0; s < MB; ++s) {
         const int b = threadIdx.x + s * kZftThreads;
         if (b < NB) {
 #pragma unroll
-            for (int q = 0; q < R; ++q) buf[dst[s] + q * NS * W] = v[s][q];
+            for (int q = 0; q < R; ++q) {
+                const int k = dk[s] + q * NS, l = dl[s];
+                if constexpr (DST_G) {
+                    if (l < zl.lines) zl.base[(size_t)k * zl.zstride + l] = v[s][q];
+                } else if constexpr (SCALE) {
+                    buf[k * W + l] = zl.divide(v[s][q], k, l);
+                } else {
+                    buf[k * W + l] = v[s][q];
+                }
+            }
         }
     }
-    __syncthreads();
+    if constexpr (!DST_G) __syncthreads();
 }
 
 // Radices of a length-N transform: 8s, 4, 2, then 3s.
@@ -225,14 +265,18 @@ constexpr RadixSeq radix_seq(int n)
     return s;
 }
 
+// The forward transform reads the lines from global memory in its first
+// stage and divides the modes in its last; the inverse one writes them back
+// to global memory in its last stage.
 template <int N, int W, bool INV, int ST = 0, int NS = 1>
-__device__ __forceinline__ void zft(double2 *buf, const double2 *tw)
+__device__ __forceinline__ void zft(double2 *buf, const double2 *tw, const ZLines &zl)
 {
     constexpr RadixSeq seq = radix_seq(N);
     if constexpr (ST < seq.count) {
         constexpr int R = seq.r[ST];
-        zft_stage<N, R, NS, W, INV>(buf, tw);
-        zft<N, W, INV, ST + 1, NS * R>(buf, tw);
+        constexpr bool last = ST + 1 == seq.count;
+        zft_stage<N, R, NS, W, INV, !INV && ST == 0, INV && last, !INV && last>(buf, tw, zl);
+        zft<N, W, INV, ST + 1, NS * R>(buf, tw, zl);
     }
 }
 
@@ -241,10 +285,10 @@ template <int N>
 constexpr int kZftW = N <= 256 ? 16 : (N <= 512 ? 8 : 4);
 
 // One CTA per (j, tile of W x-modes): z transform, c <- -c / (K ntot) with the
-// K and mask of k_spectral_divide, inverse z transform.  The tile's loads
-// and stores, and the mode scalings, run as compile-time loops of PER values
-// per thread, so each thread has all its global loads in flight at once; the
-// twiddles are copied into shared memory first.
+// K and mask of k_spectral_divide, inverse z transform.  The tile's modes go
+// from global memory straight into the first stage's registers and leave
+// the last inverse stage straight to global memory; the twiddles are copied
+// into shared memory first.
 template <int N>
 __global__ void __launch_bounds__(kZftThreads, 2)
     k_poisson_z(double2 *__restrict__ c, int nxh, int ny, const double2 *__restrict__ tw,
@@ -253,58 +297,28 @@ __global__ void __launch_bounds__(kZftThreads, 2)
                 double ntot)
 {
     constexpr int W = kZftW<N>;
-    constexpr int PER = (N * W + kZftThreads - 1) / kZftThreads;
     extern __shared__ __align__(16) double2 zbuf[];
     double2 *const tws = zbuf + N * W;
     const int tiles_i = (nxh + W - 1) / W;
     const int j = blockIdx.x / tiles_i;
     const int i0 = (blockIdx.x - j * tiles_i) * W;
-    const int lines = min(W, nxh - i0);
-    const size_t zstride = (size_t)ny * nxh;
-    double2 *const base = c + (size_t)j * nxh + i0;
+    ZLines zl;
+    zl.base = c + (size_t)j * nxh + i0;
+    zl.zstride = (size_t)ny * nxh;
+    zl.lines = min(W, nxh - i0);
+    zl.i0 = i0;
+    zl.nxh = nxh;
+    zl.tyj = __ldg(ty + j);
+    zl.k2yj = __ldg(k2y + j);
+    zl.ntot = ntot;
+    zl.tx = tx;
+    zl.k2x = k2x;
+    zl.tz = tz;
+    zl.k2z = k2z;
     for (int t = threadIdx.x; t < N; t += kZftThreads) tws[t] = __ldg(tw + t);
-    {
-        double2 v[PER];
-#pragma unroll
-        for (int s = 0; s < PER; ++s) {
-            const int e = threadIdx.x + s * kZftThreads;
-            const int k = e / W, l = e % W;
-            v[s] = e < N * W && l < lines ? base[(size_t)k * zstride + l] : make_double2(0.0, 0.0);
-        }
-#pragma unroll
-        for (int s = 0; s < PER; ++s) {
-            const int e = threadIdx.x + s * kZftThreads;
-            if (e < N * W) zbuf[e] = v[s];
-        }
-    }
     __syncthreads();
-    zft<N, W, false>(zbuf, tws);
-    const double tyj = __ldg(ty + j), k2yj = __ldg(k2y + j);
-#pragma unroll
-    for (int s = 0; s < PER; ++s) {
-        const int e = threadIdx.x + s * kZftThreads;
-        if (e < N * W) {
-            const int k = e / W, l = e % W;
-            const int i = min(i0 + l, nxh - 1);
-            const double txi = __ldg(tx + i), tzk = __ldg(tz + k);
-            const double tyz = tyj * tzk, txz = txi * tzk, txy = txi * tyj;
-            const double kk =
-                __ldg(k2x + i) * (tyz * tyz) + k2yj * (txz * txz) + __ldg(k2z + k) * (txy * txy);
-            const double f = kk < 1.e-16 ? 0.0 : -1.0 / (kk * ntot);
-            double2 v = zbuf[e];
-            v.x *= f;
-            v.y *= f;
-            zbuf[e] = v;
-        }
-    }
-    __syncthreads();
-    zft<N, W, true>(zbuf, tws);
-#pragma unroll
-    for (int s = 0; s < PER; ++s) {
-        const int e = threadIdx.x + s * kZftThreads;
-        const int k = e / W, l = e % W;
-        if (e < N * W && l < lines) base[(size_t)k * zstride + l] = zbuf[e];
-    }
+    zft<N, W, false>(zbuf, tws, zl);
+    zft<N, W, true>(zbuf, tws, zl);
 }
 
 // The z lengths with a fused kernel.
