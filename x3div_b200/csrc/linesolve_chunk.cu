@@ -366,17 +366,16 @@ __device__ __forceinline__ void load_resp(const StageProgram<S> &prog, V *dst)
 // the shared-memory copy as 16-byte vectors, so each fix is one fused
 // multiply-add per carry and half a load per point.
 template <typename T, int L, typename Load, typename S>
-__device__ __forceinline__ void chunk_solve_resp(const StageOp<S> &so, const T *resp, const Load &load,
+__device__ __forceinline__ void chunk_solve_resp(const LineOp<S> &op, int kind, const T *resp, const Load &load,
                                                  T (&r)[L], const ChunkScratch<T> &sc, int W, int l, int c,
                                                  int C, int nv, int q)
 {
     constexpr int ti = L == kChunkLong<S> ? 0 : 1;
     // operator fields into registers once (the parameters are read through
     // a generic pointer, and would be read again after every barrier)
-    const LineOp<S> &op = so.op;
     const T rho = T(op.rho), mf = T(op.mfull[ti]), ml = T(op.mlast[ti]), wrap = T(op.wrap);
     const int K = op.depth[ti];
-    chunk_rhs<T, L, 2>(so.kind, load, r, op);
+    chunk_rhs<T, L, 2>(kind, load, r, op);
     // local forward sweep; the chunk's end value goes straight to shared
     // memory (for a short last chunk, the value at point nv - 1, captured in
     // the sweep: selecting it from r afterwards would index r at run time
@@ -752,7 +751,7 @@ __global__ void __launch_bounds__(kStageThreads<T, L, PR>, 1)
                     for (int j = 0; j < NW; ++j) w[j] = at(ca + (J0 + j) * W);
                 }
             };
-            chunk_solve_resp<V, L>(so, resp_s + k * 4 * L, load, r, sc, WP, l, c, C, nv, c * WP + l);
+            chunk_solve_resp<V, L>(so.op, so.kind, resp_s + k * 4 * L, load, r, sc, WP, l, c, C, nv, c * WP + l);
             if constexpr (ACC) {
                 accumulate<V, L, 1>(so, acc, r, nv, tile_at);
                 if (so.flush && live) flush_yz<T, V, L, true>(flush_args(so), acc, obase, ostride, nv);
@@ -1106,7 +1105,7 @@ __global__ void __launch_bounds__(512, 1)
             // the previous operator's row copies must have read the staging
             // rows before anyone writes them again (after this solve's barriers)
             if (t < W) bulk_wait_read_all();
-            chunk_solve_resp<T, L>(so, resp_s + k * 4 * L, load, r, sc, W, l, c, C, nv, c * W + l);
+            chunk_solve_resp<T, L>(so.op, so.kind, resp_s + k * 4 * L, load, r, sc, W, l, c, C, nv, c * W + l);
             if constexpr (ACC) {
                 accumulate<T, L, V>(so, acc, r, nv, tile_at);
                 if (so.flush) flush_x_staged<T, L, true>(flush_args(so), acc, out_s, l, l0, rows, pitch, n, cs, nv);
@@ -1159,31 +1158,34 @@ static unsigned persistent_grid(x3d_ctx_s *ctx, Kern kern, int threads, size_t s
 // points: h_j = rho^(j+1) sum_{i < len-j} rho^(2i) and g_j = rho^(len-j),
 // len = L (resp[0..1]) and len = the last chunk's length (resp[2..3]).
 template <typename T>
-static void fill_resp(StageProgram<T> &p, int L, int n)
+static void fill_op_resp(T (&resp)[4][kChunkLong<T>], double al, int L, int n)
 {
     const int C = (n + L - 1) / L, last = n - (C - 1) * L;
-    for (int k = 0; k < p.nops; ++k) {
-        const double al = p.ops[k].op.alfa;
-        const double rho = al == 0.0 ? 0.0 : -2.0 * al / (1.0 + std::sqrt(1.0 - 4.0 * al * al));
-        double pw[kChunkLong<T>];
-        double q = 1.0;
-        for (int j = 0; j < kChunkLong<T>; ++j) pw[j] = (q *= rho);  // rho^(j+1)
-        auto fill = [&](T *h, T *g, int len) {
-            double S = 0.0, G = 1.0;
-            for (int j = kChunkLong<T> - 1; j >= 0; --j) {
-                if (j >= len) {
-                    h[j] = g[j] = T(0);
-                    continue;
-                }
-                S = 1.0 + rho * rho * S;
-                G *= rho;
-                h[j] = (T)(pw[j] * S);
-                g[j] = (T)G;
+    const double rho = al == 0.0 ? 0.0 : -2.0 * al / (1.0 + std::sqrt(1.0 - 4.0 * al * al));
+    double pw[kChunkLong<T>];
+    double q = 1.0;
+    for (int j = 0; j < kChunkLong<T>; ++j) pw[j] = (q *= rho);  // rho^(j+1)
+    auto fill = [&](T *h, T *g, int len) {
+        double S = 0.0, G = 1.0;
+        for (int j = kChunkLong<T> - 1; j >= 0; --j) {
+            if (j >= len) {
+                h[j] = g[j] = T(0);
+                continue;
             }
-        };
-        fill(p.ops[k].resp[0], p.ops[k].resp[1], L);
-        fill(p.ops[k].resp[2], p.ops[k].resp[3], last);
-    }
+            S = 1.0 + rho * rho * S;
+            G *= rho;
+            h[j] = (T)(pw[j] * S);
+            g[j] = (T)G;
+        }
+    };
+    fill(resp[0], resp[1], L);
+    fill(resp[2], resp[3], last);
+}
+
+template <typename T>
+static void fill_resp(StageProgram<T> &p, int L, int n)
+{
+    for (int k = 0; k < p.nops; ++k) fill_op_resp(p.ops[k].resp, p.ops[k].op.alfa, L, n);
 }
 
 // PR = 2: the paired y/z kernel (FP32 only).
@@ -1387,23 +1389,27 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
     if (t == 0) {
         mbar_init(&bar, 1);
         fence_mbar_init();
+        s_item = (long)atomicAdd(counter, 1ull);
     }
     __syncthreads();
     uint32_t phase = 0;
     T *tile = reinterpret_cast<T *>(smem_raw);
     const ChunkScratch<T> scf = carve_scratch<T>(smem_raw + tile_cap, kBatchThreads / 1, 1);
-    for (;;) {
-        if (t == 0) s_item = (long)atomicAdd(counter, 1ull);
-        __syncthreads();
-        const long item = s_item;
-        if (item >= total) break;
+    T *resp_s = reinterpret_cast<T *>(smem_raw + tile_cap +
+                                      (((size_t)2 * kBatchThreads * sizeof(T) + 15) & ~(size_t)15));
+    auto job_of = [&](long item) {
         int lo = 0, hi = njobs - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
             if (jobs[mid].tile0 <= item) lo = mid;
             else hi = mid - 1;
         }
-        const BatchJob<T> &J = jobs[lo];
+        return lo;
+    };
+    for (;;) {
+        const long item = s_item;  // claimed during the previous item (or above)
+        if (item >= total) break;
+        const BatchJob<T> &J = jobs[job_of(item)];
         const long tl = item - J.tile0;
         const int W = J.W, C = J.C, n = J.n;
         const int dir = J.dir;
@@ -1441,6 +1447,34 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
             return;
         }
         phase ^= 1;
+        // every thread is done with the previous item's responses (read
+        // after its last barrier): this item's go in their place
+        for (int i = t; i < J.nops * 4 * L; i += kBatchThreads) {
+            const int k = i / (4 * L), rem = i - k * 4 * L, a = rem / L, j = rem - a * L;
+            resp_s[i] = J.resp[k][a][j];
+        }
+        // every thread has read s_item: claim the next item now and start
+        // moving its lines into L2 while this one is solved
+        if (t == 0) {
+            const long next = (long)atomicAdd(counter, 1ull);
+            s_item = next;
+            if (next < total) {
+                const BatchJob<T> &N = jobs[job_of(next)];
+                const long tn = next - N.tile0;
+                if (N.dir == DX) {
+                    const long nl0 = tn * N.W;
+                    const int nrows = (int)min((long)N.W, N.span - nl0);
+                    bulk_prefetch(N.in + (size_t)nl0 * N.n, (uint32_t)((size_t)nrows * N.n * sizeof(T)));
+                } else {
+                    const int nx0 = (int)(tn % N.span) * N.W, no = (int)(tn / N.span);
+                    fence_tensormap_acquire(&N.tmap);
+                    for (int b = 0; b < N.nbox; ++b) {
+                        if (N.dir == DY) tma_prefetch_3d(&N.tmap, nx0, b * N.box_n, no);
+                        else tma_prefetch_3d(&N.tmap, nx0, no, b * N.box_n);
+                    }
+                }
+            }
+        }
         if (dir == DX) fill_halos_x<T>(smem_raw, 0, 1, rows, J.pitch, n);
         else fill_halos_yz<T>(smem_raw, 0, 1, n, W, J.halo);
         fence_proxy_async_smem();  // the next item's copies overwrite the halos
@@ -1467,7 +1501,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
                 }
             };
             for (int k = 0; k < J.nops; ++k) {
-                chunk_solve<T, L>(J.op[k], J.kind[k], load, r, sc, W, l, c, C, nv, q);
+                chunk_solve_resp<T, L>(J.op[k], J.kind[k], resp_s + k * 4 * L, load, r, sc, W, l, c, C, nv, q);
                 if (active && l < rows) {
                     T *dst = J.out[k] + (size_t)(l0 + l) * n + cs;
 #pragma unroll
@@ -1496,7 +1530,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
                                  (dir == DY ? (size_t)J.nx * J.ny * o : (size_t)J.nx * o) +
                                  (size_t)cs * ostride;
             for (int k = 0; k < J.nops; ++k) {
-                chunk_solve<T, L>(J.op[k], J.kind[k], load, r, sc, W, l, c, C, nv, q);
+                chunk_solve_resp<T, L>(J.op[k], J.kind[k], resp_s + k * 4 * L, load, r, sc, W, l, c, C, nv, q);
                 if (live) {
                     T *dst = J.out[k] + obase;
 #pragma unroll
@@ -1522,6 +1556,7 @@ bool plan_batch_job(BatchJob<T> &J, int L, size_t *tile_bytes)
     constexpr int V = Vec4<T>::N;
     for (int k = 0; k < J.nops; ++k)
         if (!J.op[k].circ || J.op[k].n != n) return false;
+    for (int k = 0; k < J.nops; ++k) fill_op_resp(J.resp[k], J.op[k].alfa, L, n);
     J.C = (n + L - 1) / L;
     if (J.C > kBatchThreads) return false;
     int W = kBatchThreads / J.C;
@@ -1568,10 +1603,12 @@ bool plan_batch_job(BatchJob<T> &J, int L, size_t *tile_bytes)
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Carry scratch, then the carry responses of the item's operators.
 template <typename T>
 size_t batch_scratch_bytes()
 {
-    return ((size_t)2 * kBatchThreads * sizeof(T) + 15) & ~(size_t)15;
+    return (((size_t)2 * kBatchThreads * sizeof(T) + 15) & ~(size_t)15) +
+           (size_t)kMaxStageOps * 4 * kChunkLong<T> * sizeof(T);
 }
 
 template <typename T>

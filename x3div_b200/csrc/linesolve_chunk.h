@@ -82,6 +82,9 @@ struct BatchJob {
     long span;   // x: number of lines; y/z: tiles across x
     long tile0;  // first work item of the job
     long ntiles;
+    // carry responses of each operator for the batch's chunk length (as
+    // StageOp::resp; set by plan_batch_job)
+    T resp[kMaxStageOps][4][kChunkLong<T>];
 };
 
 // Chooses tiling for the job (chunk length L) and encodes its tensor map;
