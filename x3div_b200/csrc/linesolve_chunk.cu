@@ -252,77 +252,6 @@ __device__ __forceinline__ T chunk_carry(const T *e, int K, T mf, T ml, T wrap, 
     return full ? carry * wrap : carry;
 }
 
-// Solves one operator for one chunk; the solved values end in r[] (chunk
-// local).  load(w, J0) fills a window u[cs+J0-4 ...] of the size of w from the
-// staged line and its periodic halos; the window is dead once the stencil is
-// evaluated.  nv = points of the chunk inside the line (L except for the last
-// chunk of a ragged line; the window values past its end are never used).
-template <typename T, int L, typename Load>
-__device__ __forceinline__ void chunk_solve(const LineOp<T> &op, int kind, const Load &load, T (&r)[L],
-                                            const ChunkScratch<T> &sc, int W, int l, int c, int C, int nv,
-                                            int q)
-{
-    constexpr int ti = L == kChunkLong<T> ? 0 : 1;
-    chunk_rhs<T, L, 1>(kind, load, r, op);
-    const T rho = op.rho;
-    T v = T(0);
-    if (nv == L) {
-#pragma unroll
-        for (int j = 0; j < L; ++j) {
-            v = fma(rho, v, r[j]);
-            r[j] = v;
-        }
-        sc.fz[q] = v;
-    } else {  // ragged last chunk: its end is point nv - 1 (captured in the sweep)
-#pragma unroll
-        for (int j = 0; j < L; ++j) {
-            v = fma(rho, v, r[j]);
-            if (j + 1 == nv) sc.fz[q] = v;
-            r[j] = v;
-        }
-    }
-    __syncthreads();
-    // forward carry (v just before the chunk), fix, local backward sweep
-    {
-        T pw = chunk_carry<T, 1>(sc.fz, op.depth[ti], op.mfull[ti], op.mlast[ti], op.wrap, W, l, c, C);
-#pragma unroll
-        for (int j = 0; j < L; ++j) {
-            pw *= rho;
-            r[j] += pw;
-        }
-    }
-    if (nv < L) {
-#pragma unroll
-        for (int j = 0; j < L; ++j)
-            if (j >= nv) r[j] = T(0);
-    }
-    T y = T(0);
-#pragma unroll
-    for (int j = L - 1; j >= 0; --j) {
-        y = fma(rho, y, r[j]);
-        r[j] = y;
-    }
-    sc.bz[q] = y;
-    __syncthreads();
-    // backward carry (y just after the chunk's last point) and fix
-    T pw = chunk_carry<T, -1>(sc.bz, op.depth[ti], op.mfull[ti], op.mlast[ti], op.wrap, W, l, c, C);
-    if (nv == L) {
-#pragma unroll
-        for (int j = L - 1; j >= 0; --j) {
-            pw *= rho;
-            r[j] += pw;
-        }
-    } else {
-#pragma unroll
-        for (int j = L - 1; j >= 0; --j) {
-            if (j < nv) {
-                pw *= rho;
-                r[j] += pw;
-            }
-        }
-    }
-}
-
 // 16-byte vector of T.
 template <typename T>
 struct Vec4;
@@ -354,9 +283,13 @@ __device__ __forceinline__ void load_resp(const StageProgram<S> &prog, V *dst)
     }
 }
 
-// The same solve with the carry fixes folded into two precomputed responses.
-// Both local sweeps run before the first barrier (the backward one on the
-// local forward values), and since the solve is linear,
+// Solves one operator for one chunk; the solved values end in r[] (chunk
+// local).  load(w, J0) fills a window u[cs+J0-4 ...] of the size of w from the
+// staged line and its periodic halos; nv = points of the chunk inside the
+// line (L except for the last chunk of a ragged line).  The carry fixes are
+// folded into two precomputed responses: both local sweeps run before the
+// first barrier (the backward one on the local forward values), and since
+// the solve is linear,
 //   y_j = y_j(local) + F h_j + B g_j,
 //   h_j = sum_{m=j}^{len-1} rho^(2m-j+1),   g_j = rho^(len-j),
 // with F the true v just before the chunk and B the true y just after it.
