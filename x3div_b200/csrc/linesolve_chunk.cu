@@ -1316,19 +1316,13 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
     using VT = typename Vec4<T>::type;
     constexpr int V = Vec4<T>::N;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    __shared__ uint64_t bar;
+    __shared__ uint64_t bars[2];
     __shared__ long s_item;
     const int t = threadIdx.x;
-    if (t == 0) {
-        mbar_init(&bar, 1);
-        fence_mbar_init();
-        s_item = (long)atomicAdd(counter, 1ull);
-    }
-    __syncthreads();
-    uint32_t phase = 0;
-    T *tile = reinterpret_cast<T *>(smem_raw);
-    const ChunkScratch<T> scf = carve_scratch<T>(smem_raw + tile_cap, kBatchThreads / 1, 1);
-    T *resp_s = reinterpret_cast<T *>(smem_raw + tile_cap +
+    // two staging slots of tile_cap bytes, then the carry scratch and the
+    // carry responses of the item's operators
+    const ChunkScratch<T> scf = carve_scratch<T>(smem_raw + 2 * tile_cap, kBatchThreads / 1, 1);
+    T *resp_s = reinterpret_cast<T *>(smem_raw + 2 * tile_cap +
                                       (((size_t)2 * kBatchThreads * sizeof(T) + 15) & ~(size_t)15));
     auto job_of = [&](long item) {
         int lo = 0, hi = njobs - 1;
@@ -1339,7 +1333,43 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
         }
         return lo;
     };
-    for (;;) {
+    // The copies of one work item into staging slot `slot` (one thread).
+    auto issue = [&](long item, int slot) {
+        const BatchJob<T> &J = jobs[job_of(item)];
+        const long tl = item - J.tile0;
+        T *tile = reinterpret_cast<T *>(smem_raw + slot * tile_cap);
+        uint64_t *bar = &bars[slot];
+        if (J.dir == DX) {
+            const long l0 = tl * J.W;
+            const int rows = (int)min((long)J.W, J.span - l0);
+            const uint32_t row_bytes = (uint32_t)(J.n * sizeof(T));
+            mbar_arrive_expect_tx(bar, row_bytes * (uint32_t)rows);
+            for (int rr = 0; rr < rows; ++rr)
+                bulk_load(tile + (size_t)rr * J.pitch + kHalo, J.in + (size_t)(l0 + rr) * J.n, row_bytes, bar);
+        } else {
+            const int x0 = (int)(tl % J.span) * J.W, o = (int)(tl / J.span);
+            fence_tensormap_acquire(&J.tmap);
+            mbar_arrive_expect_tx(bar, (uint32_t)((size_t)J.nbox * J.box_n * J.W * sizeof(T)));
+            T *dst = tile + (size_t)J.halo * J.W;
+            for (int b = 0; b < J.nbox; ++b) {
+                if (J.dir == DY)
+                    tma_load_3d(dst + (size_t)b * J.box_n * J.W, &J.tmap, bar, x0, b * J.box_n, o);
+                else
+                    tma_load_3d(dst + (size_t)b * J.box_n * J.W, &J.tmap, bar, x0, o, b * J.box_n);
+            }
+        }
+    };
+    if (t == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+        s_item = (long)atomicAdd(counter, 1ull);
+        if (s_item < total) issue(s_item, 0);
+    }
+    __syncthreads();
+    uint32_t phases = 0;  // bit s: parity of slot s's next completion
+    for (int it = 0;; ++it) {
+        const int slot = it & 1;
         const long item = s_item;  // claimed during the previous item (or above)
         if (item >= total) break;
         const BatchJob<T> &J = jobs[job_of(item)];
@@ -1355,62 +1385,32 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
             x0 = (int)(tl % J.span) * W;
             o = (int)(tl / J.span);
         }
-        if (t == 0) {
-            if (dir == DX) {
-                const uint32_t row_bytes = (uint32_t)(n * sizeof(T));
-                mbar_arrive_expect_tx(&bar, row_bytes * (uint32_t)rows);
-                for (int rr = 0; rr < rows; ++rr)
-                    bulk_load(tile + (size_t)rr * J.pitch + kHalo, J.in + (size_t)(l0 + rr) * n, row_bytes, &bar);
-            } else {
-                fence_tensormap_acquire(&J.tmap);
-                mbar_arrive_expect_tx(&bar, (uint32_t)((size_t)J.nbox * J.box_n * W * sizeof(T)));
-                T *dst = tile + (size_t)J.halo * W;
-                for (int b = 0; b < J.nbox; ++b) {
-                    if (dir == DY)
-                        tma_load_3d(dst + (size_t)b * J.box_n * W, &J.tmap, &bar, x0, b * J.box_n, o);
-                    else
-                        tma_load_3d(dst + (size_t)b * J.box_n * W, &J.tmap, &bar, x0, o, b * J.box_n);
-                }
-            }
-        }
-        const bool ok = mbar_wait_bounded(&bar, phase, kChunkWaitNs);
+        unsigned char *tbase = smem_raw + slot * tile_cap;
+        const T *tile = reinterpret_cast<const T *>(tbase);
+        const uint32_t parity = (phases >> slot) & 1u;
+        const bool ok = mbar_wait_bounded(&bars[slot], parity, kChunkWaitNs);
         if (!__syncthreads_and(ok)) {
             if (t == 0) atomicExch(err, 1);
-            mbar_wait_bounded(&bar, phase, kChunkWaitNs);
+            mbar_wait_bounded(&bars[slot], parity, kChunkWaitNs);
             return;
         }
-        phase ^= 1;
-        // every thread is done with the previous item's responses (read
-        // after its last barrier): this item's go in their place
+        phases ^= 1u << slot;
+        // every thread is done with the previous item (its responses are read
+        // after its last barrier, its tile before): this item's responses go
+        // in place, and the next item, claimed now, is copied into the other
+        // slot while this one is solved
         for (int i = t; i < J.nops * 4 * L; i += kBatchThreads) {
             const int k = i / (4 * L), rem = i - k * 4 * L, a = rem / L, j = rem - a * L;
             resp_s[i] = J.resp[k][a][j];
         }
-        // every thread has read s_item: claim the next item now and start
-        // moving its lines into L2 while this one is solved
         if (t == 0) {
             const long next = (long)atomicAdd(counter, 1ull);
             s_item = next;
-            if (next < total) {
-                const BatchJob<T> &N = jobs[job_of(next)];
-                const long tn = next - N.tile0;
-                if (N.dir == DX) {
-                    const long nl0 = tn * N.W;
-                    const int nrows = (int)min((long)N.W, N.span - nl0);
-                    bulk_prefetch(N.in + (size_t)nl0 * N.n, (uint32_t)((size_t)nrows * N.n * sizeof(T)));
-                } else {
-                    const int nx0 = (int)(tn % N.span) * N.W, no = (int)(tn / N.span);
-                    fence_tensormap_acquire(&N.tmap);
-                    for (int b = 0; b < N.nbox; ++b) {
-                        if (N.dir == DY) tma_prefetch_3d(&N.tmap, nx0, b * N.box_n, no);
-                        else tma_prefetch_3d(&N.tmap, nx0, no, b * N.box_n);
-                    }
-                }
-            }
+            if (next < total) issue(next, slot ^ 1);
         }
-        if (dir == DX) fill_halos_x<T>(smem_raw, 0, 1, rows, J.pitch, n);
-        else fill_halos_yz<T>(smem_raw, 0, 1, n, W, J.halo);
-        fence_proxy_async_smem();  // the next item's copies overwrite the halos
+        if (dir == DX) fill_halos_x<T>(tbase, 0, 1, rows, J.pitch, n);
+        else fill_halos_yz<T>(tbase, 0, 1, n, W, J.halo);
+        fence_proxy_async_smem();  // copies into this slot two items later overwrite the halos
         __syncthreads();
         const bool active = t < W * C;
         const int l = active ? t % W : 0, c = active ? t / W : 0;
@@ -1547,7 +1547,7 @@ size_t batch_scratch_bytes()
 template <typename T>
 int prepare_batch(size_t tile_cap, size_t smem_optin, int num_sms, int *grid)
 {
-    const size_t smem = tile_cap + batch_scratch_bytes<T>();
+    const size_t smem = 2 * tile_cap + batch_scratch_bytes<T>();
     if (smem + 1024 > smem_optin) return X3D_EUNSUPPORTED;
     auto kern = ls_batch<T, kChunkLong<T>>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
@@ -1562,7 +1562,7 @@ template <typename T>
 int launch_batch(cudaStream_t st, int grid, const BatchJob<T> *d_jobs, int njobs, long total,
                  unsigned long long *d_counter, size_t tile_cap, int *d_err)
 {
-    const size_t smem = tile_cap + batch_scratch_bytes<T>();
+    const size_t smem = 2 * tile_cap + batch_scratch_bytes<T>();
     if (cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), st) != cudaSuccess) return X3D_ECUDA;
     ls_batch<T, kChunkLong<T>><<<(unsigned)grid, kBatchThreads, smem, st>>>(d_jobs, njobs, total, d_counter,
                                                                              tile_cap, d_err);
