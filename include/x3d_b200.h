@@ -136,6 +136,12 @@ int x3d_ctx_get_stream(x3d_ctx ctx, void **stream);
 /* Wait for the context's stream; returns X3D_ETIMEOUT if a kernel recorded a
  * bounded-wait failure since the last call, else a CUDA error or X3D_OK. */
 int x3d_ctx_sync(x3d_ctx ctx);
+/* Checks the failure path of the bounded device waits: launches one kernel
+ * whose wait nothing can complete (an mbarrier with no arrival and no copy
+ * in flight) and which gives up after limit_s (0 < limit_s <= 1) seconds,
+ * recording the failure; the next x3d_ctx_sync returns X3D_ETIMEOUT and
+ * clears it, and the context stays usable.  No reference counterpart. */
+int x3d_ctx_selftest_timeout(x3d_ctx ctx, double limit_s);
 /* Text of the last error recorded on this context (never NULL). */
 const char *x3d_ctx_last_error(x3d_ctx ctx);
 /* Number of this library's kernels launched on the context so far (library

@@ -112,3 +112,27 @@ def test_capture_rejects_unregistered_host_arrays(torch_cuda):
         ctx.buf_register(p)  # overlaps
     ctx.buf_unregister(p)
     ctx.close()
+
+
+def test_bounded_wait_timeout_is_reported_and_the_context_survives(oracle, torch_cuda):
+    """Failure detection without a GPU fault: a bounded wait that nothing
+    completes gives up after 20 ms, the host sees X3D_ETIMEOUT at the next
+    sync (once), and the context keeps working."""
+    torch = torch_cuda
+    from x3div_b200 import Context, X3DError, to_device, to_host
+    from conftest import rel_err
+    ctx = Context(*SHAPE, lengths=LEN, precision="f64")
+    ctx.selftest_timeout(0.02)
+    with pytest.raises(X3DError) as e:
+        ctx.sync()
+    assert e.value.code == -5
+    ctx.sync()  # reported once
+    u = seeded_field(SHAPE, 9, lengths=LEN, noise=1e-2)
+    d_u = to_device(u)
+    t = torch.empty_like(d_u)
+    ctx.derx(t, d_u, ctx.op("derx"), *SHAPE)
+    ctx.sync()
+    assert rel_err(to_host(t), oracle.apply("der", 0, u, LEN[0] / SHAPE[0])) < 1e-12
+    with pytest.raises(X3DError):
+        ctx.selftest_timeout(5.0)  # limits above 1 s are refused
+    ctx.close()

@@ -132,6 +132,11 @@ class Context:
         raw = getattr(stream, "cuda_stream", stream)
         self._check(self.L.x3d_ctx_set_stream(self.handle, raw))
 
+    def selftest_timeout(self, limit_s=0.01):
+        """x3d_ctx_selftest_timeout: a bounded device wait that runs out; the
+        next sync raises X3DError with code X3D_ETIMEOUT (-5)."""
+        self._check(self.L.x3d_ctx_selftest_timeout(self.handle, float(limit_s)))
+
     def launch_count(self) -> int:
         """Kernels of this library launched on the context so far."""
         out = ctypes.c_ulonglong()

@@ -462,6 +462,14 @@ int x3d_ctx_sync(x3d_ctx ctx)
     return X3D_OK;
 }
 
+int x3d_ctx_selftest_timeout(x3d_ctx ctx, double limit_s)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!(limit_s > 0.0 && limit_s <= 1.0)) return set_error(ctx, X3D_EINVAL, "limit must be in (0, 1] s");
+    return launch_wait_selftest(ctx, (uint64_t)(limit_s * 1e9));
+}
+
 const char *x3d_ctx_last_error(x3d_ctx ctx)
 {
     if (!ctx) return "null context";

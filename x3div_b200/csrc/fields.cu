@@ -3,6 +3,7 @@
 // to a multiple of the SM count.
 #include <cmath>
 
+#include "ptx.cuh"
 #include "x3d_internal.h"
 
 namespace x3d {
@@ -188,6 +189,30 @@ int launch_sub3(x3d_ctx_s *ctx, bool fp32, void *u, void *v, void *w, const void
                    (const float *)b, (const float *)c, n);
     X3D_LAUNCH(k_sub3<double>, n, (double *)u, (double *)v, (double *)w, (const double *)a,
                (const double *)b, (const double *)c, n);
+}
+
+// A bounded wait that nothing can complete: the mbarrier expects one arrival
+// and none comes, and no copy is in flight.  The wait gives up after
+// limit_ns and records the failure in the error flag, as every bounded wait
+// of the stage and batch kernels does, so the whole path (device flag, host
+// status, context still usable) can be checked without a GPU fault.
+__global__ void k_wait_selftest(int *err, uint64_t limit_ns)
+{
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    const bool ok = mbar_wait_bounded(&bar, 0, limit_ns);
+    if (!__syncthreads_and(ok) && threadIdx.x == 0) atomicExch(err, 2);
+}
+
+int launch_wait_selftest(x3d_ctx_s *ctx, uint64_t limit_ns)
+{
+    ++ctx->launches;
+    k_wait_selftest<<<1, 32, 0, ctx->stream>>>(ctx->d_err, limit_ns);
+    return cuda_check(ctx, cudaGetLastError(), "k_wait_selftest launch");
 }
 
 int launch_scale_y(x3d_ctx_s *ctx, bool fp32, void *t, const double *ppy, int nx, int ny, int nz)

@@ -185,6 +185,7 @@ int launch_sub3(x3d_ctx_s *ctx, bool fp32, void *u, void *v, void *w, const void
                 const void *b, const void *c, size_t n);                   // u -= a
 int launch_mul(x3d_ctx_s *ctx, bool fp32, void *out, const void *a, const void *b, size_t n);
 int launch_scale_y(x3d_ctx_s *ctx, bool fp32, void *t, const double *ppy, int nx, int ny, int nz);
+int launch_wait_selftest(x3d_ctx_s *ctx, uint64_t limit_ns);
 int launch_fma_acc(x3d_ctx_s *ctx, bool fp32, void *out, const void *base, const void *a,
                    const void *b, size_t n);  // out = base + a*b
 int launch_add(x3d_ctx_s *ctx, bool fp32, void *out, const void *a, const void *b, size_t n);
