@@ -271,6 +271,7 @@ int x3d_batch_bind_sweep(x3d_batch b, int nfields, void *const *fields, void *co
 
 int x3d_batch_run(x3d_batch b)
 {
+    const TraceRange trace("batch_run");
     if (!b) return X3D_EINVAL;
     cudaSetDevice(b->device);
     return b->precision == X3D_F32 ? run_typed<float>(b) : run_typed<double>(b);

@@ -639,6 +639,7 @@ int x3d_interzpv(x3d_ctx ctx, void *tz, const void *uz, x3d_op op, int nx, int n
 
 int x3d_apply_batch(x3d_ctx ctx, const x3d_work *items, int count)
 {
+    const TraceRange trace("apply_batch");
     int rc = check_ctx(ctx);
     if (rc) return rc;
     if (count < 0 || (count > 0 && !items)) return set_error(ctx, X3D_EINVAL, "bad work-list");
@@ -835,6 +836,7 @@ int x3d_poisson(x3d_ctx ctx, double *rhs)
 static int divergence_unfused(x3d_ctx_s *ctx, double *pp3, const void *ux, const void *uy, const void *uz);
 static int divergence_dev(x3d_ctx_s *ctx, double *pp3, const void *ux, const void *uy, const void *uz)
 {
+    const TraceRange trace("divergence");
     const void *u[3] = {ux, uy, uz};
     const int rc = fused_divergence(ctx, pp3, u);
     return rc == X3D_EUNSUPPORTED ? divergence_unfused(ctx, pp3, ux, uy, uz) : rc;
@@ -876,6 +878,7 @@ static int gradp_unfused(x3d_ctx_s *ctx, void *px, void *py, void *pz, const dou
 static int gradp_dev(x3d_ctx_s *ctx, void *px, void *py, void *pz, const double *pp3,
                      void *const *ucor = nullptr)
 {
+    const TraceRange trace("gradp + cor_vel");
     void *p[3] = {px, py, pz};
     int rc = fused_gradp(ctx, p, pp3, ucor);
     if (rc != X3D_EUNSUPPORTED) return rc;
@@ -916,6 +919,7 @@ static int momentum_unfused(x3d_ctx_s *ctx, void *du[3], const void *u[3]);
 static int momentum_dev(x3d_ctx_s *ctx, void *du[3], const void *u[3], bool step = false,
                         double dt = 0.0)
 {
+    const TraceRange trace("momentum_rhs_eq");
     void *un[3] = {const_cast<void *>(u[0]), const_cast<void *>(u[1]), const_cast<void *>(u[2])};
     int rc = fused_transeq(ctx, du, u, step, dt, un);
     if (rc != X3D_EUNSUPPORTED) return rc;
@@ -1060,6 +1064,7 @@ int x3d_int_time(x3d_ctx ctx, void *ux1, void *uy1, void *uz1, const void *dux1,
 // One timestep on device fields (src/xcompact3d.f90:80-95).
 static int euler_dev(x3d_ctx_s *ctx, void *u[3], void *du[3], double *p, void *px, void *py, void *pz, double dt)
 {
+    const TraceRange trace("euler_step");
     const void *uc[3] = {u[0], u[1], u[2]};
     int rc = momentum_dev(ctx, du, uc, true, dt);             // calculate_transeq_rhs + int_time
     rc = rc ? rc : divergence_dev(ctx, p, u[0], u[1], u[2]);  // solve_poisson: divergence

@@ -409,6 +409,7 @@ static int launch_poisson_z(x3d_ctx_s *ctx)
 
 int poisson_solve(x3d_ctx_s *ctx, double *rhs)
 {
+    const TraceRange trace("poisson");
     int rc = poisson_setup(ctx);
     if (rc) return rc;
     cufftSetStream(ctx->plan_d2z, ctx->stream);

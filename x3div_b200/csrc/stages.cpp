@@ -102,6 +102,7 @@ static int tune_stage(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir, cons
 template <typename T>
 static int run_stage(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir, const char *name)
 {
+    const TraceRange trace(name);
     if (ctx->stage_tuning) return tune_stage<T>(ctx, prog, dir, name);
     const auto it = ctx->stage_tuned.find(name);
     const int first = it != ctx->stage_tuned.end() ? it->second

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 #include <cufft.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cstdint>
 #include <map>
@@ -186,6 +187,17 @@ int launch_sub3(x3d_ctx_s *ctx, bool fp32, void *u, void *v, void *w, const void
 int launch_mul(x3d_ctx_s *ctx, bool fp32, void *out, const void *a, const void *b, size_t n);
 int launch_scale_y(x3d_ctx_s *ctx, bool fp32, void *t, const double *ppy, int nx, int ny, int nz);
 int launch_wait_selftest(x3d_ctx_s *ctx, uint64_t limit_ns);
+
+// An NVTX range over one stage of the hot path, named after the reference
+// routine it replaces (the reference has these ranges commented out around
+// every stage, e.g. src/xcompact3d.f90:79-96, src/transeq.f90:84-94).  It
+// costs a call per stage and records nothing unless a profiler is attached.
+struct TraceRange {
+    explicit TraceRange(const char *name) { nvtxRangePushA(name); }
+    ~TraceRange() { nvtxRangePop(); }
+    TraceRange(const TraceRange &) = delete;
+    TraceRange &operator=(const TraceRange &) = delete;
+};
 int launch_fma_acc(x3d_ctx_s *ctx, bool fp32, void *out, const void *base, const void *a,
                    const void *b, size_t n);  // out = base + a*b
 int launch_add(x3d_ctx_s *ctx, bool fp32, void *out, const void *a, const void *b, size_t n);
