@@ -204,3 +204,41 @@ def test_nonperiodic_staggered_other_parities(oracle, torch_cuda, prec):
                 _run_stag(oracle, torch, ctx, 1, "deryvp", op, shape, lengths, prec, ncl, 1)
             op.close()
         ctx.close()
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_nonperiodic_staggered_y_stretching_metric(oracle, torch_cuda, prec):
+    """deryvp (npaire 0, its only non-periodic branch) and derypv (npaire 1)
+    with a stretching metric: the result is scaled by ppyi / ppy on the
+    output grid (src/x3d_staggered.f90:629-635, 875-881)."""
+    torch = torch_cuda
+    from x3div_b200 import Context, to_device, to_host
+    dt = torch.float64 if prec == "f64" else torch.float32
+    tol = 1e-12 if prec == "f64" else 1e-5
+    shape = (12, 20, 10)
+    nx, ny, nz = shape
+    lengths = (1.0, 2.0, 1.5)
+    ncl = (1, 2)
+    ctx = Context(*shape, lengths=lengths, precision=prec, bc=(0, 0, *ncl, 0, 0))
+    h = lengths[1] / (ny - 1)
+    for kind, routine, npaire in (("dervp", "deryvp", 0), ("derpv", "derypv", 1)):
+        lhs = oracle.lhs_stag_np(kind, ny, h, *ncl)
+        sc = oracle.rhs_scalars(kind, h)
+        op = ctx.op_create(kind, 1, lhs["m"], npaire, sc["alfa"], lhs["f"], lhs["s"], lhs["w"], None, sc["rhs"])
+        vp = kind == "dervp"
+        in_shape = (nx, ny if vp else ny - 1, nz)
+        out_n = ny - 1 if vp else ny
+        u = seeded_field(in_shape, 71, lengths=lengths, noise=1e-2)
+        d_u = to_device(u, dt)
+        used = to_host(d_u).astype(np.float64)
+        metric = 1.0 + 0.25 * np.sin(np.arange(out_n) / out_n * 2 * np.pi)
+        t = torch.full((nz, out_n, nx), float("nan"), dtype=dt, device="cuda")
+        if vp:
+            ctx.deryvp(t, d_u, op, metric, nx, ny, ny - 1, nz)
+        else:
+            ctx.derypv(t, d_u, op, metric, nx, ny - 1, ny, nz)
+        ctx.sync()
+        ref = oracle.stag_np(kind, 1, used, h, *ncl, npaire) * metric[None, :, None]
+        assert rel_err(to_host(t), ref) < tol, (routine, prec)
+        op.close()
+    ctx.close()
