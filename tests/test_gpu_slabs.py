@@ -1,0 +1,50 @@
+"""The slab code path on the B200: the library's line solves on a rank's
+local extents and the y <-> z transposes through NCCL (one rank), against the
+oracle on the whole box."""
+import socket
+
+import numpy as np
+import pytest
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+def _kind(routine):
+    if routine in ("derxx", "deryy", "derzz"):
+        return "der2"
+    if routine.startswith("inter"):
+        return "int" + routine[-2:]
+    if routine.endswith(("vp", "pv")):
+        return "der" + routine[-2:]
+    return "der"
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_slab_sweep_on_one_nccl_rank(oracle, torch_cuda, prec):
+    torch = torch_cuda
+    import torch.distributed as dist
+    from x3div_b200 import Context, to_host
+    from x3div_b200.slabs import SWEEP, SlabLayout, sweep
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1)
+    try:
+        shape = (24, 20, 16)
+        lengths = (2 * np.pi, 1.5, 3.0)
+        ctx = Context(*shape, lengths=lengths, precision=prec)
+        dt = torch.float64 if prec == "f64" else torch.float32
+        g = np.random.default_rng(3).standard_normal(shape[::-1])
+        field = torch.from_numpy(g).to(device="cuda", dtype=dt)
+        used = np.asfortranarray(field.double().cpu().numpy().transpose(2, 1, 0))
+        res = sweep(ctx, field, SlabLayout(shape, 0, 1))
+        ctx.sync()
+        tol = 1e-12 if prec == "f64" else 1e-5
+        for d in range(3):
+            for k, (routine, _) in enumerate(SWEEP[d]):
+                ref = oracle.apply(_kind(routine), d, used, lengths[d] / shape[d])
+                assert rel_err(to_host(res[d][k]), ref) < tol, (d, routine)
+        ctx.close()
+    finally:
+        dist.destroy_process_group()

@@ -1,0 +1,176 @@
+"""One periodic box over P ranks: 2decomp's 1 x P pencil decomposition.
+
+With p_row = 1 and p_col = P, the X and Y pencils of 2decomp coincide: each
+rank holds whole x lines and whole y lines of a block of z planes (a z-slab,
+(nx, ny, nz_r) in Fortran order).  A Z pencil holds whole z lines of a block of
+y rows (a y-slab, (nx, ny_r, nz)).  Lines are never split, so every line-solve
+routine of the library runs unchanged on a rank's slab with its local extents
+(e.g. x3d_derz(ctx, t, u, op, nx, ny_r, nz) on a y-slab, with the context and
+operators made for the global box).  x3d_transpose_x_to_y and y_to_x are
+local; the y <-> z transposes (x3d_transpose_y_to_z / z_to_y,
+src/x3d_transpose.f90:77-130, 2decomp's transpose_y_to_z / transpose_z_to_y)
+become one all-to-all each: rank r sends rank s the block of its slab that s
+owns in the other layout.  Blocks follow 2decomp's distribution: the first
+n mod P ranks hold one plane more.
+
+Device tensors are C-ordered (nz, ny, nx) views of the Fortran (nx, ny, nz)
+layout, as in the rest of the package.  The collectives go through
+torch.distributed: NCCL over NVLink for CUDA tensors, gloo for CPU tensors.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+
+def split(n: int, parts: int, rank: int):
+    """[start, end) of block `rank` when n points are cut into `parts` blocks,
+    the first n mod parts blocks one point longer."""
+    if parts < 1 or not 0 <= rank < parts:
+        raise ValueError("bad block request")
+    base, extra = divmod(n, parts)
+    start = rank * base + min(rank, extra)
+    return start, start + base + (1 if rank < extra else 0)
+
+
+@dataclass(frozen=True)
+class SlabLayout:
+    """Where rank `rank` of `world` keeps its part of an (nx, ny, nz) box."""
+    shape: tuple
+    rank: int
+    world: int
+
+    def __post_init__(self):
+        nx, ny, nz = self.shape
+        if ny < self.world or nz < self.world:
+            raise ValueError("need at least one y row and one z plane per rank")
+
+    def zslab(self, r=None):
+        """[z0, z1): the z planes of rank r's X/Y pencil (default: this rank)."""
+        return split(self.shape[2], self.world, self.rank if r is None else r)
+
+    def yslab(self, r=None):
+        """[y0, y1): the y rows of rank r's Z pencil (default: this rank)."""
+        return split(self.shape[1], self.world, self.rank if r is None else r)
+
+    @property
+    def xy_extents(self):
+        """(nx, ny, nz_r): local extents of this rank's X/Y pencil."""
+        z0, z1 = self.zslab()
+        return self.shape[0], self.shape[1], z1 - z0
+
+    @property
+    def z_extents(self):
+        """(nx, ny_r, nz): local extents of this rank's Z pencil."""
+        y0, y1 = self.yslab()
+        return self.shape[0], y1 - y0, self.shape[2]
+
+
+def _all_to_all(recv, send, out_splits, in_splits, group):
+    import torch.distributed as dist
+    if dist.is_available() and dist.is_initialized():
+        dist.all_to_all_single(recv, send, out_splits, in_splits, group=group)
+    else:  # one rank: the exchange is a copy
+        recv.copy_(send)
+
+
+def transpose_y_to_z(zslab, layout: SlabLayout, group=None):
+    """X/Y pencil (a (nz_r, ny, nx) tensor) -> Z pencil ((nz, ny_s, nx) on
+    rank s): 2decomp's transpose_y_to_z at p_row = 1."""
+    import torch
+    nx, ny, nz = layout.shape
+    z0, z1 = layout.zslab()
+    if tuple(zslab.shape) != (z1 - z0, ny, nx):
+        raise ValueError("not this rank's X/Y pencil")
+    blocks = [zslab[:, y0:y1, :].reshape(-1) for y0, y1 in (layout.yslab(s) for s in range(layout.world))]
+    send = torch.cat(blocks)
+    y0, y1 = layout.yslab()
+    out_splits = [(b - a) * (y1 - y0) * nx for a, b in (layout.zslab(r) for r in range(layout.world))]
+    recv = torch.empty(sum(out_splits), dtype=zslab.dtype, device=zslab.device)
+    _all_to_all(recv, send, out_splits, [b.numel() for b in blocks], group)
+    out = torch.empty((nz, y1 - y0, nx), dtype=zslab.dtype, device=zslab.device)
+    off = 0
+    for r in range(layout.world):
+        a, b = layout.zslab(r)
+        n = out_splits[r]
+        out[a:b] = recv[off:off + n].view(b - a, y1 - y0, nx)
+        off += n
+    return out
+
+
+def transpose_z_to_y(yslab, layout: SlabLayout, group=None):
+    """Z pencil ((nz, ny_r, nx)) -> X/Y pencil ((nz_s, ny, nx) on rank s):
+    2decomp's transpose_z_to_y at p_row = 1."""
+    import torch
+    nx, ny, nz = layout.shape
+    y0, y1 = layout.yslab()
+    if tuple(yslab.shape) != (nz, y1 - y0, nx):
+        raise ValueError("not this rank's Z pencil")
+    blocks = [yslab[a:b].reshape(-1) for a, b in (layout.zslab(s) for s in range(layout.world))]
+    send = torch.cat(blocks)
+    z0, z1 = layout.zslab()
+    out_splits = [(z1 - z0) * (b - a) * nx for a, b in (layout.yslab(r) for r in range(layout.world))]
+    recv = torch.empty(sum(out_splits), dtype=yslab.dtype, device=yslab.device)
+    _all_to_all(recv, send, out_splits, [b.numel() for b in blocks], group)
+    out = torch.empty((z1 - z0, ny, nx), dtype=yslab.dtype, device=yslab.device)
+    off = 0
+    for r in range(layout.world):
+        a, b = layout.yslab(r)
+        n = out_splits[r]
+        out[:, a:b, :] = recv[off:off + n].view(z1 - z0, b - a, nx)
+        off += n
+    return out
+
+
+# The six operator families of a sweep, by direction: (routine, operator).
+SWEEP = {
+    0: [("derx", "derx"), ("derxx", "derxx"), ("derxvp", "derxvp"), ("derxpv", "derxpv"),
+        ("interxvp", "intxvp"), ("interxpv", "intxpv")],
+    1: [("dery", "dery"), ("deryy", "deryy"), ("deryvp", "deryvp"), ("derypv", "derypv"),
+        ("interyvp", "intyvp"), ("interypv", "intypv")],
+    2: [("derz", "derz"), ("derzz", "derzz"), ("derzvp", "derzvp"), ("derzpv", "derzpv"),
+        ("interzvp", "intzvp"), ("interzpv", "intzpv")],
+}
+
+
+def _call(ctx, routine, t, u, op, ext):
+    nx, ny, nz = ext
+    fn = getattr(ctx, routine)
+    if routine in ("dery",):
+        fn(t, u, op, None, nx, ny, nz)
+    elif routine in ("deryvp", "derypv"):
+        fn(t, u, op, None, nx, ny, ny, nz)
+    elif routine.endswith(("xvp", "xpv")):
+        fn(t, u, op, nx, nx, ny, nz)
+    elif routine.endswith(("yvp", "ypv")):
+        fn(t, u, op, nx, ny, ny, nz)
+    elif routine.endswith(("zvp", "zpv")):
+        fn(t, u, op, nx, ny, nz, nz)
+    else:
+        fn(t, u, op, nx, ny, nz)
+
+
+def sweep(ctx, field, layout: SlabLayout, group=None):
+    """The 18 operator applications of a sweep on one field of a box that is
+    spread over the ranks: x and y families on the rank's X/Y pencil, z
+    families on its Z pencil (one transpose each way).  ctx is a periodic
+    context made for the global box; field is the rank's X/Y pencil.  Returns
+    {direction: [six outputs in X/Y-pencil layout]}."""
+    import torch
+    ext = layout.xy_extents
+    out = {}
+    for d in (0, 1):
+        res = []
+        for routine, opname in SWEEP[d]:
+            t = torch.empty_like(field)
+            _call(ctx, routine, t, field, ctx.op(opname), ext)
+            res.append(t)
+        out[d] = res
+    zp = transpose_y_to_z(field, layout, group)
+    zext = layout.z_extents
+    res = []
+    for routine, opname in SWEEP[2]:
+        t = torch.empty_like(zp)
+        _call(ctx, routine, t, zp, ctx.op(opname), zext)
+        res.append(transpose_z_to_y(t, layout, group))
+    out[2] = res
+    return out
