@@ -316,6 +316,16 @@ int x3d_transpose_y_to_x(x3d_ctx ctx, const void *in, void *out, int is_complex)
 /* poisson_000 (src/poisson.f90:276-419), in place on the FP64 pressure-grid
  * field rhs (nx*ny*nz doubles). */
 int x3d_poisson(x3d_ctx ctx, double *rhs);
+/* The z part of poisson_000 for a box whose y rows are spread over ranks:
+ * spec is this rank's block of the x-y transformed half spectrum (complex
+ * FP64, nx/2+1 x modes, ny_loc y rows starting at global row j0, nz z
+ * points, x fastest; unnormalised 2-D r2c transforms of the z planes, as
+ * cuFFT or 2decomp produce them).  In place: the forward z transform, the
+ * division of every mode by -K ntot (zero where K < 1e-16), the inverse z
+ * transform; the unnormalised 2-D c2r transforms then give the solution.
+ * Device pointer; z lengths 2^p 3^q from 8 to 1024.  With 2decomp, the z
+ * transforms of a distributed 3-D FFT run on Z pencils in the same way. */
+int x3d_poisson_zlines(x3d_ctx ctx, void *spec, int ny_loc, int j0);
 
 /* ---- projection stage: module navier (src/navier.f90) ------------------- */
 

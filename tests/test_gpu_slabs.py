@@ -48,3 +48,30 @@ def test_slab_sweep_on_one_nccl_rank(oracle, torch_cuda, prec):
         ctx.close()
     finally:
         dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("shape", [(24, 20, 16), (30, 12, 48), (16, 18, 96)])
+def test_slab_poisson_on_one_nccl_rank(oracle, torch_cuda, shape):
+    """The slab Poisson solve (torch.fft x-y transforms, the half spectrum
+    transposed through NCCL, x3d_poisson_zlines on the rank's y rows) against
+    the oracle's poisson_000 on the whole box."""
+    torch = torch_cuda
+    import torch.distributed as dist
+    from x3div_b200 import Context
+    from x3div_b200.slabs import SlabLayout, poisson
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1)
+    try:
+        lengths = (2 * np.pi, 1.5, 3.0)
+        ctx = Context(*shape, lengths=lengths, precision="f64")
+        g = np.random.default_rng(8).standard_normal(shape[::-1])
+        rhs = torch.from_numpy(g).cuda()
+        poisson(ctx, rhs, SlabLayout(shape, 0, 1))
+        torch.cuda.synchronize()
+        ref = oracle.poisson(np.asfortranarray(g.transpose(2, 1, 0)), *lengths)
+        assert rel_err(rhs.cpu().numpy().transpose(2, 1, 0), ref) < 1e-12, shape
+        ctx.close()
+    finally:
+        dist.destroy_process_group()

@@ -1,14 +1,14 @@
 """One box over several ranks (x3div_b200/slabs.py, 2decomp's 1 x P
-decomposition): block splits, the y <-> z transposes over gloo, and a whole
-sweep on slabs, with the oracle as each rank's line operator, against the
-oracle on the whole box."""
+decomposition): block splits, the y <-> z transposes over gloo, a whole
+sweep and the Poisson solve on slabs, with the oracle standing in for each
+rank's kernels, against the oracle on the whole box."""
 import os
 import socket
 
 import numpy as np
 import pytest
 
-from x3div_b200.slabs import SWEEP, SlabLayout, split, sweep, transpose_y_to_z, transpose_z_to_y
+from x3div_b200.slabs import SWEEP, SlabLayout, poisson, split, sweep, transpose_y_to_z, transpose_z_to_y
 
 KIND = {"derx": "der", "dery": "der", "derz": "der", "derxx": "der2", "deryy": "der2", "derzz": "der2",
         "derxvp": "dervp", "deryvp": "dervp", "derzvp": "dervp", "derxpv": "derpv", "derypv": "derpv",
@@ -30,10 +30,29 @@ class OracleContext:
 
     def __init__(self, oracle, shape, lengths):
         self.o = oracle
+        self.shape = shape
+        self.lengths = lengths
         self.d = [L / n for L, n in zip(lengths, shape)]
 
     def op(self, name):
         return name
+
+    def poisson_zlines(self, spec, ny_loc, j0):
+        """The z part of the spectral solve, restated with numpy's FFT and the
+        oracle's modified-wavenumber tables, on a (nz, ny_loc, nxh) block."""
+        import torch
+        nx, ny, nz = self.shape
+        t = self.o.poisson_tables(nx, ny, nz, *self.lengths)
+        c = np.fft.fft(spec.numpy(), axis=0)
+        i = np.arange(nx // 2 + 1)[None, None, :]
+        j = (j0 + np.arange(ny_loc))[None, :, None]
+        k = np.arange(nz)[:, None, None]
+        tyz = t["ty"][j] * t["tz"][k]
+        txz = t["tx"][i] * t["tz"][k]
+        txy = t["tx"][i] * t["ty"][j]
+        kk = t["k2x"][i] * tyz ** 2 + t["k2y"][j] * txz ** 2 + t["k2z"][k] * txy ** 2
+        f = np.where(kk < 1e-16, 0.0, -1.0 / (np.where(kk < 1e-16, 1.0, kk) * (nx * ny * nz)))
+        spec.copy_(torch.from_numpy(np.fft.ifft(c * f, axis=0) * nz))
 
     def __getattr__(self, routine):
         if routine not in KIND:
@@ -80,6 +99,10 @@ def _rank(rank, world, port, shape, q):
             for k, (routine, _) in enumerate(SWEEP[d]):
                 ref = oracle.apply(KIND[routine], d, gf, lengths[d] / shape[d]).transpose(2, 1, 0)[z0:z1]
                 err = max(err, float(np.abs(res[d][k].numpy() - ref).max()))
+        p = torch.from_numpy(g[z0:z1].copy())
+        poisson(ctx, p, lay)
+        ref = oracle.poisson(gf, *lengths).transpose(2, 1, 0)[z0:z1]
+        err = max(err, float(np.abs(p.numpy() - ref).max() / np.abs(ref).max()))
         q.put((rank, ok, err))
     finally:
         dist.destroy_process_group()

@@ -305,6 +305,12 @@ class Context:
     def poisson(self, rhs):
         self._check(self.L.x3d_poisson(self.handle, _ptr(rhs)))
 
+    def poisson_zlines(self, spec, ny_loc, j0):
+        """x3d_poisson_zlines: z transforms and mode division on a block of
+        y rows of the x-y transformed spectrum (a complex128 CUDA tensor of
+        shape (nz, ny_loc, nx//2 + 1))."""
+        self._check(self.L.x3d_poisson_zlines(self.handle, _ptr(spec), int(ny_loc), int(j0)))
+
     def divergence(self, pp3, ux1, uy1, uz1, nlock=1):
         self._check(self.L.x3d_divergence(self.handle, _ptr(pp3), _ptr(ux1), _ptr(uy1), _ptr(uz1), int(nlock)))
 

@@ -829,6 +829,15 @@ int x3d_poisson(x3d_ctx ctx, double *rhs)
     return sg.finish(poisson_solve(ctx, d));
 }
 
+int x3d_poisson_zlines(x3d_ctx ctx, void *spec, int ny_loc, int j0)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if ((rc = need_periodic(ctx))) return rc;
+    if (!spec || !is_device_ptr(spec)) return set_error(ctx, X3D_EINVAL, "spec must be a device array");
+    return poisson_zlines(ctx, spec, ny_loc, j0);
+}
+
 // ---- navier ----------------------------------------------------------------------------
 
 // divergence (src/navier.f90:98-236) with 1x1 transposes elided: the fused

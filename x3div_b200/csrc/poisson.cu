@@ -291,7 +291,7 @@ constexpr int kZftW = N <= 256 ? 16 : (N <= 512 ? 8 : 4);
 // into shared memory first.
 template <int N>
 __global__ void __launch_bounds__(kZftThreads, 2)
-    k_poisson_z(double2 *__restrict__ c, int nxh, int ny, const double2 *__restrict__ tw,
+    k_poisson_z(double2 *__restrict__ c, int nxh, int ny, int j0, const double2 *__restrict__ tw,
                 const double *__restrict__ k2x, const double *__restrict__ tx, const double *__restrict__ k2y,
                 const double *__restrict__ ty, const double *__restrict__ k2z, const double *__restrict__ tz,
                 double ntot)
@@ -308,8 +308,8 @@ __global__ void __launch_bounds__(kZftThreads, 2)
     zl.lines = min(W, nxh - i0);
     zl.i0 = i0;
     zl.nxh = nxh;
-    zl.tyj = __ldg(ty + j);
-    zl.k2yj = __ldg(k2y + j);
+    zl.tyj = __ldg(ty + j0 + j);  // j0: global index of the spectrum's first y row
+    zl.k2yj = __ldg(k2y + j0 + j);
     zl.ntot = ntot;
     zl.tx = tx;
     zl.k2x = k2x;
@@ -384,18 +384,20 @@ int poisson_setup(x3d_ctx_s *ctx)
     return X3D_OK;
 }
 
-static int launch_poisson_z(x3d_ctx_s *ctx)
+// The fused z kernel over a spectrum of ny_loc y rows starting at global row
+// j0 ((nz, ny_loc, nx/2+1), x fastest).
+static int launch_poisson_z(x3d_ctx_s *ctx, double2 *spec, int ny_loc, int j0)
 {
     const int nxh = ctx->nx / 2 + 1;
     const double ntot = (double)ctx->nx * (double)ctx->ny * (double)ctx->nz;
     auto go = [&](auto kern, int W) {
-        const unsigned grid = (unsigned)(((nxh + W - 1) / W) * ctx->ny);
+        const unsigned grid = (unsigned)(((nxh + W - 1) / W) * ny_loc);
         const size_t smem = ((size_t)ctx->nz * W + ctx->nz) * sizeof(double2);  // tile + twiddles
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         ++ctx->launches;
-        kern<<<grid, kZftThreads, smem, ctx->stream>>>((double2 *)ctx->spectrum, nxh, ctx->ny,
-                                                       (const double2 *)ctx->d_zft_tw, ctx->d_k2x, ctx->d_tx,
-                                                       ctx->d_k2y, ctx->d_ty, ctx->d_k2z, ctx->d_tz, ntot);
+        kern<<<grid, kZftThreads, smem, ctx->stream>>>(spec, nxh, ny_loc, j0, (const double2 *)ctx->d_zft_tw,
+                                                       ctx->d_k2x, ctx->d_tx, ctx->d_k2y, ctx->d_ty, ctx->d_k2z,
+                                                       ctx->d_tz, ntot);
         return cuda_check(ctx, cudaGetLastError(), "k_poisson_z");
     };
     switch (ctx->nz) {
@@ -417,7 +419,7 @@ int poisson_solve(x3d_ctx_s *ctx, double *rhs)
     if (cufftExecD2Z(ctx->plan_d2z, rhs, (cufftDoubleComplex *)ctx->spectrum) != CUFFT_SUCCESS)
         return set_error(ctx, X3D_ECUDA, "cufftExecD2Z failed");
     if (ctx->zfused) {
-        rc = launch_poisson_z(ctx);
+        rc = launch_poisson_z(ctx, (double2 *)ctx->spectrum, ctx->ny, 0);
         if (rc) return rc;
         if (cufftExecZ2D(ctx->plan_z2d, (cufftDoubleComplex *)ctx->spectrum, rhs) != CUFFT_SUCCESS)
             return set_error(ctx, X3D_ECUDA, "cufftExecZ2D failed");
@@ -441,6 +443,17 @@ int poisson_solve(x3d_ctx_s *ctx, double *rhs)
     if (cufftExecZ2D(ctx->plan_z2d, (cufftDoubleComplex *)ctx->spectrum, rhs) != CUFFT_SUCCESS)
         return set_error(ctx, X3D_ECUDA, "cufftExecZ2D failed");
     return X3D_OK;
+}
+
+// The z part of the spectral solve on a block of y rows of the x-y
+// transformed spectrum, for a box whose y rows are spread over ranks.
+int poisson_zlines(x3d_ctx_s *ctx, void *spec, int ny_loc, int j0)
+{
+    int rc = poisson_setup(ctx);
+    if (rc) return rc;
+    if (!ctx->zfused) return set_error(ctx, X3D_EUNSUPPORTED, "no fused z transform for this nz");
+    if (ny_loc < 1 || j0 < 0 || j0 + ny_loc > ctx->ny) return set_error(ctx, X3D_EINVAL, "bad block of y rows");
+    return launch_poisson_z(ctx, static_cast<double2 *>(spec), ny_loc, j0);
 }
 
 void poisson_free(x3d_ctx_s *ctx)

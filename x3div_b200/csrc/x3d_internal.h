@@ -187,6 +187,7 @@ int launch_sub3(x3d_ctx_s *ctx, bool fp32, void *u, void *v, void *w, const void
 int launch_mul(x3d_ctx_s *ctx, bool fp32, void *out, const void *a, const void *b, size_t n);
 int launch_scale_y(x3d_ctx_s *ctx, bool fp32, void *t, const double *ppy, int nx, int ny, int nz);
 int launch_wait_selftest(x3d_ctx_s *ctx, uint64_t limit_ns);
+int poisson_zlines(x3d_ctx_s *ctx, void *spec, int ny_loc, int j0);
 
 // An NVTX range over one stage of the hot path, named after the reference
 // routine it replaces (the reference has these ranges commented out around

@@ -174,3 +174,24 @@ def sweep(ctx, field, layout: SlabLayout, group=None):
         res.append(transpose_z_to_y(t, layout, group))
     out[2] = res
     return out
+
+
+def poisson(ctx, rhs, layout: SlabLayout, group=None):
+    """poisson_000 (src/poisson.f90:276-419) on a box spread over the ranks,
+    in place on this rank's X/Y pencil of the FP64 field ((nz_r, ny, nx)).
+    The 2-D x-y transforms of the rank's z planes (cuFFT through torch.fft,
+    unnormalised both ways) bracket the z part, which runs on the rank's
+    block of y rows after a transpose of the half spectrum
+    (x3d_poisson_zlines: z transforms and the mode division)."""
+    import torch
+    nx, ny, nz = layout.shape
+    nxh = nx // 2 + 1
+    spec = torch.fft.rfft2(rhs, norm="backward")  # (nz_r, ny, nxh)
+    half = SlabLayout((2 * nxh, ny, nz), layout.rank, layout.world)  # the spectrum as 2 nxh reals per row
+    zs = transpose_y_to_z(torch.view_as_real(spec).reshape(spec.shape[0], ny, 2 * nxh), half, group)
+    y0, y1 = layout.yslab()
+    ctx.poisson_zlines(torch.view_as_complex(zs.view(nz, y1 - y0, nxh, 2)), y1 - y0, y0)
+    back = transpose_z_to_y(zs, half, group)
+    z0, z1 = layout.zslab()
+    rhs.copy_(torch.fft.irfft2(torch.view_as_complex(back.view(z1 - z0, ny, nxh, 2)), s=(ny, nx), norm="forward"))
+    return rhs
