@@ -75,3 +75,46 @@ def test_slab_poisson_on_one_nccl_rank(oracle, torch_cuda, shape):
         ctx.close()
     finally:
         dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_slab_euler_steps_on_one_nccl_rank(oracle, torch_cuda, prec):
+    """Three Euler steps composed on slabs (line solves on local extents,
+    NCCL transposes, the slab Poisson solve) against the oracle and against
+    the library's fused single-box step."""
+    torch = torch_cuda
+    import torch.distributed as dist
+    from x3div_b200 import Context, to_host
+    from x3div_b200.slabs import SlabLayout, euler_step
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1)
+    try:
+        shape = (24, 20, 16)
+        lengths = (2 * np.pi, 1.5, 3.0)
+        dt = torch.float64 if prec == "f64" else torch.float32
+        ctx = Context(*shape, lengths=lengths, precision=prec)
+        g = [np.random.default_rng(30 + c).standard_normal(shape[::-1]) * 0.1 for c in range(3)]
+        U = [torch.from_numpy(a).to(device="cuda", dtype=dt) for a in g]
+        V = [a.clone() for a in U]
+        ref = [np.asfortranarray(a.to(torch.float64).cpu().numpy().transpose(2, 1, 0)) for a in U]
+        du = [torch.empty_like(U[0]) for _ in range(3)]
+        pg = [torch.empty_like(U[0]) for _ in range(3)]
+        pp3 = torch.empty(shape[::-1], dtype=torch.float64, device="cuda")
+        dv = [torch.empty_like(U[0]) for _ in range(3)]
+        pv = [torch.empty_like(U[0]) for _ in range(3)]
+        pq = torch.empty_like(pp3)
+        lay = SlabLayout(shape, 0, 1)
+        for _ in range(3):
+            euler_step(ctx, U, du, pp3, pg, 1e-3, lay)
+            ctx.euler_step(*V, *dv, pq, *pv, 1e-3)
+            oracle.euler_step(*ref, 1e-3, lengths=lengths)
+        torch.cuda.synchronize()
+        tol = 1e-11 if prec == "f64" else 1e-4
+        for a, b, r in zip(U, V, ref):
+            assert rel_err(to_host(a), r) < tol
+            assert rel_err(to_host(a), to_host(b).astype(np.float64)) < tol
+        ctx.close()
+    finally:
+        dist.destroy_process_group()

@@ -1,14 +1,15 @@
 """One box over several ranks (x3div_b200/slabs.py, 2decomp's 1 x P
 decomposition): block splits, the y <-> z transposes over gloo, a whole
-sweep and the Poisson solve on slabs, with the oracle standing in for each
-rank's kernels, against the oracle on the whole box."""
+sweep, the Poisson solve and two Euler steps on slabs, with the oracle
+standing in for each rank's kernels, against the oracle on the whole box."""
 import os
 import socket
 
 import numpy as np
 import pytest
 
-from x3div_b200.slabs import SWEEP, SlabLayout, poisson, split, sweep, transpose_y_to_z, transpose_z_to_y
+from x3div_b200.slabs import (SWEEP, SlabLayout, euler_step, poisson, split, sweep, transpose_y_to_z,
+                              transpose_z_to_y)
 
 KIND = {"derx": "der", "dery": "der", "derz": "der", "derxx": "der2", "deryy": "der2", "derzz": "der2",
         "derxvp": "dervp", "deryvp": "dervp", "derzvp": "dervp", "derxpv": "derpv", "derypv": "derpv",
@@ -103,6 +104,19 @@ def _rank(rank, world, port, shape, q):
         poisson(ctx, p, lay)
         ref = oracle.poisson(gf, *lengths).transpose(2, 1, 0)[z0:z1]
         err = max(err, float(np.abs(p.numpy() - ref).max() / np.abs(ref).max()))
+        # two timesteps on slabs against two on the whole box
+        U = [np.random.default_rng(20 + c).standard_normal(shape[::-1]) * 0.1 for c in range(3)]
+        ref = [np.asfortranarray(a.transpose(2, 1, 0)) for a in U]
+        mine_u = [torch.from_numpy(a[z0:z1].copy()) for a in U]
+        du = [torch.empty_like(mine_u[0]) for _ in range(3)]
+        pg = [torch.empty_like(mine_u[0]) for _ in range(3)]
+        pp3 = torch.empty_like(mine_u[0])
+        for _ in range(2):
+            euler_step(ctx, mine_u, du, pp3, pg, 1e-3, lay)
+            oracle.euler_step(*ref, 1e-3, lengths=lengths)
+        for a, r in zip(mine_u, ref):
+            rr = r.transpose(2, 1, 0)[z0:z1]
+            err = max(err, float(np.abs(a.numpy() - rr).max() / np.abs(rr).max()))
         q.put((rank, ok, err))
     finally:
         dist.destroy_process_group()

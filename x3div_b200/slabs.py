@@ -195,3 +195,70 @@ def poisson(ctx, rhs, layout: SlabLayout, group=None):
     z0, z1 = layout.zslab()
     rhs.copy_(torch.fft.irfft2(torch.view_as_complex(back.view(z1 - z0, ny, nxh, 2)), s=(ny, nx), norm="forward"))
     return rhs
+
+
+def _apply(ctx, routine, opname, u, ext):
+    import torch
+    t = torch.empty_like(u)
+    _call(ctx, routine, t, u, ctx.op(opname), ext)
+    return t
+
+
+def euler_step(ctx, u, du, pp3, pg, dt, layout: SlabLayout, group=None):
+    """One timestep (src/xcompact3d.f90:80-95) on a box spread over the
+    ranks, from the library's line solves on local extents, elementwise
+    tensor arithmetic and the slab transposes, in the reference's order:
+    momentum_rhs_eq (src/transeq.f90:44-355) with the x and y parts on the
+    rank's X/Y pencil and the z part on its Z pencil; int_time
+    (src/time_integrators.f90:40-44); divergence (src/navier.f90:98-236)
+    into the FP64 pp3; the slab Poisson solve; gradp
+    (src/navier.f90:249-359) and cor_vel (:64-91).  u, du, pg: the three
+    velocity, increment and pressure-gradient components as this rank's X/Y
+    pencils; pp3: its FP64 X/Y pencil.  In place, like x3d_euler_step."""
+    import torch
+    ext, zext = layout.xy_extents, layout.z_extents
+    T = lambda a: transpose_y_to_z(a, layout, group)  # noqa: E731
+    Ti = lambda a: transpose_z_to_y(a, layout, group)  # noqa: E731
+    ux, uy, uz = u
+    uzz = T(uz)
+    for c in range(3):  # calculate_transeq_rhs
+        uc = u[c]
+        ta = ux * uc
+        td = _apply(ctx, "derx", "derx", ta, ext)
+        ta = _apply(ctx, "derx", "derx", uc, ext)
+        duc = td + ux * ta
+        td = uc * uy
+        tg = _apply(ctx, "dery", "dery", td, ext)
+        td = _apply(ctx, "dery", "dery", uc, ext)
+        tg = tg + uy * td
+        ucz = uzz if c == 2 else T(uc)
+        tdz = ucz * uzz
+        tgz = _apply(ctx, "derz", "derz", tdz, zext)
+        tdz = _apply(ctx, "derz", "derz", ucz, zext)
+        tg = tg + Ti(tgz + uzz * tdz)
+        du[c].copy_(duc + tg)
+    for c in range(3):  # int_time, Euler: u = dt du + u
+        u[c].copy_(dt * du[c] + u[c])
+    # divergence
+    pp1 = _apply(ctx, "derxvp", "derxvp", ux, ext)
+    pgy1 = _apply(ctx, "interxvp", "intxvp", uy, ext)
+    pgz1 = _apply(ctx, "interxvp", "intxvp", uz, ext)
+    upi2 = _apply(ctx, "interyvp", "intyvp", pp1, ext)
+    duydypi2 = _apply(ctx, "deryvp", "deryvp", pgy1, ext) + upi2
+    upi2 = _apply(ctx, "interyvp", "intyvp", pgz1, ext)
+    a, b = T(duydypi2), T(upi2)
+    p3 = _apply(ctx, "interzvp", "intzvp", a, zext).double() + _apply(ctx, "derzvp", "derzvp", b, zext).double()
+    pp3.copy_(Ti(p3))
+    poisson(ctx, pp3, layout, group)
+    # gradp + cor_vel
+    p3z = T(pp3).to(ux.dtype)
+    ppi3 = Ti(_apply(ctx, "interzpv", "intzpv", p3z, zext))
+    pgz3 = Ti(_apply(ctx, "derzpv", "derzpv", p3z, zext))
+    ppi2 = _apply(ctx, "interypv", "intypv", ppi3, ext)
+    pgy2 = _apply(ctx, "derypv", "derypv", ppi3, ext)
+    pgzi2 = _apply(ctx, "interypv", "intypv", pgz3, ext)
+    pg[0].copy_(_apply(ctx, "derxpv", "derxpv", ppi2, ext))
+    pg[1].copy_(_apply(ctx, "interxpv", "intxpv", pgy2, ext))
+    pg[2].copy_(_apply(ctx, "interxpv", "intxpv", pgzi2, ext))
+    for c in range(3):
+        u[c].sub_(pg[c])
