@@ -249,6 +249,39 @@ def sweep_groups(ctx, fields, outs, fused):
     return groups
 
 
+# Lines per tile (W) of each chunked configuration (x3d_ctx_set_kernel 0..15).
+CONFIG_W = [16, 32, 16, 8, 32, 8, 16, 32, 16, 8, 32, 8, 32, 16, 32, 32]
+
+
+def pattern_ceilings(ctx, torch, src, outs):
+    """Bandwidth of one read and six writes with no arithmetic
+    (x3d_roofline_probe), flat and in the y stage kernels' tile order for
+    W = 8, 16, 32: what the sweep launches' traffic mix and access order can
+    reach on this GPU (best over 1, 2 and 4 CTAs per SM of 5 timed launches
+    after 3 warm-up ones)."""
+    nz, ny, nx = src.shape
+    bytes_moved = 7 * src.numel() * src.element_size()
+    res = {}
+    for key, pattern, w in (("flat", 0, 0), ("tile_w8", 1, 8), ("tile_w16", 1, 16), ("tile_w32", 1, 32)):
+        if pattern and (nx % w or ny % 32 or (ny // 32) * w > 1024):
+            continue
+        best = None
+        for per_sm in (1, 2, 4):
+            run = lambda: ctx.roofline_probe(pattern, w, src, outs, per_sm)  # noqa: E731
+            for _ in range(3):
+                run()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            for _ in range(5):
+                a.record()
+                run()
+                b.record()
+                b.synchronize()
+                ms = a.elapsed_time(b)
+                best = ms if best is None else min(best, ms)
+        res[key] = round(bytes_moved / (best * 1e-3) / 1e9, 1)
+    return res
+
+
 def timed_sweep(ctx, torch, fields, outs, steps, warmup, world, fused=True, per_launch=True, profile=False):
     from x3div_b200._capi import Work
     groups = sweep_groups(ctx, fields, outs, fused)
@@ -459,6 +492,16 @@ def run_b200(args, world, rank, local):
                 "frac": round(dom["gbs"] / peak, 3), "traffic": traffic_bytes,
                 "kernel": FAMILY[dom_d] + f" ({group} operators per launch)",
                 "algorithmic_bytes_per_launch": per_launch_bytes, "peak_source": peak_kind}
+    # the same traffic with no arithmetic, in the dominant launch's order
+    ceil = pattern_ceilings(ctx, torch, fields[0], outs[:6])
+    if ceil:
+        cfg = dom["config"]
+        key = "flat" if FAMILY[dom_d] == "ls_stage_x" else f"tile_w{CONFIG_W[cfg] if 0 <= cfg < 16 else 16}"
+        if key in ceil:
+            roofline["pattern_ceiling_gbs"] = ceil[key]
+            roofline["pattern"] = key
+            roofline["frac_of_pattern"] = round(dom["gbs"] / ceil[key], 3)
+    out["ceilings"] = ceil
     out.update(value=value, ms=ms, fam=fam_stats, roofline=roofline, launches=launches)
     # the same 54 applications one operator per launch
     ms1, fam1, _, launches1, _ = timed_sweep(ctx, torch, fields, outs, args.steps, args.warmup,
@@ -606,6 +649,7 @@ def main():
                        "parallelism": f"{world} independent box(es), one per GPU"},
             "gpu_launches": res["launches"],
             "roofline": res["roofline"],
+            "pattern_ceilings_gbs": res.get("ceilings"),
             "kernels": res["fam"],
             "unfused": res["unfused"],
             "cpu_baseline": {"value": round(cpu_val, 4), "unit": "Gpts/s", "cores": cpu_threads(),

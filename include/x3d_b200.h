@@ -142,6 +142,16 @@ int x3d_ctx_sync(x3d_ctx ctx);
  * recording the failure; the next x3d_ctx_sync returns X3D_ETIMEOUT and
  * clears it, and the context stays usable.  No reference counterpart. */
 int x3d_ctx_selftest_timeout(x3d_ctx ctx, double limit_s);
+/* Measurement aid for the roofline of the sweep launches (no reference
+ * counterpart): moves one FP32 (nx, ny, nz) device field to six FP32 device
+ * fields (outs[6]) with no arithmetic, in a flat order (pattern 0: 16-byte
+ * vectors, consecutive threads on consecutive vectors) or in the y stage
+ * kernels' order (pattern 1: tiles of w in {8, 16, 32} x-adjacent columns
+ * of the ny rows of a z plane, 32 rows per thread; nx % w == 0,
+ * ny % 32 == 0), so that timing it gives the bandwidth that traffic mix and
+ * access order can reach.  ctas_per_sm sets the grid (0: 2 per SM). */
+int x3d_roofline_probe(x3d_ctx ctx, int pattern, int w, int ctas_per_sm, const void *in, void *const *outs,
+                       int nx, int ny, int nz);
 /* Text of the last error recorded on this context (never NULL). */
 const char *x3d_ctx_last_error(x3d_ctx ctx);
 /* Number of this library's kernels launched on the context so far (library

@@ -305,6 +305,15 @@ class Context:
     def poisson(self, rhs):
         self._check(self.L.x3d_poisson(self.handle, _ptr(rhs)))
 
+    def roofline_probe(self, pattern, w, src, outs, ctas_per_sm=0):
+        """x3d_roofline_probe: one FP32 field to six with no arithmetic, in a
+        flat order (pattern 0) or the y stage kernels' tile order (pattern 1,
+        w columns per tile)."""
+        nz, ny, nx = src.shape
+        arr = (ctypes.c_void_p * 6)(*[o.data_ptr() for o in outs])
+        self._check(self.L.x3d_roofline_probe(self.handle, int(pattern), int(w), int(ctas_per_sm), _ptr(src), arr,
+                                              nx, ny, nz))
+
     def poisson_zlines(self, spec, ny_loc, j0):
         """x3d_poisson_zlines: z transforms and mode division on a block of
         y rows of the x-y transformed spectrum (a complex128 CUDA tensor of

@@ -462,6 +462,23 @@ int x3d_ctx_sync(x3d_ctx ctx)
     return X3D_OK;
 }
 
+int x3d_roofline_probe(x3d_ctx ctx, int pattern, int w, int ctas_per_sm, const void *in, void *const *outs, int nx,
+                       int ny, int nz)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!in || !outs || nx < 1 || ny < 1 || nz < 1 || (pattern != 0 && pattern != 1))
+        return set_error(ctx, X3D_EINVAL, "bad probe request");
+    float *o[6];
+    for (int k = 0; k < 6; ++k) {
+        if (!outs[k] || !is_device_ptr(outs[k])) return set_error(ctx, X3D_EINVAL, "probe outputs must be device arrays");
+        o[k] = static_cast<float *>(outs[k]);
+    }
+    if (!is_device_ptr(in)) return set_error(ctx, X3D_EINVAL, "probe input must be a device array");
+    if (ctas_per_sm < 0 || ctas_per_sm > 32) return set_error(ctx, X3D_EINVAL, "ctas_per_sm must be 0..32");
+    return launch_roofline_probe(ctx, pattern, w, ctas_per_sm, static_cast<const float *>(in), o, nx, ny, nz);
+}
+
 int x3d_ctx_selftest_timeout(x3d_ctx ctx, double limit_s)
 {
     int rc = check_ctx(ctx);
