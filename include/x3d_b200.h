@@ -333,9 +333,15 @@ int x3d_poisson(x3d_ctx ctx, double *rhs);
  * cuFFT or 2decomp produce them).  In place: the forward z transform, the
  * division of every mode by -K ntot (zero where K < 1e-16), the inverse z
  * transform; the unnormalised 2-D c2r transforms then give the solution.
- * Device pointer; z lengths 2^p 3^q from 8 to 1024.  With 2decomp, the z
- * transforms of a distributed 3-D FFT run on Z pencils in the same way. */
+ * Device pointer; z lengths 2^p 3^q from 8 to 1024.  Builds no cuFFT plan
+ * and no spectrum of the whole box. */
 int x3d_poisson_zlines(x3d_ctx ctx, void *spec, int ny_loc, int j0);
+/* The same on a Z pencil of a p_row x p_col decomposition (2decomp's
+ * zstart/zend of the half spectrum): spec holds x modes i0 .. i0 + nxh_loc
+ * - 1 of the nx/2+1 and y rows j0 .. j0 + ny_loc - 1, all nz z points,
+ * ((nz, ny_loc, nxh_loc) with x fastest).  x3d_poisson_zlines is the case
+ * i0 = 0, nxh_loc = nx/2+1. */
+int x3d_poisson_zpencil(x3d_ctx ctx, void *spec, int nxh_loc, int i0, int ny_loc, int j0);
 
 /* ---- projection stage: module navier (src/navier.f90) ------------------- */
 

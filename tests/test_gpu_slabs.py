@@ -118,3 +118,34 @@ def test_slab_euler_steps_on_one_nccl_rank(oracle, torch_cuda, prec):
         ctx.close()
     finally:
         dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("shape,grid", [((24, 20, 16), (2, 2)), ((30, 12, 48), (3, 2)), ((16, 18, 96), (2, 3)),
+                                        ((40, 24, 64), (1, 3))])
+def test_poisson_zpencil_on_every_rank_block(oracle, torch_cuda, shape, grid):
+    """x3d_poisson_zpencil on each rank's Z pencil of the half spectrum of a
+    p_row x p_col grid (x modes and y rows both cut into blocks), one block
+    after another on this GPU, reassembled and transformed back, against the
+    oracle's poisson_000 on the whole box."""
+    torch = torch_cuda
+    from x3div_b200 import Context, X3DError
+    from x3div_b200.pencils import PencilLayout
+    nx, ny, nz = shape
+    lengths = (2 * np.pi, 1.5, 3.0)
+    ctx = Context(*shape, lengths=lengths, precision="f64")
+    g = np.random.default_rng(9).standard_normal(shape[::-1])
+    spec = torch.fft.rfft2(torch.from_numpy(g).cuda(), norm="backward")  # (nz, ny, nx/2+1)
+    out = torch.empty_like(spec)
+    L = PencilLayout((nx // 2 + 1, ny, nz), grid[0], grid[1], 0)
+    for r in range(grid[0] * grid[1]):
+        (i0, i1), (j0, j1), _ = L.block("z", r)
+        blk = spec[:, j0:j1, i0:i1].contiguous()
+        ctx.poisson_zpencil(blk, i1 - i0, i0, j1 - j0, j0)
+        out[:, j0:j1, i0:i1] = blk
+    p = torch.fft.irfft2(out, s=(ny, nx), norm="forward")
+    torch.cuda.synchronize()
+    ref = oracle.poisson(np.asfortranarray(g.transpose(2, 1, 0)), *lengths)
+    assert rel_err(p.cpu().numpy().transpose(2, 1, 0), ref) < 1e-12, (shape, grid)
+    with pytest.raises(X3DError):  # x modes past nx/2 + 1
+        ctx.poisson_zpencil(spec, nx // 2 + 1, 1, ny, 0)
+    ctx.close()

@@ -38,14 +38,15 @@ class OracleContext:
     def op(self, name):
         return name
 
-    def poisson_zlines(self, spec, ny_loc, j0):
+    def poisson_zpencil(self, spec, nxh_loc, i0, ny_loc, j0):
         """The z part of the spectral solve, restated with numpy's FFT and the
-        oracle's modified-wavenumber tables, on a (nz, ny_loc, nxh) block."""
+        oracle's modified-wavenumber tables, on a (nz, ny_loc, nxh_loc) block
+        of x modes from i0 and y rows from j0."""
         import torch
         nx, ny, nz = self.shape
         t = self.o.poisson_tables(nx, ny, nz, *self.lengths)
         c = np.fft.fft(spec.numpy(), axis=0)
-        i = np.arange(nx // 2 + 1)[None, None, :]
+        i = (i0 + np.arange(nxh_loc))[None, None, :]
         j = (j0 + np.arange(ny_loc))[None, :, None]
         k = np.arange(nz)[:, None, None]
         tyz = t["ty"][j] * t["tz"][k]

@@ -69,6 +69,7 @@ SIGNATURES = {
     "x3d_step_launch": [_vp],
     "x3d_ctx_selftest_timeout": [_vp, ctypes.c_double],
     "x3d_poisson_zlines": [_vp, _vp, _i, _i],
+    "x3d_poisson_zpencil": [_vp, _vp, _i, _i, _i, _i],
     "x3d_roofline_probe": [_vp, _i, _i, _i, _vp, ctypes.POINTER(_vp), _i, _i, _i],
     "x3d_buf_register": [_vp, _vp, ctypes.c_size_t, ctypes.POINTER(_vp)],
     "x3d_buf_unregister": [_vp, _vp],

@@ -320,6 +320,13 @@ class Context:
         shape (nz, ny_loc, nx//2 + 1))."""
         self._check(self.L.x3d_poisson_zlines(self.handle, _ptr(spec), int(ny_loc), int(j0)))
 
+    def poisson_zpencil(self, spec, nxh_loc, i0, ny_loc, j0):
+        """x3d_poisson_zpencil: the same on x modes i0 .. i0 + nxh_loc - 1 and
+        y rows j0 .. j0 + ny_loc - 1 (a complex128 CUDA tensor of shape (nz,
+        ny_loc, nxh_loc)): the Z pencil of a p_row x p_col decomposition."""
+        self._check(self.L.x3d_poisson_zpencil(self.handle, _ptr(spec), int(nxh_loc), int(i0), int(ny_loc),
+                                               int(j0)))
+
     def divergence(self, pp3, ux1, uy1, uz1, nlock=1):
         self._check(self.L.x3d_divergence(self.handle, _ptr(pp3), _ptr(ux1), _ptr(uy1), _ptr(uz1), int(nlock)))
 

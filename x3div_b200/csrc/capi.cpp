@@ -846,13 +846,20 @@ int x3d_poisson(x3d_ctx ctx, double *rhs)
     return sg.finish(poisson_solve(ctx, d));
 }
 
-int x3d_poisson_zlines(x3d_ctx ctx, void *spec, int ny_loc, int j0)
+int x3d_poisson_zpencil(x3d_ctx ctx, void *spec, int nxh_loc, int i0, int ny_loc, int j0)
 {
     int rc = check_ctx(ctx);
     if (rc) return rc;
     if ((rc = need_periodic(ctx))) return rc;
     if (!spec || !is_device_ptr(spec)) return set_error(ctx, X3D_EINVAL, "spec must be a device array");
-    return poisson_zlines(ctx, spec, ny_loc, j0);
+    return poisson_zpencil(ctx, spec, nxh_loc, i0, ny_loc, j0);
+}
+
+int x3d_poisson_zlines(x3d_ctx ctx, void *spec, int ny_loc, int j0)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    return x3d_poisson_zpencil(ctx, spec, ctx->nx / 2 + 1, 0, ny_loc, j0);
 }
 
 // ---- navier ----------------------------------------------------------------------------

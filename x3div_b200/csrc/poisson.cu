@@ -288,25 +288,27 @@ constexpr int kZftW = N <= 256 ? 16 : (N <= 512 ? 8 : 4);
 // K and mask of k_spectral_divide, inverse z transform.  The tile's modes go
 // from global memory straight into the first stage's registers and leave
 // the last inverse stage straight to global memory; the twiddles are copied
-// into shared memory first.
+// into shared memory first.  The spectrum is (nz, ny, nxl) with x fastest:
+// x modes ig0 .. ig0 + nxl - 1 of the nxh = nx/2 + 1 and y rows j0 .. j0 +
+// ny - 1 of the box (a Z pencil of the half spectrum).
 template <int N>
 __global__ void __launch_bounds__(kZftThreads, 2)
-    k_poisson_z(double2 *__restrict__ c, int nxh, int ny, int j0, const double2 *__restrict__ tw,
-                const double *__restrict__ k2x, const double *__restrict__ tx, const double *__restrict__ k2y,
-                const double *__restrict__ ty, const double *__restrict__ k2z, const double *__restrict__ tz,
-                double ntot)
+    k_poisson_z(double2 *__restrict__ c, int nxl, int ny, int ig0, int j0, int nxh,
+                const double2 *__restrict__ tw, const double *__restrict__ k2x, const double *__restrict__ tx,
+                const double *__restrict__ k2y, const double *__restrict__ ty, const double *__restrict__ k2z,
+                const double *__restrict__ tz, double ntot)
 {
     constexpr int W = kZftW<N>;
     extern __shared__ __align__(16) double2 zbuf[];
     double2 *const tws = zbuf + N * W;
-    const int tiles_i = (nxh + W - 1) / W;
+    const int tiles_i = (nxl + W - 1) / W;
     const int j = blockIdx.x / tiles_i;
     const int i0 = (blockIdx.x - j * tiles_i) * W;
     ZLines zl;
-    zl.base = c + (size_t)j * nxh + i0;
-    zl.zstride = (size_t)ny * nxh;
-    zl.lines = min(W, nxh - i0);
-    zl.i0 = i0;
+    zl.base = c + (size_t)j * nxl + i0;
+    zl.zstride = (size_t)ny * nxl;
+    zl.lines = min(W, nxl - i0);
+    zl.i0 = ig0 + i0;  // global index of the tile's first x mode
     zl.nxh = nxh;
     zl.tyj = __ldg(ty + j0 + j);  // j0: global index of the spectrum's first y row
     zl.k2yj = __ldg(k2y + j0 + j);
@@ -333,9 +335,11 @@ static bool zft_supported(int n)
     return false;
 }
 
-int poisson_setup(x3d_ctx_s *ctx)
+// The 1-D modified-wavenumber tables and, where a fused z kernel exists for
+// nz, its twiddles: all that the z part of the solve reads.
+static int poisson_tables(x3d_ctx_s *ctx)
 {
-    if (ctx->plans_ready) return X3D_OK;
+    if (ctx->d_k2x) return X3D_OK;
     const int nx = ctx->nx, ny = ctx->ny, nz = ctx->nz;
     std::vector<double> k2x, tx, k2y, ty, k2z, tz;
     waves_tables(nx, ctx->xlx, k2x, tx);
@@ -359,10 +363,7 @@ int poisson_setup(x3d_ctx_s *ctx)
     ctx->d_ty = tab + 2 * nx + ny;
     ctx->d_k2z = tab + 2 * nx + 2 * ny;
     ctx->d_tz = tab + 2 * nx + 2 * ny + nz;
-    const size_t spec = (size_t)nz * ny * (nx / 2 + 1) * sizeof(double2);
-    if (cudaMalloc(&ctx->spectrum, spec) != cudaSuccess) return set_error(ctx, X3D_ENOMEM, "poisson spectrum");
-    ctx->zfused = zft_supported(nz) && ctx->zfuse_allowed;
-    if (ctx->zfused) {
+    if (zft_supported(nz)) {
         std::vector<double> tw(2 * (size_t)nz);
         const double twopi = 2.0 * std::acos(-1.0);
         for (int t = 0; t < nz; ++t) {
@@ -372,6 +373,20 @@ int poisson_setup(x3d_ctx_s *ctx)
         if (cudaMalloc(&ctx->d_zft_tw, tw.size() * sizeof(double)) != cudaSuccess)
             return set_error(ctx, X3D_ENOMEM, "poisson twiddles");
         cudaMemcpy(ctx->d_zft_tw, tw.data(), tw.size() * sizeof(double), cudaMemcpyHostToDevice);
+    }
+    return X3D_OK;
+}
+
+int poisson_setup(x3d_ctx_s *ctx)
+{
+    if (ctx->plans_ready) return X3D_OK;
+    int rc = poisson_tables(ctx);
+    if (rc) return rc;
+    const int nx = ctx->nx, ny = ctx->ny, nz = ctx->nz;
+    const size_t spec = (size_t)nz * ny * (nx / 2 + 1) * sizeof(double2);
+    if (cudaMalloc(&ctx->spectrum, spec) != cudaSuccess) return set_error(ctx, X3D_ENOMEM, "poisson spectrum");
+    ctx->zfused = ctx->d_zft_tw && ctx->zfuse_allowed;
+    if (ctx->zfused) {
         int dims[2] = {ny, nx};
         if (cufftPlanMany(&ctx->plan_d2z, 2, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_D2Z, nz) != CUFFT_SUCCESS ||
             cufftPlanMany(&ctx->plan_z2d, 2, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_Z2D, nz) != CUFFT_SUCCESS)
@@ -384,20 +399,21 @@ int poisson_setup(x3d_ctx_s *ctx)
     return X3D_OK;
 }
 
-// The fused z kernel over a spectrum of ny_loc y rows starting at global row
-// j0 ((nz, ny_loc, nx/2+1), x fastest).
-static int launch_poisson_z(x3d_ctx_s *ctx, double2 *spec, int ny_loc, int j0)
+// The fused z kernel over a spectrum of nxl x modes starting at global mode
+// i0 and ny_loc y rows starting at global row j0 ((nz, ny_loc, nxl), x
+// fastest).
+static int launch_poisson_z(x3d_ctx_s *ctx, double2 *spec, int nxl, int i0, int ny_loc, int j0)
 {
     const int nxh = ctx->nx / 2 + 1;
     const double ntot = (double)ctx->nx * (double)ctx->ny * (double)ctx->nz;
     auto go = [&](auto kern, int W) {
-        const unsigned grid = (unsigned)(((nxh + W - 1) / W) * ny_loc);
+        const unsigned grid = (unsigned)(((nxl + W - 1) / W) * ny_loc);
         const size_t smem = ((size_t)ctx->nz * W + ctx->nz) * sizeof(double2);  // tile + twiddles
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         ++ctx->launches;
-        kern<<<grid, kZftThreads, smem, ctx->stream>>>(spec, nxh, ny_loc, j0, (const double2 *)ctx->d_zft_tw,
-                                                       ctx->d_k2x, ctx->d_tx, ctx->d_k2y, ctx->d_ty, ctx->d_k2z,
-                                                       ctx->d_tz, ntot);
+        kern<<<grid, kZftThreads, smem, ctx->stream>>>(spec, nxl, ny_loc, i0, j0, nxh,
+                                                       (const double2 *)ctx->d_zft_tw, ctx->d_k2x, ctx->d_tx,
+                                                       ctx->d_k2y, ctx->d_ty, ctx->d_k2z, ctx->d_tz, ntot);
         return cuda_check(ctx, cudaGetLastError(), "k_poisson_z");
     };
     switch (ctx->nz) {
@@ -419,7 +435,7 @@ int poisson_solve(x3d_ctx_s *ctx, double *rhs)
     if (cufftExecD2Z(ctx->plan_d2z, rhs, (cufftDoubleComplex *)ctx->spectrum) != CUFFT_SUCCESS)
         return set_error(ctx, X3D_ECUDA, "cufftExecD2Z failed");
     if (ctx->zfused) {
-        rc = launch_poisson_z(ctx, (double2 *)ctx->spectrum, ctx->ny, 0);
+        rc = launch_poisson_z(ctx, (double2 *)ctx->spectrum, ctx->nx / 2 + 1, 0, ctx->ny, 0);
         if (rc) return rc;
         if (cufftExecZ2D(ctx->plan_z2d, (cufftDoubleComplex *)ctx->spectrum, rhs) != CUFFT_SUCCESS)
             return set_error(ctx, X3D_ECUDA, "cufftExecZ2D failed");
@@ -445,15 +461,17 @@ int poisson_solve(x3d_ctx_s *ctx, double *rhs)
     return X3D_OK;
 }
 
-// The z part of the spectral solve on a block of y rows of the x-y
-// transformed spectrum, for a box whose y rows are spread over ranks.
-int poisson_zlines(x3d_ctx_s *ctx, void *spec, int ny_loc, int j0)
+// The z part of the spectral solve on a block of x modes and y rows of the
+// x-y transformed spectrum, for a box spread over ranks.  Needs only the
+// wavenumber tables and twiddles: no plans or spectrum of the whole box.
+int poisson_zpencil(x3d_ctx_s *ctx, void *spec, int nxl, int i0, int ny_loc, int j0)
 {
-    int rc = poisson_setup(ctx);
+    int rc = poisson_tables(ctx);
     if (rc) return rc;
-    if (!ctx->zfused) return set_error(ctx, X3D_EUNSUPPORTED, "no fused z transform for this nz");
+    if (!ctx->d_zft_tw) return set_error(ctx, X3D_EUNSUPPORTED, "no fused z transform for this nz");
     if (ny_loc < 1 || j0 < 0 || j0 + ny_loc > ctx->ny) return set_error(ctx, X3D_EINVAL, "bad block of y rows");
-    return launch_poisson_z(ctx, static_cast<double2 *>(spec), ny_loc, j0);
+    if (nxl < 1 || i0 < 0 || i0 + nxl > ctx->nx / 2 + 1) return set_error(ctx, X3D_EINVAL, "bad block of x modes");
+    return launch_poisson_z(ctx, static_cast<double2 *>(spec), nxl, i0, ny_loc, j0);
 }
 
 void poisson_free(x3d_ctx_s *ctx)

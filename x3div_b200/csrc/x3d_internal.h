@@ -187,7 +187,7 @@ int launch_sub3(x3d_ctx_s *ctx, bool fp32, void *u, void *v, void *w, const void
 int launch_mul(x3d_ctx_s *ctx, bool fp32, void *out, const void *a, const void *b, size_t n);
 int launch_scale_y(x3d_ctx_s *ctx, bool fp32, void *t, const double *ppy, int nx, int ny, int nz);
 int launch_wait_selftest(x3d_ctx_s *ctx, uint64_t limit_ns);
-int poisson_zlines(x3d_ctx_s *ctx, void *spec, int ny_loc, int j0);
+int poisson_zpencil(x3d_ctx_s *ctx, void *spec, int nxl, int i0, int ny_loc, int j0);
 int launch_roofline_probe(x3d_ctx_s *ctx, int pattern, int w, int ctas_per_sm, const float *in, float *const *outs,
                           int nx, int ny, int nz);
 

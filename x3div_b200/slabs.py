@@ -13,23 +13,17 @@ become one all-to-all each: rank r sends rank s the block of its slab that s
 owns in the other layout.  Blocks follow 2decomp's distribution: the first
 n mod P ranks hold one plane more.
 
-Device tensors are C-ordered (nz, ny, nx) views of the Fortran (nx, ny, nz)
-layout, as in the rest of the package.  The collectives go through
-torch.distributed: NCCL over NVLink for CUDA tensors, gloo for CPU tensors.
+This is the p_row = 1 case of x3div_b200.pencils, with the process group
+of the y <-> z transposes passed in directly.  Device tensors are C-ordered
+(nz, ny, nx) views of the Fortran (nx, ny, nz) layout, as in the rest of the
+package.
 """
 from __future__ import annotations
 
 from dataclasses import dataclass
 
-
-def split(n: int, parts: int, rank: int):
-    """[start, end) of block `rank` when n points are cut into `parts` blocks,
-    the first n mod parts blocks one point longer."""
-    if parts < 1 or not 0 <= rank < parts:
-        raise ValueError("bad block request")
-    base, extra = divmod(n, parts)
-    start = rank * base + min(rank, extra)
-    return start, start + base + (1 if rank < extra else 0)
+from . import pencils as _pencils
+from .pencils import SWEEP, split  # noqa: F401  (re-exported)
 
 
 @dataclass(frozen=True)
@@ -64,89 +58,22 @@ class SlabLayout:
         y0, y1 = self.yslab()
         return self.shape[0], y1 - y0, self.shape[2]
 
-
-def _all_to_all(recv, send, out_splits, in_splits, group):
-    import torch.distributed as dist
-    if dist.is_available() and dist.is_initialized():
-        dist.all_to_all_single(recv, send, out_splits, in_splits, group=group)
-    else:  # one rank: the exchange is a copy
-        recv.copy_(send)
+    def pencils(self, group=None):
+        """The 1 x world pencil decomposition this layout is, with `group`
+        (default: the default process group) for the y <-> z transposes."""
+        return _pencils.Pencils(_pencils.PencilLayout(tuple(self.shape), 1, self.world, self.rank), None, group)
 
 
 def transpose_y_to_z(zslab, layout: SlabLayout, group=None):
     """X/Y pencil (a (nz_r, ny, nx) tensor) -> Z pencil ((nz, ny_s, nx) on
     rank s): 2decomp's transpose_y_to_z at p_row = 1."""
-    import torch
-    nx, ny, nz = layout.shape
-    z0, z1 = layout.zslab()
-    if tuple(zslab.shape) != (z1 - z0, ny, nx):
-        raise ValueError("not this rank's X/Y pencil")
-    blocks = [zslab[:, y0:y1, :].reshape(-1) for y0, y1 in (layout.yslab(s) for s in range(layout.world))]
-    send = torch.cat(blocks)
-    y0, y1 = layout.yslab()
-    out_splits = [(b - a) * (y1 - y0) * nx for a, b in (layout.zslab(r) for r in range(layout.world))]
-    recv = torch.empty(sum(out_splits), dtype=zslab.dtype, device=zslab.device)
-    _all_to_all(recv, send, out_splits, [b.numel() for b in blocks], group)
-    out = torch.empty((nz, y1 - y0, nx), dtype=zslab.dtype, device=zslab.device)
-    off = 0
-    for r in range(layout.world):
-        a, b = layout.zslab(r)
-        n = out_splits[r]
-        out[a:b] = recv[off:off + n].view(b - a, y1 - y0, nx)
-        off += n
-    return out
+    return _pencils.transpose_y_to_z(zslab, layout.pencils(group))
 
 
 def transpose_z_to_y(yslab, layout: SlabLayout, group=None):
     """Z pencil ((nz, ny_r, nx)) -> X/Y pencil ((nz_s, ny, nx) on rank s):
     2decomp's transpose_z_to_y at p_row = 1."""
-    import torch
-    nx, ny, nz = layout.shape
-    y0, y1 = layout.yslab()
-    if tuple(yslab.shape) != (nz, y1 - y0, nx):
-        raise ValueError("not this rank's Z pencil")
-    blocks = [yslab[a:b].reshape(-1) for a, b in (layout.zslab(s) for s in range(layout.world))]
-    send = torch.cat(blocks)
-    z0, z1 = layout.zslab()
-    out_splits = [(z1 - z0) * (b - a) * nx for a, b in (layout.yslab(r) for r in range(layout.world))]
-    recv = torch.empty(sum(out_splits), dtype=yslab.dtype, device=yslab.device)
-    _all_to_all(recv, send, out_splits, [b.numel() for b in blocks], group)
-    out = torch.empty((z1 - z0, ny, nx), dtype=yslab.dtype, device=yslab.device)
-    off = 0
-    for r in range(layout.world):
-        a, b = layout.yslab(r)
-        n = out_splits[r]
-        out[:, a:b, :] = recv[off:off + n].view(z1 - z0, b - a, nx)
-        off += n
-    return out
-
-
-# The six operator families of a sweep, by direction: (routine, operator).
-SWEEP = {
-    0: [("derx", "derx"), ("derxx", "derxx"), ("derxvp", "derxvp"), ("derxpv", "derxpv"),
-        ("interxvp", "intxvp"), ("interxpv", "intxpv")],
-    1: [("dery", "dery"), ("deryy", "deryy"), ("deryvp", "deryvp"), ("derypv", "derypv"),
-        ("interyvp", "intyvp"), ("interypv", "intypv")],
-    2: [("derz", "derz"), ("derzz", "derzz"), ("derzvp", "derzvp"), ("derzpv", "derzpv"),
-        ("interzvp", "intzvp"), ("interzpv", "intzpv")],
-}
-
-
-def _call(ctx, routine, t, u, op, ext):
-    nx, ny, nz = ext
-    fn = getattr(ctx, routine)
-    if routine in ("dery",):
-        fn(t, u, op, None, nx, ny, nz)
-    elif routine in ("deryvp", "derypv"):
-        fn(t, u, op, None, nx, ny, ny, nz)
-    elif routine.endswith(("xvp", "xpv")):
-        fn(t, u, op, nx, nx, ny, nz)
-    elif routine.endswith(("yvp", "ypv")):
-        fn(t, u, op, nx, ny, ny, nz)
-    elif routine.endswith(("zvp", "zpv")):
-        fn(t, u, op, nx, ny, nz, nz)
-    else:
-        fn(t, u, op, nx, ny, nz)
+    return _pencils.transpose_z_to_y(yslab, layout.pencils(group))
 
 
 def sweep(ctx, field, layout: SlabLayout, group=None):
@@ -155,110 +82,21 @@ def sweep(ctx, field, layout: SlabLayout, group=None):
     families on its Z pencil (one transpose each way).  ctx is a periodic
     context made for the global box; field is the rank's X/Y pencil.  Returns
     {direction: [six outputs in X/Y-pencil layout]}."""
-    import torch
-    ext = layout.xy_extents
-    out = {}
-    for d in (0, 1):
-        res = []
-        for routine, opname in SWEEP[d]:
-            t = torch.empty_like(field)
-            _call(ctx, routine, t, field, ctx.op(opname), ext)
-            res.append(t)
-        out[d] = res
-    zp = transpose_y_to_z(field, layout, group)
-    zext = layout.z_extents
-    res = []
-    for routine, opname in SWEEP[2]:
-        t = torch.empty_like(zp)
-        _call(ctx, routine, t, zp, ctx.op(opname), zext)
-        res.append(transpose_z_to_y(t, layout, group))
-    out[2] = res
-    return out
+    return _pencils.sweep(ctx, field, layout.pencils(group))
 
 
 def poisson(ctx, rhs, layout: SlabLayout, group=None):
     """poisson_000 (src/poisson.f90:276-419) on a box spread over the ranks,
-    in place on this rank's X/Y pencil of the FP64 field ((nz_r, ny, nx)).
-    The 2-D x-y transforms of the rank's z planes (cuFFT through torch.fft,
-    unnormalised both ways) bracket the z part, which runs on the rank's
-    block of y rows after a transpose of the half spectrum
-    (x3d_poisson_zlines: z transforms and the mode division)."""
-    import torch
-    nx, ny, nz = layout.shape
-    nxh = nx // 2 + 1
-    spec = torch.fft.rfft2(rhs, norm="backward")  # (nz_r, ny, nxh)
-    half = SlabLayout((2 * nxh, ny, nz), layout.rank, layout.world)  # the spectrum as 2 nxh reals per row
-    zs = transpose_y_to_z(torch.view_as_real(spec).reshape(spec.shape[0], ny, 2 * nxh), half, group)
-    y0, y1 = layout.yslab()
-    ctx.poisson_zlines(torch.view_as_complex(zs.view(nz, y1 - y0, nxh, 2)), y1 - y0, y0)
-    back = transpose_z_to_y(zs, half, group)
-    z0, z1 = layout.zslab()
-    rhs.copy_(torch.fft.irfft2(torch.view_as_complex(back.view(z1 - z0, ny, nxh, 2)), s=(ny, nx), norm="forward"))
-    return rhs
-
-
-def _apply(ctx, routine, opname, u, ext):
-    import torch
-    t = torch.empty_like(u)
-    _call(ctx, routine, t, u, ctx.op(opname), ext)
-    return t
+    in place on this rank's X/Y pencil of the FP64 field ((nz_r, ny, nx)):
+    2-D x-y transforms of the rank's z planes, the z part on its block of y
+    rows after a transpose of the half spectrum (x3d_poisson_zpencil), and
+    back."""
+    return _pencils.poisson(ctx, rhs, layout.pencils(group))
 
 
 def euler_step(ctx, u, du, pp3, pg, dt, layout: SlabLayout, group=None):
-    """One timestep (src/xcompact3d.f90:80-95) on a box spread over the
-    ranks, from the library's line solves on local extents, elementwise
-    tensor arithmetic and the slab transposes, in the reference's order:
-    momentum_rhs_eq (src/transeq.f90:44-355) with the x and y parts on the
-    rank's X/Y pencil and the z part on its Z pencil; int_time
-    (src/time_integrators.f90:40-44); divergence (src/navier.f90:98-236)
-    into the FP64 pp3; the slab Poisson solve; gradp
-    (src/navier.f90:249-359) and cor_vel (:64-91).  u, du, pg: the three
-    velocity, increment and pressure-gradient components as this rank's X/Y
-    pencils; pp3: its FP64 X/Y pencil.  In place, like x3d_euler_step."""
-    import torch
-    ext, zext = layout.xy_extents, layout.z_extents
-    T = lambda a: transpose_y_to_z(a, layout, group)  # noqa: E731
-    Ti = lambda a: transpose_z_to_y(a, layout, group)  # noqa: E731
-    ux, uy, uz = u
-    uzz = T(uz)
-    for c in range(3):  # calculate_transeq_rhs
-        uc = u[c]
-        ta = ux * uc
-        td = _apply(ctx, "derx", "derx", ta, ext)
-        ta = _apply(ctx, "derx", "derx", uc, ext)
-        duc = td + ux * ta
-        td = uc * uy
-        tg = _apply(ctx, "dery", "dery", td, ext)
-        td = _apply(ctx, "dery", "dery", uc, ext)
-        tg = tg + uy * td
-        ucz = uzz if c == 2 else T(uc)
-        tdz = ucz * uzz
-        tgz = _apply(ctx, "derz", "derz", tdz, zext)
-        tdz = _apply(ctx, "derz", "derz", ucz, zext)
-        tg = tg + Ti(tgz + uzz * tdz)
-        du[c].copy_(duc + tg)
-    for c in range(3):  # int_time, Euler: u = dt du + u
-        u[c].copy_(dt * du[c] + u[c])
-    # divergence
-    pp1 = _apply(ctx, "derxvp", "derxvp", ux, ext)
-    pgy1 = _apply(ctx, "interxvp", "intxvp", uy, ext)
-    pgz1 = _apply(ctx, "interxvp", "intxvp", uz, ext)
-    upi2 = _apply(ctx, "interyvp", "intyvp", pp1, ext)
-    duydypi2 = _apply(ctx, "deryvp", "deryvp", pgy1, ext) + upi2
-    upi2 = _apply(ctx, "interyvp", "intyvp", pgz1, ext)
-    a, b = T(duydypi2), T(upi2)
-    p3 = _apply(ctx, "interzvp", "intzvp", a, zext).double() + _apply(ctx, "derzvp", "derzvp", b, zext).double()
-    pp3.copy_(Ti(p3))
-    poisson(ctx, pp3, layout, group)
-    # gradp + cor_vel
-    p3z = T(pp3).to(ux.dtype)
-    ppi3 = Ti(_apply(ctx, "interzpv", "intzpv", p3z, zext))
-    pgz3 = Ti(_apply(ctx, "derzpv", "derzpv", p3z, zext))
-    ppi2 = _apply(ctx, "interypv", "intypv", ppi3, ext)
-    pgy2 = _apply(ctx, "derypv", "derypv", ppi3, ext)
-    pgzi2 = _apply(ctx, "interypv", "intypv", pgz3, ext)
-    pg[0].copy_(_apply(ctx, "derxpv", "derxpv", ppi2, ext))
-    pg[1].copy_(_apply(ctx, "interxpv", "intxpv", pgy2, ext))
-    pg[2].copy_(_apply(ctx, "interxpv", "intxpv", pgzi2, ext))
-    for c in range(3):
-        u[c].sub_(pg[c])
+    """One timestep (src/xcompact3d.f90:80-95) on a box spread over the ranks
+    in z-slabs (x3div_b200.pencils.euler_step at p_row = 1).  u, du, pg: the
+    three velocity, increment and pressure-gradient components as this
+    rank's X/Y pencils; pp3: its FP64 X/Y pencil.  In place."""
+    return _pencils.euler_step(ctx, u, du, pp3, pg, dt, layout.pencils(group))
