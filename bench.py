@@ -58,12 +58,14 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--profile-timed", nargs="?", const="sweep", default=None, choices=["sweep", "euler"],
-                    help="bracket the timed FP32 sweep (or the FP32-mixed Euler steps) with "
-                         "cudaProfilerStart/Stop, for ncu --profile-from-start off")
+    ap.add_argument("--profile-timed", nargs="?", const="sweep", default=None, choices=["sweep", "euler", "b48"],
+                    help="bracket the timed FP32 sweep (or the FP32-mixed Euler steps, or the batch "
+                         "replays) with cudaProfilerStart/Stop, for ncu --profile-from-start off")
     ap.add_argument("--kernel-config", type=int, default=None,
                     help="force one kernel configuration (x3d_ctx_set_kernel) instead of autotuning")
     ap.add_argument("--no-b48", action="store_true")
+    ap.add_argument("--b48-count", type=int, default=48,
+                    help="boxes in the batching workload (the first of the same seeded draw; 48 by default)")
     ap.add_argument("--c5", action="store_true",
                     help="also run 20 Euler steps at 768^3, FP32-mixed and FP64 (reported under c5)")
     return ap.parse_args()
@@ -393,7 +395,7 @@ def run_b48(args, world, rank, local, torch):
     share), 3 FP32 fields each (Taylor-Green + N(0, (1e-2)^2)), all 54 operator
     applications per box in one persistent launch, replayed from a CUDA graph."""
     from x3div_b200 import Batch, b48_boxes, box_points, shard_boxes
-    boxes = b48_boxes()
+    boxes = b48_boxes(count=args.b48_count)
     mine = shard_boxes(boxes, world)[rank]
     my = [boxes[i] for i in mine]
     g = torch.Generator(device="cuda")
@@ -423,11 +425,15 @@ def run_b48(args, world, rank, local, torch):
     torch.cuda.synchronize()
     barrier(world)
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if args.profile_timed == "b48":
+        torch.cuda.profiler.start()
     a.record()
     for _ in range(args.steps):
         batch.replay()
     b.record()
     torch.cuda.synchronize()
+    if args.profile_timed == "b48":
+        torch.cuda.profiler.stop()
     batch.sync()
     ms = max_over_ranks(a.elapsed_time(b), world)
     pts = torch.tensor([float(info["points"])], dtype=torch.float64, device="cuda")

@@ -108,6 +108,10 @@ __global__ void k_spectral_divide(double2 *c, unsigned nxh, unsigned ny, unsigne
 constexpr int kZftThreads = 512;
 constexpr int kZftVals = 8;    // values a thread holds in one stage
 
+// Lines per tile for a transform of length N (W N <= kZftThreads kZftVals).
+template <int N>
+constexpr int kZftW = N <= 256 ? 16 : (N <= 512 ? 8 : 4);
+
 __device__ __forceinline__ double2 cmul(double2 a, double2 b)
 {
     return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -172,17 +176,17 @@ struct ZLines {
     double2 *base;   // the tile's first line at k = 0
     size_t zstride;  // elements between consecutive k
     int lines;       // x modes of the tile inside the spectrum (<= W)
-    int i0, nxh;
     double tyj, k2yj, ntot;
-    const double *__restrict__ tx, *__restrict__ k2x, *__restrict__ tz, *__restrict__ k2z;
+    const double2 *xtab;  // shared: (tx, k2x) of the tile's W x modes
+    const double2 *ztab;  // shared: (tz, k2z) of the N z modes
     // c <- -c / (K ntot), zero where K < 1e-16: the K and mask of
     // k_spectral_divide for mode (i0 + l, j, k)
     __device__ __forceinline__ double2 divide(double2 v, int k, int l) const
     {
-        const int i = min(i0 + l, nxh - 1);
-        const double txi = __ldg(tx + i), tzk = __ldg(tz + k);
+        const double2 x = xtab[l], z = ztab[k];
+        const double txi = x.x, tzk = z.x;
         const double tyz = tyj * tzk, txz = txi * tzk, txy = txi * tyj;
-        const double kk = __ldg(k2x + i) * (tyz * tyz) + k2yj * (txz * txz) + __ldg(k2z + k) * (txy * txy);
+        const double kk = x.y * (tyz * tyz) + k2yj * (txz * txz) + z.y * (txy * txy);
         const double f = kk < 1.e-16 ? 0.0 : -1.0 / (kk * ntot);
         return make_double2(v.x * f, v.y * f);
     }
@@ -280,15 +284,13 @@ __device__ __forceinline__ void zft(double2 *buf, const double2 *tw, const ZLine
     }
 }
 
-// Lines per tile for a transform of length N (W N <= kZftThreads kZftVals).
-template <int N>
-constexpr int kZftW = N <= 256 ? 16 : (N <= 512 ? 8 : 4);
 
 // One CTA per (j, tile of W x-modes): z transform, c <- -c / (K ntot) with the
 // K and mask of k_spectral_divide, inverse z transform.  The tile's modes go
 // from global memory straight into the first stage's registers and leave
-// the last inverse stage straight to global memory; the twiddles are copied
-// into shared memory first.  The spectrum is (nz, ny, nxl) with x fastest:
+// the last inverse stage straight to global memory; the twiddles and the
+// wavenumber tables the division reads are copied into shared memory
+// first.  The spectrum is (nz, ny, nxl) with x fastest:
 // x modes ig0 .. ig0 + nxl - 1 of the nxh = nx/2 + 1 and y rows j0 .. j0 +
 // ny - 1 of the box (a Z pencil of the half spectrum).
 template <int N>
@@ -301,6 +303,8 @@ __global__ void __launch_bounds__(kZftThreads, 2)
     constexpr int W = kZftW<N>;
     extern __shared__ __align__(16) double2 zbuf[];
     double2 *const tws = zbuf + N * W;
+    double2 *const ztab = tws + N;
+    double2 *const xtab = ztab + N;
     const int tiles_i = (nxl + W - 1) / W;
     const int j = blockIdx.x / tiles_i;
     const int i0 = (blockIdx.x - j * tiles_i) * W;
@@ -308,16 +312,19 @@ __global__ void __launch_bounds__(kZftThreads, 2)
     zl.base = c + (size_t)j * nxl + i0;
     zl.zstride = (size_t)ny * nxl;
     zl.lines = min(W, nxl - i0);
-    zl.i0 = ig0 + i0;  // global index of the tile's first x mode
-    zl.nxh = nxh;
     zl.tyj = __ldg(ty + j0 + j);  // j0: global index of the spectrum's first y row
     zl.k2yj = __ldg(k2y + j0 + j);
     zl.ntot = ntot;
-    zl.tx = tx;
-    zl.k2x = k2x;
-    zl.tz = tz;
-    zl.k2z = k2z;
-    for (int t = threadIdx.x; t < N; t += kZftThreads) tws[t] = __ldg(tw + t);
+    zl.xtab = xtab;
+    zl.ztab = ztab;
+    for (int t = threadIdx.x; t < N; t += kZftThreads) {
+        tws[t] = __ldg(tw + t);
+        ztab[t] = make_double2(__ldg(tz + t), __ldg(k2z + t));
+    }
+    if (threadIdx.x < W) {  // ig0 + i0: global index of the tile's first x mode
+        const int i = min(ig0 + i0 + (int)threadIdx.x, nxh - 1);
+        xtab[threadIdx.x] = make_double2(__ldg(tx + i), __ldg(k2x + i));
+    }
     __syncthreads();
     zft<N, W, false>(zbuf, tws, zl);
     zft<N, W, true>(zbuf, tws, zl);
@@ -408,7 +415,8 @@ static int launch_poisson_z(x3d_ctx_s *ctx, double2 *spec, int nxl, int i0, int 
     const double ntot = (double)ctx->nx * (double)ctx->ny * (double)ctx->nz;
     auto go = [&](auto kern, int W) {
         const unsigned grid = (unsigned)(((nxl + W - 1) / W) * ny_loc);
-        const size_t smem = ((size_t)ctx->nz * W + ctx->nz) * sizeof(double2);  // tile + twiddles
+        // tile, twiddles, z and x wavenumber tables
+        const size_t smem = ((size_t)ctx->nz * W + 2 * (size_t)ctx->nz + W) * sizeof(double2);
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         ++ctx->launches;
         kern<<<grid, kZftThreads, smem, ctx->stream>>>(spec, nxl, ny_loc, i0, j0, nxh,
