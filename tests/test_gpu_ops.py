@@ -287,3 +287,26 @@ def test_y_routines_apply_stretching_metric(oracle, torch_cuda, contexts, prec, 
         ref = oracle.apply(kind, Y, u_used, ctx.dy) * metric[None, :, None]
         err = rel_err(np.asarray(got, dtype=np.float64), ref)
         assert err < tol, (routine, opname, prec, where, err)
+
+
+# Lines longer than any staged tile holds: 4096 points (16 FP32 lines of
+# 4096 need 256 KB of shared memory, above the 227 KB a CTA can have) and
+# 1024-2048 points, along each direction in turn.  The library picks
+# whichever kernel takes the shape; the results must not depend on it.
+@pytest.mark.parametrize("shape", [(4096, 8, 8), (8, 4096, 8), (8, 8, 4096), (2048, 12, 16), (16, 1024, 24)])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_long_lines(oracle, torch_cuda, contexts, shape, prec):
+    torch = torch_cuda
+    from x3div_b200 import to_device, to_host
+    ctx = contexts(shape, prec)
+    dt = torch.float64 if prec == "f64" else torch.float32
+    u_d = to_device(seeded_field(shape, seed=4096 + sum(shape), noise=1e-2), dt)
+    used = to_host(u_d).astype(np.float64)
+    d = {X: ctx.dx, Y: ctx.dy, Z: ctx.dz}
+    tol = 1e-12 if prec == "f64" else 1e-5
+    for routine, opname, kind, direction, style in ROUTINES:
+        t_d = torch.empty_like(u_d)
+        call(ctx, routine, style, t_d, u_d, ctx.op(opname), shape)
+        ctx.sync()
+        err = rel_err(to_host(t_d), oracle.apply(kind, direction, used, d[direction]))
+        assert err < tol, (routine, shape, prec, err)

@@ -36,10 +36,11 @@ def test_poisson(oracle, torch_cuda, shape):
 
 
 # z lengths of every radix pattern of the fused z-transform kernel (8s, 4, 2,
-# 3s; one to four tiles of x modes, a last tile of one mode) and one that
-# takes the 3-D cuFFT path (nz = 40 = 8 * 5)
+# 3s; one to four tiles of x modes, a last tile of one mode) and two that
+# take the 3-D cuFFT path (nz = 40 = 8 * 5, and nz = 2048, above the longest
+# fused transform)
 @pytest.mark.parametrize("shape", [(16, 10, 8), (30, 12, 12), (34, 8, 48), (20, 8, 96), (14, 8, 192),
-                                   (8, 8, 384), (8, 8, 768), (10, 8, 1024), (12, 10, 40)])
+                                   (8, 8, 384), (8, 8, 768), (10, 8, 1024), (12, 10, 40), (8, 12, 2048)])
 def test_poisson_z_lengths(oracle, torch_cuda, shape):
     from x3div_b200 import to_device, to_host
     ctx = ctx_for(shape)
