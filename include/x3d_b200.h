@@ -260,8 +260,17 @@ int x3d_ctx_set_kernel(x3d_ctx ctx, int cfg);
 int x3d_autotune_choice(x3d_ctx ctx, int dir, int group, int *cfg);
 /* The configuration chosen for a fused stage of the Euler step (*cfg = -1
  * when not tuned): stage is one of transeq_x, transeq_y, transeq_z, div_x,
- * div_y, div_z, gradp_z, gradp_y, gradp_x, gradp_x_cor. */
+ * div_y, div_z, gradp_z, gradp_y, gradp_x, gradp_x_cor.  A stage may run as
+ * several launches: "<stage>.split" = 1 for a momentum stage as two launches
+ * ("<stage>.b", then "<stage>.a"), "<stage>.parts" = k > 1 for a stage as k
+ * launches over disjoint staged inputs ("<stage>.1" .. "<stage>.k"); each
+ * launch has its own configuration under its own name. */
 int x3d_autotune_stage_choice(x3d_ctx ctx, const char *stage, int *cfg);
+/* Sets one of those choices (a saved tuning, or a form to test); value -1
+ * removes it.  Configurations are 0..15; "<stage>.split" 0 or 1;
+ * "<stage>.parts" a launch count, used only where the stage splits into
+ * exactly that many parts.  Extension. */
+int x3d_ctx_set_stage_choice(x3d_ctx ctx, const char *stage, int value);
 
 /* ---- batches of independent boxes ----------------------------------------- */
 

@@ -152,6 +152,58 @@ def test_autotuned_euler_steps_match_oracle(oracle, torch_cuda, prec):
     ctx.close()
 
 
+# Every stage that can run as several launches, forced on: the momentum
+# stages as two launches of two staged fields, the others as one launch per
+# disjoint set of staged inputs.
+SPLIT_FORMS = {"transeq_x.split": 1, "transeq_y.split": 1, "transeq_z.split": 1, "div_x.parts": 3,
+               "div_y.parts": 2, "gradp_y.parts": 2, "gradp_x.parts": 3, "gradp_x_cor.parts": 3}
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("shape", [(64, 48, 32), (36, 60, 62)])
+def test_split_stage_forms_match_the_one_launch_stages(oracle, torch_cuda, prec, shape):
+    """With every split form pinned (x3d_ctx_set_stage_choice), three Euler
+    steps equal those of the one-launch stages bit for bit (the same kernel
+    configuration and the same arithmetic per output; the z momentum stage
+    updates u in place, so its launch that writes u_z runs last) and match
+    the oracle; the split context launched more kernels."""
+    torch = torch_cuda
+    from x3div_b200 import to_device, to_host
+    one, split = ctx_for(shape, prec), ctx_for(shape, prec)
+    for k, v in SPLIT_FORMS.items():
+        split.set_stage_choice(k, v)
+        assert split.autotune_stage_choice(k) == v
+    dt_ = torch.float64 if prec == "f64" else torch.float32
+    U = [to_device(a, dt_) for a in fields(shape, (14, 15, 16))]
+    V = [a.clone() for a in U]
+    ref = [to_host(a).astype(np.float64) for a in U]
+    du = [torch.empty_like(U[0]) for _ in range(3)]
+    pg = [torch.empty_like(U[0]) for _ in range(3)]
+    dv = [torch.empty_like(U[0]) for _ in range(3)]
+    pv = [torch.empty_like(U[0]) for _ in range(3)]
+    pp3 = torch.empty(shape[::-1], dtype=torch.float64, device="cuda")
+    pq = torch.empty_like(pp3)
+    n1, n2 = one.launch_count(), split.launch_count()
+    for _ in range(3):
+        one.euler_step(*U, *du, pp3, *pg, 1e-3)
+        split.euler_step(*V, *dv, pq, *pv, 1e-3)
+        oracle.euler_step(*ref, 1e-3, lengths=LEN)
+    one.sync()
+    split.sync()
+    assert split.launch_count() - n2 > one.launch_count() - n1
+    tol = 1e-11 if prec == "f64" else 1e-4
+    for a, b, r in zip(U, V, ref):
+        assert torch.equal(a, b)
+        assert rel_err(to_host(a), r) < tol
+    assert torch.equal(pp3, pq)
+    with pytest.raises(Exception):
+        split.set_stage_choice("transeq_x.split", 2)
+    split.set_stage_choice("transeq_x.split", -1)
+    assert split.autotune_stage_choice("transeq_x.split") == -1
+    one.close()
+    split.close()
+
+
 def test_reference_test_mode(oracle, torch_cuda):
     """test_du/dv/dw on the reference vel field (src/mom.f90) match the oracle's RMS."""
     torch = torch_cuda

@@ -65,6 +65,7 @@ SIGNATURES = {
     "x3d_ctx_set_kernel": [_vp, _i],
     "x3d_autotune_choice": [_vp, _i, _i, _ip],
     "x3d_autotune_stage_choice": [_vp, ctypes.c_char_p, _ip],
+    "x3d_ctx_set_stage_choice": [_vp, ctypes.c_char_p, _i],
     "x3d_step_capture": [_vp] + [_vp] * 10 + [ctypes.c_double],
     "x3d_step_launch": [_vp],
     "x3d_ctx_selftest_timeout": [_vp, ctypes.c_double],

@@ -266,6 +266,34 @@ class Context:
 
     STAGES = ("transeq_x", "transeq_y", "transeq_z", "div_x", "div_y", "div_z",
               "gradp_z", "gradp_y", "gradp_x", "gradp_x_cor")
+    # 1 where the autotuner runs a momentum stage as two launches (stages
+    # "<name>.b" then "<name>.a"), 0 where as one
+    STAGE_SPLITS = ("transeq_x.split", "transeq_y.split", "transeq_z.split")
+
+    def set_stage_choice(self, stage, value):
+        """x3d_ctx_set_stage_choice: pin one stage choice (-1 removes it)."""
+        self._check(self.L.x3d_ctx_set_stage_choice(self.handle, stage.encode(), int(value)))
+
+    def stage_choices(self):
+        """Every autotuned stage choice: the configuration of each stage; where
+        a stage runs as several launches, "<stage>.split" (the momentum
+        stages: "<stage>.a", "<stage>.b") or "<stage>.parts" (the number of
+        launches over disjoint staged inputs: "<stage>.1", ...) and the
+        configuration of each launch."""
+        out = {s: self.autotune_stage_choice(s) for s in self.STAGES}
+        for s in self.STAGE_SPLITS:
+            if self.autotune_stage_choice(s) == 1:
+                base = s[:-len(".split")]
+                out[s] = 1
+                for p in ("a", "b"):
+                    out[f"{base}.{p}"] = self.autotune_stage_choice(f"{base}.{p}")
+        for s in self.STAGES:
+            n = self.autotune_stage_choice(s + ".parts")
+            if n > 1:
+                out[s + ".parts"] = n
+                for q in range(1, n + 1):
+                    out[f"{s}.{q}"] = self.autotune_stage_choice(f"{s}.{q}")
+        return out
 
     def autotune_stage_choice(self, stage):
         """Configuration the autotuner chose for a fused Euler-step stage (-1: not tuned)."""

@@ -767,6 +767,7 @@ int x3d_ctx_set_kernel(x3d_ctx ctx, int cfg)
     if (!ctx || cfg < -1 || cfg > kChunkConfigs) return X3D_EINVAL;
     ctx->tuned.clear();
     ctx->stage_tuned.clear();
+    ctx->stage_ms.clear();
     ctx->default_cfg = cfg < 0 ? 0 : cfg;
     return X3D_OK;
 }
@@ -787,6 +788,23 @@ int x3d_autotune_stage_choice(x3d_ctx ctx, const char *stage, int *cfg)
     if (!ctx || !stage || !cfg) return X3D_EINVAL;
     const auto it = ctx->stage_tuned.find(stage);
     *cfg = it == ctx->stage_tuned.end() ? -1 : it->second;
+    return X3D_OK;
+}
+
+int x3d_ctx_set_stage_choice(x3d_ctx ctx, const char *stage, int value)
+{
+    if (!ctx || !stage || !*stage) return X3D_EINVAL;
+    const std::string s = stage;
+    const auto ends = [&](const char *suf) {
+        const size_t n = std::strlen(suf);
+        return s.size() > n && s.compare(s.size() - n, n, suf) == 0;
+    };
+    if (value < -1) return set_error(ctx, X3D_EINVAL, "stage choice below -1");
+    if (ends(".split") && value > 1) return set_error(ctx, X3D_EINVAL, "a split choice is 0 or 1");
+    if (!ends(".split") && !ends(".parts") && value >= kChunkConfigs)
+        return set_error(ctx, X3D_EINVAL, "stage configurations are 0..15");
+    if (value == -1) ctx->stage_tuned.erase(s);
+    else ctx->stage_tuned[s] = value;
     return X3D_OK;
 }
 

@@ -6,7 +6,10 @@
 //     solving d(u_d u_c)/dx_d and d(u_c)/dx_d for the three components and
 //     accumulating  du_c += d(u_d u_c)/dx_d + u_d du_c/dx_d;  with a time step
 //     the z launch also applies int_time (src/time_integrators.f90:41-43),
-//     u_c = dt du_c + u_c, in place.
+//     u_c = dt du_c + u_c, in place.  Each direction may instead run as two
+//     launches of two staged fields each, (u_d, u_o2) for component o2, then
+//     (u_d, u_o1) for components d and o1, which fit more CTAs on an SM; the
+//     autotuner times both forms and keeps the faster.
 //   divergence (src/navier.f90:166-202): x launch derxvp/interxvp/interxvp,
 //     y launch interyvp + deryvp and interyvp, z launch interzvp + derzvp into
 //     the FP64 pressure field.
@@ -94,16 +97,16 @@ static int tune_stage(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir, cons
     if (rc && rc != X3D_EUNSUPPORTED) return rc;
     if (best < 0) return X3D_EUNSUPPORTED;
     ctx->stage_tuned[name] = best;
+    ctx->stage_ms[name] = bt;
     return X3D_OK;
 }
 
-// Runs a stage with its tuned (or the default) configuration, then, if that
-// one cannot take the grid, the others in order.
+// Runs one program with its tuned (or the default) configuration, then, if
+// that one cannot take the grid, the others in order.
 template <typename T>
-static int run_stage(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir, const char *name)
+static int run_program(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir, const std::string &name)
 {
-    const TraceRange trace(name);
-    if (ctx->stage_tuning) return tune_stage<T>(ctx, prog, dir, name);
+    if (ctx->stage_tuning) return tune_stage<T>(ctx, prog, dir, name.c_str());
     const auto it = ctx->stage_tuned.find(name);
     const int first = it != ctx->stage_tuned.end() ? it->second
                                                    : (ctx->default_cfg < kChunkConfigs ? ctx->default_cfg : 0);
@@ -113,39 +116,190 @@ static int run_stage(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir, const
     return rc;
 }
 
+// A program's operators in launches over fewer staged inputs: the operators
+// from an accumulator's start to its flush stay together, and such chains
+// that share no staged input go to different launches, which stage fewer
+// bytes per line and so fit more CTAs on an SM.  Returns the number of
+// parts (1: the program does not split, or a part would write an array
+// another part reads).
+template <typename T>
+static int split_by_inputs(const StageProgram<T> &p, StageProgram<T> (&part)[kMaxStageOps])
+{
+    int chain[kMaxStageOps], nchains = 0;
+    unsigned uses[kMaxStageOps] = {};  // bit t: chain reads staged input t
+    for (int k = 0; k < p.nops; ++k) {
+        const StageOp<T> &o = p.ops[k];
+        if (k == 0 || !o.accumulate) ++nchains;
+        chain[k] = nchains - 1;
+        unsigned &u = uses[nchains - 1];
+        for (const int t : {(int)o.src_a, (int)o.src_b, (int)o.mul_tile})
+            if (t >= 0) u |= 1u << t;
+    }
+    // chains that share an input go together (groups in order of first use)
+    int group[kMaxStageOps], ngroups = 0;
+    unsigned gin[kMaxStageOps] = {};
+    for (int c = 0; c < nchains; ++c) {
+        int g = -1;
+        for (int h = 0; h < ngroups && g < 0; ++h)
+            if (gin[h] & uses[c]) g = h;
+        if (g < 0) g = ngroups++;
+        gin[g] |= uses[c];
+        group[c] = g;
+        // a chain joining a group may connect it to a later group: merge them
+        for (int h = g + 1; h < ngroups; ++h)
+            if (gin[h] & gin[g]) {
+                gin[g] |= gin[h];
+                for (int e = 0; e < c; ++e)
+                    if (group[e] == h) group[e] = g;
+                gin[h] = 0;
+            }
+    }
+    // renumber the groups that are left, in order of first use
+    int ren[kMaxStageOps], nparts = 0;
+    for (int h = 0; h < ngroups; ++h) ren[h] = -1;
+    for (int c = 0; c < nchains; ++c)
+        if (ren[group[c]] < 0) ren[group[c]] = nparts++;
+    if (nparts < 2) return 1;
+    // no part may write an array that another part reads
+    for (int a = 0; a < p.nops; ++a)
+        for (int b = 0; b < p.nops; ++b) {
+            const StageOp<T> &w = p.ops[a], &r = p.ops[b];
+            if (ren[group[chain[a]]] == ren[group[chain[b]]]) continue;
+            for (const void *out : {(const void *)w.out, (const void *)w.out2}) {
+                if (!out) continue;
+                if (out == r.base || out == r.base2) return 1;
+                for (const int t : {(int)r.src_a, (int)r.src_b, (int)r.mul_tile})
+                    if (t >= 0 && out == p.in[t]) return 1;
+            }
+        }
+    for (int q = 0; q < nparts; ++q) {
+        StageProgram<T> &s = part[q];
+        std::memset(&s, 0, sizeof(s));
+        int map[kMaxStageTiles];
+        for (int t = 0; t < p.ntiles; ++t) map[t] = -1;
+        for (int k = 0; k < p.nops; ++k) {
+            if (ren[group[chain[k]]] != q) continue;
+            StageOp<T> o = p.ops[k];
+            for (short *t : {&o.src_a, &o.src_b, &o.mul_tile})
+                if (*t >= 0) {
+                    if (map[*t] < 0) {
+                        map[*t] = s.ntiles;
+                        s.in[s.ntiles++] = p.in[*t];
+                    }
+                    *t = (short)map[*t];
+                }
+            s.ops[s.nops++] = o;
+        }
+    }
+    return nparts;
+}
+
+// Runs a stage: one launch, or, where the autotuner found it faster, one
+// launch per part of split_by_inputs (stages "<name>.1", "<name>.2", ...).
+// While tuning, times both forms and records the choice as "<name>.parts".
+template <typename T>
+static int run_stage(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir, const char *cname)
+{
+    const TraceRange trace(cname);
+    const std::string name = cname;
+    StageProgram<T> part[kMaxStageOps];
+    const int nparts = split_by_inputs<T>(prog, part);
+    const auto it = ctx->stage_tuned.find(name + ".parts");
+    const bool split = nparts > 1 && !ctx->stage_tuning && it != ctx->stage_tuned.end() && it->second == nparts;
+    int rc = X3D_OK;
+    if (!split) {
+        rc = run_program<T>(ctx, prog, dir, name);
+        if (rc || !ctx->stage_tuning || nparts < 2) return rc;
+    }
+    float total = 0.f;
+    for (int q = 0; q < nparts && !rc; ++q) {
+        const std::string pn = name + "." + std::to_string(q + 1);
+        rc = run_program<T>(ctx, part[q], dir, pn);
+        if (!rc && ctx->stage_tuning) total += ctx->stage_ms[pn];
+    }
+    if (ctx->stage_tuning) {
+        ctx->stage_tuned[name + ".parts"] = !rc && total < ctx->stage_ms[name] ? nparts : 1;
+        return rc == X3D_EUNSUPPORTED ? X3D_OK : rc;
+    }
+    return rc;
+}
+
 static x3d_op_s *B(x3d_ctx_s *ctx, int which) { return ctx->builtin[which]; }
+
+// The momentum terms along direction d for the components comps[0..ncomp):
+// the fields they read are staged once each, in component order.
+template <typename T>
+static StageProgram<T> transeq_program(x3d_ctx_s *ctx, int d, const int *comps, int ncomp, void *const du[3],
+                                       const void *const u[3], bool step, double dt, void *const unew[3])
+{
+    const int der_op[3] = {X3D_OP_DERX, X3D_OP_DERY, X3D_OP_DERZ};
+    StageProgram<T> p;
+    std::memset(&p, 0, sizeof(p));
+    bool used[3] = {false, false, false};
+    used[d] = true;
+    for (int i = 0; i < ncomp; ++i) used[comps[i]] = true;
+    int tile[3] = {-1, -1, -1};
+    for (int c = 0; c < 3; ++c)
+        if (used[c]) {
+            tile[c] = p.ntiles;
+            p.in[p.ntiles++] = static_cast<const T *>(u[c]);
+        }
+    p.nops = 2 * ncomp;
+    for (int i = 0; i < ncomp; ++i) {
+        const int c = comps[i];
+        // u_d * d(u_c)/dx_d  (e.g. ux1 * derx(ux1), transeq.f90:107,114)
+        StageOp<T> a = sop<T>(B(ctx, der_op[d]), tile[c]);
+        a.mul_tile = (short)tile[d];
+        a.accumulate = 0;
+        // + d(u_d u_c)/dx_d   (e.g. derx(ux1*ux1), transeq.f90:101,106)
+        StageOp<T> b = sop<T>(B(ctx, der_op[d]), tile[d], tile[c]);
+        b.accumulate = 1;
+        set_flush(b, du[c], d == 0 ? nullptr : du[c]);
+        if (step && d == 2) {
+            b.out2 = unew[c];
+            b.base2 = u[c];
+            b.scale2 = dt;
+        }
+        p.ops[2 * i] = a;
+        p.ops[2 * i + 1] = b;
+    }
+    return p;
+}
 
 template <typename T>
 static int transeq_t(x3d_ctx_s *ctx, void *const du[3], const void *const u[3], bool step, double dt,
                      void *const unew[3])
 {
-    const int der_op[3] = {X3D_OP_DERX, X3D_OP_DERY, X3D_OP_DERZ};
+    static const char *const names[3] = {"transeq_x", "transeq_y", "transeq_z"};
+    static const int all[3] = {0, 1, 2};
     for (int d = 0; d < 3; ++d) {
-        StageProgram<T> p;
-        std::memset(&p, 0, sizeof(p));
-        p.ntiles = 3;
-        for (int c = 0; c < 3; ++c) p.in[c] = static_cast<const T *>(u[c]);
-        p.nops = 6;
-        for (int c = 0; c < 3; ++c) {
-            // u_d * d(u_c)/dx_d  (e.g. ux1 * derx(ux1), transeq.f90:107,114)
-            StageOp<T> a = sop<T>(B(ctx, der_op[d]), c);
-            a.mul_tile = (short)d;
-            a.accumulate = 0;
-            // + d(u_d u_c)/dx_d   (e.g. derx(ux1*ux1), transeq.f90:101,106)
-            StageOp<T> b = sop<T>(B(ctx, der_op[d]), d, c);
-            b.accumulate = 1;
-            set_flush(b, du[c], d == 0 ? nullptr : du[c]);
-            if (step && d == 2) {
-                b.out2 = unew[c];
-                b.base2 = u[c];
-                b.scale2 = dt;
-            }
-            p.ops[2 * c] = a;
-            p.ops[2 * c + 1] = b;
+        const std::string name = names[d];
+        // the split form: component o2 (staging u_d, u_o2), then d and o1
+        // (staging u_d, u_o1).  With a time step the z launches update u in
+        // place; the launch that writes u_d runs last, and neither launch
+        // reads what the other writes.
+        const int o1 = d == 0 ? 1 : 0, o2 = d == 2 ? 1 : 2;
+        const int first[2] = {d, o1};
+        const bool can_split = true;
+        const auto split_it = ctx->stage_tuned.find(name + ".split");
+        const bool split = can_split && !ctx->stage_tuning && split_it != ctx->stage_tuned.end() && split_it->second;
+        int rc;
+        if (!split || ctx->stage_tuning) {
+            rc = run_stage<T>(ctx, transeq_program<T>(ctx, d, all, 3, du, u, step, dt, unew), d, name.c_str());
+            if (rc) return rc;
         }
-        static const char *const names[3] = {"transeq_x", "transeq_y", "transeq_z"};
-        const int rc = run_stage<T>(ctx, p, d, names[d]);
-        if (rc) return rc;
+        if (split || (ctx->stage_tuning && can_split)) {
+            rc = run_stage<T>(ctx, transeq_program<T>(ctx, d, &o2, 1, du, u, step, dt, unew), d,
+                              (name + ".b").c_str());
+            if (!rc) rc = run_stage<T>(ctx, transeq_program<T>(ctx, d, first, 2, du, u, step, dt, unew), d,
+                                       (name + ".a").c_str());
+            if (rc && !(ctx->stage_tuning && rc == X3D_EUNSUPPORTED)) return rc;
+            if (ctx->stage_tuning) {
+                const float t3 = ctx->stage_ms[name];
+                const bool faster = !rc && ctx->stage_ms[name + ".a"] + ctx->stage_ms[name + ".b"] < t3;
+                ctx->stage_tuned[name + ".split"] = faster ? 1 : 0;
+            }
+        }
     }
     return X3D_OK;
 }

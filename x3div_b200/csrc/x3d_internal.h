@@ -139,6 +139,7 @@ struct x3d_ctx_s {
     // filled by the autotuner; while stage_tuning is set, each stage run
     // times every configuration instead
     std::map<std::string, int> stage_tuned;
+    std::map<std::string, float> stage_ms;  // the tuned configuration's time (ms)
     bool stage_tuning = false;
     int default_cfg = 0;
     unsigned long long launches = 0;  // kernels of this library launched on the context
