@@ -342,8 +342,9 @@ int x3d_poisson(x3d_ctx ctx, double *rhs);
  * cuFFT or 2decomp produce them).  In place: the forward z transform, the
  * division of every mode by -K ntot (zero where K < 1e-16), the inverse z
  * transform; the unnormalised 2-D c2r transforms then give the solution.
- * Device pointer; z lengths 2^p 3^q from 8 to 1024.  Builds no cuFFT plan
- * and no spectrum of the whole box. */
+ * Device pointer.  z lengths 2^p 3^q from 8 to 1024 take one fused
+ * kernel; other lengths take batched 1-D cuFFT transforms along z and a
+ * division kernel.  Builds no cuFFT plan or spectrum of the whole box. */
 int x3d_poisson_zlines(x3d_ctx ctx, void *spec, int ny_loc, int j0);
 /* The same on a Z pencil of a p_row x p_col decomposition (2decomp's
  * zstart/zend of the half spectrum): spec holds x modes i0 .. i0 + nxh_loc

@@ -50,7 +50,7 @@ def test_slab_sweep_on_one_nccl_rank(oracle, torch_cuda, prec):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("shape", [(24, 20, 16), (30, 12, 48), (16, 18, 96)])
+@pytest.mark.parametrize("shape", [(24, 20, 16), (30, 12, 48), (16, 18, 96), (12, 10, 40)])
 def test_slab_poisson_on_one_nccl_rank(oracle, torch_cuda, shape):
     """The slab Poisson solve (torch.fft x-y transforms, the half spectrum
     transposed through NCCL, x3d_poisson_zlines on the rank's y rows) against
@@ -120,8 +120,9 @@ def test_slab_euler_steps_on_one_nccl_rank(oracle, torch_cuda, prec):
         dist.destroy_process_group()
 
 
+# the last two z lengths have no fused transform (a factor 5; above 1024)
 @pytest.mark.parametrize("shape,grid", [((24, 20, 16), (2, 2)), ((30, 12, 48), (3, 2)), ((16, 18, 96), (2, 3)),
-                                        ((40, 24, 64), (1, 3))])
+                                        ((40, 24, 64), (1, 3)), ((12, 10, 40), (2, 2)), ((10, 12, 2048), (2, 3))])
 def test_poisson_zpencil_on_every_rank_block(oracle, torch_cuda, shape, grid):
     """x3d_poisson_zpencil on each rank's Z pencil of the half spectrum of a
     p_row x p_col grid (x modes and y rows both cut into blocks), one block

@@ -63,17 +63,20 @@ static void waves_tables(int n, double len, std::vector<double> &k2, std::vector
 // c(i,j,k) <- -c / (K ntot), K = k2x Ty^2 Tz^2 + k2y Tx^2 Tz^2 + k2z Tx^2 Ty^2
 // (waves :690-694: xk2(i) * ((Ty*Tz)**2) etc.), zero where K < 1e-16.
 // One division per mode (the reference divides Re and Im by ntot and then by
-// -K; the product form differs from it by a few ulp).  Indices are 32-bit:
-// the spectrum of any grid that fits one GPU has fewer than 2^32 modes.
-__global__ void k_spectral_divide(double2 *c, unsigned nxh, unsigned ny, unsigned n, const double *k2x,
-                                  const double *tx, const double *k2y, const double *ty,
+// -K; the product form differs from it by a few ulp).  The block c holds
+// x modes i0 .. i0 + nxl - 1 and y rows j0 .. j0 + nyl - 1 of every z mode
+// ((nz, nyl, nxl), x fastest; the whole spectrum with i0 = j0 = 0).
+// Indices are 32-bit: the spectrum of any grid that fits one GPU has fewer
+// than 2^32 modes.
+__global__ void k_spectral_divide(double2 *c, unsigned nxl, unsigned nyl, unsigned n, unsigned i0, unsigned j0,
+                                  const double *k2x, const double *tx, const double *k2y, const double *ty,
                                   const double *k2z, const double *tz, double ntot)
 {
     for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
-        const unsigned row = p / nxh;
-        const unsigned i = p - row * nxh;
-        const unsigned k = row / ny;
-        const unsigned j = row - k * ny;
+        const unsigned row = p / nxl;
+        const unsigned i = i0 + (p - row * nxl);
+        const unsigned k = row / nyl;
+        const unsigned j = j0 + (row - k * nyl);
         const double txi = __ldg(tx + i), tyj = __ldg(ty + j), tzk = __ldg(tz + k);
         const double tyz = tyj * tzk, txz = txi * tzk, txy = txi * tyj;
         const double kk = __ldg(k2x + i) * (tyz * tyz) + __ldg(k2y + j) * (txz * txz) +
@@ -433,6 +436,22 @@ static int launch_poisson_z(x3d_ctx_s *ctx, double2 *spec, int nxl, int i0, int 
     }
 }
 
+// k_spectral_divide over n modes of a block (see there), grid-strided.
+static int launch_divide(x3d_ctx_s *ctx, double2 *c, int nxl, int nyl, size_t n, int i0, int j0)
+{
+    if (n >= (1ull << 31)) return set_error(ctx, X3D_EUNSUPPORTED, "spectrum above 2^31 modes");
+    const int bs = 256;
+    size_t g = (n + bs - 1) / bs;
+    const size_t cap = (size_t)ctx->num_sms * 8;
+    if (g > cap) g = cap;
+    const double ntot = (double)ctx->nx * (double)ctx->ny * (double)ctx->nz;
+    ++ctx->launches;
+    k_spectral_divide<<<(unsigned)g, bs, 0, ctx->stream>>>(c, (unsigned)nxl, (unsigned)nyl, (unsigned)n,
+                                                           (unsigned)i0, (unsigned)j0, ctx->d_k2x, ctx->d_tx,
+                                                           ctx->d_k2y, ctx->d_ty, ctx->d_k2z, ctx->d_tz, ntot);
+    return cuda_check(ctx, cudaGetLastError(), "k_spectral_divide");
+}
+
 int poisson_solve(x3d_ctx_s *ctx, double *rhs)
 {
     const TraceRange trace("poisson");
@@ -450,19 +469,7 @@ int poisson_solve(x3d_ctx_s *ctx, double *rhs)
         return X3D_OK;
     }
     const int nxh = ctx->nx / 2 + 1;
-    const size_t n = (size_t)nxh * ctx->ny * ctx->nz;
-    if (n >= (1ull << 31)) return set_error(ctx, X3D_EUNSUPPORTED, "spectrum above 2^31 modes");
-    const int bs = 256;
-    size_t g = (n + bs - 1) / bs;
-    const size_t cap = (size_t)ctx->num_sms * 8;
-    if (g > cap) g = cap;
-    const double ntot = (double)ctx->nx * (double)ctx->ny * (double)ctx->nz;
-    ++ctx->launches;
-    k_spectral_divide<<<(unsigned)g, bs, 0, ctx->stream>>>((double2 *)ctx->spectrum, (unsigned)nxh,
-                                                           (unsigned)ctx->ny, (unsigned)n, ctx->d_k2x,
-                                                           ctx->d_tx, ctx->d_k2y, ctx->d_ty, ctx->d_k2z,
-                                                           ctx->d_tz, ntot);
-    rc = cuda_check(ctx, cudaGetLastError(), "k_spectral_divide");
+    rc = launch_divide(ctx, (double2 *)ctx->spectrum, nxh, ctx->ny, (size_t)nxh * ctx->ny * ctx->nz, 0, 0);
     if (rc) return rc;
     if (cufftExecZ2D(ctx->plan_z2d, (cufftDoubleComplex *)ctx->spectrum, rhs) != CUFFT_SUCCESS)
         return set_error(ctx, X3D_ECUDA, "cufftExecZ2D failed");
@@ -472,14 +479,38 @@ int poisson_solve(x3d_ctx_s *ctx, double *rhs)
 // The z part of the spectral solve on a block of x modes and y rows of the
 // x-y transformed spectrum, for a box spread over ranks.  Needs only the
 // wavenumber tables and twiddles: no plans or spectrum of the whole box.
+// z lengths without a fused kernel take batched 1-D cuFFT transforms along
+// z (one plan per block shape, kept), k_spectral_divide on the block and
+// the inverse transforms.
 int poisson_zpencil(x3d_ctx_s *ctx, void *spec, int nxl, int i0, int ny_loc, int j0)
 {
     int rc = poisson_tables(ctx);
     if (rc) return rc;
-    if (!ctx->d_zft_tw) return set_error(ctx, X3D_EUNSUPPORTED, "no fused z transform for this nz");
     if (ny_loc < 1 || j0 < 0 || j0 + ny_loc > ctx->ny) return set_error(ctx, X3D_EINVAL, "bad block of y rows");
     if (nxl < 1 || i0 < 0 || i0 + nxl > ctx->nx / 2 + 1) return set_error(ctx, X3D_EINVAL, "bad block of x modes");
-    return launch_poisson_z(ctx, static_cast<double2 *>(spec), nxl, i0, ny_loc, j0);
+    double2 *c = static_cast<double2 *>(spec);
+    if (ctx->d_zft_tw) return launch_poisson_z(ctx, c, nxl, i0, ny_loc, j0);
+    if (!ctx->zblk_ready || ctx->zblk_nxl != nxl || ctx->zblk_nyl != ny_loc) {
+        if (ctx->zblk_ready) cufftDestroy(ctx->plan_zblk);
+        ctx->zblk_ready = false;
+        int n = ctx->nz, emb = ctx->nz;
+        const int lines = nxl * ny_loc;
+        if (cufftPlanMany(&ctx->plan_zblk, 1, &n, &emb, lines, 1, &emb, lines, 1, CUFFT_Z2Z, lines) !=
+            CUFFT_SUCCESS)
+            return set_error(ctx, X3D_ECUDA, "cufftPlanMany (z lines of a block) failed");
+        ctx->zblk_ready = true;
+        ctx->zblk_nxl = nxl;
+        ctx->zblk_nyl = ny_loc;
+    }
+    cufftSetStream(ctx->plan_zblk, ctx->stream);
+    auto *cz = reinterpret_cast<cufftDoubleComplex *>(c);
+    if (cufftExecZ2Z(ctx->plan_zblk, cz, cz, CUFFT_FORWARD) != CUFFT_SUCCESS)
+        return set_error(ctx, X3D_ECUDA, "cufftExecZ2Z (forward z) failed");
+    rc = launch_divide(ctx, c, nxl, ny_loc, (size_t)nxl * ny_loc * ctx->nz, i0, j0);
+    if (rc) return rc;
+    if (cufftExecZ2Z(ctx->plan_zblk, cz, cz, CUFFT_INVERSE) != CUFFT_SUCCESS)
+        return set_error(ctx, X3D_ECUDA, "cufftExecZ2Z (inverse z) failed");
+    return X3D_OK;
 }
 
 void poisson_free(x3d_ctx_s *ctx)
@@ -496,6 +527,8 @@ void poisson_free(x3d_ctx_s *ctx)
     if (ctx->d_zft_tw) cudaFree(ctx->d_zft_tw);
     ctx->d_zft_tw = nullptr;
     ctx->zfused = false;
+    if (ctx->zblk_ready) cufftDestroy(ctx->plan_zblk);
+    ctx->zblk_ready = false;
 }
 
 }  // namespace x3d

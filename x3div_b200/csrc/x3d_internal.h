@@ -111,6 +111,11 @@ struct x3d_ctx_s {
     bool zfused = false;
     bool zfuse_allowed = true;  // cleared to force the 3-D cuFFT path
     double *d_zft_tw = nullptr;  // e^{-2 pi i t / nz}, t < nz (complex)
+    // batched 1-D z transforms of one rank's block of the half spectrum, for
+    // z lengths without a fused kernel (nxl x modes, nyl y rows)
+    cufftHandle plan_zblk = 0;
+    bool zblk_ready = false;
+    int zblk_nxl = 0, zblk_nyl = 0;
     void *spectrum = nullptr;  // complex double, nz * ny * (nx/2+1)
     double *d_k2x = nullptr, *d_tx = nullptr, *d_k2y = nullptr, *d_ty = nullptr, *d_k2z = nullptr,
            *d_tz = nullptr;
