@@ -58,9 +58,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--profile-timed", nargs="?", const="sweep", default=None, choices=["sweep", "euler", "b48"],
-                    help="bracket the timed FP32 sweep (or the FP32-mixed Euler steps, or the batch "
-                         "replays) with cudaProfilerStart/Stop, for ncu --profile-from-start off")
+    ap.add_argument("--profile-timed", nargs="?", const="sweep", default=None,
+                    choices=["sweep", "euler", "euler64", "b48"],
+                    help="bracket the timed FP32 sweep (or the FP32-mixed Euler steps, the FP64 ones, or "
+                         "the batch replays) with cudaProfilerStart/Stop, for ncu --profile-from-start off")
     ap.add_argument("--kernel-config", type=int, default=None,
                     help="force one kernel configuration (x3d_ctx_set_kernel) instead of autotuning")
     ap.add_argument("--no-b48", action="store_true")
@@ -609,7 +610,7 @@ def run_b200(args, world, rank, local):
         out["fp64"] = f64
         del fields, outs
         if not args.no_euler:
-            out["euler_f64"] = euler_ms(ctx64, torch.float64)
+            out["euler_f64"] = euler_ms(ctx64, torch.float64, profile=args.profile_timed == "euler64")
         ctx64.close()
     if not args.no_b48:
         out["b48"] = run_b48(args, world, rank, local, torch)
