@@ -149,10 +149,16 @@ def _exchange(send_blocks, recv_shapes, group, members, like):
     if len(members) == 1:
         return [send_blocks[0].reshape(recv_shapes[0])]
     import torch.distributed as dist
-    send = torch.cat([b.reshape(-1) for b in send_blocks])
+    # each block is packed once, straight into its slot of the send buffer
+    in_splits = [b.numel() for b in send_blocks]
+    send = torch.empty(sum(in_splits), dtype=like.dtype, device=like.device)
+    off = 0
+    for b, n in zip(send_blocks, in_splits):
+        send[off:off + n].view(b.shape).copy_(b)
+        off += n
     out_splits = [int(torch.Size(s).numel()) for s in recv_shapes]
     recv = torch.empty(sum(out_splits), dtype=like.dtype, device=like.device)
-    dist.all_to_all_single(recv, send, out_splits, [b.numel() for b in send_blocks], group=group)
+    dist.all_to_all_single(recv, send, out_splits, in_splits, group=group)
     res, off = [], 0
     for s, n in zip(recv_shapes, out_splits):
         res.append(recv[off:off + n].view(s))
