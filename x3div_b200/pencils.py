@@ -141,29 +141,33 @@ class Pencils:
         return Pencils(self.layout.with_shape(shape), self.xy_group, self.yz_group)
 
 
-def _exchange(send_blocks, recv_shapes, group, members, like):
+def _exchange(send_blocks, recv_shapes, group, members, like, send_flat=None):
     """All-to-all among `members` (this rank's group, in group-rank order):
     block i of send_blocks goes to members[i]; returns the blocks received,
-    block i from members[i], shaped recv_shapes[i]."""
+    block i from members[i], shaped recv_shapes[i], and the flat receive
+    buffer that holds them in that order.  send_flat, when given, already
+    holds the send blocks back to back (no packing copy)."""
     import torch
     if len(members) == 1:
-        return [send_blocks[0].reshape(recv_shapes[0])]
+        blk = send_blocks[0].reshape(recv_shapes[0])
+        return [blk], blk.reshape(-1)
     import torch.distributed as dist
-    # each block is packed once, straight into its slot of the send buffer
     in_splits = [b.numel() for b in send_blocks]
-    send = torch.empty(sum(in_splits), dtype=like.dtype, device=like.device)
-    off = 0
-    for b, n in zip(send_blocks, in_splits):
-        send[off:off + n].view(b.shape).copy_(b)
-        off += n
+    if send_flat is None:
+        # each block is packed once, straight into its slot of the send buffer
+        send_flat = torch.empty(sum(in_splits), dtype=like.dtype, device=like.device)
+        off = 0
+        for b, n in zip(send_blocks, in_splits):
+            send_flat[off:off + n].view(b.shape).copy_(b)
+            off += n
     out_splits = [int(torch.Size(s).numel()) for s in recv_shapes]
     recv = torch.empty(sum(out_splits), dtype=like.dtype, device=like.device)
-    dist.all_to_all_single(recv, send, out_splits, in_splits, group=group)
+    dist.all_to_all_single(recv, send_flat, out_splits, in_splits, group=group)
     res, off = [], 0
     for s, n in zip(recv_shapes, out_splits):
         res.append(recv[off:off + n].view(s))
         off += n
-    return res
+    return res, recv
 
 
 def _check(t, pc: Pencils, pencil):
@@ -185,7 +189,7 @@ def transpose_x_to_y(t, pc: Pencils):
     (xa, xb), _, (za, zb) = L.block("y")
     send = [t[:, :, a:b] for a, b in (L.block("y", m)[0] for m in members)]
     ys = [L.block("x", m)[1] for m in members]
-    got = _exchange(send, [(zb - za, b - a, xb - xa) + rest for a, b in ys], pc.xy_group, members, t)
+    got, _ = _exchange(send, [(zb - za, b - a, xb - xa) + rest for a, b in ys], pc.xy_group, members, t)
     out = torch.empty(L.tensor_shape("y") + rest, dtype=t.dtype, device=t.device)
     for (a, b), blk in zip(ys, got):
         out[:, a:b] = blk
@@ -204,7 +208,7 @@ def transpose_y_to_x(t, pc: Pencils):
     _, (ya, yb), (za, zb) = L.block("x")
     send = [t[:, a:b] for a, b in (L.block("x", m)[1] for m in members)]
     xs = [L.block("y", m)[0] for m in members]
-    got = _exchange(send, [(zb - za, yb - ya, b - a) + rest for a, b in xs], pc.xy_group, members, t)
+    got, _ = _exchange(send, [(zb - za, yb - ya, b - a) + rest for a, b in xs], pc.xy_group, members, t)
     out = torch.empty(L.tensor_shape("x") + rest, dtype=t.dtype, device=t.device)
     for (a, b), blk in zip(xs, got):
         out[:, :, a:b] = blk
@@ -223,11 +227,9 @@ def transpose_y_to_z(t, pc: Pencils):
     (xa, xb), (ya, yb), _ = L.block("z")
     send = [t[:, a:b] for a, b in (L.block("z", m)[1] for m in members)]
     zs = [L.block("y", m)[2] for m in members]
-    got = _exchange(send, [(b - a, yb - ya, xb - xa) + rest for a, b in zs], pc.yz_group, members, t)
-    out = torch.empty(L.tensor_shape("z") + rest, dtype=t.dtype, device=t.device)
-    for (a, b), blk in zip(zs, got):
-        out[a:b] = blk
-    return out
+    _, recv = _exchange(send, [(b - a, yb - ya, xb - xa) + rest for a, b in zs], pc.yz_group, members, t)
+    # the members' z blocks arrive in z order: the receive buffer is the Z pencil
+    return recv.view(L.tensor_shape("z") + rest)
 
 
 def transpose_z_to_y(t, pc: Pencils):
@@ -242,7 +244,9 @@ def transpose_z_to_y(t, pc: Pencils):
     (xa, xb), _, (za, zb) = L.block("y")
     send = [t[a:b] for a, b in (L.block("y", m)[2] for m in members)]
     ys = [L.block("z", m)[1] for m in members]
-    got = _exchange(send, [(zb - za, b - a, xb - xa) + rest for a, b in ys], pc.yz_group, members, t)
+    # the members' z blocks are consecutive ranges of t: t is the send buffer
+    got, _ = _exchange(send, [(zb - za, b - a, xb - xa) + rest for a, b in ys], pc.yz_group, members, t,
+                       send_flat=t.contiguous().view(-1))
     out = torch.empty(L.tensor_shape("y") + rest, dtype=t.dtype, device=t.device)
     for (a, b), blk in zip(ys, got):
         out[:, a:b] = blk
