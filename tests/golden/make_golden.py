@@ -1,6 +1,7 @@
-"""Golden vectors for the periodic hot path, written by the CPU oracle
-(oracle/): seeded inputs with the outputs of every operator family along
-every direction, of the Poisson solve and of one Euler step, on boxes small
+"""Golden vectors for the hot path, written by the CPU oracle (oracle/):
+seeded inputs with the outputs of every periodic operator family along
+every direction, of the Poisson solve and of one Euler step, and of the
+non-periodic first derivatives and staggered branches, on boxes small
 enough to commit.
 
 The reference (Fortran + MPI + 2decomp&FFT) cannot be built here and ships
@@ -28,6 +29,11 @@ STEP_SHAPE = (16, 12, 10)
 LENGTHS = (2 * np.pi, 1.5, 3.0)
 KINDS = ("der", "der2", "dervp", "derpv", "intvp", "intpv")
 DT = 1e-3
+# non-periodic first derivatives: ((ncl1, ncln), npaire) along each direction
+DER_NP = (((1, 1), 0), ((1, 1), 1), ((2, 2), 0), ((1, 2), 1))
+# non-periodic staggered branches the reference has: (kind, direction, (ncl1, ncln), npaire)
+STAG_NP = (("dervp", 0, (1, 1), 1), ("dervp", 1, (1, 1), 0), ("dervp", 2, (2, 2), 0),
+           ("intvp", 1, (1, 1), 1), ("derpv", 2, (1, 1), 1), ("intpv", 0, (2, 2), 1))
 
 
 def _taylor_green(shape, rng, noise):
@@ -58,6 +64,22 @@ def build():
     out["step_du"] = np.stack(du)
     out["step_div_before"] = div
     out["step_pp3"] = pp3
+    # non-periodic directions: the velocity grid has n points, spacing L/(n-1)
+    uv = np.asfortranarray(rng.standard_normal(OPS_SHAPE))
+    out["np_vel_input"] = uv
+    h = [L / (n - 1) for L, n in zip(LENGTHS, OPS_SHAPE)]
+    for d in range(3):
+        for (n1, nn), npaire in DER_NP:
+            out[f"dernp_{'xyz'[d]}_{n1}{nn}_p{npaire}"] = oracle.der_np(d, uv, h[d], n1, nn, npaire)
+    for kind, d, (n1, nn), npaire in STAG_NP:
+        if kind.endswith("vp"):
+            src = uv
+        else:  # pressure-grid input: one point fewer along d
+            shape = list(OPS_SHAPE)
+            shape[d] -= 1
+            src = np.asfortranarray(rng.standard_normal(shape))
+            out[f"np_pre_{kind}_{'xyz'[d]}_input"] = src
+        out[f"stagnp_{kind}_{'xyz'[d]}_{n1}{nn}_p{npaire}"] = oracle.stag_np(kind, d, src, h[d], n1, nn, npaire)
     return out
 
 

@@ -1,7 +1,8 @@
 """The committed golden vectors (tests/golden/oracle_vectors.npz, written by
 tests/golden/make_golden.py) against the oracle run now: the same seeded
-inputs give the same outputs for every operator family and direction, the
-Poisson solve and one Euler step."""
+inputs give the same outputs for every periodic operator family and
+direction, the Poisson solve, one Euler step, and the non-periodic first
+derivatives and staggered branches."""
 import importlib.util
 import os
 
