@@ -317,7 +317,8 @@ int x3d_batch_sync(x3d_batch b)
     cudaSetDevice(b->device);
     if (cudaStreamSynchronize(b->stream) != cudaSuccess) return bfail(b, X3D_ECUDA, "batch stream sync failed");
     int flag = 0;
-    cudaMemcpy(&flag, b->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (cudaMemcpy(&flag, b->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return bfail(b, X3D_ECUDA, "batch error flag read failed");
     if (flag) {
         cudaMemset(b->d_err, 0, sizeof(int));
         return bfail(b, X3D_ETIMEOUT, "a device-side bounded wait gave up");

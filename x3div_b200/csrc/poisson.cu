@@ -366,7 +366,10 @@ static int poisson_tables(x3d_ctx_s *ctx)
     h.insert(h.end(), ty.begin(), ty.end());
     h.insert(h.end(), k2z.begin(), k2z.end());
     h.insert(h.end(), tz.begin(), tz.end());
-    cudaMemcpy(tab, h.data(), tot * sizeof(double), cudaMemcpyHostToDevice);
+    if (cudaMemcpy(tab, h.data(), tot * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaFree(tab);
+        return set_error(ctx, X3D_ECUDA, "poisson tables upload");
+    }
     ctx->d_k2x = tab;
     ctx->d_tx = tab + nx;
     ctx->d_k2y = tab + 2 * nx;
@@ -382,7 +385,12 @@ static int poisson_tables(x3d_ctx_s *ctx)
         }
         if (cudaMalloc(&ctx->d_zft_tw, tw.size() * sizeof(double)) != cudaSuccess)
             return set_error(ctx, X3D_ENOMEM, "poisson twiddles");
-        cudaMemcpy(ctx->d_zft_tw, tw.data(), tw.size() * sizeof(double), cudaMemcpyHostToDevice);
+        if (cudaMemcpy(ctx->d_zft_tw, tw.data(), tw.size() * sizeof(double), cudaMemcpyHostToDevice) !=
+            cudaSuccess) {
+            cudaFree(ctx->d_zft_tw);
+            ctx->d_zft_tw = nullptr;
+            return set_error(ctx, X3D_ECUDA, "poisson twiddles upload");
+        }
     }
     return X3D_OK;
 }
