@@ -46,3 +46,23 @@ def test_no_device_reports_cuda_error():
     L = _capi.lib()
     h = ctypes.c_void_p()
     assert L.x3d_ctx_create(ctypes.byref(h), 8, 8, 8, 1.0, 1.0, 1.0, 0, 0) == _capi.X3D_ECUDA
+
+
+def test_fortran_interface_block_matches_header():
+    """INTEGRATION.md's Appendix A declares one bind(C) interface per entry
+    point, with the header's argument count (bind(C) matches by position)."""
+    import re
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    with open(os.path.join(root, "include", "x3d_b200.h")) as f:
+        header = f.read()
+    decl = {name: len([a for a in args.split(",") if a.strip()])
+            for name, args in re.findall(r"^(?:int|const char \*)\s*(x3d_\w+)\(([^;]*?)\);", header, re.M | re.S)}
+    with open(os.path.join(root, "INTEGRATION.md")) as f:
+        doc = f.read()
+    appendix = doc[doc.index("## Appendix A."):]
+    iface = {name: len([a for a in args.split(",") if a.strip()])
+             for args, name in re.findall(r"function x3d_\w+\(([^)]*)\)[\s&]*bind\(C,[\s&]*name=\"(x3d_\w+)\"\)",
+                                          appendix)}
+    assert set(decl) == set(_capi.header_symbols())
+    assert iface == decl, {k: (iface.get(k), decl.get(k)) for k in set(iface) | set(decl)
+                           if iface.get(k) != decl.get(k)}
