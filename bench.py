@@ -67,8 +67,8 @@ def parse():
     ap.add_argument("--no-b48", action="store_true")
     ap.add_argument("--b48-count", type=int, default=48,
                     help="boxes in the batching workload (the first of the same seeded draw; 48 by default)")
-    ap.add_argument("--c5", action="store_true",
-                    help="also run 20 Euler steps at 768^3, FP32-mixed and FP64 (reported under c5)")
+    ap.add_argument("--no-c5", action="store_true",
+                    help="skip the 768^3 long run (20 Euler steps, FP32-mixed and FP64, reported under c5)")
     return ap.parse_args()
 
 
@@ -181,22 +181,33 @@ def barrier(world):
 
 
 # --------------------------------------------------------------------------
-def cpu_sample(n, reps=1):
-    """The oracle on a bounded sample: one operator per direction (derx,
-    interyvp, derzz) on one n^3 FP64 field, all host threads."""
+def sample_ops(s):
+    """(oracle kind, direction) of the three applications of CPU sample step s."""
+    return [(KINDS[(s + 2 * d) % 6][0], d) for d in range(3)]
+
+
+def cpu_sample(n, reps=1, start=0):
+    """The oracle on a bounded sample of the sweep: per step three of the 54
+    applications, one per direction, on one n^3 FP64 field with all host
+    threads.  Step s applies family (s + 2 d) mod 6 along direction d, so six
+    consecutive steps visit all 18 family x direction pairs once (the
+    sweep's operator mix); start is the first step's index."""
     from oracle import oracle as O
     O.lib()
     f = np.asfortranarray(tg_noise(n, 0).transpose(2, 1, 0))
     d = 2 * np.pi / n
     times = []
-    for _ in range(reps):
+    for s in range(start, start + reps):
         t0 = time.perf_counter()
-        O.apply("der", 0, f, d)
-        O.apply("intvp", 1, f, d)
-        O.apply("der2", 2, f, d)
+        for kind, di in sample_ops(s):
+            O.apply(kind, di, f, d)
         times.append(time.perf_counter() - t0)
     pts = 3.0 * n ** 3
     return pts, times
+
+
+ROTATION = ("step s applies operator family (s + 2 d) mod 6 of (der, der2, dervp, derpv, intvp, intpv) "
+            "along direction d, so every 6 steps visit all 18 family x direction pairs of the sweep once")
 
 
 def cpu_threads():
@@ -207,10 +218,10 @@ def run_reference(args, world, rank):
     if rank != 0:
         return
     n = args.n
-    sample = ("oracle/ (FP64 C restatement, OpenMP) applying derx, interyvp, derzz to one "
-              f"{n}^3 field per step (3 of the 54 applications of a sweep step)")
-    pts, _ = cpu_sample(n, reps=max(1, args.warmup))
-    pts, times = cpu_sample(n, reps=args.steps)
+    sample = (f"oracle/ (FP64 C restatement, OpenMP) applying 3 of the 54 applications of a sweep step "
+              f"to one {n}^3 field per step, one per direction, rotating: {ROTATION}")
+    pts, _ = cpu_sample(n, reps=max(1, args.warmup), start=0)
+    pts, times = cpu_sample(n, reps=args.steps, start=0)
     t = sum(times)
     val = pts * args.steps / t / 1e9
     cores = cpu_threads()
@@ -258,18 +269,23 @@ CONFIG_W = [16, 32, 16, 8, 32, 8, 16, 32, 16, 8, 32, 8, 32, 16, 32, 32]
 
 def pattern_ceilings(ctx, torch, src, outs):
     """Bandwidth of one read and six writes with no arithmetic
-    (x3d_roofline_probe), flat and in the y stage kernels' tile order for
-    W = 8, 16, 32: what the sweep launches' traffic mix and access order can
-    reach on this GPU (best over 1, 2 and 4 CTAs per SM of 5 timed launches
-    after 3 warm-up ones)."""
+    (x3d_roofline_probe), flat, in the y stage kernels' tile order for
+    W = 8 .. 128 columns over whole lines, and over blocks of 128 rows: what
+    the sweep launches' traffic mix and access order can reach on this GPU
+    (best over 1, 2, 4 and 8 CTAs per SM of 5 timed launches after 3 warm-up
+    ones)."""
     nz, ny, nx = src.shape
     bytes_moved = 7 * src.numel() * src.element_size()
     res = {}
-    for key, pattern, w in (("flat", 0, 0), ("tile_w8", 1, 8), ("tile_w16", 1, 16), ("tile_w32", 1, 32)):
-        if pattern and (nx % w or ny % 32 or (ny // 32) * w > 1024):
+    cases = [("flat", 0, 0)] + [(f"tile_w{w}", 1, w) for w in (8, 16, 32, 64, 128)] + \
+            [(f"block128_w{w}", 2, w) for w in (32, 64, 128)]
+    for key, pattern, w in cases:
+        rt = 16 if w == 128 else 32
+        rows = ny if pattern == 1 else 128
+        if pattern and (nx % w or ny % rows or rows % rt or (w // max(1, w // 32)) * (rows // rt) > 512):
             continue
         best = None
-        for per_sm in (1, 2, 4):
+        for per_sm in (1, 2, 4, 8):
             run = lambda: ctx.roofline_probe(pattern, w, src, outs, per_sm)  # noqa: E731
             for _ in range(3):
                 run()
@@ -615,7 +631,7 @@ def run_b200(args, world, rank, local):
     if not args.no_b48:
         out["b48"] = run_b48(args, world, rank, local, torch)
     out["clocks"] = clocks.stop()
-    if args.c5 and rank == 0:
+    if not args.no_c5 and rank == 0:
         out["c5"] = run_c5(torch)
     return out, pts_step
 
@@ -633,8 +649,8 @@ def main():
     if rank == 0:
         n = args.n
         sample_n = min(n, 512)
-        pts, times = cpu_sample(sample_n, reps=1)
-        cpu_val = pts / times[0] / 1e9
+        pts, times = cpu_sample(sample_n, reps=6)
+        cpu_val = pts * len(times) / sum(times) / 1e9
         line = {
             "metric": METRIC,
             "value": round(res["value"], 2),
@@ -661,7 +677,8 @@ def main():
             "unfused": res["unfused"],
             "cpu_baseline": {"value": round(cpu_val, 4), "unit": "Gpts/s", "cores": cpu_threads(),
                              "kind": "port",
-                             "sample": f"oracle (FP64 C, OpenMP) derx+interyvp+derzz on one {sample_n}^3 field"},
+                             "sample": f"oracle (FP64 C, OpenMP) on one {sample_n}^3 field, 6 steps of 3 "
+                                       f"applications: {ROTATION}"},
         }
         if "e2e" in res:
             line["e2e"] = res["e2e"]

@@ -146,10 +146,15 @@ int x3d_ctx_selftest_timeout(x3d_ctx ctx, double limit_s);
  * counterpart): moves one FP32 (nx, ny, nz) device field to six FP32 device
  * fields (outs[6]) with no arithmetic, in a flat order (pattern 0: 16-byte
  * vectors, consecutive threads on consecutive vectors) or in the y stage
- * kernels' order (pattern 1: tiles of w in {8, 16, 32} x-adjacent columns
- * of the ny rows of a z plane, 32 rows per thread; nx % w == 0,
- * ny % 32 == 0), so that timing it gives the bandwidth that traffic mix and
- * access order can reach.  ctas_per_sm sets the grid (0: 2 per SM). */
+ * kernels' order (pattern 1: tiles of w in {8, 16, 32, 64, 128} x-adjacent
+ * columns of the ny rows of a z plane, each thread on consecutive rows;
+ * pattern 2: the same tiles over blocks of 128 rows; pattern 3: pattern 1
+ * with each store of the CTA on consecutive rows; pattern 4: pattern 1 with
+ * consecutive tiles on different z planes; nx % w == 0, ny a multiple of
+ * the rows a thread moves (32, or 16 for w = 128) and of the block), so
+ * that timing it gives the
+ * bandwidth that traffic mix and access order can reach.  ctas_per_sm sets
+ * the grid (0: 2 per SM). */
 int x3d_roofline_probe(x3d_ctx ctx, int pattern, int w, int ctas_per_sm, const void *in, void *const *outs,
                        int nx, int ny, int nz);
 /* Text of the last error recorded on this context (never NULL). */
@@ -368,14 +373,17 @@ int x3d_divergence(x3d_ctx ctx, double *pp3, const void *ux1, const void *uy1, c
  * front through OpenACC data regions and runs under a fixed memory budget,
  * or a solver sharing the GPU that must not take memory mid-step.  The five
  * intermediate fields live in one fixed array inside the library
- * (5 * X3D_NOALLOC_MAX_POINTS doubles = 10 MiB, held by every GPU that loads
- * the library until the process exits) instead of in context scratch.
+ * (5 * X3D_NOALLOC_MAX_POINTS doubles = 10 MiB) instead of in context
+ * scratch.  A GPU holds the array from the first call on it (that call loads
+ * the library's module there under CUDA's lazy module loading, so make it
+ * once before the time loop) until the process exits.
  * Inputs and output are caller-owned device pointers (host pointers are
  * refused, since staging them would allocate); the context must already
  * exist.  Grids above X3D_NOALLOC_MAX_POINTS points return X3D_EINVAL, grids
  * the fused stage kernels cannot take return X3D_EUNSUPPORTED.  The first
- * call on each device looks up the array's device address; make that first
- * call before any stream capture.  All calls share the one array: calls that
+ * call on each device looks up the array's device address (again after a
+ * device reset, which moves it); make that first call before any stream
+ * capture.  All calls share the one array: calls that
  * overlap on the GPU (other streams or contexts at the same time) race on
  * it.  Every element of the array is written before it is read, so nothing
  * has to be cleared between calls. */

@@ -59,3 +59,17 @@ def test_reference_arm_under_two_ranks_prints_from_rank_0_only():
     lines = _lines(outs[0][0])
     assert len(lines) == 1
     _check(lines[0], 2)
+
+
+def test_cpu_sample_rotation_visits_the_sweeps_operator_mix():
+    """Six consecutive CPU-sample steps apply each of the 18 family x
+    direction pairs of a sweep step exactly once, three per step, one per
+    direction."""
+    sys.path.insert(0, ROOT)
+    import bench
+    for start in (0, 5):
+        seen = [p for s in range(start, start + 6) for p in bench.sample_ops(s)]
+        assert len(seen) == 18 and len(set(seen)) == 18
+        assert {k for k, _ in seen} == {k for k, _ in bench.KINDS}
+    for s in range(6):
+        assert [d for _, d in bench.sample_ops(s)] == [0, 1, 2]

@@ -8,6 +8,7 @@
 // gives them the divergence stage without any allocation: its five
 // intermediate fields live in one fixed array compiled into the library
 // instead of in context scratch.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -20,28 +21,55 @@ namespace {
 constexpr size_t kMaxPoints = X3D_NOALLOC_MAX_POINTS;
 constexpr int kFields = 5;
 
-// The intermediate fields, kFields * kMaxPoints doubles (10 MiB).  Every GPU
-// that loads the library holds this array until the process exits.
+// The intermediate fields, kFields * kMaxPoints doubles (10 MiB).  A GPU holds
+// this array from the first x3d_divergence_noalloc call on it (when the
+// library's module is loaded there) until the process exits.
 static __device__ __align__(256) unsigned char g_div_scratch[kFields * kMaxPoints * sizeof(double)];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mutex;
+// Per device: the CUDA context the address was looked up in, and the address.
+// A device reset (cudaDeviceReset, or a primary context released and made
+// again) gives the device a new context in which the array sits elsewhere,
+// so the address is looked up again whenever the current context differs.
+CUcontext g_ctx[kMaxDevices] = {};
 void *g_addr[kMaxDevices] = {};
+
+using CtxGetCurrent = CUresult (*)(CUcontext *);
+
+CtxGetCurrent ctx_get_current()
+{
+    static CtxGetCurrent fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<CtxGetCurrent>(p);
+    }
+    return fn;
+}
 
 // Device address of the array on the current device.  Host code must not use
 // the array's name as an address (it names a host-side stand-in); the
-// address comes from cudaGetSymbolAddress, looked up once per device.
+// address comes from cudaGetSymbolAddress, looked up once per device and
+// context.  The first lookup on a device also loads the library's module
+// there (under lazy module loading), which reserves the array.
 int scratch_address(int device, void **out)
 {
     if (device < 0 || device >= kMaxDevices) return X3D_EINVAL;
     std::lock_guard<std::mutex> lock(g_mutex);
-    if (!g_addr[device]) {
+    CUcontext cur = nullptr;
+    const CtxGetCurrent get = ctx_get_current();
+    if (!get || get(&cur) != CUDA_SUCCESS || !cur) return X3D_ECUDA;
+    if (!g_addr[device] || g_ctx[device] != cur) {
         void *p = nullptr;
         if (cudaGetSymbolAddress(&p, g_div_scratch) != cudaSuccess || !p) {
             cudaGetLastError();
             return X3D_ECUDA;
         }
         g_addr[device] = p;
+        g_ctx[device] = cur;
     }
     *out = g_addr[device];
     return X3D_OK;

@@ -3,9 +3,9 @@
 //   flat:  consecutive threads on consecutive 16-byte vectors (the best case
 //          of the traffic mix);
 //   tile:  the y/z stage kernels' order: a CTA owns W x-adjacent columns of
-//          the ny rows of one z plane, thread (l, c) moves column l, rows
-//          c L .. c L + L - 1, so each warp touches W-float row segments
-//          ny-row strides apart.
+//          the ny rows of one z plane (or of a block of 128 of them), thread
+//          (l, c) moves one to four adjacent columns of 16 or 32 consecutive
+//          rows, so each warp touches W-float row segments a row apart.
 // bench.py times them next to the sweep to report how close each launch is
 // to what its traffic mix and access order allow.
 #include "x3d_internal.h"
@@ -27,23 +27,83 @@ __global__ void k_probe_flat(const float4 *__restrict__ in, const Outs6 outs, si
     }
 }
 
-template <int W>
-__global__ void k_probe_tile(const float *__restrict__ in, const Outs6 outs, int nx, int ny, int nz)
+template <int V>
+struct ProbeVec;
+template <>
+struct ProbeVec<1> {
+    using type = float;
+};
+template <>
+struct ProbeVec<2> {
+    using type = float2;
+};
+template <>
+struct ProbeVec<4> {
+    using type = float4;
+};
+
+// A CTA owns W x-adjacent columns of `rows` consecutive rows (all ny, or a
+// block of them) of one z plane; a thread moves V adjacent columns of RT
+// rows: all its loads, then its rows of each output in turn.
+//   BANDED = false: thread (l, c) takes rows c RT .. c RT + RT - 1 (the stage
+//     kernels' chunks), so one store of the CTA touches rows RT apart;
+//   BANDED = true: thread (l, r) takes rows r, r + NR, ... (NR = rows / RT),
+//     so one store of the CTA touches NR consecutive rows.
+// Tiles are numbered row block fastest, then x, then z (ZFIRST: then z,
+// then x, so consecutive CTAs work on different z planes).
+template <int W, int V, int RT, bool BANDED, bool ZFIRST>
+__global__ void k_probe_tile(const float *__restrict__ in, const Outs6 outs, int nx, int ny, int nz, int rows)
 {
-    const int t = threadIdx.x, l = t % W, c = t / W;
-    const int tiles_x = nx / W;
-    for (long tile = blockIdx.x; tile < (long)tiles_x * nz; tile += gridDim.x) {
-        const int x0 = (int)(tile % tiles_x) * W, o = (int)(tile / tiles_x);
-        const size_t base = (size_t)o * nx * ny + (size_t)c * kProbeL * nx + x0 + l;
-        float r[kProbeL];
+    using VT = typename ProbeVec<V>::type;
+    constexpr int WT = W / V;  // threads across the tile
+    const int t = threadIdx.x, l = t % WT, c = t / WT;
+    const int nr = rows / RT;
+    const int tiles_x = nx / W, nb = ny / rows;
+    const size_t r0 = BANDED ? (size_t)c : (size_t)c * RT;
+    const size_t rstep = BANDED ? (size_t)nr * nx : (size_t)nx;
+    for (long tile = blockIdx.x; tile < (long)tiles_x * nb * nz; tile += gridDim.x) {
+        const int rb = (int)(tile % nb);
+        const long xo = tile / nb;
+        const int x0 = (int)(ZFIRST ? xo / nz : xo % tiles_x) * W;
+        const int o = (int)(ZFIRST ? xo % nz : xo / tiles_x);
+        const size_t base = (size_t)o * nx * ny + ((size_t)rb * rows + r0) * nx + x0 + V * l;
+        VT r[RT];
 #pragma unroll
-        for (int j = 0; j < kProbeL; ++j) r[j] = in[base + (size_t)j * nx];
+        for (int j = 0; j < RT; ++j) r[j] = *reinterpret_cast<const VT *>(in + base + (size_t)j * rstep);
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
             float *dst = outs.p[k] + base;
 #pragma unroll
-            for (int j = 0; j < kProbeL; ++j) dst[(size_t)j * nx] = r[j];
+            for (int j = 0; j < RT; ++j) *reinterpret_cast<VT *>(dst + (size_t)j * rstep) = r[j];
         }
+    }
+}
+
+template <int W, int V, int RT, bool BANDED = false, bool ZFIRST = false>
+static int probe_tile(x3d_ctx_s *ctx, int per_sm, const float *in, const Outs6 &o, int nx, int ny, int nz, int rows)
+{
+    const int threads = (W / V) * (rows / RT);
+    // at most 512 threads: the 128-column form keeps 64 values per thread
+    // in registers (80 registers a thread)
+    if (rows % RT || threads > 512 || threads % 32)
+        return set_error(ctx, X3D_EINVAL, "tile probe: rows must give a whole number of warps (at most 512 threads)");
+    ++ctx->launches;
+    k_probe_tile<W, V, RT, BANDED, ZFIRST><<<ctx->num_sms * per_sm, threads, 0, ctx->stream>>>(in, o, nx, ny, nz,
+                                                                                               rows);
+    return cuda_check(ctx, cudaGetLastError(), "k_probe_tile launch");
+}
+
+template <bool BANDED, bool ZFIRST>
+static int probe_w(x3d_ctx_s *ctx, int w, int per_sm, const float *in, const Outs6 &o, int nx, int ny, int nz,
+                   int rows)
+{
+    switch (w) {
+    case 8: return probe_tile<8, 1, 32, BANDED, ZFIRST>(ctx, per_sm, in, o, nx, ny, nz, rows);
+    case 16: return probe_tile<16, 1, 32, BANDED, ZFIRST>(ctx, per_sm, in, o, nx, ny, nz, rows);
+    case 32: return probe_tile<32, 1, 32, BANDED, ZFIRST>(ctx, per_sm, in, o, nx, ny, nz, rows);
+    case 64: return probe_tile<64, 2, 32, BANDED, ZFIRST>(ctx, per_sm, in, o, nx, ny, nz, rows);
+    case 128: return probe_tile<128, 4, 16, BANDED, ZFIRST>(ctx, per_sm, in, o, nx, ny, nz, rows);
+    default: return set_error(ctx, X3D_EINVAL, "tile probe: w must be 8, 16, 32, 64 or 128");
     }
 }
 
@@ -61,15 +121,14 @@ int launch_roofline_probe(x3d_ctx_s *ctx, int pattern, int w, int ctas_per_sm, c
                                                                           n / 4);
         return cuda_check(ctx, cudaGetLastError(), "k_probe_flat launch");
     }
-    if (nx % w || ny % kProbeL || (w != 8 && w != 16 && w != 32) || (ny / kProbeL) * w > 1024)
-        return set_error(ctx, X3D_EINVAL, "tile probe needs nx % w == 0, ny % 32 == 0, w in {8, 16, 32}");
-    const int threads = w * (ny / kProbeL);
-    const int grid = ctx->num_sms * per_sm;
-    ++ctx->launches;
-    if (w == 8) k_probe_tile<8><<<grid, threads, 0, ctx->stream>>>(in, o, nx, ny, nz);
-    else if (w == 16) k_probe_tile<16><<<grid, threads, 0, ctx->stream>>>(in, o, nx, ny, nz);
-    else k_probe_tile<32><<<grid, threads, 0, ctx->stream>>>(in, o, nx, ny, nz);
-    return cuda_check(ctx, cudaGetLastError(), "k_probe_tile launch");
+    // 1: whole columns (rows = ny); 2: blocks of 128 rows; 3: whole
+    // columns, banded rows; 4: whole columns, tiles z plane first
+    const int rows = pattern == 2 ? 128 : ny;
+    if (nx % w || ny % rows || pattern > 4)
+        return set_error(ctx, X3D_EINVAL, "tile probe needs nx % w == 0 and ny % rows == 0");
+    if (pattern == 3) return probe_w<true, false>(ctx, w, per_sm, in, o, nx, ny, nz, rows);
+    if (pattern == 4) return probe_w<false, true>(ctx, w, per_sm, in, o, nx, ny, nz, rows);
+    return probe_w<false, false>(ctx, w, per_sm, in, o, nx, ny, nz, rows);
 }
 
 }  // namespace x3d
