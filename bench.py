@@ -267,21 +267,32 @@ def sweep_groups(ctx, fields, outs, fused):
 CONFIG_W = [16, 32, 16, 8, 32, 8, 16, 32, 16, 8, 32, 8, 32, 16, 32, 32]
 
 
+def config_pattern(cfg):
+    """The roofline probe pattern with the access order of y/z configuration
+    cfg: whole-line tiles of W columns, claimed in order from a counter by the
+    persistent configurations 6..15, at a fixed stride (one CTA per tile) by
+    the others."""
+    w = CONFIG_W[cfg] if 0 <= cfg < 16 else 16
+    return f"claim_w{w}" if 6 <= cfg < 16 else f"tile_w{w}"
+
+
 def pattern_ceilings(ctx, torch, src, outs):
     """Bandwidth of one read and six writes with no arithmetic
     (x3d_roofline_probe), flat, in the y stage kernels' tile order for
-    W = 8 .. 128 columns over whole lines, and over blocks of 128 rows: what
-    the sweep launches' traffic mix and access order can reach on this GPU
+    W = 8 .. 128 columns over whole lines, over blocks of 128 rows, and with
+    the tiles claimed in order from a counter as the persistent stage kernels
+    take them: what the sweep launches' traffic mix and access order can
+    reach on this GPU
     (best over 1, 2, 4 and 8 CTAs per SM of 5 timed launches after 3 warm-up
     ones)."""
     nz, ny, nx = src.shape
     bytes_moved = 7 * src.numel() * src.element_size()
     res = {}
     cases = [("flat", 0, 0)] + [(f"tile_w{w}", 1, w) for w in (8, 16, 32, 64, 128)] + \
-            [(f"block128_w{w}", 2, w) for w in (32, 64, 128)]
+            [(f"block128_w{w}", 2, w) for w in (32, 64, 128)] + [(f"claim_w{w}", 5, w) for w in (8, 16, 32)]
     for key, pattern, w in cases:
         rt = 16 if w == 128 else 32
-        rows = ny if pattern == 1 else 128
+        rows = 128 if pattern == 2 else ny
         if pattern and (nx % w or ny % rows or rows % rt or (w // max(1, w // 32)) * (rows // rt) > 512):
             continue
         best = None
@@ -519,7 +530,7 @@ def run_b200(args, world, rank, local):
     ceil = pattern_ceilings(ctx, torch, fields[0], outs[:6])
     if ceil:
         cfg = dom["config"]
-        key = "flat" if FAMILY[dom_d] == "ls_stage_x" else f"tile_w{CONFIG_W[cfg] if 0 <= cfg < 16 else 16}"
+        key = "flat" if FAMILY[dom_d] == "ls_stage_x" else config_pattern(cfg)
         if key in ceil:
             roofline["pattern_ceiling_gbs"] = ceil[key]
             roofline["pattern"] = key

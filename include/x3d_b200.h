@@ -150,9 +150,11 @@ int x3d_ctx_selftest_timeout(x3d_ctx ctx, double limit_s);
  * columns of the ny rows of a z plane, each thread on consecutive rows;
  * pattern 2: the same tiles over blocks of 128 rows; pattern 3: pattern 1
  * with each store of the CTA on consecutive rows; pattern 4: pattern 1 with
- * consecutive tiles on different z planes; nx % w == 0, ny a multiple of
- * the rows a thread moves (32, or 16 for w = 128) and of the block), so
- * that timing it gives the
+ * consecutive tiles on different z planes; pattern 5: pattern 1 with the
+ * tiles claimed in order from a counter, as the persistent stage kernels
+ * take them (w in {8, 16, 32}); nx % w == 0, ny a multiple of the rows a
+ * thread moves (32, or 16 for w = 128) and of the block), so that timing it
+ * gives the
  * bandwidth that traffic mix and access order can reach.  ctas_per_sm sets
  * the grid (0: 2 per SM). */
 int x3d_roofline_probe(x3d_ctx ctx, int pattern, int w, int ctas_per_sm, const void *in, void *const *outs,

@@ -353,7 +353,8 @@ int x3d_ctx_create_bc(x3d_ctx *out, int nx, int ny, int nz, double xlx, double y
     ctx->smem_optin = prop.sharedMemPerBlockOptin;
     if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc(&ctx->d_err, sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&ctx->d_red, 4 * sizeof(double)) != cudaSuccess) {
+        cudaMalloc(&ctx->d_red, 4 * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&ctx->d_claim, sizeof(unsigned long long)) != cudaSuccess) {
         x3d_ctx_destroy(ctx);
         return X3D_ECUDA;
     }
@@ -419,6 +420,7 @@ int x3d_ctx_destroy(x3d_ctx ctx)
     if (ctx->step_graph) cudaGraphDestroy(ctx->step_graph);
     if (ctx->d_err) cudaFree(ctx->d_err);
     if (ctx->d_red) cudaFree(ctx->d_red);
+    if (ctx->d_claim) cudaFree(ctx->d_claim);
     if (ctx->d_metric) cudaFree(ctx->d_metric);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
@@ -467,7 +469,7 @@ int x3d_roofline_probe(x3d_ctx ctx, int pattern, int w, int ctas_per_sm, const v
 {
     int rc = check_ctx(ctx);
     if (rc) return rc;
-    if (!in || !outs || nx < 1 || ny < 1 || nz < 1 || pattern < 0 || pattern > 4)
+    if (!in || !outs || nx < 1 || ny < 1 || nz < 1 || pattern < 0 || pattern > 5)
         return set_error(ctx, X3D_EINVAL, "bad probe request");
     float *o[6];
     for (int k = 0; k < 6; ++k) {

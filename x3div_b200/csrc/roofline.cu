@@ -107,6 +107,39 @@ static int probe_w(x3d_ctx_s *ctx, int w, int per_sm, const float *in, const Out
     }
 }
 
+// Pattern 5: the tile order of pattern 1 with tiles claimed from a counter
+// (one atomicAdd per tile) instead of at a fixed stride, as the persistent
+// stage kernels take them, so the tiles in flight stay a window of
+// consecutive tiles.
+template <int W>
+__global__ void k_probe_tile_claim(const float *__restrict__ in, const Outs6 outs, int nx, int ny, int nz,
+                                   unsigned long long *counter)
+{
+    constexpr int RT = 32;
+    __shared__ long s_tile;
+    const int t = threadIdx.x, l = t % W, c = t / W;
+    const int tiles_x = nx / W;
+    const long ntiles = (long)tiles_x * nz;
+    for (;;) {
+        if (t == 0) s_tile = (long)atomicAdd(counter, 1ull);
+        __syncthreads();
+        const long tile = s_tile;
+        __syncthreads();
+        if (tile >= ntiles) break;
+        const int x0 = (int)(tile % tiles_x) * W, o = (int)(tile / tiles_x);
+        const size_t base = (size_t)o * nx * ny + (size_t)c * RT * nx + x0 + l;
+        float r[RT];
+#pragma unroll
+        for (int j = 0; j < RT; ++j) r[j] = in[base + (size_t)j * nx];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            float *dst = outs.p[k] + base;
+#pragma unroll
+            for (int j = 0; j < RT; ++j) dst[(size_t)j * nx] = r[j];
+        }
+    }
+}
+
 int launch_roofline_probe(x3d_ctx_s *ctx, int pattern, int w, int ctas_per_sm, const float *in, float *const *outs,
                           int nx, int ny, int nz)
 {
@@ -124,8 +157,22 @@ int launch_roofline_probe(x3d_ctx_s *ctx, int pattern, int w, int ctas_per_sm, c
     // 1: whole columns (rows = ny); 2: blocks of 128 rows; 3: whole
     // columns, banded rows; 4: whole columns, tiles z plane first
     const int rows = pattern == 2 ? 128 : ny;
-    if (nx % w || ny % rows || pattern > 4)
+    if (nx % w || ny % rows || pattern > 5)
         return set_error(ctx, X3D_EINVAL, "tile probe needs nx % w == 0 and ny % rows == 0");
+    if (pattern == 5) {
+        const int threads = w * (ny / 32);
+        if ((w != 8 && w != 16 && w != 32) || ny % 32 || threads > 512 || threads % 32)
+            return set_error(ctx, X3D_EINVAL, "tile probe pattern 5: w 8, 16 or 32, ny % 32 == 0");
+        auto *counter = ctx->d_claim;
+        if (cudaMemsetAsync(counter, 0, sizeof(*counter), ctx->stream) != cudaSuccess)
+            return set_error(ctx, X3D_ECUDA, "probe counter reset");
+        const unsigned grid = (unsigned)(ctx->num_sms * per_sm);
+        ++ctx->launches;
+        if (w == 8) k_probe_tile_claim<8><<<grid, threads, 0, ctx->stream>>>(in, o, nx, ny, nz, counter);
+        else if (w == 16) k_probe_tile_claim<16><<<grid, threads, 0, ctx->stream>>>(in, o, nx, ny, nz, counter);
+        else k_probe_tile_claim<32><<<grid, threads, 0, ctx->stream>>>(in, o, nx, ny, nz, counter);
+        return cuda_check(ctx, cudaGetLastError(), "k_probe_tile_claim launch");
+    }
     if (pattern == 3) return probe_w<true, false>(ctx, w, per_sm, in, o, nx, ny, nz, rows);
     if (pattern == 4) return probe_w<false, true>(ctx, w, per_sm, in, o, nx, ny, nz, rows);
     return probe_w<false, false>(ctx, w, per_sm, in, o, nx, ny, nz, rows);

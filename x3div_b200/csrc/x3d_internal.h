@@ -126,6 +126,9 @@ struct x3d_ctx_s {
     // later calls and freed with the context
     std::vector<std::pair<void *, size_t>> staging;
     double *d_red = nullptr;  // small reduction buffer
+    // tile counter of the persistent stage kernels (zeroed before each launch
+    // on the context stream; allocated with the context, so no call allocates it)
+    unsigned long long *d_claim = nullptr;
     double *d_metric = nullptr;  // device copy of a y stretching metric (ny doubles)
     int metric_len = 0;
     // host arrays with device-resident mirrors (x3d_buf_register)
