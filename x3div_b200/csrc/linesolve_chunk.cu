@@ -404,8 +404,9 @@ __device__ __forceinline__ void accumulate(const StageOp<S> &so, T (&acc)[L], co
 // ---------------------------------------------------------------------------
 // y- and z-lines.
 struct StageMaps {
-    CUtensorMap m[kMaxStageTiles];  // inputs
-    CUtensorMap pm[kMaxStageOps];   // base (else base2) arrays prefetched into L2 (ops with prefetch_base)
+    CUtensorMap m[kMaxStageTiles];   // inputs
+    CUtensorMap hm[kMaxStageTiles];  // the same inputs in boxes of kHalo rows: the periodic halos
+    CUtensorMap pm[kMaxStageOps];    // base (else base2) arrays prefetched into L2 (ops with prefetch_base)
 };
 
 // Flush fields of a stage operator, read from the parameters once per
@@ -596,7 +597,7 @@ __device__ __forceinline__ void flush_yz(const FlushArgs<T> &fa, const V (&res)[
 template <typename T, int W, int L, bool ACC, bool PERSIST, int PR = 1>
 __global__ void __launch_bounds__(kStageThreads<T, L, PR>, 1)
     ls_stage_yz(const __grid_constant__ StageMaps maps, const __grid_constant__ StageProgram<T> prog, int nx,
-                int ny, int dir, int box_n, int nbox, size_t tile_bytes, long ntiles,
+                int ny, int dir, int box_n, int nbox, int tma_halo, size_t tile_bytes, long ntiles,
                 unsigned long long *claim, int *err)
 {
     using V = typename PairOf<T, PR>::type;
@@ -623,7 +624,8 @@ __global__ void __launch_bounds__(kStageThreads<T, L, PR>, 1)
         const int x0 = (int)(tile % tiles_x) * W;
         const int o = (int)(tile / tiles_x);
         uint64_t *bar = &bars[slot];
-        mbar_arrive_expect_tx(bar, (uint32_t)((size_t)prog.ntiles * nbox * box_n * W * sizeof(T)));
+        mbar_arrive_expect_tx(bar, (uint32_t)((size_t)prog.ntiles * (nbox * box_n + (tma_halo ? 2 * kHalo : 0)) *
+                                              W * sizeof(T)));
         for (int ti = 0; ti < prog.ntiles; ++ti) {
             T *tp = reinterpret_cast<T *>(smem_raw + slot * slot_bytes + ti * tile_bytes) + kHalo * W;
             for (int b = 0; b < nbox; ++b) {
@@ -631,6 +633,16 @@ __global__ void __launch_bounds__(kStageThreads<T, L, PR>, 1)
                     tma_load_3d(tp + (size_t)b * box_n * W, &maps.m[ti], bar, x0, b * box_n, o);
                 else
                     tma_load_3d(tp + (size_t)b * box_n * W, &maps.m[ti], bar, x0, o, b * box_n);
+            }
+            if (tma_halo) {  // points n-4 .. n-1 before the line, 0 .. 3 after it
+                T *hb = tp - kHalo * W, *ha = tp + (size_t)n * W;
+                if (dir == DY) {
+                    tma_load_3d(hb, &maps.hm[ti], bar, x0, n - kHalo, o);
+                    tma_load_3d(ha, &maps.hm[ti], bar, x0, 0, o);
+                } else {
+                    tma_load_3d(hb, &maps.hm[ti], bar, x0, o, n - kHalo);
+                    tma_load_3d(ha, &maps.hm[ti], bar, x0, o, 0);
+                }
             }
         }
         // the tile's base arrays (read back by the flushes) into L2
@@ -655,29 +667,30 @@ __global__ void __launch_bounds__(kStageThreads<T, L, PR>, 1)
     if (PERSIST) tile = s_tile[0];
     for (int it = 0; tile < ntiles; ++it) {
         const int slot = PERSIST ? (it & 1) : 0;
-        long next = ntiles;  // thread 0: the tile claimed after this one
-        if (PERSIST && t == 0) {
-            next = (long)atomicAdd(claim, 1ull);
-            s_tile[(it + 1) & 1] = next;
-            if (next < ntiles) issue(next, slot ^ 1);
-        }
-        const bool pre = next < ntiles;  // meaningful in thread 0, which alone waits on it
         const uint32_t parity = PERSIST ? ((it >> 1) & 1) : 0;
         const bool ok = mbar_wait_bounded(&bars[slot], parity, kChunkWaitNs);
+        // this barrier also ends every thread's reads of the other slot (the
+        // previous tile), so the next tile's copies may go there now
         if (!__syncthreads_and(ok)) {
             if (t == 0) {
                 atomicExch(err, 1);
                 mbar_wait_bounded(&bars[slot], parity, kChunkWaitNs);
-                if (pre) mbar_wait_bounded(&bars[slot ^ 1], ((it + 1) >> 1) & 1, kChunkWaitNs);
             }
             return;
+        }
+        if (PERSIST && t == 0) {
+            const long next = (long)atomicAdd(claim, 1ull);
+            s_tile[(it + 1) & 1] = next;  // read after this tile's operator barriers
+            if (next < ntiles) issue(next, slot ^ 1);
         }
         const int x0 = (int)(tile % tiles_x) * W;
         const int o = (int)(tile / tiles_x);
         unsigned char *base = smem_raw + slot * slot_bytes;
-        fill_halos_yz<T>(base, tile_bytes, prog.ntiles, n, W, kHalo);
-        fence_proxy_async_smem();  // the halo rows are refilled by TMA two tiles later
-        __syncthreads();
+        if (!tma_halo) {
+            fill_halos_yz<T>(base, tile_bytes, prog.ntiles, n, W, kHalo);
+            fence_proxy_async_smem();  // the halo rows are refilled by TMA two tiles later
+            __syncthreads();
+        }
         // window of this chunk: rows kHalo + cs - 4 ...
         auto col = [&](int ti) {
             return reinterpret_cast<const T *>(base + ti * tile_bytes) + (kHalo + cs - 4) * W + PR * l;
@@ -716,7 +729,9 @@ __global__ void __launch_bounds__(kStageThreads<T, L, PR>, 1)
             }
         }
         if (!PERSIST) break;
-        __syncthreads();  // the slot is refilled two tiles later; the next tile is known
+        // written by thread 0 before the operator barriers above; rewritten two
+        // tiles later, after the next wait barrier, which every thread reaches
+        // after reading it here
         tile = s_tile[(it + 1) & 1];
     }
 }
@@ -1010,23 +1025,22 @@ __global__ void __launch_bounds__(512, 1)
     if (PERSIST) tile = s_tile[0];
     for (int it = 0; tile < ntiles; ++it) {
         const int slot = PERSIST ? (it & 1) : 0;
-        long next = ntiles;  // thread 0: the tile claimed after this one
-        if (PERSIST && t == 0) {
-            next = (long)atomicAdd(claim, 1ull);
-            s_tile[(it + 1) & 1] = next;
-            if (next < ntiles) issue(next, slot ^ 1);
-        }
-        const bool pre = next < ntiles;  // meaningful in thread 0, which alone waits on it
         const uint32_t parity = PERSIST ? ((it >> 1) & 1) : 0;
         const bool ok = mbar_wait_bounded(&bars[slot], parity, kChunkWaitNs);
+        // this barrier also ends every thread's reads of the other slot (the
+        // previous tile), so the next tile's copies may go there now
         if (!__syncthreads_and(ok)) {
             if (t == 0) {
                 atomicExch(err, 1);
                 mbar_wait_bounded(&bars[slot], parity, kChunkWaitNs);
-                if (pre) mbar_wait_bounded(&bars[slot ^ 1], ((it + 1) >> 1) & 1, kChunkWaitNs);
             }
             if (t < W) bulk_wait_all();
             return;
+        }
+        if (PERSIST && t == 0) {
+            const long next = (long)atomicAdd(claim, 1ull);
+            s_tile[(it + 1) & 1] = next;  // read after this tile's barriers
+            if (next < ntiles) issue(next, slot ^ 1);
         }
         const long l0 = tile * W;
         const int rows = (int)min((long)W, nlines - l0);
@@ -1084,8 +1098,7 @@ __global__ void __launch_bounds__(512, 1)
             }
         }
         if (!PERSIST) break;
-        __syncthreads();  // the slot is refilled two tiles later; the next tile is known
-        tile = s_tile[(it + 1) & 1];
+        tile = s_tile[(it + 1) & 1];  // as in ls_stage_yz
     }
     if (t < W) bulk_wait_all();
 }
@@ -1256,11 +1269,11 @@ static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog_in, int 
         if (smem + 1024 > ctx->smem_optin) return X3D_EUNSUPPORTED;
         StageMaps maps;
         std::memset(&maps, 0, sizeof(maps));
-        auto encode = [&](CUtensorMap *m, const void *ptr) {
+        auto encode = [&](CUtensorMap *m, const void *ptr, int rows_in_box) {
             cuuint64_t gdim[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
             cuuint64_t gstride[2] = {(cuuint64_t)nx * es, (cuuint64_t)nx * ny * es};
             cuuint32_t box[3] = {(cuuint32_t)W, 1, 1};
-            box[dir == DY ? 1 : 2] = (cuuint32_t)box_n;
+            box[dir == DY ? 1 : 2] = (cuuint32_t)rows_in_box;
             cuuint32_t estr[3] = {1, 1, 1};
             return enc(m, sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
                        const_cast<void *>(ptr), gdim, gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -1268,10 +1281,16 @@ static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog_in, int 
                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
         };
         for (int ti = 0; ti < prog.ntiles; ++ti)
-            if (!encode(&maps.m[ti], prog.in[ti])) return X3D_EUNSUPPORTED;
+            if (!encode(&maps.m[ti], prog.in[ti], box_n)) return X3D_EUNSUPPORTED;
+        // the periodic halos come by TMA too where the boxes end exactly at the
+        // line's end (a box running past it would fill the rows after the line
+        // with zeros); otherwise the kernel copies them in shared memory
+        int tma_halo = nb * box_n == n ? 1 : 0;
+        for (int ti = 0; ti < prog.ntiles && tma_halo; ++ti)
+            if (!encode(&maps.hm[ti], prog.in[ti], kHalo)) tma_halo = 0;
         for (int k = 0; k < prog.nops; ++k)
             if (prog.ops[k].prefetch_base &&
-                !encode(&maps.pm[k], prog.ops[k].base ? prog.ops[k].base : prog.ops[k].base2))
+                !encode(&maps.pm[k], prog.ops[k].base ? prog.ops[k].base : prog.ops[k].base2, box_n))
                 prog.ops[k].prefetch_base = 0;
         prog.prefetch_mask = 0;
         for (int k = 0; k < prog.nops; ++k)
@@ -1287,7 +1306,7 @@ static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog_in, int 
             if (rc) return rc;
         }
         ++ctx->launches;
-        kern<<<grid, threads, smem, st>>>(maps, prog, nx, ny, dir, box_n, nb, tile, ntiles, ctx->d_claim,
+        kern<<<grid, threads, smem, st>>>(maps, prog, nx, ny, dir, box_n, nb, tma_halo, tile, ntiles, ctx->d_claim,
                                           ctx->d_err);
         return cuda_check(ctx, cudaGetLastError(), "ls_stage_yz launch");
 
