@@ -123,6 +123,11 @@ module x3d_b200_bind
        type(c_ptr), value :: ctx
        integer(c_long_long) :: cnt
      end function
+     integer(c_int) function x3d_ctx_last_kernel(ctx, cfg) bind(C, name="x3d_ctx_last_kernel")
+       import :: c_ptr, c_int
+       type(c_ptr), value :: ctx
+       integer(c_int) :: cfg
+     end function
      integer(c_int) function x3d_ctx_geometry(ctx, dims, lengths, spacing, prec) bind(C, &
           name="x3d_ctx_geometry")
        import :: c_ptr, c_int

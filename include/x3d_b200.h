@@ -164,6 +164,10 @@ const char *x3d_ctx_last_error(x3d_ctx ctx);
 /* Number of this library's kernels launched on the context so far (library
  * kernels such as cuFFT's are not counted). */
 int x3d_ctx_launch_count(x3d_ctx ctx, unsigned long long *count);
+/* Configuration (as in x3d_ctx_set_kernel) of the last periodic line-solve
+ * or fused-stage launch on the context, -1 before the first: shows which
+ * kernel a call ran after fall-backs.  No reference counterpart. */
+int x3d_ctx_last_kernel(x3d_ctx ctx, int *cfg);
 /* Geometry query: dims[3], lengths[3], spacing[3] (any may be NULL). */
 int x3d_ctx_geometry(x3d_ctx ctx, int *dims, double *lengths, double *spacing, int *precision);
 
@@ -257,13 +261,15 @@ int x3d_autotune(x3d_ctx ctx, int max_group);
 /* Force kernel configuration cfg (0..5 chunked, one CTA per tile;
  * 6..11 the same shapes as persistent double-buffered kernels; 12..15 y/z
  * kernels that carry two x-adjacent lines per thread in packed FP32
- * registers (FP32 contexts, even nx); 16 one thread per line) for
- * every later call and forget tuned choices; -1 restores the default.  A
+ * registers (FP32 contexts, even nx); 16 one thread per line; 17 the y/z
+ * kernel of configuration 6 built for three CTAs per SM, for operators that
+ * each write their own output, on lines of at most 16 chunks) for every
+ * later call and forget tuned choices; -1 restores the default.  A
  * configuration that cannot handle a call (alignment, shared memory) still
  * falls back to one that can.  No reference counterpart. */
 int x3d_ctx_set_kernel(x3d_ctx ctx, int cfg);
 /* The configuration chosen for (direction, group size): *cfg = -1 when not
- * tuned, 0..15 chunked variants, 16 one thread per line. */
+ * tuned, 0..15 and 17 chunked variants, 16 one thread per line. */
 int x3d_autotune_choice(x3d_ctx ctx, int dir, int group, int *cfg);
 /* The configuration chosen for a fused stage of the Euler step (*cfg = -1
  * when not tuned): stage is one of transeq_x, transeq_y, transeq_z, div_x,
@@ -274,7 +280,7 @@ int x3d_autotune_choice(x3d_ctx ctx, int dir, int group, int *cfg);
  * launch has its own configuration under its own name. */
 int x3d_autotune_stage_choice(x3d_ctx ctx, const char *stage, int *cfg);
 /* Sets one of those choices (a saved tuning, or a form to test); value -1
- * removes it.  Configurations are 0..15; "<stage>.split" 0 or 1;
+ * removes it.  Configurations are 0..15 and 17; "<stage>.split" 0 or 1;
  * "<stage>.parts" a launch count, used only where the stage splits into
  * exactly that many parts.  Extension. */
 int x3d_ctx_set_stage_choice(x3d_ctx ctx, const char *stage, int value);

@@ -15,7 +15,7 @@ from conftest import rel_err, seeded_field
 pytestmark = pytest.mark.gpu
 
 X, Y, Z = 0, 1, 2
-KERNEL_CONFIGS = 17  # x3d_ctx_set_kernel: 0..15 chunked, 16 one thread per line
+KERNEL_CONFIGS = 18  # x3d_ctx_set_kernel: 0..15 and 17 chunked, 16 one thread per line
 
 # (routine, operator instance, oracle kind, direction, signature style)
 ROUTINES = [
@@ -187,8 +187,9 @@ def test_bad_calls_raise(torch_cuda, contexts):
 # which the paired configurations take
 @pytest.mark.parametrize("shape", [(8, 8, 8), (64, 48, 40), (100, 36, 12), (96, 20, 200), (40, 60, 62)])
 def test_every_kernel_configuration(oracle, torch_cuda, contexts, cfg, prec, shape):
-    """Each kernel configuration (chunked variants 0-15, one thread per line 16)
-    reproduces the oracle; configurations that cannot take a shape fall back."""
+    """Each kernel configuration (chunked variants 0-15 and 17, one thread per
+    line 16) reproduces the oracle; configurations that cannot take a shape
+    fall back, and x3d_ctx_last_kernel names the one that ran."""
     torch = torch_cuda
     from x3div_b200 import to_device, to_host
     ctx = contexts(shape, prec)
@@ -203,6 +204,7 @@ def test_every_kernel_configuration(oracle, torch_cuda, contexts, cfg, prec, sha
             t_d = torch.empty_like(u_d)
             call(ctx, routine, style, t_d, u_d, ctx.op(opname), shape)
             ctx.sync()
+            assert 0 <= ctx.last_kernel() < KERNEL_CONFIGS
             err = rel_err(to_host(t_d), oracle.apply(kind, direction, used, d[direction]))
             assert err < tol, (routine, cfg, err)
     finally:
@@ -310,3 +312,53 @@ def test_long_lines(oracle, torch_cuda, contexts, shape, prec):
         ctx.sync()
         err = rel_err(to_host(t_d), oracle.apply(kind, direction, used, d[direction]))
         assert err < tol, (routine, shape, prec, err)
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("shape", [(64, 128, 256), (48, 64, 96)])
+def test_three_ctas_per_sm_configuration(oracle, torch_cuda, contexts, prec, shape):
+    """Configuration 17 (the 16-line persistent y/z kernel built for three CTAs
+    per SM) runs the y and z lines it can take -- plain outputs, at most 256
+    threads (16 chunks), an even chunk count -- as x3d_ctx_last_kernel shows,
+    alone and as a six-operator launch, and matches the oracle."""
+    torch = torch_cuda
+    from x3div_b200 import to_device, to_host
+    ctx = contexts(shape, prec)
+    ctx.set_kernel(17)
+    dt = torch.float64 if prec == "f64" else torch.float32
+    u_d = to_device(seeded_field(shape, seed=1717, noise=1e-2), dt)
+    used = to_host(u_d).astype(np.float64)
+    d = {X: ctx.dx, Y: ctx.dy, Z: ctx.dz}
+    tol = 1e-12 if prec == "f64" else 1e-5
+    L = 32 if prec == "f32" else 16
+
+    def takes(n):
+        c = -(-n // L)
+        return c * 16 <= 256 and (c * 16) % 32 == 0
+
+    names = {Y: ("dery", "deryy", "deryvp", "derypv", "intyvp", "intypv"),
+             Z: ("derz", "derzz", "derzvp", "derzpv", "intzvp", "intzpv")}
+    kinds = ["der", "der2", "dervp", "derpv", "intvp", "intpv"]
+    ran = 0
+    try:
+        for direction in (Y, Z):
+            outs = [torch.full_like(u_d, float("nan")) for _ in range(6)]
+            for k in range(6):
+                ctx.apply_batch([(ctx.op(names[direction][k]), u_d, outs[k])])
+                ctx.sync()
+                if takes(shape[direction]):
+                    assert ctx.last_kernel() == 17, (direction, k, ctx.last_kernel())
+                    ran += 1
+                err = rel_err(to_host(outs[k]), oracle.apply(kinds[k], direction, used, d[direction]))
+                assert err < tol, (direction, kinds[k], err)
+            outs = [torch.full_like(u_d, float("nan")) for _ in range(6)]
+            ctx.apply_batch([(ctx.op(names[direction][k]), u_d, outs[k]) for k in range(6)])
+            ctx.sync()
+            if takes(shape[direction]):
+                assert ctx.last_kernel() == 17
+            for k in range(6):
+                err = rel_err(to_host(outs[k]), oracle.apply(kinds[k], direction, used, d[direction]))
+                assert err < tol, (direction, kinds[k], err)
+    finally:
+        ctx.set_kernel(-1)
+    assert ran > 0

@@ -35,6 +35,7 @@ SIGNATURES = {
     "x3d_ctx_set_stream": [_vp, _vp],
     "x3d_ctx_get_stream": [_vp, ctypes.POINTER(_vp)],
     "x3d_ctx_launch_count": [_vp, ctypes.POINTER(ctypes.c_ulonglong)],
+    "x3d_ctx_last_kernel": [_vp, _ip],
     "x3d_ctx_sync": [_vp],
     "x3d_ctx_last_error": [_vp],
     "x3d_ctx_geometry": [_vp, _ip, _dp, _dp, _ip],

@@ -143,6 +143,13 @@ class Context:
         self._check(self.L.x3d_ctx_launch_count(self.handle, ctypes.byref(out)))
         return out.value
 
+    def last_kernel(self) -> int:
+        """x3d_ctx_last_kernel: configuration of the last line-solve or
+        fused-stage launch (-1 before the first)."""
+        out = ctypes.c_int()
+        self._check(self.L.x3d_ctx_last_kernel(self.handle, ctypes.byref(out)))
+        return out.value
+
     def get_stream(self) -> int:
         out = ctypes.c_void_p()
         self._check(self.L.x3d_ctx_get_stream(self.handle, ctypes.byref(out)))
@@ -256,7 +263,7 @@ class Context:
         self._check(self.L.x3d_autotune(self.handle, int(max_group)))
 
     def set_kernel(self, cfg):
-        """Force a kernel configuration (0..15 chunked, 16 thread per line, -1 default)."""
+        """Force a kernel configuration (0..15 and 17 chunked, 16 thread per line, -1 default)."""
         self._check(self.L.x3d_ctx_set_kernel(self.handle, int(cfg)))
 
     def autotune_choice(self, direction, group):

@@ -441,6 +441,13 @@ int x3d_ctx_launch_count(x3d_ctx ctx, unsigned long long *count)
     return X3D_OK;
 }
 
+int x3d_ctx_last_kernel(x3d_ctx ctx, int *cfg)
+{
+    if (!ctx || !cfg) return X3D_EINVAL;
+    *cfg = ctx->last_cfg;
+    return X3D_OK;
+}
+
 int x3d_ctx_get_stream(x3d_ctx ctx, void **stream)
 {
     if (!ctx || !stream) return X3D_EINVAL;
@@ -766,7 +773,7 @@ int x3d_autotune(x3d_ctx ctx, int max_group)
 
 int x3d_ctx_set_kernel(x3d_ctx ctx, int cfg)
 {
-    if (!ctx || cfg < -1 || cfg > kChunkConfigs) return X3D_EINVAL;
+    if (!ctx || cfg < -1 || cfg >= kAllConfigs) return X3D_EINVAL;
     ctx->tuned.clear();
     ctx->stage_tuned.clear();
     ctx->stage_ms.clear();
@@ -803,8 +810,8 @@ int x3d_ctx_set_stage_choice(x3d_ctx ctx, const char *stage, int value)
     };
     if (value < -1) return set_error(ctx, X3D_EINVAL, "stage choice below -1");
     if (ends(".split") && value > 1) return set_error(ctx, X3D_EINVAL, "a split choice is 0 or 1");
-    if (!ends(".split") && !ends(".parts") && value >= kChunkConfigs)
-        return set_error(ctx, X3D_EINVAL, "stage configurations are 0..15");
+    if (!ends(".split") && !ends(".parts") && value >= 0 && !is_stage_cfg(value))
+        return set_error(ctx, X3D_EINVAL, "stage configurations are 0..15 and 17");
     if (value == -1) ctx->stage_tuned.erase(s);
     else ctx->stage_tuned[s] = value;
     return X3D_OK;

@@ -561,6 +561,7 @@ static int run_tpl(x3d_ctx_s *ctx, int dir, const void *in, const x3d_op_s *cons
                             : run_typed<double>(ctx, ops[k], kinds[k], dir, in, outs[k], nx, ny, nz);
         if (rc) return rc;
     }
+    ctx->last_cfg = kChunkConfigs;
     return X3D_OK;
 }
 
@@ -577,11 +578,12 @@ static int run_chunk(x3d_ctx_s *ctx, int dir, const void *in, const x3d_op_s *co
     return launch_stage<T>(ctx, prog, dir, nx, ny, nz, cfg);
 }
 
-// cfg: 0..kChunkConfigs-1 chunked, kChunkConfigs thread-per-line.
+// cfg: a chunked configuration (is_stage_cfg), or kChunkConfigs for one
+// thread per line.
 static int run_cfg(x3d_ctx_s *ctx, int cfg, int dir, const void *in, const x3d_op_s *const *ops,
                    const int *kinds, void *const *outs, int nops, int nx, int ny, int nz, bool fp32)
 {
-    if (cfg < kChunkConfigs)
+    if (is_stage_cfg(cfg))
         return fp32 ? run_chunk<float>(ctx, dir, in, ops, kinds, outs, nops, nx, ny, nz, cfg)
                     : run_chunk<double>(ctx, dir, in, ops, kinds, outs, nops, nx, ny, nz, cfg);
     return run_tpl(ctx, dir, in, ops, kinds, outs, nops, nx, ny, nz, fp32);
@@ -601,7 +603,7 @@ int launch_group(x3d_ctx_s *ctx, int dir, const void *in, const x3d_op_s *const 
     const int first = it != ctx->tuned.end() ? it->second : ctx->default_cfg;
     int rc = run_cfg(ctx, first, dir, in, ops, kinds, outs, nops, nx, ny, nz, fp32);
     if (rc != X3D_EUNSUPPORTED) return rc;
-    for (int cfg = 0; cfg <= kChunkConfigs; ++cfg) {
+    for (int cfg = 0; cfg < kAllConfigs; ++cfg) {
         if (cfg == first) continue;
         rc = run_cfg(ctx, cfg, dir, in, ops, kinds, outs, nops, nx, ny, nz, fp32);
         if (rc != X3D_EUNSUPPORTED) return rc;
@@ -626,7 +628,7 @@ int autotune_group(x3d_ctx_s *ctx, int dir, const void *in, const x3d_op_s *cons
     cudaEventCreate(&b);
     int best = -1;
     float bt = 0.f;
-    for (int cfg = 0; cfg <= kChunkConfigs; ++cfg) {
+    for (int cfg = 0; cfg < kAllConfigs; ++cfg) {
         int rc = run_cfg(ctx, cfg, dir, in, ops, kinds, outs, nops, nx, ny, nz, fp32);  // warm-up / probe
         if (rc == X3D_EUNSUPPORTED) continue;
         if (rc) break;

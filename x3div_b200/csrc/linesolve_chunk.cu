@@ -298,10 +298,18 @@ __device__ __forceinline__ void load_resp(const StageProgram<S> &prog, V *dst)
 // or resp[2..3] for a short last chunk) come from this operator's block of
 // the shared-memory copy as 16-byte vectors, so each fix is one fused
 // multiply-add per carry and half a load per point.
-template <typename T, int L, typename Load, typename S>
+//
+// keep = nh | ng << 8 (full chunks): the fixes by h_j for j >= nh and by
+// g_j for j < L - ng are dropped, their responses being below 2^-32 (FP32)
+// or 2^-62 (FP64) of the largest, far under the sweep's rounding (for the
+// first derivative, rho = -0.38, that is all h past the 24th point and all g
+// before the 8th; operators with |rho| < 0.2 keep half of each).  They go in
+// blocks of 8 points, chosen by tests uniform across the CTA.
+// Only kernels whose registers allow it (TRIM) compile the trimmed form.
+template <typename T, int L, bool TRIM = false, typename Load, typename S>
 __device__ __forceinline__ void chunk_solve_resp(const LineOp<S> &op, int kind, const T *resp, const Load &load,
                                                  T (&r)[L], const ChunkScratch<T> &sc, int W, int l, int c,
-                                                 int C, int nv, int q)
+                                                 int C, int nv, int q, int keep = 0)
 {
     constexpr int ti = L == kChunkLong<S> ? 0 : 1;
     // operator fields into registers once (the parameters are read through
@@ -344,6 +352,42 @@ __device__ __forceinline__ void chunk_solve_resp(const LineOp<S> &op, int kind, 
     const T B = chunk_carry<T, -1>(sc.bz, K, mf, ml, wrap, W, l, c, C);
     using VT = typename Vec4<T>::type;
     constexpr int V = Vec4<T>::N;
+    const int nh = keep & 0xff, ng = keep >> 8;
+    if (TRIM && nv == L && keep && (nh < L || ng < L)) {
+        constexpr int B8 = L < 8 ? L : 8;
+#pragma unroll
+        for (int j0 = 0; j0 < L; j0 += B8) {
+            const bool dh = j0 < nh, dg = j0 + B8 > L - ng;
+            if (dh && dg) {
+#pragma unroll
+                for (int j = j0; j < j0 + B8; j += V) {
+                    const VT hv = *reinterpret_cast<const VT *>(h + j);
+                    const VT gv = *reinterpret_cast<const VT *>(g + j);
+                    const T *he = reinterpret_cast<const T *>(&hv);
+                    const T *ge = reinterpret_cast<const T *>(&gv);
+#pragma unroll
+                    for (int v = 0; v < V; ++v) r[j + v] = fma(F, he[v], fma(B, ge[v], r[j + v]));
+                }
+            } else if (dh) {
+#pragma unroll
+                for (int j = j0; j < j0 + B8; j += V) {
+                    const VT hv = *reinterpret_cast<const VT *>(h + j);
+                    const T *he = reinterpret_cast<const T *>(&hv);
+#pragma unroll
+                    for (int v = 0; v < V; ++v) r[j + v] = fma(F, he[v], r[j + v]);
+                }
+            } else if (dg) {
+#pragma unroll
+                for (int j = j0; j < j0 + B8; j += V) {
+                    const VT gv = *reinterpret_cast<const VT *>(g + j);
+                    const T *ge = reinterpret_cast<const T *>(&gv);
+#pragma unroll
+                    for (int v = 0; v < V; ++v) r[j + v] = fma(B, ge[v], r[j + v]);
+                }
+            }
+        }
+        return;
+    }
 #pragma unroll
     for (int j = 0; j < L; j += V) {
         const VT hv = *reinterpret_cast<const VT *>(h + j);
@@ -594,8 +638,14 @@ __device__ __forceinline__ void flush_yz(const FlushArgs<T> &fa, const V (&res)[
 // consecutive tiles: one read and six writes of 16-column y tiles run at
 // 6.4 TB/s that way against 4.6 TB/s at a fixed stride (x3d_roofline_probe
 // patterns 5 and 1).  The launcher zeroes the counter before each launch.
-template <typename T, int W, int L, bool ACC, bool PERSIST, int PR = 1>
-__global__ void __launch_bounds__(kStageThreads<T, L, PR>, 1)
+//
+// OCC > 1: the kernel is compiled for OCC CTAs of at most 256 threads per SM
+// (at most 65536 / (256 OCC) registers a thread).  With OCC = 3 the plain
+// FP32 16-line, 32-point-chunk kernel fits 80 registers without spilling, so
+// an SM holds 24 warps instead of 16 -- the sweep kernels are latency- and
+// issue-bound at 16 (issue active about half the cycles).
+template <typename T, int W, int L, bool ACC, bool PERSIST, int PR = 1, int OCC = 1>
+__global__ void __launch_bounds__(OCC > 1 ? 256 : kStageThreads<T, L, PR>, OCC)
     ls_stage_yz(const __grid_constant__ StageMaps maps, const __grid_constant__ StageProgram<T> prog, int nx,
                 int ny, int dir, int box_n, int nbox, int tma_halo, size_t tile_bytes, long ntiles,
                 unsigned long long *claim, int *err)
@@ -720,7 +770,9 @@ __global__ void __launch_bounds__(kStageThreads<T, L, PR>, 1)
                     for (int j = 0; j < NW; ++j) w[j] = at(ca + (J0 + j) * W);
                 }
             };
-            chunk_solve_resp<V, L>(so.op, so.kind, resp_s + k * 4 * L, load, r, sc, WP, l, c, C, nv, c * WP + l);
+            constexpr bool trim = !ACC && (OCC == 1 || sizeof(T) == 4);  // FP64 at 80 registers would spill
+            chunk_solve_resp<V, L, trim>(so.op, so.kind, resp_s + k * 4 * L, load, r, sc, WP, l, c, C, nv,
+                                         c * WP + l, so.keep);
             if constexpr (ACC) {
                 accumulate<V, L, 1>(so, acc, r, nv, tile_at);
                 if (so.flush && live) flush_yz<T, V, L, true>(flush_args(so), acc, obase, ostride, nv);
@@ -1089,7 +1141,8 @@ __global__ void __launch_bounds__(512, 1)
             // the previous operator's row copies must have read the staging
             // rows before anyone writes them again (after this solve's barriers)
             if (t < W) bulk_wait_read_all();
-            chunk_solve_resp<T, L>(so.op, so.kind, resp_s + k * 4 * L, load, r, sc, W, l, c, C, nv, c * W + l);
+            chunk_solve_resp<T, L, !ACC>(so.op, so.kind, resp_s + k * 4 * L, load, r, sc, W, l, c, C, nv, c * W + l,
+                                         so.keep);
             if constexpr (ACC) {
                 accumulate<T, L, V>(so, acc, r, nv, tile_at);
                 if (so.flush) flush_x_staged<T, L, true>(flush_args(so), acc, out_s, l, l0, rows, pitch, n, cs, nv);
@@ -1142,8 +1195,11 @@ static unsigned persistent_grid(x3d_ctx_s *ctx, Kern kern, int threads, size_t s
 // Carry responses of chunk_solve_resp for chunk length L on lines of n
 // points: h_j = rho^(j+1) sum_{i < len-j} rho^(2i) and g_j = rho^(len-j),
 // len = L (resp[0..1]) and len = the last chunk's length (resp[2..3]).
+// Returns chunk_solve_resp's keep for full chunks: nh | ng << 8, the counts
+// of leading h and trailing g entries above 2^-32 (FP32) or 2^-62 (FP64) of
+// the largest, rounded up to whole blocks of 8.
 template <typename T>
-static void fill_op_resp(T (&resp)[4][kChunkLong<T>], double al, int L, int n)
+static int fill_op_resp(T (&resp)[4][kChunkLong<T>], double al, int L, int n)
 {
     const int C = (n + L - 1) / L, last = n - (C - 1) * L;
     const double rho = al == 0.0 ? 0.0 : -2.0 * al / (1.0 + std::sqrt(1.0 - 4.0 * al * al));
@@ -1165,17 +1221,34 @@ static void fill_op_resp(T (&resp)[4][kChunkLong<T>], double al, int L, int n)
     };
     fill(resp[0], resp[1], L);
     fill(resp[2], resp[3], last);
+    const double thr = sizeof(T) == 4 ? std::ldexp(1.0, -32) : std::ldexp(1.0, -62);
+    double hmax = 0.0, gmax = 0.0;
+    for (int j = 0; j < L; ++j) {
+        hmax = std::max(hmax, std::fabs((double)resp[0][j]));
+        gmax = std::max(gmax, std::fabs((double)resp[1][j]));
+    }
+    int nh = 0, ng = 0;
+    for (int j = 0; j < L; ++j)
+        if (std::fabs((double)resp[0][j]) > thr * hmax) nh = j + 1;
+    for (int j = L - 1; j >= 0; --j)
+        if (std::fabs((double)resp[1][j]) > thr * gmax) ng = L - j;
+    const int b = L < 8 ? L : 8;
+    nh = std::min(L, (nh + b - 1) / b * b);
+    ng = std::min(L, (ng + b - 1) / b * b);
+    return nh | ng << 8;
 }
 
 template <typename T>
 static void fill_resp(StageProgram<T> &p, int L, int n)
 {
-    for (int k = 0; k < p.nops; ++k) fill_op_resp(p.ops[k].resp, p.ops[k].op.alfa, L, n);
+    for (int k = 0; k < p.nops; ++k) p.ops[k].keep = fill_op_resp(p.ops[k].resp, p.ops[k].op.alfa, L, n);
 }
 
-// PR = 2: the paired y/z kernel (FP32 only).  Persistent kernels claim their
-// tiles from the context's counter, zeroed here before each launch.
-template <typename T, int W, int L, bool PERSIST, int PR = 1>
+// PR = 2: the paired y/z kernel (FP32 only).  OCC > 1: the y/z kernel built
+// for OCC CTAs per SM (plain programs, at most 256 threads).  Persistent
+// kernels claim their tiles from the context's counter, zeroed here before
+// each launch.
+template <typename T, int W, int L, bool PERSIST, int PR = 1, int OCC = 1>
 static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog_in, int dir, int nx, int ny,
                             int nz)
 {
@@ -1211,6 +1284,7 @@ static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog_in, int 
         const int C = (n + L - 1) / L;
         const int threads = C * W / PR;
         if (threads > kStageThreads<T, L, PR> || threads % 32) return X3D_EUNSUPPORTED;
+        if (OCC > 1 && (acc || dir == DX || threads > 256)) return X3D_EUNSUPPORTED;
         const size_t resp_bytes = (size_t)prog.nops * 4 * L * es * PR;
         for (int ti = 0; ti < prog.ntiles; ++ti)
             if (!al16(prog.in[ti])) return X3D_EUNSUPPORTED;
@@ -1295,7 +1369,9 @@ static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog_in, int 
         prog.prefetch_mask = 0;
         for (int k = 0; k < prog.nops; ++k)
             if (prog.ops[k].prefetch_base) prog.prefetch_mask |= 1 << k;
-        auto kern = acc ? ls_stage_yz<T, W, L, true, PERSIST, PR> : ls_stage_yz<T, W, L, false, PERSIST, PR>;
+        auto kern = ls_stage_yz<T, W, L, false, PERSIST, PR, OCC>;
+        if constexpr (OCC == 1)  // the OCC > 1 kernels take plain programs only
+            if (acc) kern = ls_stage_yz<T, W, L, true, PERSIST, PR, OCC>;
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         const long tiles_x = (nx + W - 1) / W;
         const long ntiles = tiles_x * (dir == DY ? nz : ny);
@@ -1314,7 +1390,18 @@ static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog_in, int 
 }
 
 template <typename T>
+static int launch_stage_sel(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir, int nx, int ny, int nz, int cfg);
+
+template <typename T>
 int launch_stage(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir, int nx, int ny, int nz, int cfg)
+{
+    const int rc = launch_stage_sel<T>(ctx, prog, dir, nx, ny, nz, cfg);
+    if (rc == X3D_OK) ctx->last_cfg = cfg;
+    return rc;
+}
+
+template <typename T>
+static int launch_stage_sel(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir, int nx, int ny, int nz, int cfg)
 {
     if (prog.nops < 1 || prog.nops > kMaxStageOps || prog.ntiles < 1 || prog.ntiles > kMaxStageTiles)
         return X3D_EINVAL;
@@ -1340,6 +1427,8 @@ int launch_stage(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir, int nx, i
     case 13: return launch_stage_cfg<T, 16, Lsmall, true, 2>(ctx, prog, dir, nx, ny, nz);
     case 14: return launch_stage_cfg<T, 32, Lsmall, false, 2>(ctx, prog, dir, nx, ny, nz);
     case 15: return launch_stage_cfg<T, 32, Lbig, true, 2>(ctx, prog, dir, nx, ny, nz);
+    // 17: configuration 6 (y/z) compiled for three CTAs per SM (plain programs)
+    case 17: return launch_stage_cfg<T, 16, Lbig, true, 1, 3>(ctx, prog, dir, nx, ny, nz);
     default: return X3D_EUNSUPPORTED;
     }
 }
@@ -1504,7 +1593,8 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
                 }
             };
             for (int k = 0; k < J.nops; ++k) {
-                chunk_solve_resp<T, L>(J.op[k], J.kind[k], resp_s + k * 4 * L, load, r, sc, W, l, c, C, nv, q);
+                chunk_solve_resp<T, L, true>(J.op[k], J.kind[k], resp_s + k * 4 * L, load, r, sc, W, l, c, C, nv,
+                                             q, J.keep[k]);
                 if (active && l < rows) {
                     T *dst = J.out[k] + (size_t)(l0 + l) * n + cs;
 #pragma unroll
@@ -1533,7 +1623,8 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
                                  (dir == DY ? (size_t)J.nx * J.ny * o : (size_t)J.nx * o) +
                                  (size_t)cs * ostride;
             for (int k = 0; k < J.nops; ++k) {
-                chunk_solve_resp<T, L>(J.op[k], J.kind[k], resp_s + k * 4 * L, load, r, sc, W, l, c, C, nv, q);
+                chunk_solve_resp<T, L, true>(J.op[k], J.kind[k], resp_s + k * 4 * L, load, r, sc, W, l, c, C, nv,
+                                             q, J.keep[k]);
                 if (live) {
                     T *dst = J.out[k] + obase;
 #pragma unroll
@@ -1559,7 +1650,7 @@ bool plan_batch_job(BatchJob<T> &J, int L, size_t *tile_bytes)
     constexpr int V = Vec4<T>::N;
     for (int k = 0; k < J.nops; ++k)
         if (!J.op[k].circ || J.op[k].n != n) return false;
-    for (int k = 0; k < J.nops; ++k) fill_op_resp(J.resp[k], J.op[k].alfa, L, n);
+    for (int k = 0; k < J.nops; ++k) J.keep[k] = fill_op_resp(J.resp[k], J.op[k].alfa, L, n);
     J.C = (n + L - 1) / L;
     if (J.C > kBatchThreads) return false;
     int W = kBatchThreads / J.C;

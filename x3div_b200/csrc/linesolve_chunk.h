@@ -36,6 +36,9 @@ struct StageOp {
     // the tile's inputs are requested.
     short base2_tile;
     short prefetch_base;
+    // Set by launch_stage: the response entries the fixes of a full chunk
+    // use (see chunk_solve_resp).
+    int keep;
     // Responses of a chunk's solved values to its carries, for the launch's
     // chunk length L (set by launch_stage): y_j = y_j(local) + F resp[0][j]
     // + B resp[1][j] for a full chunk, resp[2], resp[3] for a short last
@@ -54,11 +57,15 @@ struct StageProgram {
 };
 
 // Number of (lines per CTA, chunk length, persistence, lines per thread)
-// configurations launch_stage knows.
+// configurations launch_stage knows in 0 .. 15; 16 is the one-thread-per-line
+// kernel (not a launch_stage configuration); 17 is configuration 6 compiled
+// for three CTAs per SM.  kAllConfigs counts every configuration the
+// dispatch tries.
 constexpr int kChunkConfigs = 16;
+constexpr int kAllConfigs = 18;
+inline bool is_stage_cfg(int cfg) { return (cfg >= 0 && cfg < kChunkConfigs) || cfg == 17; }
 
-// Launches the chunked stage kernel with configuration cfg in
-// [0, kChunkConfigs).  Returns X3D_EUNSUPPORTED, launching nothing, when the
+// Launches the chunked stage kernel with configuration cfg (is_stage_cfg).  Returns X3D_EUNSUPPORTED, launching nothing, when the
 // shape, alignment or shared-memory budget rules that configuration out.
 template <typename T>
 int launch_stage(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir, int nx, int ny, int nz,
@@ -83,8 +90,9 @@ struct BatchJob {
     long tile0;  // first work item of the job
     long ntiles;
     // carry responses of each operator for the batch's chunk length (as
-    // StageOp::resp; set by plan_batch_job)
+    // StageOp::resp and StageOp::keep; set by plan_batch_job)
     T resp[kMaxStageOps][4][kChunkLong<T>];
+    int keep[kMaxStageOps];
 };
 
 // Chooses tiling for the job (chunk length L) and encodes its tensor map;

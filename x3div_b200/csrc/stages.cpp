@@ -72,7 +72,8 @@ static int tune_stage(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir, cons
     cudaEventCreate(&b);
     int best = -1, rc = X3D_OK;
     float bt = 0.f;
-    for (int cfg = 0; cfg < kChunkConfigs; ++cfg) {
+    for (int cfg = 0; cfg < kAllConfigs; ++cfg) {
+        if (!is_stage_cfg(cfg)) continue;
         rc = launch_stage<T>(ctx, prog, dir, ctx->nx, ctx->ny, ctx->nz, cfg);
         if (rc == X3D_EUNSUPPORTED) continue;
         if (rc) break;
@@ -110,10 +111,10 @@ static int run_program(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir, con
     if (ctx->stage_tuning) return tune_stage<T>(ctx, prog, dir, name.c_str());
     const auto it = ctx->stage_tuned.find(name);
     const int first = it != ctx->stage_tuned.end() ? it->second
-                                                   : (ctx->default_cfg < kChunkConfigs ? ctx->default_cfg : 0);
+                                                   : (is_stage_cfg(ctx->default_cfg) ? ctx->default_cfg : 0);
     int rc = launch_stage<T>(ctx, prog, dir, ctx->nx, ctx->ny, ctx->nz, first);
-    for (int cfg = 0; rc == X3D_EUNSUPPORTED && cfg < kChunkConfigs; ++cfg)
-        if (cfg != first) rc = launch_stage<T>(ctx, prog, dir, ctx->nx, ctx->ny, ctx->nz, cfg);
+    for (int cfg = 0; rc == X3D_EUNSUPPORTED && cfg < kAllConfigs; ++cfg)
+        if (cfg != first && is_stage_cfg(cfg)) rc = launch_stage<T>(ctx, prog, dir, ctx->nx, ctx->ny, ctx->nz, cfg);
     return rc;
 }
 

@@ -151,6 +151,7 @@ struct x3d_ctx_s {
     bool stage_tuning = false;
     int default_cfg = 0;
     unsigned long long launches = 0;  // kernels of this library launched on the context
+    int last_cfg = -1;                // configuration of the last line-solve launch (x3d_ctx_last_kernel)
     size_t elem() const { return precision == X3D_F32 ? 4 : 8; }
     size_t npts() const { return (size_t)nx * ny * nz; }
 };
