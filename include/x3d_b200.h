@@ -152,7 +152,9 @@ int x3d_ctx_selftest_timeout(x3d_ctx ctx, double limit_s);
  * with each store of the CTA on consecutive rows; pattern 4: pattern 1 with
  * consecutive tiles on different z planes; pattern 5: pattern 1 with the
  * tiles claimed in order from a counter, as the persistent stage kernels
- * take them (w in {8, 16, 32}); nx % w == 0, ny a multiple of the rows a
+ * take them (w in {8, 16, 32}); pattern 6: pattern 5 in the z stage
+ * kernels' order (tiles of w columns of one y row over all nz planes);
+ * nx % w == 0, ny a multiple of the rows a
  * thread moves (32, or 16 for w = 128) and of the block), so that timing it
  * gives the
  * bandwidth that traffic mix and access order can reach.  ctas_per_sm sets

@@ -476,7 +476,7 @@ int x3d_roofline_probe(x3d_ctx ctx, int pattern, int w, int ctas_per_sm, const v
 {
     int rc = check_ctx(ctx);
     if (rc) return rc;
-    if (!in || !outs || nx < 1 || ny < 1 || nz < 1 || pattern < 0 || pattern > 5)
+    if (!in || !outs || nx < 1 || ny < 1 || nz < 1 || pattern < 0 || pattern > 6)
         return set_error(ctx, X3D_EINVAL, "bad probe request");
     float *o[6];
     for (int k = 0; k < 6; ++k) {

@@ -111,7 +111,9 @@ static int probe_w(x3d_ctx_s *ctx, int w, int per_sm, const float *in, const Out
 // (one atomicAdd per tile) instead of at a fixed stride, as the persistent
 // stage kernels take them, so the tiles in flight stay a window of
 // consecutive tiles.
-template <int W>
+// Pattern 6: the same for the z stage kernels' order: tiles of W columns of
+// one y row over every z plane (rows nx ny apart), x tiles fastest.
+template <int W, bool ZLINES>
 __global__ void k_probe_tile_claim(const float *__restrict__ in, const Outs6 outs, int nx, int ny, int nz,
                                    unsigned long long *counter)
 {
@@ -119,7 +121,9 @@ __global__ void k_probe_tile_claim(const float *__restrict__ in, const Outs6 out
     __shared__ long s_tile;
     const int t = threadIdx.x, l = t % W, c = t / W;
     const int tiles_x = nx / W;
-    const long ntiles = (long)tiles_x * nz;
+    const long ntiles = (long)tiles_x * (ZLINES ? ny : nz);
+    const size_t rs = ZLINES ? (size_t)nx * ny : (size_t)nx;  // elements between rows of a tile
+    const size_t os = ZLINES ? (size_t)nx : (size_t)nx * ny;  // between tiles' planes (y rows)
     for (;;) {
         if (t == 0) s_tile = (long)atomicAdd(counter, 1ull);
         __syncthreads();
@@ -127,15 +131,15 @@ __global__ void k_probe_tile_claim(const float *__restrict__ in, const Outs6 out
         __syncthreads();
         if (tile >= ntiles) break;
         const int x0 = (int)(tile % tiles_x) * W, o = (int)(tile / tiles_x);
-        const size_t base = (size_t)o * nx * ny + (size_t)c * RT * nx + x0 + l;
+        const size_t base = (size_t)o * os + (size_t)c * RT * rs + x0 + l;
         float r[RT];
 #pragma unroll
-        for (int j = 0; j < RT; ++j) r[j] = in[base + (size_t)j * nx];
+        for (int j = 0; j < RT; ++j) r[j] = in[base + (size_t)j * rs];
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
             float *dst = outs.p[k] + base;
 #pragma unroll
-            for (int j = 0; j < RT; ++j) dst[(size_t)j * nx] = r[j];
+            for (int j = 0; j < RT; ++j) dst[(size_t)j * rs] = r[j];
         }
     }
 }
@@ -157,21 +161,27 @@ int launch_roofline_probe(x3d_ctx_s *ctx, int pattern, int w, int ctas_per_sm, c
     // 1: whole columns (rows = ny); 2: blocks of 128 rows; 3: whole
     // columns, banded rows; 4: whole columns, tiles z plane first
     const int rows = pattern == 2 ? 128 : ny;
-    if (nx % w || ny % rows || pattern > 5)
+    if (nx % w || ny % rows || pattern > 6)
         return set_error(ctx, X3D_EINVAL, "tile probe needs nx % w == 0 and ny % rows == 0");
-    if (pattern == 5) {
-        const int threads = w * (ny / 32);
-        if ((w != 8 && w != 16 && w != 32) || ny % 32 || threads > 512 || threads % 32)
-            return set_error(ctx, X3D_EINVAL, "tile probe pattern 5: w 8, 16 or 32, ny % 32 == 0");
+    if (pattern == 5 || pattern == 6) {
+        const int rows = pattern == 5 ? ny : nz;
+        const int threads = w * (rows / 32);
+        if ((w != 8 && w != 16 && w != 32) || nx % w || rows % 32 || threads > 512 || threads % 32)
+            return set_error(ctx, X3D_EINVAL, "tile probe patterns 5, 6: w 8, 16 or 32, line length % 32 == 0");
         auto *counter = ctx->d_claim;
         if (cudaMemsetAsync(counter, 0, sizeof(*counter), ctx->stream) != cudaSuccess)
             return set_error(ctx, X3D_ECUDA, "probe counter reset");
         const unsigned grid = (unsigned)(ctx->num_sms * per_sm);
-        ++ctx->launches;
-        if (w == 8) k_probe_tile_claim<8><<<grid, threads, 0, ctx->stream>>>(in, o, nx, ny, nz, counter);
-        else if (w == 16) k_probe_tile_claim<16><<<grid, threads, 0, ctx->stream>>>(in, o, nx, ny, nz, counter);
-        else k_probe_tile_claim<32><<<grid, threads, 0, ctx->stream>>>(in, o, nx, ny, nz, counter);
-        return cuda_check(ctx, cudaGetLastError(), "k_probe_tile_claim launch");
+        auto go = [&](auto kern) {
+            ++ctx->launches;
+            kern<<<grid, threads, 0, ctx->stream>>>(in, o, nx, ny, nz, counter);
+            return cuda_check(ctx, cudaGetLastError(), "k_probe_tile_claim launch");
+        };
+        if (pattern == 5)
+            return w == 8 ? go(k_probe_tile_claim<8, false>)
+                          : (w == 16 ? go(k_probe_tile_claim<16, false>) : go(k_probe_tile_claim<32, false>));
+        return w == 8 ? go(k_probe_tile_claim<8, true>)
+                      : (w == 16 ? go(k_probe_tile_claim<16, true>) : go(k_probe_tile_claim<32, true>));
     }
     if (pattern == 3) return probe_w<true, false>(ctx, w, per_sm, in, o, nx, ny, nz, rows);
     if (pattern == 4) return probe_w<false, true>(ctx, w, per_sm, in, o, nx, ny, nz, rows);
