@@ -421,7 +421,9 @@ def run_c5(torch, n=768, steps=20, dt=5e-4, seed=5):
 def run_b48(args, world, rank, local, torch):
     """The batching workload: 48 seeded uneven periodic boxes (this rank's LPT
     share), 3 FP32 fields each (Taylor-Green + N(0, (1e-2)^2)), all 54 operator
-    applications per box in one persistent launch, replayed from a CUDA graph."""
+    applications per box in one persistent launch, its chunk length and tile
+    width tuned per box shape and direction (x3d_batch_autotune), replayed
+    from a CUDA graph."""
     from x3div_b200 import Batch, b48_boxes, box_points, shard_boxes
     boxes = b48_boxes(count=args.b48_count)
     mine = shard_boxes(boxes, world)[rank]
@@ -445,7 +447,14 @@ def run_b48(args, world, rank, local, torch):
         outs.append([[[torch.empty_like(fs[0]) for _ in range(6)] for _ in range(3)] for _ in range(3)])
     batch = Batch(my, precision="f32", device=local, stream=torch.cuda.current_stream())
     batch.bind_sweep(fields, outs)
+    batch.autotune()
     info = batch.info()
+    # per box shape: (chunk length, lines per tile) along x, y, z
+    choices = {}
+    for k, b in enumerate(my):
+        key = "x".join(str(v) for v in b[:3])
+        if key not in choices:
+            choices[key] = [list(batch.choice(k, d)) for d in range(3)]
     batch.capture()
     for _ in range(args.warmup):
         batch.replay()
@@ -475,6 +484,7 @@ def run_b48(args, world, rank, local, torch):
            "jobs_in_persistent_launch": info["jobs"], "fallback_jobs": info["fallback_jobs"],
            "launches_per_step": (1 if info["jobs"] else 0) + info["fallback_jobs"],
            "cuda_graph": True,
+           "tuned_per_shape_chunk_and_lines_xyz": choices,
            "bytes_per_step": int(tot_points / 6 * 4 * (1 + 6))}
     batch.close()
     del fields, outs

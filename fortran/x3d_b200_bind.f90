@@ -477,6 +477,19 @@ module x3d_b200_bind
        integer(c_int) :: jobs
        integer(c_int) :: fallback_jobs
      end function
+     integer(c_int) function x3d_batch_autotune(batch) bind(C, name="x3d_batch_autotune")
+       import :: c_ptr, c_int
+       type(c_ptr), value :: batch
+     end function
+     integer(c_int) function x3d_batch_choice(batch, box, dir, chunk, lines) bind(C, &
+          name="x3d_batch_choice")
+       import :: c_ptr, c_int
+       type(c_ptr), value :: batch
+       integer(c_int), value :: box
+       integer(c_int), value :: dir
+       integer(c_int) :: chunk
+       integer(c_int) :: lines
+     end function
      integer(c_int) function x3d_xthomas(ctx, tt, ff, fs, fw, perio, alfa, nx, ny, nz) bind(C, &
           name="x3d_xthomas")
        import :: c_ptr, c_int, c_double

@@ -320,6 +320,22 @@ int x3d_batch_sync(x3d_batch batch);
 /* points = operator-application points per run; tiles, jobs in the
  * persistent launch; fallback_jobs run as grouped launches. */
 int x3d_batch_info(x3d_batch batch, long long *points, long long *tiles, int *jobs, int *fallback_jobs);
+/* Tunes the bound sweep per box shape: for each distinct shape and
+ * direction, times the persistent kernel on that shape's jobs with the long
+ * and the short chunk length, each with as many lines per tile as its
+ * threads allow and with half as many (x jobs also with their outputs
+ * staged in shared memory and sent as row copies), keeps the fastest, then
+ * times the whole work-list with those choices, with them but no staging,
+ * with only the long-chunk choices' tile widths, and with the defaults, and
+ * keeps the fastest of the four (a shape timed alone can mislead: in the
+ * whole launch the largest tile sizes every CTA).  Overwrites the bound
+ * outputs; synchronous; not during stream capture.  No reference
+ * counterpart. */
+int x3d_batch_autotune(x3d_batch batch);
+/* The chunk length and lines per tile the jobs of box `box` along `dir`
+ * run with (*lines = 0 for jobs that run outside the persistent launch).
+ * No reference counterpart. */
+int x3d_batch_choice(x3d_batch batch, int box, int dir, int *chunk, int *lines);
 
 /* ---- batched Thomas line solves: module thomas (src/thomas.f90:15-28) --- */
 

@@ -56,3 +56,53 @@ def test_batch_sweep_matches_oracle(oracle, torch_cuda, prec):
     batch.sync()
     check()
     batch.close()
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_batch_autotune_keeps_results(oracle, torch_cuda, prec):
+    """x3d_batch_autotune picks a chunk length and tile width per box shape
+    and direction (x3d_batch_choice reports them); the re-planned persistent
+    launch still matches the oracle, plainly and from its CUDA graph."""
+    torch = torch_cuda
+    from x3div_b200 import Batch, to_device, to_host
+    dt = torch.float32 if prec == "f32" else torch.float64
+    tol = 1e-5 if prec == "f32" else 1e-12
+    boxes = [(16, 16, 16), (24, 20, 12), (64, 40, 24), (16, 16, 16), (96, 36, 20)]
+    fields, outs, used = [], [], []
+    for i, b in enumerate(boxes):
+        fs = [to_device(seeded_field(b, 300 + 10 * i + f, noise=1e-2), dt) for f in range(2)]
+        fields.append(fs)
+        used.append([to_host(a).astype(np.float64) for a in fs])
+        outs.append([[[torch.full_like(fs[0], np.nan) for _ in range(6)] for _ in range(3)] for _ in range(2)])
+    batch = Batch(boxes, precision=prec)
+    batch.bind_sweep(fields, outs)
+    batch.autotune()
+    long_chunk, short_chunk = (32, 16) if prec == "f32" else (16, 8)
+    for i in range(len(boxes)):
+        for d in range(3):
+            chunk, lines = batch.choice(i, d)
+            assert chunk in (long_chunk, short_chunk) and lines > 0, (boxes[i], d, chunk, lines)
+    assert batch.choice(0, 1) == batch.choice(3, 1)  # one choice per shape
+
+    def check():
+        for i, b in enumerate(boxes):
+            h = [2 * np.pi / n for n in b]
+            for f in range(2):
+                for d in range(3):
+                    for k, kind in enumerate(KINDS):
+                        err = rel_err(to_host(outs[i][f][d][k]), oracle.apply(kind, d, used[i][f], h[d]))
+                        assert err < tol, (b, f, d, kind, err)
+
+    for per_box in outs:
+        for per_f in per_box:
+            for per_d in per_f:
+                for o in per_d:
+                    o.fill_(np.nan)
+    batch.run()
+    batch.sync()
+    check()
+    batch.capture()
+    batch.replay()
+    batch.sync()
+    check()
+    batch.close()

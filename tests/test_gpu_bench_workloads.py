@@ -138,6 +138,7 @@ def test_b48_every_box_shape(oracle, torch_cuda):
                      for _ in range(3)])
     batch = Batch(B48_SHAPES, precision="f32")
     batch.bind_sweep(fields, outs)
+    batch.autotune()  # as the bench does: chunk length and tile width per shape
     info = batch.info()
     assert info["fallback_jobs"] == 0  # every job in the one persistent launch
     assert info["points"] == 54 * sum(b[0] * b[1] * b[2] for b in B48_SHAPES)
@@ -167,5 +168,6 @@ def test_b48_every_box_shape(oracle, torch_cuda):
     batch.replay()
     batch.sync()
     w2 = check()
-    print(f"\nB48 shapes {B48_SHAPES}: max error {w1:.3e} (run), {w2:.3e} (graph replay), {info}")
+    choices = {b: [batch.choice(i, d) for d in range(3)] for i, b in enumerate(B48_SHAPES)}
+    print(f"\nB48 shapes: max error {w1:.3e} (run), {w2:.3e} (graph replay), {info}, tuned {choices}")
     batch.close()

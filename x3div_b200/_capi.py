@@ -87,6 +87,8 @@ SIGNATURES = {
     "x3d_batch_replay": [_vp],
     "x3d_batch_sync": [_vp],
     "x3d_batch_info": [_vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong), _ip, _ip],
+    "x3d_batch_autotune": [_vp],
+    "x3d_batch_choice": [_vp, _i, _i, _ip, _ip],
     "x3d_xthomas": [_vp, _vp, _vp, _vp, _vp, _vp, _d, _i, _i, _i],
     "x3d_ythomas": [_vp, _vp, _vp, _vp, _vp, _vp, _d, _i, _i, _i],
     "x3d_zthomas": [_vp, _vp, _vp, _vp, _vp, _vp, _d, _i, _i, _i],

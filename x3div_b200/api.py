@@ -500,6 +500,17 @@ class Batch:
                                           ctypes.byref(fb)))
         return dict(points=p.value, tiles=t.value, jobs=j.value, fallback_jobs=fb.value)
 
+    def autotune(self):
+        """x3d_batch_autotune: per box shape and direction, the fastest chunk
+        length and tile width (overwrites the bound outputs)."""
+        self._check(self.L.x3d_batch_autotune(self.handle))
+
+    def choice(self, box, direction):
+        """x3d_batch_choice: (chunk length, lines per tile) of box's jobs along direction."""
+        c, w = ctypes.c_int(), ctypes.c_int()
+        self._check(self.L.x3d_batch_choice(self.handle, int(box), int(direction), ctypes.byref(c), ctypes.byref(w)))
+        return c.value, w.value
+
     def close(self):
         if getattr(self, "handle", None):
             self.L.x3d_batch_destroy(self.handle)

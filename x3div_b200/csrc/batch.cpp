@@ -33,6 +33,7 @@ struct x3d_batch_s {
     int njobs = 0;
     long total_tiles = 0;
     size_t tile_cap = 0;
+    int variant = 0;  // the batch kernel's variant the job list needs (BatchVariant)
     int grid = 0;
     // jobs the persistent kernel cannot take run as per-box grouped launches
     struct Fallback {
@@ -45,6 +46,13 @@ struct x3d_batch_s {
     };
     std::vector<Fallback> fallback;
     long long points = 0;  // operator-application points per run
+    // the bound sweep (x3d_batch_bind_sweep), kept for x3d_batch_autotune
+    int nfields = 0, nops = 0;
+    std::vector<void *> fields, outs;
+    // per (box shape, direction): chunk length (0: the long one) and the
+    // most lines per tile (0: as many as the threads allow), set by
+    // x3d_batch_autotune; and the lines per tile each shape's jobs got
+    std::vector<int> choice_L, choice_W, choice_X, planned_W;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
     std::string last_error;
@@ -71,21 +79,34 @@ const LineOp<double> &lop<double>(const x3d_op_s *op)
     return op->opd;
 }
 
+// The work-list of the bound sweep: every (box, field, direction) job, or
+// only those of box shape `shape` and direction `dir` (>= 0), each planned
+// with its shape and direction's choice of chunk length and tile width, or
+// with (L, w_req) where L > 0.  Jobs the kernel cannot take go to the
+// fallback list (for the whole work-list only).
 template <typename T>
-int bind_typed(x3d_batch_s *b, int nfields, void *const *fields, void *const *outs, int nops_per_dir)
+int make_jobs(x3d_batch_s *b, std::vector<BatchJob<T>> &jobs, size_t *tile_cap_out, long *tiles_out,
+              int shape, int dir, int L_force, int w_force, int x_force = 0)
 {
-    std::vector<BatchJob<T>> jobs;
-    b->fallback.clear();
-    b->points = 0;
+    const int nfields = b->nfields, nops_per_dir = b->nops;
+    void *const *fields = b->fields.data();
+    void *const *outs = b->outs.data();
+    const bool whole = shape < 0;
+    if (whole) {
+        b->fallback.clear();
+        b->points = 0;
+    }
     size_t tile_cap = 0;
     long tiles = 0;
     const int kinds[6] = {DER, DER2, DERVP, DERPV, INTVP, INTPV};
     for (size_t i = 0; i < b->boxes.size(); ++i) {
+        if (!whole && b->box_shape[i] != shape) continue;
         x3d_ctx_s *ctx = b->shape_ctx[b->box_shape[i]];
         const int dims[3] = {ctx->nx, ctx->ny, ctx->nz};
         for (int f = 0; f < nfields; ++f) {
             const void *in = fields[i * nfields + f];
             for (int d = 0; d < 3; ++d) {
+                if (!whole && d != dir) continue;
                 BatchJob<T> J;
                 std::memset(&J, 0, sizeof(J));
                 J.in = static_cast<const T *>(in);
@@ -114,22 +135,40 @@ int bind_typed(x3d_batch_s *b, int nfields, void *const *fields, void *const *ou
                     fb.kinds[k] = kinds[k];
                     fb.outs[k] = J.out[k];
                 }
-                b->points += (long long)nops_per_dir * dims[0] * dims[1] * dims[2];
+                if (whole) b->points += (long long)nops_per_dir * dims[0] * dims[1] * dims[2];
+                const int sd = b->box_shape[i] * 3 + d;
+                const int L = L_force > 0 ? L_force : (b->choice_L[sd] > 0 ? b->choice_L[sd] : kChunkLong<T>);
+                const int w = L_force > 0 ? w_force : b->choice_W[sd];
+                const int xs = L_force > 0 ? x_force : b->choice_X[sd];
                 size_t tb = 0;
-                if (plan_batch_job<T>(J, kChunkLong<T>, &tb)) {
+                if (plan_batch_job<T>(J, L, w, xs, &tb)) {
                     J.tile0 = tiles;
                     tiles += J.ntiles;
                     tile_cap = std::max(tile_cap, tb);
                     jobs.push_back(J);
-                } else {
+                    if (whole) b->planned_W[sd] = J.W;
+                } else if (whole) {
                     b->fallback.push_back(fb);
                 }
             }
         }
     }
+    *tile_cap_out = tile_cap;
+    *tiles_out = tiles;
+    return X3D_OK;
+}
+
+template <typename T>
+int bind_typed(x3d_batch_s *b)
+{
+    std::vector<BatchJob<T>> jobs;
+    size_t tile_cap = 0;
+    long tiles = 0;
+    make_jobs<T>(b, jobs, &tile_cap, &tiles, -1, -1, 0, 0);
     b->njobs = (int)jobs.size();
     b->total_tiles = tiles;
     b->tile_cap = tile_cap;
+    b->variant = batch_variant<T>(jobs.data(), (int)jobs.size());
     if (!jobs.empty()) {
         const size_t bytes = jobs.size() * sizeof(BatchJob<T>);
         if (bytes > b->jobs_cap) {
@@ -141,7 +180,7 @@ int bind_typed(x3d_batch_s *b, int nfields, void *const *fields, void *const *ou
         }
         if (cudaMemcpy(b->d_jobs, jobs.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess)
             return bfail(b, X3D_ECUDA, "job list upload failed");
-        const int rc = prepare_batch<T>(tile_cap, b->smem_optin, b->num_sms, &b->grid);
+        const int rc = prepare_batch<T>(tile_cap, b->variant, b->smem_optin, b->num_sms, &b->grid);
         if (rc) {
             b->njobs = 0;
             b->total_tiles = 0;
@@ -156,7 +195,7 @@ int run_typed(x3d_batch_s *b)
 {
     if (b->njobs > 0) {
         const int rc = launch_batch<T>(b->stream, b->grid, static_cast<const BatchJob<T> *>(b->d_jobs), b->njobs,
-                                       b->total_tiles, b->d_counter, b->tile_cap, b->d_err);
+                                       b->total_tiles, b->d_counter, b->tile_cap, b->variant, b->d_err);
         if (rc) return bfail(b, rc, std::string("batch launch failed: ") + cudaGetErrorString(cudaGetLastError()));
     }
     for (auto &fb : b->fallback) {
@@ -177,6 +216,150 @@ void drop_graph(x3d_batch_s *b)
     if (b->graph) cudaGraphDestroy(b->graph);
     b->gexec = nullptr;
     b->graph = nullptr;
+}
+
+}  // namespace
+
+namespace {
+
+// Times the batch kernel on the jobs of one box shape and direction with
+// each candidate and keeps the fastest: the long and the short chunk, each
+// with as many lines per tile as the threads allow and with half as many,
+// and for x jobs each with outputs straight out and staged in shared memory.
+template <typename T>
+int autotune_typed(x3d_batch_s *b)
+{
+    const int nshapes = (int)b->shape_ctx.size();
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    void *d_tmp = nullptr;
+    size_t tmp_cap = 0;
+    int rc = X3D_OK;
+    for (int sh = 0; sh < nshapes && !rc; ++sh)
+        for (int d = 0; d < 3 && !rc; ++d) {
+            float best = -1.f;
+            int bestL = 0, bestW = 0, bestX = 0;
+            const int Ls[2] = {kChunkLong<T>, kChunkShort<T>};
+            for (int cand = 0; cand < (d == 0 ? 8 : 4) && !rc; ++cand) {
+                    const int li = cand & 1, half = (cand >> 1) & 1, xs = cand >> 2;
+                    std::vector<BatchJob<T>> jobs;
+                    size_t cap = 0;
+                    long tiles = 0;
+                    // the widest tile first, to learn the width to halve
+                    int w = 0;
+                    if (half) {
+                        std::vector<BatchJob<T>> probe;
+                        make_jobs<T>(b, probe, &cap, &tiles, sh, d, Ls[li], 0);
+                        if (probe.empty()) continue;
+                        w = probe[0].W / 2;
+                        if (w < (int)(16 / sizeof(T))) continue;
+                    }
+                    make_jobs<T>(b, jobs, &cap, &tiles, sh, d, Ls[li], w, xs);
+                    if (jobs.empty()) continue;
+                    const size_t bytes = jobs.size() * sizeof(BatchJob<T>);
+                    if (bytes > tmp_cap) {
+                        if (d_tmp) cudaFree(d_tmp);
+                        d_tmp = nullptr;
+                        if (cudaMalloc(&d_tmp, bytes) != cudaSuccess) {
+                            rc = bfail(b, X3D_ENOMEM, "autotune job list allocation failed");
+                            break;
+                        }
+                        tmp_cap = bytes;
+                    }
+                    if (cudaMemcpy(d_tmp, jobs.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+                        rc = bfail(b, X3D_ECUDA, "autotune job list upload failed");
+                        break;
+                    }
+                    int grid = 0;
+                    const int var = batch_variant<T>(jobs.data(), (int)jobs.size());
+                    if (prepare_batch<T>(cap, var, b->smem_optin, b->num_sms, &grid)) continue;
+                    auto run = [&]() {
+                        return launch_batch<T>(b->stream, grid, static_cast<const BatchJob<T> *>(d_tmp),
+                                               (int)jobs.size(), tiles, b->d_counter, cap, var, b->d_err);
+                    };
+                    if ((rc = run())) break;
+                    float ms = 0.f;
+                    for (int r = 0; r < 3 && !rc; ++r) {
+                        cudaEventRecord(e0, b->stream);
+                        rc = run();
+                        cudaEventRecord(e1, b->stream);
+                        cudaEventSynchronize(e1);
+                        float m = 0.f;
+                        cudaEventElapsedTime(&m, e0, e1);
+                        ms = r == 0 ? m : std::min(ms, m);
+                    }
+                    if (!rc && (best < 0.f || ms < best)) {
+                        best = ms;
+                        bestL = Ls[li];
+                        bestW = w;
+                        bestX = xs;
+                    }
+                }
+            if (best >= 0.f) {
+                b->choice_L[sh * 3 + d] = bestL;
+                b->choice_W[sh * 3 + d] = bestW;
+                b->choice_X[sh * 3 + d] = bestX;
+            }
+        }
+    if (d_tmp) {
+        cudaStreamSynchronize(b->stream);
+        cudaFree(d_tmp);
+    }
+    // Each shape was timed alone; in the whole launch the largest tile (and
+    // the staging rows, if any job stages) sizes every CTA, so fewer may fit
+    // an SM than in a shape's trial, and a job list with any short chunk or
+    // staged x job needs a wider kernel variant.  The whole work-list is
+    // timed with the choices; with them but no x staging; with the chosen
+    // lines per tile of the long-chunk choices only (the narrowest variant);
+    // and with the defaults.  The fastest of the four is kept.
+    auto time_whole = [&](float *ms) {
+        int r = bind_typed<T>(b);
+        if (r) return r;
+        if ((r = run_typed<T>(b))) return r;
+        for (int k = 0; k < 3 && !r; ++k) {
+            cudaEventRecord(e0, b->stream);
+            r = run_typed<T>(b);
+            cudaEventRecord(e1, b->stream);
+            cudaEventSynchronize(e1);
+            float m = 0.f;
+            cudaEventElapsedTime(&m, e0, e1);
+            *ms = k == 0 ? m : std::min(*ms, m);
+        }
+        return r;
+    };
+    if (!rc) {
+        struct Set {
+            std::vector<int> L, W, X;
+        };
+        const size_t ns = b->choice_L.size();
+        const std::vector<int> zero(ns, 0);
+        const Set tuned{b->choice_L, b->choice_W, b->choice_X};
+        Set long_only{zero, zero, zero};
+        for (size_t i = 0; i < ns; ++i)
+            if (tuned.L[i] == kChunkLong<T>) long_only.W[i] = tuned.W[i];
+        const Set sets[4] = {tuned, {tuned.L, tuned.W, zero}, long_only, {zero, zero, zero}};
+        float best = -1.f;
+        int pick = 0;
+        for (int k = 0; k < 4 && !rc; ++k) {
+            b->choice_L = sets[k].L;
+            b->choice_W = sets[k].W;
+            b->choice_X = sets[k].X;
+            float ms = 0.f;
+            rc = time_whole(&ms);
+            if (!rc && (best < 0.f || ms < best)) {
+                best = ms;
+                pick = k;
+            }
+        }
+        b->choice_L = sets[pick].L;
+        b->choice_W = sets[pick].W;
+        b->choice_X = sets[pick].X;
+        if (!rc) rc = bind_typed<T>(b);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
 }
 
 }  // namespace
@@ -218,6 +401,10 @@ int x3d_batch_create(x3d_batch *out, const x3d_box *boxes, int nboxes, int preci
         b->boxes.push_back(bx);
         b->box_shape.push_back(it->second);
     }
+    b->choice_L.assign(b->shape_ctx.size() * 3, 0);
+    b->choice_W.assign(b->shape_ctx.size() * 3, 0);
+    b->choice_X.assign(b->shape_ctx.size() * 3, 0);
+    b->planned_W.assign(b->shape_ctx.size() * 3, 0);
     if (cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc(&b->d_counter, sizeof(unsigned long long)) != cudaSuccess ||
         cudaMalloc(&b->d_err, sizeof(int)) != cudaSuccess) {
@@ -265,8 +452,36 @@ int x3d_batch_bind_sweep(x3d_batch b, int nfields, void *const *fields, void *co
     for (size_t i = 0; i < nin * 18; ++i)
         if ((int)(i % 6) < nops && !outs[i]) return bfail(b, X3D_EINVAL, "null output field");
     drop_graph(b);
-    return b->precision == X3D_F32 ? bind_typed<float>(b, nfields, fields, outs, nops)
-                                   : bind_typed<double>(b, nfields, fields, outs, nops);
+    b->nfields = nfields;
+    b->nops = nops;
+    b->fields.assign(fields, fields + nin);
+    b->outs.assign(outs, outs + nin * 18);
+    return b->precision == X3D_F32 ? bind_typed<float>(b) : bind_typed<double>(b);
+}
+
+
+int x3d_batch_autotune(x3d_batch b)
+{
+    if (!b) return X3D_EINVAL;
+    if (b->nfields < 1) return bfail(b, X3D_EINVAL, "bind a sweep before tuning it");
+    cudaSetDevice(b->device);
+    if (cudaStreamCaptureStatus st; cudaStreamIsCapturing(b->stream, &st) == cudaSuccess &&
+                                    st != cudaStreamCaptureStatusNone)
+        return bfail(b, X3D_EINVAL, "cannot autotune during stream capture");
+    drop_graph(b);
+    const int rc = b->precision == X3D_F32 ? autotune_typed<float>(b) : autotune_typed<double>(b);
+    if (rc) return rc;
+    return x3d_batch_sync(b);
+}
+
+int x3d_batch_choice(x3d_batch b, int box, int dir, int *chunk, int *lines)
+{
+    if (!b || box < 0 || box >= (int)b->boxes.size() || dir < 0 || dir > 2) return X3D_EINVAL;
+    const int sd = b->box_shape[box] * 3 + dir;
+    const bool f32 = b->precision == X3D_F32;
+    if (chunk) *chunk = b->choice_L[sd] > 0 ? b->choice_L[sd] : (f32 ? kChunkLong<float> : kChunkLong<double>);
+    if (lines) *lines = b->planned_W[sd];
+    return X3D_OK;
 }
 
 int x3d_batch_run(x3d_batch b)

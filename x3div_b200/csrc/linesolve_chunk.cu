@@ -1467,13 +1467,135 @@ StageProgram<T> plain_program(const T *in, const LineOp<T> *const *ops, const in
 // counter, so boxes of different sizes balance across the SMs; each tile
 // uses its job's lines per tile (W), chunk count (C), tensor map or padded
 // rows.  Threads beyond W*C of a job idle through its barriers.
-template <typename T, int L>
+// Carry scratch, then the carry responses of the item's operators.
+template <typename T>
+constexpr size_t batch_scratch_bytes_c()
+{
+    return (((size_t)2 * kBatchThreads * sizeof(T) + 15) & ~(size_t)15) +
+           (size_t)kMaxStageOps * 4 * kChunkLong<T> * sizeof(T);
+}
+
+// Byte offset of the x staging rows: after the two slots, the scratch and
+// the responses, 128-byte aligned.
+template <typename T>
+__host__ __device__ constexpr size_t batch_out_offset(size_t tile_cap)
+{
+    return (2 * tile_cap + batch_scratch_bytes_c<T>() + 127) & ~(size_t)127;
+}
+
+// One work item of the batch kernel with chunk length L (the job's): the
+// operators of the job solved over the staged tile and written out.  y/z
+// outputs go straight to global memory, coalesced across the tile's lines;
+// x outputs either go straight out as each thread's 16-byte vectors or, for
+// jobs with xstage set, are staged in shared-memory rows (out_s, the tile's
+// pitch) and leave as one bulk copy per row, as in ls_stage_x.
+template <typename T, int L, bool XS>
+__device__ __forceinline__ void batch_item(const BatchJob<T> &J, const T *tile, T *out_s, const T *resp_s,
+                                           const ChunkScratch<T> &scf, int t, long l0, int rows, int x0, int o)
+{
+    using VT = typename Vec4<T>::type;
+    constexpr int V = Vec4<T>::N;
+    const int W = J.W, C = J.C, n = J.n;
+    const int dir = J.dir;
+    const bool active = t < W * C;
+    const int l = active ? t % W : 0, c = active ? t / W : 0;
+    const int q = t;  // scratch slot: active threads use c*W + l == t
+    ChunkScratch<T> sc = scf;
+    const int cs = c * L;
+    const int nv = min(L, n - cs);
+    T r[L];
+    if (dir == DX) {
+        const int lr = l < rows ? l : 0;
+        const T *row = tile + (size_t)lr * J.pitch + cs;  // points cs-4 .. cs+L+3
+        auto load = [&](auto &w, auto j0) {
+            constexpr int J0 = decltype(j0)::value;
+            constexpr int NW = sizeof(w) / sizeof(T);
+#pragma unroll
+            for (int j = 0; j < NW; j += V) {
+                const VT qa = *reinterpret_cast<const VT *>(row + J0 + j);
+                const T *ea = reinterpret_cast<const T *>(&qa);
+#pragma unroll
+                for (int v = 0; v < V; ++v) w[j + v] = ea[v];
+            }
+        };
+        for (int k = 0; k < J.nops; ++k) {
+            // the previous operator's row copies have read the staging
+            // rows before anyone writes them again (after this solve's barriers)
+            if (XS) bulk_wait_read_all();
+            chunk_solve_resp<T, L, true>(J.op[k], J.kind[k], resp_s + k * 4 * L, load, r, sc, W, l, c, C, nv,
+                                         q, J.keep[k]);
+            if (!XS || !J.xstage) {  // each thread's chunk straight out, 16 bytes at a time
+                if (active && l < rows) {
+                    T *dst = J.out[k] + (size_t)(l0 + l) * n + cs;
+#pragma unroll
+                    for (int j = 0; j < L; j += V) {
+                        if (j < nv) {
+                            VT qv;
+                            T *e = reinterpret_cast<T *>(&qv);
+#pragma unroll
+                            for (int v = 0; v < V; ++v) e[v] = r[j + v];
+                            *reinterpret_cast<VT *>(dst + j) = qv;
+                        }
+                    }
+                }
+                continue;
+            }
+            if (active && l < rows) {
+                T *dst = out_s + (size_t)l * J.pitch + cs;  // room for the last window past n
+#pragma unroll
+                for (int j = 0; j < L; j += V) {
+                    VT qv;
+                    T *e = reinterpret_cast<T *>(&qv);
+#pragma unroll
+                    for (int v = 0; v < V; ++v) e[v] = r[j + v];
+                    *reinterpret_cast<VT *>(dst + j) = qv;
+                }
+            }
+            fence_proxy_async_smem();
+            __syncthreads();
+            if (t < rows) {
+                bulk_store(J.out[k] + (size_t)(l0 + t) * n, out_s + (size_t)t * J.pitch,
+                           (uint32_t)(n * sizeof(T)));
+                bulk_commit();
+            }
+        }
+    } else {
+        const T *col = tile + (size_t)(J.halo + cs - 4) * W + l;  // points cs-4 .. cs+L+3
+        auto load = [&](auto &w, auto j0) {
+            constexpr int J0 = decltype(j0)::value;
+            constexpr int NW = sizeof(w) / sizeof(T);
+#pragma unroll
+            for (int j = 0; j < NW; ++j) w[j] = col[(J0 + j) * W];
+        };
+        const bool live = active && x0 + l < J.nx;
+        const size_t ostride = dir == DY ? (size_t)J.nx : (size_t)J.nx * J.ny;
+        const size_t obase = (size_t)(x0 + l) +
+                             (dir == DY ? (size_t)J.nx * J.ny * o : (size_t)J.nx * o) +
+                             (size_t)cs * ostride;
+        for (int k = 0; k < J.nops; ++k) {
+            chunk_solve_resp<T, L, true>(J.op[k], J.kind[k], resp_s + k * 4 * L, load, r, sc, W, l, c, C, nv,
+                                         q, J.keep[k]);
+            if (live) {
+                T *dst = J.out[k] + obase;
+#pragma unroll
+                for (int j = 0; j < L; ++j) {
+                    if (j < nv) *dst = r[j];
+                    dst += ostride;
+                }
+            }
+        }
+    }
+}
+
+// VAR (BatchVariant): kBatchLong runs every job with the long chunk and
+// its x outputs straight out; kBatchMixed takes each job's chunk length;
+// kBatchStaged also stages the x outputs of jobs with xstage set.  The
+// narrower variants carry less code and no staging rows.
+template <typename T, int VAR>
 __global__ void __launch_bounds__(kBatchThreads, 2)
     ls_batch(const BatchJob<T> *__restrict__ jobs, int njobs, long total,
              unsigned long long *counter, size_t tile_cap, int *err)
 {
-    using VT = typename Vec4<T>::type;
-    constexpr int V = Vec4<T>::N;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ uint64_t bars[2];
     __shared__ long s_item;
@@ -1483,6 +1605,8 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
     const ChunkScratch<T> scf = carve_scratch<T>(smem_raw + 2 * tile_cap, kBatchThreads / 1, 1);
     T *resp_s = reinterpret_cast<T *>(smem_raw + 2 * tile_cap +
                                       (((size_t)2 * kBatchThreads * sizeof(T) + 15) & ~(size_t)15));
+    // staging rows of x outputs (one tile's worth), after the responses
+    T *out_s = reinterpret_cast<T *>(smem_raw + batch_out_offset<T>(tile_cap));
     auto job_of = [&](long item) {
         int lo = 0, hi = njobs - 1;
         while (lo < hi) {
@@ -1551,6 +1675,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
         if (!__syncthreads_and(ok)) {
             if (t == 0) atomicExch(err, 1);
             mbar_wait_bounded(&bars[slot], parity, kChunkWaitNs);
+            if (VAR == kBatchStaged) bulk_wait_all();
             return;
         }
         phases ^= 1u << slot;
@@ -1558,6 +1683,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
         // after its last barrier, its tile before): this item's responses go
         // in place, and the next item, claimed now, is copied into the other
         // slot while this one is solved
+        const int L = VAR == kBatchLong ? kChunkLong<T> : J.L;
         for (int i = t; i < J.nops * 4 * L; i += kBatchThreads) {
             const int k = i / (4 * L), rem = i - k * 4 * L, a = rem / L, j = rem - a * L;
             resp_s[i] = J.resp[k][a][j];
@@ -1571,95 +1697,45 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
         else fill_halos_yz<T>(tbase, 0, 1, n, W, J.halo);
         fence_proxy_async_smem();  // copies into this slot two items later overwrite the halos
         __syncthreads();
-        const bool active = t < W * C;
-        const int l = active ? t % W : 0, c = active ? t / W : 0;
-        const int q = t;  // scratch slot: active threads use c*W + l == t
-        ChunkScratch<T> sc = scf;
-        const int cs = c * L;
-        const int nv = min(L, n - cs);
-        T r[L];
-        if (dir == DX) {
-            const int lr = l < rows ? l : 0;
-            const T *row = tile + (size_t)lr * J.pitch + cs;  // points cs-4 .. cs+L+3
-            auto load = [&](auto &w, auto j0) {
-                constexpr int J0 = decltype(j0)::value;
-                constexpr int NW = sizeof(w) / sizeof(T);
-#pragma unroll
-                for (int j = 0; j < NW; j += V) {
-                    const VT qa = *reinterpret_cast<const VT *>(row + J0 + j);
-                    const T *ea = reinterpret_cast<const T *>(&qa);
-#pragma unroll
-                    for (int v = 0; v < V; ++v) w[j + v] = ea[v];
-                }
-            };
-            for (int k = 0; k < J.nops; ++k) {
-                chunk_solve_resp<T, L, true>(J.op[k], J.kind[k], resp_s + k * 4 * L, load, r, sc, W, l, c, C, nv,
-                                             q, J.keep[k]);
-                if (active && l < rows) {
-                    T *dst = J.out[k] + (size_t)(l0 + l) * n + cs;
-#pragma unroll
-                    for (int j = 0; j < L; j += V) {
-                        if (j < nv) {
-                            VT qv;
-                            T *e = reinterpret_cast<T *>(&qv);
-#pragma unroll
-                            for (int v = 0; v < V; ++v) e[v] = r[j + v];
-                            *reinterpret_cast<VT *>(dst + j) = qv;
-                        }
-                    }
-                }
-            }
-        } else {
-            const T *col = tile + (size_t)(J.halo + cs - 4) * W + l;  // points cs-4 .. cs+L+3
-            auto load = [&](auto &w, auto j0) {
-                constexpr int J0 = decltype(j0)::value;
-                constexpr int NW = sizeof(w) / sizeof(T);
-#pragma unroll
-                for (int j = 0; j < NW; ++j) w[j] = col[(J0 + j) * W];
-            };
-            const bool live = active && x0 + l < J.nx;
-            const size_t ostride = dir == DY ? (size_t)J.nx : (size_t)J.nx * J.ny;
-            const size_t obase = (size_t)(x0 + l) +
-                                 (dir == DY ? (size_t)J.nx * J.ny * o : (size_t)J.nx * o) +
-                                 (size_t)cs * ostride;
-            for (int k = 0; k < J.nops; ++k) {
-                chunk_solve_resp<T, L, true>(J.op[k], J.kind[k], resp_s + k * 4 * L, load, r, sc, W, l, c, C, nv,
-                                             q, J.keep[k]);
-                if (live) {
-                    T *dst = J.out[k] + obase;
-#pragma unroll
-                    for (int j = 0; j < L; ++j) {
-                        if (j < nv) *dst = r[j];
-                        dst += ostride;
-                    }
-                }
-            }
-        }
+        constexpr bool XS = VAR == kBatchStaged;
+        if (VAR == kBatchLong || J.L == kChunkLong<T>)
+            batch_item<T, kChunkLong<T>, XS>(J, tile, out_s, resp_s, scf, t, l0, rows, x0, o);
+        else
+            batch_item<T, kChunkShort<T>, XS>(J, tile, out_s, resp_s, scf, t, l0, rows, x0, o);
     }
+    if (VAR == kBatchStaged) bulk_wait_all();  // x rows in flight (issued by this thread)
 }
+
 
 static int gcd_int(int a, int b) { return b ? gcd_int(b, a % b) : a; }
 
 // Fills the geometry, tiling and staging fields of a job; false when the
 // job's box cannot take the chunked batch kernel.
 template <typename T>
-bool plan_batch_job(BatchJob<T> &J, int L, size_t *tile_bytes)
+bool plan_batch_job(BatchJob<T> &J, int L, int w_req, int xstage, size_t *tile_bytes)
 {
     const size_t es = sizeof(T);
     const int n = J.n;
     constexpr int V = Vec4<T>::N;
+    if (L != kChunkLong<T> && L != kChunkShort<T>) return false;
     for (int k = 0; k < J.nops; ++k)
         if (!J.op[k].circ || J.op[k].n != n) return false;
     for (int k = 0; k < J.nops; ++k) J.keep[k] = fill_op_resp(J.resp[k], J.op[k].alfa, L, n);
+    J.L = L;
     J.C = (n + L - 1) / L;
     if (J.C > kBatchThreads) return false;
     int W = kBatchThreads / J.C;
+    if (w_req > 0) W = std::min(W, w_req);
     const int wq = (int)(16 / es);  // TMA inner extent: multiple of 16 bytes
     W = std::max(wq, W / wq * wq);
     if (W * J.C > kBatchThreads || W > 256) return false;
     J.W = W;
     if (J.dir == DX) {
         if (n % V || (reinterpret_cast<uintptr_t>(J.in) & 15)) return false;
+        // staged outputs leave as bulk row copies: 16-byte aligned rows
+        J.xstage = xstage ? 1 : 0;
+        for (int k = 0; k < J.nops && J.xstage; ++k)
+            if (reinterpret_cast<uintptr_t>(J.out[k]) & 15) J.xstage = 0;
         int pitch = J.C * L + 2 * kHalo;
         while (((size_t)pitch * es / 16) % 2 == 0) pitch += V;
         J.pitch = pitch;
@@ -1697,20 +1773,40 @@ bool plan_batch_job(BatchJob<T> &J, int L, size_t *tile_bytes)
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// Carry scratch, then the carry responses of the item's operators.
+// Two slots, scratch and responses, then (kBatchStaged) the x staging rows;
+// without them more CTAs may fit an SM.
 template <typename T>
-size_t batch_scratch_bytes()
+size_t batch_smem_bytes(size_t tile_cap, int variant)
 {
-    return (((size_t)2 * kBatchThreads * sizeof(T) + 15) & ~(size_t)15) +
-           (size_t)kMaxStageOps * 4 * kChunkLong<T> * sizeof(T);
+    return variant == kBatchStaged ? batch_out_offset<T>(tile_cap) + tile_cap
+                                   : 2 * tile_cap + batch_scratch_bytes_c<T>();
 }
 
 template <typename T>
-int prepare_batch(size_t tile_cap, size_t smem_optin, int num_sms, int *grid)
+static void (*batch_kernel(int variant))(const BatchJob<T> *, int, long, unsigned long long *, size_t, int *)
 {
-    const size_t smem = 2 * tile_cap + batch_scratch_bytes<T>();
+    if (variant == kBatchStaged) return ls_batch<T, kBatchStaged>;
+    if (variant == kBatchMixed) return ls_batch<T, kBatchMixed>;
+    return ls_batch<T, kBatchLong>;
+}
+
+template <typename T>
+int batch_variant(const BatchJob<T> *jobs, int njobs)
+{
+    int v = kBatchLong;
+    for (int i = 0; i < njobs; ++i) {
+        if (jobs[i].dir == DX && jobs[i].xstage) return kBatchStaged;
+        if (jobs[i].L != kChunkLong<T>) v = kBatchMixed;
+    }
+    return v;
+}
+
+template <typename T>
+int prepare_batch(size_t tile_cap, int variant, size_t smem_optin, int num_sms, int *grid)
+{
+    const size_t smem = batch_smem_bytes<T>(tile_cap, variant);
     if (smem + 1024 > smem_optin) return X3D_EUNSUPPORTED;
-    auto kern = ls_batch<T, kChunkLong<T>>;
+    auto kern = batch_kernel<T>(variant);
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return X3D_ECUDA;
     int per_sm = 0;
@@ -1721,23 +1817,25 @@ int prepare_batch(size_t tile_cap, size_t smem_optin, int num_sms, int *grid)
 
 template <typename T>
 int launch_batch(cudaStream_t st, int grid, const BatchJob<T> *d_jobs, int njobs, long total,
-                 unsigned long long *d_counter, size_t tile_cap, int *d_err)
+                 unsigned long long *d_counter, size_t tile_cap, int variant, int *d_err)
 {
-    const size_t smem = 2 * tile_cap + batch_scratch_bytes<T>();
+    const size_t smem = batch_smem_bytes<T>(tile_cap, variant);
     if (cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), st) != cudaSuccess) return X3D_ECUDA;
-    ls_batch<T, kChunkLong<T>><<<(unsigned)grid, kBatchThreads, smem, st>>>(d_jobs, njobs, total, d_counter,
-                                                                             tile_cap, d_err);
+    batch_kernel<T>(variant)<<<(unsigned)grid, kBatchThreads, smem, st>>>(d_jobs, njobs, total, d_counter,
+                                                                           tile_cap, d_err);
     return cudaGetLastError() == cudaSuccess ? X3D_OK : X3D_ECUDA;
 }
 
-template bool plan_batch_job<float>(BatchJob<float> &, int, size_t *);
-template bool plan_batch_job<double>(BatchJob<double> &, int, size_t *);
-template int prepare_batch<float>(size_t, size_t, int, int *);
-template int prepare_batch<double>(size_t, size_t, int, int *);
+template bool plan_batch_job<float>(BatchJob<float> &, int, int, int, size_t *);
+template bool plan_batch_job<double>(BatchJob<double> &, int, int, int, size_t *);
+template int batch_variant<float>(const BatchJob<float> *, int);
+template int batch_variant<double>(const BatchJob<double> *, int);
+template int prepare_batch<float>(size_t, int, size_t, int, int *);
+template int prepare_batch<double>(size_t, int, size_t, int, int *);
 template int launch_batch<float>(cudaStream_t, int, const BatchJob<float> *, int, long, unsigned long long *,
-                                 size_t, int *);
+                                 size_t, int, int *);
 template int launch_batch<double>(cudaStream_t, int, const BatchJob<double> *, int, long, unsigned long long *,
-                                  size_t, int *);
+                                  size_t, int, int *);
 
 template int launch_stage<float>(x3d_ctx_s *, const StageProgram<float> &, int, int, int, int, int);
 template int launch_stage<double>(x3d_ctx_s *, const StageProgram<double> &, int, int, int, int, int);

@@ -84,6 +84,8 @@ struct BatchJob {
     LineOp<T> op[kMaxStageOps];
     int kind[kMaxStageOps];
     int nops, dir, n, nx, ny, nz;
+    int L;       // chunk length (kChunkLong or kChunkShort of T)
+    int xstage;  // x jobs: outputs staged in shared-memory rows, bulk row copies
     int W, C, box_n, nbox, pitch;
     int halo;    // y/z: staged rows in front of the line (periodic halo + alignment)
     long span;   // x: number of lines; y/z: tiles across x
@@ -95,22 +97,33 @@ struct BatchJob {
     int keep[kMaxStageOps];
 };
 
-// Chooses tiling for the job (chunk length L) and encodes its tensor map;
-// false when the batch kernel cannot take the job.
+// Chooses tiling for the job (chunk length L, kChunkLong or kChunkShort of
+// T; at most w_req lines per tile when w_req > 0, else as many as the
+// threads allow; x outputs staged in shared memory when xstage) and encodes
+// its tensor map; false when the batch kernel cannot take the job.
 template <typename T>
-bool plan_batch_job(BatchJob<T> &J, int L, size_t *tile_bytes);
+bool plan_batch_job(BatchJob<T> &J, int L, int w_req, int xstage, size_t *tile_bytes);
 
-// Sets the batch kernel's shared-memory attribute for tiles up to tile_cap
-// bytes and returns the persistent grid (SMs x resident CTAs per SM).
+// Variants of the batch kernel: every job on the long chunk with x outputs
+// straight out; each job's own chunk length; and x outputs staged in shared
+// memory where a job sets xstage.  batch_variant picks the narrowest one a
+// host job list needs.
+enum BatchVariant { kBatchLong = 0, kBatchMixed = 1, kBatchStaged = 2 };
 template <typename T>
-int prepare_batch(size_t tile_cap, size_t smem_optin, int num_sms, int *grid);
+int batch_variant(const BatchJob<T> *jobs, int njobs);
+
+// Sets the shared-memory attribute of the batch kernel's variant for tiles
+// up to tile_cap bytes and returns the persistent grid (SMs x resident CTAs
+// per SM).
+template <typename T>
+int prepare_batch(size_t tile_cap, int variant, size_t smem_optin, int num_sms, int *grid);
 
 // One persistent launch over every tile of every job (jobs and counter in
 // device memory; the counter is reset by the launch itself, so the pair of
 // operations can be captured in a CUDA graph and replayed).
 template <typename T>
 int launch_batch(cudaStream_t st, int grid, const BatchJob<T> *d_jobs, int njobs, long total,
-                 unsigned long long *d_counter, size_t tile_cap, int *d_err);
+                 unsigned long long *d_counter, size_t tile_cap, int variant, int *d_err);
 
 // A plain program: operator k reads input 0 and writes out[k].
 template <typename T>
