@@ -9,7 +9,8 @@ tests/test_capi_abi.py checks that the committed module matches the header.
 
 Type mapping: handles (x3d_ctx, x3d_op, x3d_batch) and field or array
 pointers pass by value as type(c_ptr) -- c_loc of a target array, or a
-device address under !$acc host_data use_device; handles a call returns
+device address under !$acc host_data use_device; arrays of field pointers
+(void *const *) as arrays of type(c_ptr); handles a call returns
 (x3d_ctx *, ...) pass by reference; int, double and size_t pass by value;
 int * outputs pass by reference (arrays where the header takes several
 values); strings pass as character arrays (trim(name) // c_null_char).  A C
@@ -49,12 +50,12 @@ def constants(text):
 def fortran_type(ctype, pname):
     """(declaration, dimension suffix) of one dummy argument."""
     by_value_ptr = {"x3d_ctx", "x3d_op", "x3d_batch", "void *", "const void *", "double *", "const double *",
-                    "const x3d_box *", "const x3d_work *"}
+                    "const x3d_box *", "const x3d_work *", "const x3d_block *"}
     if ctype in by_value_ptr:
         return "type(c_ptr), value", ""
     if ctype in ("x3d_ctx *", "x3d_op *", "x3d_batch *", "void **"):
         return "type(c_ptr)", ""
-    if ctype == "void *const *":
+    if ctype in ("void *const *", "const void *const *"):
         return "type(c_ptr)", "(*)"
     if ctype == "int":
         return "integer(c_int), value", ""

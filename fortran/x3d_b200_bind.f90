@@ -564,6 +564,16 @@ module x3d_b200_bind
        type(c_ptr), value :: out
        integer(c_int), value :: is_complex
      end function
+     integer(c_int) function x3d_copy_blocks(ctx, dst, src, elem_bytes, blocks, cnt) bind(C, &
+          name="x3d_copy_blocks")
+       import :: c_ptr, c_int
+       type(c_ptr), value :: ctx
+       type(c_ptr), value :: dst
+       type(c_ptr), value :: src
+       integer(c_int), value :: elem_bytes
+       type(c_ptr), value :: blocks
+       integer(c_int), value :: cnt
+     end function
      integer(c_int) function x3d_poisson(ctx, rhs) bind(C, name="x3d_poisson")
        import :: c_ptr, c_int
        type(c_ptr), value :: ctx
@@ -701,6 +711,43 @@ module x3d_b200_bind
      integer(c_int) function x3d_step_launch(ctx) bind(C, name="x3d_step_launch")
        import :: c_ptr, c_int
        type(c_ptr), value :: ctx
+     end function
+     integer(c_int) function x3d_transeq_part(ctx, dir, du, u, add, unew, dt, nx, ny, &
+          nz) bind(C, name="x3d_transeq_part")
+       import :: c_ptr, c_int, c_double
+       type(c_ptr), value :: ctx
+       integer(c_int), value :: dir
+       type(c_ptr) :: du(*)
+       type(c_ptr) :: u(*)
+       type(c_ptr) :: add(*)
+       type(c_ptr) :: unew(*)
+       real(c_double), value :: dt
+       integer(c_int), value :: nx
+       integer(c_int), value :: ny
+       integer(c_int), value :: nz
+     end function
+     integer(c_int) function x3d_divergence_part(ctx, dir, out, src, nx, ny, nz) bind(C, &
+          name="x3d_divergence_part")
+       import :: c_ptr, c_int
+       type(c_ptr), value :: ctx
+       integer(c_int), value :: dir
+       type(c_ptr) :: out(*)
+       type(c_ptr) :: src(*)
+       integer(c_int), value :: nx
+       integer(c_int), value :: ny
+       integer(c_int), value :: nz
+     end function
+     integer(c_int) function x3d_gradp_part(ctx, dir, out, src, ucor, nx, ny, nz) bind(C, &
+          name="x3d_gradp_part")
+       import :: c_ptr, c_int
+       type(c_ptr), value :: ctx
+       integer(c_int), value :: dir
+       type(c_ptr) :: out(*)
+       type(c_ptr) :: src(*)
+       type(c_ptr) :: ucor(*)
+       integer(c_int), value :: nx
+       integer(c_int), value :: ny
+       integer(c_int), value :: nz
      end function
      integer(c_int) function x3d_buf_register(ctx, host, nbytes, dev) bind(C, &
           name="x3d_buf_register")

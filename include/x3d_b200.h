@@ -361,6 +361,25 @@ int x3d_transpose_y_to_z(x3d_ctx ctx, const void *in, void *out, int is_complex)
 int x3d_transpose_z_to_y(x3d_ctx ctx, const void *in, void *out, int is_complex);
 int x3d_transpose_y_to_x(x3d_ctx ctx, const void *in, void *out, int is_complex);
 
+/* Over a p_row x p_col process grid each transpose is an exchange of blocks
+ * among the ranks of one row or column of the grid (2decomp's
+ * transpose_x_to_y etc., which pack the blocks of the rank's pencil into a
+ * send buffer, exchange them with MPI_ALLTOALLV and unpack what arrives).
+ * The exchange is the host's collective (NCCL through torch.distributed in
+ * x3div_b200.pencils); x3d_copy_blocks is the packing and the unpacking: it
+ * copies `count` boxes of elements of elem_bytes (4, 8 or 16) bytes from
+ * src to dst, box i from element src_offset with the given y and z strides
+ * to element dst_offset with its own strides, in one launch per 32 boxes on
+ * the context's stream.  Device pointers; the boxes must not overlap in
+ * dst.  No reference counterpart as a routine. */
+typedef struct x3d_block {
+    long long src_offset, dst_offset; /* first element of the box */
+    int nx, ny, nz;                   /* extents of the box */
+    long long src_ystride, src_zstride; /* elements between rows / planes of src */
+    long long dst_ystride, dst_zstride; /* elements between rows / planes of dst */
+} x3d_block;
+int x3d_copy_blocks(x3d_ctx ctx, void *dst, const void *src, int elem_bytes, const x3d_block *blocks, int count);
+
 /* ---- spectral Poisson: decomp_2d_poisson (src/poisson.f90:57-65) -------- */
 
 /* poisson_000 (src/poisson.f90:276-419), in place on the FP64 pressure-grid
@@ -454,6 +473,39 @@ int x3d_euler_step(x3d_ctx ctx, void *ux1, void *uy1, void *uz1, void *dux1, voi
 int x3d_step_capture(x3d_ctx ctx, void *ux1, void *uy1, void *uz1, void *dux1, void *duy1,
                      void *duz1, double *pp3, void *px1, void *py1, void *pz1, double dt);
 int x3d_step_launch(x3d_ctx ctx);
+
+/* ---- the step's parts on one pencil of a process grid --------------------- */
+
+/* The reference computes each stage of the step pencil by pencil, with a
+ * transpose between (src/transeq.f90:44-355, src/navier.f90:98-359).  These
+ * are the fused stage kernels of x3d_momentum_rhs_eq, x3d_divergence and
+ * x3d_gradp + x3d_cor_vel, one direction at a time, on a dir-pencil of
+ * local extents (nx, ny, nz) whose lines along dir are whole (the context's
+ * length along dir); the host transposes between them.  Field arrays are
+ * device pointers of the context's precision unless stated.
+ *
+ * x3d_transeq_part: for c = 0, 1, 2
+ *   du[c] = add[c] + d(u_dir u_c)/dx_dir + u_dir d(u_c)/dx_dir
+ * (add may be NULL, or add[c] may alias du[c]); with unew != NULL also
+ *   unew[c] = u[c] + dt du[c]   (int_time, Euler; unew[c] may alias u[c]).
+ * x3d_divergence_part (navier.f90:166-202):
+ *   dir 0: out = {pp1, pgy1, pgz1} = {derxvp ux, interxvp uy, interxvp uz}, in = {ux, uy, uz}
+ *   dir 1: out = {duydypi2, upi2} = {deryvp pgy1 + interyvp pp1, interyvp pgz1}, in = {pp1, pgy1, pgz1}
+ *   dir 2: out = {pp3} = {interzvp duydypi2 + derzvp upi2} (FP64), in = {duydypi2, upi2}
+ * x3d_gradp_part (navier.f90:273-304; cor_vel :83-87):
+ *   dir 2: out = {ppi3, pgz3} = {interzpv pp3, derzpv pp3}, in = {pp3} (FP64)
+ *   dir 1: out = {ppi2, pgy2, pgzi2} = {interypv ppi3, derypv ppi3, interypv pgz3}, in = {ppi3, pgz3}
+ *   dir 0: out = {px, py, pz} = {derxpv ppi2, interxpv pgy2, interxpv pgzi2}, in = {ppi2, pgy2, pgzi2};
+ *          with ucor != NULL also ucor[c] -= out[c]
+ * Periodic contexts.  X3D_EUNSUPPORTED when the fused kernels cannot take
+ * the pencil (its lines, alignment or x extent); the host then composes the
+ * part from the single-operator routines. */
+int x3d_transeq_part(x3d_ctx ctx, int dir, void *const *du, const void *const *u, const void *const *add,
+                     void *const *unew, double dt, int nx, int ny, int nz);
+int x3d_divergence_part(x3d_ctx ctx, int dir, void *const *out, const void *const *in, int nx, int ny,
+                        int nz);
+int x3d_gradp_part(x3d_ctx ctx, int dir, void *const *out, const void *const *in, void *const *ucor, int nx,
+                   int ny, int nz);
 
 /* ---- device-resident host arrays ------------------------------------------ */
 

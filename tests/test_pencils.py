@@ -1,17 +1,25 @@
 """One box over a p_row x p_col process grid (x3div_b200/pencils.py,
-2decomp's 2-D pencil decomposition): the pencil blocks, the four transposes
-over gloo, a whole sweep, the Poisson solve and two Euler steps, with the
-oracle standing in for each rank's kernels, against the oracle on the whole
+2decomp's 2-D pencil decomposition; 1 x P is 2decomp's slabs): the pencil
+blocks, the transpose plans, the four transposes over gloo, a whole sweep,
+the Poisson solve and two Euler steps, with the oracle standing in for each
+rank's kernels (tests/oracle_context.py), against the oracle on the whole
 box."""
 import os
 
 import numpy as np
 import pytest
 
-from test_slabs import KIND, OracleContext, _free_port
-from x3div_b200.pencils import (SWEEP, PencilLayout, Pencils, euler_step, poisson, sweep, transpose_x_to_y,
-                                transpose_y_to_x, transpose_y_to_z, transpose_z_to_y)
-from x3div_b200.slabs import SlabLayout
+from oracle_context import KIND, OracleContext, free_port
+from x3div_b200.pencils import (SWEEP, PencilLayout, Pencils, copy_boxes, euler_step, plan_transpose, poisson,
+                                split, sweep, transpose_x_to_y, transpose_y_to_x, transpose_y_to_z,
+                                transpose_z_to_y)
+
+
+def test_split_matches_2decomp_blocks():
+    assert [split(10, 3, r) for r in range(3)] == [(0, 4), (4, 7), (7, 10)]
+    assert [split(8, 4, r) for r in range(4)] == [(0, 2), (2, 4), (4, 6), (6, 8)]
+    with pytest.raises(ValueError):
+        PencilLayout((8, 2, 8), 1, 3, 0)
 
 
 @pytest.mark.parametrize("grid,shape", [((2, 2), (12, 10, 9)), ((3, 2), (11, 9, 10)), ((1, 4), (8, 9, 12))])
@@ -29,17 +37,67 @@ def test_blocks_tile_the_box(grid, shape):
 
 
 def test_slabs_are_one_row_of_pencils():
+    """1 x P: the X and Y pencils coincide (z-slabs), the Z pencil is a
+    y-slab, and only the y <-> z transposes exchange anything."""
     shape = (10, 8, 11)
     for r in range(3):
-        s = SlabLayout(shape, r, 3)
         p = PencilLayout(shape, 1, 3, r)
-        assert p.extents("x") == p.extents("y") == s.xy_extents
-        assert p.extents("z") == s.z_extents
+        assert p.extents("x") == p.extents("y") == (10, 8) + (split(11, 3, r)[1] - split(11, 3, r)[0],)
+        assert p.extents("z") == (10, split(8, 3, r)[1] - split(8, 3, r)[0], 11)
+        assert plan_transpose(p, "x_to_y") is None and plan_transpose(p, "y_to_x") is None
+        assert plan_transpose(p, "y_to_z") is not None
     with pytest.raises(ValueError):
         PencilLayout((8, 2, 8), 3, 1, 0)
 
 
-def _rank(rank, grid, port, shape, q):
+@pytest.mark.parametrize("grid,shape", [((2, 2), (12, 10, 9)), ((3, 2), (11, 9, 10)), ((2, 3), (9, 11, 10)),
+                                        ((1, 4), (8, 9, 12)), ((4, 1), (9, 8, 6))])
+@pytest.mark.parametrize("rest", [(), (2,)])
+def test_transpose_plans_move_every_point_once(grid, shape, rest):
+    """Every rank's plan, executed on host tensors with the exchange done by
+    hand (member i's i-th send block to member i), rebuilds each rank's
+    target pencil of a global array; a complex spectrum travels as pairs."""
+    import torch
+    p_row, p_col = grid
+    g = np.random.default_rng(2).standard_normal(shape[::-1] + rest)
+    lays = [PencilLayout(shape, p_row, p_col, r) for r in range(p_row * p_col)]
+    r_ = int(np.prod(rest)) if rest else 1
+
+    def part(L, pencil):
+        (x0, x1), (y0, y1), (z0, z1) = L.block(pencil)
+        return torch.from_numpy(np.ascontiguousarray(g[z0:z1, y0:y1, x0:x1]))
+
+    for kind, src, dst in (("x_to_y", "x", "y"), ("y_to_x", "y", "x"), ("y_to_z", "y", "z"), ("z_to_y", "z", "y")):
+        plans = [plan_transpose(L, kind) for L in lays]
+        if plans[0] is None:
+            continue
+        sends = []
+        for L, pl in zip(lays, plans):
+            t = part(L, src)
+            if pl.pack is None:
+                sends.append(t.reshape(-1))
+            else:
+                buf = torch.empty(sum(pl.send) * r_, dtype=t.dtype)
+                copy_boxes(None, buf, t, pl.pack, r_)
+                sends.append(buf)
+        for L, pl in zip(lays, plans):
+            chunks = []
+            for m in pl.members:
+                mp_ = plans[m]
+                i = mp_.members.index(L.rank)
+                off = sum(mp_.send[:i]) * r_
+                chunks.append(sends[m][off:off + mp_.send[i] * r_])
+            recv = torch.cat(chunks)
+            assert recv.numel() == sum(pl.recv) * r_
+            if pl.unpack is None:
+                got = recv.view(pl.out_shape + rest)
+            else:
+                got = torch.empty(pl.out_shape + rest, dtype=recv.dtype)
+                copy_boxes(None, got, recv, pl.unpack, r_)
+            assert np.array_equal(got.numpy(), part(L, dst).numpy()), (kind, L.rank)
+
+
+def _rank(rank, grid, port, shape, fused, q):
     import torch
     import torch.distributed as dist
     from oracle import oracle
@@ -67,7 +125,7 @@ def _rank(rank, grid, port, shape, q):
         t2 = transpose_y_to_z(transpose_x_to_y(torch.from_numpy(part(g2, "x").copy()), pc), pc)
         ok = ok and np.array_equal(t2.numpy(), part(g2, "z"))
         lengths = (2 * np.pi, 1.5, 3.0)
-        ctx = OracleContext(oracle, shape, lengths)
+        ctx = OracleContext(oracle, shape, lengths, fused)
         res = sweep(ctx, mine, pc)
         gf = np.asfortranarray(g.transpose(2, 1, 0))
         err = 0.0
@@ -97,15 +155,19 @@ def _rank(rank, grid, port, shape, q):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("grid,shape", [((2, 1), (12, 10, 9)), ((2, 2), (12, 10, 9)), ((2, 3), (9, 11, 10)),
-                                        ((3, 2), (10, 9, 8))])
-def test_pencil_transposes_sweep_poisson_step_on_gloo_ranks(grid, shape):
+@pytest.mark.parametrize("grid,shape,fused", [((2, 1), (12, 10, 9), True), ((2, 2), (12, 10, 9), True),
+                                              ((2, 3), (9, 11, 10), True), ((3, 2), (10, 9, 8), True),
+                                              ((2, 2), (10, 9, 8), False), ((1, 2), (12, 10, 9), True),
+                                              ((1, 3), (10, 8, 11), False), ((1, 4), (9, 12, 8), True)])
+def test_pencil_transposes_sweep_poisson_step_on_gloo_ranks(grid, shape, fused):
+    """fused=False: the step's parts composed from single-operator routines
+    (the path for pencils the fused kernels refuse)."""
     import torch.multiprocessing as mp
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    port = _free_port()
+    port = free_port()
     world = grid[0] * grid[1]
-    procs = [ctx.Process(target=_rank, args=(r, grid, port, shape, q)) for r in range(world)]
+    procs = [ctx.Process(target=_rank, args=(r, grid, port, shape, fused, q)) for r in range(world)]
     for p in procs:
         p.start()
     res = sorted(q.get(timeout=240) for _ in procs)

@@ -106,6 +106,10 @@ SIGNATURES = {
     "x3d_momentum_rhs_eq": [_vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "x3d_int_time": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _d],
     "x3d_euler_step": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _d],
+    "x3d_copy_blocks": [_vp, _vp, _vp, _i, _vp, _i],
+    "x3d_transeq_part": [_vp, _i, _vp, _vp, _vp, _vp, _d, _i, _i, _i],
+    "x3d_divergence_part": [_vp, _i, _vp, _vp, _i, _i, _i],
+    "x3d_gradp_part": [_vp, _i, _vp, _vp, _vp, _i, _i, _i],
     "x3d_vel": [_vp, _vp, _vp, _vp],
     "x3d_test_rms": [_vp, _i, _vp, _dp],
 }
@@ -113,6 +117,13 @@ SIGNATURES = {
 class Box(ctypes.Structure):
     """x3d_box: one periodic box of a batch."""
     _fields_ = [("nx", _i), ("ny", _i), ("nz", _i), ("xlx", _d), ("yly", _d), ("zlz", _d)]
+
+
+class Block(ctypes.Structure):
+    """x3d_block: one box of an x3d_copy_blocks list (elements)."""
+    _fields_ = [("src_offset", ctypes.c_longlong), ("dst_offset", ctypes.c_longlong), ("nx", _i), ("ny", _i),
+                ("nz", _i), ("src_ystride", ctypes.c_longlong), ("src_zstride", ctypes.c_longlong),
+                ("dst_ystride", ctypes.c_longlong), ("dst_zstride", ctypes.c_longlong)]
 
 
 class Work(ctypes.Structure):

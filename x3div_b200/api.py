@@ -385,6 +385,39 @@ class Context:
     def int_time(self, ux1, uy1, uz1, dux1, duy1, duz1, gdt):
         self._check(self.L.x3d_int_time(self.handle, *[_ptr(a) for a in (ux1, uy1, uz1, dux1, duy1, duz1)], float(gdt)))
 
+    # -- the step's parts on one pencil of a process grid ---------------------
+    @staticmethod
+    def _ptrs(fields):
+        if fields is None:
+            return None
+        return (ctypes.c_void_p * len(fields))(*[_ptr(a) for a in fields])
+
+    def transeq_part(self, dir, du, u, add, unew, dt, ext):
+        """x3d_transeq_part on a dir-pencil of local extents ext = (nx, ny, nz):
+        du[c] = add[c] + d(u_dir u_c)/dx_dir + u_dir d(u_c)/dx_dir, and with
+        unew also unew[c] = u[c] + dt du[c] (add, unew: three fields or None)."""
+        self._check(self.L.x3d_transeq_part(self.handle, int(dir), self._ptrs(du), self._ptrs(u), self._ptrs(add),
+                                            self._ptrs(unew), float(dt), *[int(e) for e in ext]))
+
+    def divergence_part(self, dir, out, ins, ext):
+        """x3d_divergence_part: the divergence's stage along dir on a pencil."""
+        self._check(self.L.x3d_divergence_part(self.handle, int(dir), self._ptrs(out), self._ptrs(ins),
+                                               *[int(e) for e in ext]))
+
+    def gradp_part(self, dir, out, ins, ucor, ext):
+        """x3d_gradp_part: the pressure gradient's stage along dir on a pencil
+        (dir 0 with ucor: also ucor[c] -= out[c])."""
+        self._check(self.L.x3d_gradp_part(self.handle, int(dir), self._ptrs(out), self._ptrs(ins),
+                                          self._ptrs(ucor), *[int(e) for e in ext]))
+
+    def copy_blocks(self, dst, src, elem_bytes, blocks):
+        """x3d_copy_blocks: blocks is a list of (src_offset, dst_offset, nx, ny,
+        nz, src_ystride, src_zstride, dst_ystride, dst_zstride) in elements of
+        elem_bytes (4, 8 or 16) bytes; dst and src are device tensors."""
+        arr = (_capi.Block * max(1, len(blocks)))(*[_capi.Block(*b) for b in blocks])
+        self._check(self.L.x3d_copy_blocks(self.handle, dst.data_ptr(), src.data_ptr(), int(elem_bytes), arr,
+                                           len(blocks)))
+
     def euler_step(self, ux1, uy1, uz1, dux1, duy1, duz1, pp3, px1, py1, pz1, dt):
         self._check(self.L.x3d_euler_step(self.handle, *[_ptr(a) for a in (ux1, uy1, uz1, dux1, duy1, duz1, pp3, px1, py1, pz1)], float(dt)))
 

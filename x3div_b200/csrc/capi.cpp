@@ -5,6 +5,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <initializer_list>
 #include <new>
 #include <string>
 #include <vector>
@@ -849,6 +850,25 @@ int x3d_transpose_y_to_z(x3d_ctx ctx, const void *in, void *out, int c) { return
 int x3d_transpose_z_to_y(x3d_ctx ctx, const void *in, void *out, int c) { return transpose_copy(ctx, in, out, c); }
 int x3d_transpose_y_to_x(x3d_ctx ctx, const void *in, void *out, int c) { return transpose_copy(ctx, in, out, c); }
 
+int x3d_copy_blocks(x3d_ctx ctx, void *dst, const void *src, int elem_bytes, const x3d_block *blocks, int count)
+{
+    const int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (elem_bytes != 4 && elem_bytes != 8 && elem_bytes != 16)
+        return set_error(ctx, X3D_EINVAL, "elem_bytes must be 4, 8 or 16");
+    if (count < 0 || (count > 0 && !blocks)) return set_error(ctx, X3D_EINVAL, "bad block list");
+    if (count == 0) return X3D_OK;
+    if (!dst || !src || !is_device_ptr(dst) || !is_device_ptr(src))
+        return set_error(ctx, X3D_EINVAL, "block copies take device arrays");
+    for (int i = 0; i < count; ++i) {
+        const x3d_block &b = blocks[i];
+        if (b.nx < 0 || b.ny < 0 || b.nz < 0 || b.src_offset < 0 || b.dst_offset < 0 || b.src_ystride < 0 ||
+            b.src_zstride < 0 || b.dst_ystride < 0 || b.dst_zstride < 0)
+            return set_error(ctx, X3D_EINVAL, "negative block extent, offset or stride");
+    }
+    return copy_blocks(ctx, dst, src, elem_bytes, blocks, count);
+}
+
 // ---- Poisson -------------------------------------------------------------------------
 
 // The Euler-step compositions use the staggered operators, which exist only
@@ -1091,6 +1111,65 @@ int x3d_div_stats(x3d_ctx ctx, const double *pp3, double *out)
 }
 
 // ---- transeq / time integration --------------------------------------------------------
+
+// ---- the step's parts on one pencil ------------------------------------------------------
+
+// A pencil of the context's box along dir: whole lines along dir, at least
+// one line, and every listed field a device array.
+static int check_part(x3d_ctx_s *ctx, int dir, int nx, int ny, int nz, std::initializer_list<const void *> fields)
+{
+    int rc = need_periodic(ctx);
+    if (rc) return rc;
+    if (dir < 0 || dir > 2) return set_error(ctx, X3D_EINVAL, "dir must be 0, 1 or 2");
+    const int ext[3] = {nx, ny, nz}, box[3] = {ctx->nx, ctx->ny, ctx->nz};
+    for (int d = 0; d < 3; ++d)
+        if (ext[d] < 1 || ext[d] > box[d]) return set_error(ctx, X3D_EINVAL, "pencil extents outside the box");
+    if (ext[dir] != box[dir]) return set_error(ctx, X3D_EINVAL, "a pencil holds whole lines along its direction");
+    for (const void *f : fields)
+        if (!f || !is_device_ptr(f)) return set_error(ctx, X3D_EINVAL, "pencil parts take device arrays");
+    return X3D_OK;
+}
+
+int x3d_transeq_part(x3d_ctx ctx, int dir, void *const *du, const void *const *u, const void *const *add,
+                     void *const *unew, double dt, int nx, int ny, int nz)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!du || !u) return set_error(ctx, X3D_EINVAL, "null field list");
+    if ((rc = check_part(ctx, dir, nx, ny, nz, {du[0], du[1], du[2], u[0], u[1], u[2]}))) return rc;
+    if (add && (rc = check_part(ctx, dir, nx, ny, nz, {add[0], add[1], add[2]}))) return rc;
+    if (unew && (rc = check_part(ctx, dir, nx, ny, nz, {unew[0], unew[1], unew[2]}))) return rc;
+    const TraceRange trace("momentum_rhs_eq part");
+    return part_transeq(ctx, dir, du, u, add, unew, dt, nx, ny, nz);
+}
+
+int x3d_divergence_part(x3d_ctx ctx, int dir, void *const *out, const void *const *in, int nx, int ny, int nz)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!out || !in) return set_error(ctx, X3D_EINVAL, "null field list");
+    if (dir == 0) rc = check_part(ctx, dir, nx, ny, nz, {out[0], out[1], out[2], in[0], in[1], in[2]});
+    else if (dir == 1) rc = check_part(ctx, dir, nx, ny, nz, {out[0], out[1], in[0], in[1], in[2]});
+    else rc = check_part(ctx, dir, nx, ny, nz, {out[0], in[0], in[1]});
+    if (rc) return rc;
+    const TraceRange trace("divergence part");
+    return part_divergence(ctx, dir, out, in, nx, ny, nz);
+}
+
+int x3d_gradp_part(x3d_ctx ctx, int dir, void *const *out, const void *const *in, void *const *ucor, int nx,
+                   int ny, int nz)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!out || !in) return set_error(ctx, X3D_EINVAL, "null field list");
+    if (dir == 2) rc = check_part(ctx, dir, nx, ny, nz, {out[0], out[1], in[0]});
+    else if (dir == 1) rc = check_part(ctx, dir, nx, ny, nz, {out[0], out[1], out[2], in[0], in[1]});
+    else rc = check_part(ctx, dir, nx, ny, nz, {out[0], out[1], out[2], in[0], in[1], in[2]});
+    if (!rc && ucor && dir == 0) rc = check_part(ctx, dir, nx, ny, nz, {ucor[0], ucor[1], ucor[2]});
+    if (rc) return rc;
+    const TraceRange trace("gradp part");
+    return part_gradp(ctx, dir, out, in, dir == 0 ? ucor : nullptr, nx, ny, nz);
+}
 
 int x3d_momentum_rhs_eq(x3d_ctx ctx, void *dux1, void *duy1, void *duz1, const void *ux1,
                         const void *uy1, const void *uz1)

@@ -639,18 +639,23 @@ __device__ __forceinline__ void flush_yz(const FlushArgs<T> &fa, const V (&res)[
 // 6.4 TB/s that way against 4.6 TB/s at a fixed stride (x3d_roofline_probe
 // patterns 5 and 1).  The launcher zeroes the counter before each launch.
 //
+// TI: the element type of the staged inputs.  TI = double with T = float
+// (plain programs, PR = 1, OCC = 1) stages FP64 fields and solves them in FP32: the
+// pressure gradient reads the FP64 pressure this way, with no FP32 copy.
+//
 // OCC > 1: the kernel is compiled for OCC CTAs of at most 256 threads per SM
 // (at most 65536 / (256 OCC) registers a thread).  With OCC = 3 the plain
 // FP32 16-line, 32-point-chunk kernel fits 80 registers without spilling, so
 // an SM holds 24 warps instead of 16 -- the sweep kernels are latency- and
 // issue-bound at 16 (issue active about half the cycles).
-template <typename T, int W, int L, bool ACC, bool PERSIST, int PR = 1, int OCC = 1>
+template <typename T, int W, int L, bool ACC, bool PERSIST, int PR = 1, int OCC = 1, typename TI = T>
 __global__ void __launch_bounds__(OCC > 1 ? 256 : kStageThreads<T, L, PR>, OCC)
     ls_stage_yz(const __grid_constant__ StageMaps maps, const __grid_constant__ StageProgram<T> prog, int nx,
                 int ny, int dir, int box_n, int nbox, int tma_halo, size_t tile_bytes, long ntiles,
                 unsigned long long *claim, int *err)
 {
     using V = typename PairOf<T, PR>::type;
+    static_assert(std::is_same<TI, T>::value || (PR == 1 && !ACC), "wider staged inputs: plain, unpaired");
     constexpr int WP = W / PR;  // threads across the tile's lines
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ uint64_t bars[2];
@@ -675,9 +680,9 @@ __global__ void __launch_bounds__(OCC > 1 ? 256 : kStageThreads<T, L, PR>, OCC)
         const int o = (int)(tile / tiles_x);
         uint64_t *bar = &bars[slot];
         mbar_arrive_expect_tx(bar, (uint32_t)((size_t)prog.ntiles * (nbox * box_n + (tma_halo ? 2 * kHalo : 0)) *
-                                              W * sizeof(T)));
+                                              W * sizeof(TI)));
         for (int ti = 0; ti < prog.ntiles; ++ti) {
-            T *tp = reinterpret_cast<T *>(smem_raw + slot * slot_bytes + ti * tile_bytes) + kHalo * W;
+            TI *tp = reinterpret_cast<TI *>(smem_raw + slot * slot_bytes + ti * tile_bytes) + kHalo * W;
             for (int b = 0; b < nbox; ++b) {
                 if (dir == DY)
                     tma_load_3d(tp + (size_t)b * box_n * W, &maps.m[ti], bar, x0, b * box_n, o);
@@ -685,7 +690,7 @@ __global__ void __launch_bounds__(OCC > 1 ? 256 : kStageThreads<T, L, PR>, OCC)
                     tma_load_3d(tp + (size_t)b * box_n * W, &maps.m[ti], bar, x0, o, b * box_n);
             }
             if (tma_halo) {  // points n-4 .. n-1 before the line, 0 .. 3 after it
-                T *hb = tp - kHalo * W, *ha = tp + (size_t)n * W;
+                TI *hb = tp - kHalo * W, *ha = tp + (size_t)n * W;
                 if (dir == DY) {
                     tma_load_3d(hb, &maps.hm[ti], bar, x0, n - kHalo, o);
                     tma_load_3d(ha, &maps.hm[ti], bar, x0, 0, o);
@@ -737,18 +742,23 @@ __global__ void __launch_bounds__(OCC > 1 ? 256 : kStageThreads<T, L, PR>, OCC)
         const int o = (int)(tile / tiles_x);
         unsigned char *base = smem_raw + slot * slot_bytes;
         if (!tma_halo) {
-            fill_halos_yz<T>(base, tile_bytes, prog.ntiles, n, W, kHalo);
+            fill_halos_yz<TI>(base, tile_bytes, prog.ntiles, n, W, kHalo);
             fence_proxy_async_smem();  // the halo rows are refilled by TMA two tiles later
             __syncthreads();
         }
         // window of this chunk: rows kHalo + cs - 4 ...
         auto col = [&](int ti) {
-            return reinterpret_cast<const T *>(base + ti * tile_bytes) + (kHalo + cs - 4) * W + PR * l;
+            return reinterpret_cast<const TI *>(base + ti * tile_bytes) + (kHalo + cs - 4) * W + PR * l;
         };
-        auto at = [](const T *p) { return *reinterpret_cast<const V *>(p); };
+        auto at = [](const TI *p) {
+            if constexpr (std::is_same<TI, T>::value) return *reinterpret_cast<const V *>(p);
+            else return V(*p);
+        };
         auto tile_at = [&](int ti, int j) { return at(col(ti) + (4 + j) * W); };
         auto flush_args = [&](const StageOp<T> &so) {
-            return FlushArgs<T>(so, so.base2_tile >= 0 ? col(so.base2_tile) + 4 * W : nullptr, W);
+            if constexpr (std::is_same<TI, T>::value)
+                return FlushArgs<T>(so, so.base2_tile >= 0 ? col(so.base2_tile) + 4 * W : nullptr, W);
+            else return FlushArgs<T>(so);
         };
         const bool live = x0 + PR * l < nx;
         const size_t obase = (size_t)(x0 + PR * l) + (dir == DY ? (size_t)nx * ny * o : (size_t)nx * o) +
@@ -757,8 +767,8 @@ __global__ void __launch_bounds__(OCC > 1 ? 256 : kStageThreads<T, L, PR>, OCC)
         V acc[ACC ? L : 1];
         for (int k = 0; k < prog.nops; ++k) {
             const StageOp<T> &so = prog.ops[k];
-            const T *ca = col(so.src_a);
-            const T *cb = so.src_b >= 0 ? col(so.src_b) : nullptr;
+            const TI *ca = col(so.src_a);
+            const TI *cb = so.src_b >= 0 ? col(so.src_b) : nullptr;
             auto load = [&](auto &w, auto j0) {
                 constexpr int J0 = decltype(j0)::value;
                 constexpr int NW = sizeof(w) / sizeof(V);
@@ -1285,6 +1295,11 @@ static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog_in, int 
         const int threads = C * W / PR;
         if (threads > kStageThreads<T, L, PR> || threads % 32) return X3D_EUNSUPPORTED;
         if (OCC > 1 && (acc || dir == DX || threads > 256)) return X3D_EUNSUPPORTED;
+        // FP64 inputs of an FP32 program: staged as FP64 by the plain,
+        // unpaired y/z kernels only
+        const bool in64 = prog.in_f64 != 0;
+        if (in64 && (!std::is_same<T, float>::value || PR != 1 || OCC != 1 || acc || dir == DX))
+            return X3D_EUNSUPPORTED;
         const size_t resp_bytes = (size_t)prog.nops * 4 * L * es * PR;
         for (int ti = 0; ti < prog.ntiles; ++ti)
             if (!al16(prog.in[ti])) return X3D_EUNSUPPORTED;
@@ -1329,42 +1344,43 @@ static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog_in, int 
             return cuda_check(ctx, cudaGetLastError(), "ls_stage_x launch");
         }
         auto enc = encode_tiled();
-        if (!enc || ((size_t)nx * es) % 16) return X3D_EUNSUPPORTED;
+        const size_t esi = in64 ? sizeof(double) : es;  // staged element bytes
+        if (!enc || ((size_t)nx * esi) % 16) return X3D_EUNSUPPORTED;
         const int nb = (n + 255) / 256;
         int box_n = (n + nb - 1) / nb;
-        const int align_rows = (int)(128 / (W * es) > 0 ? 128 / (W * es) : 1);
+        const int align_rows = (int)(128 / (W * esi) > 0 ? 128 / (W * esi) : 1);
         box_n = (box_n + align_rows - 1) / align_rows * align_rows;
         if (box_n > 256) return X3D_EUNSUPPORTED;
-        // rows: kHalo halo rows (kHalo * W * es is a multiple of 128 bytes, so the
+        // rows: kHalo halo rows (kHalo * W * esi is a multiple of 128 bytes, so the
         // boxes land 128-byte aligned), the boxes, and room for the last window
         const int rows = kHalo + std::max(nb * box_n, C * L + kHalo);
-        const size_t tile = ((size_t)rows * W * es + 127) & ~(size_t)127;
+        const size_t tile = ((size_t)rows * W * esi + 127) & ~(size_t)127;
         const size_t smem = (PERSIST ? 2 : 1) * prog.ntiles * tile + scratch_bytes(C, W, es) + resp_bytes;
         if (smem + 1024 > ctx->smem_optin) return X3D_EUNSUPPORTED;
         StageMaps maps;
         std::memset(&maps, 0, sizeof(maps));
-        auto encode = [&](CUtensorMap *m, const void *ptr, int rows_in_box) {
+        auto encode = [&](CUtensorMap *m, const void *ptr, int rows_in_box, size_t eb) {
             cuuint64_t gdim[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
-            cuuint64_t gstride[2] = {(cuuint64_t)nx * es, (cuuint64_t)nx * ny * es};
+            cuuint64_t gstride[2] = {(cuuint64_t)nx * eb, (cuuint64_t)nx * ny * eb};
             cuuint32_t box[3] = {(cuuint32_t)W, 1, 1};
             box[dir == DY ? 1 : 2] = (cuuint32_t)rows_in_box;
             cuuint32_t estr[3] = {1, 1, 1};
-            return enc(m, sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+            return enc(m, eb == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
                        const_cast<void *>(ptr), gdim, gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
         };
         for (int ti = 0; ti < prog.ntiles; ++ti)
-            if (!encode(&maps.m[ti], prog.in[ti], box_n)) return X3D_EUNSUPPORTED;
+            if (!encode(&maps.m[ti], prog.in[ti], box_n, esi)) return X3D_EUNSUPPORTED;
         // the periodic halos come by TMA too where the boxes end exactly at the
         // line's end (a box running past it would fill the rows after the line
         // with zeros); otherwise the kernel copies them in shared memory
         int tma_halo = nb * box_n == n ? 1 : 0;
         for (int ti = 0; ti < prog.ntiles && tma_halo; ++ti)
-            if (!encode(&maps.hm[ti], prog.in[ti], kHalo)) tma_halo = 0;
+            if (!encode(&maps.hm[ti], prog.in[ti], kHalo, esi)) tma_halo = 0;
         for (int k = 0; k < prog.nops; ++k)
             if (prog.ops[k].prefetch_base &&
-                !encode(&maps.pm[k], prog.ops[k].base ? prog.ops[k].base : prog.ops[k].base2, box_n))
+                !encode(&maps.pm[k], prog.ops[k].base ? prog.ops[k].base : prog.ops[k].base2, box_n, es))
                 prog.ops[k].prefetch_base = 0;
         prog.prefetch_mask = 0;
         for (int k = 0; k < prog.nops; ++k)
@@ -1372,6 +1388,8 @@ static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog_in, int 
         auto kern = ls_stage_yz<T, W, L, false, PERSIST, PR, OCC>;
         if constexpr (OCC == 1)  // the OCC > 1 kernels take plain programs only
             if (acc) kern = ls_stage_yz<T, W, L, true, PERSIST, PR, OCC>;
+        if constexpr (std::is_same<T, float>::value && PR == 1 && OCC == 1)
+            if (in64) kern = ls_stage_yz<T, W, L, false, PERSIST, PR, OCC, double>;
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         const long tiles_x = (nx + W - 1) / W;
         const long ntiles = tiles_x * (dir == DY ? nz : ny);

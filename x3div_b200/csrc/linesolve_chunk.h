@@ -54,6 +54,7 @@ struct StageProgram {
     const T *in[kMaxStageTiles];
     int nops, ntiles;
     int prefetch_mask;  // bit k: operator k's base is prefetched (set by launch_stage)
+    int in_f64;         // T = float: in[] hold FP64 fields (y/z plain programs only)
 };
 
 // Number of (lines per CTA, chunk length, persistence, lines per thread)

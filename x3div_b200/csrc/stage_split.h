@@ -67,6 +67,7 @@ inline int split_by_inputs(const StageProgram<T> &p, StageProgram<T> (&part)[kMa
     for (int q = 0; q < nparts; ++q) {
         StageProgram<T> &s = part[q];
         std::memset(&s, 0, sizeof(s));
+        s.in_f64 = p.in_f64;
         int map[kMaxStageTiles];
         for (int t = 0; t < p.ntiles; ++t) map[t] = -1;
         for (int k = 0; k < p.nops; ++k) {

@@ -187,6 +187,15 @@ int fused_transeq(x3d_ctx_s *ctx, void *const du[3], const void *const u[3], boo
 int fused_divergence(x3d_ctx_s *ctx, double *pp3, const void *const u[3]);
 int fused_divergence_scratch(x3d_ctx_s *ctx, double *pp3, const void *const u[3], void *const s[5]);
 int fused_gradp(x3d_ctx_s *ctx, void *const px[3], const double *pp3, void *const ucor[3]);
+// the same stages one direction at a time on a pencil of local extents
+// (nx, ny, nz) whose lines along dir are whole (x3d_transeq_part etc.)
+int part_transeq(x3d_ctx_s *ctx, int dir, void *const du[3], const void *const u[3], const void *const *add,
+                 void *const *unew, double dt, int nx, int ny, int nz);
+int part_divergence(x3d_ctx_s *ctx, int dir, void *const *out, const void *const *in, int nx, int ny, int nz);
+int part_gradp(x3d_ctx_s *ctx, int dir, void *const *out, const void *const *in, void *const *ucor, int nx, int ny,
+               int nz);
+// block copies of the pencil transposes (pencil.cu)
+int copy_blocks(x3d_ctx_s *ctx, void *dst, const void *src, int elem_bytes, const x3d_block *blocks, int count);
 
 // ---- elementwise / reductions / transposes (fields.cu) ------------------
 int launch_copy(x3d_ctx_s *ctx, void *dst, const void *src, size_t bytes);
