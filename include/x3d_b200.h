@@ -28,9 +28,10 @@
  *    maps a non-zero status to that call.
  *  - Boundaries are periodic unless the context is made with
  *    x3d_ctx_create_bc; then the operators of a non-periodic direction
- *    exist, nxm = nx - 1 in its staggered signatures, and the Poisson solver
- *    and Euler-step compositions refuse it, as the reference's Poisson
- *    solver stops on non-periodic boundaries (src/poisson.f90:104-108).
+ *    exist, nxm = nx - 1 in its staggered signatures, x3d_poisson solves
+ *    with Neumann conditions on the pressure there (a case the reference's
+ *    Poisson solver stops on, src/poisson.f90:104-108), and the Euler-step
+ *    compositions refuse it.
  *    Periodic directions have nxm == nx, nym == ny, nzm == nz.
  *  - Line lengths must be >= 8 (the 8-point interpolation stencils).
  */
@@ -120,10 +121,13 @@ int x3d_ctx_create(x3d_ctx *ctx, int nx, int ny, int nz, double xlx, double yly,
  *    line or back.  Where the reference has no branch for an operator's
  *    parity (deryvp npaire 1, :595; der?pv npaire 0, :262, :843, :1199) it
  *    computes nothing, and the call returns X3D_EUNSUPPORTED;
- *  - the second derivatives do not exist, and the Poisson solver and the
- *    Euler-step compositions return X3D_EUNSUPPORTED, as the reference's
- *    Poisson solver stops on non-periodic boundaries (src/poisson.f90:
- *    104-108). */
+ *  - the second derivatives do not exist, and the Euler-step compositions
+ *    return X3D_EUNSUPPORTED;
+ *  - x3d_poisson takes the pressure grid (nxm = nx - 1 points) and solves
+ *    with the bc = 1 (Neumann) conditions that decomp_2d_poisson_init
+ *    assigns there (src/poisson.f90:85-99) and the reference then stops on
+ *    (:104-108); the pencil entry points x3d_poisson_zlines/zpencil stay
+ *    periodic. */
 int x3d_ctx_create_bc(x3d_ctx *ctx, int nx, int ny, int nz, double xlx, double yly, double zlz,
                       int precision, int device, const int *ncl);
 /* finalise_xcompact3d's device-side part (src/x3d_tools.f90:212-248). */
@@ -383,7 +387,16 @@ int x3d_copy_blocks(x3d_ctx ctx, void *dst, const void *src, int elem_bytes, con
 /* ---- spectral Poisson: decomp_2d_poisson (src/poisson.f90:57-65) -------- */
 
 /* poisson_000 (src/poisson.f90:276-419), in place on the FP64 pressure-grid
- * field rhs (nx*ny*nz doubles). */
+ * field rhs (nx*ny*nz doubles).  On a context with non-periodic directions
+ * (x3d_ctx_create_bc) rhs has nxm = nx - 1 points along each of them and
+ * the pressure gets homogeneous Neumann conditions there: the bc = 1 case
+ * of decomp_2d_poisson_init (src/poisson.f90:85-99, :114-117) with the
+ * cosine modes of waves()'s bc = 1 tables (:539-553, :573-588, :603-613),
+ * which x3div itself stops on (:104-108).  It is solved as the periodic
+ * problem on the box mirrored about both walls of every such direction
+ * (2 nxm points over 2 xlx) and cut back: the mirrored field holds exactly
+ * those cosine modes.  The first call makes the mirrored box's periodic
+ * context and right-hand side (kept until x3d_ctx_destroy). */
 int x3d_poisson(x3d_ctx ctx, double *rhs);
 /* The z part of poisson_000 for a box whose y rows are spread over ranks:
  * spec is this rank's block of the x-y transformed half spectrum (complex

@@ -49,6 +49,7 @@ def lib() -> ctypes.CDLL:
         L.orc_thomas_plain.argtypes = [i, p, i, i, i, p, p, p]
         L.orc_poisson_spectral.argtypes = [p, i, i, i, d, d, d]
         L.orc_poisson_tables.argtypes = [i, i, i, d, d, d, p, p, p, p, p, p]
+        L.orc_poisson_tables_bc1.argtypes = [i, d, p, p]
         L.orc_divergence.argtypes = [p, p, p, p, i, i, i, d, d, d]
         L.orc_gradp.argtypes = [p, p, p, p, i, i, i, d, d, d]
         L.orc_cor_vel.argtypes = [p, p, p, p, p, p, ctypes.c_long]
@@ -193,6 +194,69 @@ def poisson(rhs: np.ndarray, xlx: float, yly: float, zlz: float) -> np.ndarray:
     lib().orc_poisson_spectral(cw.ctypes.data_as(_dp), nx, ny, nz, xlx, yly, zlz)
     out = np.fft.irfftn(cw, s=(nx, ny, nz), axes=(2, 1, 0), norm="forward")
     return np.asfortranarray(out.transpose(2, 1, 0))
+
+
+def poisson_tables_bc1(m: int, length: float):
+    """waves() for a non-periodic direction of m pressure points
+    (src/poisson.f90:539-553): k2 and the transfer function of cosine mode
+    i = 0 .. m."""
+    k2, tt = np.zeros(m + 1), np.zeros(m + 1)
+    lib().orc_poisson_tables_bc1(int(m), float(length), _p(k2), _p(tt))
+    return k2, tt
+
+
+def poisson_bc(rhs: np.ndarray, lengths, periodic) -> np.ndarray:
+    """The Poisson solve with homogeneous Neumann conditions on the pressure
+    along the non-periodic directions (the bc = 1 case of
+    decomp_2d_poisson_init, src/poisson.f90:85-99, which x3div itself stops
+    on at :104-108): rhs holds the pressure grid, m = n - 1 points along a
+    non-periodic direction.  The field mirrored about both walls of every
+    non-periodic direction is even, so it has only the cosine modes of
+    waves()'s bc = 1 tables; solved as poisson_000 on the doubled box
+    (2 m points over twice the length) and cut back to the first m points."""
+    a = np.asarray(rhs, dtype=np.float64)
+    ext, lens = a, list(lengths)
+    for d in range(3):
+        if not periodic[d]:
+            ext = np.concatenate([ext, np.flip(ext, axis=d)], axis=d)
+            lens[d] = 2 * lens[d]
+    out = poisson(np.asfortranarray(ext), *lens)
+    return np.asfortranarray(out[:a.shape[0], :a.shape[1], :a.shape[2]])
+
+
+def poisson_bc_dct(rhs: np.ndarray, lengths, periodic) -> np.ndarray:
+    """The same solve in the cosine/Fourier basis directly: a DCT-II along
+    each non-periodic direction, an FFT along each periodic one, each mode
+    divided by -K with K = k2x (ty tz)^2 + k2y (tx tz)^2 + k2z (tx ty)^2
+    from waves()'s bc = 1 tables (poisson_tables_bc1) or its periodic ones,
+    zero where K < 1e-16, and the inverse transforms.  An independent check
+    of poisson_bc."""
+    import scipy.fft as sf
+    a = np.asarray(rhs, dtype=np.float64)
+    n = a.shape
+    c = a.astype(np.complex128)
+    k2, tt = [], []
+    for d in range(3):
+        if periodic[d]:
+            t = poisson_tables(n[d], n[d], n[d], lengths[d], lengths[d], lengths[d])
+            k2.append(t["k2x"])
+            tt.append(t["tx"])
+            c = np.fft.fft(c, axis=d)
+        else:
+            kk, tr = poisson_tables_bc1(n[d], lengths[d])
+            k2.append(kk[:n[d]])
+            tt.append(tr[:n[d]])
+            c = sf.dct(c.real, type=2, axis=d) + 1j * sf.dct(c.imag, type=2, axis=d)
+    tx, ty, tz = tt[0][:, None, None], tt[1][None, :, None], tt[2][None, None, :]
+    K = (k2[0][:, None, None] * (ty * tz) ** 2 + k2[1][None, :, None] * (tx * tz) ** 2
+         + k2[2][None, None, :] * (tx * ty) ** 2)
+    c = np.where(K < 1e-16, 0.0, c / np.where(K < 1e-16, 1.0, -K))
+    for d in (2, 1, 0):
+        if periodic[d]:
+            c = np.fft.ifft(c, axis=d)
+        else:
+            c = sf.idct(c.real, type=2, axis=d) + 1j * sf.idct(c.imag, type=2, axis=d)
+    return np.asfortranarray(c.real)
 
 
 def divergence(ux, uy, uz, dx, dy, dz):

@@ -564,6 +564,37 @@ void orc_poisson_tables(int nx, int ny, int nz, double xlx, double yly, double z
     free(es);
 }
 
+/* The non-periodic (bc = 1) branch of waves() for one direction of m = n - 1
+ * pressure points (src/poisson.f90:539-553 for x, :573-588 for y): mode
+ * i = 0 .. m of the cosine expansion, w = pi i / m, the staggered
+ * derivative's modified wavenumber squared k2[i] = (m wp / len)^2 (zero for
+ * i = 0) and the interpolation's transfer function tt[i] at rle = es d = w,
+ * d = len / m.  The z branch (:603-613) packs modes i and m + 1 - i of the
+ * same two functions into the real and imaginary parts of one complex
+ * entry, for 2decomp's half-length transform; its values are these. */
+void orc_poisson_tables_bc1(int m, double len, double *k2, double *tt)
+{
+    const double pi = acos(-1.0);
+    const double d = len / m;
+    double c5d[5], c5i[5];
+    orc_rhs_scalars(ORC_DERVP, d, c5d);
+    orc_rhs_scalars(ORC_INTVP, d, c5i);
+    const double alcai = c5d[0], aci = c5d[1], bci = c5d[2];
+    const double ailcai = c5i[0], aici = c5i[1], bici = c5i[2], cici = c5i[3], dici = c5i[4];
+    for (int i = 0; i <= m; ++i) {
+        const double w = 2.0 * pi * 0.5 * i / m;
+        double wp = aci * 2.0 * d * sin(w * 0.5) + bci * 2.0 * d * sin(3.0 * 0.5 * w);
+        wp = wp / (1.0 + 2.0 * alcai * cos(w));
+        const double t = m * wp / len;
+        k2[i] = i == 0 ? 0.0 : t * t;
+        const double es = i == 0 ? 0.0 : m * w / len;
+        const double rle = es * d;
+        const double tt2 = 2.0 * (bici * cos(rle * 1.5) + cici * cos(rle * 2.5) + dici * cos(rle * 3.5));
+        const double tt1 = 2.0 * aici * cos(rle * 0.5);
+        tt[i] = (tt1 + tt2) / (1.0 + 2.0 * ailcai * cos(rle));
+    }
+}
+
 int orc_poisson_spectral(double *cw, int nx, int ny, int nz, double xlx, double yly, double zlz)
 {
     const double pi = acos(-1.0);

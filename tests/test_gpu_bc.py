@@ -6,9 +6,10 @@ reference's nclx1, nclxn, ...; 1 free slip, 2 Dirichlet) builds derx (npaire
 first_deriv_imp_; they run on the one-thread-per-line kernels with the
 boundary closures of der?_ij.  Bars as for the periodic operators: FP64 within
 1e-12 of the oracle, FP32 within 1e-5 (normwise relative).  Every other
-operator of such a direction, and the routines that need the Poisson solver,
-refuse with X3D_EUNSUPPORTED (the reference's Poisson solver stops on
-non-periodic boundaries).
+operator of such a direction, and the Euler-step compositions, refuse with
+X3D_EUNSUPPORTED.  The Poisson solve takes such a context's pressure grid
+(nx - 1 points along a non-periodic direction) with Neumann conditions
+there, against the oracle's poisson_bc at 1e-12.
 """
 import numpy as np
 import pytest
@@ -241,4 +242,35 @@ def test_nonperiodic_staggered_y_stretching_metric(oracle, torch_cuda, prec):
         ref = oracle.stag_np(kind, 1, used, h, *ncl, npaire) * metric[None, :, None]
         assert rel_err(to_host(t), ref) < tol, (routine, prec)
         op.close()
+    ctx.close()
+
+
+# pressure-grid shapes: the mirrored lengths 2 (n - 1) reach the fused z
+# kernel (2 * 32 = 64, 2 * 48 = 96) and the 3-D cuFFT path (2 * 20 = 40)
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("shape,per", [((17, 12, 10), (False, True, True)), ((12, 17, 10), (True, False, True)),
+                                       ((12, 10, 33), (True, True, False)), ((17, 13, 12), (False, False, True)),
+                                       ((13, 17, 21), (False, False, False)), ((16, 10, 49), (True, False, False))])
+def test_nonperiodic_poisson_matches_oracle(oracle, torch_cuda, prec, shape, per):
+    """x3d_poisson on a context with non-periodic directions: the bc = 1
+    (Neumann) case of decomp_2d_poisson_init on the pressure grid, against
+    the oracle's mirrored-box solve (itself checked against a DCT/FFT
+    solve from waves()'s bc = 1 tables in tests/test_oracle_poisson_bc.py),
+    FP64 in both context precisions; twice, to use the kept mirrored
+    context."""
+    torch = torch_cuda
+    from x3div_b200 import Context, to_host
+    lengths = (2 * np.pi, 1.5, 3.0)
+    bc = []
+    for p_ in per:
+        bc += [0, 0] if p_ else [1, 2]
+    ctx = Context(*shape, lengths=lengths, precision=prec, bc=tuple(bc))
+    pshape = tuple(n if p_ else n - 1 for n, p_ in zip(shape, per))
+    for seed in (3, 4):
+        g = np.random.default_rng(seed).standard_normal(pshape)  # Fortran (x, y, z) values
+        rhs = torch.from_numpy(np.ascontiguousarray(g.transpose(2, 1, 0))).cuda()
+        ctx.poisson(rhs)
+        ctx.sync()
+        ref = oracle.poisson_bc(np.asfortranarray(g), lengths, per)
+        assert rel_err(to_host(rhs), ref) < 1e-12, (shape, per, seed)
     ctx.close()

@@ -885,12 +885,11 @@ int x3d_poisson(x3d_ctx ctx, double *rhs)
 {
     int rc = check_ctx(ctx);
     if (rc) return rc;
-    if ((rc = need_periodic(ctx))) return rc;
     if (!rhs) return set_error(ctx, X3D_EINVAL, "null field");
     Stager sg(ctx);
-    double *d = static_cast<double *>(sg.inout(rhs, ctx->npts() * sizeof(double)));
+    double *d = static_cast<double *>(sg.inout(rhs, ctx->ppts() * sizeof(double)));
     if (sg.status()) return sg.status();
-    return sg.finish(poisson_solve(ctx, d));
+    return sg.finish(ctx->periodic_all ? poisson_solve(ctx, d) : poisson_solve_mirror(ctx, d));
 }
 
 int x3d_poisson_zpencil(x3d_ctx ctx, void *spec, int nxh_loc, int i0, int ny_loc, int j0)

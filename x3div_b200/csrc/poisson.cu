@@ -16,6 +16,7 @@
 // waves :534-538, :568-572), so every mode of the x-halved spectrum gets
 // bit-for-bit the K value the reference uses for the same or the conjugate
 // mode, and the mask makes the same decisions.
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -521,8 +522,98 @@ int poisson_zpencil(x3d_ctx_s *ctx, void *spec, int nxl, int i0, int ny_loc, int
     return X3D_OK;
 }
 
+// ---- non-periodic directions ------------------------------------------------
+//
+// decomp_2d_poisson_init gives the pressure bc = 1 along every non-periodic
+// direction (src/poisson.f90:85-99, m = n - 1 pressure points,
+// :114-117) and tabulates that case in waves() (:539-553, :573-588,
+// :603-613): the cosine modes i = 0 .. m of w = pi i / m, i.e. homogeneous
+// Neumann conditions at the walls, half a cell beyond the first and last
+// pressure points.  x3div stops there (:104-108).  Here the solve is the
+// periodic one on the box mirrored about both walls of each such direction
+// (2 m points over twice the length): the mirrored field is even about the
+// walls, so it holds exactly those cosine modes, whose modified wavenumbers
+// on the doubled grid (w = 2 pi i / 2m, spacing 2L / 2m) are waves()'s bc = 1
+// values, and the periodic solution is even too; its first m points are
+// the solution.  The periodic solve is the library's (cuFFT 2-D transforms
+// and the fused z kernel); mirroring and cutting back are one pass each.
+
+// ext (Mx, My, Mz) from p (mx, my, mz): M = 2m along a mirrored direction,
+// M = m otherwise.
+__global__ void k_mirror_extend(double *__restrict__ ext, const double *__restrict__ p, int mx, int my, int mz,
+                                int Mx, int My, int Mz)
+{
+    const size_t total = (size_t)Mx * My * Mz;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const int X = (int)(e % Mx);
+        const size_t t = e / Mx;
+        const int Y = (int)(t % My), Z = (int)(t / My);
+        const int i = X < mx ? X : 2 * mx - 1 - X;
+        const int j = Y < my ? Y : 2 * my - 1 - Y;
+        const int k = Z < mz ? Z : 2 * mz - 1 - Z;
+        ext[e] = p[(size_t)i + (size_t)mx * ((size_t)j + (size_t)my * k)];
+    }
+}
+
+// p (mx, my, mz) = the first m points of ext along each direction.
+__global__ void k_mirror_restrict(double *__restrict__ p, const double *__restrict__ ext, int mx, int my, int mz,
+                                  int Mx, int My)
+{
+    const size_t total = (size_t)mx * my * mz;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(e % mx);
+        const size_t t = e / mx;
+        const int j = (int)(t % my), k = (int)(t / my);
+        p[e] = ext[(size_t)i + (size_t)Mx * ((size_t)j + (size_t)My * k)];
+    }
+}
+
+int poisson_solve_mirror(x3d_ctx_s *ctx, double *rhs)
+{
+    const TraceRange trace("poisson (mirrored)");
+    int m[3], M[3];
+    double len[3] = {ctx->xlx, ctx->yly, ctx->zlz};
+    for (int d = 0; d < 3; ++d) {
+        m[d] = ctx->pdim(d);
+        const bool per = ctx->ncl[2 * d] == 0 && ctx->ncl[2 * d + 1] == 0;
+        M[d] = per ? m[d] : 2 * m[d];
+        if (!per) len[d] *= 2.0;
+    }
+    if (!ctx->mirror) {
+        x3d_ctx_s *mc = nullptr;
+        const int rc = x3d_ctx_create(&mc, M[0], M[1], M[2], len[0], len[1], len[2], X3D_F64, ctx->device);
+        if (rc) return set_error(ctx, rc, "the mirrored box's periodic context could not be made (mirrored "
+                                          "lengths must be at least 8 points)");
+        ctx->mirror = mc;
+    }
+    if (!ctx->mirror_rhs &&
+        cudaMalloc(&ctx->mirror_rhs, sizeof(double) * (size_t)M[0] * M[1] * M[2]) != cudaSuccess) {
+        ctx->mirror_rhs = nullptr;
+        return set_error(ctx, X3D_ENOMEM, "mirrored right-hand side allocation failed");
+    }
+    x3d_ctx_s *mc = ctx->mirror;
+    mc->stream = ctx->stream;  // the mirrored solve runs in order with the caller's work
+    const size_t total = (size_t)M[0] * M[1] * M[2];
+    const unsigned grid = (unsigned)std::min<size_t>((total + 255) / 256, (size_t)ctx->num_sms * 8);
+    ++ctx->launches;
+    k_mirror_extend<<<grid, 256, 0, ctx->stream>>>(ctx->mirror_rhs, rhs, m[0], m[1], m[2], M[0], M[1], M[2]);
+    int rc = cuda_check(ctx, cudaGetLastError(), "k_mirror_extend");
+    if (rc) return rc;
+    const unsigned long long l0 = mc->launches;
+    rc = poisson_solve(mc, ctx->mirror_rhs);
+    ctx->launches += mc->launches - l0;
+    if (rc) return set_error(ctx, rc, mc->last_error);
+    ++ctx->launches;
+    k_mirror_restrict<<<grid, 256, 0, ctx->stream>>>(rhs, ctx->mirror_rhs, m[0], m[1], m[2], M[0], M[1]);
+    return cuda_check(ctx, cudaGetLastError(), "k_mirror_restrict");
+}
+
 void poisson_free(x3d_ctx_s *ctx)
 {
+    if (ctx->mirror) x3d_ctx_destroy(ctx->mirror);
+    ctx->mirror = nullptr;
+    if (ctx->mirror_rhs) cudaFree(ctx->mirror_rhs);
+    ctx->mirror_rhs = nullptr;
     if (ctx->plans_ready) {
         cufftDestroy(ctx->plan_d2z);
         cufftDestroy(ctx->plan_z2d);

@@ -117,6 +117,10 @@ struct x3d_ctx_s {
     bool zblk_ready = false;
     int zblk_nxl = 0, zblk_nyl = 0;
     void *spectrum = nullptr;  // complex double, nz * ny * (nx/2+1)
+    // non-periodic directions: the periodic context of the box mirrored about
+    // its walls, and the mirrored right-hand side (created on first use)
+    x3d_ctx_s *mirror = nullptr;
+    double *mirror_rhs = nullptr;
     double *d_k2x = nullptr, *d_tx = nullptr, *d_k2y = nullptr, *d_ty = nullptr, *d_k2z = nullptr,
            *d_tz = nullptr;
     // scratch fields owned by the context (sized nx*ny*nz elements)
@@ -154,6 +158,13 @@ struct x3d_ctx_s {
     int last_cfg = -1;                // configuration of the last line-solve launch (x3d_ctx_last_kernel)
     size_t elem() const { return precision == X3D_F32 ? 4 : 8; }
     size_t npts() const { return (size_t)nx * ny * nz; }
+    // points of the pressure grid: n - 1 along a non-periodic direction
+    int pdim(int d) const
+    {
+        const int n = d == 0 ? nx : (d == 1 ? ny : nz);
+        return ncl[2 * d] == 0 && ncl[2 * d + 1] == 0 ? n : n - 1;
+    }
+    size_t ppts() const { return (size_t)pdim(0) * pdim(1) * pdim(2); }
 };
 
 namespace x3d {
@@ -232,6 +243,9 @@ int reduce_absmax_mean(x3d_ctx_s *ctx, const double *p, size_t n, double *out);
 // ---- Poisson (poisson.cu) ------------------------------------------------
 int poisson_setup(x3d_ctx_s *ctx);
 int poisson_solve(x3d_ctx_s *ctx, double *rhs);
+// the solve with homogeneous Neumann conditions along the non-periodic
+// directions, rhs on the pressure grid (ppts points)
+int poisson_solve_mirror(x3d_ctx_s *ctx, double *rhs);
 void poisson_free(x3d_ctx_s *ctx);
 
 // ---- helpers (capi.cpp) --------------------------------------------------
