@@ -142,6 +142,8 @@ int make_jobs(x3d_batch_s *b, std::vector<BatchJob<T>> &jobs, size_t *tile_cap_o
                 const int xs = L_force > 0 ? x_force : b->choice_X[sd];
                 size_t tb = 0;
                 if (plan_batch_job<T>(J, L, w, xs, &tb)) {
+                    // one box shape's operators along d at one chunk length
+                    J.rclass = sd * 2 + (J.L == kChunkLong<T> ? 0 : 1);
                     J.tile0 = tiles;
                     tiles += J.ntiles;
                     tile_cap = std::max(tile_cap, tb);

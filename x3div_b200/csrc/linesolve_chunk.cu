@@ -1609,14 +1609,22 @@ __device__ __forceinline__ void batch_item(const BatchJob<T> &J, const T *tile, 
 // its x outputs straight out; kBatchMixed takes each job's chunk length;
 // kBatchStaged also stages the x outputs of jobs with xstage set.  The
 // narrower variants carry less code and no staging rows.
+// Bytes of a job's header (every field before its responses), in 16-byte units.
+template <typename T>
+constexpr int kBatchHdrVecs = (int)((offsetof(BatchJob<T>, resp) + 15) / 16);
+
 template <typename T, int VAR>
 __global__ void __launch_bounds__(kBatchThreads, 2)
     ls_batch(const BatchJob<T> *__restrict__ jobs, int njobs, long total,
              unsigned long long *counter, size_t tile_cap, int *err)
 {
+    static_assert(kBatchHdrVecs<T> <= kBatchThreads, "one 16-byte copy per thread");
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ uint64_t bars[2];
     __shared__ long s_item;
+    __shared__ int s_job;  // the job of s_item
+    // the headers of the current and the next item's jobs, by iteration parity
+    __shared__ __align__(64) uint4 s_hdr[2][kBatchHdrVecs<T>];
     const int t = threadIdx.x;
     // two staging slots of tile_cap bytes, then the carry scratch and the
     // carry responses of the item's operators
@@ -1634,9 +1642,9 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
         }
         return lo;
     };
-    // The copies of one work item into staging slot `slot` (one thread).
-    auto issue = [&](long item, int slot) {
-        const BatchJob<T> &J = jobs[job_of(item)];
+    // The copies of one work item of job jb into staging slot `slot` (one thread).
+    auto issue = [&](long item, int jb, int slot) {
+        const BatchJob<T> &J = jobs[jb];
         const long tl = item - J.tile0;
         T *tile = reinterpret_cast<T *>(smem_raw + slot * tile_cap);
         uint64_t *bar = &bars[slot];
@@ -1660,32 +1668,29 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
             }
         }
     };
+    // every thread copies at most one 16-byte piece of job jb's header
+    auto copy_header = [&](int jb, int hs) {
+        if (t < kBatchHdrVecs<T>) s_hdr[hs][t] = reinterpret_cast<const uint4 *>(jobs + jb)[t];
+    };
     if (t == 0) {
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
         fence_mbar_init();
         s_item = (long)atomicAdd(counter, 1ull);
-        if (s_item < total) issue(s_item, 0);
+        if (s_item < total) {
+            s_job = job_of(s_item);
+            issue(s_item, s_job, 0);
+        }
     }
     __syncthreads();
+    if (s_item < total) copy_header(s_job, 0);
     uint32_t phases = 0;  // bit s: parity of slot s's next completion
+    int resp_have = -1;   // the response class in resp_s (the same in every thread)
     for (int it = 0;; ++it) {
         const int slot = it & 1;
         const long item = s_item;  // claimed during the previous item (or above)
         if (item >= total) break;
-        const BatchJob<T> &J = jobs[job_of(item)];
-        const long tl = item - J.tile0;
-        const int W = J.W, C = J.C, n = J.n;
-        const int dir = J.dir;
-        long l0 = 0;
-        int rows = W, x0 = 0, o = 0;
-        if (dir == DX) {
-            l0 = tl * W;
-            rows = (int)min((long)W, J.span - l0);
-        } else {
-            x0 = (int)(tl % J.span) * W;
-            o = (int)(tl / J.span);
-        }
+        const int jb = s_job;
         unsigned char *tbase = smem_raw + slot * tile_cap;
         const T *tile = reinterpret_cast<const T *>(tbase);
         const uint32_t parity = (phases >> slot) & 1u;
@@ -1697,24 +1702,49 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
             return;
         }
         phases ^= 1u << slot;
-        // every thread is done with the previous item (its responses are read
-        // after its last barrier, its tile before): this item's responses go
-        // in place, and the next item, claimed now, is copied into the other
-        // slot while this one is solved
+        // The job's header, copied during the previous item (or above) and
+        // ordered by the barrier just passed.  Every thread is done with the
+        // previous item (its responses are read after its last barrier, its
+        // tile and header before): this item's responses go in place, and the
+        // next item, claimed now, is copied into the other slot while this
+        // one is solved.
+        const BatchJob<T> &J = *reinterpret_cast<const BatchJob<T> *>(s_hdr[slot]);
+        const long tl = item - J.tile0;
+        const int W = J.W, n = J.n;
+        const int dir = J.dir;
+        long l0 = 0;
+        int rows = W, x0 = 0, o = 0;
+        if (dir == DX) {
+            l0 = tl * W;
+            rows = (int)min((long)W, J.span - l0);
+        } else {
+            x0 = (int)(tl % J.span) * W;
+            o = (int)(tl / J.span);
+        }
         const int L = VAR == kBatchLong ? kChunkLong<T> : J.L;
-        for (int i = t; i < J.nops * 4 * L; i += kBatchThreads) {
-            const int k = i / (4 * L), rem = i - k * 4 * L, a = rem / L, j = rem - a * L;
-            resp_s[i] = J.resp[k][a][j];
+        if (J.rclass != resp_have) {  // consecutive items mostly share a job, so this is rare
+            const T *resp_g = &jobs[jb].resp[0][0][0];
+            for (int i = t; i < J.nops * 4 * L; i += kBatchThreads) {
+                const int k = i / (4 * L), rem = i - k * 4 * L, a = rem / L, j = rem - a * L;
+                resp_s[i] = resp_g[(k * 4 + a) * kChunkLong<T> + j];
+            }
+            resp_have = J.rclass;
         }
         if (t == 0) {
             const long next = (long)atomicAdd(counter, 1ull);
             s_item = next;
-            if (next < total) issue(next, slot ^ 1);
+            if (next < total) {
+                const int nj = job_of(next);
+                s_job = nj;
+                issue(next, nj, slot ^ 1);
+            }
         }
         if (dir == DX) fill_halos_x<T>(tbase, 0, 1, rows, J.pitch, n);
         else fill_halos_yz<T>(tbase, 0, 1, n, W, J.halo);
         fence_proxy_async_smem();  // copies into this slot two items later overwrite the halos
         __syncthreads();
+        // the next item's header into the other slot, read after the next wait barrier
+        if (s_item < total) copy_header(s_job, slot ^ 1);
         constexpr bool XS = VAR == kBatchStaged;
         if (VAR == kBatchLong || J.L == kChunkLong<T>)
             batch_item<T, kChunkLong<T>, XS>(J, tile, out_s, resp_s, scf, t, l0, rows, x0, o);

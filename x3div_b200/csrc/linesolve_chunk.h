@@ -86,16 +86,20 @@ struct BatchJob {
     int kind[kMaxStageOps];
     int nops, dir, n, nx, ny, nz;
     int L;       // chunk length (kChunkLong or kChunkShort of T)
+    int rclass;  // jobs with equal rclass have equal responses (same operators, line length and L)
     int xstage;  // x jobs: outputs staged in shared-memory rows, bulk row copies
     int W, C, box_n, nbox, pitch;
     int halo;    // y/z: staged rows in front of the line (periodic halo + alignment)
     long span;   // x: number of lines; y/z: tiles across x
     long tile0;  // first work item of the job
     long ntiles;
-    // carry responses of each operator for the batch's chunk length (as
-    // StageOp::resp and StageOp::keep; set by plan_batch_job)
-    T resp[kMaxStageOps][4][kChunkLong<T>];
+    // the entries of each operator's responses the fixes use (as
+    // StageOp::keep; set by plan_batch_job)
     int keep[kMaxStageOps];
+    // carry responses of each operator for the job's chunk length (as
+    // StageOp::resp).  Everything before them is the job's header, which the
+    // kernel copies to shared memory once per work item.
+    T resp[kMaxStageOps][4][kChunkLong<T>];
 };
 
 // Chooses tiling for the job (chunk length L, kChunkLong or kChunkShort of
