@@ -1595,10 +1595,18 @@ __device__ __forceinline__ void batch_item(const BatchJob<T> &J, const T *tile, 
                                          q, J.keep[k]);
             if (live) {
                 T *dst = J.out[k] + obase;
+                if (nv == L) {  // every chunk but a short last one: no per-point test
 #pragma unroll
-                for (int j = 0; j < L; ++j) {
-                    if (j < nv) *dst = r[j];
-                    dst += ostride;
+                    for (int j = 0; j < L; ++j) {
+                        *dst = r[j];
+                        dst += ostride;
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < L; ++j) {
+                        if (j < nv) *dst = r[j];
+                        dst += ostride;
+                    }
                 }
             }
         }
