@@ -198,9 +198,14 @@ struct ZLines {
 
 // One Stockham stage of radix R over sub-transforms of size NS, for the W
 // lines of the tile (element e of line l at buf[e W + l]).  SRC_G: read the
-// lines from global memory; DST_G: write them to global memory; SCALE:
-// divide each mode as it is written.
-template <int N, int R, int NS, int W, bool INV, bool SRC_G, bool DST_G, bool SCALE>
+// lines from global memory; DST_G: write them to global memory.  FUSE (the
+// forward transform's last stage, NS = N / R): divide each mode, then run
+// the inverse transform's first stage in registers -- with the inverse's
+// radices in reverse order that stage has the same radix, reads exactly the
+// values this thread holds (positions j + q N / R) with unit twiddles, and
+// writes positions j R + q -- so the modes make one shared-memory pass
+// fewer.
+template <int N, int R, int NS, int W, bool INV, bool SRC_G, bool DST_G, bool FUSE>
 __device__ __forceinline__ void zft_stage(double2 *buf, const double2 *tw, const ZLines &zl)
 {
     constexpr int MB = kZftVals / R;
@@ -234,6 +239,13 @@ __device__ __forceinline__ void zft_stage(double2 *buf, const double2 *tw, const
             dft<R, INV>(v[s]);
             dk[s] = (j / NS) * NS * R + jm;
             dl[s] = l;
+            if constexpr (FUSE) {
+                static_assert(NS * R == N, "the fused stage is the forward transform's last");
+#pragma unroll
+                for (int q = 0; q < R; ++q) v[s][q] = zl.divide(v[s][q], dk[s] + q * NS, l);
+                dft<R, true>(v[s]);
+                dk[s] = j * R;  // the inverse's first stage (sub-transforms of size 1) writes j R + q
+            }
         }
     }
     if constexpr (!SRC_G && !DST_G) __syncthreads();  // in place in shared memory
@@ -243,11 +255,9 @@ __device__ __forceinline__ void zft_stage(double2 *buf, const double2 *tw, const
         if (b < NB) {
 #pragma unroll
             for (int q = 0; q < R; ++q) {
-                const int k = dk[s] + q * NS, l = dl[s];
+                const int k = dk[s] + q * (FUSE ? 1 : NS), l = dl[s];
                 if constexpr (DST_G) {
                     if (l < zl.lines) zl.base[(size_t)k * zl.zstride + l] = v[s][q];
-                } else if constexpr (SCALE) {
-                    buf[k * W + l] = zl.divide(v[s][q], k, l);
                 } else {
                     buf[k * W + l] = v[s][q];
                 }
@@ -257,12 +267,14 @@ __device__ __forceinline__ void zft_stage(double2 *buf, const double2 *tw, const
     if constexpr (!DST_G) __syncthreads();
 }
 
-// Radices of a length-N transform: 8s, 4, 2, then 3s.
+// Radices of a length-N transform: 8s, 4, 2, then 3s (the inverse
+// transform takes them in reverse order: a Stockham sequence may run its
+// radices in any order).
 struct RadixSeq {
     int count;
     int r[10];
 };
-constexpr RadixSeq radix_seq(int n)
+constexpr RadixSeq radix_seq(int n, bool reversed = false)
 {
     RadixSeq s{0, {}};
     int m = n;
@@ -270,21 +282,35 @@ constexpr RadixSeq radix_seq(int n)
     while (m % 4 == 0) s.r[s.count++] = 4, m /= 4;
     while (m % 2 == 0) s.r[s.count++] = 2, m /= 2;
     while (m % 3 == 0) s.r[s.count++] = 3, m /= 3;
+    if (reversed)
+        for (int a = 0, b = s.count - 1; a < b; ++a, --b) {
+            const int t = s.r[a];
+            s.r[a] = s.r[b];
+            s.r[b] = t;
+        }
     return s;
 }
 
-// The forward transform reads the lines from global memory in its first
-// stage and divides the modes in its last; the inverse one writes them back
-// to global memory in its last stage.
+// The z transform, division and inverse of a tile.  The forward transform
+// reads the lines from global memory in its first stage; its last stage
+// divides the modes and runs the inverse's first stage in registers (the
+// inverse takes the radices in reverse order); the inverse writes the
+// lines back to global memory in its last stage, which is that fused stage
+// itself when the length has a single radix.
 template <int N, int W, bool INV, int ST = 0, int NS = 1>
 __device__ __forceinline__ void zft(double2 *buf, const double2 *tw, const ZLines &zl)
 {
-    constexpr RadixSeq seq = radix_seq(N);
+    constexpr RadixSeq seq = radix_seq(N, INV);
     if constexpr (ST < seq.count) {
         constexpr int R = seq.r[ST];
         constexpr bool last = ST + 1 == seq.count;
-        zft_stage<N, R, NS, W, INV, !INV && ST == 0, INV && last, !INV && last>(buf, tw, zl);
-        zft<N, W, INV, ST + 1, NS * R>(buf, tw, zl);
+        if constexpr (!INV && last) {
+            zft_stage<N, R, NS, W, false, ST == 0, seq.count == 1, true>(buf, tw, zl);
+            zft<N, W, true, 1, R>(buf, tw, zl);  // the inverse from its second stage
+        } else {
+            zft_stage<N, R, NS, W, INV, !INV && ST == 0, INV && last, false>(buf, tw, zl);
+            zft<N, W, INV, ST + 1, NS * R>(buf, tw, zl);
+        }
     }
 }
 
@@ -330,8 +356,7 @@ __global__ void __launch_bounds__(kZftThreads, 2)
         xtab[threadIdx.x] = make_double2(__ldg(tx + i), __ldg(k2x + i));
     }
     __syncthreads();
-    zft<N, W, false>(zbuf, tws, zl);
-    zft<N, W, true>(zbuf, tws, zl);
+    zft<N, W, false>(zbuf, tws, zl);  // and the inverse, from its fused first stage
 }
 
 // The z lengths with a fused kernel.
