@@ -7,6 +7,10 @@ non-zero status to decomp_2d_abort (the reference's error path).
 Run after changing the header:  python fortran/gen_bind.py
 tests/test_capi_abi.py checks that the committed module matches the header.
 
+The structs the header defines by value (x3d_work, x3d_box, x3d_block)
+become bind(C) derived types with the same members in the same order; the
+entry points take them by address (c_loc of an array of them).
+
 Type mapping: handles (x3d_ctx, x3d_op, x3d_batch) and field or array
 pointers pass by value as type(c_ptr) -- c_loc of a target array, or a
 device address under !$acc host_data use_device; arrays of field pointers
@@ -26,7 +30,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 HEADER = os.path.join(os.path.dirname(HERE), "include", "x3d_b200.h")
 OUT = os.path.join(HERE, "x3d_b200_bind.f90")
 
-RENAME = {"precision": "prec", "kind": "op_kind", "count": "cnt", "value": "val", "in": "src"}
+RENAME = {"precision": "prec", "kind": "op_kind", "count": "cnt", "value": "val", "in": "src", "out": "dst"}
 ARRAY_INTS = {"ncl", "dims", "meta"}  # int * parameters that carry several values
 KIND_ORDER = ["c_ptr", "c_int", "c_double", "c_size_t", "c_long_long", "c_char"]
 
@@ -45,6 +49,34 @@ def declarations(text):
 
 def constants(text):
     return re.findall(r"^#define\s+(X3D_\w+)\s+(-?\d+)\b", text, re.M)
+
+
+STRUCT_FIELD = {"int": "integer(c_int)", "long long": "integer(c_long_long)", "double": "real(c_double)",
+                "x3d_op": "type(c_ptr)", "void *": "type(c_ptr)", "const void *": "type(c_ptr)"}
+
+
+def structs(text):
+    """(name, [(Fortran declaration, member)]) of every struct the header
+    defines by value (typedef struct [tag] { ... } name;), members in order."""
+    out = []
+    for body, name in re.findall(r"^typedef struct(?: \w+)? \{(.*?)\} (x3d_\w+);", text, re.M | re.S):
+        body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+        fields = []
+        for decl in (d.strip() for d in body.split(";") if d.strip()):
+            m = re.match(r"((?:const )?[a-z_0-9 ]+?\s*\*?)\s*(\w+(?:\s*,\s*\w+)*)$", " ".join(decl.split()))
+            ctype = " ".join(m.group(1).split())
+            for member in (x.strip() for x in m.group(2).split(",")):
+                fields.append((STRUCT_FIELD[ctype], member))
+        out.append((name, fields))
+    return out
+
+
+def derived_type(name, fields):
+    """A bind(C) derived type with the struct's layout (members in order)."""
+    lines = [f"  type, bind(C) :: {name}"]
+    lines += [f"     {ft} :: {RENAME.get(m, m)}" for ft, m in fields]
+    lines.append(f"  end type {name}")
+    return lines
 
 
 def fortran_type(ctype, pname):
@@ -112,6 +144,9 @@ def generate(text):
            ""]
     for name, val in constants(text):
         out.append(f"  integer(c_int), parameter :: {name} = {val}")
+    out += ["", "  ! the structs the entry points take by address (pass c_loc of an array of them)"]
+    for name, fields in structs(text):
+        out += derived_type(name, fields)
     out += ["",
             "  ! the context the re-pointed routines use (x3d_b200_derive.f90)",
             "  type(c_ptr), save :: x3d_ctx = c_null_ptr",

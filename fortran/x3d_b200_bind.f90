@@ -46,6 +46,32 @@ module x3d_b200_bind
   integer(c_int), parameter :: X3D_OP_COUNT = 21
   integer(c_int), parameter :: X3D_NOALLOC_MAX_POINTS = 262144
 
+  ! the structs the entry points take by address (pass c_loc of an array of them)
+  type, bind(C) :: x3d_work
+     type(c_ptr) :: op
+     type(c_ptr) :: src
+     type(c_ptr) :: dst
+  end type x3d_work
+  type, bind(C) :: x3d_box
+     integer(c_int) :: nx
+     integer(c_int) :: ny
+     integer(c_int) :: nz
+     real(c_double) :: xlx
+     real(c_double) :: yly
+     real(c_double) :: zlz
+  end type x3d_box
+  type, bind(C) :: x3d_block
+     integer(c_long_long) :: src_offset
+     integer(c_long_long) :: dst_offset
+     integer(c_int) :: nx
+     integer(c_int) :: ny
+     integer(c_int) :: nz
+     integer(c_long_long) :: src_ystride
+     integer(c_long_long) :: src_zstride
+     integer(c_long_long) :: dst_ystride
+     integer(c_long_long) :: dst_zstride
+  end type x3d_block
+
   ! the context the re-pointed routines use (x3d_b200_derive.f90)
   type(c_ptr), save :: x3d_ctx = c_null_ptr
 
@@ -532,36 +558,36 @@ module x3d_b200_bind
        integer(c_int), value :: ny
        integer(c_int), value :: nz
      end function
-     integer(c_int) function x3d_transpose_x_to_y(ctx, src, out, is_complex) bind(C, &
+     integer(c_int) function x3d_transpose_x_to_y(ctx, src, dst, is_complex) bind(C, &
           name="x3d_transpose_x_to_y")
        import :: c_ptr, c_int
        type(c_ptr), value :: ctx
        type(c_ptr), value :: src
-       type(c_ptr), value :: out
+       type(c_ptr), value :: dst
        integer(c_int), value :: is_complex
      end function
-     integer(c_int) function x3d_transpose_y_to_z(ctx, src, out, is_complex) bind(C, &
+     integer(c_int) function x3d_transpose_y_to_z(ctx, src, dst, is_complex) bind(C, &
           name="x3d_transpose_y_to_z")
        import :: c_ptr, c_int
        type(c_ptr), value :: ctx
        type(c_ptr), value :: src
-       type(c_ptr), value :: out
+       type(c_ptr), value :: dst
        integer(c_int), value :: is_complex
      end function
-     integer(c_int) function x3d_transpose_z_to_y(ctx, src, out, is_complex) bind(C, &
+     integer(c_int) function x3d_transpose_z_to_y(ctx, src, dst, is_complex) bind(C, &
           name="x3d_transpose_z_to_y")
        import :: c_ptr, c_int
        type(c_ptr), value :: ctx
        type(c_ptr), value :: src
-       type(c_ptr), value :: out
+       type(c_ptr), value :: dst
        integer(c_int), value :: is_complex
      end function
-     integer(c_int) function x3d_transpose_y_to_x(ctx, src, out, is_complex) bind(C, &
+     integer(c_int) function x3d_transpose_y_to_x(ctx, src, dst, is_complex) bind(C, &
           name="x3d_transpose_y_to_x")
        import :: c_ptr, c_int
        type(c_ptr), value :: ctx
        type(c_ptr), value :: src
-       type(c_ptr), value :: out
+       type(c_ptr), value :: dst
        integer(c_int), value :: is_complex
      end function
      integer(c_int) function x3d_copy_blocks(ctx, dst, src, elem_bytes, blocks, cnt) bind(C, &
@@ -647,11 +673,11 @@ module x3d_b200_bind
        type(c_ptr), value :: uy1
        type(c_ptr), value :: uz1
      end function
-     integer(c_int) function x3d_div_stats(ctx, pp3, out) bind(C, name="x3d_div_stats")
+     integer(c_int) function x3d_div_stats(ctx, pp3, dst) bind(C, name="x3d_div_stats")
        import :: c_ptr, c_int
        type(c_ptr), value :: ctx
        type(c_ptr), value :: pp3
-       type(c_ptr), value :: out
+       type(c_ptr), value :: dst
      end function
      integer(c_int) function x3d_momentum_rhs_eq(ctx, dux1, duy1, duz1, ux1, uy1, uz1) bind(C, &
           name="x3d_momentum_rhs_eq")
@@ -726,23 +752,23 @@ module x3d_b200_bind
        integer(c_int), value :: ny
        integer(c_int), value :: nz
      end function
-     integer(c_int) function x3d_divergence_part(ctx, dir, out, src, nx, ny, nz) bind(C, &
+     integer(c_int) function x3d_divergence_part(ctx, dir, dst, src, nx, ny, nz) bind(C, &
           name="x3d_divergence_part")
        import :: c_ptr, c_int
        type(c_ptr), value :: ctx
        integer(c_int), value :: dir
-       type(c_ptr) :: out(*)
+       type(c_ptr) :: dst(*)
        type(c_ptr) :: src(*)
        integer(c_int), value :: nx
        integer(c_int), value :: ny
        integer(c_int), value :: nz
      end function
-     integer(c_int) function x3d_gradp_part(ctx, dir, out, src, ucor, nx, ny, nz) bind(C, &
+     integer(c_int) function x3d_gradp_part(ctx, dir, dst, src, ucor, nx, ny, nz) bind(C, &
           name="x3d_gradp_part")
        import :: c_ptr, c_int
        type(c_ptr), value :: ctx
        integer(c_int), value :: dir
-       type(c_ptr) :: out(*)
+       type(c_ptr) :: dst(*)
        type(c_ptr) :: src(*)
        type(c_ptr) :: ucor(*)
        integer(c_int), value :: nx

@@ -78,6 +78,27 @@ def test_fortran_interface_module_matches_header():
         assert gen_bind.generate(f.read()) == module, "fortran/x3d_b200_bind.f90 is stale: run fortran/gen_bind.py"
 
 
+def test_fortran_derived_types_have_the_c_layouts():
+    """The bind(C) derived types of the module list the C structs' members in
+    order with types of the same size, so an array of them has the C
+    layout: checked against the ctypes mirrors the Python binding uses."""
+    import ctypes as C
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, os.path.join(root, "fortran"))
+    import gen_bind
+    with open(os.path.join(root, "include", "x3d_b200.h")) as f:
+        types = dict(gen_bind.structs(f.read()))
+    size = {"integer(c_int)": 4, "integer(c_long_long)": 8, "real(c_double)": 8, "type(c_ptr)": 8}
+    mirrors = {"x3d_box": _capi.Box, "x3d_work": _capi.Work, "x3d_block": _capi.Block}
+    assert set(types) == set(mirrors)
+    for name, fields in types.items():
+        cfields = mirrors[name]._fields_
+        assert len(fields) == len(cfields), name
+        for (ft, _member), (_cname, ctype) in zip(fields, cfields):
+            assert size[ft] == C.sizeof(ctype), (name, ft, ctype)
+
+
 # The reference's staggered routines and their dummy arguments, in order
 # (src/x3d_staggered.f90:23-1233), and the abstract derivative interfaces
 # (src/x3d_derive.f90:19-52) the re-pointed wrappers must keep.
