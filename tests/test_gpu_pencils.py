@@ -320,3 +320,40 @@ def test_step_parts_on_every_rank_pencil(oracle, torch_cuda, prec, grid, shape):
     # copies) and FP32 x lines of 30 points are refused
     assert (refused > 0) == (shape[0] == 30), refused
     ctx.close()
+
+
+def test_pencil_entry_points_refuse_bad_arguments(torch_cuda):
+    """x3d_copy_blocks and the step parts check their arguments before
+    launching anything: element sizes, negative offsets or strides, host
+    arrays, directions, and pencils whose lines along their direction are
+    not whole; the context keeps working afterwards."""
+    torch = torch_cuda
+    from x3div_b200 import Context, X3DError
+    from x3div_b200._capi import X3D_EINVAL
+    ctx = Context(16, 12, 10, precision="f32")
+    a = torch.zeros(10, 12, 16, device="cuda")
+    b = torch.zeros_like(a)
+    good = (0, 0, 16, 12, 10, 16, 192, 16, 192)
+    for elem, box in ((12, good), (4, (-1,) + good[1:]), (4, good[:5] + (-16,) + good[6:])):
+        with pytest.raises(X3DError) as e:
+            ctx.copy_blocks(b, a, elem, [box])
+        assert e.value.code == X3D_EINVAL
+    host = torch.zeros(10, 12, 16)
+    with pytest.raises(X3DError):
+        ctx.copy_blocks(b, host, 4, [good])
+    u = [torch.zeros(10, 12, 16, device="cuda") for _ in range(3)]
+    du = [torch.empty_like(u[0]) for _ in range(3)]
+    with pytest.raises(X3DError):
+        ctx.transeq_part(3, du, u, None, None, 0.0, (16, 12, 10))  # no fourth direction
+    with pytest.raises(X3DError):
+        ctx.transeq_part(0, du, u, None, None, 0.0, (15, 12, 10))  # x lines cut short
+    with pytest.raises(X3DError):
+        ctx.divergence_part(1, du[:2], u, (16, 13, 10))  # extents outside the box
+    with pytest.raises(X3DError):
+        ctx.gradp_part(0, du, [host, host, host], None, (16, 12, 10))  # host arrays
+    # still usable: a valid copy and a valid part
+    ctx.copy_blocks(b, a, 4, [good])
+    ctx.transeq_part(0, du, u, None, None, 0.0, (16, 12, 10))
+    ctx.sync()
+    assert torch.equal(b, a)
+    ctx.close()
