@@ -271,6 +271,8 @@ def _transpose(t, pc: Pencils, kind, src_pencil, ctx=None, out=None):
     import torch
     L = pc.layout
     rest = _check(t, pc, src_pencil)
+    if out is not None and (out.dtype != t.dtype or out.device != t.device):
+        raise ValueError(f"output pencil is {out.dtype} on {out.device}, the input {t.dtype} on {t.device}")
     plan = plan_transpose(L, kind)
     if plan is None:
         if out is None or out is t:
