@@ -414,6 +414,13 @@ module x3d_b200_bind
        type(c_ptr), value :: items
        integer(c_int), value :: cnt
      end function
+     integer(c_int) function x3d_apply(ctx, op, src, dst) bind(C, name="x3d_apply")
+       import :: c_ptr, c_int
+       type(c_ptr), value :: ctx
+       type(c_ptr), value :: op
+       type(c_ptr), value :: src
+       type(c_ptr), value :: dst
+     end function
      integer(c_int) function x3d_autotune(ctx, max_group) bind(C, name="x3d_autotune")
        import :: c_ptr, c_int
        type(c_ptr), value :: ctx

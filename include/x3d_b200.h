@@ -254,6 +254,11 @@ typedef struct {
  * memory.  No reference counterpart: it replaces a sequence of der* and
  * staggered calls (src/transeq.f90, src/navier.f90) by one call. */
 int x3d_apply_batch(x3d_ctx ctx, const x3d_work *items, int count);
+/* One application out = op(in) on the context grid, whatever the operator's
+ * kind and direction: the work-list of one item.  No reference counterpart
+ * as a single routine: it stands for whichever der* or staggered routine
+ * the operator's kind and direction name. */
+int x3d_apply(x3d_ctx ctx, x3d_op op, const void *in, void *out);
 
 /* Times every kernel configuration (lines per CTA, chunk length, or one
  * thread per line) for each direction and for groups of 1, 2, 3 and 6

@@ -239,6 +239,12 @@ def test_grouped_batch_matches_single_calls(oracle, torch_cuda, contexts, prec, 
                 err = rel_err(to_host(outs[di][k]), oracle.apply(kind, di, used, d[di]))
                 assert err < tol, (cfg, di, kind, err)
     ctx.set_kernel(-1)
+    # x3d_apply: one application, the work-list of one item
+    for di in range(3):
+        one = torch.empty_like(u_d)
+        ctx.apply(ctx.op(names[di][2]), u_d, one)
+        ctx.sync()
+        assert rel_err(to_host(one), oracle.apply("dervp", di, used, d[di])) < tol, di
 
 
 def test_autotune_records_choices(torch_cuda, contexts):

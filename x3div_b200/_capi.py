@@ -62,6 +62,7 @@ SIGNATURES = {
     "x3d_derzpv": [_vp, _vp, _vp, _vp, _i, _i, _i, _i],
     "x3d_interzpv": [_vp, _vp, _vp, _vp, _i, _i, _i, _i],
     "x3d_apply_batch": [_vp, _vp, _i],
+    "x3d_apply": [_vp, _vp, _vp, _vp],
     "x3d_autotune": [_vp, _i],
     "x3d_ctx_set_kernel": [_vp, _i],
     "x3d_autotune_choice": [_vp, _i, _i, _ip],

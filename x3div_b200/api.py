@@ -258,6 +258,10 @@ class Context:
             arr[k].op, arr[k].in_, arr[k].out = op.handle, _ptr(src), _ptr(dst)
         self._check(self.L.x3d_apply_batch(self.handle, arr, len(items)))
 
+    def apply(self, op, src, dst):
+        """x3d_apply: dst = op(src) on the context grid."""
+        self._check(self.L.x3d_apply(self.handle, op.handle, _ptr(src), _ptr(dst)))
+
     def autotune(self, max_group=6):
         """Time the kernel configurations on this grid and keep the fastest."""
         self._check(self.L.x3d_autotune(self.handle, int(max_group)))

@@ -664,6 +664,12 @@ int x3d_interzpv(x3d_ctx ctx, void *tz, const void *uz, x3d_op op, int nx, int n
 
 // ---- batch ----------------------------------------------------------------------------
 
+int x3d_apply(x3d_ctx ctx, x3d_op op, const void *in, void *out)
+{
+    const x3d_work item{op, in, out};
+    return x3d_apply_batch(ctx, &item, 1);
+}
+
 int x3d_apply_batch(x3d_ctx ctx, const x3d_work *items, int count)
 {
     const TraceRange trace("apply_batch");
