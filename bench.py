@@ -263,17 +263,17 @@ def sweep_groups(ctx, fields, outs, fused):
     return groups
 
 
-# Lines per tile (W) of each chunked configuration (x3d_ctx_set_kernel 0..15
-# and 17; 16 is one thread per line).
-CONFIG_W = [16, 32, 16, 8, 32, 8, 16, 32, 16, 8, 32, 8, 32, 16, 32, 32, 1, 16]
+# Lines per tile (W) of each chunked configuration (x3d_ctx_set_kernel 0..15,
+# 17 and 18; 16 is one thread per line).
+CONFIG_W = [16, 32, 16, 8, 32, 8, 16, 32, 16, 8, 32, 8, 32, 16, 32, 32, 1, 16, 8]
 
 
 def config_pattern(cfg):
     """The roofline probe pattern with the access order of y/z configuration
     cfg: whole-line tiles of W columns, claimed in order from a counter by the
-    persistent configurations 6..15 and 17, one CTA per tile by the others."""
+    persistent configurations 6..15, 17 and 18, one CTA per tile by the others."""
     w = CONFIG_W[cfg] if 0 <= cfg < len(CONFIG_W) and cfg != 16 else 16
-    return f"claim_w{w}" if 6 <= cfg < 16 or cfg == 17 else f"tile_w{w}"
+    return f"claim_w{w}" if 6 <= cfg < 16 or cfg in (17, 18) else f"tile_w{w}"
 
 
 def pattern_ceilings(ctx, torch, src, outs):

@@ -1447,6 +1447,8 @@ static int launch_stage_sel(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir
     case 15: return launch_stage_cfg<T, 32, Lbig, true, 2>(ctx, prog, dir, nx, ny, nz);
     // 17: configuration 6 (y/z) compiled for three CTAs per SM (plain programs)
     case 17: return launch_stage_cfg<T, 16, Lbig, true, 1, 3>(ctx, prog, dir, nx, ny, nz);
+    // 18: configuration 9 (8 lines, long chunks, y/z) built for three CTAs per SM
+    case 18: return launch_stage_cfg<T, 8, Lbig, true, 1, 3>(ctx, prog, dir, nx, ny, nz);
     default: return X3D_EUNSUPPORTED;
     }
 }
