@@ -263,9 +263,9 @@ def sweep_groups(ctx, fields, outs, fused):
     return groups
 
 
-# Lines per tile (W) of each chunked configuration (x3d_ctx_set_kernel 0..15,
-# 17 and 18; 16 is one thread per line).
-CONFIG_W = [16, 32, 16, 8, 32, 8, 16, 32, 16, 8, 32, 8, 32, 16, 32, 32, 1, 16, 8]
+# Lines per tile (W) of each chunked configuration (x3d_ctx_set_kernel 0..15
+# and 17..19; 16 is one thread per line).
+CONFIG_W = [16, 32, 16, 8, 32, 8, 16, 32, 16, 8, 32, 8, 32, 16, 32, 32, 1, 16, 8, 8]
 
 
 def config_pattern(cfg):

@@ -1030,8 +1030,8 @@ __device__ __forceinline__ void fill_halos_x(unsigned char *base, size_t tile_by
     }
 }
 
-template <typename T, int W, int L, bool ACC, bool PERSIST>
-__global__ void __launch_bounds__(512, 1)
+template <typename T, int W, int L, bool ACC, bool PERSIST, int OCC = 1>
+__global__ void __launch_bounds__(OCC > 1 ? 256 : 512, OCC)
     ls_stage_x(const __grid_constant__ StageProgram<T> prog, long nlines, int pitch, size_t tile_bytes,
                long ntiles, unsigned long long *claim, int *err)
 {
@@ -1294,7 +1294,7 @@ static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog_in, int 
         const int C = (n + L - 1) / L;
         const int threads = C * W / PR;
         if (threads > kStageThreads<T, L, PR> || threads % 32) return X3D_EUNSUPPORTED;
-        if (OCC > 1 && (acc || dir == DX || threads > 256)) return X3D_EUNSUPPORTED;
+        if (OCC > 1 && (acc || threads > 256)) return X3D_EUNSUPPORTED;
         // FP64 inputs of an FP32 program: staged as FP64 by the plain,
         // unpaired y/z kernels only
         const bool in64 = prog.in_f64 != 0;
@@ -1329,7 +1329,9 @@ static int launch_stage_cfg(x3d_ctx_s *ctx, const StageProgram<T> &prog_in, int 
                                  ~(size_t)127) +
                                 (size_t)W * pitch * es;
             if (smem + 1024 > ctx->smem_optin) return X3D_EUNSUPPORTED;
-            auto kern = acc ? ls_stage_x<T, W, L, true, PERSIST> : ls_stage_x<T, W, L, false, PERSIST>;
+            auto kern = ls_stage_x<T, W, L, false, PERSIST, OCC>;
+            if constexpr (OCC == 1)  // the OCC > 1 kernels take plain programs only
+                if (acc) kern = ls_stage_x<T, W, L, true, PERSIST>;
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             const long nlines = (long)ny * nz;
             const long ntiles = (nlines + W - 1) / W;
@@ -1449,6 +1451,9 @@ static int launch_stage_sel(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir
     case 17: return launch_stage_cfg<T, 16, Lbig, true, 1, 3>(ctx, prog, dir, nx, ny, nz);
     // 18: configuration 9 (8 lines, long chunks, y/z) built for three CTAs per SM
     case 18: return launch_stage_cfg<T, 8, Lbig, true, 1, 3>(ctx, prog, dir, nx, ny, nz);
+    // 19: configuration 3 (8 lines, long chunks, one CTA per tile) built for
+    // three CTAs per SM: with one staging slot the FP64 x tiles fit three
+    case 19: return launch_stage_cfg<T, 8, Lbig, false, 1, 3>(ctx, prog, dir, nx, ny, nz);
     default: return X3D_EUNSUPPORTED;
     }
 }
