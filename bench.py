@@ -264,16 +264,18 @@ def sweep_groups(ctx, fields, outs, fused):
 
 
 # Lines per tile (W) of each chunked configuration (x3d_ctx_set_kernel 0..15
-# and 17..19; 16 is one thread per line).
-CONFIG_W = [16, 32, 16, 8, 32, 8, 16, 32, 16, 8, 32, 8, 32, 16, 32, 32, 1, 16, 8, 8]
+# and 17..20; 16 is one thread per line).
+CONFIG_W = [16, 32, 16, 8, 32, 8, 16, 32, 16, 8, 32, 8, 32, 16, 32, 32, 1, 16, 8, 8, 16]
 
 
-def config_pattern(cfg):
-    """The roofline probe pattern with the access order of y/z configuration
-    cfg: whole-line tiles of W columns, claimed in order from a counter by the
-    persistent configurations 6..15, 17 and 18, one CTA per tile by the others."""
+def config_pattern(cfg, d):
+    """The roofline probe pattern with the access order of configuration cfg
+    along y (d = 1) or z (d = 2): whole-line tiles of W columns taken in
+    order -- claimed from a counter by the persistent configurations, and
+    dispatched in block order by the hardware for the one-CTA-per-tile ones,
+    which keeps the tiles in flight a window of consecutive tiles as well."""
     w = CONFIG_W[cfg] if 0 <= cfg < len(CONFIG_W) and cfg != 16 else 16
-    return f"claim_w{w}" if 6 <= cfg < 16 or cfg in (17, 18) else f"tile_w{w}"
+    return f"claim_w{w}" if d == 1 else f"claimz_w{w}"
 
 
 def pattern_ceilings(ctx, torch, src, outs):
@@ -281,15 +283,16 @@ def pattern_ceilings(ctx, torch, src, outs):
     (x3d_roofline_probe), flat, in the y stage kernels' tile order for
     W = 8 .. 128 columns over whole lines, over blocks of 128 rows, and with
     the tiles claimed in order from a counter as the persistent stage kernels
-    take them: what the sweep launches' traffic mix and access order can
-    reach on this GPU
+    take them, along y lines (claim_w) and along z lines (claimz_w): what the
+    sweep launches' traffic mix and access order can reach on this GPU
     (best over 1, 2, 4 and 8 CTAs per SM of 5 timed launches after 3 warm-up
     ones)."""
     nz, ny, nx = src.shape
     bytes_moved = 7 * src.numel() * src.element_size()
     res = {}
     cases = [("flat", 0, 0)] + [(f"tile_w{w}", 1, w) for w in (8, 16, 32, 64, 128)] + \
-            [(f"block128_w{w}", 2, w) for w in (32, 64, 128)] + [(f"claim_w{w}", 5, w) for w in (8, 16, 32)]
+            [(f"block128_w{w}", 2, w) for w in (32, 64, 128)] + [(f"claim_w{w}", 5, w) for w in (8, 16, 32)] + \
+            [(f"claimz_w{w}", 6, w) for w in (8, 16, 32)]
     for key, pattern, w in cases:
         rt = 16 if w == 128 else 32
         rows = 128 if pattern == 2 else ny
@@ -540,7 +543,7 @@ def run_b200(args, world, rank, local):
     ceil = pattern_ceilings(ctx, torch, fields[0], outs[:6])
     if ceil:
         cfg = dom["config"]
-        key = "flat" if FAMILY[dom_d] == "ls_stage_x" else config_pattern(cfg)
+        key = "flat" if FAMILY[dom_d] == "ls_stage_x" else config_pattern(cfg, dom_d)
         if key in ceil:
             roofline["pattern_ceiling_gbs"] = ceil[key]
             roofline["pattern"] = key

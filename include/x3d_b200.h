@@ -274,14 +274,14 @@ int x3d_autotune(x3d_ctx ctx, int max_group);
  * kernels that carry two x-adjacent lines per thread in packed FP32
  * registers (FP32 contexts, even nx); 16 one thread per line; 17 the y/z
  * kernel of configuration 6 built for three CTAs per SM, for operators that
- * each write their own output, on lines of at most 16 chunks; 18 and 19 the
- * same for configurations 9 and 3, at most 32 chunks, x lines too) for every
+ * each write their own output, on lines of at most 16 chunks; 18, 19 and 20
+ * the same for configurations 9, 3 and 0, x lines too) for every
  * later call and forget tuned choices; -1 restores the default.  A
  * configuration that cannot handle a call (alignment, shared memory) still
  * falls back to one that can.  No reference counterpart. */
 int x3d_ctx_set_kernel(x3d_ctx ctx, int cfg);
 /* The configuration chosen for (direction, group size): *cfg = -1 when not
- * tuned, 0..15 and 17..19 chunked variants, 16 one thread per line. */
+ * tuned, 0..15 and 17..20 chunked variants, 16 one thread per line. */
 int x3d_autotune_choice(x3d_ctx ctx, int dir, int group, int *cfg);
 /* The configuration chosen for a fused stage of the Euler step (*cfg = -1
  * when not tuned): stage is one of transeq_x, transeq_y, transeq_z, div_x,
@@ -292,7 +292,7 @@ int x3d_autotune_choice(x3d_ctx ctx, int dir, int group, int *cfg);
  * launch has its own configuration under its own name. */
 int x3d_autotune_stage_choice(x3d_ctx ctx, const char *stage, int *cfg);
 /* Sets one of those choices (a saved tuning, or a form to test); value -1
- * removes it.  Configurations are 0..15 and 17..19; "<stage>.split" 0 or 1;
+ * removes it.  Configurations are 0..15 and 17..20; "<stage>.split" 0 or 1;
  * "<stage>.parts" a launch count, used only where the stage splits into
  * exactly that many parts.  Extension. */
 int x3d_ctx_set_stage_choice(x3d_ctx ctx, const char *stage, int value);

@@ -15,7 +15,7 @@ from conftest import rel_err, seeded_field
 pytestmark = pytest.mark.gpu
 
 X, Y, Z = 0, 1, 2
-KERNEL_CONFIGS = 20  # x3d_ctx_set_kernel: 0..15 and 17..19 chunked, 16 one thread per line
+KERNEL_CONFIGS = 21  # x3d_ctx_set_kernel: 0..15 and 17..20 chunked, 16 one thread per line
 
 # (routine, operator instance, oracle kind, direction, signature style)
 ROUTINES = [

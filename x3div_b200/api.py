@@ -267,7 +267,7 @@ class Context:
         self._check(self.L.x3d_autotune(self.handle, int(max_group)))
 
     def set_kernel(self, cfg):
-        """Force a kernel configuration (0..15 and 17..19 chunked, 16 thread per line, -1 default)."""
+        """Force a kernel configuration (0..15 and 17..20 chunked, 16 thread per line, -1 default)."""
         self._check(self.L.x3d_ctx_set_kernel(self.handle, int(cfg)))
 
     def autotune_choice(self, direction, group):

@@ -818,7 +818,7 @@ int x3d_ctx_set_stage_choice(x3d_ctx ctx, const char *stage, int value)
     if (value < -1) return set_error(ctx, X3D_EINVAL, "stage choice below -1");
     if (ends(".split") && value > 1) return set_error(ctx, X3D_EINVAL, "a split choice is 0 or 1");
     if (!ends(".split") && !ends(".parts") && value >= 0 && !is_stage_cfg(value))
-        return set_error(ctx, X3D_EINVAL, "stage configurations are 0..15 and 17..19");
+        return set_error(ctx, X3D_EINVAL, "stage configurations are 0..15 and 17..20");
     if (value == -1) ctx->stage_tuned.erase(s);
     else ctx->stage_tuned[s] = value;
     return X3D_OK;

@@ -1454,6 +1454,9 @@ static int launch_stage_sel(x3d_ctx_s *ctx, const StageProgram<T> &prog, int dir
     // 19: configuration 3 (8 lines, long chunks, one CTA per tile) built for
     // three CTAs per SM: with one staging slot the FP64 x tiles fit three
     case 19: return launch_stage_cfg<T, 8, Lbig, false, 1, 3>(ctx, prog, dir, nx, ny, nz);
+    // 20: configuration 0 (16 lines, long chunks, one CTA per tile) built for
+    // three CTAs per SM
+    case 20: return launch_stage_cfg<T, 16, Lbig, false, 1, 3>(ctx, prog, dir, nx, ny, nz);
     default: return X3D_EUNSUPPORTED;
     }
 }

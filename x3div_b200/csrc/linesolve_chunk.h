@@ -59,12 +59,13 @@ struct StageProgram {
 
 // Number of (lines per CTA, chunk length, persistence, lines per thread)
 // configurations launch_stage knows in 0 .. 15; 16 is the one-thread-per-line
-// kernel (not a launch_stage configuration); 17, 18 and 19 are
-// configurations 6, 9 and 3 compiled for three CTAs per SM (plain programs).
+// kernel (not a launch_stage configuration); 17, 18, 19 and 20 are
+// configurations 6, 9, 3 and 0 compiled for three CTAs per SM (plain
+// programs).
 // kAllConfigs counts every configuration the
 // dispatch tries.
 constexpr int kChunkConfigs = 16;
-constexpr int kAllConfigs = 20;
+constexpr int kAllConfigs = 21;
 inline bool is_stage_cfg(int cfg) { return cfg >= 0 && cfg < kAllConfigs && cfg != kChunkConfigs; }
 
 // Launches the chunked stage kernel with configuration cfg (is_stage_cfg).  Returns X3D_EUNSUPPORTED, launching nothing, when the
