@@ -294,7 +294,7 @@ int x3d_autotune_stage_choice(x3d_ctx ctx, const char *stage, int *cfg);
 /* Sets one of those choices (a saved tuning, or a form to test); value -1
  * removes it.  Configurations are 0..15 and 17..20; "<stage>.split" 0 or 1;
  * "<stage>.parts" a launch count, used only where the stage splits into
- * exactly that many parts.  Extension. */
+ * exactly that many parts; "poisson_x" 0 or 1 (x3d_poisson).  Extension. */
 int x3d_ctx_set_stage_choice(x3d_ctx ctx, const char *stage, int value);
 
 /* ---- batches of independent boxes ----------------------------------------- */
@@ -402,7 +402,12 @@ int x3d_copy_blocks(x3d_ctx ctx, void *dst, const void *src, int elem_bytes, con
  * problem on the box mirrored about both walls of every such direction
  * (2 nxm points over 2 xlx) and cut back: the mirrored field holds exactly
  * those cosine modes.  The first call makes the mirrored box's periodic
- * context and right-hand side (kept until x3d_ctx_destroy). */
+ * context and right-hand side (kept until x3d_ctx_destroy).  Where nz and
+ * nx / 2 are both 2^p 3^q from 8 to 1024 (nx even), the periodic solve is
+ * five launches: the library's x transforms (real lines to a spectrum with
+ * y fastest), batched 1-D cuFFT transforms along y, the fused z transform
+ * and mode division, and back; the stage choice "poisson_x" = 0
+ * (x3d_ctx_set_stage_choice) takes cuFFT's 2-D (x, y) transforms instead. */
 int x3d_poisson(x3d_ctx ctx, double *rhs);
 /* The z part of poisson_000 for a box whose y rows are spread over ranks:
  * spec is this rank's block of the x-y transformed half spectrum (complex

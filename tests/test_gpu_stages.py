@@ -52,6 +52,44 @@ def test_poisson_z_lengths(oracle, torch_cuda, shape):
     ctx.close()
 
 
+# x lengths of every own x transform (nx / 2 from 8 to 1024) with y extents
+# that mostly leave a partial last tile of rows (4 rows a tile), each solved
+# through the own x transforms (the default) and through cuFFT's 2-D (x, y)
+# transforms (stage choice poisson_x = 0).
+@pytest.mark.parametrize("shape", [(16, 10, 8), (24, 9, 12), (48, 9, 16), (96, 9, 24), (192, 10, 32),
+                                   (384, 12, 48), (768, 10, 16), (1024, 9, 8), (1536, 9, 8), (2048, 9, 12),
+                                   (512, 33, 64), (64, 64, 64), (128, 20, 96), (256, 17, 128), (16, 12, 768),
+                                   (32, 9, 1024)])
+def test_poisson_own_x_transforms(oracle, torch_cuda, shape):
+    from x3div_b200 import to_device, to_host
+    rhs = seeded_field(shape, 31, kind="rand", lengths=LEN, noise=0)
+    ref = oracle.poisson(rhs, *LEN)
+    outs = []
+    for choice in (-1, 0):
+        ctx = ctx_for(shape)
+        ctx.set_stage_choice("poisson_x", choice)
+        d = to_device(rhs)
+        n0 = ctx.launch_count()
+        ctx.poisson(d)
+        ctx.sync()
+        # own x transforms: x forward, z solve, x inverse (the y transforms are cuFFT's)
+        assert ctx.launch_count() - n0 == (3 if choice == -1 else 1), (shape, choice)
+        outs.append(to_host(d))
+        assert rel_err(outs[-1], ref) < 1e-12, (shape, choice)
+        ctx.close()
+    assert rel_err(outs[0], outs[1]) < 1e-13, shape
+
+
+def test_poisson_x_choice_is_checked(torch_cuda):
+    from x3div_b200 import X3DError
+    ctx = ctx_for((16, 16, 16))
+    with pytest.raises(X3DError):
+        ctx.set_stage_choice("poisson_x", 2)
+    ctx.set_stage_choice("poisson_x", 0)
+    ctx.set_stage_choice("poisson_x", -1)
+    ctx.close()
+
+
 @pytest.mark.parametrize("shape", SHAPES)
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 def test_divergence_gradp_momentum(oracle, torch_cuda, shape, prec):

@@ -816,8 +816,9 @@ int x3d_ctx_set_stage_choice(x3d_ctx ctx, const char *stage, int value)
         return s.size() > n && s.compare(s.size() - n, n, suf) == 0;
     };
     if (value < -1) return set_error(ctx, X3D_EINVAL, "stage choice below -1");
-    if (ends(".split") && value > 1) return set_error(ctx, X3D_EINVAL, "a split choice is 0 or 1");
-    if (!ends(".split") && !ends(".parts") && value >= 0 && !is_stage_cfg(value))
+    if ((ends(".split") || s == "poisson_x") && value > 1)
+        return set_error(ctx, X3D_EINVAL, "a split or poisson_x choice is 0 or 1");
+    if (!ends(".split") && !ends(".parts") && s != "poisson_x" && value >= 0 && !is_stage_cfg(value))
         return set_error(ctx, X3D_EINVAL, "stage configurations are 0..15 and 17..20");
     if (value == -1) ctx->stage_tuned.erase(s);
     else ctx->stage_tuned[s] = value;

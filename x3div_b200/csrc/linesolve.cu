@@ -440,20 +440,6 @@ __global__ void ls_np_stag(const T *__restrict__ in, T *__restrict__ out, const 
 // ---------------------------------------------------------------------------
 // Host side.
 
-static PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
-{
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    if (!fn) {
-        void *p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
-                cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    }
-    return fn;
-}
-
 template <typename T>
 static const LineOp<T> &lineop(const x3d_op_s *op);
 template <>
@@ -498,7 +484,7 @@ static int run_kind(x3d_ctx_s *ctx, const x3d_op_s *op, int dir, const T *in, T 
         const int nb = (n + 255) / 256;
         const int box_n = (n + nb - 1) / nb;
         const size_t smem = (size_t)nb * box_n * W * es;
-        auto enc = encode_fn();
+        auto enc = encode_tiled();
         if (enc && ptr_ok && ((size_t)nx * es) % 16 == 0 && smem + 1024 <= ctx->smem_optin) {
             CUtensorMap tmap;
             cuuint64_t gdim[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};

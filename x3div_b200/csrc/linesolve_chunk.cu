@@ -1169,7 +1169,7 @@ __global__ void __launch_bounds__(OCC > 1 ? 256 : 512, OCC)
 // ---------------------------------------------------------------------------
 // Host side.
 
-static PFN_cuTensorMapEncodeTiled_v12000 encode_tiled()
+PFN_cuTensorMapEncodeTiled_v12000 encode_tiled()
 {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
     if (!fn) {

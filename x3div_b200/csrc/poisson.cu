@@ -106,13 +106,18 @@ __global__ void k_spectral_divide(double2 *c, unsigned nxl, unsigned nyl, unsign
 // line, multiplies it by W_n^(q (j mod Ns) n/(Ns R)), takes the length-R DFT
 // in registers and writes the results to (j div Ns) Ns R + (j mod Ns) + q Ns.
 // Each stage reads all its inputs before a barrier and writes after it, so
-// one shared-memory buffer suffices.  Twiddles come from a table of the nz
-// roots of unity computed on the host in FP64 (copied to shared memory).
+// one shared-memory buffer suffices.  Twiddles come from a table of the
+// roots of unity computed on the host in FP64: a butterfly reads the first
+// of its R - 1 and makes the others as its powers (the recurrence of Van
+// Loan, "Computational Frameworks for the FFT", 1.4), so a stage reads one
+// table entry a butterfly rather than R - 1.
 
 constexpr int kZftThreads = 512;
 constexpr int kZftVals = 8;    // values a thread holds in one stage
 
 // Lines per tile for a transform of length N (W N <= kZftThreads kZftVals).
+// (8 lines and 1024 threads for N = 768 timed 3.62 ms against 3.52 for these
+// 4 lines and 512 threads, 768^3.)
 template <int N>
 constexpr int kZftW = N <= 256 ? 16 : (N <= 512 ? 8 : 4);
 
@@ -179,12 +184,13 @@ __device__ __forceinline__ void dft(double2 (&v)[R])
 struct ZLines {
     double2 *base;   // the tile's first line at k = 0
     size_t zstride;  // elements between consecutive k
-    int lines;       // x modes of the tile inside the spectrum (<= W)
+    size_t lstride;  // elements between consecutive lines
+    int lines;       // lines of the tile inside the array (<= W)
     double tyj, k2yj, ntot;
-    const double2 *xtab;  // shared: (tx, k2x) of the tile's W x modes
+    const double2 *xtab;  // shared: (t, k2) of the tile's W lanes
     const double2 *ztab;  // shared: (tz, k2z) of the N z modes
     // c <- -c / (K ntot), zero where K < 1e-16: the K and mask of
-    // k_spectral_divide for mode (i0 + l, j, k)
+    // k_spectral_divide for mode (lane l, row, k)
     __device__ __forceinline__ double2 divide(double2 v, int k, int l) const
     {
         const double2 x = xtab[l], z = ztab[k];
@@ -205,35 +211,44 @@ struct ZLines {
 // values this thread holds (positions j + q N / R) with unit twiddles, and
 // writes positions j R + q -- so the modes make one shared-memory pass
 // fewer.
-template <int N, int R, int NS, int W, bool INV, bool SRC_G, bool DST_G, bool FUSE>
+template <int N, int R, int NS, int W, bool INV, bool SRC_G, bool DST_G, bool FUSE, int NT = kZftThreads>
 __device__ __forceinline__ void zft_stage(double2 *buf, const double2 *tw, const ZLines &zl)
 {
     constexpr int MB = kZftVals / R;
     constexpr int NB = W * (N / R);
     constexpr int STRIDE = N / (NS * R);
-    static_assert(NB <= MB * kZftThreads, "tile too large for one pass of the stage");
+    static_assert(NB <= MB * NT, "tile too large for one pass of the stage");
     double2 v[MB][R];
     int dk[MB], dl[MB];
 #pragma unroll
     for (int s = 0; s < MB; ++s) {
-        const int b = threadIdx.x + s * kZftThreads;
+        const int b = threadIdx.x + s * NT;
         if (b < NB) {
             const int l = b % W, j = b / W;
             const int jm = j % NS;
+            // the twiddles W_n^(q jm n / (NS R)), q < R, as powers of w1 (q = 1):
+            // one table read a butterfly, each power one product from the last
+            // (a few ulp of W_n after R - 1 products)
+            double2 w1 = make_double2(1.0, 0.0);
+            if constexpr (NS > 1) {
+                w1 = tw[jm * STRIDE];
+                if (INV) w1.y = -w1.y;
+            }
+            double2 wq = w1;
 #pragma unroll
             for (int q = 0; q < R; ++q) {
                 const int k = j + q * (N / R);
                 double2 x;
                 if constexpr (SRC_G)
-                    x = l < zl.lines ? zl.base[(size_t)k * zl.zstride + l] : make_double2(0.0, 0.0);
+                    x = l < zl.lines ? zl.base[(size_t)k * zl.zstride + (size_t)l * zl.lstride]
+                                     : make_double2(0.0, 0.0);
                 else
                     x = buf[k * W + l];
-                if (q == 0) {
+                if (q == 0 || NS == 1) {  // the first stage's twiddles are all 1
                     v[s][q] = x;
                 } else {
-                    double2 w = tw[q * jm * STRIDE];
-                    if (INV) w.y = -w.y;
-                    v[s][q] = cmul(x, w);
+                    v[s][q] = cmul(x, wq);
+                    wq = cmul(wq, w1);
                 }
             }
             dft<R, INV>(v[s]);
@@ -251,13 +266,13 @@ __device__ __forceinline__ void zft_stage(double2 *buf, const double2 *tw, const
     if constexpr (!SRC_G && !DST_G) __syncthreads();  // in place in shared memory
 #pragma unroll
     for (int s = 0; s < MB; ++s) {
-        const int b = threadIdx.x + s * kZftThreads;
+        const int b = threadIdx.x + s * NT;
         if (b < NB) {
 #pragma unroll
             for (int q = 0; q < R; ++q) {
                 const int k = dk[s] + q * (FUSE ? 1 : NS), l = dl[s];
                 if constexpr (DST_G) {
-                    if (l < zl.lines) zl.base[(size_t)k * zl.zstride + l] = v[s][q];
+                    if (l < zl.lines) zl.base[(size_t)k * zl.zstride + (size_t)l * zl.lstride] = v[s][q];
                 } else {
                     buf[k * W + l] = v[s][q];
                 }
@@ -291,25 +306,28 @@ constexpr RadixSeq radix_seq(int n, bool reversed = false)
     return s;
 }
 
-// The z transform, division and inverse of a tile.  The forward transform
-// reads the lines from global memory in its first stage; its last stage
-// divides the modes and runs the inverse's first stage in registers (the
-// inverse takes the radices in reverse order); the inverse writes the
+// The z transform, division and inverse of a tile (SOLVE).  The forward
+// transform reads the lines from global memory in its first stage; its last
+// stage divides the modes and runs the inverse's first stage in registers
+// (the inverse takes the radices in reverse order); the inverse writes the
 // lines back to global memory in its last stage, which is that fused stage
-// itself when the length has a single radix.
-template <int N, int W, bool INV, int ST = 0, int NS = 1>
+// itself when the length has a single radix.  Without SOLVE: the forward
+// transform alone (!INV: lines from global memory, the transform left in
+// buf in natural order) or the inverse alone (INV: from buf to global
+// memory).
+template <int N, int W, bool INV, bool SOLVE = true, int NT = kZftThreads, int ST = 0, int NS = 1>
 __device__ __forceinline__ void zft(double2 *buf, const double2 *tw, const ZLines &zl)
 {
     constexpr RadixSeq seq = radix_seq(N, INV);
     if constexpr (ST < seq.count) {
         constexpr int R = seq.r[ST];
         constexpr bool last = ST + 1 == seq.count;
-        if constexpr (!INV && last) {
-            zft_stage<N, R, NS, W, false, ST == 0, seq.count == 1, true>(buf, tw, zl);
-            zft<N, W, true, 1, R>(buf, tw, zl);  // the inverse from its second stage
+        if constexpr (SOLVE && !INV && last) {
+            zft_stage<N, R, NS, W, false, ST == 0, seq.count == 1, true, NT>(buf, tw, zl);
+            zft<N, W, true, true, NT, 1, R>(buf, tw, zl);  // the inverse from its second stage
         } else {
-            zft_stage<N, R, NS, W, INV, !INV && ST == 0, INV && last, false>(buf, tw, zl);
-            zft<N, W, INV, ST + 1, NS * R>(buf, tw, zl);
+            zft_stage<N, R, NS, W, INV, !INV && ST == 0, INV && last, false, NT>(buf, tw, zl);
+            zft<N, W, INV, SOLVE, NT, ST + 1, NS * R>(buf, tw, zl);
         }
     }
 }
@@ -319,39 +337,39 @@ __device__ __forceinline__ void zft(double2 *buf, const double2 *tw, const ZLine
 // K and mask of k_spectral_divide, inverse z transform.  The tile's modes go
 // from global memory straight into the first stage's registers and leave
 // the last inverse stage straight to global memory; the twiddles and the
-// wavenumber tables the division reads are copied into shared memory
-// first.  The spectrum is (nz, ny, nxl) with x fastest:
+// wavenumber tables the division reads are copied into shared memory first
+// (read through L1 instead, the z kernel at 512^3 took 790 us against 720).
+// The spectrum is (nz, ny, nxl) with x fastest:
 // x modes ig0 .. ig0 + nxl - 1 of the nxh = nx/2 + 1 and y rows j0 .. j0 +
-// ny - 1 of the box (a Z pencil of the half spectrum).
+// ny - 1 of the box (a Z pencil of the half spectrum).  K is symmetric in
+// the x and y factors, so the same kernel solves a spectrum stored (nz,
+// nxh, ny) with y fastest when given the y tables as (k2x, tx), the x tables
+// as (k2y, ty) and ny as nxl and nxh, nxh as ny.
 template <int N>
 __global__ void __launch_bounds__(kZftThreads, 2)
     k_poisson_z(double2 *__restrict__ c, int nxl, int ny, int ig0, int j0, int nxh,
                 const double2 *__restrict__ tw, const double *__restrict__ k2x, const double *__restrict__ tx,
-                const double *__restrict__ k2y, const double *__restrict__ ty, const double *__restrict__ k2z,
-                const double *__restrict__ tz, double ntot)
+                const double *__restrict__ k2y, const double *__restrict__ ty, double ntot)
 {
     constexpr int W = kZftW<N>;
     extern __shared__ __align__(16) double2 zbuf[];
-    double2 *const tws = zbuf + N * W;
-    double2 *const ztab = tws + N;
-    double2 *const xtab = ztab + N;
+    double2 *const tws = zbuf + N * W;  // twiddles, then (tz, k2z), then the lanes' (t, k2)
+    double2 *const xtab = tws + 2 * N;
     const int tiles_i = (nxl + W - 1) / W;
     const int j = blockIdx.x / tiles_i;
     const int i0 = (blockIdx.x - j * tiles_i) * W;
     ZLines zl;
     zl.base = c + (size_t)j * nxl + i0;
     zl.zstride = (size_t)ny * nxl;
+    zl.lstride = 1;
     zl.lines = min(W, nxl - i0);
-    zl.tyj = __ldg(ty + j0 + j);  // j0: global index of the spectrum's first y row
+    zl.tyj = __ldg(ty + j0 + j);  // j0: global index of the spectrum's first row
     zl.k2yj = __ldg(k2y + j0 + j);
     zl.ntot = ntot;
     zl.xtab = xtab;
-    zl.ztab = ztab;
-    for (int t = threadIdx.x; t < N; t += kZftThreads) {
-        tws[t] = __ldg(tw + t);
-        ztab[t] = make_double2(__ldg(tz + t), __ldg(k2z + t));
-    }
-    if (threadIdx.x < W) {  // ig0 + i0: global index of the tile's first x mode
+    zl.ztab = tws + N;
+    for (int t = threadIdx.x; t < 2 * N; t += kZftThreads) tws[t] = __ldg(tw + t);
+    if (threadIdx.x < W) {  // ig0 + i0: global index of the tile's first lane
         const int i = min(ig0 + i0 + (int)threadIdx.x, nxh - 1);
         xtab[threadIdx.x] = make_double2(__ldg(tx + i), __ldg(k2x + i));
     }
@@ -369,6 +387,105 @@ static bool zft_supported(int n)
     X3D_ZFT_SIZES(X3D_ZFT_CASE)
 #undef X3D_ZFT_CASE
     return false;
+}
+
+// ---------------------------------------------------------------------------
+// Own x transforms: a real line of n = 2M points as the complex line z[m] =
+// f[2m] + i f[2m+1] of M points (the same memory), transformed by the
+// Stockham stages above, then split into the n/2 + 1 modes of the real
+// transform -- the half-length method for real sequences (Brigham, "The
+// Fast Fourier Transform", ch. 10; Press et al., Numerical Recipes, 12.3):
+// with Z = DFT_M(z), A = Z[k], B = conj(Z[M - k]) (indices mod M),
+//   F[k] = (A + B) / 2 - i e^{-2 pi i k / n} (A - B) / 2,   k = 0 .. M.
+// The inverse runs it backwards: from G[0 .. M] (a Hermitian half spectrum)
+//   Z[k] = (G[k] + conj(G[M - k])) + i e^{+2 pi i k / n} (G[k] - conj(G[M - k])),
+// k < M, and the unnormalised inverse DFT_M of Z is f[2m] + i f[2m+1], the
+// unnormalised c2r transform of G (cuFFT's Z2D convention).  Tiles are W
+// consecutive y rows of one z plane; the spectrum is stored (nz, M + 1, ny)
+// with y fastest, so a mode of the tile's rows is one run of W elements.
+
+// Rows per tile of the x kernels: 4, so that a warp's first-stage loads
+// take 4 rows x 8 consecutive points (128 bytes of each row), and threads
+// enough for the tile's values in one pass of every stage (8 a thread; 6
+// where a radix-3 stage takes two triples a thread), at least one warp.
+constexpr int kXftW = 4;
+template <int M>
+constexpr int kXftThreads = (((M % 3 ? kXftW * M / 8 : kXftW * M / 6) + 31) / 32) * 32;
+
+template <int M>
+__global__ void __launch_bounds__(kXftThreads<M>, 1024 / kXftThreads<M>)
+    k_rfft_x(const double *__restrict__ f, double2 *__restrict__ spec, int ny, const double2 *__restrict__ tw)
+{
+    constexpr int W = kXftW;
+    constexpr int NT = kXftThreads<M>;
+    extern __shared__ __align__(16) double2 zbuf[];
+    const double2 *const wx = tw + M;  // the tables are read through L1
+    const int tiles_j = (ny + W - 1) / W;
+    const int kz = blockIdx.x / tiles_j;
+    const int j0 = (blockIdx.x - kz * tiles_j) * W;
+    ZLines zl;
+    zl.base = const_cast<double2 *>(reinterpret_cast<const double2 *>(f)) + ((size_t)kz * ny + j0) * M;
+    zl.zstride = 1;
+    zl.lstride = M;
+    zl.lines = min(W, ny - j0);
+    zft<M, W, false, false, NT>(zbuf, tw, zl);  // Z of each row, natural order, in zbuf
+    double2 *const out = spec + (size_t)kz * (M + 1) * ny + j0;
+    for (int b = threadIdx.x; b < (M / 2 + 1) * W; b += NT) {
+        const int l = b % W, p = b / W, q = (M - p) % M;  // modes p and M - p from Z[p] and Z[q]
+        if (l >= zl.lines) continue;
+        const double2 zp = zbuf[p * W + l], zq = zbuf[q * W + l];
+        const double2 wp = __ldg(wx + p), wq = __ldg(wx + M - p);
+        // F[p]: A = Z[p], B = conj(Z[q]);  F[M - p]: A = Z[q], B = conj(Z[p])
+        const double2 e = make_double2(0.5 * (zp.x + zq.x), 0.5 * (zp.y - zq.y));  // (A + B) / 2 of F[p]
+        const double2 d = make_double2(0.5 * (zp.x - zq.x), 0.5 * (zp.y + zq.y));  // (A - B) / 2 of F[p]
+        const double2 wd = cmul(wp, d);
+        out[(size_t)p * ny + l] = make_double2(e.x + wd.y, e.y - wd.x);
+        if (M - p != p) {  // F[M - p]: (A + B) / 2 = conj(e), (A - B) / 2 = -conj(d)
+            const double2 wd2 = cmul(wq, make_double2(-d.x, d.y));
+            out[(size_t)(M - p) * ny + l] = make_double2(e.x + wd2.y, -e.y - wd2.x);
+        }
+    }
+}
+
+template <int M>
+__global__ void __launch_bounds__(kXftThreads<M>, 1024 / kXftThreads<M>)
+    k_irfft_x(const double2 *__restrict__ spec, double *__restrict__ f, int ny, const double2 *__restrict__ tw)
+{
+    constexpr int W = kXftW;
+    constexpr int NT = kXftThreads<M>;
+    extern __shared__ __align__(16) double2 zbuf[];
+    const double2 *const wx = tw + M;  // the tables are read through L1
+    const int tiles_j = (ny + W - 1) / W;
+    const int kz = blockIdx.x / tiles_j;
+    const int j0 = (blockIdx.x - kz * tiles_j) * W;
+    const int lines = min(W, ny - j0);
+    const double2 *const in = spec + (size_t)kz * (M + 1) * ny + j0;
+    for (int b = threadIdx.x; b < (M / 2 + 1) * W; b += NT) {
+        const int l = b % W, p = b / W, q = M - p;  // Z[p] and Z[q] (q < M) from G[p] and G[q]
+        double2 gp = make_double2(0.0, 0.0), gq = gp;
+        if (l < lines) {
+            gp = in[(size_t)p * ny + l];
+            gq = in[(size_t)q * ny + l];
+        }
+        // Z[p] = (G[p] + conj(G[q])) + i conj(wx[p]) (G[p] - conj(G[q]))
+        const double2 e = make_double2(gp.x + gq.x, gp.y - gq.y);
+        const double2 d = make_double2(gp.x - gq.x, gp.y + gq.y);
+        const double2 w = __ldg(wx + p);
+        const double2 od = cmul(make_double2(w.x, -w.y), d);
+        zbuf[p * W + l] = make_double2(e.x - od.y, e.y + od.x);
+        if (q != p && q < M) {  // Z[q] = (G[q] + conj(G[p])) + i conj(wx[q]) (G[q] - conj(G[p]))
+            const double2 w2 = __ldg(wx + q);
+            const double2 od2 = cmul(make_double2(w2.x, -w2.y), make_double2(-d.x, d.y));
+            zbuf[q * W + l] = make_double2(e.x - od2.y, -e.y + od2.x);
+        }
+    }
+    __syncthreads();
+    ZLines zl;
+    zl.base = reinterpret_cast<double2 *>(f) + ((size_t)kz * ny + j0) * M;
+    zl.zstride = 1;
+    zl.lstride = M;
+    zl.lines = lines;
+    zft<M, W, true, false, NT>(zbuf, tw, zl);  // the inverse, its last stage to the rows
 }
 
 // The 1-D modified-wavenumber tables and, where a fused z kernel exists for
@@ -402,12 +519,14 @@ static int poisson_tables(x3d_ctx_s *ctx)
     ctx->d_ty = tab + 2 * nx + ny;
     ctx->d_k2z = tab + 2 * nx + 2 * ny;
     ctx->d_tz = tab + 2 * nx + 2 * ny + nz;
-    if (zft_supported(nz)) {
-        std::vector<double> tw(2 * (size_t)nz);
+    if (zft_supported(nz)) {  // the twiddles, then (tz, k2z) of each z mode
+        std::vector<double> tw(4 * (size_t)nz);
         const double twopi = 2.0 * std::acos(-1.0);
         for (int t = 0; t < nz; ++t) {
             tw[2 * t] = std::cos(twopi * t / nz);
             tw[2 * t + 1] = -std::sin(twopi * t / nz);
+            tw[2 * ((size_t)nz + t)] = tz[t];
+            tw[2 * ((size_t)nz + t) + 1] = k2z[t];
         }
         if (cudaMalloc(&ctx->d_zft_tw, tw.size() * sizeof(double)) != cudaSuccess)
             return set_error(ctx, X3D_ENOMEM, "poisson twiddles");
@@ -418,18 +537,63 @@ static int poisson_tables(x3d_ctx_s *ctx)
             return set_error(ctx, X3D_ECUDA, "poisson twiddles upload");
         }
     }
+    if (nx % 2 == 0 && zft_supported(nx / 2)) {
+        const int m = nx / 2;
+        const double twopi = 2.0 * std::acos(-1.0);
+        std::vector<double> tw(2 * (size_t)(2 * m + 1));
+        for (int t = 0; t < m; ++t) {
+            tw[2 * t] = std::cos(twopi * t / m);
+            tw[2 * t + 1] = -std::sin(twopi * t / m);
+        }
+        for (int k = 0; k <= m; ++k) {
+            tw[2 * (m + k)] = std::cos(twopi * k / nx);
+            tw[2 * (m + k) + 1] = -std::sin(twopi * k / nx);
+        }
+        if (cudaMalloc(&ctx->d_xft_tw, tw.size() * sizeof(double)) != cudaSuccess) {
+            ctx->d_xft_tw = nullptr;
+            return set_error(ctx, X3D_ENOMEM, "poisson x twiddles");
+        }
+        if (cudaMemcpy(ctx->d_xft_tw, tw.data(), tw.size() * sizeof(double), cudaMemcpyHostToDevice) !=
+            cudaSuccess) {
+            cudaFree(ctx->d_xft_tw);
+            ctx->d_xft_tw = nullptr;
+            return set_error(ctx, X3D_ECUDA, "poisson x twiddles upload");
+        }
+    }
     return X3D_OK;
+}
+
+// Whether a solve on this context takes the own x transforms: the fused z
+// kernel and a fused length nx / 2, unless the stage choice "poisson_x" is 0.
+static bool poisson_own_x(const x3d_ctx_s *ctx)
+{
+    const auto it = ctx->stage_tuned.find("poisson_x");
+    return ctx->zfused && ctx->d_xft_tw && (it == ctx->stage_tuned.end() || it->second != 0);
 }
 
 int poisson_setup(x3d_ctx_s *ctx)
 {
-    if (ctx->plans_ready) return X3D_OK;
-    int rc = poisson_tables(ctx);
-    if (rc) return rc;
+    if (!ctx->spectrum) {
+        int rc = poisson_tables(ctx);
+        if (rc) return rc;
+        const size_t spec = (size_t)ctx->nz * ctx->ny * (ctx->nx / 2 + 1) * sizeof(double2);
+        if (cudaMalloc(&ctx->spectrum, spec) != cudaSuccess) {
+            ctx->spectrum = nullptr;
+            return set_error(ctx, X3D_ENOMEM, "poisson spectrum");
+        }
+        ctx->zfused = ctx->d_zft_tw && ctx->zfuse_allowed;
+    }
     const int nx = ctx->nx, ny = ctx->ny, nz = ctx->nz;
-    const size_t spec = (size_t)nz * ny * (nx / 2 + 1) * sizeof(double2);
-    if (cudaMalloc(&ctx->spectrum, spec) != cudaSuccess) return set_error(ctx, X3D_ENOMEM, "poisson spectrum");
-    ctx->zfused = ctx->d_zft_tw && ctx->zfuse_allowed;
+    if (poisson_own_x(ctx)) {
+        if (ctx->plan_y_ready) return X3D_OK;
+        int n = ny;
+        if (cufftPlanMany(&ctx->plan_y, 1, &n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_Z2Z, nz * (nx / 2 + 1)) !=
+            CUFFT_SUCCESS)
+            return set_error(ctx, X3D_ECUDA, "cufftPlanMany (y lines) failed");
+        ctx->plan_y_ready = true;
+        return X3D_OK;
+    }
+    if (ctx->plans_ready) return X3D_OK;
     if (ctx->zfused) {
         int dims[2] = {ny, nx};
         if (cufftPlanMany(&ctx->plan_d2z, 2, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_D2Z, nz) != CUFFT_SUCCESS ||
@@ -443,30 +607,61 @@ int poisson_setup(x3d_ctx_s *ctx)
     return X3D_OK;
 }
 
-// The fused z kernel over a spectrum of nxl x modes starting at global mode
-// i0 and ny_loc y rows starting at global row j0 ((nz, ny_loc, nxl), x
-// fastest).
-static int launch_poisson_z(x3d_ctx_s *ctx, double2 *spec, int nxl, int i0, int ny_loc, int j0)
+// The fused z kernel over a spectrum of nxl lanes (the fastest index)
+// starting at global index i0, ny_loc rows starting at global row j0 and nz
+// planes; lanes and rows are x modes and y rows ((nz, ny_loc, nxl)) unless
+// yfast, where they are y rows and x modes ((nz, nxh, ny)).
+static int launch_poisson_z(x3d_ctx_s *ctx, double2 *spec, int nxl, int i0, int ny_loc, int j0, bool yfast = false)
 {
     const int nxh = ctx->nx / 2 + 1;
     const double ntot = (double)ctx->nx * (double)ctx->ny * (double)ctx->nz;
-    auto go = [&](auto kern, int W) {
+    const double *lk2 = yfast ? ctx->d_k2y : ctx->d_k2x, *lt = yfast ? ctx->d_ty : ctx->d_tx;
+    const double *rk2 = yfast ? ctx->d_k2x : ctx->d_k2y, *rt = yfast ? ctx->d_tx : ctx->d_ty;
+    const int lane_end = yfast ? ctx->ny : nxh;
+    const auto *ztw = reinterpret_cast<const double2 *>(ctx->d_zft_tw);
+    auto go = [&](auto kern, int W, int NT) {
         const unsigned grid = (unsigned)(((nxl + W - 1) / W) * ny_loc);
-        // tile, twiddles, z and x wavenumber tables
+        // tile, twiddles, z and lane wavenumber tables
         const size_t smem = ((size_t)ctx->nz * W + 2 * (size_t)ctx->nz + W) * sizeof(double2);
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         ++ctx->launches;
-        kern<<<grid, kZftThreads, smem, ctx->stream>>>(spec, nxl, ny_loc, i0, j0, nxh,
-                                                       (const double2 *)ctx->d_zft_tw, ctx->d_k2x, ctx->d_tx,
-                                                       ctx->d_k2y, ctx->d_ty, ctx->d_k2z, ctx->d_tz, ntot);
+        kern<<<grid, NT, smem, ctx->stream>>>(spec, nxl, ny_loc, i0, j0, lane_end, ztw, lk2, lt, rk2, rt, ntot);
         return cuda_check(ctx, cudaGetLastError(), "k_poisson_z");
     };
     switch (ctx->nz) {
 #define X3D_ZFT_LAUNCH(N) \
-    case N: return go(k_poisson_z<N>, kZftW<N>);
+    case N: return go(k_poisson_z<N>, kZftW<N>, kZftThreads);
         X3D_ZFT_SIZES(X3D_ZFT_LAUNCH)
 #undef X3D_ZFT_LAUNCH
     default: return set_error(ctx, X3D_EUNSUPPORTED, "no fused z transform for this nz");
+    }
+}
+
+// k_rfft_x (forward) or k_irfft_x over the whole box: real (nz, ny, nx) and
+// the spectrum (nz, nx/2 + 1, ny).
+static int launch_xft(x3d_ctx_s *ctx, double *f, double2 *spec, bool forward)
+{
+    auto go = [&](auto fwd, auto inv, int M, int NT) {
+        const int W = kXftW;
+        const unsigned grid = (unsigned)(((ctx->ny + W - 1) / W) * ctx->nz);
+        const size_t smem = (size_t)M * W * sizeof(double2);  // the tile
+        const auto *tw = reinterpret_cast<const double2 *>(ctx->d_xft_tw);
+        ++ctx->launches;
+        if (forward) {
+            cudaFuncSetAttribute(fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            fwd<<<grid, NT, smem, ctx->stream>>>(f, spec, ctx->ny, tw);
+        } else {
+            cudaFuncSetAttribute(inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            inv<<<grid, NT, smem, ctx->stream>>>(spec, f, ctx->ny, tw);
+        }
+        return cuda_check(ctx, cudaGetLastError(), forward ? "k_rfft_x" : "k_irfft_x");
+    };
+    switch (ctx->nx / 2) {
+#define X3D_XFT_LAUNCH(N) \
+    case N: return go(k_rfft_x<N>, k_irfft_x<N>, N, kXftThreads<N>);
+        X3D_ZFT_SIZES(X3D_XFT_LAUNCH)
+#undef X3D_XFT_LAUNCH
+    default: return set_error(ctx, X3D_EUNSUPPORTED, "no own x transform for this nx");
     }
 }
 
@@ -491,6 +686,21 @@ int poisson_solve(x3d_ctx_s *ctx, double *rhs)
     const TraceRange trace("poisson");
     int rc = poisson_setup(ctx);
     if (rc) return rc;
+    if (poisson_own_x(ctx)) {
+        // x transforms (spectrum y fastest), y transforms, z solve, and back
+        auto *spec = static_cast<double2 *>(ctx->spectrum);
+        auto *cs = reinterpret_cast<cufftDoubleComplex *>(spec);
+        cufftSetStream(ctx->plan_y, ctx->stream);
+        rc = launch_xft(ctx, rhs, spec, true);
+        if (rc) return rc;
+        if (cufftExecZ2Z(ctx->plan_y, cs, cs, CUFFT_FORWARD) != CUFFT_SUCCESS)
+            return set_error(ctx, X3D_ECUDA, "cufftExecZ2Z (y lines, forward) failed");
+        rc = launch_poisson_z(ctx, spec, ctx->ny, 0, ctx->nx / 2 + 1, 0, true);
+        if (rc) return rc;
+        if (cufftExecZ2Z(ctx->plan_y, cs, cs, CUFFT_INVERSE) != CUFFT_SUCCESS)
+            return set_error(ctx, X3D_ECUDA, "cufftExecZ2Z (y lines, inverse) failed");
+        return launch_xft(ctx, rhs, spec, false);
+    }
     cufftSetStream(ctx->plan_d2z, ctx->stream);
     cufftSetStream(ctx->plan_z2d, ctx->stream);
     if (cufftExecD2Z(ctx->plan_d2z, rhs, (cufftDoubleComplex *)ctx->spectrum) != CUFFT_SUCCESS)
@@ -650,6 +860,10 @@ void poisson_free(x3d_ctx_s *ctx)
     ctx->d_k2x = nullptr;
     if (ctx->d_zft_tw) cudaFree(ctx->d_zft_tw);
     ctx->d_zft_tw = nullptr;
+    if (ctx->d_xft_tw) cudaFree(ctx->d_xft_tw);
+    ctx->d_xft_tw = nullptr;
+    if (ctx->plan_y_ready) cufftDestroy(ctx->plan_y);
+    ctx->plan_y_ready = false;
     ctx->zfused = false;
     if (ctx->zblk_ready) cufftDestroy(ctx->plan_zblk);
     ctx->zblk_ready = false;

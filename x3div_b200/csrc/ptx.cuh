@@ -4,9 +4,15 @@
 #pragma once
 
 #include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <cstdint>
 
 namespace x3d {
+
+// The driver's cuTensorMapEncodeTiled, looked up once (nullptr where the
+// driver lacks it; the TMA kernels are then not used).
+PFN_cuTensorMapEncodeTiled_v12000 encode_tiled();
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
 {

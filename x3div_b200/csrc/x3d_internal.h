@@ -110,7 +110,15 @@ struct x3d_ctx_s {
     bool plans_ready = false;
     bool zfused = false;
     bool zfuse_allowed = true;  // cleared to force the 3-D cuFFT path
-    double *d_zft_tw = nullptr;  // e^{-2 pi i t / nz}, t < nz (complex)
+    double *d_zft_tw = nullptr;  // e^{-2 pi i t / nz}, t < nz, then (tz, k2z) of each z mode (complex)
+    // Own x transforms (nx / 2 a fused-transform length, with zfused): real
+    // x lines to a spectrum stored (nz, nx/2 + 1, ny) with y fastest, 1-D
+    // cuFFT transforms along the contiguous y lines, the fused z kernel on
+    // that layout, and back.  d_xft_tw: e^{-2 pi i t / (nx/2)}, t < nx/2, then
+    // e^{-2 pi i k / nx}, k <= nx/2 (complex).
+    double *d_xft_tw = nullptr;
+    cufftHandle plan_y = 0;
+    bool plan_y_ready = false;
     // batched 1-D z transforms of one rank's block of the half spectrum, for
     // z lengths without a fused kernel (nxl x modes, nyl y rows)
     cufftHandle plan_zblk = 0;
