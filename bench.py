@@ -59,9 +59,13 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--profile-timed", nargs="?", const="sweep", default=None,
-                    choices=["sweep", "euler", "euler64", "b48"],
-                    help="bracket the timed FP32 sweep (or the FP32-mixed Euler steps, the FP64 ones, or "
-                         "the batch replays) with cudaProfilerStart/Stop, for ncu --profile-from-start off")
+                    choices=["sweep", "euler", "euler64", "b48", "poisson"],
+                    help="bracket the timed FP32 sweep (or the FP32-mixed Euler steps, the FP64 ones, the "
+                         "batch replays, or the --poisson-times solves through the own x transforms) with "
+                         "cudaProfilerStart/Stop, for ncu --profile-from-start off")
+    ap.add_argument("--poisson-times", action="store_true",
+                    help="only time the FP64 Poisson solve on an n^3 box, through the library's own x "
+                         "transforms and through cuFFT's 2-D (x, y) transforms, and print one JSON line")
     ap.add_argument("--kernel-config", type=int, default=None,
                     help="force one kernel configuration (x3d_ctx_set_kernel) instead of autotuning")
     ap.add_argument("--no-b48", action="store_true")
@@ -372,6 +376,40 @@ def timed_sweep(ctx, torch, fields, outs, steps, warmup, world, fused=True, per_
     return ms, fam, sum(len(g) for _, g in groups), launches, group
 
 
+def poisson_times(torch, n, steps, warmup, profile=False, seed=7):
+    """One FP64 x3d_poisson solve on an n^3 periodic box of side 2 pi (a
+    seeded N(0, 1) right-hand side, solved in place), timed with CUDA events
+    over `steps` solves after `warmup`: through the library's own x
+    transforms (the default) and through cuFFT's 2-D (x, y) transforms
+    around the same fused z kernel (stage choice poisson_x = 0)."""
+    from x3div_b200 import Context
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    base = torch.randn(n, n, n, dtype=torch.float64, device="cuda", generator=gen)
+    out = {}
+    for name, choice in (("own_x_transforms", -1), ("cufft_2d_xy", 0)):
+        ctx = Context(n, n, n, lengths=(2 * np.pi,) * 3, precision="f64", stream=torch.cuda.current_stream())
+        ctx.set_stage_choice("poisson_x", choice)
+        rhs = base.clone()
+        for _ in range(warmup):
+            ctx.poisson(rhs)
+        torch.cuda.synchronize()
+        prof = profile and choice == -1
+        if prof:
+            torch.cuda.profiler.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            ctx.poisson(rhs)
+        e1.record()
+        torch.cuda.synchronize()
+        if prof:
+            torch.cuda.profiler.stop()
+        out[name] = round(e0.elapsed_time(e1) / steps, 4)
+        ctx.close()
+        del rhs
+    return {"poisson_ms": out, "grid": [n, n, n], "steps": steps, "warmup": warmup, "dtype": "f64"}
+
+
 def run_c5(torch, n=768, steps=20, dt=5e-4, seed=5):
     """Long-run check at 768^3: 20 Euler steps (dt = 5e-4) from the same
     Taylor-Green + N(0, (1e-3)^2) field with FP32 derivatives (FP64 Poisson)
@@ -668,6 +706,13 @@ def main():
         if world > 1:
             import torch.distributed as dist
             dist.destroy_process_group()
+        return
+    if args.poisson_times:
+        if rank == 0:
+            import torch
+            torch.cuda.set_device(local)
+            print(json.dumps(poisson_times(torch, args.n, args.steps, args.warmup,
+                                           profile=args.profile_timed == "poisson")), flush=True)
         return
     res, pts_step = run_b200(args, world, rank, local)
     if rank == 0:
