@@ -65,3 +65,108 @@ def test_merge_is_the_unnormalised_c2r_transform(n):
     got[0::2], got[1::2] = zi.real, zi.imag
     ref = np.fft.irfft(g, n) * n
     assert np.abs(got - ref).max() <= 1e-14 * np.abs(ref).max()
+
+
+# --- the split fused into the last Stockham stage (k_rfft_x) and the merge
+# into the first inverse stage (k_irfft_x), for lengths whose last radix R is
+# 2, 3 or 4: one thread takes butterflies a = i and b = M/R - i (a = 0 with b =
+# M/(2R)), whose outputs hold each other's partners M - k.
+
+def radix_seq(n, reverse=False):
+    r, m = [], n
+    while m % 8 == 0 and m > 1:
+        r.append(8)
+        m //= 8
+    for f in (4, 2):
+        while m % f == 0:
+            r.append(f)
+            m //= f
+    while m % 3 == 0:
+        r.append(3)
+        m //= 3
+    return r[::-1] if reverse else r
+
+
+def stockham_stage(x, r, ns, inverse):
+    """One Stockham stage of radix r over sub-transforms of ns, as zft_stage."""
+    n, s = len(x), (1 if inverse else -1)
+    y = np.empty_like(x)
+    for j in range(n // r):
+        jm = j % ns
+        v = np.array([x[j + q * (n // r)] * np.exp(s * 2j * np.pi * q * jm / (ns * r)) for q in range(r)])
+        out = np.fft.ifft(v) * r if inverse else np.fft.fft(v)
+        for q in range(r):
+            y[(j // ns) * ns * r + jm + q * ns] = out[q]
+    return y
+
+
+def paired_items(nsl):
+    return [(i, nsl - i if i else nsl // 2) for i in range(nsl // 2)]
+
+
+PAIRED = [n for n in LENGTHS if radix_seq(n // 2)[-1] <= 4 and (n // 2 // radix_seq(n // 2)[-1]) % 2 == 0]
+
+
+@pytest.mark.parametrize("n", PAIRED)
+def test_paired_last_stage_is_the_real_transform(n):
+    m = n // 2
+    seq = radix_seq(m)
+    r, nsl = seq[-1], m // seq[-1]
+    f = np.random.default_rng(n + 2).standard_normal(n)
+    x, ns = f[0::2] + 1j * f[1::2], 1
+    for rr in seq[:-1]:
+        x = stockham_stage(x, rr, ns, False)
+        ns *= rr
+    wx = np.exp(-2j * np.pi * np.arange(m + 1) / n)
+    out = np.full(m + 1, np.nan, dtype=complex)
+
+    def butterfly(j):
+        return np.fft.fft([x[j + q * nsl] * np.exp(-2j * np.pi * q * j / m) for q in range(r)])
+
+    for i, (a, b) in enumerate(paired_items(nsl)):
+        ya, yb = butterfly(a), butterfly(b)
+        for q in range(r):
+            pa = yb[r - 1 - q] if i else ya[(r - q) % r]
+            pb = ya[r - 1 - q] if i else yb[r - 1 - q]
+            for j, y, p in ((a, ya, pa), (b, yb, pb)):
+                k = j + q * nsl
+                out[k] = 0.5 * (y[q] + np.conj(p)) - 0.5j * wx[k] * (y[q] - np.conj(p))
+        if i == 0:
+            out[m] = 0.5 * (ya[0] + np.conj(ya[0])) - 0.5j * wx[m] * (ya[0] - np.conj(ya[0]))
+    ref = np.fft.rfft(f)
+    assert np.abs(out - ref).max() <= 1e-14 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("n", PAIRED)
+def test_paired_first_inverse_stage_is_the_c2r_transform(n):
+    m = n // 2
+    seq = radix_seq(m, reverse=True)
+    r, nsl = seq[0], m // seq[0]
+    g = np.fft.rfft(np.random.default_rng(n + 3).standard_normal(n))
+    wx = np.exp(-2j * np.pi * np.arange(m + 1) / n)
+    x = np.full(m, np.nan, dtype=complex)
+
+    def merge(k, kp):
+        return (g[k] + np.conj(g[kp])) + 1j * np.conj(wx[k]) * (g[k] - np.conj(g[kp]))
+
+    for i, (a, b) in enumerate(paired_items(nsl)):
+        for j in (a, b):
+            z = []
+            for q in range(r):
+                k = j + q * nsl
+                if j == 0:
+                    kp = m if q == 0 else ((r - q) % r) * nsl
+                else:
+                    kp = (nsl - j) + (r - 1 - q) * nsl
+                assert k + kp == m or (k + kp) % m == 0
+                z.append(merge(k, kp))
+            out = np.fft.ifft(z) * r  # sub-transforms of size 1: no twiddles
+            x[j * r: j * r + r] = out
+    ns = r
+    for rr in seq[1:]:
+        x = stockham_stage(x, rr, ns, True)
+        ns *= rr
+    got = np.empty(n)
+    got[0::2], got[1::2] = x.real, x.imag
+    ref = np.fft.irfft(g, n) * n
+    assert np.abs(got - ref).max() <= 1e-14 * np.abs(ref).max()

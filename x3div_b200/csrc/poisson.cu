@@ -315,11 +315,13 @@ constexpr RadixSeq radix_seq(int n, bool reversed = false)
 // transform alone (!INV: lines from global memory, the transform left in
 // buf in natural order) or the inverse alone (INV: from buf to global
 // memory).
-template <int N, int W, bool INV, bool SOLVE = true, int NT = kZftThreads, int ST = 0, int NS = 1>
+// Stages ST .. END - 1 only where END >= 0 (a stage before the sequence's
+// last then writes shared memory and ends with a barrier).
+template <int N, int W, bool INV, bool SOLVE = true, int NT = kZftThreads, int ST = 0, int NS = 1, int END = -1>
 __device__ __forceinline__ void zft(double2 *buf, const double2 *tw, const ZLines &zl)
 {
     constexpr RadixSeq seq = radix_seq(N, INV);
-    if constexpr (ST < seq.count) {
+    if constexpr (ST < (END < 0 ? seq.count : END)) {
         constexpr int R = seq.r[ST];
         constexpr bool last = ST + 1 == seq.count;
         if constexpr (SOLVE && !INV && last) {
@@ -327,7 +329,7 @@ __device__ __forceinline__ void zft(double2 *buf, const double2 *tw, const ZLine
             zft<N, W, true, true, NT, 1, R>(buf, tw, zl);  // the inverse from its second stage
         } else {
             zft_stage<N, R, NS, W, INV, !INV && ST == 0, INV && last, false, NT>(buf, tw, zl);
-            zft<N, W, INV, SOLVE, NT, ST + 1, NS * R>(buf, tw, zl);
+            zft<N, W, INV, SOLVE, NT, ST + 1, NS * R, END>(buf, tw, zl);
         }
     }
 }
@@ -412,6 +414,59 @@ constexpr int kXftW = 4;
 template <int M>
 constexpr int kXftThreads = (((M % 3 ? kXftW * M / 8 : kXftW * M / 6) + 31) / 32) * 32;
 
+// The last radix R of a length-M forward transform (the first of the
+// inverse).  Where R <= 4 and M / R is even, the split runs inside the last
+// forward stage and the merge inside the first inverse one: the partner M - k
+// of a mode k = j + q M/R (0 < j < M/R) is mode (M/R - j) + (R - 1 - q) M/R,
+// an output of butterfly M/R - j, and butterfly 0 holds its own partners
+// (q -> R - q); so one thread takes butterflies j and M/R - j (0 and M/(2R)
+// together) and splits or merges in registers, one shared-memory pass fewer
+// each way.  Radix-8 last stages keep the separate pass (16 complex values a
+// thread do not fit the 64 registers).
+template <int M>
+constexpr int kXftLastR = radix_seq(M).r[radix_seq(M).count - 1];
+template <int M>
+constexpr bool kXftPaired = kXftLastR<M> <= 4 && (M / kXftLastR<M>) % 2 == 0;
+
+// F[k] = (A + B) / 2 - i w (A - B) / 2 with B = conj(zp), w = e^{-2 pi i k / n}
+__device__ __forceinline__ double2 split_mode(double2 a, double2 zp, double2 w)
+{
+    const double2 e = make_double2(0.5 * (a.x + zp.x), 0.5 * (a.y - zp.y));
+    const double2 d = make_double2(0.5 * (a.x - zp.x), 0.5 * (a.y + zp.y));
+    const double2 wd = cmul(w, d);
+    return make_double2(e.x + wd.y, e.y - wd.x);
+}
+
+// Z[k] = (G[k] + conj(gp)) + i conj(w) (G[k] - conj(gp)), gp = G[M - k]
+__device__ __forceinline__ double2 merge_mode(double2 g, double2 gp, double2 w)
+{
+    const double2 e = make_double2(g.x + gp.x, g.y - gp.y);
+    const double2 d = make_double2(g.x - gp.x, g.y + gp.y);
+    const double2 od = cmul(make_double2(w.x, -w.y), d);
+    return make_double2(e.x - od.y, e.y + od.x);
+}
+
+// Butterfly j of the last forward stage (sub-transforms of M/R, twiddle
+// stride 1) for line l: y[q] = Z[j + q M/R].
+template <int M, int R, int W>
+__device__ __forceinline__ void last_butterfly(const double2 *buf, const double2 *tw, int j, int l, double2 (&y)[R])
+{
+    constexpr int NSL = M / R;
+    const double2 w1 = tw[j];
+    double2 wq = w1;
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+        const double2 x = buf[(j + q * NSL) * W + l];
+        if (q == 0) {
+            y[q] = x;
+        } else {
+            y[q] = cmul(x, wq);
+            wq = cmul(wq, w1);
+        }
+    }
+    dft<R, false>(y);
+}
+
 template <int M>
 __global__ void __launch_bounds__(kXftThreads<M>, 1024 / kXftThreads<M>)
     k_rfft_x(const double *__restrict__ f, double2 *__restrict__ spec, int ny, const double2 *__restrict__ tw)
@@ -428,8 +483,31 @@ __global__ void __launch_bounds__(kXftThreads<M>, 1024 / kXftThreads<M>)
     zl.zstride = 1;
     zl.lstride = M;
     zl.lines = min(W, ny - j0);
-    zft<M, W, false, false, NT>(zbuf, tw, zl);  // Z of each row, natural order, in zbuf
     double2 *const out = spec + (size_t)kz * (M + 1) * ny + j0;
+    if constexpr (kXftPaired<M>) {
+        constexpr RadixSeq seq = radix_seq(M);
+        constexpr int R = kXftLastR<M>, NSL = M / R;
+        zft<M, W, false, false, NT, 0, 1, seq.count - 1>(zbuf, tw, zl);  // every stage but the last
+        for (int it = threadIdx.x; it < W * (NSL / 2); it += NT) {
+            const int l = it % W, i = it / W;
+            if (l >= zl.lines) continue;
+            const int a = i, b = i > 0 ? NSL - i : NSL / 2;  // butterflies a and b, partners of each other
+            double2 ya[R], yb[R];
+            last_butterfly<M, R, W>(zbuf, tw, a, l, ya);
+            last_butterfly<M, R, W>(zbuf, tw, b, l, yb);
+#pragma unroll
+            for (int q = 0; q < R; ++q) {
+                // Z[M - k] of k = a + q M/R and of k = b + q M/R
+                const double2 pa = i > 0 ? yb[R - 1 - q] : ya[(R - q) % R];
+                const double2 pb = i > 0 ? ya[R - 1 - q] : yb[R - 1 - q];
+                out[(size_t)(a + q * NSL) * ny + l] = split_mode(ya[q], pa, __ldg(wx + a + q * NSL));
+                out[(size_t)(b + q * NSL) * ny + l] = split_mode(yb[q], pb, __ldg(wx + b + q * NSL));
+            }
+            if (i == 0) out[(size_t)M * ny + l] = split_mode(ya[0], ya[0], __ldg(wx + M));
+        }
+        return;
+    }
+    zft<M, W, false, false, NT>(zbuf, tw, zl);  // Z of each row, natural order, in zbuf
     for (int b = threadIdx.x; b < (M / 2 + 1) * W; b += NT) {
         const int l = b % W, p = b / W, q = (M - p) % M;  // modes p and M - p from Z[p] and Z[q]
         if (l >= zl.lines) continue;
@@ -460,6 +538,57 @@ __global__ void __launch_bounds__(kXftThreads<M>, 1024 / kXftThreads<M>)
     const int j0 = (blockIdx.x - kz * tiles_j) * W;
     const int lines = min(W, ny - j0);
     const double2 *const in = spec + (size_t)kz * (M + 1) * ny + j0;
+    ZLines zl;
+    zl.base = reinterpret_cast<double2 *>(f) + ((size_t)kz * ny + j0) * M;
+    zl.zstride = 1;
+    zl.lstride = M;
+    zl.lines = lines;
+    if constexpr (kXftPaired<M>) {
+        constexpr int R = kXftLastR<M>, NSL = M / R;  // the inverse's first radix
+        static_assert(radix_seq(M, true).r[0] == R, "the inverse takes the radices in reverse order");
+        for (int it = threadIdx.x; it < W * (NSL / 2); it += NT) {
+            const int l = it % W, i = it / W;
+            const int a = i, b = i > 0 ? NSL - i : NSL / 2;
+            double2 ga[R], gb[R], gm = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int q = 0; q < R; ++q) ga[q] = gb[q] = gm;
+            if (l < lines) {
+#pragma unroll
+                for (int q = 0; q < R; ++q) {
+                    ga[q] = in[(size_t)(a + q * NSL) * ny + l];
+                    gb[q] = in[(size_t)(b + q * NSL) * ny + l];
+                }
+                if (i == 0) gm = in[(size_t)M * ny + l];
+            }
+            // merged in place, a mode and its partner together
+            auto pair = [&](double2 &g1, double2 &g2, int k1, int k2) {
+                const double2 x1 = g1, x2 = g2;
+                g1 = merge_mode(x1, x2, __ldg(wx + k1));
+                if (k2 != k1) g2 = merge_mode(x2, x1, __ldg(wx + k2));
+            };
+            if (i > 0) {  // partner of a + q M/R is b + (R - 1 - q) M/R
+#pragma unroll
+                for (int q = 0; q < R; ++q) pair(ga[q], gb[R - 1 - q], a + q * NSL, b + (R - 1 - q) * NSL);
+            } else {  // butterfly 0: q M/R and (R - q) M/R, and 0 with M; butterfly M/(2R) as above
+                const double2 g0 = merge_mode(ga[0], gm, __ldg(wx));
+#pragma unroll
+                for (int q = 1; 2 * q <= R; ++q) pair(ga[q], ga[R - q], q * NSL, (R - q) * NSL);
+                ga[0] = g0;
+#pragma unroll
+                for (int q = 0; 2 * q < R; ++q) pair(gb[q], gb[R - 1 - q], b + q * NSL, b + (R - 1 - q) * NSL);
+            }
+            dft<R, true>(ga);  // the inverse's first stage: sub-transforms of size 1, no twiddles
+            dft<R, true>(gb);
+#pragma unroll
+            for (int q = 0; q < R; ++q) {
+                zbuf[(a * R + q) * W + l] = ga[q];
+                zbuf[(b * R + q) * W + l] = gb[q];
+            }
+        }
+        __syncthreads();
+        zft<M, W, true, false, NT, 1, R>(zbuf, tw, zl);  // the inverse from its second stage
+        return;
+    }
     for (int b = threadIdx.x; b < (M / 2 + 1) * W; b += NT) {
         const int l = b % W, p = b / W, q = M - p;  // Z[p] and Z[q] (q < M) from G[p] and G[q]
         double2 gp = make_double2(0.0, 0.0), gq = gp;
@@ -480,11 +609,6 @@ __global__ void __launch_bounds__(kXftThreads<M>, 1024 / kXftThreads<M>)
         }
     }
     __syncthreads();
-    ZLines zl;
-    zl.base = reinterpret_cast<double2 *>(f) + ((size_t)kz * ny + j0) * M;
-    zl.zstride = 1;
-    zl.lstride = M;
-    zl.lines = lines;
     zft<M, W, true, false, NT>(zbuf, tw, zl);  // the inverse, its last stage to the rows
 }
 
