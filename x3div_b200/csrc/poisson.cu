@@ -92,12 +92,14 @@ __global__ void k_spectral_divide(double2 *c, unsigned nxl, unsigned nyl, unsign
 
 // ---------------------------------------------------------------------------
 // z transforms fused with the mode division.  The 3-D transform of the
-// (nz, ny, nx) field separates into 2-D (x, y) transforms of each z plane,
-// which cuFFT does batched, and 1-D transforms along z of each (i, j) line of
-// the half spectrum.  One kernel takes a tile of W x-adjacent z lines into
-// shared memory, transforms them forward along z, divides each mode, and
-// transforms them back, so the spectrum crosses HBM once for all three steps
-// (cuFFT's z passes and a separate division kernel cross it three times).
+// (nz, ny, nx) field separates into 1-D transforms along x, y and z: the
+// library's own real x transforms (below) and batched 1-D cuFFT transforms
+// along y, or cuFFT's 2-D (x, y) transforms of each z plane, then the z
+// lines of the half spectrum.  One kernel takes a tile of W lane-adjacent z
+// lines into shared memory, transforms them forward along z, divides each
+// mode, and transforms them back, so the spectrum crosses HBM once for all
+// three steps (cuFFT's z passes and a separate division kernel cross it
+// three times).
 //
 // The z transforms are mixed-radix Stockham autosort FFTs (radix 8, 4, 2,
 // then 3), the formulation of Govindaraju et al., "High performance discrete
