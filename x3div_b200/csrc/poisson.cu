@@ -448,6 +448,20 @@ __device__ __forceinline__ double2 merge_mode(double2 g, double2 gp, double2 w)
     return make_double2(e.x - od.y, e.y + od.x);
 }
 
+// e^{-i pi q / R}, q < R: the factor between e^{-2 pi i j / n} and
+// e^{-2 pi i (j + q M/R) / n} (n = 2M), so a butterfly's split or merge
+// reads one table entry and scales it (q is a constant once unrolled).
+template <int R>
+__device__ __forceinline__ double2 half_turn(int q)
+{
+    constexpr double s2 = 0.70710678118654752440;  // sqrt(1/2)
+    constexpr double s3 = 0.86602540378443864676;  // sqrt(3)/2
+    if (q == 0) return make_double2(1.0, 0.0);
+    if constexpr (R == 2) return make_double2(0.0, -1.0);
+    if constexpr (R == 3) return q == 1 ? make_double2(0.5, -s3) : make_double2(-0.5, -s3);
+    return q == 1 ? make_double2(s2, -s2) : (q == 2 ? make_double2(0.0, -1.0) : make_double2(-s2, -s2));
+}
+
 // Butterfly j of the last forward stage (sub-transforms of M/R, twiddle
 // stride 1) for line l: y[q] = Z[j + q M/R].
 template <int M, int R, int W>
@@ -497,15 +511,17 @@ __global__ void __launch_bounds__(kXftThreads<M>, 1024 / kXftThreads<M>)
             double2 ya[R], yb[R];
             last_butterfly<M, R, W>(zbuf, tw, a, l, ya);
             last_butterfly<M, R, W>(zbuf, tw, b, l, yb);
+            const double2 wa = __ldg(wx + a), wb = __ldg(wx + b);
 #pragma unroll
             for (int q = 0; q < R; ++q) {
                 // Z[M - k] of k = a + q M/R and of k = b + q M/R
                 const double2 pa = i > 0 ? yb[R - 1 - q] : ya[(R - q) % R];
                 const double2 pb = i > 0 ? ya[R - 1 - q] : yb[R - 1 - q];
-                out[(size_t)(a + q * NSL) * ny + l] = split_mode(ya[q], pa, __ldg(wx + a + q * NSL));
-                out[(size_t)(b + q * NSL) * ny + l] = split_mode(yb[q], pb, __ldg(wx + b + q * NSL));
+                const double2 h = half_turn<R>(q);
+                out[(size_t)(a + q * NSL) * ny + l] = split_mode(ya[q], pa, q ? cmul(wa, h) : wa);
+                out[(size_t)(b + q * NSL) * ny + l] = split_mode(yb[q], pb, q ? cmul(wb, h) : wb);
             }
-            if (i == 0) out[(size_t)M * ny + l] = split_mode(ya[0], ya[0], __ldg(wx + M));
+            if (i == 0) out[(size_t)M * ny + l] = split_mode(ya[0], ya[0], make_double2(-1.0, 0.0));
         }
         return;
     }
@@ -562,22 +578,30 @@ __global__ void __launch_bounds__(kXftThreads<M>, 1024 / kXftThreads<M>)
                 }
                 if (i == 0) gm = in[(size_t)M * ny + l];
             }
-            // merged in place, a mode and its partner together
-            auto pair = [&](double2 &g1, double2 &g2, int k1, int k2) {
+            // merged in place, a mode and its partner together; the table
+            // entry of mode j + q M/R is wx[j] times half_turn(q)
+            const double2 wa = __ldg(wx + a), wb = __ldg(wx + b);
+            auto pair = [&](double2 &g1, double2 &g2, double2 w1, double2 w2, bool self) {
                 const double2 x1 = g1, x2 = g2;
-                g1 = merge_mode(x1, x2, __ldg(wx + k1));
-                if (k2 != k1) g2 = merge_mode(x2, x1, __ldg(wx + k2));
+                g1 = merge_mode(x1, x2, w1);
+                if (!self) g2 = merge_mode(x2, x1, w2);
             };
+            auto scaled = [](double2 w, int q, double2 h) { return q ? cmul(w, h) : w; };
             if (i > 0) {  // partner of a + q M/R is b + (R - 1 - q) M/R
 #pragma unroll
-                for (int q = 0; q < R; ++q) pair(ga[q], gb[R - 1 - q], a + q * NSL, b + (R - 1 - q) * NSL);
+                for (int q = 0; q < R; ++q)
+                    pair(ga[q], gb[R - 1 - q], scaled(wa, q, half_turn<R>(q)),
+                         scaled(wb, R - 1 - q, half_turn<R>(R - 1 - q)), false);
             } else {  // butterfly 0: q M/R and (R - q) M/R, and 0 with M; butterfly M/(2R) as above
-                const double2 g0 = merge_mode(ga[0], gm, __ldg(wx));
+                const double2 g0 = merge_mode(ga[0], gm, make_double2(1.0, 0.0));
 #pragma unroll
-                for (int q = 1; 2 * q <= R; ++q) pair(ga[q], ga[R - q], q * NSL, (R - q) * NSL);
+                for (int q = 1; 2 * q <= R; ++q)
+                    pair(ga[q], ga[R - q], half_turn<R>(q), half_turn<R>(R - q), 2 * q == R);
                 ga[0] = g0;
 #pragma unroll
-                for (int q = 0; 2 * q < R; ++q) pair(gb[q], gb[R - 1 - q], b + q * NSL, b + (R - 1 - q) * NSL);
+                for (int q = 0; 2 * q < R; ++q)
+                    pair(gb[q], gb[R - 1 - q], scaled(wb, q, half_turn<R>(q)),
+                         scaled(wb, R - 1 - q, half_turn<R>(R - 1 - q)), 2 * q == R - 1);
             }
             dft<R, true>(ga);  // the inverse's first stage: sub-transforms of size 1, no twiddles
             dft<R, true>(gb);
